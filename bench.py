@@ -1,0 +1,332 @@
+#!/usr/bin/env python
+"""Benchmark of the LBcuda hot path on B200.
+
+Workload (one GPU): two-component colour-gradient spinodal decomposition,
+128^3 periodic, rhoR = rhoB = 0.5 + U(-0.01, 0.01) per cell from seed 1,
+tauR = tauB = 1, sigma = 0.02, beta = 0.7.  One bench step = 500 lattice
+steps (nIterOut of the reference's own 128^3 deck, Tests/CPC_Tab2_128/
+input.dat, the interval at which it prints Mlup/s); the default 20 timed
+steps are the 10,000 steps of the workload.  Headline: MLUPS (interior
+cells, 10^6 lattice-cell updates per second) with FP16 shifted storage;
+the FP32-storage run, the errors against an FP64 run and the roofline are
+reported beside it.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 (torchrun): every rank advances its own independent box (replicas,
+weak scaling, no data-path collective); the time is the max over ranks.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+L = 128
+SEED = 1
+SIGMA, BETA = 0.02, 0.7
+LB_PER_STEP = 500
+BYTES_PER_CELL = {"f16": 160, "bf16": 160, "f32": 312, "f64": 616}  # algorithmic bytes per cell-step
+MINIMAL_BYTES = {"f16": 152, "bf16": 152, "f32": 304, "f64": 608}   # populations only (phi kept on chip)
+METRIC = "MLUPS (FP16-shifted storage, colour-gradient 128^3)"
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = str(index)
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-i", self.index, "-lms", "200"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def reference_arm(args, ws, rank):
+    """The oracle (CPU restatement of the reference) on all host cores."""
+    if rank != 0:
+        return 0
+    from oracle.orc import OracleSim, num_threads
+    from lbcuda_b200 import make_params
+    from lbcuda_b200.inputs import seeded_noise_fields
+    p = make_params(L, model="cg", storage="f32", sigma=SIGMA, beta=BETA)
+    rR, rB = seeded_noise_fields(L, L, L, seed=SEED)
+    o = OracleSim(p, "ref")
+    o.set_fields(rR, rB)
+    per = 2  # lattice steps per bench step: a bounded sample of the workload
+    for _ in range(args.warmup):
+        o.step(per)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        o.step(per)
+    dt = time.perf_counter() - t0
+    mlups = args.steps * per * L ** 3 / dt / 1e6
+    line = {
+        "impl": "reference", "metric": METRIC, "value": mlups, "unit": "MLUPS", "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "colour-gradient spinodal 128^3, sigma=0.02, beta=0.7, tau=1",
+                   "lattice_steps_per_bench_step": per, "storage": "f32"},
+        "cpu_baseline": {"value": mlups, "unit": "MLUPS", "cores": num_threads(), "kind": "port",
+                         "sample": f"{args.steps} x {per} lattice steps of 128^3 after {args.warmup} x {per} warm-up"},
+        "e2e": {"value": mlups, "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def cpu_baseline_sample():
+    from oracle.orc import OracleSim, num_threads
+    from lbcuda_b200 import make_params
+    from lbcuda_b200.inputs import seeded_noise_fields
+    p = make_params(L, model="cg", storage="f32", sigma=SIGMA, beta=BETA)
+    rR, rB = seeded_noise_fields(L, L, L, seed=SEED)
+    o = OracleSim(p, "ref")
+    o.set_fields(rR, rB)
+    o.step(1)
+    n = 0
+    t0 = time.perf_counter()
+    while time.perf_counter() - t0 < 10.0:
+        o.step(1)
+        n += 1
+    dt = time.perf_counter() - t0
+    return {"value": n * L ** 3 / dt / 1e6, "unit": "MLUPS", "cores": num_threads(), "kind": "port",
+            "sample": f"{n} lattice steps of the 128^3 workload (about 10 s), FP32, OpenMP"}
+
+
+def error_vs_f64(nsteps_list=(1000, 10000)):
+    """Relative L2 error of |u| and phi of each storage against the FP64-storage run."""
+    from lbcuda_b200 import LBSim, make_params
+    from lbcuda_b200.inputs import seeded_noise_fields
+    rR, rB = seeded_noise_fields(L, L, L, seed=SEED)
+    out = {}
+    sims = {}
+    for st in ("f64", "f32", "f16", "bf16"):
+        s = LBSim(make_params(L, model="cg", storage=st, sigma=SIGMA, beta=BETA))
+        s.set_fields(rR, rB)
+        sims[st] = s
+    done = 0
+    for n in nsteps_list:
+        res = {}
+        for st, s in sims.items():
+            s.step(n - done)
+            res[st] = s.get_fields(f64=True)
+        done = n
+        u64, p64 = res["f64"][2], res["f64"][3]
+        m64 = res["f64"][0].sum() + res["f64"][1].sum()
+        for st in ("f32", "f16", "bf16"):
+            eu = float(np.linalg.norm(res[st][2] - u64) / np.linalg.norm(u64))
+            ep = float(np.linalg.norm(res[st][3] - p64) / np.linalg.norm(p64))
+            out.setdefault(st, {})[f"after_{n}"] = {"u_rel_l2": eu, "phi_rel_l2": ep}
+        out.setdefault("f64", {})[f"after_{n}"] = {"mass": float(m64)}
+    for s in sims.values():
+        s.close()
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-extras", action="store_true", help="skip the error runs and the CPU baseline")
+    args = ap.parse_args()
+    ws, rank, local = dist_env()
+    if args.impl == "reference":
+        return reference_arm(args, ws, rank)
+
+    import torch
+    torch.cuda.set_device(local)
+    pg = None
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        pg = dist
+
+    from lbcuda_b200 import LBSim, make_params
+    from lbcuda_b200.inputs import seeded_noise_fields
+
+    rR, rB = seeded_noise_fields(L, L, L, seed=SEED + rank)
+    hbm, peak_kind = peaks()
+
+    def barrier():
+        torch.cuda.synchronize()
+        if pg is not None:
+            pg.barrier()
+
+    def run_storage(storage, timed_steps, warm):
+        s = LBSim(make_params(L, model="cg", storage=storage, sigma=SIGMA, beta=BETA))
+        s.set_fields(rR, rB)
+        for _ in range(warm):
+            s.step(LB_PER_STEP)
+        s.sync()
+        barrier()
+        clk = Clocks(local)
+        clk.start()
+        total_ms, kernel_ms, launches = s.time_steps(timed_steps * LB_PER_STEP, kernel_timing=True)
+        clocks = clk.stop()
+        barrier()
+        code = s.status()[0]
+        s.close()
+        return total_ms, kernel_ms, launches, clocks, code
+
+    # headline: FP16 shifted storage
+    tot16, k16, n16, clocks, code16 = run_storage("f16", args.steps, args.warmup)
+    tot32, k32, n32, _, code32 = run_storage("f32", args.steps, args.warmup)
+
+    def maxr(v):
+        if pg is None:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        return float(t.item())
+
+    tot16, tot32 = maxr(tot16), maxr(tot32)
+    cells = L ** 3
+    lb_steps = args.steps * LB_PER_STEP
+    mlups16 = ws * cells * lb_steps / (tot16 * 1e-3) / 1e6
+    mlups32 = ws * cells * lb_steps / (tot32 * 1e-3) / 1e6
+
+    def roofline(storage, kernel_ms, launches):
+        per_launch_ms = kernel_ms / max(launches, 1)
+        alg = BYTES_PER_CELL[storage] * cells
+        achieved = alg / (per_launch_ms * 1e-3) / 1e9
+        return {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                "traffic": None, "peak_kind": peak_kind, "kernel": "k_cg_fused", "bytes_per_cell": BYTES_PER_CELL[storage],
+                "kernel_us_per_launch": per_launch_ms * 1e3,
+                "minimal_bytes_frac": MINIMAL_BYTES[storage] * cells / (per_launch_ms * 1e-3) / 1e9 / hbm}
+
+    # e2e through the public API with host buffers: upload the fields from
+    # pinned memory, run one bench step of lattice steps, read the fields back
+    pin = lambda shape: torch.empty(shape, dtype=torch.float32, pin_memory=True).numpy()
+    hR, hB = pin((L, L, L)), pin((L, L, L))
+    hR[...] = rR
+    hB[...] = rB
+    s = LBSim(make_params(L, model="cg", storage="f16", sigma=SIGMA, beta=BETA))
+    import ctypes
+    fp = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+    oR, oB, oV, oP = pin((L, L, L)), pin((L, L, L)), pin((L, L, L, 3)), pin((L, L, L))
+    lib = s._L
+
+    def e2e_step():
+        lib.lbx_set_fields(s._h, fp(hR), fp(hB), 0.0, 0.0, 0.0)
+        lib.lbx_step(s._h, LB_PER_STEP)
+        rc = lib.lbx_get_fields(s._h, fp(oR), fp(oB), fp(oV), fp(oP))
+        if rc:
+            raise RuntimeError(f"lbx_get_fields {rc}")
+
+    for _ in range(args.warmup):
+        e2e_step()
+    barrier()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0 = time.perf_counter()
+    ev0.record()
+    for _ in range(args.steps):
+        e2e_step()
+    ev1.record()
+    barrier()
+    e2e_wall = time.perf_counter() - t0
+    e2e_ms = maxr(e2e_wall * 1e3)
+    s.close()
+    e2e_mlups = ws * cells * lb_steps / (e2e_ms * 1e-3) / 1e6
+
+    extras = {}
+    if rank == 0 and not args.no_extras:
+        extras["error_vs_f64"] = error_vs_f64()
+        extras["cpu_baseline"] = cpu_baseline_sample()
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": mlups16, "unit": "MLUPS", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": tot16 / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f16 storage / f32 arithmetic", "data": "synthetic",
+            "config": {"workload": "colour-gradient spinodal 128^3 periodic, rho=0.5+U(-0.01,0.01) seed 1, "
+                                   "tau=1, sigma=0.02, beta=0.7",
+                       "lattice_steps_per_bench_step": LB_PER_STEP, "storage": "f16 shifted (f - w*0.5)",
+                       "cells": cells, "l2": "inputs larger than L2 (2 x 160 MB population buffers)",
+                       "parallelism": "replicas" if ws > 1 else "single"},
+            "roofline": roofline("f16", k16, n16),
+            "fp32_storage": {"value": mlups32, "unit": "MLUPS", "ms_per_step": tot32 / args.steps,
+                             "roofline": roofline("f32", k32, n32)},
+            "fp16_over_fp32": mlups16 / mlups32,
+            "clocks": clocks,
+            "e2e": {"value": e2e_mlups, "unit": "MLUPS", "h2d_bytes_per_step": 2 * 4 * cells,
+                    "d2h_bytes_per_step": 6 * 4 * cells, "ms_per_step": e2e_ms / args.steps},
+            "gpu_launches": n16 + (n32 if True else 0) + args.steps * (LB_PER_STEP + 2),
+            "device_errors": [code16, code32],
+        }
+        line.update(extras)
+        print(json.dumps(line), flush=True)
+    if pg is not None:
+        pg.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,169 @@
+/*
+ * lbx.h — C ABI of the B200-native LBcuda hot path.
+ *
+ * The reference (LBcuda, CUDA Fortran) drives its kernels from `program TestLB`
+ * (main.CUF:1-316) on module-global device arrays (kernels_fluid.CUF:9-48)
+ * with parameters in Fortran `parameter`s and `constant` memory
+ * (dimensions_m.CUF:1-365, main.CUF:1043-1162).  This header replaces that
+ * surface with an opaque context and plain-pointer entry points that a
+ * Fortran host can bind with ISO_C_BINDING (`bind(C)`, `type(c_ptr)`,
+ * `integer(c_int), value`).  No entry point takes or returns a torch or CUDA
+ * type.
+ *
+ * Conventions
+ *  - Every function returns an int status: 0 = ok, <0 = CUDA/runtime error
+ *    (LBX_ERR_*), >0 = device range-check error raised by a kernel (the
+ *    reference's `stop_d = __LINE__` protocol, main.CUF:2410-2442).  No entry
+ *    point aborts the process.
+ *  - Host field buffers are x-fastest, interior cells only, nx*ny*nz values
+ *    (Fortran order `a(1:nx,1:ny,1:nz)`); vector fields are (3, nx, ny, nz).
+ *  - Population buffers are (nx, ny, nz, Q) x-fastest, Q = 19 (D3Q19, the
+ *    reference default `noD3Q27`, defines.h:8) in the reference lattice order
+ *    (dimensions_m.CUF:211-218).
+ *  - Particle arrays are FP64, (3, n) or (4, n) column-major like the
+ *    reference's pos_d(13,N,2) slices (dimensions_m.CUF:352-360).
+ *  - One context per CUDA stream; calls on one context are not thread-safe.
+ *    lbx_step only enqueues work; lbx_get_*, lbx_sync and lbx_status
+ *    synchronise.
+ */
+#ifndef LBX_H
+#define LBX_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- enumerations ------------------------------------------------------ */
+#define LBX_MODEL_BGK 0 /* single-component BGK (kernels_fluid_BGK.CUF)        */
+#define LBX_MODEL_CG 1  /* two-component colour gradient (kernels_fluid_CG.CUF) */
+
+#define LBX_STORE_F32 0  /* FP32 populations (reference storage)            */
+#define LBX_STORE_F16 1  /* FP16 populations shifted by w_l * rho0           */
+#define LBX_STORE_BF16 2 /* BF16 populations shifted by w_l * rho0           */
+#define LBX_STORE_F64 3  /* FP64 populations and FP64 arithmetic (error runs) */
+
+#define LBX_WET_JANUS 0   /* compute_virtual_rho, kernels_fluid_PART.CUF:299-352 */
+#define LBX_WET_NEUTRAL 1 /* compute_densities_wall, kernels_fluid_PART.CUF:267-297 */
+
+/* cell flags, dimensions_m.CUF:306-310 */
+#define LBX_FLUID_WALL 0
+#define LBX_FLUID_FLUID 1
+#define LBX_FLUID_SPHERELIST 2
+#define LBX_FLUID_SPHEREDEAD 4
+#define LBX_FLUID_PARTICLECM 5
+
+/* host-side error codes (negative) */
+#define LBX_ERR_CUDA (-1)
+#define LBX_ERR_ARG (-2)
+#define LBX_ERR_ALLOC (-3)
+#define LBX_ERR_STATE (-4)
+#define LBX_ERR_TIMEOUT (-5)
+#define LBX_ERR_NOSYM (-6)
+
+/* device error codes (positive, first one wins), each tied to the reference
+ * check it restates */
+#define LBX_DEV_RHO_RANGE 1       /* init_rhoR_CG/init_rhoB_CG, kernels_fluid_CG.CUF:438-441,496-499 */
+#define LBX_DEV_BIG_FORCE 2       /* nve_lf, kernels_fluid_PART.CUF:1532-1537 */
+#define LBX_DEV_EXTREME_VEL 3     /* nve_lf, kernels_fluid_PART.CUF:1545-1549 */
+#define LBX_DEV_POSITION 4        /* nve_lf, kernels_fluid_PART.CUF:1581-1598 */
+#define LBX_DEV_LIST_OVERFLOW 5   /* makeListAtomsGPU, kernels_fluid_PART.CUF:2436-2439 */
+#define LBX_DEV_BELT_RANGE 6      /* compute_onebelt_*, kernels_fluid_PART.CUF:800-803 */
+
+/* ---- parameters -------------------------------------------------------- */
+/* The reference keeps these as compile-time `parameter`s (dimensions_m.CUF:
+ * 50-84) plus the runtime input.dat values (main.CUF:409-496).  Here they are
+ * one runtime struct; lbx_default_params fills the reference values. */
+typedef struct lbx_params {
+  int32_t nx, ny, nz;     /* interior lattice (glx, gly, glz) */
+  int32_t model;          /* LBX_MODEL_* */
+  int32_t storage;        /* LBX_STORE_* */
+  int32_t wetting;        /* LBX_WET_* */
+  int32_t lrotate;        /* particle rotation (input.dat line 9) */
+  int32_t max_particles;  /* capacity of the particle arrays */
+  float tau;              /* BGK relaxation time, omega = 1/tau */
+  float tauR, tauB;       /* CG relaxation times (dimensions_m.CUF:98-99) */
+  float sigma, beta;      /* sigma_CG, beta_CG (dimensions_m.CUF:50) */
+  float rho0R, rho0B;     /* shift densities of the 16-bit storage */
+  float radius;           /* rdim (dimensions_m.CUF:59) */
+  float rmass;            /* 1/mass (dimensions_m.CUF:60) */
+  float max_vel;          /* MAX_PARTICLE_VEL (input.dat line 8) */
+  float ext_force[3];     /* ext_fxx, ext_fyy, ext_fzz */
+  float ext_torque[3];    /* ext_tqx, ext_tqy, ext_tqz */
+  float hz_k, hz_rmin, hz_rcap;             /* Hertz (dimensions_m.CUF:77-80) */
+  int32_t lubrication;                      /* llubrication (dimensions_m.CUF:81) */
+  float lubric_k, lubric_rmin, lubric_rcap; /* dimensions_m.CUF:82-84 */
+  int32_t reserved[8];
+} lbx_params;
+
+/* Fill the reference defaults for an nx*ny*nz periodic box: CG model, FP32
+ * storage, Janus wetting, tau = 1, sigma = 0.1, beta = 0.999, r = 5.5,
+ * rmass = 1/1500, Hertz k = 10, rmin = 10.5, rcap = 9. */
+void lbx_default_params(lbx_params* p, int32_t nx, int32_t ny, int32_t nz);
+
+/* ---- lifetime ---------------------------------------------------------- */
+/* Replaces setupGPUgridAndAlloc + SetConstants (main.CUF:2133-2407,
+ * 1043-1162): allocates every device array of the path and uploads the
+ * lattice tables.  The library owns all device memory. */
+int lbx_create(const lbx_params* p, void** ctx);
+int lbx_destroy(void* ctx);
+
+/* ---- initial conditions ------------------------------------------------ */
+/* setupPops (kernels_fluid_CG.CUF:313-346): equilibrium populations at
+ * density rhoR/rhoB and uniform velocity (vx,vy,vz); all flags fluid.  For
+ * the BGK model rhoB is ignored (may be NULL).  Covers initType 1,2,3,5,6
+ * once the host has built the density fields (main.CUF:2531-2608). */
+int lbx_set_fields(void* ctx, const float* rhoR, const float* rhoB, float vx, float vy, float vz);
+/* initType 4 (read_and_setPops, main.CUF:2489-2529): raw populations. */
+int lbx_set_pops(void* ctx, const float* popsR, const float* popsB);
+
+/* ---- the time step ----------------------------------------------------- */
+/* One or more full steps in the order of main.CUF:125-308 (fluid: moments,
+ * collision, streaming; with particles also flags, fill/drain, wetting,
+ * bounce-back, pair forces and the particle integrator). */
+int lbx_step(void* ctx, int32_t nsteps);
+/* Kernel-level entries of the same step, for callers that drive the order
+ * themselves (the reference's host does, main.CUF:130-271). */
+int lbx_init_rho(void* ctx);          /* init_rhoR_CG + init_rhoB_CG (+ periodic rho halo) */
+int lbx_time_step_cg(void* ctx);      /* time_step_CG + flipflop*Pop0 + stream*_CG (+ halos) */
+int lbx_time_step_bgk(void* ctx);     /* init_rho_isfluid_BGK + time_step_BGK + stream_BGK */
+
+/* ---- readback ---------------------------------------------------------- */
+/* moments2Fl (write_output.f90:975-1041) of the populations the reference
+ * holds after the last step: rhoR, rhoB (nx*ny*nz), vel (3*nx*ny*nz),
+ * phase (nx*ny*nz); zero on non-fluid cells.  Any pointer may be NULL. */
+int lbx_get_fields(void* ctx, float* rhoR, float* rhoB, float* vel, float* phase);
+/* The same in FP64 (exact moments of the stored populations). */
+int lbx_get_fields_f64(void* ctx, double* rhoR, double* rhoB, double* vel, double* phase);
+/* Post-streaming populations (the reference's `flip` buffer after a step). */
+int lbx_get_pops(void* ctx, float* popsR, float* popsB);
+/* Cell flags of the last step (myfluid_d(:,:,:,flip)), int8 nx*ny*nz. */
+int lbx_get_flags(void* ctx, int8_t* flags);
+/* FP64 global sums: mass[2] (red, blue) and momentum[3], over fluid cells. */
+int lbx_get_sums(void* ctx, double* mass, double* momentum);
+
+/* ---- status ------------------------------------------------------------ */
+int lbx_sync(void* ctx);
+/* First device error since the last call: code (LBX_DEV_*), step, and the
+ * cell (x + nx*(y + ny*z)) or particle index it concerns.  Clears it. */
+int lbx_status(void* ctx, int32_t* code, int32_t* step, int64_t* where);
+const char* lbx_error_string(int code);
+/* Steps taken so far (the reference's `step`). */
+int lbx_get_step(void* ctx, int64_t* step);
+
+/* ---- measurement ------------------------------------------------------- */
+/* Colour-gradient schedule: 1 = single-pass fused kernel (default), 0 = two
+ * passes (phase field, then collision).  The reference prints Mlup/s from
+ * CUDA events around the step loop (main.CUF:274-292); these are the hooks
+ * the benchmark uses for the same. */
+int lbx_set_schedule(void* ctx, int32_t fused);
+/* Enqueue nsteps steps bracketed by CUDA events on the context stream and
+ * wait: total device ms, and the summed duration / launch count of the
+ * step's dominant kernel (NULL kernel_ms disables per-kernel events). */
+int lbx_time_steps(void* ctx, int32_t nsteps, double* total_ms, double* kernel_ms, int64_t* kernel_launches);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LBX_H */

@@ -1,0 +1,48 @@
+"""Build the sm_100a shared library of the hot path in-tree.
+
+    python -m lbcuda_b200.build          # -> lbcuda_b200/liblbx.so
+
+The library is plain nvcc output (no torch extension): its C ABI is
+include/lbx.h, loaded from Python through ctypes.
+"""
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+LIB = os.path.join(HERE, "liblbx.so")
+
+SOURCES = ["lbx_api.cu", "lbx_fluid.cu", "lbx_particles.cu"]
+NVCC_FLAGS = [
+    "-gencode", "arch=compute_100a,code=sm_100a",
+    "-lineinfo", "-O3", "-std=c++17",
+    "--expt-relaxed-constexpr",
+    "-Xcompiler", "-fPIC", "-shared",
+    "-I", os.path.join(ROOT, "include"),
+]
+
+
+def nvcc():
+    for cand in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc", "nvcc"):
+        if cand and (os.path.isabs(cand) and os.path.exists(cand) or not os.path.isabs(cand)):
+            return cand
+    return "nvcc"
+
+
+def build(verbose=False, extra=()):
+    srcs = [os.path.join(CSRC, s) for s in SOURCES]
+    newest = max(os.path.getmtime(p) for p in srcs + [os.path.join(CSRC, h) for h in os.listdir(CSRC)]
+                 + [os.path.join(ROOT, "include", "lbx.h")])
+    if os.path.exists(LIB) and os.path.getmtime(LIB) >= newest and not extra:
+        return LIB
+    cmd = [nvcc()] + NVCC_FLAGS + list(extra) + srcs + ["-o", LIB]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    subprocess.run(cmd, check=True)
+    return LIB
+
+
+if __name__ == "__main__":
+    build(verbose=True, extra=sys.argv[1:])

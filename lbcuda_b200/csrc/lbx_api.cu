@@ -1,0 +1,373 @@
+// lbx_api.cu — the extern "C" boundary declared in include/lbx.h.
+//
+// Replaces the host side of the reference's hot path: allocation and constant
+// upload (setupGPUgridAndAlloc / SetConstants, main.CUF:2133-2407,
+// 1043-1162), initial conditions (setupRho_Pops, main.CUF:2531-2608), the
+// per-step launch sequence (main.CUF:125-308), the stop_d error protocol
+// (abortOnLastErrorAndSync, main.CUF:2410-2442) and the readback used by
+// OutputVTK (main.CUF:1812-1929).
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <cstring>
+#include <new>
+
+#include "../../include/lbx.h"
+#include "lbx_ctx.h"
+#include "lbx_common.cuh"
+
+namespace lbx {
+int particles_create(Ctx& c);
+void particles_destroy(Ctx& c);
+int particles_step_pre(Ctx& c);
+int particles_step_post(Ctx& c);
+}  // namespace lbx
+
+using lbx::Ctx;
+
+namespace {
+
+int cuda_rc(cudaError_t e) { return e == cudaSuccess ? 0 : LBX_ERR_CUDA; }
+
+// device error word -> status; clears it
+int poll_error(Ctx& c, int32_t* code, int32_t* step, int64_t* where) {
+  unsigned long long v = 0;
+  cudaError_t e = cudaMemcpyAsync(&v, c.d_err, sizeof(v), cudaMemcpyDeviceToHost, c.stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c.stream);
+  if (e != cudaSuccess) return LBX_ERR_CUDA;
+  int cd = int(v >> 56);
+  if (code) *code = cd;
+  if (step) *step = int32_t((v >> 32) & 0xffffff);
+  if (where) *where = int64_t(v & 0xffffffffull);
+  if (v) cudaMemsetAsync(c.d_err, 0, sizeof(v), c.stream);
+  return 0;
+}
+
+// synchronise and fold a pending device error into the return status
+int sync_status(Ctx& c) {
+  cudaError_t e = cudaStreamSynchronize(c.stream);
+  if (e != cudaSuccess) return LBX_ERR_CUDA;
+  unsigned long long v = 0;
+  e = cudaMemcpy(&v, c.d_err, sizeof(v), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return LBX_ERR_CUDA;
+  return v ? int(v >> 56) : 0;
+}
+
+// temporary device buffer for host<->device staging of one call
+struct DevBuf {
+  void* p = nullptr;
+  explicit DevBuf(size_t bytes) {
+    if (bytes && cudaMalloc(&p, bytes) != cudaSuccess) p = nullptr;
+  }
+  ~DevBuf() {
+    if (p) cudaFree(p);
+  }
+};
+
+Ctx* as_ctx(void* ctx) { return static_cast<Ctx*>(ctx); }
+
+}  // namespace
+
+extern "C" {
+
+void lbx_default_params(lbx_params* p, int32_t nx, int32_t ny, int32_t nz) {
+  if (!p) return;
+  std::memset(p, 0, sizeof(*p));
+  p->nx = nx;
+  p->ny = ny;
+  p->nz = nz;
+  p->model = LBX_MODEL_CG;
+  p->storage = LBX_STORE_F32;
+  p->wetting = LBX_WET_JANUS;
+  p->lrotate = 0;
+  p->max_particles = 0;
+  p->tau = 1.0f;
+  p->tauR = 1.0f;  // dimensions_m.CUF:98-99
+  p->tauB = 1.0f;
+  p->sigma = 0.1f;  // dimensions_m.CUF:50
+  p->beta = 0.999f;
+  p->rho0R = 0.5f;
+  p->rho0B = 0.5f;
+  p->radius = 5.5f;             // dimensions_m.CUF:59
+  p->rmass = 1.0f / 1500.0f;    // dimensions_m.CUF:60
+  p->max_vel = 0.0f;
+  p->hz_k = 10.0f;              // dimensions_m.CUF:77-80
+  p->hz_rmin = 10.5f;
+  p->hz_rcap = 9.0f;
+  p->lubrication = 0;           // dimensions_m.CUF:81-84
+  p->lubric_k = 10.0f;
+  p->lubric_rmin = 10.0f;
+  p->lubric_rcap = 9.0f;
+}
+
+int lbx_create(const lbx_params* p, void** out) {
+  if (!p || !out) return LBX_ERR_ARG;
+  *out = nullptr;
+  if (p->nx < 3 || p->ny < 3 || p->nz < 3) return LBX_ERR_ARG;
+  if (p->model != LBX_MODEL_BGK && p->model != LBX_MODEL_CG) return LBX_ERR_ARG;
+  if (p->storage < LBX_STORE_F32 || p->storage > LBX_STORE_F64) return LBX_ERR_ARG;
+  int64_t n = int64_t(p->nx) * p->ny * p->nz;
+  if (n >= (int64_t(1) << 31)) return LBX_ERR_ARG;  // 32-bit cell indices
+  Ctx* c = new (std::nothrow) Ctx();
+  if (!c) return LBX_ERR_ALLOC;
+  c->p = *p;
+  c->nx = p->nx;
+  c->ny = p->ny;
+  c->nz = p->nz;
+  c->n = n;
+  c->ncomp = (p->model == LBX_MODEL_CG) ? 2 : 1;
+  c->storage = p->storage;
+  c->elem = (p->storage == LBX_STORE_F32) ? 4 : (p->storage == LBX_STORE_F64 ? 8 : 2);
+  int rc = cuda_rc(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+  if (!rc) rc = cuda_rc(cudaMalloc(&c->d_err, sizeof(unsigned long long)));
+  if (!rc) rc = cuda_rc(cudaMemsetAsync(c->d_err, 0, sizeof(unsigned long long), c->stream));
+  if (!rc) rc = lbx::fluid_alloc(*c);
+  if (!rc && p->max_particles > 0) rc = lbx::particles_create(*c);
+  if (!rc) rc = cuda_rc(cudaStreamSynchronize(c->stream));
+  if (rc) {
+    lbx_destroy(c);
+    return rc;
+  }
+  *out = c;
+  return 0;
+}
+
+int lbx_destroy(void* ctx) {
+  Ctx* c = as_ctx(ctx);
+  if (!c) return LBX_ERR_ARG;
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  lbx::particles_destroy(*c);
+  lbx::fluid_free(*c);
+  for (auto e : c->kt_ev) cudaEventDestroy(e);
+  if (c->d_err) cudaFree(c->d_err);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return 0;
+}
+
+int lbx_set_fields(void* ctx, const float* rhoR, const float* rhoB, float vx, float vy, float vz) {
+  Ctx* c = as_ctx(ctx);
+  if (!c || !rhoR || (c->ncomp == 2 && !rhoB)) return LBX_ERR_ARG;
+  size_t bytes = size_t(c->n) * sizeof(float);
+  DevBuf buf(bytes * c->ncomp);
+  if (!buf.p) return LBX_ERR_ALLOC;
+  float* dR = static_cast<float*>(buf.p);
+  float* dB = (c->ncomp == 2) ? dR + c->n : nullptr;
+  int rc = cuda_rc(cudaMemcpyAsync(dR, rhoR, bytes, cudaMemcpyHostToDevice, c->stream));
+  if (!rc && dB) rc = cuda_rc(cudaMemcpyAsync(dB, rhoB, bytes, cudaMemcpyHostToDevice, c->stream));
+  if (!rc) rc = lbx::fluid_set_fields(*c, dR, dB, vx, vy, vz);
+  if (!rc) rc = cuda_rc(cudaMemsetAsync(c->d_err, 0, sizeof(unsigned long long), c->stream));
+  c->step = 0;
+  if (!rc) rc = cuda_rc(cudaStreamSynchronize(c->stream));
+  return rc;
+}
+
+int lbx_set_pops(void* ctx, const float* popsR, const float* popsB) {
+  Ctx* c = as_ctx(ctx);
+  if (!c || !popsR || (c->ncomp == 2 && !popsB)) return LBX_ERR_ARG;
+  size_t bytes = size_t(c->n) * lbx::Q * sizeof(float);
+  DevBuf buf(bytes * c->ncomp);
+  if (!buf.p) return LBX_ERR_ALLOC;
+  float* dR = static_cast<float*>(buf.p);
+  float* dB = (c->ncomp == 2) ? dR + c->n * lbx::Q : nullptr;
+  int rc = cuda_rc(cudaMemcpyAsync(dR, popsR, bytes, cudaMemcpyHostToDevice, c->stream));
+  if (!rc && dB) rc = cuda_rc(cudaMemcpyAsync(dB, popsB, bytes, cudaMemcpyHostToDevice, c->stream));
+  if (!rc) rc = lbx::fluid_set_pops(*c, dR, dB);
+  c->step = 0;
+  if (!rc) rc = cuda_rc(cudaStreamSynchronize(c->stream));
+  return rc;
+}
+
+int lbx_step(void* ctx, int32_t nsteps) {
+  Ctx* c = as_ctx(ctx);
+  if (!c || nsteps < 0) return LBX_ERR_ARG;
+  for (int s = 0; s < nsteps; ++s) {
+    int rc = 0;
+    if (c->part) rc = lbx::particles_step_pre(*c);
+    if (!rc) rc = lbx::fluid_step(*c);
+    if (!rc && c->part) rc = lbx::particles_step_post(*c);
+    if (rc) return rc;
+  }
+  return 0;
+}
+
+int lbx_init_rho(void* ctx) {
+  Ctx* c = as_ctx(ctx);
+  if (!c) return LBX_ERR_ARG;
+  return lbx::fluid_init_rho(*c);
+}
+
+int lbx_time_step_cg(void* ctx) {
+  Ctx* c = as_ctx(ctx);
+  if (!c) return LBX_ERR_ARG;
+  int rc = lbx::fluid_collide_stream(*c);
+  if (!rc) c->step += 1;
+  return rc;
+}
+
+int lbx_time_step_bgk(void* ctx) {
+  Ctx* c = as_ctx(ctx);
+  if (!c) return LBX_ERR_ARG;
+  int rc = lbx::fluid_bgk(*c);
+  if (!rc) c->step += 1;
+  return rc;
+}
+
+static int get_fields_impl(Ctx* c, void* rR, void* rB, void* vel, void* phase, int f64) {
+  size_t es = f64 ? 8 : 4;
+  size_t nb = size_t(c->n) * es;
+  DevBuf buf(nb * 6);
+  if (!buf.p) return LBX_ERR_ALLOC;
+  char* d = static_cast<char*>(buf.p);
+  void* dR = rR ? d : nullptr;
+  void* dB = rB ? d + nb : nullptr;
+  void* dV = vel ? d + 2 * nb : nullptr;
+  void* dP = phase ? d + 5 * nb : nullptr;
+  int rc = lbx::fluid_get_fields(*c, dR, dB, dV, dP, f64);
+  if (!rc && rR) rc = cuda_rc(cudaMemcpyAsync(rR, dR, nb, cudaMemcpyDeviceToHost, c->stream));
+  if (!rc && rB) rc = cuda_rc(cudaMemcpyAsync(rB, dB, nb, cudaMemcpyDeviceToHost, c->stream));
+  if (!rc && vel) rc = cuda_rc(cudaMemcpyAsync(vel, dV, 3 * nb, cudaMemcpyDeviceToHost, c->stream));
+  if (!rc && phase) rc = cuda_rc(cudaMemcpyAsync(phase, dP, nb, cudaMemcpyDeviceToHost, c->stream));
+  if (!rc) rc = sync_status(*c);
+  return rc;
+}
+
+int lbx_get_fields(void* ctx, float* rhoR, float* rhoB, float* vel, float* phase) {
+  Ctx* c = as_ctx(ctx);
+  if (!c) return LBX_ERR_ARG;
+  return get_fields_impl(c, rhoR, rhoB, vel, phase, 0);
+}
+
+int lbx_get_fields_f64(void* ctx, double* rhoR, double* rhoB, double* vel, double* phase) {
+  Ctx* c = as_ctx(ctx);
+  if (!c) return LBX_ERR_ARG;
+  return get_fields_impl(c, rhoR, rhoB, vel, phase, 1);
+}
+
+int lbx_get_pops(void* ctx, float* popsR, float* popsB) {
+  Ctx* c = as_ctx(ctx);
+  if (!c) return LBX_ERR_ARG;
+  size_t nb = size_t(c->n) * lbx::Q * sizeof(float);
+  DevBuf buf(nb * 2);
+  if (!buf.p) return LBX_ERR_ALLOC;
+  float* dR = popsR ? static_cast<float*>(buf.p) : nullptr;
+  float* dB = popsB ? static_cast<float*>(buf.p) + size_t(c->n) * lbx::Q : nullptr;
+  int rc = lbx::fluid_get_pops(*c, dR, dB);
+  if (!rc && popsR) rc = cuda_rc(cudaMemcpyAsync(popsR, dR, nb, cudaMemcpyDeviceToHost, c->stream));
+  if (!rc && popsB) {
+    if (c->ncomp == 2) rc = cuda_rc(cudaMemcpyAsync(popsB, dB, nb, cudaMemcpyDeviceToHost, c->stream));
+    else std::memset(popsB, 0, nb);
+  }
+  if (!rc) rc = sync_status(*c);
+  return rc;
+}
+
+int lbx_get_flags(void* ctx, int8_t* flags) {
+  Ctx* c = as_ctx(ctx);
+  if (!c || !flags) return LBX_ERR_ARG;
+  int rc = cuda_rc(cudaMemcpyAsync(flags, c->flags[c->fcur], size_t(c->n), cudaMemcpyDeviceToHost, c->stream));
+  if (!rc) rc = sync_status(*c);
+  return rc;
+}
+
+int lbx_get_sums(void* ctx, double* mass, double* momentum) {
+  Ctx* c = as_ctx(ctx);
+  if (!c) return LBX_ERR_ARG;
+  DevBuf buf(5 * sizeof(double));
+  if (!buf.p) return LBX_ERR_ALLOC;
+  double h[5];
+  int rc = lbx::fluid_get_sums(*c, static_cast<double*>(buf.p));
+  if (!rc) rc = cuda_rc(cudaMemcpyAsync(h, buf.p, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+  if (!rc) rc = sync_status(*c);
+  if (!rc) {
+    if (mass) { mass[0] = h[0]; mass[1] = h[1]; }
+    if (momentum) { momentum[0] = h[2]; momentum[1] = h[3]; momentum[2] = h[4]; }
+  }
+  return rc;
+}
+
+int lbx_sync(void* ctx) {
+  Ctx* c = as_ctx(ctx);
+  if (!c) return LBX_ERR_ARG;
+  return sync_status(*c);
+}
+
+int lbx_status(void* ctx, int32_t* code, int32_t* step, int64_t* where) {
+  Ctx* c = as_ctx(ctx);
+  if (!c) return LBX_ERR_ARG;
+  return poll_error(*c, code, step, where);
+}
+
+int lbx_get_step(void* ctx, int64_t* step) {
+  Ctx* c = as_ctx(ctx);
+  if (!c || !step) return LBX_ERR_ARG;
+  *step = c->step;
+  return 0;
+}
+
+const char* lbx_error_string(int code) {
+  switch (code) {
+    case 0: return "ok";
+    case LBX_ERR_CUDA: return "CUDA runtime error";
+    case LBX_ERR_ARG: return "invalid argument";
+    case LBX_ERR_ALLOC: return "device allocation failed";
+    case LBX_ERR_STATE: return "operation not valid for this context";
+    case LBX_ERR_TIMEOUT: return "device wait timed out";
+    case LBX_ERR_NOSYM: return "device symbol not available";
+    case LBX_DEV_RHO_RANGE: return "density out of range [-10, 10] (init_rho*_CG)";
+    case LBX_DEV_BIG_FORCE: return "particle force too large (nve_lf)";
+    case LBX_DEV_EXTREME_VEL: return "particle speed above MAX_PARTICLE_VEL (nve_lf)";
+    case LBX_DEV_POSITION: return "particle position outside the box (nve_lf)";
+    case LBX_DEV_LIST_OVERFLOW: return "too many particles near one cell block";
+    case LBX_DEV_BELT_RANGE: return "belt neighbour outside the lattice";
+  }
+  return "unknown error";
+}
+
+/* ---- measurement hooks used by the benchmark --------------------------- */
+/* Select the colour-gradient schedule: 1 = single-pass fused kernel (default),
+ * 0 = two passes (phase field, then collision). */
+int lbx_set_schedule(void* ctx, int32_t fused) {
+  Ctx* c = as_ctx(ctx);
+  if (!c) return LBX_ERR_ARG;
+  c->fused = fused ? 1 : 0;
+  return 0;
+}
+
+/* Time nsteps steps on the context stream with CUDA events: total device
+ * time in ms, and the summed duration of the step's dominant kernel (the
+ * fused collide-stream kernel) with its launch count. */
+int lbx_time_steps(void* ctx, int32_t nsteps, double* total_ms, double* kernel_ms, int64_t* kernel_launches) {
+  Ctx* c = as_ctx(ctx);
+  if (!c || nsteps < 0) return LBX_ERR_ARG;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  c->kt_on = kernel_ms ? 1 : 0;
+  c->kt_n = 0;
+  cudaEventRecord(e0, c->stream);
+  int rc = lbx_step(ctx, nsteps);
+  cudaEventRecord(e1, c->stream);
+  if (!rc) rc = cuda_rc(cudaEventSynchronize(e1));
+  float ms = 0.f;
+  if (!rc) cudaEventElapsedTime(&ms, e0, e1);
+  if (total_ms) *total_ms = ms;
+  double kms = 0.0;
+  if (!rc && c->kt_on) {
+    for (int i = 0; i < c->kt_n; ++i) {
+      float t = 0.f;
+      cudaEventElapsedTime(&t, c->kt_ev[2 * i], c->kt_ev[2 * i + 1]);
+      kms += t;
+    }
+  }
+  if (kernel_ms) *kernel_ms = kms;
+  if (kernel_launches) *kernel_launches = c->kt_n;
+  c->kt_on = 0;
+  c->kt_n = 0;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (!rc) rc = sync_status(*c);
+  return rc;
+}
+
+}  // extern "C"

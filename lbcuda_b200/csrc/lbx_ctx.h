@@ -1,0 +1,65 @@
+// lbx_ctx.h — the context behind the opaque `void* ctx` of include/lbx.h.
+//
+// The reference keeps its state as module-global device arrays
+// (kernels_fluid.CUF:9-48) with a 1-cell halo, two ping-pong copies of the
+// populations indexed by `flip`, FP32 densities and int8 flags.  Here the
+// state lives in one context per simulation:
+//   pops[2]   two SoA population buffers, [component][direction][z][y][x],
+//             no halo (periodic wrap is index arithmetic), storage type S.
+//             Buffer `cur` holds the post-collision populations of the last
+//             step (pull convention: the next step gathers f_l(x - e_l)).
+//   phi       phase field (rhoR - rhoB)/(rhoR + rhoB) of the current step
+//             (only the two-pass colour-gradient path and the particle path).
+//   rho[2]    FP32/FP64 densities (particle path, readback).
+//   flags[2]  int8 cell flags of the current and previous step.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <vector>
+
+#include "../../include/lbx.h"
+
+namespace lbx {
+
+struct ParticleState;  // lbx_particles.cu
+
+struct Ctx {
+  lbx_params p;
+  int nx = 0, ny = 0, nz = 0;
+  int64_t n = 0;            // interior cells
+  int ncomp = 1;            // 1 (BGK) or 2 (CG)
+  int storage = LBX_STORE_F32;
+  size_t elem = 4;          // bytes per stored population
+  void* pops[2] = {nullptr, nullptr};
+  int cur = 0;              // buffer holding the current state
+  void* phi = nullptr;      // float or double, n
+  void* rho[2] = {nullptr, nullptr};
+  int8_t* flags[2] = {nullptr, nullptr};
+  int fcur = 0;             // flags slot of the current step
+  unsigned long long* d_err = nullptr;
+  cudaStream_t stream = nullptr;
+  int64_t step = 0;
+  int fused = 1;            // 1: single-pass colour-gradient kernel, 0: two passes
+  // timing of the dominant kernel (opt-in)
+  int kt_on = 0;
+  std::vector<cudaEvent_t> kt_ev;
+  int kt_n = 0;
+  double kt_ms = 0.0;
+  int64_t kt_launches = 0;
+  ParticleState* part = nullptr;
+};
+
+// lbx_fluid.cu
+int fluid_alloc(Ctx& c);
+void fluid_free(Ctx& c);
+int fluid_set_fields(Ctx& c, const float* d_rhoR, const float* d_rhoB, float vx, float vy, float vz);
+int fluid_set_pops(Ctx& c, const float* d_pR, const float* d_pB);
+int fluid_init_rho(Ctx& c);
+int fluid_collide_stream(Ctx& c);
+int fluid_bgk(Ctx& c);
+int fluid_step(Ctx& c);
+int fluid_get_fields(Ctx& c, void* d_rR, void* d_rB, void* d_vel, void* d_phase, int f64);
+int fluid_get_pops(Ctx& c, float* d_pR, float* d_pB);
+int fluid_get_sums(Ctx& c, double* d_out5);
+
+}  // namespace lbx

@@ -1,0 +1,772 @@
+// lbx_fluid.cu — fluid kernels of the LBcuda hot path for sm_100a.
+//
+// Reference behaviour restated (paths relative to the reference project):
+//   equil                         kernels_fluid_CG.CUF:30-38
+//   init_rhoR_CG / init_rhoB_CG   kernels_fluid_CG.CUF:398-509
+//   time_step_CG                  kernels_fluid_CG.CUF:531-848
+//   flipflop*Pop0_CG, stream*_CG  kernels_fluid_CG.CUF:851-1015
+//   stream_CG_x/_y/_z + fixPeriodic (halo wrap)  kernels_fluid_CG.CUF:1017-1141,
+//                                 1215-1426; main.CUF:577-1000
+//   time_step_BGK + stream_BGK    kernels_fluid_BGK.CUF:205-417
+//   moments2Fl (readback)         write_output.f90:975-1041
+//
+// B200 design (not a translation): SoA populations without a halo ring,
+// periodic wrap by index arithmetic, pull streaming (each thread gathers
+// f_l(x - e_l) of the previous post-collision buffer, so every store is
+// aligned and coalesced), one thread per cell along contiguous x rows, and
+// FP16/BF16 storage of f_l - w_l*rho0 with FP32 arithmetic.
+//
+// The colour-gradient collision needs the phase field of all 26 neighbours at
+// the same time level.  Two schedules are provided:
+//   two-pass: k_cg_phi (pull + densities -> phi) then k_cg_collide;
+//   single-pass: k_cg_fused, where each CTA owns a (BX x BY) column of cells
+//   and marches it along z, computing the phase field of its own cells and of
+//   a one-cell ring around the column from the pulled populations into a
+//   rolling 3-plane shared-memory window, so phi never goes through HBM.
+#include "lbx_common.cuh"
+#include "lbx_ctx.h"
+
+#include <cstdio>
+
+namespace lbx {
+
+// ---------------------------------------------------------------------------
+// indexing
+// ---------------------------------------------------------------------------
+struct Nbr {
+  int x, xm, xp;  // column index and its periodic neighbours
+  int ry[3];      // ny-row offsets (y-1, y, y+1) * nx
+  int rz[3];      // plane offsets (z-1, z, z+1) * nx * ny
+};
+
+__device__ __forceinline__ void make_nbr(const Geom& g, int x, int y, int z, Nbr& b) {
+  b.x = x;
+  b.xm = (x == 0) ? g.nx - 1 : x - 1;
+  b.xp = (x == g.nx - 1) ? 0 : x + 1;
+  int ym = (y == 0) ? g.ny - 1 : y - 1, yp = (y == g.ny - 1) ? 0 : y + 1;
+  int zm = (z == 0) ? g.nz - 1 : z - 1, zp = (z == g.nz - 1) ? 0 : z + 1;
+  b.ry[0] = ym * g.nx; b.ry[1] = y * g.nx; b.ry[2] = yp * g.nx;
+  const int plane = g.nx * g.ny;
+  b.rz[0] = zm * plane; b.rz[1] = z * plane; b.rz[2] = zp * plane;
+}
+
+// linear index of x + (dx,dy,dz), periodic
+__device__ __forceinline__ int at(const Nbr& b, int dx, int dy, int dz) {
+  int xx = dx == 0 ? b.x : (dx > 0 ? b.xp : b.xm);
+  return xx + b.ry[dy + 1] + b.rz[dz + 1];
+}
+
+// e_l . (u,v,w) with the zero components dropped, summed in x,y,z order
+template <typename C>
+__device__ __forceinline__ C edot(int l, C u, C v, C w) {
+  C s = C(0);
+  bool any = false;
+  if (ex(l)) { s = ex(l) > 0 ? u : -u; any = true; }
+  if (ey(l)) { s = any ? (ey(l) > 0 ? s + v : s - v) : (ey(l) > 0 ? v : -v); any = true; }
+  if (ez(l)) { s = any ? (ez(l) > 0 ? s + w : s - w) : (ez(l) > 0 ? w : -w); any = true; }
+  return s;
+}
+
+// equil, kernels_fluid_CG.CUF:30-38, with the velocity-square term hoisted
+template <typename C>
+__device__ __forceinline__ C equil_u(const LatticeT<C>& L, C rho, C edu, C usq_term, int l) {
+  C uv = L.inv_cssq * edu;
+  return rho * L.w[wclass(l)] * (C(1) + uv + C(0.5) * (uv * uv) - usq_term);
+}
+
+// gather the post-streaming populations of one component (pull of the push
+// streaming of stream*_CG + halo pushes)
+template <typename S, typename C>
+__device__ __forceinline__ void pull(const S* __restrict__ A, const Geom& g, const Nbr& b, int comp,
+                                     const Shift<C>& sh, C f[Q]) {
+  const S* base = A + size_t(comp) * Q * size_t(g.n);
+#pragma unroll
+  for (int l = 0; l < Q; ++l)
+    f[l] = Store<S>::ld(base + size_t(l) * size_t(g.n) + at(b, -ex(l), -ey(l), -ez(l)), sh.at(comp, l));
+}
+
+template <typename S, typename C>
+__device__ __forceinline__ void store_all(S* __restrict__ B, const Geom& g, int cell, int comp, const Shift<C>& sh,
+                                          const C f[Q]) {
+  S* base = B + size_t(comp) * Q * size_t(g.n) + cell;
+#pragma unroll
+  for (int l = 0; l < Q; ++l) Store<S>::st(base + size_t(l) * size_t(g.n), f[l], sh.at(comp, l));
+}
+
+template <typename C>
+__device__ __forceinline__ C sum_q(const C f[Q]) {
+  C r = f[0];
+#pragma unroll
+  for (int l = 1; l < Q; ++l) r = r + f[l];
+  return r;
+}
+// manual_u/v/w sums, kernels_fluid_CG.CUF:511-529 (without the 1/rho factor)
+template <typename C> __device__ __forceinline__ C mx(const C q[Q]) { return q[1] - q[2] + q[7] - q[8] - q[9] + q[10] + q[11] - q[12] - q[13] + q[14]; }
+template <typename C> __device__ __forceinline__ C my(const C q[Q]) { return q[3] - q[4] + q[7] - q[8] + q[9] - q[10] + q[15] - q[16] - q[17] + q[18]; }
+template <typename C> __device__ __forceinline__ C mz(const C q[Q]) { return q[5] - q[6] + q[11] - q[12] + q[13] - q[14] + q[15] - q[16] + q[17] - q[18]; }
+
+// Constants of the colour-gradient collision, derived on the host like
+// SetConstants (main.CUF:1043-1162).
+template <typename C>
+struct CGConst {
+  LatticeT<C> L;
+  C inv_viscR, inv_viscB;  // 1/viscR, 1/viscB
+  C sigma, beta;
+};
+
+// ---------------------------------------------------------------------------
+// time_step_CG at one fluid cell (kernels_fluid_CG.CUF:689-846).  fR/fB hold
+// the post-streaming populations on entry and the post-collision ones on exit.
+// rhoR/rhoB are the clamped densities of init_rho*_CG, psi the colour
+// gradient (HIGHGRAD, D3Q27 weights).
+// ---------------------------------------------------------------------------
+template <typename C>
+__device__ __forceinline__ void cg_collide_cell(const CGConst<C>& K, C fR[Q], C fB[Q], C rhoR, C rhoB, C psix,
+                                                C psiy, C psiz) {
+  const C ONE = 1, HALF = C(0.5);
+  const LatticeT<C>& L = K.L;
+  C rhosum = rhoR + rhoB;
+  C phase_field = (rhoR - rhoB) / (rhoR + rhoB);
+  C viscavg = ONE / (HALF * (ONE + phase_field) * K.inv_viscR + HALF * (ONE - phase_field) * K.inv_viscB);
+  C omega = ONE / (viscavg / L.cssq + HALF);
+  C omm = ONE - omega;
+  C invrho = ONE / rhosum;
+  C u = invrho * mx(fR) + invrho * mx(fB);
+  C v = invrho * my(fR) + invrho * my(fB);
+  C w = invrho * mz(fR) + invrho * mz(fB);
+  C usq = L.half_inv_cssq * (u * u + v * v + w * w);
+#pragma unroll
+  for (int l = 0; l < Q; ++l) {
+    C e = edot(l, u, v, w);
+    fR[l] = fR[l] * omm + equil_u(L, rhoR, e, usq, l) * omega;
+    fB[l] = fB[l] * omm + equil_u(L, rhoB, e, usq, l) * omega;
+  }
+  C psinorm_sq = psix * psix + psiy * psiy + psiz * psiz;
+  if (psinorm_sq > C(1.e-20)) {
+    C psinorm = sqrt(psinorm_sq);
+    C inv_psq = ONE / psinorm_sq;
+    C acoeff = C(9) / C(4) * omega * K.sigma;
+    C kR = rhoR * invrho, kB = rhoB * invrho;
+    C coef = K.beta * rhoR * rhoB * (invrho * invrho);
+    C inv_t1 = ONE / psinorm;                 // rec_fact = 1
+    C inv_t2 = ONE / (L.rec[2] * psinorm);    // rec_fact = sqrt(2)
+#pragma unroll
+    for (int l = 0; l < Q; ++l) {
+      C edp = edot(l, psix, psiy, psiz);
+      C temp = psinorm * (L.w[wclass(l)] * (edp * edp) * inv_psq - L.b[wclass(l)]);
+      C fd = fR[l] + fB[l] + acoeff * temp;
+      C feq = rhoR * L.w[wclass(l)] + rhoB * L.w[wclass(l)];
+      C cosphi;
+      if (l == 0) cosphi = C(0);
+      else {
+        C t1 = L.rec[wclass(l)] * psinorm;
+        cosphi = (t1 <= C(1.e-20)) ? C(0) : edp * (wclass(l) == 1 ? inv_t1 : inv_t2);
+      }
+      C t = coef * cosphi;
+      fR[l] = fd * kR + t * feq;
+      fB[l] = fd * kB - t * feq;
+    }
+  }
+}
+
+// colour gradient psi = sum_l a27_l e_l phi(x + e_l), l = 1..26 in reference order
+template <typename C, typename F>
+__device__ __forceinline__ void grad27(const LatticeT<C>& L, F&& phi_at, C& psix, C& psiy, C& psiz) {
+  psix = C(0); psiy = C(0); psiz = C(0);
+#pragma unroll
+  for (int l = 1; l < Q27; ++l) {
+    C ps = phi_at(ex27(l), ey27(l), ez27(l));
+    C a = L.a27[wclass27(l)];
+    if (ex27(l)) psix = psix + (ex27(l) > 0 ? a : -a) * ps;
+    if (ey27(l)) psiy = psiy + (ey27(l) > 0 ? a : -a) * ps;
+    if (ez27(l)) psiz = psiz + (ez27(l) > 0 ? a : -a) * ps;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// kernels
+// ---------------------------------------------------------------------------
+struct LaunchDims {
+  dim3 grid, block;
+};
+
+static LaunchDims cell_dims(const Ctx& c) {
+  int bx = (c.nx % 128 == 0) ? 128 : ((c.nx % 64 == 0) ? 64 : 32);
+  int by = 256 / bx;
+  LaunchDims d;
+  d.block = dim3(bx, by, 1);
+  d.grid = dim3((c.nx + bx - 1) / bx, (c.ny + by - 1) / by, c.nz);
+  return d;
+}
+
+// setupPops (kernels_fluid_CG.CUF:313-346) written in pull convention: the
+// stored buffer holds, at x, the populations that streaming moves to x + e_l,
+// so that the first step gathers exactly the equilibrium of the given fields.
+template <typename S>
+__global__ void k_set_fields(S* __restrict__ A, S* __restrict__ B, Geom g, int ncomp, const float* __restrict__ rR,
+                             const float* __restrict__ rB, float vx, float vy, float vz,
+                             LatticeT<typename Store<S>::C> L, Shift<typename Store<S>::C> sh) {
+  using C = typename Store<S>::C;
+  int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y, z = blockIdx.z;
+  if (x >= g.nx || y >= g.ny) return;
+  Nbr b;
+  make_nbr(g, x, y, z, b);
+  int cell = at(b, 0, 0, 0);
+  C u = C(vx), v = C(vy), w = C(vz);
+  C usq = L.half_inv_cssq * (u * u + v * v + w * w);
+  for (int comp = 0; comp < ncomp; ++comp) {
+    const float* r = comp ? rB : rR;
+    S* base = A + size_t(comp) * Q * size_t(g.n);
+    S* baseB = B + size_t(comp) * Q * size_t(g.n);
+#pragma unroll
+    for (int l = 0; l < Q; ++l) {
+      C rho = C(r[at(b, ex(l), ey(l), ez(l))]);
+      C val = equil_u(L, rho, edot(l, u, v, w), usq, l);
+      Store<S>::st(base + size_t(l) * size_t(g.n) + cell, val, sh.at(comp, l));
+      Store<S>::st(baseB + size_t(l) * size_t(g.n) + cell, C(0), sh.at(comp, l));
+    }
+  }
+}
+
+// initType 4: raw post-streaming populations, stored in pull convention
+template <typename S>
+__global__ void k_set_pops(S* __restrict__ A, Geom g, int ncomp, const float* __restrict__ pR,
+                           const float* __restrict__ pB, Shift<typename Store<S>::C> sh) {
+  using C = typename Store<S>::C;
+  int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y, z = blockIdx.z;
+  if (x >= g.nx || y >= g.ny) return;
+  Nbr b;
+  make_nbr(g, x, y, z, b);
+  int cell = at(b, 0, 0, 0);
+  for (int comp = 0; comp < ncomp; ++comp) {
+    const float* p = comp ? pB : pR;
+    S* base = A + size_t(comp) * Q * size_t(g.n);
+#pragma unroll
+    for (int l = 0; l < Q; ++l)
+      Store<S>::st(base + size_t(l) * size_t(g.n) + cell,
+                   C(p[size_t(l) * size_t(g.n) + at(b, ex(l), ey(l), ez(l))]), sh.at(comp, l));
+  }
+}
+
+// init_rhoR_CG + init_rhoB_CG (all cells fluid) producing the phase field of
+// the two-pass schedule and, optionally, the densities.
+template <typename S>
+__global__ void __launch_bounds__(256) k_cg_phi(const S* __restrict__ A, Geom g, Shift<typename Store<S>::C> sh,
+                                                 typename Store<S>::C* __restrict__ phi,
+                                                 typename Store<S>::C* __restrict__ rhoR,
+                                                 typename Store<S>::C* __restrict__ rhoB,
+                                                 unsigned long long* err, int64_t step) {
+  using C = typename Store<S>::C;
+  int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y, z = blockIdx.z;
+  if (x >= g.nx || y >= g.ny) return;
+  Nbr b;
+  make_nbr(g, x, y, z, b);
+  int cell = at(b, 0, 0, 0);
+  C f[Q];
+  pull(A, g, b, 0, sh, f);
+  C rR = sum_q(f);
+  pull(A, g, b, 1, sh, f);
+  C rB = sum_q(f);
+  if (rR < C(-10) || rR > C(10) || rB < C(-10) || rB > C(10)) raise_error(err, LBX_DEV_RHO_RANGE, step, cell);
+  if (rR < C(0)) rR = C(0);
+  if (rB < C(0)) rB = C(0);
+  phi[cell] = (rR - rB) / (rR + rB);
+  if (rhoR) { rhoR[cell] = rR; rhoB[cell] = rB; }
+}
+
+// time_step_CG + streaming, two-pass schedule: pull, densities, gradient from
+// the phase-field array, collision, aligned store.
+template <typename S>
+__global__ void __launch_bounds__(256) k_cg_collide(const S* __restrict__ A, S* __restrict__ B, Geom g,
+                                                     Shift<typename Store<S>::C> sh,
+                                                     const typename Store<S>::C* __restrict__ phi,
+                                                     CGConst<typename Store<S>::C> K) {
+  using C = typename Store<S>::C;
+  int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y, z = blockIdx.z;
+  if (x >= g.nx || y >= g.ny) return;
+  Nbr b;
+  make_nbr(g, x, y, z, b);
+  int cell = at(b, 0, 0, 0);
+  C fR[Q], fB[Q];
+  pull(A, g, b, 0, sh, fR);
+  pull(A, g, b, 1, sh, fB);
+  C rR = sum_q(fR), rB = sum_q(fB);
+  if (rR < C(0)) rR = C(0);
+  if (rB < C(0)) rB = C(0);
+  C psix, psiy, psiz;
+  grad27(K.L, [&](int dx, int dy, int dz) { return __ldg(phi + at(b, dx, dy, dz)); }, psix, psiy, psiz);
+  cg_collide_cell(K, fR, fB, rR, rB, psix, psiy, psiz);
+  store_all(B, g, cell, 0, sh, fR);
+  store_all(B, g, cell, 1, sh, fB);
+}
+
+// ---------------------------------------------------------------------------
+// Single-pass colour-gradient step.  CTA = TX x TY threads owning the column
+// [x0, x0+TX) x [y0, y0+TY) x [z0, z0+ZLEN).  For every plane it computes the
+// phase field of the (TX+2) x (TY+2) cells of the column plus its ring from
+// the pulled populations into a rolling 4-slot shared window, then collides
+// the plane behind it.  The interior threads keep their pulled populations of
+// the plane ahead in registers for the next iteration.
+// ---------------------------------------------------------------------------
+template <int TX, int TY>
+struct FusedShape {
+  static constexpr int RX = TX + 2, RY = TY + 2, RING = RX * RY, NT = TX * TY;
+};
+
+__device__ __forceinline__ int wrapc(int v, int n) {
+  v %= n;
+  return v < 0 ? v + n : v;
+}
+
+template <typename S, int TX, int TY>
+__global__ void __launch_bounds__(TX* TY) k_cg_fused(const S* __restrict__ A, S* __restrict__ B, Geom g,
+                                                      Shift<typename Store<S>::C> sh,
+                                                      CGConst<typename Store<S>::C> K, int zlen,
+                                                      unsigned long long* err, int64_t step) {
+  using C = typename Store<S>::C;
+  using SH = FusedShape<TX, TY>;
+  constexpr int NRING = 2 * SH::RX + 2 * TY;  // bottom row, top row, left and right columns
+  __shared__ C sphi[4][SH::RING];
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
+  const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
+  const int z0 = blockIdx.z * zlen;
+  const int zend = min(z0 + zlen, g.nz);
+  // every thread computes the phase field of its (wrapped) position, so a
+  // partial tile still fills its shared window; only in-range cells collide
+  const bool active = (x0 + tx < g.nx) && (y0 + ty < g.ny);
+  const int x = wrapc(x0 + tx, g.nx), y = wrapc(y0 + ty, g.ny);
+
+  // phase field of the ring cells of plane z into sphi[slot]
+  auto ring_phi = [&](int z, int slot) {
+    for (int t = tid; t < NRING; t += SH::NT) {
+      int rx, ry;
+      if (t < SH::RX) { rx = t; ry = 0; }
+      else if (t < 2 * SH::RX) { rx = t - SH::RX; ry = SH::RY - 1; }
+      else if (t < 2 * SH::RX + TY) { rx = 0; ry = 1 + t - 2 * SH::RX; }
+      else { rx = SH::RX - 1; ry = 1 + t - 2 * SH::RX - TY; }
+      Nbr b;
+      make_nbr(g, wrapc(x0 + rx - 1, g.nx), wrapc(y0 + ry - 1, g.ny), wrapc(z, g.nz), b);
+      C f[Q];
+      pull(A, g, b, 0, sh, f);
+      C rR = sum_q(f);
+      pull(A, g, b, 1, sh, f);
+      C rB = sum_q(f);
+      if (rR < C(0)) rR = C(0);
+      if (rB < C(0)) rB = C(0);
+      sphi[slot][ry * SH::RX + rx] = (rR - rB) / (rR + rB);
+    }
+  };
+
+  C fR[Q], fB[Q];     // populations of the plane being collided
+  C nR[Q], nB[Q];     // populations of the plane ahead
+  C rRn = 0, rBn = 0; // clamped densities of the plane ahead
+  const int own = (ty + 1) * SH::RX + (tx + 1);
+
+  // pull the own cell of plane z into n*, write its phase field to the slot
+  auto own_phi = [&](int z, int slot) {
+    Nbr b;
+    make_nbr(g, x, y, wrapc(z, g.nz), b);
+    pull(A, g, b, 0, sh, nR);
+    pull(A, g, b, 1, sh, nB);
+    C rR = sum_q(nR), rB = sum_q(nB);
+    // range check of init_rho*_CG, raised by the CTA that owns the plane
+    if (active && z >= z0 && z < zend && (rR < C(-10) || rR > C(10) || rB < C(-10) || rB > C(10)))
+      raise_error(err, LBX_DEV_RHO_RANGE, step, at(b, 0, 0, 0));
+    if (rR < C(0)) rR = C(0);
+    if (rB < C(0)) rB = C(0);
+    rRn = rR; rBn = rB;
+    sphi[slot][own] = (rR - rB) / (rR + rB);
+  };
+
+  // prologue: planes z0-1 and z0
+  own_phi(z0 - 1, (z0 + 3) & 3);
+  ring_phi(z0 - 1, (z0 + 3) & 3);
+  own_phi(z0, z0 & 3);
+  ring_phi(z0, z0 & 3);
+  for (int z = z0; z < zend; ++z) {
+#pragma unroll
+    for (int l = 0; l < Q; ++l) { fR[l] = nR[l]; fB[l] = nB[l]; }
+    C rR = rRn, rB = rBn;
+    own_phi(z + 1, (z + 1) & 3);
+    ring_phi(z + 1, (z + 1) & 3);
+    __syncthreads();
+    if (active) {
+      const C* pm = sphi[(z + 3) & 3];
+      const C* p0 = sphi[z & 3];
+      const C* pp = sphi[(z + 1) & 3];
+      C psix, psiy, psiz;
+      grad27(K.L,
+             [&](int dx, int dy, int dz) {
+               const C* pl = dz < 0 ? pm : (dz > 0 ? pp : p0);
+               return pl[own + dy * SH::RX + dx];
+             },
+             psix, psiy, psiz);
+      cg_collide_cell(K, fR, fB, rR, rB, psix, psiy, psiz);
+      int cell = x + g.nx * (y + g.ny * z);
+      store_all(B, g, cell, 0, sh, fR);
+      store_all(B, g, cell, 1, sh, fB);
+    }
+    // The slot read here as plane z-1 is rewritten at iteration z+2 (plane
+    // z+3); the barrier of iteration z+1 orders that write after these reads.
+  }
+}
+
+// init_rho_isfluid_BGK + time_step_BGK + stream_BGK in one pass
+template <typename S>
+__global__ void __launch_bounds__(256) k_bgk(const S* __restrict__ A, S* __restrict__ B, Geom g,
+                                              Shift<typename Store<S>::C> sh, LatticeT<typename Store<S>::C> L,
+                                              typename Store<S>::C omega, unsigned long long* err, int64_t step) {
+  using C = typename Store<S>::C;
+  int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y, z = blockIdx.z;
+  if (x >= g.nx || y >= g.ny) return;
+  Nbr b;
+  make_nbr(g, x, y, z, b);
+  int cell = at(b, 0, 0, 0);
+  C f[Q];
+  pull(A, g, b, 0, sh, f);
+  C r = sum_q(f);
+  if (r < C(-10) || r > C(10)) raise_error(err, LBX_DEV_RHO_RANGE, step, cell);
+  const C ONE = 1;
+  C invrho = ONE / r;
+  C u = invrho * mx(f), v = invrho * my(f), w = invrho * mz(f);
+  C usq = L.half_inv_cssq * (u * u + v * v + w * w);
+  C omm = ONE - omega;
+#pragma unroll
+  for (int l = 0; l < Q; ++l) f[l] = f[l] * omm + equil_u(L, r, edot(l, u, v, w), usq, l) * omega;
+  store_all(B, g, cell, 0, sh, f);
+}
+
+// moments2Fl on the post-streaming populations (pulled from the state)
+template <typename S, typename O>
+__global__ void k_fields(const S* __restrict__ A, Geom g, int ncomp, Shift<typename Store<S>::C> sh,
+                         const int8_t* __restrict__ flags, O* rR, O* rB, O* vel, O* phase) {
+  using C = typename Store<S>::C;
+  int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y, z = blockIdx.z;
+  if (x >= g.nx || y >= g.ny) return;
+  Nbr b;
+  make_nbr(g, x, y, z, b);
+  int cell = at(b, 0, 0, 0);
+  C fR[Q], fB[Q];
+  pull(A, g, b, 0, sh, fR);
+  if (ncomp == 2) pull(A, g, b, 1, sh, fB);
+  else {
+#pragma unroll
+    for (int l = 0; l < Q; ++l) fB[l] = C(0);
+  }
+  C lr = sum_q(fR), lb = sum_q(fB);
+  C rs = lr + lb;
+  C inv = C(1) / rs;
+  C u = inv * (mx(fR) + mx(fB)), v = inv * (my(fR) + my(fB)), w = inv * (mz(fR) + mz(fB));
+  bool ok = (!flags || flags[cell] == LBX_FLUID_FLUID) && rs > C(0);
+  if (rR) rR[cell] = ok ? O(lr) : O(0);
+  if (rB) rB[cell] = ok ? O(lb) : O(0);
+  if (vel) {
+    vel[3 * size_t(cell) + 0] = ok ? O(u) : O(0);
+    vel[3 * size_t(cell) + 1] = ok ? O(v) : O(0);
+    vel[3 * size_t(cell) + 2] = ok ? O(w) : O(0);
+  }
+  if (phase) phase[cell] = ok ? O((lr - lb) / (lr + lb)) : O(0);
+}
+
+template <typename S>
+__global__ void k_get_pops(const S* __restrict__ A, Geom g, int ncomp, Shift<typename Store<S>::C> sh,
+                           float* pR, float* pB) {
+  using C = typename Store<S>::C;
+  int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y, z = blockIdx.z;
+  if (x >= g.nx || y >= g.ny) return;
+  Nbr b;
+  make_nbr(g, x, y, z, b);
+  int cell = at(b, 0, 0, 0);
+  C f[Q];
+  for (int comp = 0; comp < ncomp; ++comp) {
+    float* out = comp ? pB : pR;
+    if (!out) continue;
+    pull(A, g, b, comp, sh, f);
+#pragma unroll
+    for (int l = 0; l < Q; ++l) out[size_t(l) * size_t(g.n) + cell] = float(f[l]);
+  }
+}
+
+// FP64 mass (per component) and momentum of the post-streaming populations,
+// block partial sums combined with FP64 atomics.
+template <typename S>
+__global__ void k_sums(const S* __restrict__ A, Geom g, int ncomp, Shift<typename Store<S>::C> sh,
+                       const int8_t* __restrict__ flags, double* out) {
+  using C = typename Store<S>::C;
+  int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y, z = blockIdx.z;
+  double acc[5] = {0, 0, 0, 0, 0};
+  if (x < g.nx && y < g.ny) {
+    Nbr b;
+    make_nbr(g, x, y, z, b);
+    int cell = at(b, 0, 0, 0);
+    if (!flags || flags[cell] == LBX_FLUID_FLUID) {
+      C f[Q];
+      for (int comp = 0; comp < ncomp; ++comp) {
+        pull(A, g, b, comp, sh, f);
+        double m = 0;
+#pragma unroll
+        for (int l = 0; l < Q; ++l) m += double(f[l]);
+        acc[comp] = m;
+        acc[2] += double(mx(f));
+        acc[3] += double(my(f));
+        acc[4] += double(mz(f));
+      }
+    }
+  }
+  for (int i = 0; i < 5; ++i) {
+    double v = acc[i];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(out + i, v);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+template <typename C>
+static Shift<C> make_shift(const Ctx& c) {
+  Shift<C> s;
+  LatticeT<C> L = make_lattice<C>();
+  bool shifted = (c.storage == LBX_STORE_F16 || c.storage == LBX_STORE_BF16);
+  float r0[2] = {c.p.rho0R, c.p.rho0B};
+  for (int comp = 0; comp < 2; ++comp)
+    for (int k = 0; k < 3; ++k) s.s[comp][k] = shifted ? C(L.w[k] * C(r0[comp])) : C(0);
+  return s;
+}
+
+template <typename C>
+static CGConst<C> make_cg(const Ctx& c) {
+  CGConst<C> K;
+  K.L = make_lattice<C>();
+  const C HALF = C(0.5);
+  C viscR = K.L.cssq * (C(c.p.tauR) - HALF);  // SetConstants, main.CUF:1069-1070
+  C viscB = K.L.cssq * (C(c.p.tauB) - HALF);
+  K.inv_viscR = C(1) / viscR;
+  K.inv_viscB = C(1) / viscB;
+  K.sigma = C(c.p.sigma);
+  K.beta = C(c.p.beta);
+  return K;
+}
+
+static Geom geom(const Ctx& c) { return Geom{c.nx, c.ny, c.nz, c.n}; }
+
+template <typename F>
+static int by_storage(const Ctx& c, F&& fn) {
+  switch (c.storage) {
+    case LBX_STORE_F32: return fn((float*)nullptr);
+    case LBX_STORE_F16: return fn((__half*)nullptr);
+    case LBX_STORE_BF16: return fn((__nv_bfloat16*)nullptr);
+    case LBX_STORE_F64: return fn((double*)nullptr);
+  }
+  return LBX_ERR_ARG;
+}
+
+static int launch_status() {
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? 0 : LBX_ERR_CUDA;
+}
+
+int fluid_alloc(Ctx& c) {
+  size_t bytes = size_t(c.ncomp) * Q * size_t(c.n) * c.elem;
+  for (int i = 0; i < 2; ++i)
+    if (cudaMalloc(&c.pops[i], bytes) != cudaSuccess) return LBX_ERR_ALLOC;
+  size_t cb = (c.storage == LBX_STORE_F64) ? 8 : 4;
+  if (cudaMalloc(&c.phi, size_t(c.n) * cb) != cudaSuccess) return LBX_ERR_ALLOC;
+  for (int i = 0; i < 2; ++i)
+    if (cudaMalloc(&c.rho[i], size_t(c.n) * cb) != cudaSuccess) return LBX_ERR_ALLOC;
+  for (int i = 0; i < 2; ++i) {
+    if (cudaMalloc(&c.flags[i], size_t(c.n)) != cudaSuccess) return LBX_ERR_ALLOC;
+    cudaMemsetAsync(c.flags[i], LBX_FLUID_FLUID, size_t(c.n), c.stream);
+  }
+  cudaMemsetAsync(c.pops[0], 0, bytes, c.stream);
+  cudaMemsetAsync(c.pops[1], 0, bytes, c.stream);
+  return launch_status();
+}
+
+void fluid_free(Ctx& c) {
+  for (int i = 0; i < 2; ++i) {
+    if (c.pops[i]) cudaFree(c.pops[i]);
+    if (c.rho[i]) cudaFree(c.rho[i]);
+    if (c.flags[i]) cudaFree(c.flags[i]);
+    c.pops[i] = nullptr; c.rho[i] = nullptr; c.flags[i] = nullptr;
+  }
+  if (c.phi) cudaFree(c.phi);
+  c.phi = nullptr;
+}
+
+int fluid_set_fields(Ctx& c, const float* d_rR, const float* d_rB, float vx, float vy, float vz) {
+  LaunchDims d = cell_dims(c);
+  Geom g = geom(c);
+  c.cur = 0;
+  return by_storage(c, [&](auto* tag) {
+    using S = std::remove_pointer_t<decltype(tag)>;
+    using C = typename Store<S>::C;
+    k_set_fields<S><<<d.grid, d.block, 0, c.stream>>>((S*)c.pops[0], (S*)c.pops[1], g, c.ncomp, d_rR, d_rB, vx, vy,
+                                                      vz, make_lattice<C>(), make_shift<C>(c));
+    return launch_status();
+  });
+}
+
+int fluid_set_pops(Ctx& c, const float* d_pR, const float* d_pB) {
+  LaunchDims d = cell_dims(c);
+  Geom g = geom(c);
+  c.cur = 0;
+  return by_storage(c, [&](auto* tag) {
+    using S = std::remove_pointer_t<decltype(tag)>;
+    using C = typename Store<S>::C;
+    k_set_pops<S><<<d.grid, d.block, 0, c.stream>>>((S*)c.pops[0], g, c.ncomp, d_pR, d_pB, make_shift<C>(c));
+    return launch_status();
+  });
+}
+
+static void kt_begin(Ctx& c) {
+  if (!c.kt_on) return;
+  if (c.kt_ev.size() < size_t(2 * (c.kt_n + 1))) {
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    c.kt_ev.push_back(e0);
+    c.kt_ev.push_back(e1);
+  }
+  cudaEventRecord(c.kt_ev[2 * c.kt_n], c.stream);
+}
+static void kt_end(Ctx& c) {
+  if (!c.kt_on) return;
+  cudaEventRecord(c.kt_ev[2 * c.kt_n + 1], c.stream);
+  c.kt_n += 1;
+}
+
+int fluid_init_rho(Ctx& c) {
+  if (c.ncomp != 2) return LBX_ERR_STATE;
+  LaunchDims d = cell_dims(c);
+  Geom g = geom(c);
+  return by_storage(c, [&](auto* tag) {
+    using S = std::remove_pointer_t<decltype(tag)>;
+    using C = typename Store<S>::C;
+    k_cg_phi<S><<<d.grid, d.block, 0, c.stream>>>((const S*)c.pops[c.cur], g, make_shift<C>(c), (C*)c.phi,
+                                                  (C*)c.rho[0], (C*)c.rho[1], c.d_err, c.step + 1);
+    return launch_status();
+  });
+}
+
+int fluid_collide_stream(Ctx& c) {
+  if (c.ncomp != 2) return LBX_ERR_STATE;
+  LaunchDims d = cell_dims(c);
+  Geom g = geom(c);
+  return by_storage(c, [&](auto* tag) {
+    using S = std::remove_pointer_t<decltype(tag)>;
+    using C = typename Store<S>::C;
+    kt_begin(c);
+    k_cg_collide<S><<<d.grid, d.block, 0, c.stream>>>((const S*)c.pops[c.cur], (S*)c.pops[1 - c.cur], g,
+                                                      make_shift<C>(c), (const C*)c.phi, make_cg<C>(c));
+    kt_end(c);
+    c.cur = 1 - c.cur;
+    return launch_status();
+  });
+}
+
+// column shape of the single-pass kernel
+constexpr int FTX = 32, FTY = 8;
+
+static int fused_zlen(const Ctx& c) {
+  // enough z-segments to give every SM a few CTAs; longer columns amortise
+  // the two extra planes each segment recomputes
+  long cols = long((c.nx + FTX - 1) / FTX) * long((c.ny + FTY - 1) / FTY);
+  long target = 148L * 4;
+  long segs = (target + cols - 1) / cols;
+  if (segs < 1) segs = 1;
+  int zlen = int((c.nz + segs - 1) / segs);
+  if (zlen < 4) zlen = (c.nz < 4) ? c.nz : 4;
+  return zlen;
+}
+
+int fluid_fused(Ctx& c) {
+  Geom g = geom(c);
+  int zlen = fused_zlen(c);
+  dim3 block(FTX, FTY, 1);
+  dim3 grid((c.nx + FTX - 1) / FTX, (c.ny + FTY - 1) / FTY, (c.nz + zlen - 1) / zlen);
+  return by_storage(c, [&](auto* tag) {
+    using S = std::remove_pointer_t<decltype(tag)>;
+    using C = typename Store<S>::C;
+    kt_begin(c);
+    k_cg_fused<S, FTX, FTY><<<grid, block, 0, c.stream>>>((const S*)c.pops[c.cur], (S*)c.pops[1 - c.cur], g,
+                                                          make_shift<C>(c), make_cg<C>(c), zlen, c.d_err,
+                                                          c.step + 1);
+    kt_end(c);
+    c.cur = 1 - c.cur;
+    return launch_status();
+  });
+}
+
+int fluid_bgk(Ctx& c) {
+  if (c.ncomp != 1) return LBX_ERR_STATE;
+  LaunchDims d = cell_dims(c);
+  Geom g = geom(c);
+  return by_storage(c, [&](auto* tag) {
+    using S = std::remove_pointer_t<decltype(tag)>;
+    using C = typename Store<S>::C;
+    kt_begin(c);
+    k_bgk<S><<<d.grid, d.block, 0, c.stream>>>((const S*)c.pops[c.cur], (S*)c.pops[1 - c.cur], g, make_shift<C>(c),
+                                               make_lattice<C>(), C(1) / C(c.p.tau), c.d_err, c.step + 1);
+    kt_end(c);
+    c.cur = 1 - c.cur;
+    return launch_status();
+  });
+}
+
+int fluid_step(Ctx& c) {
+  int rc;
+  if (c.ncomp == 1) {
+    rc = fluid_bgk(c);
+  } else if (c.fused) {
+    rc = fluid_fused(c);
+  } else {
+    rc = fluid_init_rho(c);
+    if (!rc) rc = fluid_collide_stream(c);
+  }
+  if (!rc) c.step += 1;
+  return rc;
+}
+
+int fluid_get_fields(Ctx& c, void* rR, void* rB, void* vel, void* phase, int f64) {
+  LaunchDims d = cell_dims(c);
+  Geom g = geom(c);
+  return by_storage(c, [&](auto* tag) {
+    using S = std::remove_pointer_t<decltype(tag)>;
+    using C = typename Store<S>::C;
+    if (f64)
+      k_fields<S, double><<<d.grid, d.block, 0, c.stream>>>((const S*)c.pops[c.cur], g, c.ncomp, make_shift<C>(c),
+                                                            nullptr, (double*)rR, (double*)rB, (double*)vel,
+                                                            (double*)phase);
+    else
+      k_fields<S, float><<<d.grid, d.block, 0, c.stream>>>((const S*)c.pops[c.cur], g, c.ncomp, make_shift<C>(c),
+                                                           nullptr, (float*)rR, (float*)rB, (float*)vel,
+                                                           (float*)phase);
+    return launch_status();
+  });
+}
+
+int fluid_get_pops(Ctx& c, float* pR, float* pB) {
+  LaunchDims d = cell_dims(c);
+  Geom g = geom(c);
+  return by_storage(c, [&](auto* tag) {
+    using S = std::remove_pointer_t<decltype(tag)>;
+    using C = typename Store<S>::C;
+    k_get_pops<S><<<d.grid, d.block, 0, c.stream>>>((const S*)c.pops[c.cur], g, c.ncomp, make_shift<C>(c), pR, pB);
+    return launch_status();
+  });
+}
+
+int fluid_get_sums(Ctx& c, double* d_out5) {
+  LaunchDims d = cell_dims(c);
+  Geom g = geom(c);
+  cudaMemsetAsync(d_out5, 0, 5 * sizeof(double), c.stream);
+  return by_storage(c, [&](auto* tag) {
+    using S = std::remove_pointer_t<decltype(tag)>;
+    using C = typename Store<S>::C;
+    k_sums<S><<<d.grid, d.block, 0, c.stream>>>((const S*)c.pops[c.cur], g, c.ncomp, make_shift<C>(c), nullptr, d_out5);
+    return launch_status();
+  });
+}
+
+}  // namespace lbx

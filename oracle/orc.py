@@ -1,0 +1,116 @@
+"""ctypes binding of the CPU oracle (oracle/lbx_oracle.cpp).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, the smoke check and the
+benchmark's CPU baseline / reference arm, never by the product package.
+PARITY UNPINNED: see the header of lbx_oracle.cpp.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+from lbcuda_b200.capi import LbxParams
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = os.path.join(_HERE, "liblbx_oracle.so")
+Q = 19
+MODES = {"ref": 0, "f32p64": 1, "f64": 2}
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB):
+            from . import build
+            build.build()
+        L = C.CDLL(_LIB)
+        P = C.c_void_p
+        L.orc_create.restype = P
+        L.orc_create.argtypes = [C.POINTER(LbxParams), C.c_int]
+        L.orc_destroy.argtypes = [P]
+        L.orc_set_fields.argtypes = [P, C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_float, C.c_float, C.c_float]
+        L.orc_set_pops.argtypes = [P, C.POINTER(C.c_float), C.POINTER(C.c_float)]
+        L.orc_step.argtypes = [P, C.c_int]
+        D = C.POINTER(C.c_double)
+        L.orc_get_fields.argtypes = [P, D, D, D, D]
+        L.orc_get_pops.argtypes = [P, D, D]
+        L.orc_get_flags.argtypes = [P, C.POINTER(C.c_int8)]
+        L.orc_status.argtypes = [P, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int64)]
+        L.orc_num_threads.restype = C.c_int
+        _lib = L
+    return _lib
+
+
+def num_threads():
+    return lib().orc_num_threads()
+
+
+def _p(a, t):
+    return a.ctypes.data_as(C.POINTER(t)) if a is not None else None
+
+
+class OracleSim:
+    """Same surface as lbcuda_b200.LBSim, computed by the CPU restatement."""
+
+    def __init__(self, params, mode="ref"):
+        self.params = params
+        self.nx, self.ny, self.nz = params.nx, params.ny, params.nz
+        self.ncomp = 2 if params.model == 1 else 1
+        self._L = lib()
+        self._h = self._L.orc_create(C.byref(params), MODES[mode])
+        if not self._h:
+            raise RuntimeError("orc_create failed")
+
+    @property
+    def shape(self):
+        return (self.nz, self.ny, self.nx)
+
+    def close(self):
+        if self._h:
+            self._L.orc_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_fields(self, rhoR, rhoB=None, vel=(0.0, 0.0, 0.0)):
+        rR = np.ascontiguousarray(rhoR, dtype=np.float32)
+        rB = None if rhoB is None else np.ascontiguousarray(rhoB, dtype=np.float32)
+        self._L.orc_set_fields(self._h, _p(rR, C.c_float), _p(rB, C.c_float), *map(float, vel))
+
+    def set_pops(self, popsR, popsB=None):
+        pR = np.ascontiguousarray(popsR, dtype=np.float32)
+        pB = None if popsB is None else np.ascontiguousarray(popsB, dtype=np.float32)
+        self._L.orc_set_pops(self._h, _p(pR, C.c_float), _p(pB, C.c_float))
+
+    def step(self, n=1):
+        return self._L.orc_step(self._h, int(n))
+
+    def get_fields(self):
+        rR = np.empty(self.shape)
+        rB = np.empty(self.shape)
+        vel = np.empty(self.shape + (3,))
+        ph = np.empty(self.shape)
+        D = C.c_double
+        self._L.orc_get_fields(self._h, _p(rR, D), _p(rB, D), _p(vel, D), _p(ph, D))
+        return rR, rB, vel, ph
+
+    def get_pops(self):
+        pR = np.empty((Q,) + self.shape)
+        pB = np.empty((Q,) + self.shape)
+        self._L.orc_get_pops(self._h, _p(pR, C.c_double), _p(pB, C.c_double))
+        return pR, (pB if self.ncomp == 2 else None)
+
+    def get_flags(self):
+        f = np.empty(self.shape, np.int8)
+        self._L.orc_get_flags(self._h, _p(f, C.c_int8))
+        return f
+
+    def status(self):
+        c, s, w = C.c_int(), C.c_int(), C.c_int64()
+        self._L.orc_status(self._h, C.byref(c), C.byref(s), C.byref(w))
+        return c.value, s.value, w.value

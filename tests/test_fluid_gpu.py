@@ -1,0 +1,174 @@
+"""Parity of the CUDA fluid path against the CPU oracle, through the C ABI.
+
+Tolerances (stated here, per field, as max|gpu - oracle| / max|oracle|):
+  FP32 storage vs the FP32 oracle (reference precision):   1e-5
+  FP64 storage vs the FP64 oracle:                         1e-12
+  FP16/BF16 shifted storage vs the GPU's FP64 run: bounds in the tests below.
+"""
+import numpy as np
+import pytest
+
+from lbcuda_b200 import LBSim, make_params
+from lbcuda_b200.inputs import seeded_noise_fields
+from oracle.orc import OracleSim
+
+pytestmark = pytest.mark.gpu
+
+TOL32 = 1e-5
+TOL64 = 1e-12
+
+
+def rel(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-30))
+
+
+def compare_fields(g, o, tol, what):
+    names = ("rhoR", "rhoB", "vel", "phase")
+    for name, a, b in zip(names, g, o):
+        if b is None:
+            continue
+        e = rel(a, b)
+        assert e <= tol, f"{what}: {name} rel err {e:.3e} > {tol:.1e}"
+
+
+def run_pair(params, rR, rB, vel, nsteps, mode="ref", fused=None):
+    g = LBSim(params)
+    if fused is not None:
+        g.set_schedule(fused)
+    g.set_fields(rR, rB, vel)
+    g.step(nsteps)
+    o = OracleSim(params, mode)
+    o.set_fields(rR, rB, vel)
+    assert o.step(nsteps) == 0
+    return g, o
+
+
+@pytest.mark.parametrize("shape", [(32, 32, 32), (48, 20, 16)])
+def test_bgk_f32_matches_oracle(shape):
+    nx, ny, nz = shape
+    p = make_params(nx, ny, nz, model="bgk", storage="f32", tau=0.8)
+    rho = seeded_noise_fields(nx, ny, nz, mean=1.0, amp=1e-3, seed=11, ncomp=1)[0]
+    g, o = run_pair(p, rho, None, (0.02, -0.01, 0.005), 40)
+    gf = g.get_fields()
+    of = o.get_fields()
+    compare_fields((gf[0], None, gf[2], None), (of[0], None, of[2], None), TOL32, "bgk")
+    pg = g.get_pops()[0]
+    po = o.get_pops()[0]
+    assert rel(pg, po) <= TOL32
+
+
+@pytest.mark.parametrize("fused", [1, 0])
+@pytest.mark.parametrize("shape", [(32, 32, 32), (40, 24, 20)])
+def test_cg_f32_matches_oracle(shape, fused):
+    nx, ny, nz = shape
+    p = make_params(nx, ny, nz, model="cg", storage="f32", sigma=0.02, beta=0.7)
+    rR, rB = seeded_noise_fields(nx, ny, nz, seed=5)
+    g, o = run_pair(p, rR, rB, (0.0, 0.0, 0.0), 30, fused=fused)
+    compare_fields(g.get_fields(), o.get_fields(), TOL32, f"cg fused={fused}")
+    pg = g.get_pops()
+    po = o.get_pops()
+    assert rel(pg[0], po[0]) <= TOL32 and rel(pg[1], po[1]) <= TOL32
+
+
+def test_cg_droplet_reference_constants():
+    """initType 1 droplet with the reference's sigma=0.1, beta=0.999 and a flow."""
+    from lbcuda_b200.inputs import initial_fields
+    n = 32
+    p = make_params(n, model="cg", storage="f32")
+    rR, rB = initial_fields(1, n, n, n)
+    g, o = run_pair(p, rR, rB, (0.05, 0.05, 0.05), 25)
+    compare_fields(g.get_fields(), o.get_fields(), TOL32, "droplet")
+
+
+def test_cg_f64_matches_oracle_f64():
+    n = 24
+    p = make_params(n, model="cg", storage="f64", sigma=0.02, beta=0.7)
+    rR, rB = seeded_noise_fields(n, n, n, seed=3)
+    g = LBSim(p)
+    g.set_fields(rR, rB)
+    g.step(20)
+    o = OracleSim(p, "f64")
+    o.set_fields(rR, rB)
+    o.step(20)
+    compare_fields(g.get_fields(f64=True), o.get_fields(), TOL64, "cg f64")
+
+
+def test_fused_equals_two_pass():
+    n = 32
+    p = make_params(n, model="cg", storage="f32", sigma=0.02, beta=0.7)
+    rR, rB = seeded_noise_fields(n, n, n, seed=9)
+    out = []
+    for fused in (1, 0):
+        g = LBSim(p)
+        g.set_schedule(fused)
+        g.set_fields(rR, rB)
+        g.step(15)
+        out.append(g.get_pops())
+    assert rel(out[0][0], out[1][0]) <= 1e-6 and rel(out[0][1], out[1][1]) <= 1e-6
+
+
+def test_set_pops_get_pops_roundtrip():
+    n = 16
+    p = make_params(n, model="cg", storage="f32")
+    rng = np.random.default_rng(0)
+    pR = rng.uniform(0.0, 0.1, (19, n, n, n)).astype(np.float32)
+    pB = rng.uniform(0.0, 0.1, (19, n, n, n)).astype(np.float32)
+    g = LBSim(p)
+    g.set_pops(pR, pB)
+    a, b = g.get_pops()
+    assert np.array_equal(a, pR) and np.array_equal(b, pB)
+
+
+def test_equilibrium_and_uniform_flow_are_fixed_points():
+    n = 32
+    for storage, tol in (("f32", 2e-6), ("f16", 2e-3), ("f64", 1e-13)):
+        p = make_params(n, model="cg", storage=storage)
+        g = LBSim(p)
+        r = np.full((n, n, n), 0.5, np.float32)
+        g.set_fields(r, r, (0.05, -0.02, 0.03))
+        g.step(10)
+        rR, rB, vel, ph = g.get_fields(f64=True)
+        assert np.abs(rR - 0.5).max() < tol * 0.5 + 1e-7, storage
+        assert np.abs(vel - np.array([0.05, -0.02, 0.03])).max() < tol * 0.05 + 1e-7, storage
+
+
+@pytest.mark.parametrize("storage,tol", [("f32", 1e-6), ("f16", 1e-6), ("bf16", 1e-6), ("f64", 1e-12)])
+def test_mass_conservation_full_size(storage, tol):
+    """128^3 spinodal: FP64 sums of each component's mass are conserved by the step.
+
+    The 16-bit storages round each population, so their check compares the
+    FP64 sum after a step with the FP64 sum of the rounded state before it.
+    """
+    n = 128
+    p = make_params(n, model="cg", storage=storage, sigma=0.02, beta=0.7)
+    rR, rB = seeded_noise_fields(n, n, n, seed=1)
+    g = LBSim(p)
+    g.set_fields(rR, rB)
+    g.step(1)
+    m0, _ = g.get_sums()
+    g.step(50)
+    m1, _ = g.get_sums()
+    drift = np.abs(m1 - m0) / m0
+    assert (drift <= tol).all(), (storage, drift)
+
+
+@pytest.mark.parametrize("storage,bound_u,bound_phi", [("f16", 5e-2, 1e-2), ("bf16", 3e-1, 5e-2)])
+def test_16bit_storage_error_vs_f64(storage, bound_u, bound_phi):
+    """Relative L2 error of |u| and of phi after 200 steps vs the FP64 run."""
+    n = 48
+    rR, rB = seeded_noise_fields(n, n, n, seed=2)
+    res = {}
+    for st in ("f64", storage):
+        p = make_params(n, model="cg", storage=st, sigma=0.02, beta=0.7)
+        g = LBSim(p)
+        g.set_fields(rR, rB)
+        g.step(200)
+        res[st] = g.get_fields(f64=True)
+    u64 = res["f64"][2]
+    u16 = res[storage][2]
+    eu = np.linalg.norm(u16 - u64) / np.linalg.norm(u64)
+    ep = np.linalg.norm(res[storage][3] - res["f64"][3]) / np.linalg.norm(res["f64"][3])
+    print(f"{storage}: rel L2 err u {eu:.3e} phi {ep:.3e}")
+    assert eu <= bound_u and ep <= bound_phi
