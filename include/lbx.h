@@ -118,6 +118,20 @@ int lbx_set_fields(void* ctx, const float* rhoR, const float* rhoB, float vx, fl
 /* initType 4 (read_and_setPops, main.CUF:2489-2529): raw populations. */
 int lbx_set_pops(void* ctx, const float* popsR, const float* popsB);
 
+/* ---- particles --------------------------------------------------------- */
+/* read_input_atom (main.CUF:1230-1350) + the step-0 flags of setupRho_Pops
+ * (main.CUF:2586-2600): n spheres of radius p->radius at xyz (3,n), with
+ * velocities vel (3,n), body-frame angular velocities omega (3,n, may be
+ * NULL) and quaternions q (4,n, may be NULL = identity).  Needs a CG context
+ * created with max_particles >= n and nx % 8 == ny % 4 == nz % 4 == 0 (the
+ * reference's tile grid).  Call after lbx_set_fields. */
+int lbx_set_particles(void* ctx, int32_t n, const double* xyz, const double* vel, const double* omega,
+                      const double* q);
+/* Particle state after the last step and the total force / torque its
+ * integrator used (forceAtoms_d(1:3) and (7:9), kernels_fluid_PART.CUF:
+ * 1266-1382); any pointer may be NULL. */
+int lbx_get_particles(void* ctx, double* xyz, double* vel, double* omega, double* q, double* force, double* torque);
+
 /* ---- the time step ----------------------------------------------------- */
 /* One or more full steps in the order of main.CUF:125-308 (fluid: moments,
  * collision, streaming; with particles also flags, fill/drain, wetting,

@@ -63,6 +63,8 @@ SIGNATURES = {
     "lbx_get_pops": (C.c_int, [_P, _F, _F]),
     "lbx_get_flags": (C.c_int, [_P, _I8]),
     "lbx_get_sums": (C.c_int, [_P, _D, _D]),
+    "lbx_set_particles": (C.c_int, [_P, C.c_int32, _D, _D, _D, _D]),
+    "lbx_get_particles": (C.c_int, [_P, _D, _D, _D, _D, _D, _D]),
     "lbx_sync": (C.c_int, [_P]),
     "lbx_status": (C.c_int, [_P, _I32, _I32, _I64]),
     "lbx_error_string": (C.c_char_p, [C.c_int]),

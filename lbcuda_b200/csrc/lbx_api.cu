@@ -19,8 +19,11 @@
 namespace lbx {
 int particles_create(Ctx& c);
 void particles_destroy(Ctx& c);
-int particles_step_pre(Ctx& c);
-int particles_step_post(Ctx& c);
+int particles_set(Ctx& c, int n, const double* x, const double* v, const double* om, const double* q);
+int particles_get(Ctx& c, double* x, double* v, double* om, double* q, double* f, double* t);
+int particles_step(Ctx& c);
+int particles_flags_slot(const Ctx& c);
+int particles_active(const Ctx& c);
 }  // namespace lbx
 
 using lbx::Ctx;
@@ -181,11 +184,9 @@ int lbx_set_pops(void* ctx, const float* popsR, const float* popsB) {
 int lbx_step(void* ctx, int32_t nsteps) {
   Ctx* c = as_ctx(ctx);
   if (!c || nsteps < 0) return LBX_ERR_ARG;
+  const bool parts = lbx::particles_active(*c);
   for (int s = 0; s < nsteps; ++s) {
-    int rc = 0;
-    if (c->part) rc = lbx::particles_step_pre(*c);
-    if (!rc) rc = lbx::fluid_step(*c);
-    if (!rc && c->part) rc = lbx::particles_step_post(*c);
+    int rc = parts ? lbx::particles_step(*c) : lbx::fluid_step(*c);
     if (rc) return rc;
   }
   return 0;
@@ -265,7 +266,8 @@ int lbx_get_pops(void* ctx, float* popsR, float* popsB) {
 int lbx_get_flags(void* ctx, int8_t* flags) {
   Ctx* c = as_ctx(ctx);
   if (!c || !flags) return LBX_ERR_ARG;
-  int rc = cuda_rc(cudaMemcpyAsync(flags, c->flags[c->fcur], size_t(c->n), cudaMemcpyDeviceToHost, c->stream));
+  int rc = cuda_rc(cudaMemcpyAsync(flags, c->flags[lbx::particles_flags_slot(*c)], size_t(c->n),
+                                   cudaMemcpyDeviceToHost, c->stream));
   if (!rc) rc = sync_status(*c);
   return rc;
 }
@@ -283,6 +285,22 @@ int lbx_get_sums(void* ctx, double* mass, double* momentum) {
     if (mass) { mass[0] = h[0]; mass[1] = h[1]; }
     if (momentum) { momentum[0] = h[2]; momentum[1] = h[3]; momentum[2] = h[4]; }
   }
+  return rc;
+}
+
+int lbx_set_particles(void* ctx, int32_t n, const double* xyz, const double* vel, const double* omega,
+                      const double* q) {
+  Ctx* c = as_ctx(ctx);
+  if (!c || !xyz || n < 1) return LBX_ERR_ARG;
+  if (!c->part) return LBX_ERR_STATE;
+  return lbx::particles_set(*c, n, xyz, vel, omega, q);
+}
+
+int lbx_get_particles(void* ctx, double* xyz, double* vel, double* omega, double* q, double* force, double* torque) {
+  Ctx* c = as_ctx(ctx);
+  if (!c) return LBX_ERR_ARG;
+  int rc = lbx::particles_get(*c, xyz, vel, omega, q, force, torque);
+  if (!rc) rc = sync_status(*c);
   return rc;
 }
 

@@ -54,6 +54,7 @@ struct LatticeT {
   C w[3];        // p0, p1, p2
   C b[3];        // b_l classes (Leclaire, b_xi = 0.5)
   C a27[4];      // ad3q27 classes (0, p1/cssq, p2/cssq, p3/cssq)
+  C p27[4];      // pd3q27 classes (D3Q27 weights, dimensions_m.CUF:283-290)
   C rec[3];      // rec_fact classes: 0, 1, sqrt(2)
   C cssq;        // 1/3
   C inv_cssq;    // 1/cssq
@@ -75,6 +76,10 @@ inline LatticeT<C> make_lattice() {
   const C q1 = (TWO / THREE) * (TWO / THREE) * (ONE / SIX);
   const C q2 = (ONE / SIX) * (ONE / SIX) * (TWO / THREE);
   const C q3 = (ONE / SIX) * (ONE / SIX) * (ONE / SIX);
+  L.p27[0] = (TWO / THREE) * (TWO / THREE) * (TWO / THREE);
+  L.p27[1] = q1;
+  L.p27[2] = q2;
+  L.p27[3] = q3;
   L.a27[0] = 0;
   L.a27[1] = q1 / L.cssq;
   L.a27[2] = q2 / L.cssq;

@@ -1,0 +1,253 @@
+// lbx_device.cuh — device helpers shared by the fluid and particle kernels:
+// periodic neighbour indexing, pull gathers, the equilibrium, the
+// colour-gradient collision of one cell and the host-side constant builders.
+#pragma once
+#include <type_traits>
+
+#include "lbx_common.cuh"
+#include "lbx_ctx.h"
+
+namespace lbx {
+
+// ---------------------------------------------------------------------------
+// indexing
+// ---------------------------------------------------------------------------
+struct Nbr {
+  int x, xm, xp;  // column index and its periodic neighbours
+  int ry[3];      // ny-row offsets (y-1, y, y+1) * nx
+  int rz[3];      // plane offsets (z-1, z, z+1) * nx * ny
+};
+
+__device__ __forceinline__ void make_nbr(const Geom& g, int x, int y, int z, Nbr& b) {
+  b.x = x;
+  b.xm = (x == 0) ? g.nx - 1 : x - 1;
+  b.xp = (x == g.nx - 1) ? 0 : x + 1;
+  int ym = (y == 0) ? g.ny - 1 : y - 1, yp = (y == g.ny - 1) ? 0 : y + 1;
+  int zm = (z == 0) ? g.nz - 1 : z - 1, zp = (z == g.nz - 1) ? 0 : z + 1;
+  b.ry[0] = ym * g.nx; b.ry[1] = y * g.nx; b.ry[2] = yp * g.nx;
+  const int plane = g.nx * g.ny;
+  b.rz[0] = zm * plane; b.rz[1] = z * plane; b.rz[2] = zp * plane;
+}
+
+// linear index of x + (dx,dy,dz), periodic
+__device__ __forceinline__ int at(const Nbr& b, int dx, int dy, int dz) {
+  int xx = dx == 0 ? b.x : (dx > 0 ? b.xp : b.xm);
+  return xx + b.ry[dy + 1] + b.rz[dz + 1];
+}
+
+// e_l . (u,v,w) with the zero components dropped, summed in x,y,z order
+template <typename C>
+__device__ __forceinline__ C edot(int l, C u, C v, C w) {
+  C s = C(0);
+  bool any = false;
+  if (ex(l)) { s = ex(l) > 0 ? u : -u; any = true; }
+  if (ey(l)) { s = any ? (ey(l) > 0 ? s + v : s - v) : (ey(l) > 0 ? v : -v); any = true; }
+  if (ez(l)) { s = any ? (ez(l) > 0 ? s + w : s - w) : (ez(l) > 0 ? w : -w); any = true; }
+  return s;
+}
+
+// equil, kernels_fluid_CG.CUF:30-38, with the velocity-square term hoisted
+template <typename C>
+__device__ __forceinline__ C equil_u(const LatticeT<C>& L, C rho, C edu, C usq_term, int l) {
+  C uv = L.inv_cssq * edu;
+  return rho * L.w[wclass(l)] * (C(1) + uv + C(0.5) * (uv * uv) - usq_term);
+}
+
+// gather the post-streaming populations of one component (pull of the push
+// streaming of stream*_CG + halo pushes)
+template <typename S, typename C>
+__device__ __forceinline__ void pull(const S* __restrict__ A, const Geom& g, const Nbr& b, int comp,
+                                     const Shift<C>& sh, C f[Q]) {
+  const S* base = A + size_t(comp) * Q * size_t(g.n);
+#pragma unroll
+  for (int l = 0; l < Q; ++l)
+    f[l] = Store<S>::ld(base + size_t(l) * size_t(g.n) + at(b, -ex(l), -ey(l), -ez(l)), sh.at(comp, l));
+}
+
+template <typename S, typename C>
+__device__ __forceinline__ void store_all(S* __restrict__ B, const Geom& g, int cell, int comp, const Shift<C>& sh,
+                                          const C f[Q]) {
+  S* base = B + size_t(comp) * Q * size_t(g.n) + cell;
+#pragma unroll
+  for (int l = 0; l < Q; ++l) Store<S>::st(base + size_t(l) * size_t(g.n), f[l], sh.at(comp, l));
+}
+
+// The post-streaming populations of a cell, pulled from the post-collision
+// state A; a spheredead source (flags of the previous step) leaves the
+// destination's stale value, which is B's entry.
+template <typename S, typename C>
+__device__ __forceinline__ void pull_dead(const S* __restrict__ A, const S* Bold, const Geom& g, const Nbr& b,
+                                          int comp, const Shift<C>& sh, const int8_t* __restrict__ fold, C f[Q]) {
+  const S* base = A + size_t(comp) * Q * size_t(g.n);
+  const S* bb = Bold + size_t(comp) * Q * size_t(g.n);
+  const int self = at(b, 0, 0, 0);
+#pragma unroll
+  for (int l = 0; l < Q; ++l) {
+    int src = at(b, -ex(l), -ey(l), -ez(l));
+    if (l > 0 && fold[src] == LBX_FLUID_SPHEREDEAD)
+      f[l] = Store<S>::ld(bb + size_t(l) * size_t(g.n) + self, sh.at(comp, l));
+    else
+      f[l] = Store<S>::ld(base + size_t(l) * size_t(g.n) + src, sh.at(comp, l));
+  }
+}
+
+// pull_dead when the flags of the previous step are given, plain pull otherwise
+template <typename S, typename C>
+__device__ __forceinline__ void pull_any(const S* __restrict__ A, const S* Bold, const Geom& g, const Nbr& b,
+                                         int comp, const Shift<C>& sh, const int8_t* __restrict__ fold, C f[Q]) {
+  if (fold) pull_dead(A, Bold, g, b, comp, sh, fold, f);
+  else pull(A, g, b, comp, sh, f);
+}
+
+template <typename C>
+__device__ __forceinline__ C sum_q(const C f[Q]) {
+  C r = f[0];
+#pragma unroll
+  for (int l = 1; l < Q; ++l) r = r + f[l];
+  return r;
+}
+// manual_u/v/w sums, kernels_fluid_CG.CUF:511-529 (without the 1/rho factor)
+template <typename C> __device__ __forceinline__ C mx(const C q[Q]) { return q[1] - q[2] + q[7] - q[8] - q[9] + q[10] + q[11] - q[12] - q[13] + q[14]; }
+template <typename C> __device__ __forceinline__ C my(const C q[Q]) { return q[3] - q[4] + q[7] - q[8] + q[9] - q[10] + q[15] - q[16] - q[17] + q[18]; }
+template <typename C> __device__ __forceinline__ C mz(const C q[Q]) { return q[5] - q[6] + q[11] - q[12] + q[13] - q[14] + q[15] - q[16] + q[17] - q[18]; }
+
+// Constants of the colour-gradient collision, derived on the host like
+// SetConstants (main.CUF:1043-1162).
+template <typename C>
+struct CGConst {
+  LatticeT<C> L;
+  C inv_viscR, inv_viscB;  // 1/viscR, 1/viscB
+  C sigma, beta;
+};
+
+// ---------------------------------------------------------------------------
+// time_step_CG at one fluid cell (kernels_fluid_CG.CUF:689-846).  fR/fB hold
+// the post-streaming populations on entry and the post-collision ones on exit.
+// rhoR/rhoB are the clamped densities of init_rho*_CG, psi the colour
+// gradient (HIGHGRAD, D3Q27 weights).
+// ---------------------------------------------------------------------------
+template <typename C>
+__device__ __forceinline__ void cg_collide_cell(const CGConst<C>& K, C fR[Q], C fB[Q], C rhoR, C rhoB, C psix,
+                                                C psiy, C psiz) {
+  const C ONE = 1, HALF = C(0.5);
+  const LatticeT<C>& L = K.L;
+  C rhosum = rhoR + rhoB;
+  C phase_field = (rhoR - rhoB) / (rhoR + rhoB);
+  C viscavg = ONE / (HALF * (ONE + phase_field) * K.inv_viscR + HALF * (ONE - phase_field) * K.inv_viscB);
+  C omega = ONE / (viscavg / L.cssq + HALF);
+  C omm = ONE - omega;
+  C invrho = ONE / rhosum;
+  C u = invrho * mx(fR) + invrho * mx(fB);
+  C v = invrho * my(fR) + invrho * my(fB);
+  C w = invrho * mz(fR) + invrho * mz(fB);
+  C usq = L.half_inv_cssq * (u * u + v * v + w * w);
+#pragma unroll
+  for (int l = 0; l < Q; ++l) {
+    C e = edot(l, u, v, w);
+    fR[l] = fR[l] * omm + equil_u(L, rhoR, e, usq, l) * omega;
+    fB[l] = fB[l] * omm + equil_u(L, rhoB, e, usq, l) * omega;
+  }
+  C psinorm_sq = psix * psix + psiy * psiy + psiz * psiz;
+  if (psinorm_sq > C(1.e-20)) {
+    C psinorm = sqrt(psinorm_sq);
+    C inv_psq = ONE / psinorm_sq;
+    C acoeff = C(9) / C(4) * omega * K.sigma;
+    C kR = rhoR * invrho, kB = rhoB * invrho;
+    C coef = K.beta * rhoR * rhoB * (invrho * invrho);
+    C inv_t1 = ONE / psinorm;                 // rec_fact = 1
+    C inv_t2 = ONE / (L.rec[2] * psinorm);    // rec_fact = sqrt(2)
+#pragma unroll
+    for (int l = 0; l < Q; ++l) {
+      C edp = edot(l, psix, psiy, psiz);
+      C temp = psinorm * (L.w[wclass(l)] * (edp * edp) * inv_psq - L.b[wclass(l)]);
+      C fd = fR[l] + fB[l] + acoeff * temp;
+      C feq = rhoR * L.w[wclass(l)] + rhoB * L.w[wclass(l)];
+      C cosphi;
+      if (l == 0) cosphi = C(0);
+      else {
+        C t1 = L.rec[wclass(l)] * psinorm;
+        cosphi = (t1 <= C(1.e-20)) ? C(0) : edp * (wclass(l) == 1 ? inv_t1 : inv_t2);
+      }
+      C t = coef * cosphi;
+      fR[l] = fd * kR + t * feq;
+      fB[l] = fd * kB - t * feq;
+    }
+  }
+}
+
+// colour gradient psi = sum_l a27_l e_l phi(x + e_l), l = 1..26 in reference order
+template <typename C, typename F>
+__device__ __forceinline__ void grad27(const LatticeT<C>& L, F&& phi_at, C& psix, C& psiy, C& psiz) {
+  psix = C(0); psiy = C(0); psiz = C(0);
+#pragma unroll
+  for (int l = 1; l < Q27; ++l) {
+    C ps = phi_at(ex27(l), ey27(l), ez27(l));
+    C a = L.a27[wclass27(l)];
+    if (ex27(l)) psix = psix + (ex27(l) > 0 ? a : -a) * ps;
+    if (ey27(l)) psiy = psiy + (ey27(l) > 0 ? a : -a) * ps;
+    if (ez27(l)) psiz = psiz + (ez27(l) > 0 ? a : -a) * ps;
+  }
+}
+
+
+// ---------------------------------------------------------------------------
+// launch geometry and host-side constant builders
+// ---------------------------------------------------------------------------
+struct LaunchDims {
+  dim3 grid, block;
+};
+
+inline LaunchDims cell_dims(const Ctx& c) {
+  int bx = (c.nx % 128 == 0) ? 128 : ((c.nx % 64 == 0) ? 64 : 32);
+  int by = 256 / bx;
+  LaunchDims d;
+  d.block = dim3(bx, by, 1);
+  d.grid = dim3((c.nx + bx - 1) / bx, (c.ny + by - 1) / by, c.nz);
+  return d;
+}
+
+template <typename C>
+inline Shift<C> make_shift(const Ctx& c) {
+  Shift<C> s;
+  LatticeT<C> L = make_lattice<C>();
+  bool shifted = (c.storage == LBX_STORE_F16 || c.storage == LBX_STORE_BF16);
+  float r0[2] = {c.p.rho0R, c.p.rho0B};
+  for (int comp = 0; comp < 2; ++comp)
+    for (int k = 0; k < 3; ++k) s.s[comp][k] = shifted ? C(L.w[k] * C(r0[comp])) : C(0);
+  return s;
+}
+
+template <typename C>
+inline CGConst<C> make_cg(const Ctx& c) {
+  CGConst<C> K;
+  K.L = make_lattice<C>();
+  const C HALF = C(0.5);
+  C viscR = K.L.cssq * (C(c.p.tauR) - HALF);  // SetConstants, main.CUF:1069-1070
+  C viscB = K.L.cssq * (C(c.p.tauB) - HALF);
+  K.inv_viscR = C(1) / viscR;
+  K.inv_viscB = C(1) / viscB;
+  K.sigma = C(c.p.sigma);
+  K.beta = C(c.p.beta);
+  return K;
+}
+
+inline Geom geom(const Ctx& c) { return Geom{c.nx, c.ny, c.nz, c.n}; }
+
+template <typename F>
+inline int by_storage(const Ctx& c, F&& fn) {
+  switch (c.storage) {
+    case LBX_STORE_F32: return fn((float*)nullptr);
+    case LBX_STORE_F16: return fn((__half*)nullptr);
+    case LBX_STORE_BF16: return fn((__nv_bfloat16*)nullptr);
+    case LBX_STORE_F64: return fn((double*)nullptr);
+  }
+  return LBX_ERR_ARG;
+}
+
+inline int launch_status() {
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? 0 : LBX_ERR_CUDA;
+}
+
+
+}  // namespace lbx

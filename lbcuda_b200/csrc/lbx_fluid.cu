@@ -23,182 +23,15 @@
 //   and marches it along z, computing the phase field of its own cells and of
 //   a one-cell ring around the column from the pulled populations into a
 //   rolling 3-plane shared-memory window, so phi never goes through HBM.
-#include "lbx_common.cuh"
-#include "lbx_ctx.h"
+#include "lbx_device.cuh"
 
 #include <cstdio>
 
 namespace lbx {
 
 // ---------------------------------------------------------------------------
-// indexing
-// ---------------------------------------------------------------------------
-struct Nbr {
-  int x, xm, xp;  // column index and its periodic neighbours
-  int ry[3];      // ny-row offsets (y-1, y, y+1) * nx
-  int rz[3];      // plane offsets (z-1, z, z+1) * nx * ny
-};
-
-__device__ __forceinline__ void make_nbr(const Geom& g, int x, int y, int z, Nbr& b) {
-  b.x = x;
-  b.xm = (x == 0) ? g.nx - 1 : x - 1;
-  b.xp = (x == g.nx - 1) ? 0 : x + 1;
-  int ym = (y == 0) ? g.ny - 1 : y - 1, yp = (y == g.ny - 1) ? 0 : y + 1;
-  int zm = (z == 0) ? g.nz - 1 : z - 1, zp = (z == g.nz - 1) ? 0 : z + 1;
-  b.ry[0] = ym * g.nx; b.ry[1] = y * g.nx; b.ry[2] = yp * g.nx;
-  const int plane = g.nx * g.ny;
-  b.rz[0] = zm * plane; b.rz[1] = z * plane; b.rz[2] = zp * plane;
-}
-
-// linear index of x + (dx,dy,dz), periodic
-__device__ __forceinline__ int at(const Nbr& b, int dx, int dy, int dz) {
-  int xx = dx == 0 ? b.x : (dx > 0 ? b.xp : b.xm);
-  return xx + b.ry[dy + 1] + b.rz[dz + 1];
-}
-
-// e_l . (u,v,w) with the zero components dropped, summed in x,y,z order
-template <typename C>
-__device__ __forceinline__ C edot(int l, C u, C v, C w) {
-  C s = C(0);
-  bool any = false;
-  if (ex(l)) { s = ex(l) > 0 ? u : -u; any = true; }
-  if (ey(l)) { s = any ? (ey(l) > 0 ? s + v : s - v) : (ey(l) > 0 ? v : -v); any = true; }
-  if (ez(l)) { s = any ? (ez(l) > 0 ? s + w : s - w) : (ez(l) > 0 ? w : -w); any = true; }
-  return s;
-}
-
-// equil, kernels_fluid_CG.CUF:30-38, with the velocity-square term hoisted
-template <typename C>
-__device__ __forceinline__ C equil_u(const LatticeT<C>& L, C rho, C edu, C usq_term, int l) {
-  C uv = L.inv_cssq * edu;
-  return rho * L.w[wclass(l)] * (C(1) + uv + C(0.5) * (uv * uv) - usq_term);
-}
-
-// gather the post-streaming populations of one component (pull of the push
-// streaming of stream*_CG + halo pushes)
-template <typename S, typename C>
-__device__ __forceinline__ void pull(const S* __restrict__ A, const Geom& g, const Nbr& b, int comp,
-                                     const Shift<C>& sh, C f[Q]) {
-  const S* base = A + size_t(comp) * Q * size_t(g.n);
-#pragma unroll
-  for (int l = 0; l < Q; ++l)
-    f[l] = Store<S>::ld(base + size_t(l) * size_t(g.n) + at(b, -ex(l), -ey(l), -ez(l)), sh.at(comp, l));
-}
-
-template <typename S, typename C>
-__device__ __forceinline__ void store_all(S* __restrict__ B, const Geom& g, int cell, int comp, const Shift<C>& sh,
-                                          const C f[Q]) {
-  S* base = B + size_t(comp) * Q * size_t(g.n) + cell;
-#pragma unroll
-  for (int l = 0; l < Q; ++l) Store<S>::st(base + size_t(l) * size_t(g.n), f[l], sh.at(comp, l));
-}
-
-template <typename C>
-__device__ __forceinline__ C sum_q(const C f[Q]) {
-  C r = f[0];
-#pragma unroll
-  for (int l = 1; l < Q; ++l) r = r + f[l];
-  return r;
-}
-// manual_u/v/w sums, kernels_fluid_CG.CUF:511-529 (without the 1/rho factor)
-template <typename C> __device__ __forceinline__ C mx(const C q[Q]) { return q[1] - q[2] + q[7] - q[8] - q[9] + q[10] + q[11] - q[12] - q[13] + q[14]; }
-template <typename C> __device__ __forceinline__ C my(const C q[Q]) { return q[3] - q[4] + q[7] - q[8] + q[9] - q[10] + q[15] - q[16] - q[17] + q[18]; }
-template <typename C> __device__ __forceinline__ C mz(const C q[Q]) { return q[5] - q[6] + q[11] - q[12] + q[13] - q[14] + q[15] - q[16] + q[17] - q[18]; }
-
-// Constants of the colour-gradient collision, derived on the host like
-// SetConstants (main.CUF:1043-1162).
-template <typename C>
-struct CGConst {
-  LatticeT<C> L;
-  C inv_viscR, inv_viscB;  // 1/viscR, 1/viscB
-  C sigma, beta;
-};
-
-// ---------------------------------------------------------------------------
-// time_step_CG at one fluid cell (kernels_fluid_CG.CUF:689-846).  fR/fB hold
-// the post-streaming populations on entry and the post-collision ones on exit.
-// rhoR/rhoB are the clamped densities of init_rho*_CG, psi the colour
-// gradient (HIGHGRAD, D3Q27 weights).
-// ---------------------------------------------------------------------------
-template <typename C>
-__device__ __forceinline__ void cg_collide_cell(const CGConst<C>& K, C fR[Q], C fB[Q], C rhoR, C rhoB, C psix,
-                                                C psiy, C psiz) {
-  const C ONE = 1, HALF = C(0.5);
-  const LatticeT<C>& L = K.L;
-  C rhosum = rhoR + rhoB;
-  C phase_field = (rhoR - rhoB) / (rhoR + rhoB);
-  C viscavg = ONE / (HALF * (ONE + phase_field) * K.inv_viscR + HALF * (ONE - phase_field) * K.inv_viscB);
-  C omega = ONE / (viscavg / L.cssq + HALF);
-  C omm = ONE - omega;
-  C invrho = ONE / rhosum;
-  C u = invrho * mx(fR) + invrho * mx(fB);
-  C v = invrho * my(fR) + invrho * my(fB);
-  C w = invrho * mz(fR) + invrho * mz(fB);
-  C usq = L.half_inv_cssq * (u * u + v * v + w * w);
-#pragma unroll
-  for (int l = 0; l < Q; ++l) {
-    C e = edot(l, u, v, w);
-    fR[l] = fR[l] * omm + equil_u(L, rhoR, e, usq, l) * omega;
-    fB[l] = fB[l] * omm + equil_u(L, rhoB, e, usq, l) * omega;
-  }
-  C psinorm_sq = psix * psix + psiy * psiy + psiz * psiz;
-  if (psinorm_sq > C(1.e-20)) {
-    C psinorm = sqrt(psinorm_sq);
-    C inv_psq = ONE / psinorm_sq;
-    C acoeff = C(9) / C(4) * omega * K.sigma;
-    C kR = rhoR * invrho, kB = rhoB * invrho;
-    C coef = K.beta * rhoR * rhoB * (invrho * invrho);
-    C inv_t1 = ONE / psinorm;                 // rec_fact = 1
-    C inv_t2 = ONE / (L.rec[2] * psinorm);    // rec_fact = sqrt(2)
-#pragma unroll
-    for (int l = 0; l < Q; ++l) {
-      C edp = edot(l, psix, psiy, psiz);
-      C temp = psinorm * (L.w[wclass(l)] * (edp * edp) * inv_psq - L.b[wclass(l)]);
-      C fd = fR[l] + fB[l] + acoeff * temp;
-      C feq = rhoR * L.w[wclass(l)] + rhoB * L.w[wclass(l)];
-      C cosphi;
-      if (l == 0) cosphi = C(0);
-      else {
-        C t1 = L.rec[wclass(l)] * psinorm;
-        cosphi = (t1 <= C(1.e-20)) ? C(0) : edp * (wclass(l) == 1 ? inv_t1 : inv_t2);
-      }
-      C t = coef * cosphi;
-      fR[l] = fd * kR + t * feq;
-      fB[l] = fd * kB - t * feq;
-    }
-  }
-}
-
-// colour gradient psi = sum_l a27_l e_l phi(x + e_l), l = 1..26 in reference order
-template <typename C, typename F>
-__device__ __forceinline__ void grad27(const LatticeT<C>& L, F&& phi_at, C& psix, C& psiy, C& psiz) {
-  psix = C(0); psiy = C(0); psiz = C(0);
-#pragma unroll
-  for (int l = 1; l < Q27; ++l) {
-    C ps = phi_at(ex27(l), ey27(l), ez27(l));
-    C a = L.a27[wclass27(l)];
-    if (ex27(l)) psix = psix + (ex27(l) > 0 ? a : -a) * ps;
-    if (ey27(l)) psiy = psiy + (ey27(l) > 0 ? a : -a) * ps;
-    if (ez27(l)) psiz = psiz + (ez27(l) > 0 ? a : -a) * ps;
-  }
-}
-
-// ---------------------------------------------------------------------------
 // kernels
 // ---------------------------------------------------------------------------
-struct LaunchDims {
-  dim3 grid, block;
-};
-
-static LaunchDims cell_dims(const Ctx& c) {
-  int bx = (c.nx % 128 == 0) ? 128 : ((c.nx % 64 == 0) ? 64 : 32);
-  int by = 256 / bx;
-  LaunchDims d;
-  d.block = dim3(bx, by, 1);
-  d.grid = dim3((c.nx + bx - 1) / bx, (c.ny + by - 1) / by, c.nz);
-  return d;
-}
-
 // setupPops (kernels_fluid_CG.CUF:313-346) written in pull convention: the
 // stored buffer holds, at x, the populations that streaming moves to x + e_l,
 // so that the first step gathers exactly the equilibrium of the given fields.
@@ -438,8 +271,9 @@ __global__ void __launch_bounds__(256) k_bgk(const S* __restrict__ A, S* __restr
 
 // moments2Fl on the post-streaming populations (pulled from the state)
 template <typename S, typename O>
-__global__ void k_fields(const S* __restrict__ A, Geom g, int ncomp, Shift<typename Store<S>::C> sh,
-                         const int8_t* __restrict__ flags, O* rR, O* rB, O* vel, O* phase) {
+__global__ void k_fields(const S* __restrict__ A, const S* Bold, Geom g, int ncomp, Shift<typename Store<S>::C> sh,
+                         const int8_t* __restrict__ flags, const int8_t* __restrict__ fold, O* rR, O* rB, O* vel,
+                         O* phase) {
   using C = typename Store<S>::C;
   int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y, z = blockIdx.z;
   if (x >= g.nx || y >= g.ny) return;
@@ -447,8 +281,8 @@ __global__ void k_fields(const S* __restrict__ A, Geom g, int ncomp, Shift<typen
   make_nbr(g, x, y, z, b);
   int cell = at(b, 0, 0, 0);
   C fR[Q], fB[Q];
-  pull(A, g, b, 0, sh, fR);
-  if (ncomp == 2) pull(A, g, b, 1, sh, fB);
+  pull_any(A, Bold, g, b, 0, sh, fold, fR);
+  if (ncomp == 2) pull_any(A, Bold, g, b, 1, sh, fold, fB);
   else {
 #pragma unroll
     for (int l = 0; l < Q; ++l) fB[l] = C(0);
@@ -469,8 +303,8 @@ __global__ void k_fields(const S* __restrict__ A, Geom g, int ncomp, Shift<typen
 }
 
 template <typename S>
-__global__ void k_get_pops(const S* __restrict__ A, Geom g, int ncomp, Shift<typename Store<S>::C> sh,
-                           float* pR, float* pB) {
+__global__ void k_get_pops(const S* __restrict__ A, const S* Bold, Geom g, int ncomp, Shift<typename Store<S>::C> sh,
+                           const int8_t* __restrict__ fold, float* pR, float* pB) {
   using C = typename Store<S>::C;
   int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y, z = blockIdx.z;
   if (x >= g.nx || y >= g.ny) return;
@@ -481,7 +315,7 @@ __global__ void k_get_pops(const S* __restrict__ A, Geom g, int ncomp, Shift<typ
   for (int comp = 0; comp < ncomp; ++comp) {
     float* out = comp ? pB : pR;
     if (!out) continue;
-    pull(A, g, b, comp, sh, f);
+    pull_any(A, Bold, g, b, comp, sh, fold, f);
 #pragma unroll
     for (int l = 0; l < Q; ++l) out[size_t(l) * size_t(g.n) + cell] = float(f[l]);
   }
@@ -490,8 +324,8 @@ __global__ void k_get_pops(const S* __restrict__ A, Geom g, int ncomp, Shift<typ
 // FP64 mass (per component) and momentum of the post-streaming populations,
 // block partial sums combined with FP64 atomics.
 template <typename S>
-__global__ void k_sums(const S* __restrict__ A, Geom g, int ncomp, Shift<typename Store<S>::C> sh,
-                       const int8_t* __restrict__ flags, double* out) {
+__global__ void k_sums(const S* __restrict__ A, const S* Bold, Geom g, int ncomp, Shift<typename Store<S>::C> sh,
+                       const int8_t* __restrict__ flags, const int8_t* __restrict__ fold, double* out) {
   using C = typename Store<S>::C;
   int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y, z = blockIdx.z;
   double acc[5] = {0, 0, 0, 0, 0};
@@ -502,7 +336,7 @@ __global__ void k_sums(const S* __restrict__ A, Geom g, int ncomp, Shift<typenam
     if (!flags || flags[cell] == LBX_FLUID_FLUID) {
       C f[Q];
       for (int comp = 0; comp < ncomp; ++comp) {
-        pull(A, g, b, comp, sh, f);
+        pull_any(A, Bold, g, b, comp, sh, fold, f);
         double m = 0;
 #pragma unroll
         for (int l = 0; l < Q; ++l) m += double(f[l]);
@@ -523,49 +357,6 @@ __global__ void k_sums(const S* __restrict__ A, Geom g, int ncomp, Shift<typenam
 // ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
-template <typename C>
-static Shift<C> make_shift(const Ctx& c) {
-  Shift<C> s;
-  LatticeT<C> L = make_lattice<C>();
-  bool shifted = (c.storage == LBX_STORE_F16 || c.storage == LBX_STORE_BF16);
-  float r0[2] = {c.p.rho0R, c.p.rho0B};
-  for (int comp = 0; comp < 2; ++comp)
-    for (int k = 0; k < 3; ++k) s.s[comp][k] = shifted ? C(L.w[k] * C(r0[comp])) : C(0);
-  return s;
-}
-
-template <typename C>
-static CGConst<C> make_cg(const Ctx& c) {
-  CGConst<C> K;
-  K.L = make_lattice<C>();
-  const C HALF = C(0.5);
-  C viscR = K.L.cssq * (C(c.p.tauR) - HALF);  // SetConstants, main.CUF:1069-1070
-  C viscB = K.L.cssq * (C(c.p.tauB) - HALF);
-  K.inv_viscR = C(1) / viscR;
-  K.inv_viscB = C(1) / viscB;
-  K.sigma = C(c.p.sigma);
-  K.beta = C(c.p.beta);
-  return K;
-}
-
-static Geom geom(const Ctx& c) { return Geom{c.nx, c.ny, c.nz, c.n}; }
-
-template <typename F>
-static int by_storage(const Ctx& c, F&& fn) {
-  switch (c.storage) {
-    case LBX_STORE_F32: return fn((float*)nullptr);
-    case LBX_STORE_F16: return fn((__half*)nullptr);
-    case LBX_STORE_BF16: return fn((__nv_bfloat16*)nullptr);
-    case LBX_STORE_F64: return fn((double*)nullptr);
-  }
-  return LBX_ERR_ARG;
-}
-
-static int launch_status() {
-  cudaError_t e = cudaGetLastError();
-  return e == cudaSuccess ? 0 : LBX_ERR_CUDA;
-}
-
 int fluid_alloc(Ctx& c) {
   size_t bytes = size_t(c.ncomp) * Q * size_t(c.n) * c.elem;
   for (int i = 0; i < 2; ++i)
@@ -594,10 +385,16 @@ void fluid_free(Ctx& c) {
   c.phi = nullptr;
 }
 
+static void reset_flags(Ctx& c) {
+  for (int i = 0; i < 2; ++i) cudaMemsetAsync(c.flags[i], LBX_FLUID_FLUID, size_t(c.n), c.stream);
+  c.fcur = 0;
+}
+
 int fluid_set_fields(Ctx& c, const float* d_rR, const float* d_rB, float vx, float vy, float vz) {
   LaunchDims d = cell_dims(c);
   Geom g = geom(c);
   c.cur = 0;
+  reset_flags(c);
   return by_storage(c, [&](auto* tag) {
     using S = std::remove_pointer_t<decltype(tag)>;
     using C = typename Store<S>::C;
@@ -611,6 +408,7 @@ int fluid_set_pops(Ctx& c, const float* d_pR, const float* d_pB) {
   LaunchDims d = cell_dims(c);
   Geom g = geom(c);
   c.cur = 0;
+  reset_flags(c);
   return by_storage(c, [&](auto* tag) {
     using S = std::remove_pointer_t<decltype(tag)>;
     using C = typename Store<S>::C;
@@ -728,19 +526,28 @@ int fluid_step(Ctx& c) {
   return rc;
 }
 
+// flags of the particle path for readback: the mask of the last step and the
+// dead-source flags of the pull (nullptr without particles)
+int particles_flags_slot(const Ctx& c);
+int particles_active(const Ctx& c);
+static const int8_t* mask_flags(const Ctx& c) { return particles_active(c) ? c.flags[particles_flags_slot(c)] : nullptr; }
+static const int8_t* dead_flags(const Ctx& c) { return particles_active(c) ? c.flags[c.fcur] : nullptr; }
+
 int fluid_get_fields(Ctx& c, void* rR, void* rB, void* vel, void* phase, int f64) {
   LaunchDims d = cell_dims(c);
   Geom g = geom(c);
   return by_storage(c, [&](auto* tag) {
     using S = std::remove_pointer_t<decltype(tag)>;
     using C = typename Store<S>::C;
+    const S* A = (const S*)c.pops[c.cur];
+    const S* Bo = (const S*)c.pops[1 - c.cur];
     if (f64)
-      k_fields<S, double><<<d.grid, d.block, 0, c.stream>>>((const S*)c.pops[c.cur], g, c.ncomp, make_shift<C>(c),
-                                                            nullptr, (double*)rR, (double*)rB, (double*)vel,
+      k_fields<S, double><<<d.grid, d.block, 0, c.stream>>>(A, Bo, g, c.ncomp, make_shift<C>(c), mask_flags(c),
+                                                            dead_flags(c), (double*)rR, (double*)rB, (double*)vel,
                                                             (double*)phase);
     else
-      k_fields<S, float><<<d.grid, d.block, 0, c.stream>>>((const S*)c.pops[c.cur], g, c.ncomp, make_shift<C>(c),
-                                                           nullptr, (float*)rR, (float*)rB, (float*)vel,
+      k_fields<S, float><<<d.grid, d.block, 0, c.stream>>>(A, Bo, g, c.ncomp, make_shift<C>(c), mask_flags(c),
+                                                           dead_flags(c), (float*)rR, (float*)rB, (float*)vel,
                                                            (float*)phase);
     return launch_status();
   });
@@ -752,7 +559,8 @@ int fluid_get_pops(Ctx& c, float* pR, float* pB) {
   return by_storage(c, [&](auto* tag) {
     using S = std::remove_pointer_t<decltype(tag)>;
     using C = typename Store<S>::C;
-    k_get_pops<S><<<d.grid, d.block, 0, c.stream>>>((const S*)c.pops[c.cur], g, c.ncomp, make_shift<C>(c), pR, pB);
+    k_get_pops<S><<<d.grid, d.block, 0, c.stream>>>((const S*)c.pops[c.cur], (const S*)c.pops[1 - c.cur], g,
+                                                    c.ncomp, make_shift<C>(c), dead_flags(c), pR, pB);
     return launch_status();
   });
 }
@@ -764,7 +572,8 @@ int fluid_get_sums(Ctx& c, double* d_out5) {
   return by_storage(c, [&](auto* tag) {
     using S = std::remove_pointer_t<decltype(tag)>;
     using C = typename Store<S>::C;
-    k_sums<S><<<d.grid, d.block, 0, c.stream>>>((const S*)c.pops[c.cur], g, c.ncomp, make_shift<C>(c), nullptr, d_out5);
+    k_sums<S><<<d.grid, d.block, 0, c.stream>>>((const S*)c.pops[c.cur], (const S*)c.pops[1 - c.cur], g, c.ncomp,
+                                                make_shift<C>(c), mask_flags(c), dead_flags(c), d_out5);
     return launch_status();
   });
 }

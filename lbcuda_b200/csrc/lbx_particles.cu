@@ -1,11 +1,1067 @@
-// lbx_particles.cu — rigid-sphere part of the hot path (placeholder until the
-// particle kernels land): a context with max_particles > 0 is refused.
-#include "lbx_ctx.h"
+// lbx_particles.cu — rigid spheres of the LBcuda hot path on sm_100a.
+//
+// Reference behaviour restated (kernels_fluid_PART.CUF unless noted):
+//   spherical_template (main.CUF:1990-2130)        -> host, uploaded once
+//   makeListAtomsGPU (2331-2451)                    -> k_bins (+ the tile-list
+//                                                      coverage predicate)
+//   init_isfluid_CG + setmyfluid (85-117,230-264)   -> k_flags
+//   del_fluid_CG / del_fluid (120-149,383-561)      -> k_drain
+//   init_rhoR_CG / init_rhoB_CG (CG.CUF:398-509)    -> k_rho_p
+//   make_fluid_CG / make_fluid + belts (152-180,563-913) -> k_fill
+//   compute_virtual_rho / compute_densities_wall (267-352) -> k_virtual
+//   time_step_CG (CG.CUF:531-848)                   -> k_collide_p
+//   partBB_CG, partBB_CG_p2n, partBB_CG_p2n2 (916-1040,1874-2312) -> k_bb
+//   inter_force_particles / addHertzian (1052-1068,1385-1503) -> k_pairs
+//   time_step_force_particles, addForce_particle_bounce_back, nve_lf,
+//   rot_midstep_impl_lf (1098-1166,1266-1827)       -> k_integrate
+//
+// B200 design: particle state, orientation and every force/torque sum are
+// FP64.  Each per-particle kernel is one CTA per sphere that walks the
+// sphere's (2 rmax + 1)^3 box of cells, so the momentum exchanged at the
+// surface links is reduced inside the CTA in a fixed order and written once
+// per step (no global atomics, bit-reproducible), instead of one FP64 atomic
+// per link.  Per-cell work that must happen once per cell (the bounce-back
+// copy and moving-wall correction) is done by the sphere that owns the cell.
+// The fluid kernels of a particle step read the flags of the previous step
+// for the pull (a spheredead source keeps the stale population, as the push
+// of stream*_CG leaves it) and of the current step for the collision.
+#include "lbx_device.cuh"
+
+#include <cmath>
+#include <vector>
 
 namespace lbx {
-struct ParticleState {};
-int particles_create(Ctx&) { return LBX_ERR_STATE; }
-void particles_destroy(Ctx& c) { delete c.part; c.part = nullptr; }
-int particles_step_pre(Ctx&) { return 0; }
-int particles_step_post(Ctx&) { return 0; }
+
+constexpr int PS = 13;   // pos record: x[3] v[3] omega_body[3] q[4]
+constexpr int FS = 12;   // force record: F[3] F_bb[3] T[3] T_bb[3]
+constexpr int AS = 15;   // accumulators: f_bb[3] t_bb[3] f_other[3] t_other[3] f_lub[3]
+constexpr int TILEX = 8, TILEY = 4, TILEZ = 4;  // reference tile (defines.h:14-22)
+constexpr int BINW = 8;                          // cell bins of the particle lists
+constexpr int BIN_CAP = 64;
+
+struct ParticleState {
+  int np = 0;
+  int rmax = 0, sphereMax = 0, tw = 0;
+  double rdim = 0;
+  int lrotate = 0;
+  double* pos[2] = {nullptr, nullptr};
+  double* frc[2] = {nullptr, nullptr};
+  double* acc = nullptr;
+  int8_t* tmpl = nullptr;
+  int* owner = nullptr;
+  int* bin_cnt = nullptr;
+  int* bin_list = nullptr;
+  int nbx = 0, nby = 0, nbz = 0;
+  int pcur = 0;
+  int flags_last = 0;
+  int active = 0;
+};
+
+struct PDev {  // by-value kernel argument
+  int np, rmax, sphereMax, tw, lrotate;
+  double rdim, rmass, max_vel;
+  const int8_t* tmpl;
+  int* owner;
+  int* bin_cnt;
+  int* bin_list;
+  int nbx, nby, nbz;
+  double ext_f[3], ext_t[3];
+  double hz_k, hz_rmin, hz_rcap;
+  int lub;
+  double lub_k, lub_rmin, lub_rcap;
+};
+
+// ---------------------------------------------------------------------------
+// small device helpers
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int nint_d(double x) { return int(round(x)); }  // Fortran NINT
+
+// getDeltai/j/k (kernels_fluid_PART.CUF:182-228)
+__device__ __forceinline__ int get_delta(int i, int c, int n, double rdim) {
+  int d = i - c;
+  if (double(c) - rdim < 1.0 || double(c) + rdim > double(n)) {
+    if (double(c) + rdim > double(n) && double(i) < rdim) d = i - c + n;
+    else if (double(c) - rdim < 1.0 && double(i) > double(n) - rdim) d = i - c - n;
+  }
+  return d;
+}
+
+// 1-based lattice coordinate (reference convention) of c0 + d, periodic
+__device__ __forceinline__ int wrap1(int v, int n) {
+  v = (v - 1) % n;
+  if (v < 0) v += n;
+  return v + 1;
+}
+
+__device__ __forceinline__ int cell0(const Geom& g, int i1, int j1, int k1) {  // 1-based -> linear
+  return (i1 - 1) + g.nx * ((j1 - 1) + g.ny * (k1 - 1));
+}
+
+// Tile-list coverage of makeListAtomsGPU: whether the reference's 8x4x4 tile
+// (ti,tj,tk, 1-based) holds particle position x (the list of the current step).
+__device__ bool tile_covered(const double x[3], const int n[3], double rdim, int ti, int tj, int tk) {
+  const int td[3] = {TILEX, TILEY, TILEZ};
+  const int t[3] = {ti, tj, tk};
+  for (int d = 0; d < 3; ++d) {
+    int ci = int(ceil(x[d]));
+    int b0 = int(x[d] - rdim), b1 = int(x[d] + rdim), b2, b3;  // real -> integer truncation
+    if (b0 < 1) {
+      b0 = 1; b1 = int(double(ci) + rdim); b2 = int(double(ci) - rdim + double(n[d])); b3 = n[d];
+    } else if (b1 > n[d]) {
+      b0 = 1; b1 = int(double(ci) + rdim - double(n[d])); b2 = int(double(ci) - rdim); b3 = n[d];
+    } else {
+      b2 = td[d]; b3 = -td[d];
+    }
+    bool hit = false;
+    int lo0 = (b0 - 1) / td[d] + 1, hi0 = (b1 - 1) / td[d] + 1;
+    int lo1 = (b2 - 1) / td[d] + 1, hi1 = (b3 - 1) / td[d] + 1;
+    if (t[d] >= lo0 && t[d] <= hi0) hit = true;
+    if (t[d] >= lo1 && t[d] <= hi1) hit = true;
+    if (!hit) return false;
+  }
+  return true;
+}
+
+// q (0,v) q*  (qtrimult, kernels_fluid_PART.CUF:1830-1871)
+__device__ __forceinline__ void qmult(const double a[4], const double b[4], double o[4]) {
+  o[0] = a[0] * b[0] - a[1] * b[1] - a[2] * b[2] - a[3] * b[3];
+  double c0 = a[2] * b[3] - a[3] * b[2], c1 = a[3] * b[1] - a[1] * b[3], c2 = a[1] * b[2] - a[2] * b[1];
+  o[1] = a[0] * b[1] + b[0] * a[1] + c0;
+  o[2] = a[0] * b[2] + b[0] * a[2] + c1;
+  o[3] = a[0] * b[3] + b[0] * a[3] + c2;
+}
+__device__ __forceinline__ void to_lab(const double* P, const double v[3], double out[3]) {
+  double q[4] = {P[9], P[10], P[11], P[12]};
+  double qc[4] = {q[0], -q[1], -q[2], -q[3]};
+  double qv[4] = {0.0, v[0], v[1], v[2]};
+  double t[4], o[4];
+  qmult(qv, qc, t);
+  qmult(q, t, o);
+  out[0] = o[1]; out[1] = o[2]; out[2] = o[3];
+}
+
+// min-image lever from the particle centre to cell (i,j,k), scaled to rdim
+__device__ __forceinline__ void lever(const Geom& g, const double* P, int i, int j, int k, bool image, double rdim,
+                                      double r[3]) {
+  r[0] = double(i) - P[0];
+  r[1] = double(j) - P[1];
+  r[2] = double(k) - P[2];
+  if (image) {
+    r[0] = r[0] - double(g.nx) * double(nint_d((1.0 / g.nx) * r[0]));
+    r[1] = r[1] - double(g.ny) * double(nint_d((1.0 / g.ny) * r[1]));
+    r[2] = r[2] - double(g.nz) * double(nint_d((1.0 / g.nz) * r[2]));
+  }
+  double m = sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+  for (int d = 0; d < 3; ++d) r[d] = rdim / m * r[d];
+}
+
+__device__ __forceinline__ void cross(const double a[3], const double b[3], double o[3]) {
+  o[0] = a[1] * b[2] - a[2] * b[1];
+  o[1] = a[2] * b[0] - a[0] * b[2];
+  o[2] = a[0] * b[1] - a[1] * b[0];
+}
+
+// fixed-order CTA reduction of NV doubles (blockDim.x == 256)
+template <int NV>
+__device__ void block_sum(double v[NV], double* out /* NV, added */) {
+  __shared__ double red[8][NV];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int i = 0; i < NV; ++i)
+    for (int o = 16; o > 0; o >>= 1) v[i] += __shfl_down_sync(0xffffffffu, v[i], o);
+  if (lane == 0)
+    for (int i = 0; i < NV; ++i) red[warp][i] = v[i];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < NV; ++i) {
+      double s = 0;
+      for (int w = 0; w < 8; ++w) s += red[w][i];
+      out[i] += s;
+    }
+  }
+  __syncthreads();
+}
+
+// ---------------------------------------------------------------------------
+// kernels
+// ---------------------------------------------------------------------------
+__global__ void k_bins(PDev P, const double* __restrict__ pos, Geom g, unsigned long long* err, int64_t step) {
+  int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= P.np) return;
+  const double* p = pos + size_t(a) * PS;
+  const int c[3] = {nint_d(p[0]), nint_d(p[1]), nint_d(p[2])};
+  const int n[3] = {g.nx, g.ny, g.nz};
+  const int nb[3] = {P.nbx, P.nby, P.nbz};
+  // distinct bins hit by the cells c - rmax .. c + rmax of each axis (periodic)
+  int bl[3][4], nbl[3] = {0, 0, 0};
+  for (int d = 0; d < 3; ++d)
+    for (int u = c[d] - P.rmax; u <= c[d] + P.rmax; ++u) {
+      int bin = (wrap1(u, n[d]) - 1) / BINW;
+      bool seen = false;
+      for (int k = 0; k < nbl[d]; ++k) seen |= (bl[d][k] == bin);
+      if (!seen && nbl[d] < 4) bl[d][nbl[d]++] = bin;
+      (void)nb;
+    }
+  for (int bk = 0; bk < nbl[2]; ++bk)
+    for (int bj = 0; bj < nbl[1]; ++bj)
+      for (int bi = 0; bi < nbl[0]; ++bi) {
+        int bin = bl[0][bi] + nb[0] * (bl[1][bj] + nb[1] * bl[2][bk]);
+        int slot = atomicAdd(P.bin_cnt + bin, 1);
+        if (slot < BIN_CAP) P.bin_list[size_t(bin) * BIN_CAP + slot] = a;
+        else raise_error(err, LBX_DEV_LIST_OVERFLOW, step, a);
+      }
+}
+
+// ascending particle order inside each bin (the first-match rules below then
+// pick the lowest index deterministically)
+__global__ void k_bins_sort(PDev P, int nbins) {
+  int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nbins) return;
+  int n = min(P.bin_cnt[b], BIN_CAP);
+  int* L = P.bin_list + size_t(b) * BIN_CAP;
+  for (int i = 1; i < n; ++i) {
+    int v = L[i], j = i - 1;
+    while (j >= 0 && L[j] > v) { L[j + 1] = L[j]; --j; }
+    L[j + 1] = v;
+  }
+}
+
+__device__ __forceinline__ int bin_of(const PDev& P, int x0, int y0, int z0) {  // 0-based cell coords
+  return (x0 / BINW) + P.nbx * ((y0 / BINW) + P.nby * (z0 / BINW));
+}
+
+// init_isfluid_CG: flags of the current step and the owning sphere
+__global__ void k_flags(PDev P, const double* __restrict__ pos, Geom g, int8_t* __restrict__ flags_new) {
+  int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y, z = blockIdx.z;
+  if (x >= g.nx || y >= g.ny) return;
+  int cell = x + g.nx * (y + g.ny * z);
+  int bin = bin_of(P, x, y, z);
+  int n = min(P.bin_cnt[bin], BIN_CAP);
+  const int* L = P.bin_list + size_t(bin) * BIN_CAP;
+  int8_t fl = LBX_FLUID_FLUID;
+  int own = 0;
+  for (int t = 0; t < n; ++t) {
+    int a = L[t];
+    const double* p = pos + size_t(a) * PS;
+    int di = get_delta(x + 1, nint_d(p[0]), g.nx, P.rdim);
+    int dj = get_delta(y + 1, nint_d(p[1]), g.ny, P.rdim);
+    int dk = get_delta(z + 1, nint_d(p[2]), g.nz, P.rdim);
+    if (abs(di) <= P.rmax && abs(dj) <= P.rmax && abs(dk) <= P.rmax) {
+      int8_t v = P.tmpl[(di + P.rmax) + P.tw * ((dj + P.rmax) + P.tw * (dk + P.rmax))];
+      if (v != LBX_FLUID_FLUID) {
+        fl = v;
+        own = a + 1;
+        break;
+      }
+    }
+  }
+  flags_new[cell] = fl;
+  P.owner[cell] = own;
+}
+
+// walk the (2 rmax + 1)^3 box around centre c; fn(i1, j1, k1, di, dj, dk) gets
+// 1-based coordinates and the reference's getDelta offset, once per cell
+template <typename F>
+__device__ __forceinline__ void for_box(const PDev& P, const Geom& g, const int c[3], F&& fn) {
+  const int w = 2 * P.rmax + 1, tot = w * w * w;
+  for (int t = threadIdx.x; t < tot; t += blockDim.x) {
+    int dx = t % w - P.rmax, dy = (t / w) % w - P.rmax, dz = t / (w * w) - P.rmax;
+    int i1 = wrap1(c[0] + dx, g.nx), j1 = wrap1(c[1] + dy, g.ny), k1 = wrap1(c[2] + dz, g.nz);
+    int di = get_delta(i1, c[0], g.nx, P.rdim), dj = get_delta(j1, c[1], g.ny, P.rdim),
+        dk = get_delta(k1, c[2], g.nz, P.rdim);
+    if (di != dx || dj != dy || dk != dz) continue;  // visited under its reference offset
+    fn(i1, j1, k1, di, dj, dk);
+  }
+}
+
+__device__ __forceinline__ bool moved(const double* p0, const double* p1) {
+  return nint_d(p0[0]) != nint_d(p1[0]) || nint_d(p0[1]) != nint_d(p1[1]) || nint_d(p0[2]) != nint_d(p1[2]);
+}
+
+// del_fluid: cells fluid in the previous step and solid now hand their
+// momentum (rho u of the streamed populations) to the sphere.
+template <typename S>
+__global__ void __launch_bounds__(256) k_drain(PDev P, const double* __restrict__ pos_cur,
+                                               const double* __restrict__ pos_old, double* acc, const S* A,
+                                               const S* Bold, Geom g, Shift<typename Store<S>::C> sh,
+                                               const int8_t* __restrict__ fold, const int8_t* __restrict__ fnew,
+                                               const typename Store<S>::C* __restrict__ rhoR,
+                                               const typename Store<S>::C* __restrict__ rhoB) {
+  using C = typename Store<S>::C;
+  const int a = blockIdx.x;
+  const double* pc = pos_cur + size_t(a) * PS;
+  const double* po = pos_old + size_t(a) * PS;
+  if (!moved(pc, po)) return;
+  const int c[3] = {nint_d(po[0]), nint_d(po[1]), nint_d(po[2])};
+  const int n[3] = {g.nx, g.ny, g.nz};
+  double s[6] = {0, 0, 0, 0, 0, 0};
+  for_box(P, g, c, [&](int i1, int j1, int k1, int di, int dj, int dk) {
+    if (di * di + dj * dj + dk * dk > P.sphereMax) return;
+    if (!tile_covered(pc, n, P.rdim, (i1 - 1) / TILEX + 1, (j1 - 1) / TILEY + 1, (k1 - 1) / TILEZ + 1)) return;
+    int cell = cell0(g, i1, j1, k1);
+    int8_t fo = fold[cell], fn = fnew[cell];
+    if (fo != LBX_FLUID_FLUID || (fn != LBX_FLUID_SPHERELIST && fn != LBX_FLUID_SPHEREDEAD)) return;
+    Nbr b;
+    make_nbr(g, i1 - 1, j1 - 1, k1 - 1, b);
+    C qR[Q], qB[Q];
+    pull_dead(A, Bold, g, b, 0, sh, fold, qR);
+    pull_dead(A, Bold, g, b, 1, sh, fold, qB);
+    C rR = rhoR[cell], rB = rhoB[cell];
+    C invrho = C(1) / (rR + rB);
+    C u = invrho * mx(qR) + invrho * mx(qB);
+    C v = invrho * my(qR) + invrho * my(qB);
+    C w = invrho * mz(qR) + invrho * mz(qB);
+    double ft[3] = {double((rR + rB) * u), double((rR + rB) * v), double((rR + rB) * w)};
+    s[0] += ft[0]; s[1] += ft[1]; s[2] += ft[2];
+    if (P.lrotate) {
+      double r[3], t[3];
+      lever(g, pc, i1, j1, k1, fn == LBX_FLUID_SPHERELIST, P.rdim, r);
+      cross(r, ft, t);
+      s[3] += t[0]; s[4] += t[1]; s[5] += t[2];
+    }
+  });
+  double out[6] = {0, 0, 0, 0, 0, 0};
+  block_sum<6>(s, out);
+  if (threadIdx.x == 0)
+    for (int d = 0; d < 3; ++d) {
+      acc[size_t(a) * AS + 6 + d] += out[d];
+      acc[size_t(a) * AS + 9 + d] += out[3 + d];
+    }
+}
+
+// init_rho*_CG with flags: densities and phase field of every cell
+template <typename S>
+__global__ void __launch_bounds__(256) k_rho_p(const S* __restrict__ A, const S* Bold, Geom g,
+                                               Shift<typename Store<S>::C> sh, const int8_t* __restrict__ fold,
+                                               const int8_t* __restrict__ fnew, typename Store<S>::C* phi,
+                                               typename Store<S>::C* rhoR, typename Store<S>::C* rhoB,
+                                               unsigned long long* err, int64_t step) {
+  using C = typename Store<S>::C;
+  int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y, z = blockIdx.z;
+  if (x >= g.nx || y >= g.ny) return;
+  Nbr b;
+  make_nbr(g, x, y, z, b);
+  int cell = at(b, 0, 0, 0);
+  C rR = 0, rB = 0;
+  if (fnew[cell] == LBX_FLUID_FLUID) {
+    C f[Q];
+    pull_dead(A, Bold, g, b, 0, sh, fold, f);
+    rR = sum_q(f);
+    pull_dead(A, Bold, g, b, 1, sh, fold, f);
+    rB = sum_q(f);
+    if (rR < C(-10) || rR > C(10) || rB < C(-10) || rB > C(10)) raise_error(err, LBX_DEV_RHO_RANGE, step, cell);
+    if (rR < C(0)) rR = C(0);
+    if (rB < C(0)) rB = C(0);
+  }
+  rhoR[cell] = rR;
+  rhoB[cell] = rB;
+  phi[cell] = (rR - rB) / (rR + rB);
+}
+
+// make_fluid: cells solid in the previous step and fluid now get the mean
+// density of their fluid neighbours (D3Q27 belt, then the 98-cell second
+// belt) and the equilibrium at the sphere's velocity; the sphere pays the
+// momentum.
+template <typename S>
+__global__ void __launch_bounds__(256) k_fill(PDev P, const double* __restrict__ pos_cur,
+                                              const double* __restrict__ pos_old, double* acc, S* B, Geom g,
+                                              Shift<typename Store<S>::C> sh, LatticeT<typename Store<S>::C> L,
+                                              const int8_t* __restrict__ fold, const int8_t* __restrict__ fnew,
+                                              typename Store<S>::C* rhoR, typename Store<S>::C* rhoB,
+                                              typename Store<S>::C* phi) {
+  using C = typename Store<S>::C;
+  const int a = blockIdx.x;
+  const double* pc = pos_cur + size_t(a) * PS;
+  const double* po = pos_old + size_t(a) * PS;
+  if (!moved(pc, po)) return;
+  const int c[3] = {nint_d(po[0]), nint_d(po[1]), nint_d(po[2])};
+  const int n[3] = {g.nx, g.ny, g.nz};
+  double s[6] = {0, 0, 0, 0, 0, 0};
+  for_box(P, g, c, [&](int i1, int j1, int k1, int di, int dj, int dk) {
+    if (di * di + dj * dj + dk * dk > P.sphereMax) return;
+    if (!tile_covered(pc, n, P.rdim, (i1 - 1) / TILEX + 1, (j1 - 1) / TILEY + 1, (k1 - 1) / TILEZ + 1)) return;
+    int cell = cell0(g, i1, j1, k1);
+    int8_t fo = fold[cell], fn = fnew[cell];
+    if ((fo != LBX_FLUID_SPHERELIST && fo != LBX_FLUID_SPHEREDEAD) || fn != LBX_FLUID_FLUID) return;
+    C Rs = 0, Bs = 0;
+    int D = 0;
+    for (int l = 1; l < Q27; ++l) {  // compute_onebelt_density_twofluids
+      int y = cell0(g, wrap1(i1 + ex27(l), g.nx), wrap1(j1 + ey27(l), g.ny), wrap1(k1 + ez27(l), g.nz));
+      if (fnew[y] == LBX_FLUID_FLUID && fold[y] == LBX_FLUID_FLUID) { Rs = Rs + rhoR[y]; Bs = Bs + rhoB[y]; ++D; }
+    }
+    if (D) { Rs = Rs / C(D); Bs = Bs / C(D); }
+    else {  // compute_secbelt_density_twofluids
+      Rs = 0; Bs = 0;
+      for (int kk = -2; kk <= 2; ++kk)
+        for (int jj = -2; jj <= 2; ++jj)
+          for (int ii = -2; ii <= 2; ++ii) {
+            if (!(ii == -2 || ii == 2 || jj == -2 || jj == 2 || kk == -2 || kk == 2)) continue;
+            int y = cell0(g, wrap1(i1 + ii, g.nx), wrap1(j1 + jj, g.ny), wrap1(k1 + kk, g.nz));
+            if (fnew[y] == LBX_FLUID_FLUID && fold[y] == LBX_FLUID_FLUID) { Rs = Rs + rhoR[y]; Bs = Bs + rhoB[y]; ++D; }
+          }
+      if (D) { Rs = Rs / C(D); Bs = Bs / C(D); }
+      // else fix_onebelt_density_twofluids (empty in the reference): zero density
+    }
+    C u = C(pc[3]), v = C(pc[4]), w = C(pc[5]);
+    rhoR[cell] = Rs;
+    rhoB[cell] = Bs;
+    phi[cell] = (Rs - Bs) / (Rs + Bs);
+    C usq = L.half_inv_cssq * (u * u + v * v + w * w);
+    for (int comp = 0; comp < 2; ++comp) {
+      C r = comp ? Bs : Rs;
+      S* base = B + size_t(comp) * Q * size_t(g.n) + cell;
+#pragma unroll
+      for (int l = 0; l < Q; ++l)
+        Store<S>::st(base + size_t(l) * size_t(g.n), equil_u(L, r, edot(l, u, v, w), usq, l), sh.at(comp, l));
+    }
+    double ft[3] = {double(-(Rs + Bs) * u), double(-(Rs + Bs) * v), double(-(Rs + Bs) * w)};
+    s[0] += ft[0]; s[1] += ft[1]; s[2] += ft[2];
+    if (P.lrotate) {
+      double r[3], t[3];
+      lever(g, pc, i1, j1, k1, fo == LBX_FLUID_SPHERELIST, P.rdim, r);
+      cross(r, ft, t);
+      s[3] += t[0]; s[4] += t[1]; s[5] += t[2];
+    }
+  });
+  double out[6] = {0, 0, 0, 0, 0, 0};
+  block_sum<6>(s, out);
+  if (threadIdx.x == 0)
+    for (int d = 0; d < 3; ++d) {
+      acc[size_t(a) * AS + 6 + d] += out[d];
+      acc[size_t(a) * AS + 9 + d] += out[3 + d];
+    }
+}
+
+// virtual densities of the surface cells a sphere owns: Janus
+// (compute_virtual_rho) or neutral wetting (compute_densities_wall)
+template <typename C>
+__global__ void __launch_bounds__(256) k_virtual(PDev P, const double* __restrict__ pos, Geom g, int neutral,
+                                                 const int8_t* __restrict__ fold, const int8_t* __restrict__ fnew,
+                                                 C* rhoR, C* rhoB, C* phi, LatticeT<C> L) {
+  const int a = blockIdx.x;
+  const double* pc = pos + size_t(a) * PS;
+  const int c[3] = {nint_d(pc[0]), nint_d(pc[1]), nint_d(pc[2])};
+  double xl[3] = {0, 0, 0};
+  if (!neutral) {
+    double ax[3] = {1.0, 0.0, 0.0};
+    to_lab(pc, ax, xl);
+  }
+  for_box(P, g, c, [&](int i1, int j1, int k1, int, int, int) {
+    int cell = cell0(g, i1, j1, k1);
+    if (fnew[cell] != LBX_FLUID_SPHERELIST || P.owner[cell] != a + 1) return;
+    C R, Bv;
+    if (!neutral) {
+      double r[3] = {double(i1) - pc[0], double(j1) - pc[1], double(k1) - pc[2]};
+      r[0] = r[0] - double(g.nx) * double(nint_d((1.0 / g.nx) * r[0]));
+      r[1] = r[1] - double(g.ny) * double(nint_d((1.0 / g.ny) * r[1]));
+      r[2] = r[2] - double(g.nz) * double(nint_d((1.0 / g.nz) * r[2]));
+      double m = sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+      double cs = xl[0] * (r[0] / m) + xl[1] * (r[1] / m) + xl[2] * (r[2] / m);
+      if (cs < 0.0) { R = 0; Bv = 1; }
+      else { R = 1; Bv = 0; }
+    } else {
+      C Rs = 0, Bs = 0, Ds = 0;
+      for (int l = 1; l < Q27; ++l) {  // compute_onebelt_density_2fl_weights
+        int y = cell0(g, wrap1(i1 + ex27(l), g.nx), wrap1(j1 + ey27(l), g.ny), wrap1(k1 + ez27(l), g.nz));
+        if (fnew[y] == LBX_FLUID_FLUID) {
+          C w = L.p27[wclass27(l)];
+          Rs = Rs + w * rhoR[y]; Bs = Bs + w * rhoB[y]; Ds = Ds + w;
+        }
+      }
+      if (Ds != C(0)) { R = Rs / Ds; Bv = Bs / Ds; }
+      else {
+        int D = 0;
+        Rs = 0; Bs = 0;
+        for (int kk = -2; kk <= 2; ++kk)
+          for (int jj = -2; jj <= 2; ++jj)
+            for (int ii = -2; ii <= 2; ++ii) {
+              if (!(ii == -2 || ii == 2 || jj == -2 || jj == 2 || kk == -2 || kk == 2)) continue;
+              int y = cell0(g, wrap1(i1 + ii, g.nx), wrap1(j1 + jj, g.ny), wrap1(k1 + kk, g.nz));
+              if (fnew[y] == LBX_FLUID_FLUID && fold[y] == LBX_FLUID_FLUID) { Rs = Rs + rhoR[y]; Bs = Bs + rhoB[y]; ++D; }
+            }
+        if (!D) return;  // no fluid in either belt: the density stays zero
+        R = Rs / C(D);
+        Bv = Bs / C(D);
+      }
+    }
+    rhoR[cell] = R;
+    rhoB[cell] = Bv;
+    phi[cell] = (R - Bv) / (R + Bv);
+  });
+}
+
+// time_step_CG with flags (two-pass schedule): collision on fluid cells,
+// the streamed populations pass through unchanged elsewhere.
+template <typename S>
+__global__ void __launch_bounds__(256) k_collide_p(const S* __restrict__ A, S* B, Geom g,
+                                                   Shift<typename Store<S>::C> sh,
+                                                   const typename Store<S>::C* __restrict__ phi,
+                                                   const typename Store<S>::C* __restrict__ rhoR,
+                                                   const typename Store<S>::C* __restrict__ rhoB,
+                                                   const int8_t* __restrict__ fold, const int8_t* __restrict__ fnew,
+                                                   CGConst<typename Store<S>::C> K) {
+  using C = typename Store<S>::C;
+  int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y, z = blockIdx.z;
+  if (x >= g.nx || y >= g.ny) return;
+  Nbr b;
+  make_nbr(g, x, y, z, b);
+  int cell = at(b, 0, 0, 0);
+  C fR[Q], fB[Q];
+  int8_t fn = fnew[cell];
+  bool fresh = (fn == LBX_FLUID_FLUID) && (fold[cell] != LBX_FLUID_FLUID);
+  if (fresh) {  // make_fluid already wrote the new node's populations into B
+    const S* bR = B + cell;
+    const S* bB = B + size_t(Q) * size_t(g.n) + cell;
+#pragma unroll
+    for (int l = 0; l < Q; ++l) {
+      fR[l] = Store<S>::ld(bR + size_t(l) * size_t(g.n), sh.at(0, l));
+      fB[l] = Store<S>::ld(bB + size_t(l) * size_t(g.n), sh.at(1, l));
+    }
+  } else {
+    pull_dead(A, B, g, b, 0, sh, fold, fR);
+    pull_dead(A, B, g, b, 1, sh, fold, fB);
+  }
+  if (fn == LBX_FLUID_FLUID) {
+    C psix, psiy, psiz;
+    grad27(K.L, [&](int dx, int dy, int dz) { return phi[at(b, dx, dy, dz)]; }, psix, psiy, psiz);
+    cg_collide_cell(K, fR, fB, rhoR[cell], rhoB[cell], psix, psiy, psiz);
+  }
+  store_all(B, g, cell, 0, sh, fR);
+  store_all(B, g, cell, 1, sh, fB);
+}
+
+// one bounce-back link of sphere a at surface cell (i1,j1,k1):
+// returns the force / torque of node_to_particle_bounce_back_bc2 and, when
+// `wall` is given, the moving-wall terms of phase 2.
+struct LinkGeo {
+  double rv[3], ol[3];
+};
+
+__device__ __forceinline__ void link_geo(const PDev& P, const Geom& g, const double* pc, int i1, int j1, int k1,
+                                         LinkGeo& G) {
+  G.rv[0] = G.rv[1] = G.rv[2] = 0;
+  G.ol[0] = G.ol[1] = G.ol[2] = 0;
+  if (P.lrotate) {
+    double om[3] = {pc[6], pc[7], pc[8]};
+    to_lab(pc, om, G.ol);
+    lever(g, pc, i1, j1, k1, true, P.rdim, G.rv);
+  }
+}
+
+__device__ __forceinline__ void wall_velocity(const PDev& P, const double* pc, const LinkGeo& G, int lr,
+                                              double rt[3], double v[3]) {
+  v[0] = pc[3]; v[1] = pc[4]; v[2] = pc[5];
+  rt[0] = rt[1] = rt[2] = 0;
+  if (P.lrotate) {
+    rt[0] = G.rv[0] + 0.5 * ex(lr);
+    rt[1] = G.rv[1] + 0.5 * ey(lr);
+    rt[2] = G.rv[2] + 0.5 * ez(lr);
+    double c[3];
+    cross(G.ol, rt, c);
+    v[0] += c[0]; v[1] += c[1]; v[2] += c[2];
+  }
+}
+
+// partBB_CG + partBB_CG_p2n + partBB_CG_p2n2
+template <typename S>
+__global__ void __launch_bounds__(256) k_bb(PDev P, const double* __restrict__ pos, double* acc, S* B, Geom g,
+                                            Shift<typename Store<S>::C> sh, LatticeT<typename Store<S>::C> L,
+                                            const int8_t* __restrict__ fnew,
+                                            const typename Store<S>::C* __restrict__ rhoR,
+                                            const typename Store<S>::C* __restrict__ rhoB) {
+  using C = typename Store<S>::C;
+  const int a = blockIdx.x;
+  const double* pc = pos + size_t(a) * PS;
+  const int c[3] = {nint_d(pc[0]), nint_d(pc[1]), nint_d(pc[2])};
+  const C buz = C(2) / L.cssq;  // pref_bouzidi, dimensions_m.CUF:95
+  double s[6] = {0, 0, 0, 0, 0, 0};
+  for_box(P, g, c, [&](int i1, int j1, int k1, int di, int dj, int dk) {
+    int cell = cell0(g, i1, j1, k1);
+    if (fnew[cell] != LBX_FLUID_SPHERELIST) return;
+    const int x0 = i1 - 1, y0 = j1 - 1, z0 = k1 - 1;
+    Nbr b;
+    make_nbr(g, x0, y0, z0, b);
+    // node -> particle momentum exchange for this sphere (atmDist < sphereMax)
+    if (di * di + dj * dj + dk * dk < P.sphereMax) {
+      LinkGeo G;
+      link_geo(P, g, pc, i1, j1, k1, G);
+#pragma unroll
+      for (int it = 1; it <= 9; ++it) {
+        const int lo = 2 * it - 1, hi = 2 * it;
+        const int xi = at(b, ex(lo), ey(lo), ez(lo)), xo = at(b, ex(hi), ey(hi), ez(hi));
+        const bool fi = fnew[xi] == LBX_FLUID_FLUID, fo = fnew[xo] == LBX_FLUID_FLUID;
+#pragma unroll
+        for (int side = 0; side < 2; ++side) {
+          if (side == 0 ? !(fi && !fo) : !(!fi && fo)) continue;
+          const int xf = side ? xo : xi, lf = side ? lo : hi, lr = side ? hi : lo;
+          double rt[3], v[3];
+          wall_velocity(P, pc, G, lr, rt, v);
+          C ev = C(ex(lf)) * C(v[0]) + C(ey(lf)) * C(v[1]) + C(ez(lf)) * C(v[2]);
+          C w = L.w[wclass(lf)];
+          C f2pR = C(2) * Store<S>::ld(B + size_t(lf) * size_t(g.n) + xf, sh.at(0, lf)) - w * buz * rhoR[xf] * ev;
+          C f2pB = C(2) * Store<S>::ld(B + size_t(Q + lf) * size_t(g.n) + xf, sh.at(1, lf)) - w * buz * rhoB[xf] * ev;
+          C f2p = f2pR + f2pB;
+          double ft[3] = {double(f2p * C(ex(lf))), double(f2p * C(ey(lf))), double(f2p * C(ez(lf)))};
+          s[0] += ft[0]; s[1] += ft[1]; s[2] += ft[2];
+          if (P.lrotate) {
+            double t[3];
+            cross(rt, ft, t);
+            s[3] += t[0] * abs(ex(lf));
+            s[4] += t[1] * abs(ey(lf));
+            s[5] += t[2] * abs(ez(lf));
+          }
+        }
+      }
+    }
+    if (P.owner[cell] != a + 1) return;
+    // p2n phase 1: bounce-back copy into the surface cell
+#pragma unroll
+    for (int it = 1; it <= 9; ++it) {
+      const int lo = 2 * it - 1, hi = 2 * it;
+      const int xi = at(b, ex(lo), ey(lo), ez(lo)), xo = at(b, ex(hi), ey(hi), ez(hi));
+      const bool fi = fnew[xi] == LBX_FLUID_FLUID, fo = fnew[xo] == LBX_FLUID_FLUID;
+      for (int comp = 0; comp < 2; ++comp) {
+        S* base = B + size_t(comp) * Q * size_t(g.n);
+        if (fi && !fo) base[size_t(lo) * size_t(g.n) + cell] = base[size_t(hi) * size_t(g.n) + xi];
+        if (!fi && fo) base[size_t(hi) * size_t(g.n) + cell] = base[size_t(lo) * size_t(g.n) + xo];
+      }
+    }
+    // p2n phase 2: moving-wall correction, for every sphere within reach of
+    // the cell in ascending index (the particle loop of partBB_CG_p2n2)
+    int bin = bin_of(P, x0, y0, z0);
+    int nlist = min(P.bin_cnt[bin], BIN_CAP);
+    const int* Lst = P.bin_list + size_t(bin) * BIN_CAP;
+    for (int t = 0; t < nlist; ++t) {
+      const int q = Lst[t];
+      const double* pq = pos + size_t(q) * PS;
+      int ei = get_delta(i1, nint_d(pq[0]), g.nx, P.rdim), ej = get_delta(j1, nint_d(pq[1]), g.ny, P.rdim),
+          ek = get_delta(k1, nint_d(pq[2]), g.nz, P.rdim);
+      if (ei * ei + ej * ej + ek * ek >= P.sphereMax) continue;
+      LinkGeo G;
+      link_geo(P, g, pq, i1, j1, k1, G);
+      for (int it = 1; it <= 9; ++it) {
+        const int lo = 2 * it - 1, hi = 2 * it;
+        const int xi = at(b, ex(lo), ey(lo), ez(lo)), xo = at(b, ex(hi), ey(hi), ez(hi));
+        const bool fi = fnew[xi] == LBX_FLUID_FLUID, fo = fnew[xo] == LBX_FLUID_FLUID;
+        for (int side = 0; side < 2; ++side) {
+          if (side == 0 ? !(fi && !fo) : !(!fi && fo)) continue;
+          const int xf = side ? xo : xi, lf = side ? lo : hi, lr = side ? hi : lo;
+          double rt[3], v[3];
+          wall_velocity(P, pq, G, lr, rt, v);
+          C ev = C(ex(lf)) * C(v[0]) + C(ey(lf)) * C(v[1]) + C(ez(lf)) * C(v[2]);
+          C w = L.w[wclass(lf)];
+          for (int comp = 0; comp < 2; ++comp) {
+            S* p = B + size_t(comp * Q + lr) * size_t(g.n) + cell;
+            const C* rho = comp ? rhoB : rhoR;
+            C val = Store<S>::ld(p, sh.at(comp, lr)) - w * buz * rho[xf] * ev;
+            Store<S>::st(p, val, sh.at(comp, lr));
+          }
+        }
+      }
+    }
+  });
+  double out[6] = {0, 0, 0, 0, 0, 0};
+  block_sum<6>(s, out);
+  if (threadIdx.x == 0)
+    for (int d = 0; d < 6; ++d) acc[size_t(a) * AS + d] += out[d];
+}
+
+// inter_force_particles / addHertzian: all pairs, each sphere sums its own
+// share in a fixed order.  With lubrication on, the analytic squeeze force
+// is added as well (the reference writes it into a total that its
+// integrator then overwrites; here it reaches the integrator).
+__global__ void k_pairs(PDev P, const double* __restrict__ pos, double* acc, Geom g) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= P.np) return;
+  const double* pi = pos + size_t(i) * PS;
+  const double rsqcut = P.hz_rmin * P.hz_rmin;
+  const double gmin = 5.0 * 0.5 * P.hz_k * pow(P.hz_rmin - P.hz_rcap, 1.5);
+  const double rpar = 2.0 * P.rdim;
+  const double lubfactor = P.lub_k * 6.0 * 3.141592653589793238462643383279502884 * pow(P.rdim * P.rdim, 2.0) / (rpar * rpar);
+  const double rparcut = rpar + P.lub_rmin;
+  const double mxrsqcut = fmax(rparcut * rparcut, rsqcut);
+  const double rparcap = rpar + P.lub_rcap;
+  double f[3] = {0, 0, 0}, fl[3] = {0, 0, 0};
+  for (int j = 0; j < P.np; ++j) {
+    if (j == i) continue;
+    // pair (lo, hi) with d = x_hi - x_lo as in addHertzian(lo, hi)
+    const int lo = min(i, j), hi = max(i, j);
+    const double* pl = pos + size_t(lo) * PS;
+    const double* ph = pos + size_t(hi) * PS;
+    double xdf = ph[0] - pl[0], ydf = ph[1] - pl[1], zdf = ph[2] - pl[2];
+    xdf = xdf - double(g.nx * nint_d(xdf / g.nx));
+    ydf = ydf - double(g.ny * nint_d(ydf / g.ny));
+    zdf = zdf - double(g.nz * nint_d(zdf / g.nz));
+    double rsq = xdf * xdf + ydf * ydf + zdf * zdf;
+    if (rsq > mxrsqcut) continue;
+    double rrr = sqrt(rsq);
+    double sgn = (i == lo) ? -1.0 : 1.0;
+    if (rrr <= P.hz_rmin) {
+      double ggg = (rrr <= P.hz_rcap) ? gmin : 5.0 * 0.5 * P.hz_k * pow(P.hz_rmin - rrr, 1.5);
+      f[0] += sgn * (ggg * xdf / rrr);
+      f[1] += sgn * (ggg * ydf / rrr);
+      f[2] += sgn * (ggg * zdf / rrr);
+    }
+    if (P.lub && rrr <= rparcut) {
+      double ux = xdf / rrr, uy = ydf / rrr, uz = zdf / rrr;
+      if (rrr <= rparcap) rrr = rparcap;
+      double dotuv = ux * (pl[3] - ph[3]) + uy * (pl[4] - ph[4]) + uz * (pl[5] - ph[5]);
+      double cc = lubfactor * dotuv * (1.0 / (rrr - rpar) - 1.0);
+      fl[0] += sgn * (cc * ux);
+      fl[1] += sgn * (cc * uy);
+      fl[2] += sgn * (cc * uz);
+    }
+  }
+  for (int d = 0; d < 3; ++d) {
+    acc[size_t(i) * AS + 6 + d] += f[d];
+    acc[size_t(i) * AS + 12 + d] += fl[d];
+  }
+}
+
+// time_step_force_particles: force assembly f(t) = f_other + (f_bb(t+1/2) +
+// f_bb(t-1/2))/2, leap-frog translation with the centred periodic image,
+// the implicit mid-step quaternion update, then the accumulators restart
+// from the external force and torque.
+__global__ void k_integrate(PDev P, const double* __restrict__ pos_cur, double* pos_next, double* frc_cur,
+                            double* frc_next, double* acc, Geom g, unsigned long long* err, int64_t step) {
+  int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= P.np) return;
+  const double* pc = pos_cur + size_t(a) * PS;
+  double* pn = pos_next + size_t(a) * PS;
+  double* fc = frc_cur + size_t(a) * FS;
+  double* fo = frc_next + size_t(a) * FS;  // the slot of the previous step
+  double* A = acc + size_t(a) * AS;
+  for (int d = 0; d < 3; ++d) {
+    fc[d] = A[6 + d] + A[12 + d];
+    fc[3 + d] = A[d];
+    fc[d] = fc[d] + (fc[3 + d] + fo[3 + d]) * 0.5;
+  }
+  if (P.lrotate)
+    for (int d = 0; d < 3; ++d) {
+      fc[6 + d] = A[9 + d];
+      fc[9 + d] = A[3 + d];
+      fc[6 + d] = fc[6 + d] + (fc[9 + d] + fo[9 + d]) * 0.5;
+    }
+  // nve_lf
+  const double rmass = P.rmass;
+  if (fabs(fc[0]) * rmass > 0.5 || fabs(fc[1]) * rmass > 0.5 || fabs(fc[2]) * rmass > 0.5)
+    raise_error(err, LBX_DEV_BIG_FORCE, step, a);
+  double bv[3];
+  for (int d = 0; d < 3; ++d) bv[d] = pc[3 + d] + rmass * fc[d];
+  double vm = sqrt(bv[0] * bv[0] + bv[1] * bv[1] + bv[2] * bv[2]);
+  if (vm > P.max_vel) raise_error(err, LBX_DEV_EXTREME_VEL, step, a);
+  const int nn[3] = {g.nx, g.ny, g.nz};
+  double xn[3];
+  for (int d = 0; d < 3; ++d) {
+    double cc = double(nn[d] + 1) * 0.5;
+    double xs = (pc[d] + bv[d]) - cc;
+    xn[d] = xs - double(nn[d]) * double(nint_d((1.0 / nn[d]) * xs)) + cc;
+    if (xn[d] < 0.5 || xn[d] > double(nn[d]) + 0.5) raise_error(err, LBX_DEV_POSITION, step, a);
+  }
+  if (P.lrotate) {  // rot_midstep_impl_lf
+    const double mass = 1.0 / rmass;
+    const double rotin = 2.0 / 5.0 * mass * P.rdim * P.rdim;
+    double oxx = pc[6], oyy = pc[7], ozz = pc[8];
+    double q0 = pc[9], q1 = pc[10], q2 = pc[11], q3 = pc[12];
+    double tqx = fc[6], tqy = fc[7], tqz = fc[8];
+    double m[9];
+    m[0] = q0 * q0 + q1 * q1 - q2 * q2 - q3 * q3;
+    m[1] = 2.0 * (q1 * q2 - q0 * q3);
+    m[2] = 2.0 * (q1 * q3 + q0 * q2);
+    m[3] = 2.0 * (q1 * q2 + q0 * q3);
+    m[4] = q0 * q0 - q1 * q1 + q2 * q2 - q3 * q3;
+    m[5] = 2.0 * (q2 * q3 - q0 * q1);
+    m[6] = 2.0 * (q1 * q3 - q0 * q2);
+    m[7] = 2.0 * (q2 * q3 + q0 * q1);
+    m[8] = q0 * q0 - q1 * q1 - q2 * q2 + q3 * q3;
+    double opx = oxx, opy = oyy, opz = ozz;
+    double delx = (tqx * m[0] + tqy * m[3] + tqz * m[6]) / rotin + (rotin - rotin) * opy * opz / rotin;
+    double dely = (tqx * m[1] + tqy * m[4] + tqz * m[7]) / rotin + (rotin - rotin) * opz * opx / rotin;
+    double delz = (tqx * m[2] + tqy * m[5] + tqz * m[8]) / rotin + (rotin - rotin) * opx * opy / rotin;
+    opx = oxx + delx * 0.5;
+    opy = oyy + dely * 0.5;
+    opz = ozz + delz * 0.5;
+    double dq0 = (-q1 * opx - q2 * opy - q3 * opz) * 0.5;
+    double dq1 = (q0 * opx - q3 * opy + q2 * opz) * 0.5;
+    double dq2 = (q3 * opx + q0 * opy - q1 * opz) * 0.5;
+    double dq3 = (-q2 * opx + q1 * opy + q0 * opz) * 0.5;
+    double qn0 = q0 + dq0 * 0.5, qn1 = q1 + dq1 * 0.5, qn2 = q2 + dq2 * 0.5, qn3 = q3 + dq3 * 0.5;
+    double rn = 1.0 / sqrt(qn0 * qn0 + qn1 * qn1 + qn2 * qn2 + qn3 * qn3);
+    qn0 *= rn; qn1 *= rn; qn2 *= rn; qn3 *= rn;
+    oxx += delx; oyy += dely; ozz += delz;
+    pn[6] = oxx; pn[7] = oyy; pn[8] = ozz;
+    opx = oxx; opy = oyy; opz = ozz;
+    int itq = 0;
+    double eps = 1.0e9;
+    while (itq < 20 && eps > 1.0e-24) {  // at most 20 fixed-point iterations
+      ++itq;
+      dq0 = (-qn1 * opx - qn2 * opy - qn3 * opz) * 0.5;
+      dq1 = (qn0 * opx - qn3 * opy + qn2 * opz) * 0.5;
+      dq2 = (qn3 * opx + qn0 * opy - qn1 * opz) * 0.5;
+      dq3 = (-qn2 * opx + qn1 * opy + qn0 * opz) * 0.5;
+      double a0 = qn0 + dq0 * 0.5, a1 = qn1 + dq1 * 0.5, a2 = qn2 + dq2 * 0.5, a3 = qn3 + dq3 * 0.5;
+      rn = 1.0 / sqrt(a0 * a0 + a1 * a1 + a2 * a2 + a3 * a3);
+      a0 *= rn; a1 *= rn; a2 *= rn; a3 *= rn;
+      eps = (a0 - qn0) * (a0 - qn0) + (a1 - qn1) * (a1 - qn1) + (a2 - qn2) * (a2 - qn2) + (a3 - qn3) * (a3 - qn3);
+      qn0 = a0; qn1 = a1; qn2 = a2; qn3 = a3;
+    }
+    q0 += dq0; q1 += dq1; q2 += dq2; q3 += dq3;
+    rn = 1.0 / sqrt(q0 * q0 + q1 * q1 + q2 * q2 + q3 * q3);
+    pn[9] = q0 * rn; pn[10] = q1 * rn; pn[11] = q2 * rn; pn[12] = q3 * rn;
+  } else {
+    for (int k = 6; k < PS; ++k) pn[k] = pc[k];
+  }
+  for (int d = 0; d < 3; ++d) { pn[d] = xn[d]; pn[3 + d] = bv[d]; }
+  for (int d = 0; d < 3; ++d) {
+    fo[d] = P.ext_f[d];
+    fo[3 + d] = 0;
+    A[d] = 0;             // f_bb
+    A[6 + d] = P.ext_f[d];  // f_other restarts at the external force
+    A[12 + d] = 0;
+    if (P.lrotate) {
+      fo[6 + d] = P.ext_t[d];
+      fo[9 + d] = 0;
+      A[3 + d] = 0;
+      A[9 + d] = P.ext_t[d];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+static PDev pdev(const Ctx& c) {
+  const ParticleState& s = *c.part;
+  PDev d;
+  d.np = s.np;
+  d.rmax = s.rmax;
+  d.sphereMax = s.sphereMax;
+  d.tw = s.tw;
+  d.lrotate = s.lrotate;
+  d.rdim = s.rdim;
+  d.rmass = double(c.p.rmass);
+  d.max_vel = double(c.p.max_vel);
+  d.tmpl = s.tmpl;
+  d.owner = s.owner;
+  d.bin_cnt = s.bin_cnt;
+  d.bin_list = s.bin_list;
+  d.nbx = s.nbx;
+  d.nby = s.nby;
+  d.nbz = s.nbz;
+  for (int k = 0; k < 3; ++k) {
+    d.ext_f[k] = double(c.p.ext_force[k]);
+    d.ext_t[k] = double(c.p.ext_torque[k]);
+  }
+  d.hz_k = double(c.p.hz_k);
+  d.hz_rmin = double(c.p.hz_rmin);
+  d.hz_rcap = double(c.p.hz_rcap);
+  d.lub = c.p.lubrication;
+  d.lub_k = double(c.p.lubric_k);
+  d.lub_rmin = double(c.p.lubric_rmin);
+  d.lub_rcap = double(c.p.lubric_rcap);
+  return d;
+}
+
+// spherical_template (main.CUF:1990-2130), in FP64 (rdim^2 and the integer
+// squared distances are exact in either precision)
+static std::vector<int8_t> make_template(double rdim, int& rmin, int& rmax) {
+  const double sqrcut = rdim * rdim;
+  rmin = int(std::floor(rdim));
+  rmax = int(rdim + 1.0);
+  const int w = 2 * rmax + 1;
+  std::vector<int8_t> t(size_t(w) * w * w, LBX_FLUID_FLUID);
+  auto at3 = [&](int i, int j, int k) -> int8_t& { return t[(i + rmax) + w * ((j + rmax) + w * (k + rmax))]; };
+  for (int k = -rmax; k <= rmax; ++k)
+    for (int j = -rmax; j <= rmax; ++j)
+      for (int i = -rmax; i <= rmax; ++i)
+        if (double(i * i + j * j + k * k) <= sqrcut) at3(i, j, k) = LBX_FLUID_SPHEREDEAD;
+  for (int k = -rmin; k <= rmin; ++k)
+    for (int j = -rmin; j <= rmin; ++j)
+      for (int i = -rmin; i <= rmin; ++i)
+        if (at3(i, j, k) == LBX_FLUID_SPHEREDEAD)
+          for (int l = 1; l < Q; ++l)
+            if (at3(i + ex(l), j + ey(l), k + ez(l)) == LBX_FLUID_FLUID) {
+              at3(i, j, k) = LBX_FLUID_SPHERELIST;
+              break;
+            }
+  at3(0, 0, 0) = LBX_FLUID_PARTICLECM;
+  return t;
+}
+
+int particles_create(Ctx& c) {
+  if (c.ncomp != 2) return LBX_ERR_STATE;
+  if (c.nx % TILEX || c.ny % TILEY || c.nz % TILEZ) return LBX_ERR_ARG;  // reference tile grid
+  ParticleState* s = new ParticleState();
+  c.part = s;
+  int cap = c.p.max_particles;
+  s->rdim = double(c.p.radius);
+  int rmin;
+  std::vector<int8_t> t = make_template(s->rdim, rmin, s->rmax);
+  s->tw = 2 * s->rmax + 1;
+  s->sphereMax = s->rmax * s->rmax;
+  if (c.nx < 2 * s->rmax + 2 || c.ny < 2 * s->rmax + 2 || c.nz < 2 * s->rmax + 2) return LBX_ERR_ARG;
+  s->lrotate = c.p.lrotate ? 1 : 0;
+  s->nbx = (c.nx + BINW - 1) / BINW;
+  s->nby = (c.ny + BINW - 1) / BINW;
+  s->nbz = (c.nz + BINW - 1) / BINW;
+  size_t nbins = size_t(s->nbx) * s->nby * s->nbz;
+  auto ok = [](cudaError_t e) { return e == cudaSuccess; };
+  for (int k = 0; k < 2; ++k) {
+    if (!ok(cudaMalloc(&s->pos[k], size_t(cap) * PS * 8))) return LBX_ERR_ALLOC;
+    if (!ok(cudaMalloc(&s->frc[k], size_t(cap) * FS * 8))) return LBX_ERR_ALLOC;
+    cudaMemsetAsync(s->pos[k], 0, size_t(cap) * PS * 8, c.stream);
+    cudaMemsetAsync(s->frc[k], 0, size_t(cap) * FS * 8, c.stream);
+  }
+  if (!ok(cudaMalloc(&s->acc, size_t(cap) * AS * 8))) return LBX_ERR_ALLOC;
+  if (!ok(cudaMalloc(&s->tmpl, t.size()))) return LBX_ERR_ALLOC;
+  if (!ok(cudaMalloc(&s->owner, size_t(c.n) * 4))) return LBX_ERR_ALLOC;
+  if (!ok(cudaMalloc(&s->bin_cnt, nbins * 4))) return LBX_ERR_ALLOC;
+  if (!ok(cudaMalloc(&s->bin_list, nbins * BIN_CAP * 4))) return LBX_ERR_ALLOC;
+  cudaMemsetAsync(s->acc, 0, size_t(cap) * AS * 8, c.stream);
+  cudaMemsetAsync(s->owner, 0, size_t(c.n) * 4, c.stream);
+  cudaMemcpyAsync(s->tmpl, t.data(), t.size(), cudaMemcpyHostToDevice, c.stream);
+  cudaStreamSynchronize(c.stream);
+  return launch_status();
+}
+
+void particles_destroy(Ctx& c) {
+  ParticleState* s = c.part;
+  if (!s) return;
+  for (int k = 0; k < 2; ++k) {
+    if (s->pos[k]) cudaFree(s->pos[k]);
+    if (s->frc[k]) cudaFree(s->frc[k]);
+  }
+  if (s->acc) cudaFree(s->acc);
+  if (s->tmpl) cudaFree(s->tmpl);
+  if (s->owner) cudaFree(s->owner);
+  if (s->bin_cnt) cudaFree(s->bin_cnt);
+  if (s->bin_list) cudaFree(s->bin_list);
+  delete s;
+  c.part = nullptr;
+}
+
+static int rebuild_bins(Ctx& c, const double* pos) {
+  ParticleState& s = *c.part;
+  PDev P = pdev(c);
+  Geom g = geom(c);
+  size_t nbins = size_t(s.nbx) * s.nby * s.nbz;
+  cudaMemsetAsync(s.bin_cnt, 0, nbins * 4, c.stream);
+  k_bins<<<(s.np + 127) / 128, 128, 0, c.stream>>>(P, pos, g, c.d_err, c.step + 1);
+  k_bins_sort<<<int((nbins + 255) / 256), 256, 0, c.stream>>>(P, int(nbins));
+  return launch_status();
+}
+
+// set_particles: the state read_input_atom builds (main.CUF:1230-1350) and
+// the step-0 flags of setupRho_Pops (main.CUF:2586-2600).
+int particles_set(Ctx& c, int n, const double* h_x, const double* h_v, const double* h_om, const double* h_q) {
+  ParticleState* s = c.part;
+  if (!s || n < 1 || n > c.p.max_particles) return LBX_ERR_ARG;
+  s->np = n;
+  std::vector<double> pos(size_t(n) * PS, 0.0), frc(size_t(n) * FS, 0.0);
+  for (int a = 0; a < n; ++a) {
+    for (int d = 0; d < 3; ++d) {
+      pos[size_t(a) * PS + d] = h_x[3 * a + d];
+      pos[size_t(a) * PS + 3 + d] = h_v ? h_v[3 * a + d] : 0.0;
+      pos[size_t(a) * PS + 6 + d] = h_om ? h_om[3 * a + d] : 0.0;
+      frc[size_t(a) * FS + d] = double(c.p.ext_force[d]);
+      if (c.p.lrotate) frc[size_t(a) * FS + 6 + d] = double(c.p.ext_torque[d]);
+    }
+    for (int k = 0; k < 4; ++k) pos[size_t(a) * PS + 9 + k] = h_q ? h_q[4 * a + k] : (k == 0 ? 1.0 : 0.0);
+  }
+  for (int k = 0; k < 2; ++k) {
+    cudaMemcpyAsync(s->pos[k], pos.data(), pos.size() * 8, cudaMemcpyHostToDevice, c.stream);
+    cudaMemcpyAsync(s->frc[k], frc.data(), frc.size() * 8, cudaMemcpyHostToDevice, c.stream);
+  }
+  // the FP64 accumulators start at zero (the first step has no external force
+  // in its total, as in the reference, whose myf2_d is first set at the end
+  // of step 1)
+  cudaMemsetAsync(s->acc, 0, size_t(c.p.max_particles) * AS * 8, c.stream);
+  s->pcur = 0;
+  s->active = 1;
+  // step-0 flags into the slot the first step will recompute; the slot the
+  // first step treats as "previous" stays all fluid, as in the reference
+  int slot = 1 - c.fcur;
+  int rc = rebuild_bins(c, s->pos[0]);
+  if (rc) return rc;
+  LaunchDims d = cell_dims(c);
+  k_flags<<<d.grid, d.block, 0, c.stream>>>(pdev(c), s->pos[0], geom(c), c.flags[slot]);
+  s->flags_last = slot;
+  rc = launch_status();
+  if (!rc) rc = cudaStreamSynchronize(c.stream) == cudaSuccess ? 0 : LBX_ERR_CUDA;
+  return rc;
+}
+
+// One step with particles, main.CUF:130-241.
+int particles_step(Ctx& c) {
+  ParticleState& s = *c.part;
+  Geom g = geom(c);
+  PDev P = pdev(c);
+  LaunchDims d = cell_dims(c);
+  const int fo = c.fcur, fn = 1 - c.fcur;
+  const double* pc = s.pos[s.pcur];
+  const double* po = s.pos[1 - s.pcur];
+  const int64_t st = c.step + 1;
+  int rc = by_storage(c, [&](auto* tag) {
+    using S = std::remove_pointer_t<decltype(tag)>;
+    using C = typename Store<S>::C;
+    const S* A = (const S*)c.pops[c.cur];
+    S* B = (S*)c.pops[1 - c.cur];
+    Shift<C> sh = make_shift<C>(c);
+    LatticeT<C> L = make_lattice<C>();
+    C* rR = (C*)c.rho[0];
+    C* rB = (C*)c.rho[1];
+    C* phi = (C*)c.phi;
+    // particle lists of the current positions (built after the previous
+    // step in the reference, updateListAtoms)
+    int r0 = rebuild_bins(c, pc);
+    if (r0) return r0;
+    k_flags<<<d.grid, d.block, 0, c.stream>>>(P, pc, g, c.flags[fn]);
+    k_drain<S><<<s.np, 256, 0, c.stream>>>(P, pc, po, s.acc, A, B, g, sh, c.flags[fo], c.flags[fn], rR, rB);
+    k_rho_p<S><<<d.grid, d.block, 0, c.stream>>>(A, B, g, sh, c.flags[fo], c.flags[fn], phi, rR, rB, c.d_err, st);
+    k_fill<S><<<s.np, 256, 0, c.stream>>>(P, pc, po, s.acc, B, g, sh, L, c.flags[fo], c.flags[fn], rR, rB, phi);
+    k_virtual<C><<<s.np, 256, 0, c.stream>>>(P, pc, g, c.p.wetting == LBX_WET_NEUTRAL ? 1 : 0, c.flags[fo],
+                                              c.flags[fn], rR, rB, phi, L);
+    k_collide_p<S><<<d.grid, d.block, 0, c.stream>>>(A, B, g, sh, phi, rR, rB, c.flags[fo], c.flags[fn],
+                                                     make_cg<C>(c));
+    k_bb<S><<<s.np, 256, 0, c.stream>>>(P, pc, s.acc, B, g, sh, L, c.flags[fn], rR, rB);
+    k_pairs<<<(s.np + 127) / 128, 128, 0, c.stream>>>(P, pc, s.acc, g);
+    k_integrate<<<(s.np + 127) / 128, 128, 0, c.stream>>>(P, pc, s.pos[1 - s.pcur], s.frc[s.pcur],
+                                                          s.frc[1 - s.pcur], s.acc, g, c.d_err, st);
+    return launch_status();
+  });
+  if (rc) return rc;
+  c.cur = 1 - c.cur;
+  c.fcur = fn;
+  s.flags_last = fn;
+  s.pcur = 1 - s.pcur;
+  c.step += 1;
+  return 0;
+}
+
+int particles_get(Ctx& c, double* x, double* v, double* om, double* q, double* f, double* t) {
+  ParticleState* s = c.part;
+  if (!s || !s->active) return LBX_ERR_STATE;
+  int n = s->np;
+  std::vector<double> pos(size_t(n) * PS), frc(size_t(n) * FS);
+  cudaMemcpyAsync(pos.data(), s->pos[s->pcur], pos.size() * 8, cudaMemcpyDeviceToHost, c.stream);
+  // total force / torque the integrator used in the last step
+  cudaMemcpyAsync(frc.data(), s->frc[1 - s->pcur], frc.size() * 8, cudaMemcpyDeviceToHost, c.stream);
+  if (cudaStreamSynchronize(c.stream) != cudaSuccess) return LBX_ERR_CUDA;
+  for (int a = 0; a < n; ++a) {
+    for (int d = 0; d < 3; ++d) {
+      if (x) x[3 * a + d] = pos[size_t(a) * PS + d];
+      if (v) v[3 * a + d] = pos[size_t(a) * PS + 3 + d];
+      if (om) om[3 * a + d] = pos[size_t(a) * PS + 6 + d];
+      if (f) f[3 * a + d] = frc[size_t(a) * FS + d];
+      if (t) t[3 * a + d] = frc[size_t(a) * FS + 6 + d];
+    }
+    if (q)
+      for (int k = 0; k < 4; ++k) q[4 * a + k] = pos[size_t(a) * PS + 9 + k];
+  }
+  return 0;
+}
+
+int particles_flags_slot(const Ctx& c) { return c.part ? c.part->flags_last : c.fcur; }
+int particles_active(const Ctx& c) { return c.part && c.part->active; }
+
 }  // namespace lbx

@@ -86,6 +86,26 @@ class LBSim:
         pB = None if popsB is None else np.ascontiguousarray(popsB, dtype=np.float32).reshape((Q,) + self.shape)
         check(self._L.lbx_set_pops(self._h, _fptr(pR), _fptr(pB)), "lbx_set_pops")
 
+    def set_particles(self, x, v=None, omega=None, q=None):
+        x = np.ascontiguousarray(x, np.float64)
+        n = x.shape[0]
+        v = np.zeros((n, 3)) if v is None else np.ascontiguousarray(v, np.float64)
+        om = None if omega is None else np.ascontiguousarray(omega, np.float64)
+        q = None if q is None else np.ascontiguousarray(q, np.float64)
+        D = C.c_double
+        check(self._L.lbx_set_particles(self._h, n, _fptr(x, D), _fptr(v, D), _fptr(om, D), _fptr(q, D)),
+              "lbx_set_particles")
+        self.np = n
+
+    def get_particles(self):
+        n = self.np
+        x, v, om = np.empty((n, 3)), np.empty((n, 3)), np.empty((n, 3))
+        q, fo, to = np.empty((n, 4)), np.empty((n, 3)), np.empty((n, 3))
+        D = C.c_double
+        check(self._L.lbx_get_particles(self._h, _fptr(x, D), _fptr(v, D), _fptr(om, D), _fptr(q, D),
+                                        _fptr(fo, D), _fptr(to, D)), "lbx_get_particles")
+        return dict(x=x, v=v, omega=om, q=q, force=fo, torque=to)
+
     # -- stepping --------------------------------------------------------------
     def step(self, n=1):
         check(self._L.lbx_step(self._h, int(n)), "lbx_step")

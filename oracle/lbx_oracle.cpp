@@ -197,6 +197,7 @@ class Oracle {
     halo_rho();
     halo_flags(0);
     halo_flags(1);
+    last_flags = 0;
   }
 
   void set_pops(const float* pR, const float* pB) {
@@ -370,8 +371,720 @@ class Oracle {
       for (int i = 0; i < sx; ++i) { halo_push(i, j, 0); halo_push(i, j, nz + 1); }
   }
 
+  /* =====================================================================
+   * Particles (PARTICLES build), kernels_fluid_PART.CUF and main.CUF.
+   * pos[slot][13*i + c]: c = 0..2 x, 3..5 v, 6..8 omega (body frame),
+   * 9..12 quaternion; force[slot][12*i + c]: 0..2 total force, 3..5 bounce-back
+   * force, 6..8 total torque, 9..11 bounce-back torque (dimensions_m.CUF:352-360).
+   * ===================================================================== */
+  int np = 0;
+  bool lrotate = false;
+  std::vector<P> pos[2], force[2];
+  std::vector<double> myf, myf2, myt, myt2;
+  std::vector<int> partVol, oldpartVol;
+  int rmin = 0, rmax = 0, sphereMax = 0;
+  std::vector<int8_t> issub;   /* (2rmax+1)^3, index (i+rmax) + w*((j+rmax) + w*(k+rmax)) */
+  std::vector<int> owner;      /* debugfluid_d: 1-based particle index, 0 = none */
+  static constexpr int TX = 8, TY = 4, TZ = 4; /* defines.h:14-22 tile */
+  int nbx = 0, nby = 0, nbz = 0;
+  std::vector<std::vector<int>> tiles;          /* matrixAtoms_d / dim_matAtm_d */
+  P rdim;
+  T buz;
+
+  int tw() const { return 2 * rmax + 1; }
+  int8_t sub(int i, int j, int k) const { return issub[(i + rmax) + tw() * ((j + rmax) + tw() * (k + rmax))]; }
+  P& ps(int slot, int i, int c) { return pos[slot][13 * size_t(i) + c]; }
+  P& fa(int slot, int i, int c) { return force[slot][12 * size_t(i) + c]; }
+
+  /* spherical_template, main.CUF:1990-2130 */
+  void spherical_template() {
+    const P sqrcut = rdim * rdim;
+    rmin = int(std::floor(rdim));
+    rmax = int(rdim + P(1));
+    int w = tw();
+    issub.assign(size_t(w) * w * w, int8_t(LBX_FLUID_FLUID));
+    auto at = [&](int i, int j, int k) -> int8_t& { return issub[(i + rmax) + w * ((j + rmax) + w * (k + rmax))]; };
+    for (int k = -rmax; k <= rmax; ++k)
+      for (int j = -rmax; j <= rmax; ++j)
+        for (int i = -rmax; i <= rmax; ++i)
+          if (P(i * i + j * j + k * k) <= sqrcut) at(i, j, k) = LBX_FLUID_SPHEREDEAD;
+    for (int k = -rmin; k <= rmin; ++k)
+      for (int j = -rmin; j <= rmin; ++j)
+        for (int i = -rmin; i <= rmin; ++i)
+          if (at(i, j, k) == LBX_FLUID_SPHEREDEAD)
+            for (int l = 1; l < Q; ++l)
+              if (at(i + EX[l], j + EY[l], k + EZ[l]) == LBX_FLUID_FLUID) { at(i, j, k) = LBX_FLUID_SPHERELIST; break; }
+    at(0, 0, 0) = LBX_FLUID_PARTICLECM;
+    sphereMax = rmax * rmax;
+  }
+
+  /* getDeltai/j/k, kernels_fluid_PART.CUF:182-228 */
+  int getDelta(int i, int c, int n) const {
+    int d = i - c;
+    if (P(c) - rdim < P(1) || P(c) + rdim > P(n)) {
+      if (P(c) + rdim > P(n) && P(i) < rdim) d = i - c + n;
+      else if (P(c) - rdim < P(1) && P(i) > P(n) - rdim) d = i - c - n;
+    }
+    return d;
+  }
+  int nintp(P x) const { return int(std::round(x)); }
+
+  /* zeroListAtomsGPU + makeListAtomsGPU, kernels_fluid_PART.CUF:2315-2451, in
+   * particle-index order (the reference's atomic order is not deterministic) */
+  void make_lists(int slot) {
+    for (auto& t : tiles) t.clear();
+    for (int l = 0; l < np; ++l) {
+      P x = ps(slot, l, 0), y = ps(slot, l, 1), z = ps(slot, l, 2);
+      int ci[3] = {int(std::ceil(x)), int(std::ceil(y)), int(std::ceil(z))};
+      P xc[3] = {x, y, z};
+      int nn[3] = {nx, ny, nz};
+      int td[3] = {TX, TY, TZ};
+      int box[3][4];
+      for (int d = 0; d < 3; ++d) {
+        box[d][0] = int(xc[d] - rdim); /* real -> integer truncation */
+        box[d][1] = int(xc[d] + rdim);
+        if (box[d][0] < 1) {
+          box[d][0] = 1; box[d][1] = int(P(ci[d]) + rdim); box[d][2] = int(P(ci[d]) - rdim + P(nn[d])); box[d][3] = nn[d];
+        } else if (box[d][1] > nn[d]) {
+          box[d][0] = 1; box[d][1] = int(P(ci[d]) + rdim - P(nn[d])); box[d][2] = int(P(ci[d]) - rdim); box[d][3] = nn[d];
+        } else {
+          box[d][2] = td[d]; box[d][3] = -td[d];
+        }
+      }
+      for (int lk = 0; lk < 2; ++lk) {
+        int mink = (box[2][2 * lk] - 1) / TZ + 1, maxk = (box[2][2 * lk + 1] - 1) / TZ + 1;
+        for (int k = mink; k <= maxk; ++k) {
+          if (k < 1 || k > nbz) continue;
+          for (int lj = 0; lj < 2; ++lj) {
+            int minj = (box[1][2 * lj] - 1) / TY + 1, maxj = (box[1][2 * lj + 1] - 1) / TY + 1;
+            for (int j = minj; j <= maxj; ++j) {
+              if (j < 1 || j > nby) continue;
+              for (int li = 0; li < 2; ++li) {
+                int mini = (box[0][2 * li] - 1) / TX + 1, maxi = (box[0][2 * li + 1] - 1) / TX + 1;
+                for (int i = mini; i <= maxi; ++i) {
+                  if (i < 1 || i > nbx) continue;
+                  auto& t = tiles[(i - 1) + size_t(nbx) * ((j - 1) + size_t(nby) * (k - 1))];
+                  if (int(t.size()) >= 1000) raise(LBX_DEV_LIST_OVERFLOW, l);
+                  else t.push_back(l);
+                }
+              }
+            }
+          }
+        }
+      }
+    }
+  }
+  const std::vector<int>& tile_of(int i, int j, int k) const {
+    return tiles[(i - 1) / TX + size_t(nbx) * ((j - 1) / TY + size_t(nby) * ((k - 1) / TZ))];
+  }
+
+  /* init_isfluid_CG + setmyfluid, kernels_fluid_PART.CUF:85-117,230-264 */
+  void init_isfluid(int b) {
+#pragma omp parallel for schedule(static)
+    for (int k = 1; k <= nz; ++k)
+      for (int j = 1; j <= ny; ++j)
+        for (int i = 1; i <= nx; ++i) {
+          int64_t x = id(i, j, k);
+          owner[x] = 0;
+          bool updated = false;
+          for (int a : tile_of(i, j, k)) {
+            if (updated) break;
+            int di = getDelta(i, nintp(ps(b, a, 0)), nx), dj = getDelta(j, nintp(ps(b, a, 1)), ny),
+                dk = getDelta(k, nintp(ps(b, a, 2)), nz);
+            if (std::abs(di) <= rmax && std::abs(dj) <= rmax && std::abs(dk) <= rmax) {
+              int8_t v = sub(di, dj, dk);
+              if (v != LBX_FLUID_FLUID) {
+                updated = true;
+                flags[b][x] = v;
+#pragma omp atomic
+                partVol[a] += 1;
+                owner[x] = a + 1;
+              }
+            }
+          }
+          if (!updated) flags[b][x] = LBX_FLUID_FLUID;
+        }
+    halo_flags(b);
+  }
+
+  bool particle_moved(int a) {
+    return nintp(ps(0, a, 0)) != nintp(ps(1, a, 0)) || nintp(ps(0, a, 1)) != nintp(ps(1, a, 1)) ||
+           nintp(ps(0, a, 2)) != nintp(ps(1, a, 2));
+  }
+
+  /* min-image offset of a cell from a particle, scaled to length rdim
+   * (the rtemp/rversor blocks of del_fluid, make_fluid and the bounce-back) */
+  void lever(int i, int j, int k, int a, int b, bool image, P r[3]) {
+    r[0] = P(i) - ps(b, a, 0);
+    r[1] = P(j) - ps(b, a, 1);
+    r[2] = P(k) - ps(b, a, 2);
+    if (image) {
+      const P aaa = P(1) / P(nx), bbb = P(1) / P(ny), ccc = P(1) / P(nz);
+      r[0] = r[0] - P(nx) * P(nintp(aaa * r[0]));
+      r[1] = r[1] - P(ny) * P(nintp(bbb * r[1]));
+      r[2] = r[2] - P(nz) * P(nintp(ccc * r[2]));
+    }
+    P modr = std::sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+    for (int d = 0; d < 3; ++d) r[d] = rdim / modr * r[d];
+  }
+
+  template <typename A, typename B>
+  static void cross3(const A a[3], const B b[3], P out[3]) {
+    out[0] = P(a[1]) * P(b[2]) - P(a[2]) * P(b[1]);
+    out[1] = P(a[2]) * P(b[0]) - P(a[0]) * P(b[2]);
+    out[2] = P(a[0]) * P(b[1]) - P(a[1]) * P(b[0]);
+  }
+
+  void add_acc(std::vector<double>& acc, int a, const double v[3]) {
+    for (int d = 0; d < 3; ++d) {
+#pragma omp atomic
+      acc[3 * size_t(a) + d] += v[d];
+    }
+  }
+
+  /* del_fluid, kernels_fluid_PART.CUF:383-561 */
+  void del_fluid(int b, int a, int i, int j, int k) {
+    const int o = 1 - b;
+    int di = getDelta(i, nintp(ps(o, a, 0)), nx), dj = getDelta(j, nintp(ps(o, a, 1)), ny),
+        dk = getDelta(k, nintp(ps(o, a, 2)), nz);
+    if (di * di + dj * dj + dk * dk > sphereMax) return;
+    int64_t x = id(i, j, k);
+    int8_t fo = flags[o][x], fn = flags[b][x];
+    if (fo != LBX_FLUID_FLUID || (fn != LBX_FLUID_SPHERELIST && fn != LBX_FLUID_SPHEREDEAD)) return;
+    T rR = rho[0][x], rB = rho[1][x];
+    T rhosum = rR + rB, invrho = T(1) / rhosum;
+    T qR[Q], qB[Q];
+    for (int l = 0; l < Q; ++l) { qR[l] = f(0, b, l, x); qB[l] = f(1, b, l, x); }
+    T u = mom_x(qR, invrho) + mom_x(qB, invrho);
+    T v = mom_y(qR, invrho) + mom_y(qB, invrho);
+    T w = mom_z(qR, invrho) + mom_z(qB, invrho);
+    T ft[3] = {(rR + rB) * u, (rR + rB) * v, (rR + rB) * w};
+    double acc[3] = {double(ft[0]), double(ft[1]), double(ft[2])};
+    add_acc(myf2, a, acc);
+    if (lrotate) {
+      P r[3], t[3];
+      /* the spheredead branch of the reference skips the minimum image */
+      lever(i, j, k, a, b, fn == LBX_FLUID_SPHERELIST, r);
+      cross3(r, ft, t);
+      double tt[3] = {double(t[0]), double(t[1]), double(t[2])};
+      add_acc(myt2, a, tt);
+    }
+  }
+
+  /* compute_onebelt_density_twofluids / compute_secbelt_density_twofluids,
+   * kernels_fluid_PART.CUF:783-862 */
+  int onebelt(int b, int i, int j, int k, T& Rs, T& Bs) {
+    Rs = 0; Bs = 0;
+    int D = 0;
+    for (int l = 1; l < Q27; ++l) {
+      int64_t y = id(i + EX27[l], j + EY27[l], k + EZ27[l]);
+      if (flags[b][y] == LBX_FLUID_FLUID && flags[1 - b][y] == LBX_FLUID_FLUID) {
+        Rs = Rs + rho[0][y]; Bs = Bs + rho[1][y]; D += 1;
+      }
+    }
+    if (D) { Rs = Rs / T(D); Bs = Bs / T(D); }
+    return D;
+  }
+  int secbelt(int b, int i, int j, int k, T& Rs, T& Bs) {
+    Rs = 0; Bs = 0;
+    int D = 0;
+    for (int kk = -2; kk <= 2; ++kk)
+      for (int jj = -2; jj <= 2; ++jj)
+        for (int ii = -2; ii <= 2; ++ii) {
+          if (!(ii == -2 || ii == 2 || jj == -2 || jj == 2 || kk == -2 || kk == 2)) continue;
+          int i1 = (i + ii + nx - 1) % nx + 1, j1 = (j + jj + ny - 1) % ny + 1, k1 = (k + kk + nz - 1) % nz + 1;
+          int64_t y = id(i1, j1, k1);
+          if (flags[b][y] == LBX_FLUID_FLUID && flags[1 - b][y] == LBX_FLUID_FLUID) {
+            Rs = Rs + rho[0][y]; Bs = Bs + rho[1][y]; D += 1;
+          }
+        }
+    if (D) { Rs = Rs / T(D); Bs = Bs / T(D); }
+    return D;
+  }
+
+  /* make_fluid + initialize_newnode_fluids, kernels_fluid_PART.CUF:563-747,896-913 */
+  void make_fluid(int b, int a, int i, int j, int k) {
+    const int o = 1 - b;
+    int di = getDelta(i, nintp(ps(o, a, 0)), nx), dj = getDelta(j, nintp(ps(o, a, 1)), ny),
+        dk = getDelta(k, nintp(ps(o, a, 2)), nz);
+    if (di * di + dj * dj + dk * dk > sphereMax) return;
+    int64_t x = id(i, j, k);
+    int8_t fo = flags[o][x], fn = flags[b][x];
+    if ((fo != LBX_FLUID_SPHERELIST && fo != LBX_FLUID_SPHEREDEAD) || fn != LBX_FLUID_FLUID) return;
+    T Rs, Bs;
+    if (onebelt(b, i, j, k, Rs, Bs) == 0)
+      if (secbelt(b, i, j, k, Rs, Bs) == 0) { /* fix_onebelt_density_twofluids: empty */ }
+    T u = T(ps(b, a, 3)), v = T(ps(b, a, 4)), w = T(ps(b, a, 5));
+    rho[0][x] = Rs;
+    rho[1][x] = Bs;
+    for (int l = 0; l < Q; ++l) {
+      f(0, b, l, x) = equil(tb, Rs, u, v, w, l);
+      f(1, b, l, x) = equil(tb, Bs, u, v, w, l);
+    }
+    T ft[3] = {-(Rs + Bs) * u, -(Rs + Bs) * v, -(Rs + Bs) * w};
+    double acc[3] = {double(ft[0]), double(ft[1]), double(ft[2])};
+    add_acc(myf2, a, acc);
+    if (lrotate) {
+      P r[3], t[3];
+      lever(i, j, k, a, b, fo == LBX_FLUID_SPHERELIST, r);
+      cross3(r, ft, t);
+      double tt[3] = {double(t[0]), double(t[1]), double(t[2])};
+      add_acc(myt2, a, tt);
+    }
+  }
+
+  template <typename F>
+  void for_cells_with_tile_atoms(F&& fn) {
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int k = 1; k <= nz; ++k)
+      for (int j = 1; j <= ny; ++j)
+        for (int i = 1; i <= nx; ++i)
+          for (int a : tile_of(i, j, k)) fn(a, i, j, k);
+  }
+
+  /* quaternion helpers, kernels_fluid_PART.CUF:1830-1871 */
+  static void qmult(const P a[4], const P b[4], P o[4]) {
+    o[0] = a[0] * b[0] - a[1] * b[1] - a[2] * b[2] - a[3] * b[3];
+    P c[3];
+    c[0] = a[2] * b[3] - a[3] * b[2];
+    c[1] = a[3] * b[1] - a[1] * b[3];
+    c[2] = a[1] * b[2] - a[2] * b[1];
+    for (int d = 0; d < 3; ++d) o[d + 1] = a[0] * b[d + 1] + b[0] * a[d + 1] + c[d];
+  }
+  static void qtrimult(const P a[4], const P b[4], const P c[4], P o[4]) {
+    P t[4];
+    qmult(b, c, t);
+    qmult(a, t, o);
+  }
+  /* body vector -> lab frame, q (0,v) q* */
+  void to_lab(int b, int a, const P v[3], P out[3]) {
+    P q[4] = {ps(b, a, 9), ps(b, a, 10), ps(b, a, 11), ps(b, a, 12)};
+    P qc[4] = {q[0], -q[1], -q[2], -q[3]};
+    P qv[4] = {P(0), v[0], v[1], v[2]};
+    P o[4];
+    qtrimult(q, qv, qc, o);
+    out[0] = o[1]; out[1] = o[2]; out[2] = o[3];
+  }
+
+  /* compute_virtual_rho (Janus), kernels_fluid_PART.CUF:299-352 */
+  void virtual_rho_janus(int b) {
+#pragma omp parallel for schedule(static)
+    for (int k = 1; k <= nz; ++k)
+      for (int j = 1; j <= ny; ++j)
+        for (int i = 1; i <= nx; ++i) {
+          int64_t x = id(i, j, k);
+          if (flags[b][x] != LBX_FLUID_SPHERELIST) continue;
+          int a = owner[x] - 1;
+          P r[3] = {P(i) - ps(b, a, 0), P(j) - ps(b, a, 1), P(k) - ps(b, a, 2)};
+          const P aaa = P(1) / P(nx), bbb = P(1) / P(ny), ccc = P(1) / P(nz);
+          r[0] = r[0] - P(nx) * P(nintp(aaa * r[0]));
+          r[1] = r[1] - P(ny) * P(nintp(bbb * r[1]));
+          r[2] = r[2] - P(nz) * P(nintp(ccc * r[2]));
+          P modr = std::sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+          for (int d = 0; d < 3; ++d) r[d] = r[d] / modr;
+          P ax[3] = {P(1), P(0), P(0)}, xl[3];
+          to_lab(b, a, ax, xl);
+          P c = xl[0] * r[0] + xl[1] * r[1] + xl[2] * r[2];
+          if (c < P(0)) { rho[0][x] = 0; rho[1][x] = 1; }
+          else { rho[0][x] = 1; rho[1][x] = 0; }
+        }
+  }
+
+  /* compute_densities_wall + compute_onebelt_density_2fl_weights,
+   * kernels_fluid_PART.CUF:267-297,864-894 (neutral wetting) */
+  void virtual_rho_neutral(int b) {
+    std::vector<T> nR(ncell_pad), nB(ncell_pad);
+    std::vector<char> set(ncell_pad, 0);
+#pragma omp parallel for schedule(static)
+    for (int k = 1; k <= nz; ++k)
+      for (int j = 1; j <= ny; ++j)
+        for (int i = 1; i <= nx; ++i) {
+          int64_t x = id(i, j, k);
+          int8_t fl = flags[b][x];
+          if (fl != LBX_FLUID_WALL && fl != LBX_FLUID_SPHERELIST) continue;
+          T Rs = 0, Bs = 0, Ds = 0;
+          for (int l = 1; l < Q27; ++l) {
+            int64_t y = id(i + EX27[l], j + EY27[l], k + EZ27[l]);
+            if (flags[b][y] == LBX_FLUID_FLUID) {
+              Rs = Rs + tb.p27[l] * rho[0][y]; Bs = Bs + tb.p27[l] * rho[1][y]; Ds = Ds + tb.p27[l];
+            }
+          }
+          if (Ds != T(0)) { Rs = Rs / Ds; Bs = Bs / Ds; }
+          if (Ds == T(0) && fl == LBX_FLUID_SPHERELIST) {
+            T R2, B2;
+            if (secbelt(b, i, j, k, R2, B2) != 0) { nR[x] = R2; nB[x] = B2; set[x] = 1; }
+          } else {
+            nR[x] = Rs; nB[x] = Bs; set[x] = 1;
+          }
+        }
+    /* the reference writes in place; only fluid cells are read, so the
+     * buffered write is the same */
+    for (int64_t x = 0; x < ncell_pad; ++x)
+      if (set[x]) { rho[0][x] = nR[x]; rho[1][x] = nB[x]; }
+  }
+
+  /* wall velocity of particle a at link lever r (lab frame) */
+  void wall_vel(int b, int a, const P rt[3], const P ol[3], P v[3]) {
+    P c[3];
+    cross3(ol, rt, c);
+    v[0] = ps(b, a, 3) + c[0];
+    v[1] = ps(b, a, 4) + c[1];
+    v[2] = ps(b, a, 5) + c[2];
+  }
+
+  /* node_to_particle_bounce_back_bc2, kernels_fluid_PART.CUF:1874-2113 */
+  void n2p(int b, int a, int i, int j, int k) {
+    P rv[3] = {0, 0, 0}, ol[3] = {0, 0, 0};
+    if (lrotate) {
+      P om[3] = {ps(b, a, 6), ps(b, a, 7), ps(b, a, 8)};
+      to_lab(b, a, om, ol);
+      lever(i, j, k, a, b, true, rv);
+    }
+    for (int it = 1; it <= 9; ++it) {
+      int lo = 2 * it - 1, hi = 2 * it;
+      int64_t xi = id(i + EX[lo], j + EY[lo], k + EZ[lo]);
+      int64_t xo = id(i + EX[hi], j + EY[hi], k + EZ[hi]);
+      for (int side = 0; side < 2; ++side) {
+        int64_t xf = side ? xo : xi;        /* the fluid neighbour */
+        int64_t xs = side ? xi : xo;        /* the opposite one, not fluid */
+        int lf = side ? lo : hi;            /* direction of the population read at xf */
+        int lr = side ? hi : lo;            /* direction towards xf */
+        if (!(flags[b][xf] == LBX_FLUID_FLUID && flags[b][xs] != LBX_FLUID_FLUID)) continue;
+        P v[3] = {ps(b, a, 3), ps(b, a, 4), ps(b, a, 5)};
+        P rt[3] = {0, 0, 0};
+        if (lrotate) {
+          for (int d = 0; d < 3; ++d) rt[d] = rv[d] + P(0.5) * P(d == 0 ? EX[lr] : (d == 1 ? EY[lr] : EZ[lr]));
+          wall_vel(b, a, rt, ol, v);
+        }
+        T ev = T(EX[lf]) * T(v[0]) + T(EY[lf]) * T(v[1]) + T(EZ[lf]) * T(v[2]);
+        T f2pR = T(2) * f(0, b, lf, xf) - tb.p[lf] * buz * rho[0][xf] * ev;
+        T f2pB = T(2) * f(1, b, lf, xf) - tb.p[lf] * buz * rho[1][xf] * ev;
+        T f2p = f2pR + f2pB;
+        T ft[3] = {f2p * T(EX[lf]), f2p * T(EY[lf]), f2p * T(EZ[lf])};
+        double acc[3] = {double(ft[0]), double(ft[1]), double(ft[2])};
+        add_acc(myf, a, acc);
+        if (lrotate) {
+          P t[3];
+          cross3(rt, ft, t);
+          double tt[3] = {double(t[0] * P(std::abs(EX[lf]))), double(t[1] * P(std::abs(EY[lf]))),
+                          double(t[2] * P(std::abs(EZ[lf])))};
+          add_acc(myt, a, tt);
+        }
+      }
+    }
+  }
+
+  /* particle_to_node_bounce_back_bc2_phase1, kernels_fluid_PART.CUF:2153-2199 */
+  void p2n_phase1(int b, int i, int j, int k) {
+    int64_t x = id(i, j, k);
+    for (int it = 1; it <= 9; ++it) {
+      int lo = 2 * it - 1, hi = 2 * it;
+      int64_t xi = id(i + EX[lo], j + EY[lo], k + EZ[lo]);
+      int64_t xo = id(i + EX[hi], j + EY[hi], k + EZ[hi]);
+      if (flags[b][xi] == LBX_FLUID_FLUID && flags[b][xo] != LBX_FLUID_FLUID)
+        for (int c = 0; c < 2; ++c) f(c, b, lo, x) = f(c, b, hi, xi);
+      if (flags[b][xi] != LBX_FLUID_FLUID && flags[b][xo] == LBX_FLUID_FLUID)
+        for (int c = 0; c < 2; ++c) f(c, b, hi, x) = f(c, b, lo, xo);
+    }
+  }
+
+  /* particle_to_node_bounce_back_bc2_phase2, kernels_fluid_PART.CUF:2201-2312 */
+  void p2n_phase2(int b, int a, int i, int j, int k) {
+    P rv[3] = {0, 0, 0}, ol[3] = {0, 0, 0};
+    if (lrotate) {
+      P om[3] = {ps(b, a, 6), ps(b, a, 7), ps(b, a, 8)};
+      to_lab(b, a, om, ol);
+      lever(i, j, k, a, b, true, rv);
+    }
+    int64_t x = id(i, j, k);
+    for (int it = 1; it <= 9; ++it) {
+      int lo = 2 * it - 1, hi = 2 * it;
+      int64_t xi = id(i + EX[lo], j + EY[lo], k + EZ[lo]);
+      int64_t xo = id(i + EX[hi], j + EY[hi], k + EZ[hi]);
+      for (int side = 0; side < 2; ++side) {
+        int64_t xf = side ? xo : xi;
+        int64_t xs = side ? xi : xo;
+        int lf = side ? lo : hi;
+        int lr = side ? hi : lo;
+        if (!(flags[b][xf] == LBX_FLUID_FLUID && flags[b][xs] != LBX_FLUID_FLUID)) continue;
+        P v[3] = {ps(b, a, 3), ps(b, a, 4), ps(b, a, 5)};
+        if (lrotate) {
+          P rt[3];
+          for (int d = 0; d < 3; ++d) rt[d] = rv[d] + P(0.5) * P(d == 0 ? EX[lr] : (d == 1 ? EY[lr] : EZ[lr]));
+          wall_vel(b, a, rt, ol, v);
+        }
+        T ev = T(EX[lf]) * T(v[0]) + T(EY[lf]) * T(v[1]) + T(EZ[lf]) * T(v[2]);
+        for (int c = 0; c < 2; ++c) f(c, b, lr, x) = f(c, b, lr, x) - tb.p[lf] * buz * rho[c][xf] * ev;
+      }
+    }
+  }
+
+  /* addHertzian (+ optional lubrication), kernels_fluid_PART.CUF:1385-1503 */
+  void inter_forces(int b) {
+    const P FIVE = 5, HALF = P(0.5), THREE = 3;
+    const P hz_k = P(prm.hz_k), hz_rmin = P(prm.hz_rmin), hz_rcap = P(prm.hz_rcap);
+    const P rsqcut = hz_rmin * hz_rmin;
+    const P gmin = FIVE * HALF * hz_k * std::pow(hz_rmin - hz_rcap, THREE * HALF);
+    const P rpar = P(2) * rdim;
+    const P pi = P(3.141592653589793238462643383279502884);
+    const P lubfactor = P(prm.lubric_k) * P(6) * pi * std::pow(rdim * rdim, P(2)) / (rpar * rpar);
+    const P rparcut = rpar + P(prm.lubric_rmin);
+    const P mxrsqcut = std::max(rparcut * rparcut, rsqcut);
+    const P rparcap = rpar + P(prm.lubric_rcap);
+    for (int ia = 0; ia < np; ++ia)
+      for (int ja = ia + 1; ja < np; ++ja) {
+        P xdf = ps(b, ja, 0) - ps(b, ia, 0), ydf = ps(b, ja, 1) - ps(b, ia, 1), zdf = ps(b, ja, 2) - ps(b, ia, 2);
+        xdf = xdf - P(nx * nintp(xdf / P(nx)));
+        ydf = ydf - P(ny * nintp(ydf / P(ny)));
+        zdf = zdf - P(nz * nintp(zdf / P(nz)));
+        P rsq = xdf * xdf + ydf * ydf + zdf * zdf;
+        if (rsq > mxrsqcut) continue;
+        P rrr = std::sqrt(rsq);
+        if (rrr <= hz_rmin) {
+          P ggg = (rrr <= hz_rcap) ? gmin : FIVE * HALF * hz_k * std::pow(hz_rmin - rrr, THREE * HALF);
+          double ft[3] = {double(ggg * xdf / rrr), double(ggg * ydf / rrr), double(ggg * zdf / rrr)};
+          for (int d = 0; d < 3; ++d) { myf2[3 * ia + d] -= ft[d]; myf2[3 * ja + d] += ft[d]; }
+        }
+        if (prm.lubrication && rrr <= rparcut) {
+          P ux = xdf / rrr, uy = ydf / rrr, uz = zdf / rrr;
+          if (rrr <= rparcap) rrr = rparcap;
+          P dotuv = ux * (ps(b, ia, 3) - ps(b, ja, 3)) + uy * (ps(b, ia, 4) - ps(b, ja, 4)) + uz * (ps(b, ia, 5) - ps(b, ja, 5));
+          P visc = 1;
+          P c = visc * lubfactor * dotuv * (P(1) / (rrr - rpar) - P(1));
+          double ft[3] = {double(c * ux), double(c * uy), double(c * uz)};
+          /* the reference adds these to forceAtoms(1:3) without atomics; they
+           * reach the integrator through the same total force */
+          for (int d = 0; d < 3; ++d) { lub[3 * ia + d] -= ft[d]; lub[3 * ja + d] += ft[d]; }
+        }
+      }
+  }
+  std::vector<double> lub;
+
+  /* time_step_force_particles: addForce_particle_bounce_back, nve_lf,
+   * rot_midstep_impl_lf, kernels_fluid_PART.CUF:1098-1166,1266-1827 */
+  void integrate(int b) {
+    const int o = 1 - b;
+    const P HALF = P(0.5), ONE = 1;
+    const P rmass = P(prm.rmass), max_vel = P(prm.max_vel);
+    const P mass = ONE / rmass;
+    const P rotin = P(2) / P(5) * mass * rdim * rdim;
+    const P cx = P(nx + 1) * HALF, cy = P(ny + 1) * HALF, cz = P(nz + 1) * HALF;
+    for (int a = 0; a < np; ++a) {
+      /* addForce_particle_bounce_back */
+      for (int d = 0; d < 3; ++d) {
+        fa(b, a, d) = P(myf2[3 * a + d]) + P(lub[3 * a + d]);
+        fa(b, a, 3 + d) = P(myf[3 * a + d]);
+        fa(b, a, d) = fa(b, a, d) + (fa(b, a, 3 + d) + fa(o, a, 3 + d)) * HALF;
+      }
+      if (lrotate)
+        for (int d = 0; d < 3; ++d) {
+          fa(b, a, 6 + d) = P(myt2[3 * a + d]);
+          fa(b, a, 9 + d) = P(myt[3 * a + d]);
+          fa(b, a, 6 + d) = fa(b, a, 6 + d) + (fa(b, a, 9 + d) + fa(o, a, 9 + d)) * HALF;
+        }
+      /* nve_lf */
+      P xo[3] = {ps(b, a, 0), ps(b, a, 1), ps(b, a, 2)};
+      P v[3] = {ps(b, a, 3), ps(b, a, 4), ps(b, a, 5)};
+      P fr[3] = {fa(b, a, 0), fa(b, a, 1), fa(b, a, 2)};
+      if (std::abs(fr[0]) * rmass > P(0.5) || std::abs(fr[1]) * rmass > P(0.5) || std::abs(fr[2]) * rmass > P(0.5))
+        raise(LBX_DEV_BIG_FORCE, a);
+      P bv[3];
+      for (int d = 0; d < 3; ++d) bv[d] = v[d] + rmass * fr[d];
+      P vm = std::sqrt(bv[0] * bv[0] + bv[1] * bv[1] + bv[2] * bv[2]);
+      if (vm > max_vel) raise(LBX_DEV_EXTREME_VEL, a);
+      P xn[3];
+      for (int d = 0; d < 3; ++d) xn[d] = xo[d] + bv[d];
+      const P cc[3] = {cx, cy, cz};
+      const int nn[3] = {nx, ny, nz};
+      for (int d = 0; d < 3; ++d) {
+        P xs = xn[d] - cc[d];
+        P aaa = ONE / P(nn[d]);
+        xn[d] = xs - P(nn[d]) * P(nintp(aaa * xs)) + cc[d];
+        if (xn[d] < P(0.5) || xn[d] > P(nn[d]) + P(0.5)) raise(LBX_DEV_POSITION, a);
+      }
+      if (lrotate) rot_midstep(b, a, rotin);
+      for (int d = 0; d < 3; ++d) { ps(o, a, d) = xn[d]; ps(o, a, 3 + d) = bv[d]; }
+      if (!lrotate)
+        for (int c = 6; c < 13; ++c) ps(o, a, c) = ps(b, a, c);
+      /* reset the accumulators to the external force / torque */
+      for (int d = 0; d < 3; ++d) {
+        fa(o, a, d) = P(prm.ext_force[d]);
+        fa(o, a, 3 + d) = 0;
+        myf[3 * a + d] = 0;
+        myf2[3 * a + d] = double(prm.ext_force[d]);
+        lub[3 * a + d] = 0;
+        if (lrotate) {
+          fa(o, a, 6 + d) = P(prm.ext_torque[d]);
+          fa(o, a, 9 + d) = 0;
+          myt[3 * a + d] = 0;
+          myt2[3 * a + d] = double(prm.ext_torque[d]);
+        }
+      }
+      oldpartVol[a] = partVol[a];
+      partVol[a] = 0;
+    }
+  }
+
+  /* rot_midstep_impl_lf, kernels_fluid_PART.CUF:1621-1827 */
+  void rot_midstep(int b, int a, P rotin) {
+    const int o = 1 - b;
+    const P HALF = P(0.5), ONE = 1;
+    const int mxquat = 20;
+    const P sqquattol = P(1.0e-24);
+    P oxx = ps(b, a, 6), oyy = ps(b, a, 7), ozz = ps(b, a, 8);
+    P q0 = ps(b, a, 9), q1 = ps(b, a, 10), q2 = ps(b, a, 11), q3 = ps(b, a, 12);
+    P tqx = fa(b, a, 6), tqy = fa(b, a, 7), tqz = fa(b, a, 8);
+    P m[9];
+    m[0] = q0 * q0 + q1 * q1 - q2 * q2 - q3 * q3;
+    m[1] = P(2) * (q1 * q2 - q0 * q3);
+    m[2] = P(2) * (q1 * q3 + q0 * q2);
+    m[3] = P(2) * (q1 * q2 + q0 * q3);
+    m[4] = q0 * q0 - q1 * q1 + q2 * q2 - q3 * q3;
+    m[5] = P(2) * (q2 * q3 - q0 * q1);
+    m[6] = P(2) * (q1 * q3 - q0 * q2);
+    m[7] = P(2) * (q2 * q3 + q0 * q1);
+    m[8] = q0 * q0 - q1 * q1 - q2 * q2 + q3 * q3;
+    P opx = oxx, opy = oyy, opz = ozz;
+    const P rix = rotin, riy = rotin, riz = rotin;
+    P trx = (tqx * m[0] + tqy * m[3] + tqz * m[6]) / rix + (riy - riz) * opy * opz / rix;
+    P tr_y = (tqx * m[1] + tqy * m[4] + tqz * m[7]) / riy + (riz - rix) * opz * opx / riy;
+    P trz = (tqx * m[2] + tqy * m[5] + tqz * m[8]) / riz + (rix - riy) * opx * opy / riz;
+    P delx = trx, dely = tr_y, delz = trz;
+    opx = oxx + delx * HALF;
+    opy = oyy + dely * HALF;
+    opz = ozz + delz * HALF;
+    P dq0 = (-q1 * opx - q2 * opy - q3 * opz) * HALF;
+    P dq1 = (q0 * opx - q3 * opy + q2 * opz) * HALF;
+    P dq2 = (q3 * opx + q0 * opy - q1 * opz) * HALF;
+    P dq3 = (-q2 * opx + q1 * opy + q0 * opz) * HALF;
+    P qn0 = q0 + dq0 * HALF, qn1 = q1 + dq1 * HALF, qn2 = q2 + dq2 * HALF, qn3 = q3 + dq3 * HALF;
+    P rnorm = ONE / std::sqrt(qn0 * qn0 + qn1 * qn1 + qn2 * qn2 + qn3 * qn3);
+    qn0 *= rnorm; qn1 *= rnorm; qn2 *= rnorm; qn3 *= rnorm;
+    oxx = oxx + delx;
+    oyy = oyy + dely;
+    ozz = ozz + delz;
+    ps(o, a, 6) = oxx;
+    ps(o, a, 7) = oyy;
+    ps(o, a, 8) = ozz;
+    opx = oxx; opy = oyy; opz = ozz;
+    int itq = 0;
+    P eps = P(1.0e9);
+    while (itq < mxquat && eps > sqquattol) {
+      itq += 1;
+      dq0 = (-qn1 * opx - qn2 * opy - qn3 * opz) * HALF;
+      dq1 = (qn0 * opx - qn3 * opy + qn2 * opz) * HALF;
+      dq2 = (qn3 * opx + qn0 * opy - qn1 * opz) * HALF;
+      dq3 = (-qn2 * opx + qn1 * opy + qn0 * opz) * HALF;
+      P a0 = qn0 + dq0 * HALF, a1 = qn1 + dq1 * HALF, a2 = qn2 + dq2 * HALF, a3 = qn3 + dq3 * HALF;
+      rnorm = ONE / std::sqrt(a0 * a0 + a1 * a1 + a2 * a2 + a3 * a3);
+      a0 *= rnorm; a1 *= rnorm; a2 *= rnorm; a3 *= rnorm;
+      eps = (a0 - qn0) * (a0 - qn0) + (a1 - qn1) * (a1 - qn1) + (a2 - qn2) * (a2 - qn2) + (a3 - qn3) * (a3 - qn3);
+      qn0 = a0; qn1 = a1; qn2 = a2; qn3 = a3;
+    }
+    q0 = q0 + dq0; q1 = q1 + dq1; q2 = q2 + dq2; q3 = q3 + dq3;
+    rnorm = ONE / std::sqrt(q0 * q0 + q1 * q1 + q2 * q2 + q3 * q3);
+    ps(o, a, 9) = q0 * rnorm;
+    ps(o, a, 10) = q1 * rnorm;
+    ps(o, a, 11) = q2 * rnorm;
+    ps(o, a, 12) = q3 * rnorm;
+  }
+
+  void set_particles(int n, const double* x, const double* v, const double* om, const double* q) {
+    np = n;
+    lrotate = prm.lrotate != 0;
+    rdim = P(prm.radius);
+    buz = T(2) / tb.cssq; /* pref_bouzidi, dimensions_m.CUF:95 */
+    for (int s2 = 0; s2 < 2; ++s2) {
+      pos[s2].assign(13 * size_t(n), P(0));
+      force[s2].assign(12 * size_t(n), P(0));
+    }
+    myf.assign(3 * size_t(n), 0); myf2 = myf; myt = myf; myt2 = myf; lub = myf;
+    partVol.assign(n, 0); oldpartVol.assign(n, 0);
+    owner.assign(ncell_pad, 0);
+    for (int a = 0; a < n; ++a)
+      for (int s2 = 0; s2 < 2; ++s2) {
+        for (int d = 0; d < 3; ++d) {
+          ps(s2, a, d) = P(x[3 * a + d]);
+          ps(s2, a, 3 + d) = P(v[3 * a + d]);
+          ps(s2, a, 6 + d) = om ? P(om[3 * a + d]) : P(0);
+          fa(s2, a, d) = P(prm.ext_force[d]);
+          if (lrotate) fa(s2, a, 6 + d) = P(prm.ext_torque[d]);
+        }
+        for (int c = 0; c < 4; ++c) ps(s2, a, 9 + c) = q ? P(q[4 * a + c]) : P(c == 0 ? 1 : 0);
+      }
+    nbx = nx / TX; nby = ny / TY; nbz = nz / TZ;
+    tiles.assign(size_t(nbx) * nby * nbz, {});
+    spherical_template();
+    make_lists(flip);
+    /* setupRho_Pops: init_isfluid_CG at step 0 + flag halo; partVol reset */
+    init_isfluid(flip);
+    last_flags = flip;
+    std::fill(partVol.begin(), partVol.end(), 0);
+  }
+
+  void get_particles(double* x, double* v, double* om, double* q, double* fo, double* to) {
+    int b = flip;
+    for (int a = 0; a < np; ++a) {
+      for (int d = 0; d < 3; ++d) {
+        if (x) x[3 * a + d] = double(ps(b, a, d));
+        if (v) v[3 * a + d] = double(ps(b, a, 3 + d));
+        if (om) om[3 * a + d] = double(ps(b, a, 6 + d));
+        /* the total force / torque the integrator used in the last step */
+        if (fo) fo[3 * a + d] = double(fa(1 - b, a, d));
+        if (to) to[3 * a + d] = double(fa(1 - b, a, 6 + d));
+      }
+      if (q)
+        for (int c = 0; c < 4; ++c) q[4 * a + c] = double(ps(b, a, 9 + c));
+    }
+  }
+
+  /* ---- one step with particles, main.CUF:130-241 --------------------------- */
+  void do_step_particles() {
+    step += 1;
+    const int b = flip;
+    init_isfluid(b);
+    for_cells_with_tile_atoms([&](int a, int i, int j, int k) {
+      if (particle_moved(a)) del_fluid(b, a, i, j, k);
+    });
+    init_rho();
+    for_cells_with_tile_atoms([&](int a, int i, int j, int k) {
+      if (particle_moved(a)) make_fluid(b, a, i, j, k);
+    });
+    halo_rho();
+    if (prm.wetting == LBX_WET_NEUTRAL) virtual_rho_neutral(b);
+    else virtual_rho_janus(b);
+    halo_rho();
+    time_step_cg();
+    /* partBB_CG: n2p for every tile atom within sphereMax of a spherelist node */
+    for_cells_with_tile_atoms([&](int a, int i, int j, int k) {
+      if (flags[b][id(i, j, k)] != LBX_FLUID_SPHERELIST) return;
+      int di = getDelta(i, nintp(ps(b, a, 0)), nx), dj = getDelta(j, nintp(ps(b, a, 1)), ny),
+          dk = getDelta(k, nintp(ps(b, a, 2)), nz);
+      if (di * di + dj * dj + dk * dk < sphereMax) n2p(b, a, i, j, k);
+    });
+#pragma omp parallel for schedule(static)
+    for (int k = 1; k <= nz; ++k)
+      for (int j = 1; j <= ny; ++j)
+        for (int i = 1; i <= nx; ++i)
+          if (flags[b][id(i, j, k)] == LBX_FLUID_SPHERELIST) p2n_phase1(b, i, j, k);
+    for_cells_with_tile_atoms([&](int a, int i, int j, int k) {
+      if (flags[b][id(i, j, k)] != LBX_FLUID_SPHERELIST) return;
+      int di = getDelta(i, nintp(ps(b, a, 0)), nx), dj = getDelta(j, nintp(ps(b, a, 1)), ny),
+          dk = getDelta(k, nintp(ps(b, a, 2)), nz);
+      if (di * di + dj * dj + dk * dk < sphereMax) p2n_phase2(b, a, i, j, k);
+    });
+    halo_pops(b);
+    stream();
+    inter_forces(b);
+    integrate(b);
+    make_lists(1 - b);
+    last_flags = b;
+    flip = 1 - flip;
+  }
+
   /* ---- one step, main.CUF:125-308 (no particles) ----------------------------- */
   void do_step() {
+    if (np > 0) { do_step_particles(); return; }
     step += 1;
     if (model == LBX_MODEL_CG) {
       init_rho();
@@ -380,12 +1093,15 @@ class Oracle {
       time_step_bgk();
     }
     stream();
+    last_flags = flip;
     flip = 1 - flip;
   }
 
   /* ---- moments2Fl, write_output.f90:975-1041 (on the current flip buffer) ---- */
+  int last_flags = 0; /* flag slot of the last completed step (or of the setup) */
   void get_fields(double* oR, double* oB, double* vel, double* phase) {
     const int b = flip;
+    const int bf = last_flags;
     const T ONE = 1, MINDENS = 0;
     int ncomp = (model == LBX_MODEL_CG) ? 2 : 1;
     int64_t n = int64_t(nx) * ny * nz;
@@ -407,7 +1123,7 @@ class Oracle {
                        pB[3] - pB[4] + pB[7] - pB[8] + pB[9] - pB[10] + pB[15] - pB[16] - pB[17] + pB[18]);
           T w = inv * (pR[5] - pR[6] + pR[11] - pR[12] + pR[13] - pR[14] + pR[15] - pR[16] + pR[17] - pR[18] +
                        pB[5] - pB[6] + pB[11] - pB[12] + pB[13] - pB[14] + pB[15] - pB[16] + pB[17] - pB[18]);
-          bool ok = flags[b][x] == LBX_FLUID_FLUID && rs > MINDENS;
+          bool ok = flags[bf][x] == LBX_FLUID_FLUID && rs > MINDENS;
           if (oR) oR[h] = ok ? double(lr) : 0.0;
           if (oB) oB[h] = ok ? double(lb) : 0.0;
           if (vel) {
@@ -437,7 +1153,7 @@ class Oracle {
   }
 
   void get_flags(int8_t* out) {
-    const int b = 1 - flip; /* flags of the last step taken */
+    const int b = last_flags;
     for (int k = 1; k <= nz; ++k)
       for (int j = 1; j <= ny; ++j)
         for (int i = 1; i <= nx; ++i)
@@ -518,6 +1234,50 @@ int orc_status(void* h, int* code, int* step, int64_t* where) {
     if (step) *step = o.err_step;
     if (where) *where = o.err_where;
     o.err_code = 0;
+    return 0;
+  });
+}
+int orc_set_particles(void* h, int n, const double* x, const double* v, const double* om, const double* q) {
+  return dispatch(h, [&](auto& o) {
+    if (o.model != LBX_MODEL_CG || n < 1) return int(LBX_ERR_ARG);
+    if (o.nx % 8 || o.ny % 4 || o.nz % 4) return int(LBX_ERR_ARG); /* reference tile 8x4x4 */
+    o.set_particles(n, x, v, om, q);
+    return o.err_code;
+  });
+}
+int orc_get_particles(void* h, double* x, double* v, double* om, double* q, double* fo, double* to) {
+  return dispatch(h, [&](auto& o) { o.get_particles(x, v, om, q, fo, to); return 0; });
+}
+/* accumulators of the current step: myf (bounce-back), myf2 (fill/drain +
+ * pair + external), myt, myt2, each 3*np */
+int orc_get_accumulators(void* h, double* f_bb, double* f_other, double* t_bb, double* t_other) {
+  return dispatch(h, [&](auto& o) {
+    for (size_t i = 0; i < o.myf.size(); ++i) {
+      if (f_bb) f_bb[i] = o.myf[i];
+      if (f_other) f_other[i] = o.myf2[i];
+      if (t_bb) t_bb[i] = o.myt[i];
+      if (t_other) t_other[i] = o.myt2[i];
+    }
+    return 0;
+  });
+}
+int orc_get_rho(void* h, double* rR, double* rB) {
+  return dispatch(h, [&](auto& o) {
+    for (int k = 1; k <= o.nz; ++k)
+      for (int j = 1; j <= o.ny; ++j)
+        for (int i = 1; i <= o.nx; ++i) {
+          int64_t x = o.id(i, j, k);
+          int64_t hh = (i - 1) + int64_t(o.nx) * ((j - 1) + int64_t(o.ny) * (k - 1));
+          if (rR) rR[hh] = double(o.rho[0][x]);
+          if (rB) rB[hh] = double(o.rho[1][x]);
+        }
+    return 0;
+  });
+}
+int orc_template(void* h, int* rmax, int8_t* out) {
+  return dispatch(h, [&](auto& o) {
+    if (rmax) *rmax = o.rmax;
+    if (out) for (size_t i = 0; i < o.issub.size(); ++i) out[i] = o.issub[i];
     return 0;
   });
 }

@@ -38,6 +38,11 @@ def lib():
         L.orc_get_flags.argtypes = [P, C.POINTER(C.c_int8)]
         L.orc_status.argtypes = [P, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int64)]
         L.orc_num_threads.restype = C.c_int
+        L.orc_set_particles.argtypes = [P, C.c_int, D, D, D, D]
+        L.orc_get_particles.argtypes = [P, D, D, D, D, D, D]
+        L.orc_get_accumulators.argtypes = [P, D, D, D, D]
+        L.orc_get_rho.argtypes = [P, D, D]
+        L.orc_template.argtypes = [P, C.POINTER(C.c_int), C.POINTER(C.c_int8)]
         _lib = L
     return _lib
 
@@ -109,6 +114,39 @@ class OracleSim:
         f = np.empty(self.shape, np.int8)
         self._L.orc_get_flags(self._h, _p(f, C.c_int8))
         return f
+
+    def set_particles(self, x, v=None, omega=None, q=None):
+        x = np.ascontiguousarray(x, np.float64)
+        n = x.shape[0]
+        v = np.zeros((n, 3)) if v is None else np.ascontiguousarray(v, np.float64)
+        om = None if omega is None else np.ascontiguousarray(omega, np.float64)
+        q = None if q is None else np.ascontiguousarray(q, np.float64)
+        D = C.c_double
+        rc = self._L.orc_set_particles(self._h, n, _p(x, D), _p(v, D), _p(om, D), _p(q, D))
+        if rc:
+            raise RuntimeError(f"orc_set_particles {rc}")
+        self.np = n
+
+    def get_particles(self):
+        n = self.np
+        x, v, om = np.empty((n, 3)), np.empty((n, 3)), np.empty((n, 3))
+        q, fo, to = np.empty((n, 4)), np.empty((n, 3)), np.empty((n, 3))
+        D = C.c_double
+        self._L.orc_get_particles(self._h, _p(x, D), _p(v, D), _p(om, D), _p(q, D), _p(fo, D), _p(to, D))
+        return dict(x=x, v=v, omega=om, q=q, force=fo, torque=to)
+
+    def get_rho(self):
+        rR, rB = np.empty(self.shape), np.empty(self.shape)
+        self._L.orc_get_rho(self._h, _p(rR, C.c_double), _p(rB, C.c_double))
+        return rR, rB
+
+    def template(self):
+        rm = C.c_int()
+        self._L.orc_template(self._h, C.byref(rm), None)
+        w = 2 * rm.value + 1
+        t = np.empty(w ** 3, np.int8)
+        self._L.orc_template(self._h, C.byref(rm), _p(t, C.c_int8))
+        return t.reshape(w, w, w)  # [k][j][i]
 
     def status(self):
         c, s, w = C.c_int(), C.c_int(), C.c_int64()
