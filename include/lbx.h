@@ -167,11 +167,14 @@ const char* lbx_error_string(int code);
 int lbx_get_step(void* ctx, int64_t* step);
 
 /* ---- measurement ------------------------------------------------------- */
-/* Colour-gradient schedule: 1 = single-pass fused kernel (default), 0 = two
- * passes (phase field, then collision).  The reference prints Mlup/s from
- * CUDA events around the step loop (main.CUF:274-292); these are the hooks
- * the benchmark uses for the same. */
+/* Colour-gradient schedule: 2 = lean single-pass kernel (default), 1 = the
+ * first single-pass kernel, 0 = two passes (phase field, then collision).
+ * The reference prints Mlup/s from CUDA events around the step loop
+ * (main.CUF:274-292); these are the hooks the benchmark uses for the same. */
 int lbx_set_schedule(void* ctx, int32_t fused);
+/* Lean single-pass kernel shape: 0 = 32x8 cells per CTA, 1 = 32x16; zlen =
+ * lattice planes per z-segment (0 = automatic). */
+int lbx_set_lean_shape(void* ctx, int32_t shape, int32_t zlen);
 /* Enqueue nsteps steps bracketed by CUDA events on the context stream and
  * wait: total device ms, and the summed duration / launch count of the
  * step's dominant kernel (NULL kernel_ms disables per-kernel events). */

@@ -13,8 +13,10 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "liblbx.so")
+DRIVER = os.path.join(HERE, "lbx_run")
 
-SOURCES = ["lbx_api.cu", "lbx_fluid.cu", "lbx_particles.cu"]
+SOURCES = ["lbx_api.cu", "lbx_fluid.cu", "lbx_fused.cu", "lbx_particles.cu"]
+HOST_SOURCES = ["lbx_driver.cpp"]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-lineinfo", "-O3", "-std=c++17",
@@ -35,9 +37,17 @@ def build(verbose=False, extra=()):
     srcs = [os.path.join(CSRC, s) for s in SOURCES]
     newest = max(os.path.getmtime(p) for p in srcs + [os.path.join(CSRC, h) for h in os.listdir(CSRC)]
                  + [os.path.join(ROOT, "include", "lbx.h")])
-    if os.path.exists(LIB) and os.path.getmtime(LIB) >= newest and not extra:
+    fresh = all(os.path.exists(f) and os.path.getmtime(f) >= newest for f in (LIB, DRIVER))
+    if fresh and not extra:
         return LIB
     cmd = [nvcc()] + NVCC_FLAGS + list(extra) + srcs + ["-o", LIB]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    subprocess.run(cmd, check=True)
+    # command-line host (input.dat driver), linked against the library
+    cmd = ["g++", "-O2", "-std=c++17", os.path.join(CSRC, "lbx_driver.cpp"), "-I", os.path.join(ROOT, "include"),
+           "-I", "/usr/local/cuda/include", "-L", HERE, "-llbx", "-L", "/usr/local/cuda/lib64", "-lcudart",
+           "-Wl,-rpath,$ORIGIN", "-Wl,-rpath,/usr/local/cuda/lib64", "-o", DRIVER]
     if verbose:
         print(" ".join(cmd), flush=True)
     subprocess.run(cmd, check=True)

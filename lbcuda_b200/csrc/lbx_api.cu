@@ -348,7 +348,18 @@ const char* lbx_error_string(int code) {
 int lbx_set_schedule(void* ctx, int32_t fused) {
   Ctx* c = as_ctx(ctx);
   if (!c) return LBX_ERR_ARG;
-  c->fused = fused ? 1 : 0;
+  if (fused < 0 || fused > 2) return LBX_ERR_ARG;
+  c->fused = fused;
+  return 0;
+}
+
+/* Shape of the lean single-pass kernel: shape 0 = 32x8 cells per CTA, 1 =
+ * 32x16; zlen = planes per z-segment (0 = automatic). */
+int lbx_set_lean_shape(void* ctx, int32_t shape, int32_t zlen) {
+  Ctx* c = as_ctx(ctx);
+  if (!c || shape < 0 || shape > 1 || zlen < 0) return LBX_ERR_ARG;
+  c->lean_shape = shape;
+  c->lean_zlen = zlen;
   return 0;
 }
 

@@ -39,7 +39,9 @@ struct Ctx {
   unsigned long long* d_err = nullptr;
   cudaStream_t stream = nullptr;
   int64_t step = 0;
-  int fused = 1;            // 1: single-pass colour-gradient kernel, 0: two passes
+  int fused = 2;            // colour-gradient schedule: 0 two passes, 1 first single-pass kernel, 2 lean single pass
+  int lean_shape = 0;       // lean kernel CTA: 0 = 32x8 (2 per SM), 1 = 32x16
+  int lean_zlen = 0;        // z-segment length of the lean kernel (0 = automatic)
   // timing of the dominant kernel (opt-in)
   int kt_on = 0;
   std::vector<cudaEvent_t> kt_ev;
@@ -61,5 +63,6 @@ int fluid_step(Ctx& c);
 int fluid_get_fields(Ctx& c, void* d_rR, void* d_rB, void* d_vel, void* d_phase, int f64);
 int fluid_get_pops(Ctx& c, float* d_pR, float* d_pB);
 int fluid_get_sums(Ctx& c, double* d_out5);
+int fluid_lean(Ctx& c);
 
 }  // namespace lbx

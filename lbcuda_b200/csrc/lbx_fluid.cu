@@ -417,7 +417,7 @@ int fluid_set_pops(Ctx& c, const float* d_pR, const float* d_pB) {
   });
 }
 
-static void kt_begin(Ctx& c) {
+void kt_begin(Ctx& c) {
   if (!c.kt_on) return;
   if (c.kt_ev.size() < size_t(2 * (c.kt_n + 1))) {
     cudaEvent_t e0, e1;
@@ -428,7 +428,7 @@ static void kt_begin(Ctx& c) {
   }
   cudaEventRecord(c.kt_ev[2 * c.kt_n], c.stream);
 }
-static void kt_end(Ctx& c) {
+void kt_end(Ctx& c) {
   if (!c.kt_on) return;
   cudaEventRecord(c.kt_ev[2 * c.kt_n + 1], c.stream);
   c.kt_n += 1;
@@ -516,7 +516,9 @@ int fluid_step(Ctx& c) {
   int rc;
   if (c.ncomp == 1) {
     rc = fluid_bgk(c);
-  } else if (c.fused) {
+  } else if (c.fused == 2) {
+    rc = fluid_lean(c);
+  } else if (c.fused == 1) {
     rc = fluid_fused(c);
   } else {
     rc = fluid_init_rho(c);

@@ -75,6 +75,12 @@ struct PDev {  // by-value kernel argument
 // small device helpers
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ int nint_d(double x) { return int(round(x)); }  // Fortran NINT
+// NINT of a coordinate used to index the lattice: a non-finite or far
+// out-of-box value (the integrator has already raised LBX_DEV_POSITION for it)
+// maps to cell 1 so that no index leaves the arrays
+__device__ __forceinline__ int nint_idx(double x, int n) {
+  return (x > -double(n) && x < 2.0 * double(n)) ? int(round(x)) : 1;
+}
 
 // getDeltai/j/k (kernels_fluid_PART.CUF:182-228)
 __device__ __forceinline__ int get_delta(int i, int c, int n, double rdim) {
@@ -189,7 +195,7 @@ __global__ void k_bins(PDev P, const double* __restrict__ pos, Geom g, unsigned 
   int a = blockIdx.x * blockDim.x + threadIdx.x;
   if (a >= P.np) return;
   const double* p = pos + size_t(a) * PS;
-  const int c[3] = {nint_d(p[0]), nint_d(p[1]), nint_d(p[2])};
+  const int c[3] = {nint_idx(p[0], g.nx), nint_idx(p[1], g.ny), nint_idx(p[2], g.nz)};
   const int n[3] = {g.nx, g.ny, g.nz};
   const int nb[3] = {P.nbx, P.nby, P.nbz};
   // distinct bins hit by the cells c - rmax .. c + rmax of each axis (periodic)
@@ -243,9 +249,9 @@ __global__ void k_flags(PDev P, const double* __restrict__ pos, Geom g, int8_t* 
   for (int t = 0; t < n; ++t) {
     int a = L[t];
     const double* p = pos + size_t(a) * PS;
-    int di = get_delta(x + 1, nint_d(p[0]), g.nx, P.rdim);
-    int dj = get_delta(y + 1, nint_d(p[1]), g.ny, P.rdim);
-    int dk = get_delta(z + 1, nint_d(p[2]), g.nz, P.rdim);
+    int di = get_delta(x + 1, nint_idx(p[0], g.nx), g.nx, P.rdim);
+    int dj = get_delta(y + 1, nint_idx(p[1], g.ny), g.ny, P.rdim);
+    int dk = get_delta(z + 1, nint_idx(p[2], g.nz), g.nz, P.rdim);
     if (abs(di) <= P.rmax && abs(dj) <= P.rmax && abs(dk) <= P.rmax) {
       int8_t v = P.tmpl[(di + P.rmax) + P.tw * ((dj + P.rmax) + P.tw * (dk + P.rmax))];
       if (v != LBX_FLUID_FLUID) {
@@ -292,7 +298,7 @@ __global__ void __launch_bounds__(256) k_drain(PDev P, const double* __restrict_
   const double* pc = pos_cur + size_t(a) * PS;
   const double* po = pos_old + size_t(a) * PS;
   if (!moved(pc, po)) return;
-  const int c[3] = {nint_d(po[0]), nint_d(po[1]), nint_d(po[2])};
+  const int c[3] = {nint_idx(po[0], g.nx), nint_idx(po[1], g.ny), nint_idx(po[2], g.nz)};
   const int n[3] = {g.nx, g.ny, g.nz};
   double s[6] = {0, 0, 0, 0, 0, 0};
   for_box(P, g, c, [&](int i1, int j1, int k1, int di, int dj, int dk) {
@@ -374,7 +380,7 @@ __global__ void __launch_bounds__(256) k_fill(PDev P, const double* __restrict__
   const double* pc = pos_cur + size_t(a) * PS;
   const double* po = pos_old + size_t(a) * PS;
   if (!moved(pc, po)) return;
-  const int c[3] = {nint_d(po[0]), nint_d(po[1]), nint_d(po[2])};
+  const int c[3] = {nint_idx(po[0], g.nx), nint_idx(po[1], g.ny), nint_idx(po[2], g.nz)};
   const int n[3] = {g.nx, g.ny, g.nz};
   double s[6] = {0, 0, 0, 0, 0, 0};
   for_box(P, g, c, [&](int i1, int j1, int k1, int di, int dj, int dk) {
@@ -440,7 +446,7 @@ __global__ void __launch_bounds__(256) k_virtual(PDev P, const double* __restric
                                                  C* rhoR, C* rhoB, C* phi, LatticeT<C> L) {
   const int a = blockIdx.x;
   const double* pc = pos + size_t(a) * PS;
-  const int c[3] = {nint_d(pc[0]), nint_d(pc[1]), nint_d(pc[2])};
+  const int c[3] = {nint_idx(pc[0], g.nx), nint_idx(pc[1], g.ny), nint_idx(pc[2], g.nz)};
   double xl[3] = {0, 0, 0};
   if (!neutral) {
     double ax[3] = {1.0, 0.0, 0.0};
@@ -572,7 +578,7 @@ __global__ void __launch_bounds__(256) k_bb(PDev P, const double* __restrict__ p
   using C = typename Store<S>::C;
   const int a = blockIdx.x;
   const double* pc = pos + size_t(a) * PS;
-  const int c[3] = {nint_d(pc[0]), nint_d(pc[1]), nint_d(pc[2])};
+  const int c[3] = {nint_idx(pc[0], g.nx), nint_idx(pc[1], g.ny), nint_idx(pc[2], g.nz)};
   const C buz = C(2) / L.cssq;  // pref_bouzidi, dimensions_m.CUF:95
   double s[6] = {0, 0, 0, 0, 0, 0};
   for_box(P, g, c, [&](int i1, int j1, int k1, int di, int dj, int dk) {
@@ -634,8 +640,9 @@ __global__ void __launch_bounds__(256) k_bb(PDev P, const double* __restrict__ p
     for (int t = 0; t < nlist; ++t) {
       const int q = Lst[t];
       const double* pq = pos + size_t(q) * PS;
-      int ei = get_delta(i1, nint_d(pq[0]), g.nx, P.rdim), ej = get_delta(j1, nint_d(pq[1]), g.ny, P.rdim),
-          ek = get_delta(k1, nint_d(pq[2]), g.nz, P.rdim);
+      int ei = get_delta(i1, nint_idx(pq[0], g.nx), g.nx, P.rdim),
+          ej = get_delta(j1, nint_idx(pq[1], g.ny), g.ny, P.rdim),
+          ek = get_delta(k1, nint_idx(pq[2], g.nz), g.nz, P.rdim);
       if (ei * ei + ej * ej + ek * ek >= P.sphereMax) continue;
       LinkGeo G;
       link_geo(P, g, pq, i1, j1, k1, G);

@@ -114,7 +114,11 @@ class LBSim:
         check(self._L.lbx_sync(self._h), "lbx_sync")
 
     def set_schedule(self, fused):
-        check(self._L.lbx_set_schedule(self._h, 1 if fused else 0), "lbx_set_schedule")
+        """0 = two passes, 1 = first single-pass kernel, 2 = lean single-pass kernel (default)."""
+        check(self._L.lbx_set_schedule(self._h, int(fused)), "lbx_set_schedule")
+
+    def set_lean_shape(self, shape, zlen=0):
+        check(self._L.lbx_set_lean_shape(self._h, int(shape), int(zlen)), "lbx_set_lean_shape")
 
     def time_steps(self, n, kernel_timing=True):
         """(total_ms, kernel_ms, kernel_launches) of n steps, CUDA events on the context stream."""
