@@ -94,7 +94,12 @@ typedef struct lbx_params {
   float hz_k, hz_rmin, hz_rcap;             /* Hertz (dimensions_m.CUF:77-80) */
   int32_t lubrication;                      /* llubrication (dimensions_m.CUF:81) */
   float lubric_k, lubric_rmin, lubric_rcap; /* dimensions_m.CUF:82-84 */
-  int32_t reserved[8];
+  int32_t kinematic;      /* 1: spheres keep their position and velocity (force probes) */
+  int32_t closure;        /* 1: learned pair closure with analytic fallback (lbx_closure_*) */
+  float closure_gap_min;  /* training envelope of the closure: gap / R in [min, max] */
+  float closure_gap_max;
+  float closure_vmax;     /* and |relative velocity| components <= vmax */
+  int32_t reserved[3];
 } lbx_params;
 
 /* Fill the reference defaults for an nx*ny*nz periodic box: CG model, FP32
@@ -165,6 +170,35 @@ int lbx_status(void* ctx, int32_t* code, int32_t* step, int64_t* where);
 const char* lbx_error_string(int code);
 /* Steps taken so far (the reference's `step`). */
 int lbx_get_step(void* ctx, int64_t* step);
+
+/* ---- learned pair closure (no counterpart in the reference) ------------ */
+/* MLP 11 -> 64 -> 64 -> 64 -> 12 (SiLU, FP32) correcting the pair force and
+ * torque of near-contact spheres; the reference's analytic lubrication
+ * (addHertzian, kernels_fluid_PART.CUF:1463-1501) is the fallback outside
+ * the training envelope.  The weights travel as one flat blob of
+ * LBX_CLOSURE_NWEIGHTS floats: W0[64][11] b0 W1[64][64] b1 W2[64][64] b2
+ * W3[12][64] b3, then the input mean[11], std[11] and output mean[12],
+ * std[12] used to standardise. */
+#define LBX_CLOSURE_NWEIGHTS 9914
+/* Glorot-uniform initial weights, identity standardisation. */
+int lbx_closure_init(float* weights, int32_t seed);
+/* Train on the GPU (one fused forward/backward/Adam kernel for all epochs):
+ * X (n,11), T (n,12) raw features and targets, standardised with the
+ * statistics in the blob; weights updated in place; loss[epochs] optional. */
+int lbx_closure_train(float* weights, const float* X, const float* T, int32_t n, int32_t epochs, float lr,
+                      int32_t seed, float* loss);
+/* Gradient of the mean-squared error over the first min(n,128) standardised
+ * samples (no update), for checking the backward pass. */
+int lbx_closure_grad(const float* weights, const float* Xs, const float* Ts, int32_t n, float* grad);
+/* Batched inference on raw features: Y (n,12). */
+int lbx_closure_infer(const float* weights, const float* X, int32_t n, float* Y);
+/* Attach trained weights to a particle context; with p->closure = 1 each
+ * step then corrects every close pair inside the envelope (closure_gap_min
+ * <= gap/R <= closure_gap_max, relative velocity and angular velocity
+ * components <= closure_vmax) and applies the analytic lubrication
+ * (p->lubrication) to the pairs outside it.  Without weights every pair
+ * takes the fallback. */
+int lbx_closure_set(void* ctx, const float* weights);
 
 /* ---- measurement ------------------------------------------------------- */
 /* Colour-gradient schedule: 2 = lean single-pass kernel (default), 1 = the

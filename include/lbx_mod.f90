@@ -35,7 +35,9 @@ module lbx_mod
     real(c_float) :: hz_k, hz_rmin, hz_rcap
     integer(c_int32_t) :: lubrication
     real(c_float) :: lubric_k, lubric_rmin, lubric_rcap
-    integer(c_int32_t) :: reserved(8)
+    integer(c_int32_t) :: kinematic, closure
+    real(c_float) :: closure_gap_min, closure_gap_max, closure_vmax
+    integer(c_int32_t) :: reserved(3)
   end type lbx_params
 
   interface

@@ -26,7 +26,9 @@ class LbxParams(C.Structure):
         ("hz_k", C.c_float), ("hz_rmin", C.c_float), ("hz_rcap", C.c_float),
         ("lubrication", C.c_int32),
         ("lubric_k", C.c_float), ("lubric_rmin", C.c_float), ("lubric_rcap", C.c_float),
-        ("reserved", C.c_int32 * 8),
+        ("kinematic", C.c_int32), ("closure", C.c_int32),
+        ("closure_gap_min", C.c_float), ("closure_gap_max", C.c_float), ("closure_vmax", C.c_float),
+        ("reserved", C.c_int32 * 3),
     ]
 
 
@@ -65,6 +67,11 @@ SIGNATURES = {
     "lbx_get_sums": (C.c_int, [_P, _D, _D]),
     "lbx_set_particles": (C.c_int, [_P, C.c_int32, _D, _D, _D, _D]),
     "lbx_get_particles": (C.c_int, [_P, _D, _D, _D, _D, _D, _D]),
+    "lbx_closure_init": (C.c_int, [_F, C.c_int32]),
+    "lbx_closure_train": (C.c_int, [_F, _F, _F, C.c_int32, C.c_int32, C.c_float, C.c_int32, _F]),
+    "lbx_closure_grad": (C.c_int, [_F, _F, _F, C.c_int32, _F]),
+    "lbx_closure_infer": (C.c_int, [_F, _F, C.c_int32, _F]),
+    "lbx_closure_set": (C.c_int, [_P, _F]),
     "lbx_sync": (C.c_int, [_P]),
     "lbx_status": (C.c_int, [_P, _I32, _I32, _I64]),
     "lbx_error_string": (C.c_char_p, [C.c_int]),

@@ -1,0 +1,191 @@
+"""Learned pair closure: data generation, training and use (host side).
+
+The closure corrects the force and torque of near-contact sphere pairs that
+the lattice resolves poorly (small radius).  Its training data come from the
+method itself: the same two-sphere configuration is run with prescribed
+sphere motion (``kinematic`` contexts) once well resolved (radius R_hi in an
+L_hi^3 box) and once at the deployment radius R_lo (box scaled by
+R_lo/R_hi); the target is the resolved force scaled to R_lo (forces of
+Stokes and lubrication flows scale as mu R U at fixed gap/R, torques as
+mu R^2 U) minus the under-resolved one, in the pair frame.  Training and
+inference run in the library's own kernels (lbx_closure_train /
+lbx_closure_infer); the analytic lubrication of the reference stays the
+fallback outside the training envelope and the judge of the gain.
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import capi
+from .sim import LBSim, make_params
+
+DIN, H, DOUT = 11, 64, 12
+NW = 9914
+NPARAM = 9868
+XMU, XSD, YMU, YSD = NPARAM, NPARAM + DIN, NPARAM + 2 * DIN, NPARAM + 2 * DIN + DOUT
+
+
+def _fp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+def pair_frame(n):
+    """(t1, t2) completing n: t1 = unit(n x e_k), e_k the axis least aligned with n."""
+    n = np.asarray(n, np.float64)
+    k = int(np.argmin(np.abs(n)))
+    e = np.zeros(3)
+    e[k] = 1.0
+    t1 = np.cross(n, e)
+    t1 /= np.linalg.norm(t1)
+    return t1, np.cross(n, t1)
+
+
+def features(xi, xj, vi, vj, oi, oj, R, box):
+    """The 11 closure inputs of pair (i, j) (lab angular velocities)."""
+    d = np.asarray(xj, np.float64) - np.asarray(xi, np.float64)
+    box = np.asarray(box, np.float64)
+    d = d - box * np.round(d / box)
+    r = np.linalg.norm(d)
+    n = d / r
+    t1, t2 = pair_frame(n)
+    F = np.stack([n, t1, t2])
+    dv = F @ (np.asarray(vj) - np.asarray(vi))
+    return np.concatenate([[(r - 2 * R) / R], dv, F @ np.asarray(oi), F @ np.asarray(oj), [R]]), F
+
+
+def sample_configs(n, seed=0, gap_range=(0.05, 4.0), vmax=1e-3):
+    """gap/R log-uniform, pair-frame relative velocity and both angular velocities uniform in +-vmax."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    gaps = np.exp(rng.uniform(np.log(gap_range[0]), np.log(gap_range[1]), n))
+    dirs = rng.normal(size=(n, 3))
+    dirs /= np.linalg.norm(dirs, axis=1, keepdims=True)
+    dv = rng.uniform(-vmax, vmax, (n, 3))
+    oi = rng.uniform(-vmax, vmax, (n, 3))
+    oj = rng.uniform(-vmax, vmax, (n, 3))
+    return [dict(gap=g, n=d, dv=a, oi=b, oj=c) for g, d, a, b, c in zip(gaps, dirs, dv, oi, oj)]
+
+
+def run_pair(cfg, R, L, steps, average=0.25, storage="f32", lubrication=False, sim_cache=None):
+    """Forces / torques on both spheres of a prescribed-motion two-sphere run.
+
+    Spheres of radius R at distance 2R + gap*R along cfg['n'] around the box
+    centre, velocities -dv/2 and +dv/2 (pair frame -> lab), angular
+    velocities oi, oj (pair frame -> lab, body frame = lab, identity
+    orientation).  Returns (F_i, T_i, F_j, T_j) in the lab frame, averaged
+    over the last `average` fraction of the steps.
+    """
+    n = np.asarray(cfg["n"], np.float64)
+    t1, t2 = pair_frame(n)
+    Fm = np.stack([n, t1, t2])
+    dv = Fm.T @ cfg["dv"]
+    oi = Fm.T @ cfg["oi"]
+    oj = Fm.T @ cfg["oj"]
+    c = np.full(3, (L + 1) / 2.0)
+    half = R + 0.5 * cfg["gap"] * R
+    x = np.stack([c - half * n, c + half * n])
+    v = np.stack([-0.5 * dv, 0.5 * dv])
+    om = np.stack([oi, oj])
+    key = (R, L, storage, lubrication)
+    sim = sim_cache.get(key) if sim_cache is not None else None
+    if sim is None:
+        p = make_params(L, model="cg", storage=storage, max_particles=2, radius=float(R), kinematic=1,
+                        lrotate=1, wetting="neutral", max_vel=1.0,
+                        hz_rmin=float(2 * R - 0.5), hz_rcap=float(2 * R - 2.0),
+                        lubrication=1 if lubrication else 0, lubric_k=1.0 / 6.0, lubric_rmin=1.0,
+                        lubric_rcap=float(0.05 * R))
+        sim = LBSim(p)
+        if sim_cache is not None:
+            sim_cache[key] = sim
+    one = np.ones((L, L, L), np.float32)
+    sim.set_fields(one, np.zeros_like(one))
+    sim.set_particles(x, v, om, None)
+    nav = max(1, int(round(steps * average)))
+    sim.step(steps - nav)
+    acc = np.zeros((4, 3))
+    for _ in range(nav):
+        sim.step(1)
+        d = sim.get_particles()
+        acc += np.stack([d["force"][0], d["torque"][0], d["force"][1], d["torque"][1]])
+    return acc / nav, x, v, om
+
+
+def generate(n_samples, R_hi=12, L_hi=96, R_lo=3, steps_hi=300, seed=0, progress=None):
+    """(X, T, info): features at R_lo and targets (resolved - under-resolved, pair frame)."""
+    s = R_lo / R_hi
+    L_lo = int(round(L_hi * s))
+    steps_lo = max(8, int(round(steps_hi * s * s)))
+    cfgs = sample_configs(n_samples, seed)
+    X = np.zeros((n_samples, DIN))
+    T = np.zeros((n_samples, DOUT))
+    base = np.zeros((n_samples, DOUT))
+    cache = {}
+    for k, cfg in enumerate(cfgs):
+        hi, *_ = run_pair(cfg, R_hi, L_hi, steps_hi, sim_cache=cache)
+        lo, x, v, om = run_pair(cfg, R_lo, L_lo, steps_lo, sim_cache=cache)
+        feat, Fm = features(x[0], x[1], v[0], v[1], om[0], om[1], R_lo, (L_lo,) * 3)
+        scale = np.array([s, s * s, s, s * s])[:, None]
+        target = hi * scale - lo
+        X[k] = feat
+        T[k] = (target @ Fm.T).ravel()          # pair frame
+        base[k] = (lo @ Fm.T).ravel()
+        if progress and (k + 1) % progress == 0:
+            print(f"closure data {k + 1}/{n_samples}", flush=True)
+    for sim in cache.values():
+        sim.close()
+    return X, T, dict(base=base, cfgs=cfgs, steps_hi=steps_hi, steps_lo=steps_lo, L_lo=L_lo)
+
+
+def init_weights(X, T, seed=0):
+    w = np.zeros(NW, np.float32)
+    capi.check(capi.lib().lbx_closure_init(_fp(w), int(seed)), "lbx_closure_init")
+    w[XMU:XMU + DIN] = X.mean(0)
+    w[XSD:XSD + DIN] = np.maximum(X.std(0), 1e-12)
+    w[YMU:YMU + DOUT] = T.mean(0)
+    w[YSD:YSD + DOUT] = np.maximum(T.std(0), 1e-12)
+    return w
+
+
+def train(X, T, epochs=500, lr=2e-3, seed=0, w=None):
+    X = np.ascontiguousarray(X, np.float32)
+    T = np.ascontiguousarray(T, np.float32)
+    if w is None:
+        w = init_weights(X, T, seed)
+    loss = np.zeros(epochs, np.float32)
+    capi.check(capi.lib().lbx_closure_train(_fp(w), _fp(X), _fp(T), X.shape[0], int(epochs), float(lr), int(seed),
+                                            _fp(loss)), "lbx_closure_train")
+    return w, loss
+
+
+def infer(w, X):
+    X = np.ascontiguousarray(X, np.float32)
+    Y = np.zeros((X.shape[0], DOUT), np.float32)
+    capi.check(capi.lib().lbx_closure_infer(_fp(np.ascontiguousarray(w, np.float32)), _fp(X), X.shape[0], _fp(Y)),
+               "lbx_closure_infer")
+    return Y
+
+
+def grad(w, Xs, Ts):
+    Xs = np.ascontiguousarray(Xs, np.float32)
+    Ts = np.ascontiguousarray(Ts, np.float32)
+    g = np.zeros(NPARAM, np.float32)
+    capi.check(capi.lib().lbx_closure_grad(_fp(np.ascontiguousarray(w, np.float32)), _fp(Xs), _fp(Ts), Xs.shape[0],
+                                           _fp(g)), "lbx_closure_grad")
+    return g
+
+
+def analytic_lubrication(X, R, mu=1.0 / 6.0, rcut_gap=1.0, rcap_gap=None):
+    """The reference's normal squeeze force (addHertzian's lubrication branch) in the pair frame.
+
+    F_j = -F_i = lubfactor n (n.(v_i - v_j)) (1/h - 1), h = max(gap, rcap) (lattice units),
+    applied for gap <= rcut_gap; lubfactor = mu 6 pi R^4 / (2R)^2.
+    """
+    rcap_gap = 0.05 * R if rcap_gap is None else rcap_gap
+    out = np.zeros((X.shape[0], DOUT))
+    h = X[:, 0] * R
+    lubfactor = mu * 6 * np.pi * R ** 4 / (2 * R) ** 2
+    dvn = X[:, 1]                      # (v_j - v_i).n
+    hh = np.maximum(h, rcap_gap)
+    f = np.where(h <= rcut_gap, lubfactor * (-dvn) * (1.0 / hh - 1.0), 0.0)
+    out[:, 0] = -f
+    out[:, 6] = f
+    return out

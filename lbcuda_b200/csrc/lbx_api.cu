@@ -22,6 +22,7 @@ void particles_destroy(Ctx& c);
 int particles_set(Ctx& c, int n, const double* x, const double* v, const double* om, const double* q);
 int particles_get(Ctx& c, double* x, double* v, double* om, double* q, double* f, double* t);
 int particles_step(Ctx& c);
+int particles_set_closure(Ctx& c, const float* w);
 int particles_flags_slot(const Ctx& c);
 int particles_active(const Ctx& c);
 }  // namespace lbx
@@ -101,6 +102,11 @@ void lbx_default_params(lbx_params* p, int32_t nx, int32_t ny, int32_t nz) {
   p->lubric_k = 10.0f;
   p->lubric_rmin = 10.0f;
   p->lubric_rcap = 9.0f;
+  p->kinematic = 0;
+  p->closure = 0;
+  p->closure_gap_min = 0.05f;
+  p->closure_gap_max = 4.0f;
+  p->closure_vmax = 1.0e-3f;
 }
 
 int lbx_create(const lbx_params* p, void** out) {
@@ -302,6 +308,12 @@ int lbx_get_particles(void* ctx, double* xyz, double* vel, double* omega, double
   int rc = lbx::particles_get(*c, xyz, vel, omega, q, force, torque);
   if (!rc) rc = sync_status(*c);
   return rc;
+}
+
+int lbx_closure_set(void* ctx, const float* weights) {
+  Ctx* c = as_ctx(ctx);
+  if (!c || !weights) return LBX_ERR_ARG;
+  return lbx::particles_set_closure(*c, weights);
 }
 
 int lbx_sync(void* ctx) {

@@ -1,0 +1,351 @@
+// lbx_closure.cu — learned lubrication / sub-resolution closure for sphere
+// pairs (no counterpart in the reference; it attaches where the reference's
+// analytic lubrication branch sits, addHertzian, kernels_fluid_PART.CUF:
+// 1463-1501, which stays the fallback and the judge).
+//
+// Network: 11 -> 64 -> 64 -> 64 -> 12, SiLU, FP32.  Inputs (pair frame of
+// spheres i < j, n = (x_j - x_i)/|x_j - x_i|, t1 = unit(n x e_k) with e_k the
+// axis least aligned with n, t2 = n x t1):
+//   gap/R, (v_j - v_i).{n,t1,t2}, omega_i.{n,t1,t2}, omega_j.{n,t1,t2}, R
+// (angular velocities in the lab frame).  Outputs: force and torque
+// corrections on i and on j in the same frame.  Inputs and outputs are
+// standardised with the mean / std stored after the weights.
+//
+// Kernels
+//   k_mlp_train  one CTA runs every epoch of minibatch Adam on the whole data
+//                set: forward, backward and update fused, activations in
+//                shared memory, gradients reduced in a fixed order.
+//   k_mlp_infer  one warp per sample (pair), weights in shared memory.
+//   k_pair_nbrs / k_closure_pairs / k_closure_accum: per step, the close
+//                pairs of each sphere (ascending index), the closure (or the
+//                analytic lubrication when the pair leaves the training
+//                envelope) and a fixed-order accumulation per sphere.
+#include "lbx_device.cuh"
+#include "lbx_closure.h"
+
+#include <cmath>
+#include <vector>
+
+namespace lbx {
+
+// ---------------------------------------------------------------------------
+// training: one CTA of 256 threads, minibatch B
+// ---------------------------------------------------------------------------
+constexpr int TB = 64;    // minibatch (shared-memory bound)
+constexpr int TT = 256;   // threads
+
+struct TrainArgs {
+  const float* X;   // n x DIN, standardised
+  const float* T;   // n x DOUT, standardised
+  int n;
+  float* w;         // NPARAM (updated)
+  float* m;         // Adam moments
+  float* v;
+  float* loss;      // per epoch (may be null)
+  float* grad_out;  // grad-only mode: NPARAM gradient of the first minibatch
+  int epochs;
+  float lr, beta1, beta2, eps;
+  unsigned seed;
+};
+
+// Z[b][o] = sum_k A[b][k] W[o][k] + bias[o]   (A: TB x K in smem, W: O x K in smem)
+__device__ void dense_fwd(const float* A, int K, const float* W, const float* bias, int O, float* Z) {
+  for (int idx = threadIdx.x; idx < TB * O; idx += TT) {
+    int b = idx / O, o = idx % O;
+    const float* a = A + b * K;
+    const float* wr = W + o * K;
+    float s = bias[o];
+    for (int k = 0; k < K; ++k) s = fmaf(a[k], wr[k], s);
+    Z[idx] = s;
+  }
+}
+
+__global__ void __launch_bounds__(TT) k_mlp_train(TrainArgs a) {
+  using L = MlpLayout;
+  extern __shared__ float sm[];
+  float* W = sm;                       // NPARAM
+  float* X0 = W + L::NPARAM;           // TB x DIN
+  float* Z1 = X0 + TB * DIN;           // TB x H (pre-activations)
+  float* Z2 = Z1 + TB * H;
+  float* Z3 = Z2 + TB * H;
+  float* Y = Z3 + TB * H;              // TB x DOUT
+  float* D = Y + TB * DOUT;            // TB x H   (gradient w.r.t. the current layer's pre-activation)
+  float* E = D + TB * H;               // TB x H   (scratch: activations / next gradient)
+  float* G = E + TB * H;               // NPARAM gradient of the minibatch
+  __shared__ float red[TT];
+  __shared__ int idxs[TB];
+  for (int i = threadIdx.x; i < L::NPARAM; i += TT) W[i] = a.w[i];
+  __syncthreads();
+  const int nb = (a.n + TB - 1) / TB;
+  const bool grad_only = a.grad_out != nullptr;
+  int t_adam = 0;
+  for (int ep = 0; ep < (grad_only ? 1 : a.epochs); ++ep) {
+    // epoch order: i -> (i * stride + off) mod n with stride coprime to n
+    unsigned h = a.seed * 2654435761u + unsigned(ep) * 40503u + 12345u;
+    int off = int(h % unsigned(a.n));
+    int stride = 1 + int((h >> 8) % unsigned(a.n));
+    while (true) {  // gcd(stride, n) == 1
+      int x = stride, y = a.n;
+      while (y) { int t = x % y; x = y; y = t; }
+      if (x == 1) break;
+      stride = stride % a.n + 1;
+    }
+    float ep_loss = 0.f;
+    for (int bi = 0; bi < (grad_only ? 1 : nb); ++bi) {
+      const int cnt = min(TB, a.n - bi * TB);
+      for (int b = threadIdx.x; b < TB; b += TT)
+        idxs[b] = grad_only ? min(b, a.n - 1) : int((long long)(bi * TB + min(b, cnt - 1)) * stride % a.n + off) % a.n;
+      __syncthreads();
+      for (int i = threadIdx.x; i < TB * DIN; i += TT) X0[i] = a.X[size_t(idxs[i / DIN]) * DIN + i % DIN];
+      __syncthreads();
+      // forward
+      dense_fwd(X0, DIN, W + L::W0, W + L::B0, H, Z1);
+      __syncthreads();
+      for (int i = threadIdx.x; i < TB * H; i += TT) E[i] = silu(Z1[i]);
+      __syncthreads();
+      dense_fwd(E, H, W + L::W1, W + L::B1, H, Z2);
+      __syncthreads();
+      for (int i = threadIdx.x; i < TB * H; i += TT) E[i] = silu(Z2[i]);
+      __syncthreads();
+      dense_fwd(E, H, W + L::W2, W + L::B2, H, Z3);
+      __syncthreads();
+      for (int i = threadIdx.x; i < TB * H; i += TT) E[i] = silu(Z3[i]);
+      __syncthreads();
+      dense_fwd(E, H, W + L::W3, W + L::B3, DOUT, Y);
+      __syncthreads();
+      // loss = mean over valid samples and outputs of (y - t)^2; dY in D (TB x DOUT)
+      float part = 0.f;
+      const float scale = 2.0f / float(cnt * DOUT);
+      for (int i = threadIdx.x; i < TB * DOUT; i += TT) {
+        int b = i / DOUT;
+        float d = (b < cnt) ? Y[i] - a.T[size_t(idxs[b]) * DOUT + i % DOUT] : 0.f;
+        part += d * d;
+        D[i] = d * scale;
+      }
+      red[threadIdx.x] = part;
+      __syncthreads();
+      for (int s = TT / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
+        __syncthreads();
+      }
+      if (threadIdx.x == 0) ep_loss += red[0];
+      // layer 3: G[W3] = dY^T A3 (A3 = silu(Z3) is in E), G[B3] = sum dY
+      for (int idx = threadIdx.x; idx < DOUT * H; idx += TT) {
+        int o = idx / H, k = idx % H;
+        float s = 0.f;
+        for (int b = 0; b < TB; ++b) s = fmaf(D[b * DOUT + o], E[b * H + k], s);
+        G[L::W3 + idx] = s;
+      }
+      for (int o = threadIdx.x; o < DOUT; o += TT) {
+        float s = 0.f;
+        for (int b = 0; b < TB; ++b) s += D[b * DOUT + o];
+        G[L::B3 + o] = s;
+      }
+      __syncthreads();
+      // dA3 = dY W3 -> dZ3 = dA3 * silu'(Z3), into E (A3 no longer needed)
+      for (int idx = threadIdx.x; idx < TB * H; idx += TT) {
+        int b = idx / H, k = idx % H;
+        float s = 0.f;
+        for (int o = 0; o < DOUT; ++o) s = fmaf(D[b * DOUT + o], W[L::W3 + o * H + k], s);
+        E[idx] = s * dsilu(Z3[idx]);
+      }
+      __syncthreads();
+      // hidden layers 2 and 1 (and the input layer): dZ in E, A_prev = silu(Z_prev)
+      const float* Zs[3] = {Z2, Z1, nullptr};
+      const int Wo[3] = {L::W2, L::W1, L::W0}, Bo[3] = {L::B2, L::B1, L::B0};
+      for (int layer = 0; layer < 3; ++layer) {
+        const float* Zp = Zs[layer];
+        const int K = Zp ? H : DIN;
+        for (int idx = threadIdx.x; idx < H * K; idx += TT) {
+          int o = idx / K, k = idx % K;
+          float s = 0.f;
+          if (Zp)
+            for (int b = 0; b < TB; ++b) s = fmaf(E[b * H + o], silu(Zp[b * H + k]), s);
+          else
+            for (int b = 0; b < TB; ++b) s = fmaf(E[b * H + o], X0[b * DIN + k], s);
+          G[Wo[layer] + idx] = s;
+        }
+        for (int o = threadIdx.x; o < H; o += TT) {
+          float s = 0.f;
+          for (int b = 0; b < TB; ++b) s += E[b * H + o];
+          G[Bo[layer] + o] = s;
+        }
+        __syncthreads();
+        if (Zp) {
+          // dZ_prev = (dZ W) * silu'(Z_prev) into D, then swap into E
+          for (int idx = threadIdx.x; idx < TB * H; idx += TT) {
+            int b = idx / H, k = idx % H;
+            float s = 0.f;
+            for (int o = 0; o < H; ++o) s = fmaf(E[b * H + o], W[Wo[layer] + o * H + k], s);
+            D[idx] = s * dsilu(Zp[idx]);
+          }
+          __syncthreads();
+          for (int idx = threadIdx.x; idx < TB * H; idx += TT) E[idx] = D[idx];
+          __syncthreads();
+        }
+      }
+      if (grad_only) {
+        for (int i = threadIdx.x; i < L::NPARAM; i += TT) a.grad_out[i] = G[i];
+        __syncthreads();
+        break;
+      }
+      // Adam
+      ++t_adam;
+      const float c1 = 1.0f - powf(a.beta1, float(t_adam)), c2 = 1.0f - powf(a.beta2, float(t_adam));
+      for (int i = threadIdx.x; i < L::NPARAM; i += TT) {
+        float gi = G[i];
+        float mi = a.beta1 * a.m[i] + (1.0f - a.beta1) * gi;
+        float vi = a.beta2 * a.v[i] + (1.0f - a.beta2) * gi * gi;
+        a.m[i] = mi;
+        a.v[i] = vi;
+        W[i] -= a.lr * (mi / c1) / (sqrtf(vi / c2) + a.eps);
+      }
+      __syncthreads();
+    }
+    if (threadIdx.x == 0 && a.loss && !grad_only) a.loss[ep] = ep_loss / float(a.n * DOUT);
+  }
+  if (!grad_only)
+    for (int i = threadIdx.x; i < L::NPARAM; i += TT) a.w[i] = W[i];
+}
+
+// ---------------------------------------------------------------------------
+// inference: one warp per sample, weights (and normalisation) in shared memory
+// ---------------------------------------------------------------------------
+__global__ void k_mlp_infer(const float* __restrict__ Wg, const float* __restrict__ X, int n, float* Y) {
+  extern __shared__ float sm[];
+  float* W = sm;
+  float* bufs = W + MlpLayout::TOTAL;
+  load_infer_weights(Wg, W);
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  float* buf = bufs + warp * 2 * H;
+  for (int s = blockIdx.x * nw + warp; s < n; s += gridDim.x * nw) {
+    float x[DIN], y[DOUT];
+    for (int k = 0; k < DIN; ++k) x[k] = X[size_t(s) * DIN + k];
+    mlp_warp(W, x, y, buf);
+    if ((threadIdx.x & 31) == 0)
+      for (int o = 0; o < DOUT; ++o) Y[size_t(s) * DOUT + o] = y[o];
+  }
+}
+
+}  // namespace lbx
+
+// ---------------------------------------------------------------------------
+// host entry points (C ABI, include/lbx.h)
+// ---------------------------------------------------------------------------
+namespace {
+struct Dev {
+  void* p = nullptr;
+  explicit Dev(size_t b) {
+    if (b && cudaMalloc(&p, b) != cudaSuccess) p = nullptr;
+  }
+  ~Dev() {
+    if (p) cudaFree(p);
+  }
+};
+size_t train_smem() {
+  using L = lbx::MlpLayout;
+  return sizeof(float) * (2 * size_t(L::NPARAM) + lbx::TB * lbx::DIN + 5 * lbx::TB * lbx::H + lbx::TB * lbx::DOUT);
+}
+int rc_of(cudaError_t e) { return e == cudaSuccess ? 0 : LBX_ERR_CUDA; }
+}  // namespace
+
+extern "C" {
+
+int lbx_closure_init(float* weights, int32_t seed) {
+  using L = lbx::MlpLayout;
+  if (!weights) return LBX_ERR_ARG;
+  // Glorot-uniform weights, zero biases, identity standardisation
+  unsigned long long s = 0x9E3779B97F4A7C15ull ^ (unsigned long long)(seed);
+  auto rnd = [&]() {
+    s ^= s << 13; s ^= s >> 7; s ^= s << 17;
+    return double(s >> 11) * (1.0 / 9007199254740992.0);
+  };
+  auto fill = [&](int off, int fan_out, int fan_in) {
+    double lim = std::sqrt(6.0 / double(fan_in + fan_out));
+    for (int i = 0; i < fan_out * fan_in; ++i) weights[off + i] = float((2.0 * rnd() - 1.0) * lim);
+  };
+  for (int i = 0; i < L::TOTAL; ++i) weights[i] = 0.f;
+  fill(L::W0, lbx::H, lbx::DIN);
+  fill(L::W1, lbx::H, lbx::H);
+  fill(L::W2, lbx::H, lbx::H);
+  fill(L::W3, lbx::DOUT, lbx::H);
+  for (int i = 0; i < lbx::DIN; ++i) weights[L::XSD + i] = 1.f;
+  for (int i = 0; i < lbx::DOUT; ++i) weights[L::YSD + i] = 1.f;
+  return 0;
+}
+
+int lbx_closure_train(float* weights, const float* X, const float* T, int32_t n, int32_t epochs, float lr,
+                      int32_t seed, float* loss) {
+  using L = lbx::MlpLayout;
+  if (!weights || !X || !T || n < 1 || epochs < 1) return LBX_ERR_ARG;
+  const size_t nx = size_t(n) * lbx::DIN, nt = size_t(n) * lbx::DOUT;
+  Dev dX(nx * 4), dT(nt * 4), dW(size_t(L::TOTAL) * 4), dM(size_t(L::NPARAM) * 4), dV(size_t(L::NPARAM) * 4),
+      dL(size_t(epochs) * 4);
+  if (!dX.p || !dT.p || !dW.p || !dM.p || !dV.p || !dL.p) return LBX_ERR_ALLOC;
+  // standardise with the statistics stored in the blob
+  std::vector<float> Xs(nx), Ts(nt);
+  for (size_t i = 0; i < nx; ++i) Xs[i] = (X[i] - weights[L::XMU + i % lbx::DIN]) / weights[L::XSD + i % lbx::DIN];
+  for (size_t i = 0; i < nt; ++i) Ts[i] = (T[i] - weights[L::YMU + i % lbx::DOUT]) / weights[L::YSD + i % lbx::DOUT];
+  int rc = rc_of(cudaMemcpy(dX.p, Xs.data(), nx * 4, cudaMemcpyHostToDevice));
+  if (!rc) rc = rc_of(cudaMemcpy(dT.p, Ts.data(), nt * 4, cudaMemcpyHostToDevice));
+  if (!rc) rc = rc_of(cudaMemcpy(dW.p, weights, size_t(L::TOTAL) * 4, cudaMemcpyHostToDevice));
+  if (!rc) rc = rc_of(cudaMemset(dM.p, 0, size_t(L::NPARAM) * 4));
+  if (!rc) rc = rc_of(cudaMemset(dV.p, 0, size_t(L::NPARAM) * 4));
+  if (rc) return rc;
+  lbx::TrainArgs a{(const float*)dX.p, (const float*)dT.p, n, (float*)dW.p, (float*)dM.p, (float*)dV.p,
+                   (float*)dL.p, nullptr, epochs, lr, 0.9f, 0.999f, 1e-8f, unsigned(seed)};
+  size_t smem = train_smem();
+  rc = rc_of(cudaFuncSetAttribute(lbx::k_mlp_train, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+  if (rc) return rc;
+  lbx::k_mlp_train<<<1, lbx::TT, smem>>>(a);
+  rc = rc_of(cudaGetLastError());
+  if (!rc) rc = rc_of(cudaDeviceSynchronize());
+  if (!rc) rc = rc_of(cudaMemcpy(weights, dW.p, size_t(L::NPARAM) * 4, cudaMemcpyDeviceToHost));
+  if (!rc && loss) rc = rc_of(cudaMemcpy(loss, dL.p, size_t(epochs) * 4, cudaMemcpyDeviceToHost));
+  return rc;
+}
+
+int lbx_closure_grad(const float* weights, const float* Xs, const float* Ts, int32_t n, float* grad) {
+  using L = lbx::MlpLayout;
+  if (!weights || !Xs || !Ts || !grad || n < 1) return LBX_ERR_ARG;
+  const size_t nx = size_t(n) * lbx::DIN, nt = size_t(n) * lbx::DOUT;
+  Dev dX(nx * 4), dT(nt * 4), dW(size_t(L::TOTAL) * 4), dG(size_t(L::NPARAM) * 4);
+  if (!dX.p || !dT.p || !dW.p || !dG.p) return LBX_ERR_ALLOC;
+  int rc = rc_of(cudaMemcpy(dX.p, Xs, nx * 4, cudaMemcpyHostToDevice));
+  if (!rc) rc = rc_of(cudaMemcpy(dT.p, Ts, nt * 4, cudaMemcpyHostToDevice));
+  if (!rc) rc = rc_of(cudaMemcpy(dW.p, weights, size_t(L::TOTAL) * 4, cudaMemcpyHostToDevice));
+  if (rc) return rc;
+  lbx::TrainArgs a{(const float*)dX.p, (const float*)dT.p, n, (float*)dW.p, nullptr, nullptr, nullptr,
+                   (float*)dG.p, 1, 0.f, 0.9f, 0.999f, 1e-8f, 0u};
+  size_t smem = train_smem();
+  rc = rc_of(cudaFuncSetAttribute(lbx::k_mlp_train, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+  if (rc) return rc;
+  lbx::k_mlp_train<<<1, lbx::TT, smem>>>(a);
+  rc = rc_of(cudaGetLastError());
+  if (!rc) rc = rc_of(cudaDeviceSynchronize());
+  if (!rc) rc = rc_of(cudaMemcpy(grad, dG.p, size_t(L::NPARAM) * 4, cudaMemcpyDeviceToHost));
+  return rc;
+}
+
+int lbx_closure_infer(const float* weights, const float* X, int32_t n, float* Y) {
+  using L = lbx::MlpLayout;
+  if (!weights || !X || !Y || n < 1) return LBX_ERR_ARG;
+  Dev dX(size_t(n) * lbx::DIN * 4), dY(size_t(n) * lbx::DOUT * 4), dW(size_t(L::TOTAL) * 4);
+  if (!dX.p || !dY.p || !dW.p) return LBX_ERR_ALLOC;
+  int rc = rc_of(cudaMemcpy(dX.p, X, size_t(n) * lbx::DIN * 4, cudaMemcpyHostToDevice));
+  if (!rc) rc = rc_of(cudaMemcpy(dW.p, weights, size_t(L::TOTAL) * 4, cudaMemcpyHostToDevice));
+  if (rc) return rc;
+  size_t smem = sizeof(float) * (size_t(L::TOTAL) + 8 * 2 * lbx::H);
+  rc = rc_of(cudaFuncSetAttribute(lbx::k_mlp_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+  if (rc) return rc;
+  int blocks = (n + 7) / 8;
+  if (blocks > 148 * 4) blocks = 148 * 4;
+  lbx::k_mlp_infer<<<blocks, 256, smem>>>((const float*)dW.p, (const float*)dX.p, n, (float*)dY.p);
+  rc = rc_of(cudaGetLastError());
+  if (!rc) rc = rc_of(cudaDeviceSynchronize());
+  if (!rc) rc = rc_of(cudaMemcpy(Y, dY.p, size_t(n) * lbx::DOUT * 4, cudaMemcpyDeviceToHost));
+  return rc;
+}
+
+}  // extern "C"

@@ -26,6 +26,7 @@
 // for the pull (a spheredead source keeps the stale population, as the push
 // of stream*_CG leaves it) and of the current step for the collision.
 #include "lbx_device.cuh"
+#include "lbx_closure.h"
 
 #include <cmath>
 #include <vector>
@@ -38,6 +39,7 @@ constexpr int AS = 15;   // accumulators: f_bb[3] t_bb[3] f_other[3] t_other[3] 
 constexpr int TILEX = 8, TILEY = 4, TILEZ = 4;  // reference tile (defines.h:14-22)
 constexpr int BINW = 8;                          // cell bins of the particle lists
 constexpr int BIN_CAP = 64;
+constexpr int NBCAP = 32;                        // close neighbours per sphere (closure)
 
 struct ParticleState {
   int np = 0;
@@ -55,6 +57,12 @@ struct ParticleState {
   int pcur = 0;
   int flags_last = 0;
   int active = 0;
+  // learned closure
+  float* wclosure = nullptr;  // LBX_CLOSURE_NWEIGHTS
+  int closure_ready = 0;
+  int* nbr = nullptr;         // np x NBCAP
+  int* nbr_cnt = nullptr;
+  float* corr = nullptr;      // np x NBCAP x 12
 };
 
 struct PDev {  // by-value kernel argument
@@ -69,6 +77,9 @@ struct PDev {  // by-value kernel argument
   double hz_k, hz_rmin, hz_rcap;
   int lub;
   double lub_k, lub_rmin, lub_rcap;
+  int kinematic;
+  int closure;
+  float cl_gmin, cl_gmax, cl_vmax;
 };
 
 // ---------------------------------------------------------------------------
@@ -709,7 +720,7 @@ __global__ void k_pairs(PDev P, const double* __restrict__ pos, double* acc, Geo
       f[1] += sgn * (ggg * ydf / rrr);
       f[2] += sgn * (ggg * zdf / rrr);
     }
-    if (P.lub && rrr <= rparcut) {
+    if (P.lub && !P.closure && rrr <= rparcut) {
       double ux = xdf / rrr, uy = ydf / rrr, uz = zdf / rrr;
       if (rrr <= rparcap) rrr = rparcap;
       double dotuv = ux * (pl[3] - ph[3]) + uy * (pl[4] - ph[4]) + uz * (pl[5] - ph[5]);
@@ -722,6 +733,141 @@ __global__ void k_pairs(PDev P, const double* __restrict__ pos, double* acc, Geo
   for (int d = 0; d < 3; ++d) {
     acc[size_t(i) * AS + 6 + d] += f[d];
     acc[size_t(i) * AS + 12 + d] += fl[d];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// learned closure in the step
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void min_image(const Geom& g, const double* pl, const double* ph, double d[3]) {
+  d[0] = ph[0] - pl[0];
+  d[1] = ph[1] - pl[1];
+  d[2] = ph[2] - pl[2];
+  d[0] = d[0] - double(g.nx * nint_d(d[0] / g.nx));
+  d[1] = d[1] - double(g.ny * nint_d(d[1] / g.ny));
+  d[2] = d[2] - double(g.nz * nint_d(d[2] / g.nz));
+}
+
+// close neighbours of each sphere in ascending index (gap below the cut)
+__global__ void k_pair_nbrs(PDev P, const double* __restrict__ pos, Geom g, double gap_cut, int* nbr, int* cnt,
+                            unsigned long long* err, int64_t step) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= P.np) return;
+  const double* pi = pos + size_t(i) * PS;
+  int c = 0;
+  for (int j = 0; j < P.np; ++j) {
+    if (j == i) continue;
+    double d[3];
+    min_image(g, pi, pos + size_t(j) * PS, d);
+    double r = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+    if (r - 2.0 * P.rdim < gap_cut) {
+      if (c < NBCAP) nbr[size_t(i) * NBCAP + c] = j;
+      else raise_error(err, LBX_DEV_LIST_OVERFLOW, step, i);
+      ++c;
+    }
+  }
+  cnt[i] = min(c, NBCAP);
+}
+
+// one warp per close pair (i < j): the network inside its training envelope,
+// the analytic squeeze force of addHertzian's lubrication branch outside it
+__global__ void k_closure_pairs(PDev P, const double* __restrict__ pos, Geom g, const float* __restrict__ Wg,
+                                int use_net, const int* __restrict__ nbr, const int* __restrict__ cnt, float* corr) {
+  extern __shared__ float sm[];
+  float* W = sm;
+  float* bufs = W + MlpLayout::TOTAL;
+  if (use_net) load_infer_weights(Wg, W);
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, nw = blockDim.x >> 5, lane = threadIdx.x & 31;
+  float* buf = bufs + warp * 2 * H;
+  const int ntask = P.np * NBCAP;
+  for (int t = blockIdx.x * nw + warp; t < ntask; t += gridDim.x * nw) {
+    const int i = t / NBCAP, k = t % NBCAP;
+    if (k >= cnt[i]) continue;
+    const int j = nbr[size_t(i) * NBCAP + k];
+    if (j < i) continue;
+    const double* pi = pos + size_t(i) * PS;
+    const double* pj = pos + size_t(j) * PS;
+    double d[3];
+    min_image(g, pi, pj, d);
+    const double r = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+    const double n[3] = {d[0] / r, d[1] / r, d[2] / r};
+    double t1[3], t2[3];
+    pair_frame(n, t1, t2);
+    const double dv[3] = {pj[3] - pi[3], pj[4] - pi[4], pj[5] - pi[5]};
+    double oi[3] = {0, 0, 0}, oj[3] = {0, 0, 0};
+    {
+      double bi[3] = {pi[6], pi[7], pi[8]}, bj[3] = {pj[6], pj[7], pj[8]};
+      to_lab(pi, bi, oi);
+      to_lab(pj, bj, oj);
+    }
+    auto proj = [&](const double v[3], double o[3]) {
+      o[0] = v[0] * n[0] + v[1] * n[1] + v[2] * n[2];
+      o[1] = v[0] * t1[0] + v[1] * t1[1] + v[2] * t1[2];
+      o[2] = v[0] * t2[0] + v[1] * t2[1] + v[2] * t2[2];
+    };
+    double fv[3], fi[3], fj[3];
+    proj(dv, fv);
+    proj(oi, fi);
+    proj(oj, fj);
+    const double gapR = (r - 2.0 * P.rdim) / P.rdim;
+    bool inside = use_net && gapR >= P.cl_gmin && gapR <= P.cl_gmax;
+    for (int c = 0; c < 3 && inside; ++c)
+      inside = fabs(fv[c]) <= P.cl_vmax && fabs(fi[c]) <= P.cl_vmax && fabs(fj[c]) <= P.cl_vmax;
+    float out[12];
+    for (int c = 0; c < 12; ++c) out[c] = 0.f;
+    if (inside) {
+      float x[DIN] = {float(gapR), float(fv[0]), float(fv[1]), float(fv[2]), float(fi[0]), float(fi[1]),
+                      float(fi[2]), float(fj[0]), float(fj[1]), float(fj[2]), float(P.rdim)};
+      float y[DOUT];
+      mlp_warp(W, x, y, buf);
+      for (int q = 0; q < 4; ++q)
+        for (int c = 0; c < 3; ++c)
+          out[3 * q + c] = float(y[3 * q] * n[c] + y[3 * q + 1] * t1[c] + y[3 * q + 2] * t2[c]);
+    } else if (P.lub) {
+      const double rpar = 2.0 * P.rdim, rparcut = rpar + P.lub_rmin, rparcap = rpar + P.lub_rcap;
+      if (r <= rparcut) {
+        const double lubfactor =
+            P.lub_k * 6.0 * 3.141592653589793238462643383279502884 * pow(P.rdim * P.rdim, 2.0) / (rpar * rpar);
+        double rr = r <= rparcap ? rparcap : r;
+        double dotuv = n[0] * (pi[3] - pj[3]) + n[1] * (pi[4] - pj[4]) + n[2] * (pi[5] - pj[5]);
+        double cc = lubfactor * dotuv * (1.0 / (rr - rpar) - 1.0);
+        for (int c = 0; c < 3; ++c) {
+          out[c] = float(-cc * n[c]);
+          out[6 + c] = float(cc * n[c]);
+        }
+      }
+    }
+    if (lane == 0)
+      for (int c = 0; c < 12; ++c) corr[(size_t(i) * NBCAP + k) * 12 + c] = out[c];
+  }
+}
+
+// per sphere, in ascending partner index: its share of every pair correction
+__global__ void k_closure_accum(PDev P, const int* __restrict__ nbr, const int* __restrict__ cnt,
+                                const float* __restrict__ corr, double* acc) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= P.np) return;
+  double F[3] = {0, 0, 0}, T[3] = {0, 0, 0};
+  for (int k = 0; k < cnt[i]; ++k) {
+    const int j = nbr[size_t(i) * NBCAP + k];
+    const float* cp;
+    if (j > i) {
+      cp = corr + (size_t(i) * NBCAP + k) * 12;
+    } else {
+      int kk = 0;
+      while (kk < cnt[j] && nbr[size_t(j) * NBCAP + kk] != i) ++kk;
+      if (kk >= cnt[j]) continue;
+      cp = corr + (size_t(j) * NBCAP + kk) * 12 + 6;
+    }
+    for (int c = 0; c < 3; ++c) {
+      F[c] += double(cp[c]);
+      T[c] += double(cp[3 + c]);
+    }
+  }
+  for (int c = 0; c < 3; ++c) {
+    acc[size_t(i) * AS + 12 + c] += F[c];
+    if (P.lrotate) acc[size_t(i) * AS + 9 + c] += T[c];
   }
 }
 
@@ -751,12 +897,12 @@ __global__ void k_integrate(PDev P, const double* __restrict__ pos_cur, double* 
     }
   // nve_lf
   const double rmass = P.rmass;
-  if (fabs(fc[0]) * rmass > 0.5 || fabs(fc[1]) * rmass > 0.5 || fabs(fc[2]) * rmass > 0.5)
+  if (!P.kinematic && (fabs(fc[0]) * rmass > 0.5 || fabs(fc[1]) * rmass > 0.5 || fabs(fc[2]) * rmass > 0.5))
     raise_error(err, LBX_DEV_BIG_FORCE, step, a);
   double bv[3];
   for (int d = 0; d < 3; ++d) bv[d] = pc[3 + d] + rmass * fc[d];
   double vm = sqrt(bv[0] * bv[0] + bv[1] * bv[1] + bv[2] * bv[2]);
-  if (vm > P.max_vel) raise_error(err, LBX_DEV_EXTREME_VEL, step, a);
+  if (!P.kinematic && vm > P.max_vel) raise_error(err, LBX_DEV_EXTREME_VEL, step, a);
   const int nn[3] = {g.nx, g.ny, g.nz};
   double xn[3];
   for (int d = 0; d < 3; ++d) {
@@ -819,6 +965,8 @@ __global__ void k_integrate(PDev P, const double* __restrict__ pos_cur, double* 
     for (int k = 6; k < PS; ++k) pn[k] = pc[k];
   }
   for (int d = 0; d < 3; ++d) { pn[d] = xn[d]; pn[3 + d] = bv[d]; }
+  if (P.kinematic)  // prescribed motion: the sphere keeps its state, forces are only recorded
+    for (int k = 0; k < PS; ++k) pn[k] = pc[k];
   for (int d = 0; d < 3; ++d) {
     fo[d] = P.ext_f[d];
     fo[3 + d] = 0;
@@ -866,6 +1014,11 @@ static PDev pdev(const Ctx& c) {
   d.lub_k = double(c.p.lubric_k);
   d.lub_rmin = double(c.p.lubric_rmin);
   d.lub_rcap = double(c.p.lubric_rcap);
+  d.kinematic = c.p.kinematic;
+  d.closure = c.p.closure;
+  d.cl_gmin = c.p.closure_gap_min;
+  d.cl_gmax = c.p.closure_gap_max;
+  d.cl_vmax = c.p.closure_vmax;
   return d;
 }
 
@@ -924,6 +1077,10 @@ int particles_create(Ctx& c) {
   if (!ok(cudaMalloc(&s->owner, size_t(c.n) * 4))) return LBX_ERR_ALLOC;
   if (!ok(cudaMalloc(&s->bin_cnt, nbins * 4))) return LBX_ERR_ALLOC;
   if (!ok(cudaMalloc(&s->bin_list, nbins * BIN_CAP * 4))) return LBX_ERR_ALLOC;
+  if (!ok(cudaMalloc(&s->wclosure, size_t(LBX_CLOSURE_NWEIGHTS) * 4))) return LBX_ERR_ALLOC;
+  if (!ok(cudaMalloc(&s->nbr, size_t(cap) * NBCAP * 4))) return LBX_ERR_ALLOC;
+  if (!ok(cudaMalloc(&s->nbr_cnt, size_t(cap) * 4))) return LBX_ERR_ALLOC;
+  if (!ok(cudaMalloc(&s->corr, size_t(cap) * NBCAP * 12 * 4))) return LBX_ERR_ALLOC;
   cudaMemsetAsync(s->acc, 0, size_t(cap) * AS * 8, c.stream);
   cudaMemsetAsync(s->owner, 0, size_t(c.n) * 4, c.stream);
   cudaMemcpyAsync(s->tmpl, t.data(), t.size(), cudaMemcpyHostToDevice, c.stream);
@@ -943,6 +1100,10 @@ void particles_destroy(Ctx& c) {
   if (s->owner) cudaFree(s->owner);
   if (s->bin_cnt) cudaFree(s->bin_cnt);
   if (s->bin_list) cudaFree(s->bin_list);
+  if (s->wclosure) cudaFree(s->wclosure);
+  if (s->nbr) cudaFree(s->nbr);
+  if (s->nbr_cnt) cudaFree(s->nbr_cnt);
+  if (s->corr) cudaFree(s->corr);
   delete s;
   c.part = nullptr;
 }
@@ -1032,6 +1193,16 @@ int particles_step(Ctx& c) {
                                                      make_cg<C>(c));
     k_bb<S><<<s.np, 256, 0, c.stream>>>(P, pc, s.acc, B, g, sh, L, c.flags[fn], rR, rB);
     k_pairs<<<(s.np + 127) / 128, 128, 0, c.stream>>>(P, pc, s.acc, g);
+    if (c.p.closure) {
+      const int use_net = s.closure_ready;
+      const double cut = fmax(double(c.p.closure_gap_max) * s.rdim, c.p.lubrication ? double(c.p.lubric_rmin) : 0.0);
+      k_pair_nbrs<<<(s.np + 127) / 128, 128, 0, c.stream>>>(P, pc, g, cut, s.nbr, s.nbr_cnt, c.d_err, st);
+      size_t smem = sizeof(float) * (size_t(LBX_CLOSURE_NWEIGHTS) + 8 * 2 * H);
+      int blocks = (s.np * NBCAP + 7) / 8;
+      if (blocks > 148 * 4) blocks = 148 * 4;
+      k_closure_pairs<<<blocks, 256, smem, c.stream>>>(P, pc, g, s.wclosure, use_net, s.nbr, s.nbr_cnt, s.corr);
+      k_closure_accum<<<(s.np + 127) / 128, 128, 0, c.stream>>>(P, s.nbr, s.nbr_cnt, s.corr, s.acc);
+    }
     k_integrate<<<(s.np + 127) / 128, 128, 0, c.stream>>>(P, pc, s.pos[1 - s.pcur], s.frc[s.pcur],
                                                           s.frc[1 - s.pcur], s.acc, g, c.d_err, st);
     return launch_status();
@@ -1066,6 +1237,22 @@ int particles_get(Ctx& c, double* x, double* v, double* om, double* q, double* f
       for (int k = 0; k < 4; ++k) q[4 * a + k] = pos[size_t(a) * PS + 9 + k];
   }
   return 0;
+}
+
+int particles_set_closure(Ctx& c, const float* h_w) {
+  ParticleState* s = c.part;
+  if (!s) return LBX_ERR_STATE;
+  if (cudaMemcpyAsync(s->wclosure, h_w, size_t(LBX_CLOSURE_NWEIGHTS) * 4, cudaMemcpyHostToDevice, c.stream) !=
+      cudaSuccess)
+    return LBX_ERR_CUDA;
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_closure_pairs, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         int(sizeof(float) * (size_t(LBX_CLOSURE_NWEIGHTS) + 8 * 2 * H)));
+    attr = true;
+  }
+  s->closure_ready = 1;
+  return cudaStreamSynchronize(c.stream) == cudaSuccess ? 0 : LBX_ERR_CUDA;
 }
 
 int particles_flags_slot(const Ctx& c) { return c.part ? c.part->flags_last : c.fcur; }

@@ -886,12 +886,13 @@ class Oracle {
       P xo[3] = {ps(b, a, 0), ps(b, a, 1), ps(b, a, 2)};
       P v[3] = {ps(b, a, 3), ps(b, a, 4), ps(b, a, 5)};
       P fr[3] = {fa(b, a, 0), fa(b, a, 1), fa(b, a, 2)};
-      if (std::abs(fr[0]) * rmass > P(0.5) || std::abs(fr[1]) * rmass > P(0.5) || std::abs(fr[2]) * rmass > P(0.5))
+      if (!prm.kinematic &&
+          (std::abs(fr[0]) * rmass > P(0.5) || std::abs(fr[1]) * rmass > P(0.5) || std::abs(fr[2]) * rmass > P(0.5)))
         raise(LBX_DEV_BIG_FORCE, a);
       P bv[3];
       for (int d = 0; d < 3; ++d) bv[d] = v[d] + rmass * fr[d];
       P vm = std::sqrt(bv[0] * bv[0] + bv[1] * bv[1] + bv[2] * bv[2]);
-      if (vm > max_vel) raise(LBX_DEV_EXTREME_VEL, a);
+      if (!prm.kinematic && vm > max_vel) raise(LBX_DEV_EXTREME_VEL, a);
       P xn[3];
       for (int d = 0; d < 3; ++d) xn[d] = xo[d] + bv[d];
       const P cc[3] = {cx, cy, cz};
@@ -906,6 +907,8 @@ class Oracle {
       for (int d = 0; d < 3; ++d) { ps(o, a, d) = xn[d]; ps(o, a, 3 + d) = bv[d]; }
       if (!lrotate)
         for (int c = 6; c < 13; ++c) ps(o, a, c) = ps(b, a, c);
+      if (prm.kinematic) /* prescribed motion: state kept, forces only recorded */
+        for (int c = 0; c < 13; ++c) ps(o, a, c) = ps(b, a, c);
       /* reset the accumulators to the external force / torque */
       for (int d = 0; d < 3; ++d) {
         fa(o, a, d) = P(prm.ext_force[d]);
