@@ -188,17 +188,84 @@ def error_vs_f64(nsteps_list=(1000, 10000)):
     return out
 
 
+COLLOID_L = 256
+COLLOID_N = 1280
+
+
+def colloid_sim(storage, schedule=2):
+    """256^3 CG fluid with 1280 spheres of radius 5.5 (the first 1280 of the
+    reference's Tests/07-1280-Particle placement), density 1, neutral wetting, at rest."""
+    from lbcuda_b200 import LBSim, make_params
+    from lbcuda_b200.inputs import read_input_xyz, seeded_noise_fields
+    deck = os.path.join(ROOT, "tests", "golden", "decks", "07-1280.input.xyz.256cube.r5.5")
+    x, _, q = read_input_xyz(deck, COLLOID_N, True)
+    L = COLLOID_L
+    vol = 4.0 / 3.0 * np.pi * 5.5 ** 3
+    p = make_params(L, model="cg", storage=storage, sigma=SIGMA, beta=BETA, max_particles=COLLOID_N, radius=5.5,
+                    rmass=float(1.0 / vol), wetting="neutral", lrotate=1, max_vel=1.0)
+    s = LBSim(p)
+    s.set_schedule(schedule)
+    rR, rB = seeded_noise_fields(L, L, L, seed=SEED)
+    s.set_fields(rR, rB)
+    s.set_particles(x, np.zeros_like(x), None, q)
+    return s
+
+
+def colloid_timing(storage, steps=50, warm=10):
+    s = colloid_sim(storage)
+    s.step(warm)
+    s.sync()
+    tot, k, nl = s.time_steps(steps, kernel_timing=True)
+    code = s.status()[0]
+    s.close()
+    cells = COLLOID_L ** 3
+    mlups = cells * steps / (tot * 1e-3) / 1e6
+    return {"storage": storage, "mlups": mlups, "ms_per_step": tot / steps, "steps": steps,
+            "achieved_gbs_at_basis": mlups * 1e6 * BYTES_PER_CELL[storage] / 1e9,
+            "frac_at_basis": mlups * 1e6 * BYTES_PER_CELL[storage] / 1e9 / peaks()[0], "device_error": code}
+
+
+def only_region(args, local):
+    import torch
+    torch.cuda.set_device(local)
+    from lbcuda_b200 import LBSim, make_params
+    from lbcuda_b200.inputs import seeded_noise_fields
+    if args.only.startswith("colloid"):
+        r = colloid_timing(args.only.split("-")[1], steps=max(1, args.steps) * 5, warm=args.warmup)
+        print(json.dumps(r), flush=True)
+        return 0
+    rR, rB = seeded_noise_fields(L, L, L, seed=SEED)
+    s = LBSim(make_params(L, model="cg", storage=args.only, sigma=SIGMA, beta=BETA))
+    s.set_schedule(args.schedule)
+    s.set_fields(rR, rB)
+    s.step(args.warmup * args.lb_steps)
+    s.sync()
+    tot, k, nl = s.time_steps(args.steps * args.lb_steps, kernel_timing=args.schedule != 0)
+    n = args.steps * args.lb_steps
+    print(json.dumps({"only": args.only, "schedule": args.schedule, "ms_per_lattice_step": tot / n,
+                      "mlups": L ** 3 * n / (tot * 1e-3) / 1e6, "kernel_us": (k / nl * 1e3) if nl else None}),
+          flush=True)
+    s.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--no-extras", action="store_true", help="skip the error runs and the CPU baseline")
+    ap.add_argument("--no-extras", action="store_true", help="skip the error runs, the colloid case and the CPU baseline")
+    ap.add_argument("--only", choices=["f16", "f32", "bf16", "f64", "colloid-f16", "colloid-f32"],
+                    help="profiling aid: run one timed region only and print its timing")
+    ap.add_argument("--lb-steps", type=int, default=LB_PER_STEP, help="lattice steps per bench step")
+    ap.add_argument("--schedule", type=int, default=2, help="colour-gradient schedule (0, 1, 2)")
     args = ap.parse_args()
     ws, rank, local = dist_env()
     if args.impl == "reference":
         return reference_arm(args, ws, rank)
+    if args.only:
+        return only_region(args, local)
 
     import torch
     torch.cuda.set_device(local)
@@ -299,6 +366,7 @@ def main():
     extras = {}
     if rank == 0 and not args.no_extras:
         extras["error_vs_f64"] = error_vs_f64()
+        extras["colloid_256_1280"] = {st: colloid_timing(st) for st in ("f16", "f32")}
         extras["cpu_baseline"] = cpu_baseline_sample()
 
     if rank == 0:
