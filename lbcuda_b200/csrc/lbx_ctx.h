@@ -64,5 +64,8 @@ int fluid_get_fields(Ctx& c, void* d_rR, void* d_rB, void* d_vel, void* d_phase,
 int fluid_get_pops(Ctx& c, float* d_pR, float* d_pB);
 int fluid_get_sums(Ctx& c, double* d_out5);
 int fluid_lean(Ctx& c);
+int fluid_lean_particles(Ctx& c, int fo, int fn);
+void kt_begin(Ctx& c);
+void kt_end(Ctx& c);
 
 }  // namespace lbx

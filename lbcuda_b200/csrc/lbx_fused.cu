@@ -220,10 +220,22 @@ __device__ __forceinline__ int wrap0(int v, int n) {
   return v < 0 ? v + n : v;
 }
 
-template <typename S, int TX, int TY, int MINB>
+// Particle data of a step (flags of this and of the previous step, the side
+// densities written by the fill and wetting kernels, written back here for
+// every fluid cell for the bounce-back of the same step and the drain of the
+// next).
+template <typename C>
+struct LeanPart {
+  const int8_t* __restrict__ fold;
+  const int8_t* __restrict__ fnew;
+  C* rhoR;
+  C* rhoB;
+};
+
+template <typename S, int TX, int TY, int MINB, bool PART>
 __global__ void __launch_bounds__(TX* TY, MINB)
     k_cg_lean(const S* __restrict__ A, S* __restrict__ B, Geom g, LeanConst<typename Store<S>::C> K, int zlen,
-              unsigned long long* err, int64_t step) {
+              unsigned long long* err, int64_t step, LeanPart<typename Store<S>::C> PT) {
   using C = typename Store<S>::C;
   using R = Ring<TX, TY>;
   __shared__ C sphi[4][R::CELLS];
@@ -243,27 +255,54 @@ __global__ void __launch_bounds__(TX* TY, MINB)
   const int rxg = wrap0(x0 + rx - 1, g.nx), ryg = wrap0(y0 + ry - 1, g.ny);
   const int rslot = ry * R::RX + rx;
 
+  // clamped densities of cell (cx, cy, zz): pulled (fluid in both steps),
+  // from the side arrays (new fluid, or the virtual density of a surface
+  // cell), zero for every other solid cell (init_rho*_CG's MINDENS)
+  auto densities = [&](int cx, int cy, int zz, bool check, C& rR, C& rB) {
+    const int cell = cx + g.nx * (cy + g.ny * zz);
+    if constexpr (PART) {
+      const int8_t fn = PT.fnew[cell];
+      if (fn != LBX_FLUID_FLUID) {
+        if (fn == LBX_FLUID_SPHERELIST) { rR = PT.rhoR[cell]; rB = PT.rhoB[cell]; }
+        else { rR = C(0); rB = C(0); }
+        return false;
+      }
+      if (PT.fold[cell] != LBX_FLUID_FLUID) {
+        rR = PT.rhoR[cell];
+        rB = PT.rhoB[cell];
+        return false;
+      }
+    }
+    PullIdx P;
+    pull_idx(g, cx, cy, zz, P);
+    pull_rho<S, C>(A, g.n, P, K, rR, rB);
+    if (check && (rR < C(-10) || rR > C(10) || rB < C(-10) || rB > C(10)))
+      raise_error(err, LBX_DEV_RHO_RANGE, step, cell);
+    rR = clamp0(rR);
+    rB = clamp0(rB);
+    return true;
+  };
+
   // phase field of plane z (own cell and ring cell) into slot
   auto phase_plane = [&](int z, int slot, C& rRo, C& rBo) {
     const int zz = wrap0(z, g.nz);
-    PullIdx P;
-    pull_idx(g, x, y, zz, P);
+    const bool owned = active && z >= z0 && z < zend;
     C rR, rB;
-    pull_rho<S, C>(A, g.n, P, K, rR, rB);
-    if (active && z >= z0 && z < zend && (rR < C(-10) || rR > C(10) || rB < C(-10) || rB > C(10)))
-      raise_error(err, LBX_DEV_RHO_RANGE, step, x + g.nx * (y + g.ny * zz));
-    rR = clamp0(rR);
-    rB = clamp0(rB);
+    const bool pulled = densities(x, y, zz, owned, rR, rB);
+    if constexpr (PART) {
+      if (owned && pulled) {  // the densities of init_rho*_CG for the particle kernels
+        const int cell = x + g.nx * (y + g.ny * zz);
+        PT.rhoR[cell] = rR;
+        PT.rhoB[cell] = rB;
+      }
+    }
+    (void)pulled;
     rRo = rR;
     rBo = rB;
     sphi[slot][own] = (rR - rB) / (rR + rB);
     if (ringer) {
-      PullIdx Pr;
-      pull_idx(g, rxg, ryg, zz, Pr);
       C qR, qB;
-      pull_rho<S, C>(A, g.n, Pr, K, qR, qB);
-      qR = clamp0(qR);
-      qB = clamp0(qB);
+      densities(rxg, ryg, zz, false, qR, qB);
       sphi[slot][rslot] = (qR - qB) / (qR + qB);
     }
   };
@@ -277,33 +316,66 @@ __global__ void __launch_bounds__(TX* TY, MINB)
     phase_plane(z + 1, (z + 1) & 3, rRn, rBn);
     __syncthreads();
     if (active) {
-      const C* pm = sphi[(z + 3) & 3];
-      const C* p0 = sphi[z & 3];
-      const C* pp = sphi[(z + 1) & 3];
-      C px = 0, py = 0, pz = 0;
-#pragma unroll
-      for (int l = 1; l < Q27; ++l) {
-        const int dx = ex27(l), dy = ey27(l), dz = ez27(l);
-        const C* pl = dz < 0 ? pm : (dz > 0 ? pp : p0);
-        const C ps = pl[own + dy * R::RX + dx];
-        const C a = K.a27[wclass27(l)];
-        if (dx) px = px + (dx > 0 ? a : -a) * ps;
-        if (dy) py = py + (dy > 0 ? a : -a) * ps;
-        if (dz) pz = pz + (dz > 0 ? a : -a) * ps;
-      }
+      const int cell = x + g.nx * (y + g.ny * z);
       PullIdx P;
       pull_idx(g, x, y, z, P);
       C gR[Q], gB[Q];
       const S* aB = A + size_t(Q) * size_t(g.n);
-#pragma unroll
-      for (int l = 0; l < Q; ++l) {
-        gR[l] = load_raw<S, C>(A + size_t(l) * size_t(g.n) + P.src[l]);
-        gB[l] = load_raw<S, C>(aB + size_t(l) * size_t(g.n) + P.src[l]);
-      }
-      collide_lean(K, gR, gB, rRc, rBc, px, py, pz);
-      const int cell = x + g.nx * (y + g.ny * z);
       S* bR = B + cell;
       S* bB = B + size_t(Q) * size_t(g.n) + cell;
+      bool collide = true;
+      if constexpr (PART) {
+        const int8_t fn = PT.fnew[cell], fo = PT.fold[cell];
+        collide = fn == LBX_FLUID_FLUID;
+        if (collide && fo != LBX_FLUID_FLUID) {
+          // make_fluid already wrote the new node's populations (stored form) into B
+#pragma unroll
+          for (int l = 0; l < Q; ++l) {
+            gR[l] = load_raw<S, C>(bR + size_t(l) * size_t(g.n));
+            gB[l] = load_raw<S, C>(bB + size_t(l) * size_t(g.n));
+          }
+        } else if (!collide) {
+          // solid cell: streamed populations only; a spheredead source (previous
+          // step) leaves the destination's stale value, which is B's entry
+#pragma unroll
+          for (int l = 0; l < Q; ++l) {
+            const bool dead = l > 0 && PT.fold[P.src[l]] == LBX_FLUID_SPHEREDEAD;
+            gR[l] = dead ? load_raw<S, C>(bR + size_t(l) * size_t(g.n))
+                         : load_raw<S, C>(A + size_t(l) * size_t(g.n) + P.src[l]);
+            gB[l] = dead ? load_raw<S, C>(bB + size_t(l) * size_t(g.n))
+                         : load_raw<S, C>(aB + size_t(l) * size_t(g.n) + P.src[l]);
+          }
+        } else {
+#pragma unroll
+          for (int l = 0; l < Q; ++l) {
+            gR[l] = load_raw<S, C>(A + size_t(l) * size_t(g.n) + P.src[l]);
+            gB[l] = load_raw<S, C>(aB + size_t(l) * size_t(g.n) + P.src[l]);
+          }
+        }
+      } else {
+#pragma unroll
+        for (int l = 0; l < Q; ++l) {
+          gR[l] = load_raw<S, C>(A + size_t(l) * size_t(g.n) + P.src[l]);
+          gB[l] = load_raw<S, C>(aB + size_t(l) * size_t(g.n) + P.src[l]);
+        }
+      }
+      if (collide) {
+        const C* pm = sphi[(z + 3) & 3];
+        const C* p0 = sphi[z & 3];
+        const C* pp = sphi[(z + 1) & 3];
+        C px = 0, py = 0, pz = 0;
+#pragma unroll
+        for (int l = 1; l < Q27; ++l) {
+          const int dx = ex27(l), dy = ey27(l), dz = ez27(l);
+          const C* pl = dz < 0 ? pm : (dz > 0 ? pp : p0);
+          const C ps = pl[own + dy * R::RX + dx];
+          const C a = K.a27[wclass27(l)];
+          if (dx) px = px + (dx > 0 ? a : -a) * ps;
+          if (dy) py = py + (dy > 0 ? a : -a) * ps;
+          if (dz) pz = pz + (dz > 0 ? a : -a) * ps;
+        }
+        collide_lean(K, gR, gB, rRc, rBc, px, py, pz);
+      }
 #pragma unroll
       for (int l = 0; l < Q; ++l) {
         store_raw<S, C>(bR + size_t(l) * size_t(g.n), gR[l]);
@@ -325,14 +397,14 @@ static int lean_zlen(const Ctx& c, int tx, int ty, int per_sm) {
   return int((c.nz + segs - 1) / segs);
 }
 
-template <typename S, int TX, int TY, int MINB>
-static void launch_lean(Ctx& c, int zlen_override) {
+template <typename S, int TX, int TY, int MINB, bool PART>
+static void launch_lean(Ctx& c, int zlen_override, LeanPart<typename Store<S>::C> pt) {
   using C = typename Store<S>::C;
   int zlen = zlen_override > 0 ? zlen_override : lean_zlen(c, TX, TY, MINB);
   dim3 block(TX, TY, 1);
   dim3 grid((c.nx + TX - 1) / TX, (c.ny + TY - 1) / TY, (c.nz + zlen - 1) / zlen);
-  k_cg_lean<S, TX, TY, MINB><<<grid, block, 0, c.stream>>>((const S*)c.pops[c.cur], (S*)c.pops[1 - c.cur], geom(c),
-                                                         make_lean<C>(c), zlen, c.d_err, c.step + 1);
+  k_cg_lean<S, TX, TY, MINB, PART><<<grid, block, 0, c.stream>>>(
+      (const S*)c.pops[c.cur], (S*)c.pops[1 - c.cur], geom(c), make_lean<C>(c), zlen, c.d_err, c.step + 1, pt);
 }
 
 void kt_begin(Ctx& c);
@@ -342,18 +414,35 @@ void kt_end(Ctx& c);
 int fluid_lean(Ctx& c) {
   int rc = by_storage(c, [&](auto* tag) {
     using S = std::remove_pointer_t<decltype(tag)>;
+    using C = typename Store<S>::C;
+    LeanPart<C> none{nullptr, nullptr, nullptr, nullptr};
     kt_begin(c);
     if constexpr (std::is_same<S, double>::value) {
-      launch_lean<S, 32, 8, 1>(c, c.lean_zlen);
+      launch_lean<S, 32, 8, 1, false>(c, c.lean_zlen, none);
     } else {
-      if (c.lean_shape == 1) launch_lean<S, 32, 16, 1>(c, c.lean_zlen);
-      else launch_lean<S, 32, 8, 2>(c, c.lean_zlen);
+      if (c.lean_shape == 1) launch_lean<S, 32, 16, 1, false>(c, c.lean_zlen, none);
+      else launch_lean<S, 32, 8, 2, false>(c, c.lean_zlen, none);
     }
     kt_end(c);
     return launch_status();
   });
   if (!rc) c.cur = 1 - c.cur;
   return rc;
+}
+
+// the same step with particle flags (fo: flags of the previous step, fn: of this one)
+int fluid_lean_particles(Ctx& c, int fo, int fn) {
+  int rc = by_storage(c, [&](auto* tag) {
+    using S = std::remove_pointer_t<decltype(tag)>;
+    using C = typename Store<S>::C;
+    LeanPart<C> pt{c.flags[fo], c.flags[fn], (C*)c.rho[0], (C*)c.rho[1]};
+    kt_begin(c);
+    if constexpr (std::is_same<S, double>::value) launch_lean<S, 32, 8, 1, true>(c, c.lean_zlen, pt);
+    else launch_lean<S, 32, 8, 2, true>(c, c.lean_zlen, pt);
+    kt_end(c);
+    return launch_status();
+  });
+  return rc;  // the particle step swaps the buffers after its bounce-back
 }
 
 }  // namespace lbx

@@ -199,6 +199,31 @@ __device__ void block_sum(double v[NV], double* out /* NV, added */) {
   __syncthreads();
 }
 
+// Densities of this step at cell y (1-based coordinates): init_rho*_CG's
+// clamped sums of the streamed populations for a cell fluid in both steps,
+// the side arrays for any other cell (a node filled in this step, or a
+// surface cell's virtual density).
+template <typename S, typename C>
+__device__ __forceinline__ void rho_now(const S* __restrict__ A, const Geom& g, const Shift<C>& sh,
+                                        const int8_t* __restrict__ fold, const int8_t* __restrict__ fnew,
+                                        const C* rhoR, const C* rhoB, int i1, int j1, int k1, C& rR, C& rB) {
+  const int y = (i1 - 1) + g.nx * ((j1 - 1) + g.ny * (k1 - 1));
+  if (fnew[y] == LBX_FLUID_FLUID && fold[y] == LBX_FLUID_FLUID) {
+    Nbr b;
+    make_nbr(g, i1 - 1, j1 - 1, k1 - 1, b);
+    C f[Q];
+    pull(A, g, b, 0, sh, f);
+    rR = sum_q(f);
+    pull(A, g, b, 1, sh, f);
+    rB = sum_q(f);
+    if (rR < C(0)) rR = C(0);
+    if (rB < C(0)) rB = C(0);
+  } else {
+    rR = rhoR[y];
+    rB = rhoB[y];
+  }
+}
+
 // ---------------------------------------------------------------------------
 // kernels
 // ---------------------------------------------------------------------------
@@ -381,7 +406,7 @@ __global__ void __launch_bounds__(256) k_rho_p(const S* __restrict__ A, const S*
 // momentum.
 template <typename S>
 __global__ void __launch_bounds__(256) k_fill(PDev P, const double* __restrict__ pos_cur,
-                                              const double* __restrict__ pos_old, double* acc, S* B, Geom g,
+                                              const double* __restrict__ pos_old, double* acc, const S* A, S* B, Geom g,
                                               Shift<typename Store<S>::C> sh, LatticeT<typename Store<S>::C> L,
                                               const int8_t* __restrict__ fold, const int8_t* __restrict__ fnew,
                                               typename Store<S>::C* rhoR, typename Store<S>::C* rhoB,
@@ -403,8 +428,13 @@ __global__ void __launch_bounds__(256) k_fill(PDev P, const double* __restrict__
     C Rs = 0, Bs = 0;
     int D = 0;
     for (int l = 1; l < Q27; ++l) {  // compute_onebelt_density_twofluids
-      int y = cell0(g, wrap1(i1 + ex27(l), g.nx), wrap1(j1 + ey27(l), g.ny), wrap1(k1 + ez27(l), g.nz));
-      if (fnew[y] == LBX_FLUID_FLUID && fold[y] == LBX_FLUID_FLUID) { Rs = Rs + rhoR[y]; Bs = Bs + rhoB[y]; ++D; }
+      int yi = wrap1(i1 + ex27(l), g.nx), yj = wrap1(j1 + ey27(l), g.ny), yk = wrap1(k1 + ez27(l), g.nz);
+      int y = cell0(g, yi, yj, yk);
+      if (fnew[y] == LBX_FLUID_FLUID && fold[y] == LBX_FLUID_FLUID) {
+        C a, b2;
+        rho_now(A, g, sh, fold, fnew, rhoR, rhoB, yi, yj, yk, a, b2);
+        Rs = Rs + a; Bs = Bs + b2; ++D;
+      }
     }
     if (D) { Rs = Rs / C(D); Bs = Bs / C(D); }
     else {  // compute_secbelt_density_twofluids
@@ -413,8 +443,13 @@ __global__ void __launch_bounds__(256) k_fill(PDev P, const double* __restrict__
         for (int jj = -2; jj <= 2; ++jj)
           for (int ii = -2; ii <= 2; ++ii) {
             if (!(ii == -2 || ii == 2 || jj == -2 || jj == 2 || kk == -2 || kk == 2)) continue;
-            int y = cell0(g, wrap1(i1 + ii, g.nx), wrap1(j1 + jj, g.ny), wrap1(k1 + kk, g.nz));
-            if (fnew[y] == LBX_FLUID_FLUID && fold[y] == LBX_FLUID_FLUID) { Rs = Rs + rhoR[y]; Bs = Bs + rhoB[y]; ++D; }
+            int yi = wrap1(i1 + ii, g.nx), yj = wrap1(j1 + jj, g.ny), yk = wrap1(k1 + kk, g.nz);
+            int y = cell0(g, yi, yj, yk);
+            if (fnew[y] == LBX_FLUID_FLUID && fold[y] == LBX_FLUID_FLUID) {
+              C a, b2;
+              rho_now(A, g, sh, fold, fnew, rhoR, rhoB, yi, yj, yk, a, b2);
+              Rs = Rs + a; Bs = Bs + b2; ++D;
+            }
           }
       if (D) { Rs = Rs / C(D); Bs = Bs / C(D); }
       // else fix_onebelt_density_twofluids (empty in the reference): zero density
@@ -451,8 +486,9 @@ __global__ void __launch_bounds__(256) k_fill(PDev P, const double* __restrict__
 
 // virtual densities of the surface cells a sphere owns: Janus
 // (compute_virtual_rho) or neutral wetting (compute_densities_wall)
-template <typename C>
+template <typename S, typename C = typename Store<S>::C>
 __global__ void __launch_bounds__(256) k_virtual(PDev P, const double* __restrict__ pos, Geom g, int neutral,
+                                                 const S* A, Shift<C> sh,
                                                  const int8_t* __restrict__ fold, const int8_t* __restrict__ fnew,
                                                  C* rhoR, C* rhoB, C* phi, LatticeT<C> L) {
   const int a = blockIdx.x;
@@ -479,10 +515,13 @@ __global__ void __launch_bounds__(256) k_virtual(PDev P, const double* __restric
     } else {
       C Rs = 0, Bs = 0, Ds = 0;
       for (int l = 1; l < Q27; ++l) {  // compute_onebelt_density_2fl_weights
-        int y = cell0(g, wrap1(i1 + ex27(l), g.nx), wrap1(j1 + ey27(l), g.ny), wrap1(k1 + ez27(l), g.nz));
+        int yi = wrap1(i1 + ex27(l), g.nx), yj = wrap1(j1 + ey27(l), g.ny), yk = wrap1(k1 + ez27(l), g.nz);
+        int y = cell0(g, yi, yj, yk);
         if (fnew[y] == LBX_FLUID_FLUID) {
           C w = L.p27[wclass27(l)];
-          Rs = Rs + w * rhoR[y]; Bs = Bs + w * rhoB[y]; Ds = Ds + w;
+          C a, b2;
+          rho_now(A, g, sh, fold, fnew, rhoR, rhoB, yi, yj, yk, a, b2);
+          Rs = Rs + w * a; Bs = Bs + w * b2; Ds = Ds + w;
         }
       }
       if (Ds != C(0)) { R = Rs / Ds; Bv = Bs / Ds; }
@@ -493,12 +532,17 @@ __global__ void __launch_bounds__(256) k_virtual(PDev P, const double* __restric
           for (int jj = -2; jj <= 2; ++jj)
             for (int ii = -2; ii <= 2; ++ii) {
               if (!(ii == -2 || ii == 2 || jj == -2 || jj == 2 || kk == -2 || kk == 2)) continue;
-              int y = cell0(g, wrap1(i1 + ii, g.nx), wrap1(j1 + jj, g.ny), wrap1(k1 + kk, g.nz));
-              if (fnew[y] == LBX_FLUID_FLUID && fold[y] == LBX_FLUID_FLUID) { Rs = Rs + rhoR[y]; Bs = Bs + rhoB[y]; ++D; }
+              int yi = wrap1(i1 + ii, g.nx), yj = wrap1(j1 + jj, g.ny), yk = wrap1(k1 + kk, g.nz);
+              int y = cell0(g, yi, yj, yk);
+              if (fnew[y] == LBX_FLUID_FLUID && fold[y] == LBX_FLUID_FLUID) {
+                C a, b2;
+                rho_now(A, g, sh, fold, fnew, rhoR, rhoB, yi, yj, yk, a, b2);
+                Rs = Rs + a; Bs = Bs + b2; ++D;
+              }
             }
-        if (!D) return;  // no fluid in either belt: the density stays zero
-        R = Rs / C(D);
-        Bv = Bs / C(D);
+        // no fluid in either belt: the density stays at init_rho*_CG's zero
+        R = D ? Rs / C(D) : C(0);
+        Bv = D ? Bs / C(D) : C(0);
       }
     }
     rhoR[cell] = R;
@@ -1185,12 +1229,21 @@ int particles_step(Ctx& c) {
     if (r0) return r0;
     k_flags<<<d.grid, d.block, 0, c.stream>>>(P, pc, g, c.flags[fn]);
     k_drain<S><<<s.np, 256, 0, c.stream>>>(P, pc, po, s.acc, A, B, g, sh, c.flags[fo], c.flags[fn], rR, rB);
-    k_rho_p<S><<<d.grid, d.block, 0, c.stream>>>(A, B, g, sh, c.flags[fo], c.flags[fn], phi, rR, rB, c.d_err, st);
-    k_fill<S><<<s.np, 256, 0, c.stream>>>(P, pc, po, s.acc, B, g, sh, L, c.flags[fo], c.flags[fn], rR, rB, phi);
-    k_virtual<C><<<s.np, 256, 0, c.stream>>>(P, pc, g, c.p.wetting == LBX_WET_NEUTRAL ? 1 : 0, c.flags[fo],
+    const bool fused = c.fused == 2;
+    if (!fused)
+      k_rho_p<S><<<d.grid, d.block, 0, c.stream>>>(A, B, g, sh, c.flags[fo], c.flags[fn], phi, rR, rB, c.d_err, st);
+    k_fill<S><<<s.np, 256, 0, c.stream>>>(P, pc, po, s.acc, A, B, g, sh, L, c.flags[fo], c.flags[fn], rR, rB, phi);
+    k_virtual<S><<<s.np, 256, 0, c.stream>>>(P, pc, g, c.p.wetting == LBX_WET_NEUTRAL ? 1 : 0, A, sh, c.flags[fo],
                                               c.flags[fn], rR, rB, phi, L);
-    k_collide_p<S><<<d.grid, d.block, 0, c.stream>>>(A, B, g, sh, phi, rR, rB, c.flags[fo], c.flags[fn],
-                                                     make_cg<C>(c));
+    if (fused) {
+      int r1 = fluid_lean_particles(c, fo, fn);
+      if (r1) return r1;
+    } else {
+      kt_begin(c);
+      k_collide_p<S><<<d.grid, d.block, 0, c.stream>>>(A, B, g, sh, phi, rR, rB, c.flags[fo], c.flags[fn],
+                                                       make_cg<C>(c));
+      kt_end(c);
+    }
     k_bb<S><<<s.np, 256, 0, c.stream>>>(P, pc, s.acc, B, g, sh, L, c.flags[fn], rR, rB);
     k_pairs<<<(s.np + 127) / 128, 128, 0, c.stream>>>(P, pc, s.acc, g);
     if (c.p.closure) {

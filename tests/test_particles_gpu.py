@@ -24,13 +24,14 @@ def rel(a, b):
     return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-30))
 
 
-def make_pair(n, x, v, omega=None, q=None, steps=0, fields=None, **kw):
+def make_pair(n, x, v, omega=None, q=None, steps=0, fields=None, sched=2, **kw):
     kw.setdefault("max_vel", 1.0)
     p = make_params(n, model="cg", storage="f32", max_particles=len(x), **kw)
     if fields is None:
         r = np.full((n, n, n), 0.5, np.float32)
         fields = (r, r)
     g = LBSim(p)
+    g.set_schedule(sched)
     g.set_fields(*fields)
     g.set_particles(x, v, omega, q)
     o = OracleSim(p, "f32p64")
@@ -57,16 +58,18 @@ def test_flags_bit_exact_with_periodic_wrap():
     assert np.array_equal(g.get_flags(), o.get_flags())
 
 
+@pytest.mark.parametrize("sched", [2, 0])
 @pytest.mark.parametrize("wetting", ["janus", "neutral"])
 @pytest.mark.parametrize("lrotate", [0, 1])
-def test_moving_spheres_match_oracle(wetting, lrotate):
+def test_moving_spheres_match_oracle(wetting, lrotate, sched):
+    """25 steps with fill/drain (the spheres cross cell boundaries), single-pass (2) and two-pass (0) fluid."""
     n = 32
     x = np.array([[8.3, 9.1, 10.2], [22.6, 20.4, 24.9], [15.2, 27.7, 3.1]])
     v = np.array([[0.04, -0.03, 0.02], [-0.05, 0.01, 0.03], [0.02, 0.04, -0.05]])
     om = np.array([[0.0, 0.0, 0.01], [0.005, -0.004, 0.0], [0.0, 0.006, 0.003]]) if lrotate else None
     rR, rB = seeded_noise_fields(n, n, n, seed=3)
     g, o = make_pair(n, x, v, om, None, steps=25, fields=(rR, rB), lrotate=lrotate, wetting=wetting,
-                     sigma=0.02, beta=0.7)
+                     sigma=0.02, beta=0.7, sched=sched)
     assert g.status()[0] == 0 and o.status()[0] == 0
     assert np.array_equal(g.get_flags(), o.get_flags())
     gp, op = g.get_particles(), o.get_particles()
