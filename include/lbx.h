@@ -99,7 +99,10 @@ typedef struct lbx_params {
   float closure_gap_min;  /* training envelope of the closure: gap / R in [min, max] */
   float closure_gap_max;
   float closure_vmax;     /* and |relative velocity| components <= vmax */
-  int32_t reserved[3];
+  int32_t exact_tiles;    /* 1 (default): a sphere acts on a cell only where the reference's 8x4x4
+                             tile lists (makeListAtomsGPU) reach it; for integer radii those lists
+                             miss template cells.  0: every cell of the sphere's template box */
+  int32_t reserved[2];
 } lbx_params;
 
 /* Fill the reference defaults for an nx*ny*nz periodic box: CG model, FP32
@@ -199,6 +202,23 @@ int lbx_closure_infer(const float* weights, const float* X, int32_t n, float* Y)
  * (p->lubrication) to the pairs outside it.  Without weights every pair
  * takes the fallback. */
 int lbx_closure_set(void* ctx, const float* weights);
+
+/* ---- ensemble of boxes (no counterpart in the reference) ---------------- */
+/* nbox independent colour-gradient boxes (params[i]: sizes and spheres may
+ * differ; storage, tau, sigma, beta, rho0 must agree) advanced together:
+ * one persistent fluid kernel for all boxes per step, the sphere kernels of
+ * each box around it, two steps captured into one CUDA graph. */
+int lbx_ensemble_create(int32_t nbox, const lbx_params* params, void** ens);
+int lbx_ensemble_destroy(void* ens);
+/* Context of box i, for lbx_set_fields / lbx_set_particles / lbx_get_* /
+ * lbx_closure_set; owned by the ensemble (do not destroy). */
+int lbx_ensemble_box(void* ens, int32_t i, void** ctx);
+int lbx_ensemble_step(void* ens, int32_t nsteps);
+int lbx_ensemble_time(void* ens, int32_t nsteps, double* ms);
+/* Autotuner: times every (CTA shape, z-segment length) candidate for
+ * `trial` steps on the boxes themselves (this advances them) and keeps the
+ * fastest; chosen = {shape, zlen}, best_ms = per-step time. */
+int lbx_ensemble_tune(void* ens, int32_t trial, int32_t* chosen, double* best_ms);
 
 /* ---- measurement ------------------------------------------------------- */
 /* Colour-gradient schedule: 2 = lean single-pass kernel (default), 1 = the

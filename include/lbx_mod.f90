@@ -37,7 +37,8 @@ module lbx_mod
     real(c_float) :: lubric_k, lubric_rmin, lubric_rcap
     integer(c_int32_t) :: kinematic, closure
     real(c_float) :: closure_gap_min, closure_gap_max, closure_vmax
-    integer(c_int32_t) :: reserved(3)
+    integer(c_int32_t) :: exact_tiles
+    integer(c_int32_t) :: reserved(2)
   end type lbx_params
 
   interface

@@ -28,7 +28,7 @@ class LbxParams(C.Structure):
         ("lubric_k", C.c_float), ("lubric_rmin", C.c_float), ("lubric_rcap", C.c_float),
         ("kinematic", C.c_int32), ("closure", C.c_int32),
         ("closure_gap_min", C.c_float), ("closure_gap_max", C.c_float), ("closure_vmax", C.c_float),
-        ("reserved", C.c_int32 * 3),
+        ("exact_tiles", C.c_int32), ("reserved", C.c_int32 * 2),
     ]
 
 
@@ -72,6 +72,12 @@ SIGNATURES = {
     "lbx_closure_grad": (C.c_int, [_F, _F, _F, C.c_int32, _F]),
     "lbx_closure_infer": (C.c_int, [_F, _F, C.c_int32, _F]),
     "lbx_closure_set": (C.c_int, [_P, _F]),
+    "lbx_ensemble_create": (C.c_int, [C.c_int32, C.POINTER(LbxParams), _PP]),
+    "lbx_ensemble_destroy": (C.c_int, [_P]),
+    "lbx_ensemble_box": (C.c_int, [_P, C.c_int32, _PP]),
+    "lbx_ensemble_step": (C.c_int, [_P, C.c_int32]),
+    "lbx_ensemble_time": (C.c_int, [_P, C.c_int32, _D]),
+    "lbx_ensemble_tune": (C.c_int, [_P, C.c_int32, _I32, _D]),
     "lbx_sync": (C.c_int, [_P]),
     "lbx_status": (C.c_int, [_P, _I32, _I32, _I64]),
     "lbx_error_string": (C.c_char_p, [C.c_int]),

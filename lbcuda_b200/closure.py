@@ -4,10 +4,12 @@ The closure corrects the force and torque of near-contact sphere pairs that
 the lattice resolves poorly (small radius).  Its training data come from the
 method itself: the same two-sphere configuration is run with prescribed
 sphere motion (``kinematic`` contexts) once well resolved (radius R_hi in an
-L_hi^3 box) and once at the deployment radius R_lo (box scaled by
-R_lo/R_hi); the target is the resolved force scaled to R_lo (forces of
-Stokes and lubrication flows scale as mu R U at fixed gap/R, torques as
-mu R^2 U) minus the under-resolved one, in the pair frame.  Training and
+L_hi^3 box) and once at the deployment radius R_lo (box, gap and time scaled
+by s = R_lo/R_hi, s^2 for time; translational velocities equal, angular
+velocities scaled by s so that the surface velocities agree).  For such
+dynamically similar Stokes flows forces scale as mu R U and torques as
+mu R^2 U, so the target is F_hi s - F_lo and T_hi s^2 - T_lo, in the pair
+frame.  Training and
 inference run in the library's own kernels (lbx_closure_train /
 lbx_closure_infer); the analytic lubrication of the reference stays the
 fallback outside the training envelope and the judge of the gain.
@@ -92,7 +94,7 @@ def run_pair(cfg, R, L, steps, average=0.25, storage="f32", lubrication=False, s
                         lrotate=1, wetting="neutral", max_vel=1.0,
                         hz_rmin=float(2 * R - 0.5), hz_rcap=float(2 * R - 2.0),
                         lubrication=1 if lubrication else 0, lubric_k=1.0 / 6.0, lubric_rmin=1.0,
-                        lubric_rcap=float(0.05 * R))
+                        lubric_rcap=float(0.05 * R), exact_tiles=0)
         sim = LBSim(p)
         if sim_cache is not None:
             sim_cache[key] = sim
@@ -120,7 +122,8 @@ def generate(n_samples, R_hi=12, L_hi=96, R_lo=3, steps_hi=300, seed=0, progress
     base = np.zeros((n_samples, DOUT))
     cache = {}
     for k, cfg in enumerate(cfgs):
-        hi, *_ = run_pair(cfg, R_hi, L_hi, steps_hi, sim_cache=cache)
+        cfg_hi = dict(cfg, oi=np.asarray(cfg["oi"]) * s, oj=np.asarray(cfg["oj"]) * s)
+        hi, *_ = run_pair(cfg_hi, R_hi, L_hi, steps_hi, sim_cache=cache)
         lo, x, v, om = run_pair(cfg, R_lo, L_lo, steps_lo, sim_cache=cache)
         feat, Fm = features(x[0], x[1], v[0], v[1], om[0], om[1], R_lo, (L_lo,) * 3)
         scale = np.array([s, s * s, s, s * s])[:, None]

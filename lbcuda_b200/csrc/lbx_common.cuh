@@ -128,10 +128,19 @@ struct Shift {
 };
 
 // ---- geometry ---------------------------------------------------------------
+// Population layout: element (l * n + cell) * nc + comp, i.e. the
+// components of one direction and cell are adjacent (a half2 / float2 / double2
+// for the two colour-gradient components), direction planes of n cells, x
+// fastest inside a plane.
 struct Geom {
   int nx, ny, nz;
-  int64_t n;  // nx*ny*nz, population plane stride
+  int64_t n;  // nx*ny*nz cells per direction plane
+  int nc;     // components (1 BGK, 2 colour gradient)
 };
+
+__host__ __device__ __forceinline__ size_t pidx(const Geom& g, int comp, int l, int64_t cell) {
+  return (size_t(l) * size_t(g.n) + size_t(cell)) * size_t(g.nc) + size_t(comp);
+}
 
 // ---- device error word -------------------------------------------------------
 // One 64-bit word: [63:56] code, [55:32] step (mod 2^24), [31:0] cell/particle.

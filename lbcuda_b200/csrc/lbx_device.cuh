@@ -58,18 +58,15 @@ __device__ __forceinline__ C equil_u(const LatticeT<C>& L, C rho, C edu, C usq_t
 template <typename S, typename C>
 __device__ __forceinline__ void pull(const S* __restrict__ A, const Geom& g, const Nbr& b, int comp,
                                      const Shift<C>& sh, C f[Q]) {
-  const S* base = A + size_t(comp) * Q * size_t(g.n);
 #pragma unroll
-  for (int l = 0; l < Q; ++l)
-    f[l] = Store<S>::ld(base + size_t(l) * size_t(g.n) + at(b, -ex(l), -ey(l), -ez(l)), sh.at(comp, l));
+  for (int l = 0; l < Q; ++l) f[l] = Store<S>::ld(A + pidx(g, comp, l, at(b, -ex(l), -ey(l), -ez(l))), sh.at(comp, l));
 }
 
 template <typename S, typename C>
 __device__ __forceinline__ void store_all(S* __restrict__ B, const Geom& g, int cell, int comp, const Shift<C>& sh,
                                           const C f[Q]) {
-  S* base = B + size_t(comp) * Q * size_t(g.n) + cell;
 #pragma unroll
-  for (int l = 0; l < Q; ++l) Store<S>::st(base + size_t(l) * size_t(g.n), f[l], sh.at(comp, l));
+  for (int l = 0; l < Q; ++l) Store<S>::st(B + pidx(g, comp, l, cell), f[l], sh.at(comp, l));
 }
 
 // The post-streaming populations of a cell, pulled from the post-collision
@@ -78,16 +75,14 @@ __device__ __forceinline__ void store_all(S* __restrict__ B, const Geom& g, int 
 template <typename S, typename C>
 __device__ __forceinline__ void pull_dead(const S* __restrict__ A, const S* Bold, const Geom& g, const Nbr& b,
                                           int comp, const Shift<C>& sh, const int8_t* __restrict__ fold, C f[Q]) {
-  const S* base = A + size_t(comp) * Q * size_t(g.n);
-  const S* bb = Bold + size_t(comp) * Q * size_t(g.n);
   const int self = at(b, 0, 0, 0);
 #pragma unroll
   for (int l = 0; l < Q; ++l) {
     int src = at(b, -ex(l), -ey(l), -ez(l));
     if (l > 0 && fold[src] == LBX_FLUID_SPHEREDEAD)
-      f[l] = Store<S>::ld(bb + size_t(l) * size_t(g.n) + self, sh.at(comp, l));
+      f[l] = Store<S>::ld(Bold + pidx(g, comp, l, self), sh.at(comp, l));
     else
-      f[l] = Store<S>::ld(base + size_t(l) * size_t(g.n) + src, sh.at(comp, l));
+      f[l] = Store<S>::ld(A + pidx(g, comp, l, src), sh.at(comp, l));
   }
 }
 
@@ -231,7 +226,7 @@ inline CGConst<C> make_cg(const Ctx& c) {
   return K;
 }
 
-inline Geom geom(const Ctx& c) { return Geom{c.nx, c.ny, c.nz, c.n}; }
+inline Geom geom(const Ctx& c) { return Geom{c.nx, c.ny, c.nz, c.n, c.ncomp}; }
 
 template <typename F>
 inline int by_storage(const Ctx& c, F&& fn) {

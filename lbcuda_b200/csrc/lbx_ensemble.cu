@@ -1,0 +1,275 @@
+// lbx_ensemble.cu — many independent boxes of uneven size advanced together
+// (no counterpart in the reference, which runs one compile-time cubic box).
+//
+// Every box is a full context (include/lbx.h), so its fields, spheres and
+// closure are set and read with the ordinary entry points.  A step of the
+// ensemble launches, on one stream: the sphere pre-kernels of every box with
+// spheres, ONE persistent colour-gradient kernel for the fluid of all boxes
+// (k_cg_lean_multi: CTAs take (box, column, z-segment) work items, longest
+// first), then the sphere post-kernels.  Two consecutive steps (the
+// ping-pong parity) are captured once into a CUDA graph and replayed, so the
+// host issues one graph launch per two steps.  lbx_ensemble_tune times the
+// candidate CTA shapes and z-segment lengths on the boxes themselves and
+// keeps the fastest.
+#include <algorithm>
+#include <new>
+#include <vector>
+
+#include "lbx_device.cuh"
+
+namespace lbx {
+
+template <typename C> struct LeanConst;
+template <typename C> struct LeanPart;
+template <typename C> struct BoxDesc;
+struct WorkItem;
+template <typename C> LeanConst<C> make_lean(const Ctx& c);
+
+int particles_active(const Ctx& c);
+int particles_pre(Ctx& c);
+int particles_post(Ctx& c);
+
+// implemented in lbx_fused.cu
+int ensemble_launch(const std::vector<Ctx*>& boxes, int shape, const std::vector<int>& zlen, void* d_desc,
+                    void* d_work, int nwork, cudaStream_t stream, int build_only, int parity);
+
+}  // namespace lbx
+
+namespace {
+
+struct Ensemble {
+  std::vector<lbx::Ctx*> boxes;
+  cudaStream_t stream = nullptr;
+  int shape = 0;                 // 0: 32x8 CTAs, 1: 32x16
+  std::vector<int> zlen;         // per box
+  void* d_desc[2] = {nullptr, nullptr};
+  void* d_work[2] = {nullptr, nullptr};
+  int nwork = 0;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  bool tables_ok = false;
+};
+
+void drop_graph(Ensemble& e) {
+  if (e.exec) cudaGraphExecDestroy(e.exec);
+  if (e.graph) cudaGraphDestroy(e.graph);
+  e.exec = nullptr;
+  e.graph = nullptr;
+}
+
+int build_tables(Ensemble& e) {
+  for (int p = 0; p < 2; ++p) {
+    int rc = lbx::ensemble_launch(e.boxes, e.shape, e.zlen, e.d_desc[p], e.d_work[p], 0, e.stream, 1, p);
+    if (rc < 0) return rc;
+    e.nwork = rc;
+  }
+  e.tables_ok = true;
+  return 0;
+}
+
+// one eager step of every box
+int step_once(Ensemble& e) {
+  if (!e.tables_ok) {
+    int rc = build_tables(e);
+    if (rc) return rc;
+  }
+  const int parity = e.boxes[0]->cur;
+  for (auto* c : e.boxes)
+    if (c->cur != parity) return LBX_ERR_STATE;  // boxes must be stepped together
+  for (auto* c : e.boxes)
+    if (lbx::particles_active(*c)) {
+      int rc = lbx::particles_pre(*c);
+      if (rc) return rc;
+    }
+  int rc = lbx::ensemble_launch(e.boxes, e.shape, e.zlen, e.d_desc[parity], e.d_work[parity], e.nwork, e.stream, 0,
+                                parity);
+  if (rc) return rc;
+  for (auto* c : e.boxes) {
+    if (lbx::particles_active(*c)) {
+      rc = lbx::particles_post(*c);
+      if (rc) return rc;
+    } else {
+      c->cur = 1 - c->cur;
+      c->step += 1;
+    }
+  }
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int lbx_ensemble_create(int32_t nbox, const lbx_params* params, void** out) {
+  if (!params || !out || nbox < 1) return LBX_ERR_ARG;
+  *out = nullptr;
+  for (int i = 1; i < nbox; ++i)
+    if (params[i].storage != params[0].storage || params[i].model != LBX_MODEL_CG ||
+        params[i].tauR != params[0].tauR || params[i].tauB != params[0].tauB || params[i].sigma != params[0].sigma ||
+        params[i].beta != params[0].beta || params[i].rho0R != params[0].rho0R || params[i].rho0B != params[0].rho0B)
+      return LBX_ERR_ARG;  // one fluid kernel (and its constants) for every box
+  if (params[0].model != LBX_MODEL_CG) return LBX_ERR_ARG;
+  Ensemble* e = new (std::nothrow) Ensemble();
+  if (!e) return LBX_ERR_ALLOC;
+  int rc = cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) == cudaSuccess ? 0 : LBX_ERR_CUDA;
+  for (int i = 0; i < nbox && !rc; ++i) {
+    void* h = nullptr;
+    rc = lbx_create(&params[i], &h);
+    if (rc) break;
+    auto* c = static_cast<lbx::Ctx*>(h);
+    cudaStreamDestroy(c->stream);  // every box runs on the ensemble's stream
+    c->stream = e->stream;
+    c->fused = 2;
+    e->boxes.push_back(c);
+    e->zlen.push_back(std::min(c->nz, 16));
+  }
+  size_t desc_bytes = 512 * size_t(nbox), work_cap = 0;
+  for (auto* c : e->boxes) work_cap += size_t((c->nx + 31) / 32) * ((c->ny + 7) / 8) * c->nz;
+  for (int p = 0; p < 2 && !rc; ++p) {
+    if (cudaMalloc(&e->d_desc[p], desc_bytes) != cudaSuccess) rc = LBX_ERR_ALLOC;
+    if (!rc && cudaMalloc(&e->d_work[p], work_cap * 20 + 64) != cudaSuccess) rc = LBX_ERR_ALLOC;
+  }
+  if (rc) {
+    *out = e;
+    lbx_ensemble_destroy(e);
+    *out = nullptr;
+    return rc;
+  }
+  *out = e;
+  return 0;
+}
+
+int lbx_ensemble_destroy(void* ens) {
+  Ensemble* e = static_cast<Ensemble*>(ens);
+  if (!e) return LBX_ERR_ARG;
+  if (e->stream) cudaStreamSynchronize(e->stream);
+  drop_graph(*e);
+  for (auto* c : e->boxes) {
+    c->stream = nullptr;  // owned by the ensemble
+    lbx_destroy(c);
+  }
+  for (int p = 0; p < 2; ++p) {
+    if (e->d_desc[p]) cudaFree(e->d_desc[p]);
+    if (e->d_work[p]) cudaFree(e->d_work[p]);
+  }
+  if (e->stream) cudaStreamDestroy(e->stream);
+  delete e;
+  return 0;
+}
+
+int lbx_ensemble_box(void* ens, int32_t i, void** ctx) {
+  Ensemble* e = static_cast<Ensemble*>(ens);
+  if (!e || !ctx || i < 0 || i >= int(e->boxes.size())) return LBX_ERR_ARG;
+  *ctx = e->boxes[size_t(i)];
+  drop_graph(*e);  // the caller may change the boxes' state
+  return 0;
+}
+
+int lbx_ensemble_step(void* ens, int32_t nsteps) {
+  Ensemble* e = static_cast<Ensemble*>(ens);
+  if (!e || nsteps < 0) return LBX_ERR_ARG;
+  int rc = 0;
+  int done = 0;
+  if (nsteps >= 2 && e->boxes[0]->cur == 0) {
+    if (!e->exec) {
+      if (!e->tables_ok && (rc = build_tables(*e))) return rc;
+      // capture two steps: the buffers come back to the same parity
+      if (cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return LBX_ERR_CUDA;
+      int r1 = step_once(*e);
+      int r2 = r1 ? r1 : step_once(*e);
+      cudaGraph_t g = nullptr;
+      cudaError_t ce = cudaStreamEndCapture(e->stream, &g);
+      // the captured launches did not run: undo the host-side step bookkeeping
+      for (auto* c : e->boxes) c->step -= 2;
+      if (r2 || ce != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        return r2 ? r2 : LBX_ERR_CUDA;
+      }
+      e->graph = g;
+      if (cudaGraphInstantiate(&e->exec, e->graph, 0) != cudaSuccess) {
+        drop_graph(*e);
+        return LBX_ERR_CUDA;
+      }
+    }
+    for (; done + 2 <= nsteps; done += 2) {
+      if (cudaGraphLaunch(e->exec, e->stream) != cudaSuccess) return LBX_ERR_CUDA;
+      for (auto* c : e->boxes) c->step += 2;
+    }
+  }
+  for (; done < nsteps; ++done)
+    if ((rc = step_once(*e))) return rc;
+  return 0;
+}
+
+// Time steps of the ensemble on its stream (CUDA events).
+int lbx_ensemble_time(void* ens, int32_t nsteps, double* ms) {
+  Ensemble* e = static_cast<Ensemble*>(ens);
+  if (!e || nsteps < 0) return LBX_ERR_ARG;
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  cudaEventRecord(a, e->stream);
+  int rc = lbx_ensemble_step(ens, nsteps);
+  cudaEventRecord(b, e->stream);
+  if (!rc && cudaEventSynchronize(b) != cudaSuccess) rc = LBX_ERR_CUDA;
+  float t = 0.f;
+  if (!rc) cudaEventElapsedTime(&t, a, b);
+  if (ms) *ms = t;
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  return rc;
+}
+
+// Autotuner: for every candidate (CTA shape, z-segment length), build the
+// work tables, run `trial` eager steps (always an even number, so the state
+// parity is kept) and keep the fastest.  Returns the choice in chosen[2] =
+// {shape, zlen} (zlen capped per box at its nz).
+int lbx_ensemble_tune(void* ens, int32_t trial, int32_t* chosen, double* best_ms) {
+  Ensemble* e = static_cast<Ensemble*>(ens);
+  if (!e || trial < 2) return LBX_ERR_ARG;
+  trial += trial & 1;
+  drop_graph(*e);
+  const int shapes[2] = {0, 1};
+  const int zl[5] = {4, 8, 16, 32, 64};
+  double best = 1e30;
+  int bs = 0, bz = 16;
+  for (int si = 0; si < 2; ++si)
+    for (int zi = 0; zi < 5; ++zi) {
+      e->shape = shapes[si];
+      for (size_t i = 0; i < e->boxes.size(); ++i) e->zlen[i] = std::min(e->boxes[i]->nz, zl[zi]);
+      e->tables_ok = false;
+      int rc = build_tables(*e);
+      if (rc) return rc;
+      for (int w = 0; w < 2; ++w)
+        if ((rc = step_once(*e))) return rc;
+      cudaEvent_t a, b;
+      cudaEventCreate(&a);
+      cudaEventCreate(&b);
+      cudaEventRecord(a, e->stream);
+      for (int s = 0; s < trial && !rc; ++s) rc = step_once(*e);
+      cudaEventRecord(b, e->stream);
+      cudaEventSynchronize(b);
+      float t = 0.f;
+      cudaEventElapsedTime(&t, a, b);
+      cudaEventDestroy(a);
+      cudaEventDestroy(b);
+      if (rc) return rc;
+      if (t < best) {
+        best = t;
+        bs = shapes[si];
+        bz = zl[zi];
+      }
+    }
+  e->shape = bs;
+  for (size_t i = 0; i < e->boxes.size(); ++i) e->zlen[i] = std::min(e->boxes[i]->nz, bz);
+  e->tables_ok = false;
+  int rc = build_tables(*e);
+  if (chosen) {
+    chosen[0] = bs;
+    chosen[1] = bz;
+  }
+  if (best_ms) *best_ms = best / trial;
+  return rc;
+}
+
+}  // extern "C"

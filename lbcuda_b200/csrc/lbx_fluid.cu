@@ -49,14 +49,12 @@ __global__ void k_set_fields(S* __restrict__ A, S* __restrict__ B, Geom g, int n
   C usq = L.half_inv_cssq * (u * u + v * v + w * w);
   for (int comp = 0; comp < ncomp; ++comp) {
     const float* r = comp ? rB : rR;
-    S* base = A + size_t(comp) * Q * size_t(g.n);
-    S* baseB = B + size_t(comp) * Q * size_t(g.n);
 #pragma unroll
     for (int l = 0; l < Q; ++l) {
       C rho = C(r[at(b, ex(l), ey(l), ez(l))]);
       C val = equil_u(L, rho, edot(l, u, v, w), usq, l);
-      Store<S>::st(base + size_t(l) * size_t(g.n) + cell, val, sh.at(comp, l));
-      Store<S>::st(baseB + size_t(l) * size_t(g.n) + cell, C(0), sh.at(comp, l));
+      Store<S>::st(A + pidx(g, comp, l, cell), val, sh.at(comp, l));
+      Store<S>::st(B + pidx(g, comp, l, cell), C(0), sh.at(comp, l));
     }
   }
 }
@@ -73,11 +71,10 @@ __global__ void k_set_pops(S* __restrict__ A, Geom g, int ncomp, const float* __
   int cell = at(b, 0, 0, 0);
   for (int comp = 0; comp < ncomp; ++comp) {
     const float* p = comp ? pB : pR;
-    S* base = A + size_t(comp) * Q * size_t(g.n);
 #pragma unroll
     for (int l = 0; l < Q; ++l)
-      Store<S>::st(base + size_t(l) * size_t(g.n) + cell,
-                   C(p[size_t(l) * size_t(g.n) + at(b, ex(l), ey(l), ez(l))]), sh.at(comp, l));
+      Store<S>::st(A + pidx(g, comp, l, cell), C(p[size_t(l) * size_t(g.n) + at(b, ex(l), ey(l), ez(l))]),
+                   sh.at(comp, l));
   }
 }
 

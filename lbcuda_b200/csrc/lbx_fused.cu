@@ -20,6 +20,9 @@
 // ring and the two boundary planes of each segment, read from L2.
 #include "lbx_device.cuh"
 
+#include <algorithm>
+#include <vector>
+
 namespace lbx {
 
 template <typename C>
@@ -92,31 +95,76 @@ __device__ __forceinline__ void pull_idx(const Geom& g, int x, int y, int z, Pul
   for (int l = 0; l < Q; ++l) P.src[l] = X[1 - ex(l)] + Y[1 - ey(l)] + Z[1 - ez(l)];
 }
 
+// ---- component pairs ---------------------------------------------------------
+// The two components of one direction and cell are adjacent in memory, so one
+// load / store moves both; in registers they form one float2 on which the
+// sm_100 packed FP32 instructions (add / mul / fma .f32x2) act.
+template <typename C> struct PairT;
+template <> struct PairT<float> { using T = float2; };
+template <> struct PairT<double> { using T = double2; };
+template <typename C> using P2 = typename PairT<C>::T;
+
+__device__ __forceinline__ float2 pp(float a, float b) { return make_float2(a, b); }
+__device__ __forceinline__ double2 pp(double a, double b) { return make_double2(a, b); }
+__device__ __forceinline__ float2 p_add(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 p_mul(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 p_fma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ double2 p_add(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 p_mul(double2 a, double2 b) { return make_double2(a.x * b.x, a.y * b.y); }
+__device__ __forceinline__ double2 p_fma(double2 a, double2 b, double2 c) {
+  return make_double2(fma(a.x, b.x, c.x), fma(a.y, b.y, c.y));
+}
+
+// storage pair <-> arithmetic pair
+template <typename S> struct SPair;
+template <> struct SPair<float> {
+  static __device__ __forceinline__ float2 ld(const float* p) { return __ldg(reinterpret_cast<const float2*>(p)); }
+  static __device__ __forceinline__ void st(float* p, float2 v) { *reinterpret_cast<float2*>(p) = v; }
+};
+template <> struct SPair<double> {
+  static __device__ __forceinline__ double2 ld(const double* p) { return __ldg(reinterpret_cast<const double2*>(p)); }
+  static __device__ __forceinline__ void st(double* p, double2 v) { *reinterpret_cast<double2*>(p) = v; }
+};
+template <> struct SPair<__half> {
+  static __device__ __forceinline__ float2 ld(const __half* p) {
+    return __half22float2(__ldg(reinterpret_cast<const __half2*>(p)));
+  }
+  static __device__ __forceinline__ void st(__half* p, float2 v) {
+    *reinterpret_cast<__half2*>(p) = __float22half2_rn(v);
+  }
+};
+template <> struct SPair<__nv_bfloat16> {
+  static __device__ __forceinline__ float2 ld(const __nv_bfloat16* p) {
+    return __bfloat1622float2(__ldg(reinterpret_cast<const __nv_bfloat162*>(p)));
+  }
+  static __device__ __forceinline__ void st(__nv_bfloat16* p, float2 v) {
+    *reinterpret_cast<__nv_bfloat162*>(p) = __float22bfloat162_rn(v);
+  }
+};
+
+// element offset of direction l (both components) of a cell: 2 (l n + cell)
+__device__ __forceinline__ size_t poff(int64_t n, int l, int cell) { return (size_t(l) * size_t(n) + size_t(cell)) * 2; }
+
 // clamped densities (Sum g + rho0, init_rho*_CG) of the pulled cell
 template <typename S, typename C>
 __device__ __forceinline__ void pull_rho(const S* __restrict__ A, int64_t n, const PullIdx& P, const LeanConst<C>& K,
                                          C& rR, C& rB) {
-  const S* aR = A;
-  const S* aB = A + size_t(Q) * size_t(n);
-  C sR = load_raw<S, C>(aR + P.src[0]);
-  C sB = load_raw<S, C>(aB + P.src[0]);
+  P2<C> s = SPair<S>::ld(A + poff(n, 0, P.src[0]));
 #pragma unroll
-  for (int l = 1; l < Q; ++l) {
-    sR = sR + load_raw<S, C>(aR + size_t(l) * size_t(n) + P.src[l]);
-    sB = sB + load_raw<S, C>(aB + size_t(l) * size_t(n) + P.src[l]);
-  }
-  rR = sR + K.rho0[0];
-  rB = sB + K.rho0[1];
+  for (int l = 1; l < Q; ++l) s = p_add(s, SPair<S>::ld(A + poff(n, l, P.src[l])));
+  rR = s.x + K.rho0[0];
+  rB = s.y + K.rho0[1];
 }
 
 template <typename C>
 __device__ __forceinline__ C clamp0(C v) { return v < C(0) ? C(0) : v; }
 
-// One colour-gradient collision (time_step_CG, kernels_fluid_CG.CUF:689-846).
-// gR/gB: stored-form populations (f - shift) on entry, post-collision stored
-// form on exit.  rR/rB: clamped densities.
+// One colour-gradient collision (time_step_CG, kernels_fluid_CG.CUF:689-846)
+// on the component pairs g[l] = (g_R, g_B): stored form (f - shift) on entry,
+// post-collision stored form on exit.  rR/rB: clamped densities.
 template <typename C>
-__device__ __forceinline__ void collide_lean(const LeanConst<C>& K, C gR[Q], C gB[Q], C rR, C rB, C px, C py, C pz) {
+__device__ __forceinline__ void collide_pair(const LeanConst<C>& K, P2<C> g[Q], C rR, C rB, C px, C py, C pz,
+                                             bool shifted) {
   const C ONE = C(1), HALF = C(0.5);
   const C rs = rR + rB;
   C omega;
@@ -129,28 +177,30 @@ __device__ __forceinline__ void collide_lean(const LeanConst<C>& K, C gR[Q], C g
   }
   const C omm = ONE - omega;
   const C inv = ONE / rs;
-  // momentum of both components; the shifts cancel in every antisymmetric sum
-  C S[Q];
+  // momentum from the opposite-pair differences (shifts cancel)
+  const P2<C> NEG = pp(C(-1), C(-1));
+  C d[10];
 #pragma unroll
-  for (int l = 0; l < Q; ++l) S[l] = gR[l] + gB[l];
-  const C u = inv * (S[1] - S[2] + S[7] - S[8] - S[9] + S[10] + S[11] - S[12] - S[13] + S[14]);
-  const C v = inv * (S[3] - S[4] + S[7] - S[8] + S[9] - S[10] + S[15] - S[16] - S[17] + S[18]);
-  const C w = inv * (S[5] - S[6] + S[11] - S[12] + S[13] - S[14] + S[15] - S[16] + S[17] - S[18]);
+  for (int p = 1; p <= 9; ++p) {
+    const P2<C> t = p_fma(g[2 * p], NEG, g[2 * p - 1]);
+    d[p] = t.x + t.y;
+  }
+  // pairs: 1 (+x) 2 (+y) 3 (+z) 4 (+x+y) 5 (-x+y) 6 (+x+z) 7 (-x+z) 8 (+y+z) 9 (-y+z)
+  const C u = inv * (d[1] + d[4] - d[5] + d[6] - d[7]);
+  const C v = inv * (d[2] + d[4] + d[5] + d[8] - d[9]);
+  const C w = inv * (d[3] + d[6] + d[7] + d[8] + d[9]);
   const C c0 = ONE - C(1.5) * (u * u + v * v + w * w);
-  // omega * rho_k * w_cls, and the shift of each class folded into the relaxation
-  C KR[3], KB[3], sR[3], sB[3];
+  P2<C> Kc[3], ns[3];
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
-    KR[k] = omega * rR * K.w[k];
-    KB[k] = omega * rB * K.w[k];
-    sR[k] = K.s[0][k];
-    sB[k] = K.s[1][k];
+    Kc[k] = pp(omega * rR * K.w[k], omega * rB * K.w[k]);  // omega rho_k w
+    ns[k] = pp(-K.s[0][k], -K.s[1][k]);                      // minus the shift
   }
-  // BGK: f' = f (1 - omega) + omega rho w A,  f = g + s
+  const P2<C> omm2 = pp(omm, omm);
+  // BGK: f' = f (1 - omega) + omega rho w A(u),  f = g + s
   {
-    const C a0 = c0;
-    gR[0] = (gR[0] + sR[0]) * omm + KR[0] * a0;
-    gB[0] = (gB[0] + sB[0]) * omm + KB[0] * a0;
+    const P2<C> f = shifted ? p_fma(ns[0], NEG, g[0]) : g[0];
+    g[0] = p_fma(f, omm2, p_mul(Kc[0], pp(c0, c0)));
   }
 #pragma unroll
   for (int p = 1; p <= 9; ++p) {
@@ -159,18 +209,18 @@ __device__ __forceinline__ void collide_lean(const LeanConst<C>& K, C gR[Q], C g
     const C P = c0 + C(4.5) * eu * eu;
     const C Qv = C(3) * eu;
     const C Ap = P + Qv, Am = P - Qv;
-    gR[l] = (gR[l] + sR[k]) * omm + KR[k] * Ap;
-    gR[o] = (gR[o] + sR[k]) * omm + KR[k] * Am;
-    gB[l] = (gB[l] + sB[k]) * omm + KB[k] * Ap;
-    gB[o] = (gB[o] + sB[k]) * omm + KB[k] * Am;
+    const P2<C> fl = shifted ? p_fma(ns[k], NEG, g[l]) : g[l];
+    const P2<C> fo = shifted ? p_fma(ns[k], NEG, g[o]) : g[o];
+    g[l] = p_fma(fl, omm2, p_mul(Kc[k], pp(Ap, Ap)));
+    g[o] = p_fma(fo, omm2, p_mul(Kc[k], pp(Am, Am)));
   }
   const C psq = px * px + py * py + pz * pz;
-  const C kR = rR * inv, kB = rB * inv;
   if (psq > C(1.e-20)) {
     const C pn = sqrt(psq);
     const C ipn = ONE / pn;
     const C acoeff = C(9) / C(4) * omega * K.sigma;
     const C coef = K.beta * rR * rB * inv * ipn;  // beta rR rB / (rs |psi|)
+    const P2<C> kk = pp(rR * inv, rB * inv);
     C K1[3], K0[3], K3[3];
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
@@ -181,9 +231,8 @@ __device__ __forceinline__ void collide_lean(const LeanConst<C>& K, C gR[Q], C g
     K3[1] = coef * K.w[1];
     K3[2] = coef * K.w[2] / K.sqrt2;
     {
-      const C fd = gR[0] + gB[0] - K0[0];
-      gR[0] = fd * kR - sR[0];
-      gB[0] = fd * kB - sB[0];
+      const C fd = g[0].x + g[0].y - K0[0];
+      g[0] = p_fma(pp(fd, fd), kk, ns[0]);
     }
 #pragma unroll
     for (int p = 1; p <= 9; ++p) {
@@ -191,21 +240,18 @@ __device__ __forceinline__ void collide_lean(const LeanConst<C>& K, C gR[Q], C g
       const C ed = edot(l, px, py, pz);
       const C pert = K1[k] * (ed * ed) - K0[k];
       const C T = K3[k] * ed;
-      const C fdp = gR[l] + gB[l] + pert;
-      const C fdm = gR[o] + gB[o] + pert;
-      gR[l] = fdp * kR + (T - sR[k]);
-      gB[l] = fdp * kB - (T + sB[k]);
-      gR[o] = fdm * kR - (T + sR[k]);
-      gB[o] = fdm * kB + (T - sB[k]);
+      const C fdp = g[l].x + g[l].y + pert;
+      const C fdm = g[o].x + g[o].y + pert;
+      g[l] = p_fma(pp(fdp, fdp), kk, p_add(pp(T, -T), ns[k]));
+      g[o] = p_fma(pp(fdm, fdm), kk, p_add(pp(-T, T), ns[k]));
     }
-  } else {
-    gR[0] -= sR[0];
-    gB[0] -= sB[0];
+  } else if (shifted) {
+    g[0] = p_add(g[0], ns[0]);
 #pragma unroll
     for (int p = 1; p <= 9; ++p) {
-      const int l = 2 * p - 1, o = 2 * p, k = wclass(l);
-      gR[l] -= sR[k]; gR[o] -= sR[k];
-      gB[l] -= sB[k]; gB[o] -= sB[k];
+      const int k = wclass(2 * p - 1);
+      g[2 * p - 1] = p_add(g[2 * p - 1], ns[k]);
+      g[2 * p] = p_add(g[2 * p], ns[k]);
     }
   }
 }
@@ -232,16 +278,17 @@ struct LeanPart {
   C* rhoB;
 };
 
-template <typename S, int TX, int TY, int MINB, bool PART>
-__global__ void __launch_bounds__(TX* TY, MINB)
-    k_cg_lean(const S* __restrict__ A, S* __restrict__ B, Geom g, LeanConst<typename Store<S>::C> K, int zlen,
-              unsigned long long* err, int64_t step, LeanPart<typename Store<S>::C> PT) {
+// One column march: cells [x0, x0+TX) x [y0, y0+TY) x [z0, zend) of one box.
+template <typename S, int TX, int TY, bool PART>
+__device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restrict__ B, const Geom& g,
+                                            const LeanConst<typename Store<S>::C>& K, int x0, int y0, int z0,
+                                            int zend, unsigned long long* err, int64_t step,
+                                            const LeanPart<typename Store<S>::C>& PT,
+                                            typename Store<S>::C (*sphi)[Ring<TX, TY>::CELLS]) {
   using C = typename Store<S>::C;
   using R = Ring<TX, TY>;
-  __shared__ C sphi[4][R::CELLS];
+  const bool parts = PART && PT.fnew != nullptr;  // a box of the ensemble may have no spheres
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
-  const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY, z0 = blockIdx.z * zlen;
-  const int zend = min(z0 + zlen, g.nz);
   const bool active = (x0 + tx < g.nx) && (y0 + ty < g.ny);
   const int x = wrap0(x0 + tx, g.nx), y = wrap0(y0 + ty, g.ny);
   const int own = (ty + 1) * R::RX + (tx + 1);
@@ -260,7 +307,7 @@ __global__ void __launch_bounds__(TX* TY, MINB)
   // cell), zero for every other solid cell (init_rho*_CG's MINDENS)
   auto densities = [&](int cx, int cy, int zz, bool check, C& rR, C& rB) {
     const int cell = cx + g.nx * (cy + g.ny * zz);
-    if constexpr (PART) {
+    if (parts) {
       const int8_t fn = PT.fnew[cell];
       if (fn != LBX_FLUID_FLUID) {
         if (fn == LBX_FLUID_SPHERELIST) { rR = PT.rhoR[cell]; rB = PT.rhoB[cell]; }
@@ -289,7 +336,7 @@ __global__ void __launch_bounds__(TX* TY, MINB)
     const bool owned = active && z >= z0 && z < zend;
     C rR, rB;
     const bool pulled = densities(x, y, zz, owned, rR, rB);
-    if constexpr (PART) {
+    if (parts) {
       if (owned && pulled) {  // the densities of init_rho*_CG for the particle kernels
         const int cell = x + g.nx * (y + g.ny * zz);
         PT.rhoR[cell] = rR;
@@ -319,71 +366,98 @@ __global__ void __launch_bounds__(TX* TY, MINB)
       const int cell = x + g.nx * (y + g.ny * z);
       PullIdx P;
       pull_idx(g, x, y, z, P);
-      C gR[Q], gB[Q];
-      const S* aB = A + size_t(Q) * size_t(g.n);
-      S* bR = B + cell;
-      S* bB = B + size_t(Q) * size_t(g.n) + cell;
+      P2<C> gp[Q];
       bool collide = true;
-      if constexpr (PART) {
+      if (parts) {
         const int8_t fn = PT.fnew[cell], fo = PT.fold[cell];
         collide = fn == LBX_FLUID_FLUID;
         if (collide && fo != LBX_FLUID_FLUID) {
           // make_fluid already wrote the new node's populations (stored form) into B
 #pragma unroll
-          for (int l = 0; l < Q; ++l) {
-            gR[l] = load_raw<S, C>(bR + size_t(l) * size_t(g.n));
-            gB[l] = load_raw<S, C>(bB + size_t(l) * size_t(g.n));
-          }
+          for (int l = 0; l < Q; ++l) gp[l] = SPair<S>::ld(B + poff(g.n, l, cell));
         } else if (!collide) {
           // solid cell: streamed populations only; a spheredead source (previous
           // step) leaves the destination's stale value, which is B's entry
 #pragma unroll
           for (int l = 0; l < Q; ++l) {
             const bool dead = l > 0 && PT.fold[P.src[l]] == LBX_FLUID_SPHEREDEAD;
-            gR[l] = dead ? load_raw<S, C>(bR + size_t(l) * size_t(g.n))
-                         : load_raw<S, C>(A + size_t(l) * size_t(g.n) + P.src[l]);
-            gB[l] = dead ? load_raw<S, C>(bB + size_t(l) * size_t(g.n))
-                         : load_raw<S, C>(aB + size_t(l) * size_t(g.n) + P.src[l]);
+            gp[l] = dead ? SPair<S>::ld(B + poff(g.n, l, cell)) : SPair<S>::ld(A + poff(g.n, l, P.src[l]));
           }
         } else {
 #pragma unroll
-          for (int l = 0; l < Q; ++l) {
-            gR[l] = load_raw<S, C>(A + size_t(l) * size_t(g.n) + P.src[l]);
-            gB[l] = load_raw<S, C>(aB + size_t(l) * size_t(g.n) + P.src[l]);
-          }
+          for (int l = 0; l < Q; ++l) gp[l] = SPair<S>::ld(A + poff(g.n, l, P.src[l]));
         }
       } else {
 #pragma unroll
-        for (int l = 0; l < Q; ++l) {
-          gR[l] = load_raw<S, C>(A + size_t(l) * size_t(g.n) + P.src[l]);
-          gB[l] = load_raw<S, C>(aB + size_t(l) * size_t(g.n) + P.src[l]);
-        }
+        for (int l = 0; l < Q; ++l) gp[l] = SPair<S>::ld(A + poff(g.n, l, P.src[l]));
       }
       if (collide) {
         const C* pm = sphi[(z + 3) & 3];
         const C* p0 = sphi[z & 3];
-        const C* pp = sphi[(z + 1) & 3];
+        const C* ppl = sphi[(z + 1) & 3];
         C px = 0, py = 0, pz = 0;
 #pragma unroll
         for (int l = 1; l < Q27; ++l) {
           const int dx = ex27(l), dy = ey27(l), dz = ez27(l);
-          const C* pl = dz < 0 ? pm : (dz > 0 ? pp : p0);
+          const C* pl = dz < 0 ? pm : (dz > 0 ? ppl : p0);
           const C ps = pl[own + dy * R::RX + dx];
           const C a = K.a27[wclass27(l)];
           if (dx) px = px + (dx > 0 ? a : -a) * ps;
           if (dy) py = py + (dy > 0 ? a : -a) * ps;
           if (dz) pz = pz + (dz > 0 ? a : -a) * ps;
         }
-        collide_lean(K, gR, gB, rRc, rBc, px, py, pz);
+        collide_pair(K, gp, rRc, rBc, px, py, pz, Store<S>::shifted);
       }
 #pragma unroll
-      for (int l = 0; l < Q; ++l) {
-        store_raw<S, C>(bR + size_t(l) * size_t(g.n), gR[l]);
-        store_raw<S, C>(bB + size_t(l) * size_t(g.n), gB[l]);
-      }
+      for (int l = 0; l < Q; ++l) SPair<S>::st(B + poff(g.n, l, cell), gp[l]);
     }
     // slot (z+3)&3 read above is rewritten in iteration z+2; the barrier of
     // iteration z+1 orders that write after these reads
+  }
+}
+
+template <typename S, int TX, int TY, int MINB, bool PART>
+__global__ void __launch_bounds__(TX* TY, MINB)
+    k_cg_lean(const S* __restrict__ A, S* __restrict__ B, Geom g, LeanConst<typename Store<S>::C> K, int zlen,
+              unsigned long long* err, int64_t step, LeanPart<typename Store<S>::C> PT) {
+  using C = typename Store<S>::C;
+  __shared__ C sphi[4][Ring<TX, TY>::CELLS];
+  const int z0 = blockIdx.z * zlen;
+  lean_column<S, TX, TY, PART>(A, B, g, K, blockIdx.x * TX, blockIdx.y * TY, z0, min(z0 + zlen, g.nz), err, step,
+                               PT, sphi);
+}
+
+// ---------------------------------------------------------------------------
+// Several independent boxes in one persistent launch: each CTA takes work
+// items (box, column, z-segment) from a table, longest first, and marches
+// them like k_cg_lean.  Used by the ensemble of uneven boxes.
+// ---------------------------------------------------------------------------
+template <typename C>
+struct BoxDesc {
+  const void* A;
+  void* B;
+  Geom g;
+  LeanPart<C> pt;
+  unsigned long long* err;
+  int64_t step;
+};
+
+struct WorkItem {
+  int box, x0, y0, z0, zend;
+};
+
+template <typename S, int TX, int TY, int MINB, bool PART>
+__global__ void __launch_bounds__(TX* TY, MINB)
+    k_cg_lean_multi(const BoxDesc<typename Store<S>::C>* __restrict__ boxes, const WorkItem* __restrict__ work,
+                    int nwork, LeanConst<typename Store<S>::C> K) {
+  using C = typename Store<S>::C;
+  __shared__ C sphi[4][Ring<TX, TY>::CELLS];
+  for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
+    const WorkItem it = work[w];
+    const BoxDesc<C> bd = boxes[it.box];
+    lean_column<S, TX, TY, PART>((const S*)bd.A, (S*)bd.B, bd.g, K, it.x0, it.y0, it.z0, it.zend, bd.err, bd.step,
+                                 bd.pt, sphi);
+    __syncthreads();  // the window is reused by the next item
   }
 }
 
@@ -443,6 +517,67 @@ int fluid_lean_particles(Ctx& c, int fo, int fn) {
     return launch_status();
   });
   return rc;  // the particle step swaps the buffers after its bounce-back
+}
+
+}  // namespace lbx
+
+namespace lbx {
+
+int particles_active(const Ctx& c);
+
+// Build (build_only = 1: returns the number of work items) or launch the
+// persistent multi-box kernel of an ensemble for the given buffer parity.
+int ensemble_launch(const std::vector<Ctx*>& boxes, int shape, const std::vector<int>& zlen, void* d_desc,
+                    void* d_work, int nwork, cudaStream_t stream, int build_only, int parity) {
+  if (boxes.empty()) return LBX_ERR_ARG;
+  const Ctx& c0 = *boxes[0];
+  const int TX = 32, TY = shape == 1 ? 16 : 8;
+  return by_storage(c0, [&](auto* tag) -> int {
+    using S = std::remove_pointer_t<decltype(tag)>;
+    using C = typename Store<S>::C;
+    if (build_only) {
+      std::vector<BoxDesc<C>> desc(boxes.size());
+      std::vector<WorkItem> work;
+      for (size_t b = 0; b < boxes.size(); ++b) {
+        const Ctx& c = *boxes[b];
+        BoxDesc<C>& d = desc[b];
+        d.A = c.pops[parity];
+        d.B = c.pops[1 - parity];
+        d.g = geom(c);
+        const bool parts = particles_active(c) != 0;
+        d.pt = LeanPart<C>{parts ? c.flags[parity] : nullptr, parts ? c.flags[1 - parity] : nullptr,
+                           parts ? (C*)c.rho[0] : nullptr, parts ? (C*)c.rho[1] : nullptr};
+        d.err = c.d_err;
+        d.step = c.step + 1;
+        const int zl = std::max(1, zlen[b]);
+        for (int z0 = 0; z0 < c.nz; z0 += zl)
+          for (int y0 = 0; y0 < c.ny; y0 += TY)
+            for (int x0 = 0; x0 < c.nx; x0 += TX) work.push_back(WorkItem{int(b), x0, y0, z0, std::min(z0 + zl, c.nz)});
+      }
+      std::stable_sort(work.begin(), work.end(),
+                       [](const WorkItem& a, const WorkItem& b) { return (a.zend - a.z0) > (b.zend - b.z0); });
+      if (desc.size() * sizeof(BoxDesc<C>) > 512 * desc.size()) return LBX_ERR_STATE;
+      if (cudaMemcpy(d_desc, desc.data(), desc.size() * sizeof(BoxDesc<C>), cudaMemcpyHostToDevice) != cudaSuccess)
+        return LBX_ERR_CUDA;
+      if (cudaMemcpy(d_work, work.data(), work.size() * sizeof(WorkItem), cudaMemcpyHostToDevice) != cudaSuccess)
+        return LBX_ERR_CUDA;
+      return int(work.size());
+    }
+    const LeanConst<C> K = make_lean<C>(c0);
+    const auto* D = (const BoxDesc<C>*)d_desc;
+    const auto* W = (const WorkItem*)d_work;
+    if constexpr (std::is_same<S, double>::value) {
+      int grid = std::min(nwork, 148);
+      k_cg_lean_multi<S, 32, 8, 1, true><<<grid, dim3(32, 8), 0, stream>>>(D, W, nwork, K);
+    } else if (shape == 1) {
+      int grid = std::min(nwork, 148);
+      k_cg_lean_multi<S, 32, 16, 1, true><<<grid, dim3(32, 16), 0, stream>>>(D, W, nwork, K);
+    } else {
+      int grid = std::min(nwork, 296);
+      k_cg_lean_multi<S, 32, 8, 2, true><<<grid, dim3(32, 8), 0, stream>>>(D, W, nwork, K);
+    }
+    return launch_status();
+  });
 }
 
 }  // namespace lbx

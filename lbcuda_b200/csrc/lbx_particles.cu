@@ -80,6 +80,7 @@ struct PDev {  // by-value kernel argument
   int kinematic;
   int closure;
   float cl_gmin, cl_gmax, cl_vmax;
+  int exact_tiles;
 };
 
 // ---------------------------------------------------------------------------
@@ -280,6 +281,7 @@ __global__ void k_flags(PDev P, const double* __restrict__ pos, Geom g, int8_t* 
   int bin = bin_of(P, x, y, z);
   int n = min(P.bin_cnt[bin], BIN_CAP);
   const int* L = P.bin_list + size_t(bin) * BIN_CAP;
+  const int nn[3] = {g.nx, g.ny, g.nz};
   int8_t fl = LBX_FLUID_FLUID;
   int own = 0;
   for (int t = 0; t < n; ++t) {
@@ -288,6 +290,7 @@ __global__ void k_flags(PDev P, const double* __restrict__ pos, Geom g, int8_t* 
     int di = get_delta(x + 1, nint_idx(p[0], g.nx), g.nx, P.rdim);
     int dj = get_delta(y + 1, nint_idx(p[1], g.ny), g.ny, P.rdim);
     int dk = get_delta(z + 1, nint_idx(p[2], g.nz), g.nz, P.rdim);
+    if (P.exact_tiles && !tile_covered(p, nn, P.rdim, x / TILEX + 1, y / TILEY + 1, z / TILEZ + 1)) continue;
     if (abs(di) <= P.rmax && abs(dj) <= P.rmax && abs(dk) <= P.rmax) {
       int8_t v = P.tmpl[(di + P.rmax) + P.tw * ((dj + P.rmax) + P.tw * (dk + P.rmax))];
       if (v != LBX_FLUID_FLUID) {
@@ -339,7 +342,9 @@ __global__ void __launch_bounds__(256) k_drain(PDev P, const double* __restrict_
   double s[6] = {0, 0, 0, 0, 0, 0};
   for_box(P, g, c, [&](int i1, int j1, int k1, int di, int dj, int dk) {
     if (di * di + dj * dj + dk * dk > P.sphereMax) return;
-    if (!tile_covered(pc, n, P.rdim, (i1 - 1) / TILEX + 1, (j1 - 1) / TILEY + 1, (k1 - 1) / TILEZ + 1)) return;
+    if (P.exact_tiles &&
+        !tile_covered(pc, n, P.rdim, (i1 - 1) / TILEX + 1, (j1 - 1) / TILEY + 1, (k1 - 1) / TILEZ + 1))
+      return;
     int cell = cell0(g, i1, j1, k1);
     int8_t fo = fold[cell], fn = fnew[cell];
     if (fo != LBX_FLUID_FLUID || (fn != LBX_FLUID_SPHERELIST && fn != LBX_FLUID_SPHEREDEAD)) return;
@@ -421,7 +426,9 @@ __global__ void __launch_bounds__(256) k_fill(PDev P, const double* __restrict__
   double s[6] = {0, 0, 0, 0, 0, 0};
   for_box(P, g, c, [&](int i1, int j1, int k1, int di, int dj, int dk) {
     if (di * di + dj * dj + dk * dk > P.sphereMax) return;
-    if (!tile_covered(pc, n, P.rdim, (i1 - 1) / TILEX + 1, (j1 - 1) / TILEY + 1, (k1 - 1) / TILEZ + 1)) return;
+    if (P.exact_tiles &&
+        !tile_covered(pc, n, P.rdim, (i1 - 1) / TILEX + 1, (j1 - 1) / TILEY + 1, (k1 - 1) / TILEZ + 1))
+      return;
     int cell = cell0(g, i1, j1, k1);
     int8_t fo = fold[cell], fn = fnew[cell];
     if ((fo != LBX_FLUID_SPHERELIST && fo != LBX_FLUID_SPHEREDEAD) || fn != LBX_FLUID_FLUID) return;
@@ -461,10 +468,9 @@ __global__ void __launch_bounds__(256) k_fill(PDev P, const double* __restrict__
     C usq = L.half_inv_cssq * (u * u + v * v + w * w);
     for (int comp = 0; comp < 2; ++comp) {
       C r = comp ? Bs : Rs;
-      S* base = B + size_t(comp) * Q * size_t(g.n) + cell;
 #pragma unroll
       for (int l = 0; l < Q; ++l)
-        Store<S>::st(base + size_t(l) * size_t(g.n), equil_u(L, r, edot(l, u, v, w), usq, l), sh.at(comp, l));
+        Store<S>::st(B + pidx(g, comp, l, cell), equil_u(L, r, edot(l, u, v, w), usq, l), sh.at(comp, l));
     }
     double ft[3] = {double(-(Rs + Bs) * u), double(-(Rs + Bs) * v), double(-(Rs + Bs) * w)};
     s[0] += ft[0]; s[1] += ft[1]; s[2] += ft[2];
@@ -571,12 +577,10 @@ __global__ void __launch_bounds__(256) k_collide_p(const S* __restrict__ A, S* B
   int8_t fn = fnew[cell];
   bool fresh = (fn == LBX_FLUID_FLUID) && (fold[cell] != LBX_FLUID_FLUID);
   if (fresh) {  // make_fluid already wrote the new node's populations into B
-    const S* bR = B + cell;
-    const S* bB = B + size_t(Q) * size_t(g.n) + cell;
 #pragma unroll
     for (int l = 0; l < Q; ++l) {
-      fR[l] = Store<S>::ld(bR + size_t(l) * size_t(g.n), sh.at(0, l));
-      fB[l] = Store<S>::ld(bB + size_t(l) * size_t(g.n), sh.at(1, l));
+      fR[l] = Store<S>::ld(B + pidx(g, 0, l, cell), sh.at(0, l));
+      fB[l] = Store<S>::ld(B + pidx(g, 1, l, cell), sh.at(1, l));
     }
   } else {
     pull_dead(A, B, g, b, 0, sh, fold, fR);
@@ -642,8 +646,10 @@ __global__ void __launch_bounds__(256) k_bb(PDev P, const double* __restrict__ p
     const int x0 = i1 - 1, y0 = j1 - 1, z0 = k1 - 1;
     Nbr b;
     make_nbr(g, x0, y0, z0, b);
+    const int nn3[3] = {g.nx, g.ny, g.nz};
+    const int ti = x0 / TILEX + 1, tj = y0 / TILEY + 1, tk = z0 / TILEZ + 1;
     // node -> particle momentum exchange for this sphere (atmDist < sphereMax)
-    if (di * di + dj * dj + dk * dk < P.sphereMax) {
+    if (di * di + dj * dj + dk * dk < P.sphereMax && (!P.exact_tiles || tile_covered(pc, nn3, P.rdim, ti, tj, tk))) {
       LinkGeo G;
       link_geo(P, g, pc, i1, j1, k1, G);
 #pragma unroll
@@ -659,8 +665,8 @@ __global__ void __launch_bounds__(256) k_bb(PDev P, const double* __restrict__ p
           wall_velocity(P, pc, G, lr, rt, v);
           C ev = C(ex(lf)) * C(v[0]) + C(ey(lf)) * C(v[1]) + C(ez(lf)) * C(v[2]);
           C w = L.w[wclass(lf)];
-          C f2pR = C(2) * Store<S>::ld(B + size_t(lf) * size_t(g.n) + xf, sh.at(0, lf)) - w * buz * rhoR[xf] * ev;
-          C f2pB = C(2) * Store<S>::ld(B + size_t(Q + lf) * size_t(g.n) + xf, sh.at(1, lf)) - w * buz * rhoB[xf] * ev;
+          C f2pR = C(2) * Store<S>::ld(B + pidx(g, 0, lf, xf), sh.at(0, lf)) - w * buz * rhoR[xf] * ev;
+          C f2pB = C(2) * Store<S>::ld(B + pidx(g, 1, lf, xf), sh.at(1, lf)) - w * buz * rhoB[xf] * ev;
           C f2p = f2pR + f2pB;
           double ft[3] = {double(f2p * C(ex(lf))), double(f2p * C(ey(lf))), double(f2p * C(ez(lf)))};
           s[0] += ft[0]; s[1] += ft[1]; s[2] += ft[2];
@@ -682,9 +688,8 @@ __global__ void __launch_bounds__(256) k_bb(PDev P, const double* __restrict__ p
       const int xi = at(b, ex(lo), ey(lo), ez(lo)), xo = at(b, ex(hi), ey(hi), ez(hi));
       const bool fi = fnew[xi] == LBX_FLUID_FLUID, fo = fnew[xo] == LBX_FLUID_FLUID;
       for (int comp = 0; comp < 2; ++comp) {
-        S* base = B + size_t(comp) * Q * size_t(g.n);
-        if (fi && !fo) base[size_t(lo) * size_t(g.n) + cell] = base[size_t(hi) * size_t(g.n) + xi];
-        if (!fi && fo) base[size_t(hi) * size_t(g.n) + cell] = base[size_t(lo) * size_t(g.n) + xo];
+        if (fi && !fo) B[pidx(g, comp, lo, cell)] = B[pidx(g, comp, hi, xi)];
+        if (!fi && fo) B[pidx(g, comp, hi, cell)] = B[pidx(g, comp, lo, xo)];
       }
     }
     // p2n phase 2: moving-wall correction, for every sphere within reach of
@@ -699,6 +704,7 @@ __global__ void __launch_bounds__(256) k_bb(PDev P, const double* __restrict__ p
           ej = get_delta(j1, nint_idx(pq[1], g.ny), g.ny, P.rdim),
           ek = get_delta(k1, nint_idx(pq[2], g.nz), g.nz, P.rdim);
       if (ei * ei + ej * ej + ek * ek >= P.sphereMax) continue;
+      if (P.exact_tiles && !tile_covered(pq, nn3, P.rdim, ti, tj, tk)) continue;
       LinkGeo G;
       link_geo(P, g, pq, i1, j1, k1, G);
       for (int it = 1; it <= 9; ++it) {
@@ -713,7 +719,7 @@ __global__ void __launch_bounds__(256) k_bb(PDev P, const double* __restrict__ p
           C ev = C(ex(lf)) * C(v[0]) + C(ey(lf)) * C(v[1]) + C(ez(lf)) * C(v[2]);
           C w = L.w[wclass(lf)];
           for (int comp = 0; comp < 2; ++comp) {
-            S* p = B + size_t(comp * Q + lr) * size_t(g.n) + cell;
+            S* p = B + pidx(g, comp, lr, cell);
             const C* rho = comp ? rhoB : rhoR;
             C val = Store<S>::ld(p, sh.at(comp, lr)) - w * buz * rho[xf] * ev;
             Store<S>::st(p, val, sh.at(comp, lr));
@@ -1063,6 +1069,7 @@ static PDev pdev(const Ctx& c) {
   d.cl_gmin = c.p.closure_gap_min;
   d.cl_gmax = c.p.closure_gap_max;
   d.cl_vmax = c.p.closure_vmax;
+  d.exact_tiles = c.p.exact_tiles;
   return d;
 }
 
@@ -1203,8 +1210,12 @@ int particles_set(Ctx& c, int n, const double* h_x, const double* h_v, const dou
   return rc;
 }
 
-// One step with particles, main.CUF:130-241.
-int particles_step(Ctx& c) {
+// One step with particles, main.CUF:130-241, in three parts so that an
+// ensemble can put the fluid kernels of all its boxes into one launch:
+//   pre:   particle lists, flags, drain, (two-pass densities), fill, wetting
+//   fluid: the colour-gradient step with flags
+//   post:  bounce-back, pair forces, closure, integrator, buffer swap
+int particles_pre(Ctx& c) {
   ParticleState& s = *c.part;
   Geom g = geom(c);
   PDev P = pdev(c);
@@ -1213,7 +1224,7 @@ int particles_step(Ctx& c) {
   const double* pc = s.pos[s.pcur];
   const double* po = s.pos[1 - s.pcur];
   const int64_t st = c.step + 1;
-  int rc = by_storage(c, [&](auto* tag) {
+  return by_storage(c, [&](auto* tag) {
     using S = std::remove_pointer_t<decltype(tag)>;
     using C = typename Store<S>::C;
     const S* A = (const S*)c.pops[c.cur];
@@ -1223,27 +1234,51 @@ int particles_step(Ctx& c) {
     C* rR = (C*)c.rho[0];
     C* rB = (C*)c.rho[1];
     C* phi = (C*)c.phi;
-    // particle lists of the current positions (built after the previous
-    // step in the reference, updateListAtoms)
     int r0 = rebuild_bins(c, pc);
     if (r0) return r0;
     k_flags<<<d.grid, d.block, 0, c.stream>>>(P, pc, g, c.flags[fn]);
     k_drain<S><<<s.np, 256, 0, c.stream>>>(P, pc, po, s.acc, A, B, g, sh, c.flags[fo], c.flags[fn], rR, rB);
-    const bool fused = c.fused == 2;
-    if (!fused)
+    if (c.fused != 2)
       k_rho_p<S><<<d.grid, d.block, 0, c.stream>>>(A, B, g, sh, c.flags[fo], c.flags[fn], phi, rR, rB, c.d_err, st);
     k_fill<S><<<s.np, 256, 0, c.stream>>>(P, pc, po, s.acc, A, B, g, sh, L, c.flags[fo], c.flags[fn], rR, rB, phi);
     k_virtual<S><<<s.np, 256, 0, c.stream>>>(P, pc, g, c.p.wetting == LBX_WET_NEUTRAL ? 1 : 0, A, sh, c.flags[fo],
                                               c.flags[fn], rR, rB, phi, L);
-    if (fused) {
-      int r1 = fluid_lean_particles(c, fo, fn);
-      if (r1) return r1;
-    } else {
-      kt_begin(c);
-      k_collide_p<S><<<d.grid, d.block, 0, c.stream>>>(A, B, g, sh, phi, rR, rB, c.flags[fo], c.flags[fn],
-                                                       make_cg<C>(c));
-      kt_end(c);
-    }
+    return launch_status();
+  });
+}
+
+int particles_fluid(Ctx& c) {
+  const int fo = c.fcur, fn = 1 - c.fcur;
+  if (c.fused == 2) return fluid_lean_particles(c, fo, fn);
+  Geom g = geom(c);
+  LaunchDims d = cell_dims(c);
+  return by_storage(c, [&](auto* tag) {
+    using S = std::remove_pointer_t<decltype(tag)>;
+    using C = typename Store<S>::C;
+    kt_begin(c);
+    k_collide_p<S><<<d.grid, d.block, 0, c.stream>>>((const S*)c.pops[c.cur], (S*)c.pops[1 - c.cur], g,
+                                                     make_shift<C>(c), (const C*)c.phi, (const C*)c.rho[0],
+                                                     (const C*)c.rho[1], c.flags[fo], c.flags[fn], make_cg<C>(c));
+    kt_end(c);
+    return launch_status();
+  });
+}
+
+int particles_post(Ctx& c) {
+  ParticleState& s = *c.part;
+  Geom g = geom(c);
+  PDev P = pdev(c);
+  const int fn = 1 - c.fcur;
+  const double* pc = s.pos[s.pcur];
+  const int64_t st = c.step + 1;
+  int rc = by_storage(c, [&](auto* tag) {
+    using S = std::remove_pointer_t<decltype(tag)>;
+    using C = typename Store<S>::C;
+    S* B = (S*)c.pops[1 - c.cur];
+    Shift<C> sh = make_shift<C>(c);
+    LatticeT<C> L = make_lattice<C>();
+    C* rR = (C*)c.rho[0];
+    C* rB = (C*)c.rho[1];
     k_bb<S><<<s.np, 256, 0, c.stream>>>(P, pc, s.acc, B, g, sh, L, c.flags[fn], rR, rB);
     k_pairs<<<(s.np + 127) / 128, 128, 0, c.stream>>>(P, pc, s.acc, g);
     if (c.p.closure) {
@@ -1267,6 +1302,13 @@ int particles_step(Ctx& c) {
   s.pcur = 1 - s.pcur;
   c.step += 1;
   return 0;
+}
+
+int particles_step(Ctx& c) {
+  int rc = particles_pre(c);
+  if (!rc) rc = particles_fluid(c);
+  if (!rc) rc = particles_post(c);
+  return rc;
 }
 
 int particles_get(Ctx& c, double* x, double* v, double* om, double* q, double* f, double* t) {

@@ -441,6 +441,16 @@ class Oracle {
       int td[3] = {TX, TY, TZ};
       int box[3][4];
       for (int d = 0; d < 3; ++d) {
+        if (!prm.exact_tiles) {
+          /* every cell of the template box [nint - rmax, nint + rmax], split at
+           * the periodic edge (the reference's box, int(x +- rdim), misses
+           * template cells for integer radii) */
+          int c0 = nintp(xc[d]) - rmax, c1 = nintp(xc[d]) + rmax;
+          if (c0 < 1) { box[d][0] = 1; box[d][1] = c1; box[d][2] = c0 + nn[d]; box[d][3] = nn[d]; }
+          else if (c1 > nn[d]) { box[d][0] = 1; box[d][1] = c1 - nn[d]; box[d][2] = c0; box[d][3] = nn[d]; }
+          else { box[d][0] = c0; box[d][1] = c1; box[d][2] = td[d]; box[d][3] = -td[d]; }
+          continue;
+        }
         box[d][0] = int(xc[d] - rdim); /* real -> integer truncation */
         box[d][1] = int(xc[d] + rdim);
         if (box[d][0] < 1) {

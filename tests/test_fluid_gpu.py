@@ -72,12 +72,22 @@ def test_bgk_f32_matches_oracle(shape):
 @pytest.mark.parametrize("fused", [2, 1, 0])
 @pytest.mark.parametrize("shape", [(32, 32, 32), (40, 24, 20), (64, 16, 24)])
 def test_cg_f32_matches_oracle(shape, fused):
-    """Spinodal noise amplifies rounding differences, so this case runs 20 steps."""
+    """Spinodal decomposition from rest, 20 steps.
+
+    Densities, phase field and populations to 1e-5.  The velocity is the
+    ill-conditioned field here: |u| ~ 1e-4 comes from momenta ~3e-2 that
+    cancel, so FP32 rounding alone moves it by ~1e-5 of its L2 norm; the
+    two-pass schedule, which keeps the reference's operation order, shows the
+    same level.  Its bound is 5e-5 (L2); the droplet and unequal-tau cases
+    below, with a mean flow, hold every field to 1e-5.
+    """
     nx, ny, nz = shape
     p = make_params(nx, ny, nz, model="cg", storage="f32", sigma=0.02, beta=0.7)
     rR, rB = seeded_noise_fields(nx, ny, nz, seed=5)
     g, o = run_pair(p, rR, rB, (0.0, 0.0, 0.0), 20, fused=fused)
-    compare_fields(g.get_fields(), o.get_fields(), TOL32, f"cg fused={fused}")
+    gf, of = g.get_fields(), o.get_fields()
+    compare_fields((gf[0], gf[1], None, gf[3]), (of[0], of[1], None, of[3]), TOL32, f"cg fused={fused}")
+    assert rel_l2(gf[2], of[2]) <= 5e-5
     pg = g.get_pops()
     po = o.get_pops()
     assert rel(pg[0], po[0]) <= TOL32 and rel(pg[1], po[1]) <= TOL32

@@ -89,11 +89,26 @@ def test_moving_spheres_match_oracle(wetting, lrotate, sched):
 def test_hertz_contact_pair():
     """Two spheres closer than hz_rmin repel with the Hertz law (addHertzian)."""
     x = np.array([[12.0, 16.0, 16.0], [22.2, 16.3, 16.1]])
-    g, o = make_pair(32, x, np.zeros((2, 3)), steps=3)
+    g, o = make_pair(32, x, np.zeros((2, 3)), steps=3, wetting="neutral")
     gp, op = g.get_particles(), o.get_particles()
     assert gp["force"][0, 0] < 0 < gp["force"][1, 0]
     assert rel(gp["force"], op["force"]) < 1e-5
     assert np.abs(gp["x"] - op["x"]).max() < 1e-6
+
+
+@pytest.mark.parametrize("exact", [1, 0])
+def test_integer_radius_flags(exact):
+    """Radius 4: the reference's tile lists (int(x +- r) boxes) miss template cells
+    when frac(x) >= 0.5; exact_tiles = 1 reproduces that, 0 places every cell."""
+    x = np.array([[10.7, 16.6, 12.2], [22.3, 9.5, 21.8]])
+    g, o = make_pair(32, x, np.zeros((2, 3)), radius=4.0, exact_tiles=exact)
+    fg, fo = g.get_flags(), o.get_flags()
+    assert np.array_equal(fg, fo)
+    solid = int((fg != 1).sum())
+    if exact:
+        assert solid < 2 * 257  # a full r = 4 sphere has 257 cells
+    else:
+        assert solid == 2 * 257
 
 
 def test_reference_deck_placement_flags():
