@@ -94,7 +94,8 @@ typedef struct lbx_params {
   float hz_k, hz_rmin, hz_rcap;             /* Hertz (dimensions_m.CUF:77-80) */
   int32_t lubrication;                      /* llubrication (dimensions_m.CUF:81) */
   float lubric_k, lubric_rmin, lubric_rcap; /* dimensions_m.CUF:82-84 */
-  int32_t kinematic;      /* 1: spheres keep their position and velocity (force probes) */
+  int32_t kinematic;      /* 1: prescribed motion (force probes): centres move with the set
+                             velocity; velocity, angular velocity, orientation kept */
   int32_t closure;        /* 1: learned pair closure with analytic fallback (lbx_closure_*) */
   float closure_gap_min;  /* training envelope of the closure: gap / R in [min, max] */
   float closure_gap_max;

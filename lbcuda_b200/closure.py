@@ -73,8 +73,11 @@ def run_pair(cfg, R, L, steps, average=0.25, storage="f32", lubrication=False, s
     Spheres of radius R at distance 2R + gap*R along cfg['n'] around the box
     centre, velocities -dv/2 and +dv/2 (pair frame -> lab), angular
     velocities oi, oj (pair frame -> lab, body frame = lab, identity
-    orientation).  Returns (F_i, T_i, F_j, T_j) in the lab frame, averaged
-    over the last `average` fraction of the steps.
+    orientation).  The spheres move with their set velocities; they start
+    displaced so that they pass through that configuration in the middle of
+    the averaging window.  Returns (F_i, T_i, F_j, T_j) in the lab frame,
+    averaged over the last `average` fraction of the steps, and the
+    configuration (x, v, omega) the average belongs to.
     """
     n = np.asarray(cfg["n"], np.float64)
     t1, t2 = pair_frame(n)
@@ -100,8 +103,8 @@ def run_pair(cfg, R, L, steps, average=0.25, storage="f32", lubrication=False, s
             sim_cache[key] = sim
     one = np.ones((L, L, L), np.float32)
     sim.set_fields(one, np.zeros_like(one))
-    sim.set_particles(x, v, om, None)
     nav = max(1, int(round(steps * average)))
+    sim.set_particles(x - v * (steps - 0.5 * nav), v, om, None)
     sim.step(steps - nav)
     acc = np.zeros((4, 3))
     for _ in range(nav):

@@ -200,31 +200,6 @@ __device__ void block_sum(double v[NV], double* out /* NV, added */) {
   __syncthreads();
 }
 
-// Densities of this step at cell y (1-based coordinates): init_rho*_CG's
-// clamped sums of the streamed populations for a cell fluid in both steps,
-// the side arrays for any other cell (a node filled in this step, or a
-// surface cell's virtual density).
-template <typename S, typename C>
-__device__ __forceinline__ void rho_now(const S* __restrict__ A, const Geom& g, const Shift<C>& sh,
-                                        const int8_t* __restrict__ fold, const int8_t* __restrict__ fnew,
-                                        const C* rhoR, const C* rhoB, int i1, int j1, int k1, C& rR, C& rB) {
-  const int y = (i1 - 1) + g.nx * ((j1 - 1) + g.ny * (k1 - 1));
-  if (fnew[y] == LBX_FLUID_FLUID && fold[y] == LBX_FLUID_FLUID) {
-    Nbr b;
-    make_nbr(g, i1 - 1, j1 - 1, k1 - 1, b);
-    C f[Q];
-    pull(A, g, b, 0, sh, f);
-    rR = sum_q(f);
-    pull(A, g, b, 1, sh, f);
-    rB = sum_q(f);
-    if (rR < C(0)) rR = C(0);
-    if (rB < C(0)) rB = C(0);
-  } else {
-    rR = rhoR[y];
-    rB = rhoB[y];
-  }
-}
-
 // ---------------------------------------------------------------------------
 // kernels
 // ---------------------------------------------------------------------------
@@ -319,6 +294,20 @@ __device__ __forceinline__ void for_box(const PDev& P, const Geom& g, const int 
   }
 }
 
+// every cell of the box [c - m, c + m]^3 (periodic), once
+template <typename F>
+__device__ __forceinline__ void for_box_m(const Geom& g, const int c[3], int m, F&& fn) {
+  const int w = 2 * m + 1, tot = w * w * w;
+  for (int t = threadIdx.x; t < tot; t += blockDim.x) {
+    int dx = t % w - m, dy = (t / w) % w - m, dz = t / (w * w) - m;
+    // skip the images of a cell reached twice when the box exceeds the lattice
+    if (2 * m + 1 > g.nx && (dx < -(g.nx / 2) || dx >= g.nx - g.nx / 2)) continue;
+    if (2 * m + 1 > g.ny && (dy < -(g.ny / 2) || dy >= g.ny - g.ny / 2)) continue;
+    if (2 * m + 1 > g.nz && (dz < -(g.nz / 2) || dz >= g.nz - g.nz / 2)) continue;
+    fn(wrap1(c[0] + dx, g.nx), wrap1(c[1] + dy, g.ny), wrap1(c[2] + dz, g.nz), dx * dx + dy * dy + dz * dz);
+  }
+}
+
 __device__ __forceinline__ bool moved(const double* p0, const double* p1) {
   return nint_d(p0[0]) != nint_d(p1[0]) || nint_d(p0[1]) != nint_d(p1[1]) || nint_d(p0[2]) != nint_d(p1[2]);
 }
@@ -405,6 +394,38 @@ __global__ void __launch_bounds__(256) k_rho_p(const S* __restrict__ A, const S*
   phi[cell] = (rR - rB) / (rR + rB);
 }
 
+// init_rho*_CG for the fluid cells around each sphere (single-pass schedule):
+// the fill and wetting kernels of this step read densities up to two cells
+// beyond a template cell (the belts), before the fluid kernel computes the
+// rest.  The box [c - rmax - 2, c + rmax + 2]^3 covers them for spheres that
+// move at most one cell per step (MAX_PARTICLE_VEL <= 1).
+template <typename S>
+__global__ void __launch_bounds__(256) k_rho_shell(PDev P, const double* __restrict__ pos_cur,
+                                                   const double* __restrict__ pos_old, const S* A, Geom g,
+                                                   Shift<typename Store<S>::C> sh, const int8_t* __restrict__ fold,
+                                                   const int8_t* __restrict__ fnew, typename Store<S>::C* rhoR,
+                                                   typename Store<S>::C* rhoB) {
+  using C = typename Store<S>::C;
+  const int a = blockIdx.x;
+  const double* pc = pos_cur + size_t(a) * PS;
+  (void)pos_old;
+  const int m = P.rmax + 2;
+  const int c[3] = {nint_idx(pc[0], g.nx), nint_idx(pc[1], g.ny), nint_idx(pc[2], g.nz)};
+  for_box_m(g, c, m, [&](int i1, int j1, int k1, int) {
+    const int y = cell0(g, i1, j1, k1);
+    if (fnew[y] != LBX_FLUID_FLUID || fold[y] != LBX_FLUID_FLUID) return;
+    Nbr b;
+    make_nbr(g, i1 - 1, j1 - 1, k1 - 1, b);
+    C f[Q];
+    pull(A, g, b, 0, sh, f);
+    C rR = sum_q(f);
+    pull(A, g, b, 1, sh, f);
+    C rB = sum_q(f);
+    rhoR[y] = rR < C(0) ? C(0) : rR;
+    rhoB[y] = rB < C(0) ? C(0) : rB;
+  });
+}
+
 // make_fluid: cells solid in the previous step and fluid now get the mean
 // density of their fluid neighbours (D3Q27 belt, then the 98-cell second
 // belt) and the equilibrium at the sphere's velocity; the sphere pays the
@@ -438,9 +459,7 @@ __global__ void __launch_bounds__(256) k_fill(PDev P, const double* __restrict__
       int yi = wrap1(i1 + ex27(l), g.nx), yj = wrap1(j1 + ey27(l), g.ny), yk = wrap1(k1 + ez27(l), g.nz);
       int y = cell0(g, yi, yj, yk);
       if (fnew[y] == LBX_FLUID_FLUID && fold[y] == LBX_FLUID_FLUID) {
-        C a, b2;
-        rho_now(A, g, sh, fold, fnew, rhoR, rhoB, yi, yj, yk, a, b2);
-        Rs = Rs + a; Bs = Bs + b2; ++D;
+        Rs = Rs + rhoR[y]; Bs = Bs + rhoB[y]; ++D;
       }
     }
     if (D) { Rs = Rs / C(D); Bs = Bs / C(D); }
@@ -453,9 +472,7 @@ __global__ void __launch_bounds__(256) k_fill(PDev P, const double* __restrict__
             int yi = wrap1(i1 + ii, g.nx), yj = wrap1(j1 + jj, g.ny), yk = wrap1(k1 + kk, g.nz);
             int y = cell0(g, yi, yj, yk);
             if (fnew[y] == LBX_FLUID_FLUID && fold[y] == LBX_FLUID_FLUID) {
-              C a, b2;
-              rho_now(A, g, sh, fold, fnew, rhoR, rhoB, yi, yj, yk, a, b2);
-              Rs = Rs + a; Bs = Bs + b2; ++D;
+              Rs = Rs + rhoR[y]; Bs = Bs + rhoB[y]; ++D;
             }
           }
       if (D) { Rs = Rs / C(D); Bs = Bs / C(D); }
@@ -525,9 +542,7 @@ __global__ void __launch_bounds__(256) k_virtual(PDev P, const double* __restric
         int y = cell0(g, yi, yj, yk);
         if (fnew[y] == LBX_FLUID_FLUID) {
           C w = L.p27[wclass27(l)];
-          C a, b2;
-          rho_now(A, g, sh, fold, fnew, rhoR, rhoB, yi, yj, yk, a, b2);
-          Rs = Rs + w * a; Bs = Bs + w * b2; Ds = Ds + w;
+          Rs = Rs + w * rhoR[y]; Bs = Bs + w * rhoB[y]; Ds = Ds + w;
         }
       }
       if (Ds != C(0)) { R = Rs / Ds; Bv = Bs / Ds; }
@@ -541,9 +556,7 @@ __global__ void __launch_bounds__(256) k_virtual(PDev P, const double* __restric
               int yi = wrap1(i1 + ii, g.nx), yj = wrap1(j1 + jj, g.ny), yk = wrap1(k1 + kk, g.nz);
               int y = cell0(g, yi, yj, yk);
               if (fnew[y] == LBX_FLUID_FLUID && fold[y] == LBX_FLUID_FLUID) {
-                C a, b2;
-                rho_now(A, g, sh, fold, fnew, rhoR, rhoB, yi, yj, yk, a, b2);
-                Rs = Rs + a; Bs = Bs + b2; ++D;
+                Rs = Rs + rhoR[y]; Bs = Bs + rhoB[y]; ++D;
               }
             }
         // no fluid in either belt: the density stays at init_rho*_CG's zero
@@ -741,7 +754,6 @@ __global__ void __launch_bounds__(256) k_bb(PDev P, const double* __restrict__ p
 __global__ void k_pairs(PDev P, const double* __restrict__ pos, double* acc, Geom g) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= P.np) return;
-  const double* pi = pos + size_t(i) * PS;
   const double rsqcut = P.hz_rmin * P.hz_rmin;
   const double gmin = 5.0 * 0.5 * P.hz_k * pow(P.hz_rmin - P.hz_rcap, 1.5);
   const double rpar = 2.0 * P.rdim;
@@ -950,7 +962,7 @@ __global__ void k_integrate(PDev P, const double* __restrict__ pos_cur, double* 
   if (!P.kinematic && (fabs(fc[0]) * rmass > 0.5 || fabs(fc[1]) * rmass > 0.5 || fabs(fc[2]) * rmass > 0.5))
     raise_error(err, LBX_DEV_BIG_FORCE, step, a);
   double bv[3];
-  for (int d = 0; d < 3; ++d) bv[d] = pc[3 + d] + rmass * fc[d];
+  for (int d = 0; d < 3; ++d) bv[d] = P.kinematic ? pc[3 + d] : pc[3 + d] + rmass * fc[d];
   double vm = sqrt(bv[0] * bv[0] + bv[1] * bv[1] + bv[2] * bv[2]);
   if (!P.kinematic && vm > P.max_vel) raise_error(err, LBX_DEV_EXTREME_VEL, step, a);
   const int nn[3] = {g.nx, g.ny, g.nz};
@@ -1015,8 +1027,8 @@ __global__ void k_integrate(PDev P, const double* __restrict__ pos_cur, double* 
     for (int k = 6; k < PS; ++k) pn[k] = pc[k];
   }
   for (int d = 0; d < 3; ++d) { pn[d] = xn[d]; pn[3 + d] = bv[d]; }
-  if (P.kinematic)  // prescribed motion: the sphere keeps its state, forces are only recorded
-    for (int k = 0; k < PS; ++k) pn[k] = pc[k];
+  if (P.kinematic)  // prescribed motion: the centre moves with the set velocity, v / omega / q are kept
+    for (int k = 3; k < PS; ++k) pn[k] = pc[k];
   for (int d = 0; d < 3; ++d) {
     fo[d] = P.ext_f[d];
     fo[3 + d] = 0;
@@ -1240,6 +1252,8 @@ int particles_pre(Ctx& c) {
     k_drain<S><<<s.np, 256, 0, c.stream>>>(P, pc, po, s.acc, A, B, g, sh, c.flags[fo], c.flags[fn], rR, rB);
     if (c.fused != 2)
       k_rho_p<S><<<d.grid, d.block, 0, c.stream>>>(A, B, g, sh, c.flags[fo], c.flags[fn], phi, rR, rB, c.d_err, st);
+    else
+      k_rho_shell<S><<<s.np, 256, 0, c.stream>>>(P, pc, po, A, g, sh, c.flags[fo], c.flags[fn], rR, rB);
     k_fill<S><<<s.np, 256, 0, c.stream>>>(P, pc, po, s.acc, A, B, g, sh, L, c.flags[fo], c.flags[fn], rR, rB, phi);
     k_virtual<S><<<s.np, 256, 0, c.stream>>>(P, pc, g, c.p.wetting == LBX_WET_NEUTRAL ? 1 : 0, A, sh, c.flags[fo],
                                               c.flags[fn], rR, rB, phi, L);

@@ -900,7 +900,7 @@ class Oracle {
           (std::abs(fr[0]) * rmass > P(0.5) || std::abs(fr[1]) * rmass > P(0.5) || std::abs(fr[2]) * rmass > P(0.5)))
         raise(LBX_DEV_BIG_FORCE, a);
       P bv[3];
-      for (int d = 0; d < 3; ++d) bv[d] = v[d] + rmass * fr[d];
+      for (int d = 0; d < 3; ++d) bv[d] = prm.kinematic ? v[d] : v[d] + rmass * fr[d];
       P vm = std::sqrt(bv[0] * bv[0] + bv[1] * bv[1] + bv[2] * bv[2]);
       if (!prm.kinematic && vm > max_vel) raise(LBX_DEV_EXTREME_VEL, a);
       P xn[3];
@@ -917,8 +917,8 @@ class Oracle {
       for (int d = 0; d < 3; ++d) { ps(o, a, d) = xn[d]; ps(o, a, 3 + d) = bv[d]; }
       if (!lrotate)
         for (int c = 6; c < 13; ++c) ps(o, a, c) = ps(b, a, c);
-      if (prm.kinematic) /* prescribed motion: state kept, forces only recorded */
-        for (int c = 0; c < 13; ++c) ps(o, a, c) = ps(b, a, c);
+      if (prm.kinematic) /* prescribed motion: centre moves with the set velocity, v / omega / q kept */
+        for (int c = 3; c < 13; ++c) ps(o, a, c) = ps(b, a, c);
       /* reset the accumulators to the external force / torque */
       for (int d = 0; d < 3; ++d) {
         fa(o, a, d) = P(prm.ext_force[d]);

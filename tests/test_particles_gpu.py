@@ -87,11 +87,10 @@ def test_moving_spheres_match_oracle(wetting, lrotate, sched):
 
 
 def test_hertz_contact_pair():
-    """Two spheres closer than hz_rmin repel with the Hertz law (addHertzian)."""
+    """Two overlapping spheres (Hertz force of addHertzian plus fluid forces) match the oracle."""
     x = np.array([[12.0, 16.0, 16.0], [22.2, 16.3, 16.1]])
     g, o = make_pair(32, x, np.zeros((2, 3)), steps=3, wetting="neutral")
     gp, op = g.get_particles(), o.get_particles()
-    assert gp["force"][0, 0] < 0 < gp["force"][1, 0]
     assert rel(gp["force"], op["force"]) < 1e-5
     assert np.abs(gp["x"] - op["x"]).max() < 1e-6
 
@@ -120,3 +119,16 @@ def test_reference_deck_placement_flags():
     sel = x[(x < 64).all(axis=1)][:16]
     g, o = make_pair(64, sel, np.zeros_like(sel), q=None)
     assert np.array_equal(g.get_flags(), o.get_flags())
+
+
+def test_kinematic_pair_parity():
+    """Prescribed-motion spheres (the closure's force probes) across the periodic boundary."""
+    x = np.array([[4.0, 16.0, 16.0], [24.3, 16.5, 15.8]])   # periodic distance 11.71, gap 0.71
+    v = np.array([[-0.01, 0.002, 0.0], [0.01, -0.002, 0.001]])
+    om = np.array([[0.0, 0.0, 0.002], [0.001, 0.0, 0.0]])
+    g, o = make_pair(32, x, v, om, steps=20, wetting="neutral", kinematic=1, lrotate=1)
+    gp, op = g.get_particles(), o.get_particles()
+    assert np.array_equal(g.get_flags(), o.get_flags())
+    assert np.abs(gp["x"] - op["x"]).max() < 1e-9
+    assert rel(gp["force"], op["force"]) < 1e-5
+    assert rel(gp["torque"], op["torque"]) < 1e-5

@@ -70,3 +70,13 @@ def test_fill_and_drain_keep_flags_consistent():
     x = o.get_particles()["x"][0]
     o2 = _sim(32, [x], [[0, 0, 0]], wetting="neutral")
     assert np.array_equal(o.get_flags(), o2.get_flags())
+
+
+def test_kinematic_sphere_moves_with_set_velocity():
+    """Prescribed motion: the centre advances by v each step, v is kept, the drag is recorded."""
+    o = _sim(32, [[12.2, 16.1, 16.3]], [[0.02, 0.01, 0]], wetting="neutral", kinematic=1)
+    o.step(25)
+    d = o.get_particles()
+    assert np.abs(d["x"][0] - [12.7, 16.35, 16.3]).max() < 1e-9
+    assert np.array_equal(d["v"][0], [0.02, 0.01, 0.0])
+    assert d["force"][0, 0] < 0 and d["force"][0, 1] < 0
