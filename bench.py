@@ -193,7 +193,7 @@ COLLOID_N = 1280
 
 
 def colloid_sim(storage, schedule=2):
-    """256^3 CG fluid with 1280 spheres of radius 5.5 (the first 1280 of the
+    """Colloid workload: 256^3 CG fluid with 1280 spheres of radius 5.5 (the first 1280 of the
     reference's Tests/07-1280-Particle placement), density 1, neutral wetting, at rest."""
     from lbcuda_b200 import LBSim, make_params
     from lbcuda_b200.inputs import read_input_xyz, seeded_noise_fields

@@ -55,7 +55,7 @@ def features(xi, xj, vi, vj, oi, oj, R, box):
     return np.concatenate([[(r - 2 * R) / R], dv, F @ np.asarray(oi), F @ np.asarray(oj), [R]]), F
 
 
-def sample_configs(n, seed=0, gap_range=(0.05, 4.0), vmax=1e-3):
+def sample_configs(n, seed=0, gap_range=(0.05, 1.5), vmax=1e-3):
     """gap/R log-uniform, pair-frame relative velocity and both angular velocities uniform in +-vmax."""
     rng = np.random.Generator(np.random.PCG64(seed))
     gaps = np.exp(rng.uniform(np.log(gap_range[0]), np.log(gap_range[1]), n))
@@ -114,12 +114,19 @@ def run_pair(cfg, R, L, steps, average=0.25, storage="f32", lubrication=False, s
     return acc / nav, x, v, om
 
 
-def generate(n_samples, R_hi=12, L_hi=96, R_lo=3, steps_hi=300, seed=0, progress=None):
-    """(X, T, info): features at R_lo and targets (resolved - under-resolved, pair frame)."""
+def generate(n_samples, R_hi=12, L_hi=128, R_lo=3, steps_hi=300, seed=0, progress=None, gap_range=(0.05, 1.5)):
+    """(X, T, info): features at R_lo and targets (resolved - under-resolved, pair frame).
+
+    The periodic box must keep each sphere's image farther away than its
+    partner: L >= (4 + 2 gap_max) R, checked at both resolutions.
+    """
     s = R_lo / R_hi
     L_lo = int(round(L_hi * s))
     steps_lo = max(8, int(round(steps_hi * s * s)))
-    cfgs = sample_configs(n_samples, seed)
+    for L, R in ((L_hi, R_hi), (L_lo, R_lo)):
+        if L < (4.0 + 2.0 * gap_range[1]) * R:
+            raise ValueError(f"box {L} too small for radius {R} and gap/R up to {gap_range[1]}")
+    cfgs = sample_configs(n_samples, seed, gap_range=gap_range)
     X = np.zeros((n_samples, DIN))
     T = np.zeros((n_samples, DOUT))
     base = np.zeros((n_samples, DOUT))

@@ -105,7 +105,7 @@ void lbx_default_params(lbx_params* p, int32_t nx, int32_t ny, int32_t nz) {
   p->kinematic = 0;
   p->closure = 0;
   p->closure_gap_min = 0.05f;
-  p->closure_gap_max = 4.0f;
+  p->closure_gap_max = 1.5f;
   p->closure_vmax = 1.0e-3f;
   p->exact_tiles = 1;
 }

@@ -99,24 +99,32 @@ template <> struct Store<float> {
   using C = float;
   static __device__ __forceinline__ float ld(const float* p, float) { return __ldg(p); }
   static __device__ __forceinline__ void st(float* p, float v, float) { *p = v; }
+  static __device__ __forceinline__ float enc(float v, float) { return v; }
+  static __device__ __forceinline__ float dec(float h, float) { return h; }
   static constexpr bool shifted = false;
 };
 template <> struct Store<double> {
   using C = double;
   static __device__ __forceinline__ double ld(const double* p, double) { return __ldg(p); }
   static __device__ __forceinline__ void st(double* p, double v, double) { *p = v; }
+  static __device__ __forceinline__ double enc(double v, double) { return v; }
+  static __device__ __forceinline__ double dec(double h, double) { return h; }
   static constexpr bool shifted = false;
 };
 template <> struct Store<__half> {
   using C = float;
   static __device__ __forceinline__ float ld(const __half* p, float s) { return __half2float(__ldg(p)) + s; }
   static __device__ __forceinline__ void st(__half* p, float v, float s) { *p = __float2half_rn(v - s); }
+  static __device__ __forceinline__ __half enc(float v, float s) { return __float2half_rn(v - s); }
+  static __device__ __forceinline__ float dec(__half h, float s) { return __half2float(h) + s; }
   static constexpr bool shifted = true;
 };
 template <> struct Store<__nv_bfloat16> {
   using C = float;
   static __device__ __forceinline__ float ld(const __nv_bfloat16* p, float s) { return __bfloat162float(__ldg(p)) + s; }
   static __device__ __forceinline__ void st(__nv_bfloat16* p, float v, float s) { *p = __float2bfloat16_rn(v - s); }
+  static __device__ __forceinline__ __nv_bfloat16 enc(float v, float s) { return __float2bfloat16_rn(v - s); }
+  static __device__ __forceinline__ float dec(__nv_bfloat16 h, float s) { return __bfloat162float(h) + s; }
   static constexpr bool shifted = true;
 };
 

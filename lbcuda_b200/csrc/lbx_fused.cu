@@ -266,16 +266,17 @@ __device__ __forceinline__ int wrap0(int v, int n) {
   return v < 0 ? v + n : v;
 }
 
-// Particle data of a step (flags of this and of the previous step, the side
-// densities written by the fill and wetting kernels, written back here for
-// every fluid cell for the bounce-back of the same step and the drain of the
-// next).
+// Particle data of a step: flags of this and of the previous step, and the
+// side densities of the cells that are not pulled here (new fluid cells from
+// the fill kernel, surface cells from the wetting kernel).  The densities of
+// the fluid cells the particle kernels read come from their own shell pass
+// (k_rho_shell), so nothing is written back here.
 template <typename C>
 struct LeanPart {
   const int8_t* __restrict__ fold;
   const int8_t* __restrict__ fnew;
-  C* rhoR;
-  C* rhoB;
+  const C* __restrict__ rhoR;
+  const C* __restrict__ rhoB;
 };
 
 // One column march: cells [x0, x0+TX) x [y0, y0+TY) x [z0, zend) of one box.
@@ -335,15 +336,7 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
     const int zz = wrap0(z, g.nz);
     const bool owned = active && z >= z0 && z < zend;
     C rR, rB;
-    const bool pulled = densities(x, y, zz, owned, rR, rB);
-    if (parts) {
-      if (owned && pulled) {  // the densities of init_rho*_CG for the particle kernels
-        const int cell = x + g.nx * (y + g.ny * zz);
-        PT.rhoR[cell] = rR;
-        PT.rhoB[cell] = rB;
-      }
-    }
-    (void)pulled;
+    densities(x, y, zz, owned, rR, rB);
     rRo = rR;
     rBo = rB;
     sphi[slot][own] = (rR - rB) / (rR + rB);

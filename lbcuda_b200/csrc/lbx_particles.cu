@@ -4,7 +4,7 @@
 //   spherical_template (main.CUF:1990-2130)        -> host, uploaded once
 //   makeListAtomsGPU (2331-2451)                    -> k_bins (+ the tile-list
 //                                                      coverage predicate)
-//   init_isfluid_CG + setmyfluid (85-117,230-264)   -> k_flags
+//   init_isfluid_CG + setmyfluid (85-117,230-264)   -> k_stamp, k_stamp_flags
 //   del_fluid_CG / del_fluid (120-149,383-561)      -> k_drain
 //   init_rhoR_CG / init_rhoB_CG (CG.CUF:398-509)    -> k_rho_p
 //   make_fluid_CG / make_fluid + belts (152-180,563-913) -> k_fill
@@ -16,8 +16,9 @@
 //   rot_midstep_impl_lf (1098-1166,1266-1827)       -> k_integrate
 //
 // B200 design: particle state, orientation and every force/torque sum are
-// FP64.  Each per-particle kernel is one CTA per sphere that walks the
-// sphere's (2 rmax + 1)^3 box of cells, so the momentum exchanged at the
+// FP64.  Each per-particle kernel is one CTA per sphere that walks a list of
+// cell offsets around the sphere's centre (the template's solid cells, or
+// the cells within its reach), so the momentum exchanged at the
 // surface links is reduced inside the CTA in a fixed order and written once
 // per step (no global atomics, bit-reproducible), instead of one FP64 atomic
 // per link.  Per-cell work that must happen once per cell (the bounce-back
@@ -50,7 +51,9 @@ struct ParticleState {
   double* frc[2] = {nullptr, nullptr};
   double* acc = nullptr;
   int8_t* tmpl = nullptr;
-  int* owner = nullptr;
+  int* offs = nullptr;        // packed template offsets (pack_off): solid cells, then the bounce-back list
+  int n_surf = 0, n_solid = 0, n_bb = 0;
+  int* owner = nullptr;       // lowest index of the spheres whose template holds the cell, -1 if none
   int* bin_cnt = nullptr;
   int* bin_list = nullptr;
   int nbx = 0, nby = 0, nbz = 0;
@@ -69,6 +72,9 @@ struct PDev {  // by-value kernel argument
   int np, rmax, sphereMax, tw, lrotate;
   double rdim, rmass, max_vel;
   const int8_t* tmpl;
+  const int* offs;     // [0, n_surf) surface offsets, [n_surf, n_solid) dead + centre
+  const int* offs_bb;  // surface offsets, then the other offsets with d^2 < sphereMax
+  int n_surf, n_solid, n_bb;
   int* owner;
   int* bin_cnt;
   int* bin_list;
@@ -113,6 +119,28 @@ __device__ __forceinline__ int wrap1(int v, int n) {
 
 __device__ __forceinline__ int cell0(const Geom& g, int i1, int j1, int k1) {  // 1-based -> linear
   return (i1 - 1) + g.nx * ((j1 - 1) + g.ny * (k1 - 1));
+}
+
+// template offset (dx, dy, dz) and template value packed in one word
+__host__ __device__ __forceinline__ int pack_off(int dx, int dy, int dz, int v) {
+  return (dx + 64) | ((dy + 64) << 8) | ((dz + 64) << 16) | (v << 24);
+}
+__device__ __forceinline__ void unpack_off(int w, int& dx, int& dy, int& dz, int& v) {
+  dx = (w & 255) - 64;
+  dy = ((w >> 8) & 255) - 64;
+  dz = ((w >> 16) & 255) - 64;
+  v = (w >> 24) & 255;
+}
+
+// cell of sphere offset d around centre c, when d is the offset getDelta
+// assigns to that cell (the reference visits each cell under that offset only)
+__device__ __forceinline__ bool offset_cell(const PDev& P, const Geom& g, const int c[3], int dx, int dy, int dz,
+                                            int& i1, int& j1, int& k1) {
+  i1 = wrap1(c[0] + dx, g.nx);
+  j1 = wrap1(c[1] + dy, g.ny);
+  k1 = wrap1(c[2] + dz, g.nz);
+  return get_delta(i1, c[0], g.nx, P.rdim) == dx && get_delta(j1, c[1], g.ny, P.rdim) == dy &&
+         get_delta(k1, c[2], g.nz, P.rdim) == dz;
 }
 
 // Tile-list coverage of makeListAtomsGPU: whether the reference's 8x4x4 tile
@@ -248,35 +276,39 @@ __device__ __forceinline__ int bin_of(const PDev& P, int x0, int y0, int z0) {  
   return (x0 / BINW) + P.nbx * ((y0 / BINW) + P.nby * (z0 / BINW));
 }
 
-// init_isfluid_CG: flags of the current step and the owning sphere
-__global__ void k_flags(PDev P, const double* __restrict__ pos, Geom g, int8_t* __restrict__ flags_new) {
-  int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y, z = blockIdx.z;
-  if (x >= g.nx || y >= g.ny) return;
-  int cell = x + g.nx * (y + g.ny * z);
-  int bin = bin_of(P, x, y, z);
-  int n = min(P.bin_cnt[bin], BIN_CAP);
-  const int* L = P.bin_list + size_t(bin) * BIN_CAP;
+// init_isfluid_CG: flags of the current step and the owning sphere.  A cell
+// takes the template value of the lowest-index sphere whose template holds it
+// (the reference's first match over its ascending particle lists).  Two
+// passes over the solid template cells of every sphere: the owner as an
+// atomic minimum (owner and flags start at -1 / fluid), then the owner's
+// template value.
+__global__ void __launch_bounds__(256) k_stamp(PDev P, const double* __restrict__ pos, Geom g) {
+  const int a = blockIdx.x;
+  const double* p = pos + size_t(a) * PS;
+  const int c[3] = {nint_idx(p[0], g.nx), nint_idx(p[1], g.ny), nint_idx(p[2], g.nz)};
   const int nn[3] = {g.nx, g.ny, g.nz};
-  int8_t fl = LBX_FLUID_FLUID;
-  int own = 0;
-  for (int t = 0; t < n; ++t) {
-    int a = L[t];
-    const double* p = pos + size_t(a) * PS;
-    int di = get_delta(x + 1, nint_idx(p[0], g.nx), g.nx, P.rdim);
-    int dj = get_delta(y + 1, nint_idx(p[1], g.ny), g.ny, P.rdim);
-    int dk = get_delta(z + 1, nint_idx(p[2], g.nz), g.nz, P.rdim);
-    if (P.exact_tiles && !tile_covered(p, nn, P.rdim, x / TILEX + 1, y / TILEY + 1, z / TILEZ + 1)) continue;
-    if (abs(di) <= P.rmax && abs(dj) <= P.rmax && abs(dk) <= P.rmax) {
-      int8_t v = P.tmpl[(di + P.rmax) + P.tw * ((dj + P.rmax) + P.tw * (dk + P.rmax))];
-      if (v != LBX_FLUID_FLUID) {
-        fl = v;
-        own = a + 1;
-        break;
-      }
-    }
+  for (int t = threadIdx.x; t < P.n_solid; t += blockDim.x) {
+    int dx, dy, dz, v, i1, j1, k1;
+    unpack_off(P.offs[t], dx, dy, dz, v);
+    if (!offset_cell(P, g, c, dx, dy, dz, i1, j1, k1)) continue;
+    if (P.exact_tiles && !tile_covered(p, nn, P.rdim, (i1 - 1) / TILEX + 1, (j1 - 1) / TILEY + 1, (k1 - 1) / TILEZ + 1))
+      continue;
+    atomicMin(reinterpret_cast<unsigned*>(P.owner) + cell0(g, i1, j1, k1), unsigned(a));
   }
-  flags_new[cell] = fl;
-  P.owner[cell] = own;
+}
+
+__global__ void __launch_bounds__(256) k_stamp_flags(PDev P, const double* __restrict__ pos, Geom g,
+                                                     int8_t* __restrict__ flags_new) {
+  const int a = blockIdx.x;
+  const double* p = pos + size_t(a) * PS;
+  const int c[3] = {nint_idx(p[0], g.nx), nint_idx(p[1], g.ny), nint_idx(p[2], g.nz)};
+  for (int t = threadIdx.x; t < P.n_solid; t += blockDim.x) {
+    int dx, dy, dz, v, i1, j1, k1;
+    unpack_off(P.offs[t], dx, dy, dz, v);
+    if (!offset_cell(P, g, c, dx, dy, dz, i1, j1, k1)) continue;
+    const int cell = cell0(g, i1, j1, k1);
+    if (P.owner[cell] == a) flags_new[cell] = int8_t(v);
+  }
 }
 
 // walk the (2 rmax + 1)^3 box around centre c; fn(i1, j1, k1, di, dj, dk) gets
@@ -394,11 +426,14 @@ __global__ void __launch_bounds__(256) k_rho_p(const S* __restrict__ A, const S*
   phi[cell] = (rR - rB) / (rR + rB);
 }
 
-// init_rho*_CG for the fluid cells around each sphere (single-pass schedule):
-// the fill and wetting kernels of this step read densities up to two cells
-// beyond a template cell (the belts), before the fluid kernel computes the
-// rest.  The box [c - rmax - 2, c + rmax + 2]^3 covers them for spheres that
-// move at most one cell per step (MAX_PARTICLE_VEL <= 1).
+// init_rho*_CG for the fluid cells around each sphere (single-pass schedule).
+// The particle kernels are the only readers of the densities of fluid cells
+// (the fluid kernel pulls its own): the fill and wetting kernels of this step
+// read them up to two cells beyond a template cell (the belts), the
+// bounce-back of this step at the fluid end of each surface link, the drain
+// of the next step at the cells the spheres then cover.  The box
+// [c - rmax - 2, c + rmax + 2]^3 covers all of them for spheres that move at
+// most one cell per step (MAX_PARTICLE_VEL <= 1).
 template <typename S>
 __global__ void __launch_bounds__(256) k_rho_shell(PDev P, const double* __restrict__ pos_cur,
                                                    const double* __restrict__ pos_old, const S* A, Geom g,
@@ -522,9 +557,13 @@ __global__ void __launch_bounds__(256) k_virtual(PDev P, const double* __restric
     double ax[3] = {1.0, 0.0, 0.0};
     to_lab(pc, ax, xl);
   }
-  for_box(P, g, c, [&](int i1, int j1, int k1, int, int, int) {
+  // the cells a sphere owns as surface cells are surface cells of its template
+  for (int t = threadIdx.x; t < P.n_surf; t += blockDim.x) {
+    int dx, dy, dz, tv, i1, j1, k1;
+    unpack_off(P.offs[t], dx, dy, dz, tv);
+    if (!offset_cell(P, g, c, dx, dy, dz, i1, j1, k1)) continue;
     int cell = cell0(g, i1, j1, k1);
-    if (fnew[cell] != LBX_FLUID_SPHERELIST || P.owner[cell] != a + 1) return;
+    if (fnew[cell] != LBX_FLUID_SPHERELIST || P.owner[cell] != a) continue;
     C R, Bv;
     if (!neutral) {
       double r[3] = {double(i1) - pc[0], double(j1) - pc[1], double(k1) - pc[2]};
@@ -567,7 +606,7 @@ __global__ void __launch_bounds__(256) k_virtual(PDev P, const double* __restric
     rhoR[cell] = R;
     rhoB[cell] = Bv;
     phi[cell] = (R - Bv) / (R + Bv);
-  });
+  }
 }
 
 // time_step_CG with flags (two-pass schedule): collision on fluid cells,
@@ -640,7 +679,14 @@ __device__ __forceinline__ void wall_velocity(const PDev& P, const double* pc, c
   }
 }
 
-// partBB_CG + partBB_CG_p2n + partBB_CG_p2n2
+// partBB_CG + partBB_CG_p2n + partBB_CG_p2n2.  A thread takes one surface
+// cell within the sphere's reach.  The links that cross the surface are found
+// first (at most one per opposite pair), the populations and densities of
+// their fluid ends are loaded together, then: the node -> particle momentum
+// of this sphere; and, for the cell's owner only, the bounce-back copy and
+// the moving-wall corrections of every sphere in reach (ascending index, each
+// rounded to the storage type as a store and reload would), kept in
+// registers and stored once.
 template <typename S>
 __global__ void __launch_bounds__(256) k_bb(PDev P, const double* __restrict__ pos, double* acc, S* B, Geom g,
                                             Shift<typename Store<S>::C> sh, LatticeT<typename Store<S>::C> L,
@@ -648,70 +694,91 @@ __global__ void __launch_bounds__(256) k_bb(PDev P, const double* __restrict__ p
                                             const typename Store<S>::C* __restrict__ rhoR,
                                             const typename Store<S>::C* __restrict__ rhoB) {
   using C = typename Store<S>::C;
+  using St = Store<S>;
   const int a = blockIdx.x;
   const double* pc = pos + size_t(a) * PS;
   const int c[3] = {nint_idx(pc[0], g.nx), nint_idx(pc[1], g.ny), nint_idx(pc[2], g.nz)};
+  const int nn3[3] = {g.nx, g.ny, g.nz};
   const C buz = C(2) / L.cssq;  // pref_bouzidi, dimensions_m.CUF:95
   double s[6] = {0, 0, 0, 0, 0, 0};
-  for_box(P, g, c, [&](int i1, int j1, int k1, int di, int dj, int dk) {
-    int cell = cell0(g, i1, j1, k1);
-    if (fnew[cell] != LBX_FLUID_SPHERELIST) return;
+  for (int t = threadIdx.x; t < P.n_bb; t += blockDim.x) {
+    int dx, dy, dz, tv, i1, j1, k1;
+    unpack_off(P.offs_bb[t], dx, dy, dz, tv);
+    if (!offset_cell(P, g, c, dx, dy, dz, i1, j1, k1)) continue;
+    const int cell = cell0(g, i1, j1, k1);
+    if (fnew[cell] != LBX_FLUID_SPHERELIST) continue;
     const int x0 = i1 - 1, y0 = j1 - 1, z0 = k1 - 1;
-    Nbr b;
-    make_nbr(g, x0, y0, z0, b);
-    const int nn3[3] = {g.nx, g.ny, g.nz};
     const int ti = x0 / TILEX + 1, tj = y0 / TILEY + 1, tk = z0 / TILEZ + 1;
     // node -> particle momentum exchange for this sphere (atmDist < sphereMax)
-    if (di * di + dj * dj + dk * dk < P.sphereMax && (!P.exact_tiles || tile_covered(pc, nn3, P.rdim, ti, tj, tk))) {
+    const bool n2p = dx * dx + dy * dy + dz * dz < P.sphereMax &&
+                     (!P.exact_tiles || tile_covered(pc, nn3, P.rdim, ti, tj, tk));
+    const bool own = P.owner[cell] == a;
+    if (!n2p && !own) continue;
+    Nbr b;
+    make_nbr(g, x0, y0, z0, b);
+    // link pair it = (lo, hi) = (2it+1, 2it+2) crosses when exactly one end is
+    // fluid; hib: the fluid end is hi (then lf = lo, lr = hi), else lo
+    int xf[9];
+    unsigned act = 0, hib = 0;
+#pragma unroll
+    for (int it = 0; it < 9; ++it) {
+      const int lo = 2 * it + 1, hi = 2 * it + 2;
+      const int xi = at(b, ex(lo), ey(lo), ez(lo)), xo = at(b, ex(hi), ey(hi), ez(hi));
+      const bool fi = fnew[xi] == LBX_FLUID_FLUID, fo = fnew[xo] == LBX_FLUID_FLUID;
+      xf[it] = fo ? xo : xi;
+      act |= unsigned(fi != fo) << it;
+      hib |= unsigned(fo) << it;
+    }
+    if (!act) continue;
+    S hR[9], hB[9];
+    C rR[9], rB[9];
+#pragma unroll
+    for (int it = 0; it < 9; ++it) {
+      hR[it] = hB[it] = S(0.f);
+      rR[it] = rB[it] = C(0);
+      if (act >> it & 1) {
+        const int lf = (hib >> it & 1) ? 2 * it + 1 : 2 * it + 2;
+        const S* p = B + pidx(g, 0, lf, xf[it]);
+        hR[it] = __ldg(p);
+        hB[it] = __ldg(p + 1);
+        rR[it] = rhoR[xf[it]];
+        rB[it] = rhoB[xf[it]];
+      }
+    }
+    if (n2p) {
       LinkGeo G;
       link_geo(P, g, pc, i1, j1, k1, G);
 #pragma unroll
-      for (int it = 1; it <= 9; ++it) {
-        const int lo = 2 * it - 1, hi = 2 * it;
-        const int xi = at(b, ex(lo), ey(lo), ez(lo)), xo = at(b, ex(hi), ey(hi), ez(hi));
-        const bool fi = fnew[xi] == LBX_FLUID_FLUID, fo = fnew[xo] == LBX_FLUID_FLUID;
-#pragma unroll
-        for (int side = 0; side < 2; ++side) {
-          if (side == 0 ? !(fi && !fo) : !(!fi && fo)) continue;
-          const int xf = side ? xo : xi, lf = side ? lo : hi, lr = side ? hi : lo;
-          double rt[3], v[3];
-          wall_velocity(P, pc, G, lr, rt, v);
-          C ev = C(ex(lf)) * C(v[0]) + C(ey(lf)) * C(v[1]) + C(ez(lf)) * C(v[2]);
-          C w = L.w[wclass(lf)];
-          C f2pR = C(2) * Store<S>::ld(B + pidx(g, 0, lf, xf), sh.at(0, lf)) - w * buz * rhoR[xf] * ev;
-          C f2pB = C(2) * Store<S>::ld(B + pidx(g, 1, lf, xf), sh.at(1, lf)) - w * buz * rhoB[xf] * ev;
-          C f2p = f2pR + f2pB;
-          double ft[3] = {double(f2p * C(ex(lf))), double(f2p * C(ey(lf))), double(f2p * C(ez(lf)))};
-          s[0] += ft[0]; s[1] += ft[1]; s[2] += ft[2];
-          if (P.lrotate) {
-            double t[3];
-            cross(rt, ft, t);
-            s[3] += t[0] * abs(ex(lf));
-            s[4] += t[1] * abs(ey(lf));
-            s[5] += t[2] * abs(ez(lf));
-          }
+      for (int it = 0; it < 9; ++it) {
+        if (!(act >> it & 1)) continue;
+        const bool h = hib >> it & 1;
+        const int lf = h ? 2 * it + 1 : 2 * it + 2, lr = h ? 2 * it + 2 : 2 * it + 1;
+        double rt[3], v[3];
+        wall_velocity(P, pc, G, lr, rt, v);
+        C ev = C(ex(lf)) * C(v[0]) + C(ey(lf)) * C(v[1]) + C(ez(lf)) * C(v[2]);
+        C w = L.w[wclass(lf)];
+        C f2pR = C(2) * St::dec(hR[it], sh.at(0, lf)) - w * buz * rR[it] * ev;
+        C f2pB = C(2) * St::dec(hB[it], sh.at(1, lf)) - w * buz * rB[it] * ev;
+        C f2p = f2pR + f2pB;
+        double ft[3] = {double(f2p * C(ex(lf))), double(f2p * C(ey(lf))), double(f2p * C(ez(lf)))};
+        s[0] += ft[0]; s[1] += ft[1]; s[2] += ft[2];
+        if (P.lrotate) {
+          double tq[3];
+          cross(rt, ft, tq);
+          s[3] += tq[0] * abs(ex(lf));
+          s[4] += tq[1] * abs(ey(lf));
+          s[5] += tq[2] * abs(ez(lf));
         }
       }
     }
-    if (P.owner[cell] != a + 1) return;
-    // p2n phase 1: bounce-back copy into the surface cell
-#pragma unroll
-    for (int it = 1; it <= 9; ++it) {
-      const int lo = 2 * it - 1, hi = 2 * it;
-      const int xi = at(b, ex(lo), ey(lo), ez(lo)), xo = at(b, ex(hi), ey(hi), ez(hi));
-      const bool fi = fnew[xi] == LBX_FLUID_FLUID, fo = fnew[xo] == LBX_FLUID_FLUID;
-      for (int comp = 0; comp < 2; ++comp) {
-        if (fi && !fo) B[pidx(g, comp, lo, cell)] = B[pidx(g, comp, hi, xi)];
-        if (!fi && fo) B[pidx(g, comp, hi, cell)] = B[pidx(g, comp, lo, xo)];
-      }
-    }
-    // p2n phase 2: moving-wall correction, for every sphere within reach of
-    // the cell in ascending index (the particle loop of partBB_CG_p2n2)
-    int bin = bin_of(P, x0, y0, z0);
-    int nlist = min(P.bin_cnt[bin], BIN_CAP);
+    if (!own) continue;
+    // p2n phase 1: B(lr, cell) = B(lf, fluid end); lr and lf share their shift
+    // p2n phase 2: moving-wall corrections of the spheres in reach
+    const int bin = bin_of(P, x0, y0, z0);
+    const int nlist = min(P.bin_cnt[bin], BIN_CAP);
     const int* Lst = P.bin_list + size_t(bin) * BIN_CAP;
-    for (int t = 0; t < nlist; ++t) {
-      const int q = Lst[t];
+    for (int u = 0; u < nlist; ++u) {
+      const int q = Lst[u];
       const double* pq = pos + size_t(q) * PS;
       int ei = get_delta(i1, nint_idx(pq[0], g.nx), g.nx, P.rdim),
           ej = get_delta(j1, nint_idx(pq[1], g.ny), g.ny, P.rdim),
@@ -720,39 +787,41 @@ __global__ void __launch_bounds__(256) k_bb(PDev P, const double* __restrict__ p
       if (P.exact_tiles && !tile_covered(pq, nn3, P.rdim, ti, tj, tk)) continue;
       LinkGeo G;
       link_geo(P, g, pq, i1, j1, k1, G);
-      for (int it = 1; it <= 9; ++it) {
-        const int lo = 2 * it - 1, hi = 2 * it;
-        const int xi = at(b, ex(lo), ey(lo), ez(lo)), xo = at(b, ex(hi), ey(hi), ez(hi));
-        const bool fi = fnew[xi] == LBX_FLUID_FLUID, fo = fnew[xo] == LBX_FLUID_FLUID;
-        for (int side = 0; side < 2; ++side) {
-          if (side == 0 ? !(fi && !fo) : !(!fi && fo)) continue;
-          const int xf = side ? xo : xi, lf = side ? lo : hi, lr = side ? hi : lo;
-          double rt[3], v[3];
-          wall_velocity(P, pq, G, lr, rt, v);
-          C ev = C(ex(lf)) * C(v[0]) + C(ey(lf)) * C(v[1]) + C(ez(lf)) * C(v[2]);
-          C w = L.w[wclass(lf)];
-          for (int comp = 0; comp < 2; ++comp) {
-            S* p = B + pidx(g, comp, lr, cell);
-            const C* rho = comp ? rhoB : rhoR;
-            C val = Store<S>::ld(p, sh.at(comp, lr)) - w * buz * rho[xf] * ev;
-            Store<S>::st(p, val, sh.at(comp, lr));
-          }
-        }
+#pragma unroll
+      for (int it = 0; it < 9; ++it) {
+        if (!(act >> it & 1)) continue;
+        const bool h = hib >> it & 1;
+        const int lf = h ? 2 * it + 1 : 2 * it + 2, lr = h ? 2 * it + 2 : 2 * it + 1;
+        double rt[3], v[3];
+        wall_velocity(P, pq, G, lr, rt, v);
+        C ev = C(ex(lf)) * C(v[0]) + C(ey(lf)) * C(v[1]) + C(ez(lf)) * C(v[2]);
+        C w = L.w[wclass(lf)];
+        hR[it] = St::enc(St::dec(hR[it], sh.at(0, lr)) - w * buz * rR[it] * ev, sh.at(0, lr));
+        hB[it] = St::enc(St::dec(hB[it], sh.at(1, lr)) - w * buz * rB[it] * ev, sh.at(1, lr));
       }
     }
-  });
+#pragma unroll
+    for (int it = 0; it < 9; ++it) {
+      if (!(act >> it & 1)) continue;
+      const int lr = (hib >> it & 1) ? 2 * it + 2 : 2 * it + 1;
+      S* p = B + pidx(g, 0, lr, cell);
+      p[0] = hR[it];
+      p[1] = hB[it];
+    }
+  }
   double out[6] = {0, 0, 0, 0, 0, 0};
   block_sum<6>(s, out);
   if (threadIdx.x == 0)
     for (int d = 0; d < 6; ++d) acc[size_t(a) * AS + d] += out[d];
 }
 
-// inter_force_particles / addHertzian: all pairs, each sphere sums its own
-// share in a fixed order.  With lubrication on, the analytic squeeze force
-// is added as well (the reference writes it into a total that its
-// integrator then overwrites; here it reaches the integrator).
-__global__ void k_pairs(PDev P, const double* __restrict__ pos, double* acc, Geom g) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
+// inter_force_particles / addHertzian: all pairs; one warp per sphere, the
+// lanes take every 32nd partner and the warp sums their shares in a fixed
+// order.  With lubrication on, the analytic squeeze force is added as well
+// (the reference writes it into a total that its integrator then
+// overwrites; here it reaches the integrator).
+__global__ void __launch_bounds__(256) k_pairs(PDev P, const double* __restrict__ pos, double* acc, Geom g) {
+  const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
   if (i >= P.np) return;
   const double rsqcut = P.hz_rmin * P.hz_rmin;
   const double gmin = 5.0 * 0.5 * P.hz_k * pow(P.hz_rmin - P.hz_rcap, 1.5);
@@ -762,7 +831,7 @@ __global__ void k_pairs(PDev P, const double* __restrict__ pos, double* acc, Geo
   const double mxrsqcut = fmax(rparcut * rparcut, rsqcut);
   const double rparcap = rpar + P.lub_rcap;
   double f[3] = {0, 0, 0}, fl[3] = {0, 0, 0};
-  for (int j = 0; j < P.np; ++j) {
+  for (int j = lane; j < P.np; j += 32) {
     if (j == i) continue;
     // pair (lo, hi) with d = x_hi - x_lo as in addHertzian(lo, hi)
     const int lo = min(i, j), hi = max(i, j);
@@ -792,10 +861,17 @@ __global__ void k_pairs(PDev P, const double* __restrict__ pos, double* acc, Geo
       fl[2] += sgn * (cc * uz);
     }
   }
-  for (int d = 0; d < 3; ++d) {
-    acc[size_t(i) * AS + 6 + d] += f[d];
-    acc[size_t(i) * AS + 12 + d] += fl[d];
-  }
+#pragma unroll
+  for (int d = 0; d < 3; ++d)
+    for (int o = 16; o > 0; o >>= 1) {
+      f[d] += __shfl_down_sync(0xffffffffu, f[d], o);
+      fl[d] += __shfl_down_sync(0xffffffffu, fl[d], o);
+    }
+  if (lane == 0)
+    for (int d = 0; d < 3; ++d) {
+      acc[size_t(i) * AS + 6 + d] += f[d];
+      acc[size_t(i) * AS + 12 + d] += fl[d];
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -810,25 +886,33 @@ __device__ __forceinline__ void min_image(const Geom& g, const double* pl, const
   d[2] = d[2] - double(g.nz * nint_d(d[2] / g.nz));
 }
 
-// close neighbours of each sphere in ascending index (gap below the cut)
-__global__ void k_pair_nbrs(PDev P, const double* __restrict__ pos, Geom g, double gap_cut, int* nbr, int* cnt,
-                            unsigned long long* err, int64_t step) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
+// close neighbours of each sphere in ascending index (gap below the cut):
+// one warp per sphere tests 32 partners at a time and appends the hits in
+// lane order
+__global__ void __launch_bounds__(256) k_pair_nbrs(PDev P, const double* __restrict__ pos, Geom g, double gap_cut,
+                                                   int* nbr, int* cnt, unsigned long long* err, int64_t step) {
+  const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
   if (i >= P.np) return;
   const double* pi = pos + size_t(i) * PS;
   int c = 0;
-  for (int j = 0; j < P.np; ++j) {
-    if (j == i) continue;
-    double d[3];
-    min_image(g, pi, pos + size_t(j) * PS, d);
-    double r = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
-    if (r - 2.0 * P.rdim < gap_cut) {
-      if (c < NBCAP) nbr[size_t(i) * NBCAP + c] = j;
-      else raise_error(err, LBX_DEV_LIST_OVERFLOW, step, i);
-      ++c;
+  for (int j0 = 0; j0 < P.np; j0 += 32) {
+    const int j = j0 + lane;
+    bool hit = false;
+    if (j < P.np && j != i) {
+      double d[3];
+      min_image(g, pi, pos + size_t(j) * PS, d);
+      double r = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+      hit = r - 2.0 * P.rdim < gap_cut;
     }
+    const unsigned m = __ballot_sync(0xffffffffu, hit);
+    const int slot = c + __popc(m & ((1u << lane) - 1u));
+    if (hit) {
+      if (slot < NBCAP) nbr[size_t(i) * NBCAP + slot] = j;
+      else raise_error(err, LBX_DEV_LIST_OVERFLOW, step, i);
+    }
+    c += __popc(m);
   }
-  cnt[i] = min(c, NBCAP);
+  if (lane == 0) cnt[i] = min(c, NBCAP);
 }
 
 // one warp per close pair (i < j): the network inside its training envelope,
@@ -1059,6 +1143,11 @@ static PDev pdev(const Ctx& c) {
   d.rmass = double(c.p.rmass);
   d.max_vel = double(c.p.max_vel);
   d.tmpl = s.tmpl;
+  d.offs = s.offs;
+  d.offs_bb = s.offs ? s.offs + s.n_solid : nullptr;
+  d.n_surf = s.n_surf;
+  d.n_solid = s.n_solid;
+  d.n_bb = s.n_bb;
   d.owner = s.owner;
   d.bin_cnt = s.bin_cnt;
   d.bin_list = s.bin_list;
@@ -1137,6 +1226,32 @@ int particles_create(Ctx& c) {
   }
   if (!ok(cudaMalloc(&s->acc, size_t(cap) * AS * 8))) return LBX_ERR_ALLOC;
   if (!ok(cudaMalloc(&s->tmpl, t.size()))) return LBX_ERR_ALLOC;
+  // offset lists: solid template cells (surface first), then the bounce-back
+  // list (surface cells, then the rest of the reach d^2 < sphereMax)
+  std::vector<int> offs;
+  const int R = s->rmax, w = s->tw;
+  auto tv = [&](int i, int j, int k) { return int(t[(i + R) + w * ((j + R) + w * (k + R))]); };
+  for (int pass = 0; pass < 3; ++pass)
+    for (int k = -R; k <= R; ++k)
+      for (int j = -R; j <= R; ++j)
+        for (int i = -R; i <= R; ++i) {
+          const int v = tv(i, j, k);
+          const bool take = pass == 0 ? v == LBX_FLUID_SPHERELIST
+                                      : pass == 1 ? v == LBX_FLUID_SPHEREDEAD : v == LBX_FLUID_PARTICLECM;
+          if (take) offs.push_back(pack_off(i, j, k, v));
+        }
+  s->n_solid = int(offs.size());
+  for (int q = 0; q < s->n_solid; ++q)
+    if (((offs[size_t(q)] >> 24) & 255) == LBX_FLUID_SPHERELIST) s->n_surf = q + 1;
+  for (int q = 0; q < s->n_surf; ++q) offs.push_back(offs[size_t(q)]);
+  for (int k = -R; k <= R; ++k)
+    for (int j = -R; j <= R; ++j)
+      for (int i = -R; i <= R; ++i)
+        if (i * i + j * j + k * k < s->sphereMax && tv(i, j, k) != LBX_FLUID_SPHERELIST)
+          offs.push_back(pack_off(i, j, k, tv(i, j, k)));
+  s->n_bb = int(offs.size()) - s->n_solid;
+  if (!ok(cudaMalloc(&s->offs, offs.size() * 4))) return LBX_ERR_ALLOC;
+  cudaMemcpyAsync(s->offs, offs.data(), offs.size() * 4, cudaMemcpyHostToDevice, c.stream);
   if (!ok(cudaMalloc(&s->owner, size_t(c.n) * 4))) return LBX_ERR_ALLOC;
   if (!ok(cudaMalloc(&s->bin_cnt, nbins * 4))) return LBX_ERR_ALLOC;
   if (!ok(cudaMalloc(&s->bin_list, nbins * BIN_CAP * 4))) return LBX_ERR_ALLOC;
@@ -1145,7 +1260,7 @@ int particles_create(Ctx& c) {
   if (!ok(cudaMalloc(&s->nbr_cnt, size_t(cap) * 4))) return LBX_ERR_ALLOC;
   if (!ok(cudaMalloc(&s->corr, size_t(cap) * NBCAP * 12 * 4))) return LBX_ERR_ALLOC;
   cudaMemsetAsync(s->acc, 0, size_t(cap) * AS * 8, c.stream);
-  cudaMemsetAsync(s->owner, 0, size_t(c.n) * 4, c.stream);
+  cudaMemsetAsync(s->owner, 0xFF, size_t(c.n) * 4, c.stream);
   cudaMemcpyAsync(s->tmpl, t.data(), t.size(), cudaMemcpyHostToDevice, c.stream);
   cudaStreamSynchronize(c.stream);
   return launch_status();
@@ -1160,6 +1275,7 @@ void particles_destroy(Ctx& c) {
   }
   if (s->acc) cudaFree(s->acc);
   if (s->tmpl) cudaFree(s->tmpl);
+  if (s->offs) cudaFree(s->offs);
   if (s->owner) cudaFree(s->owner);
   if (s->bin_cnt) cudaFree(s->bin_cnt);
   if (s->bin_list) cudaFree(s->bin_list);
@@ -1179,6 +1295,18 @@ static int rebuild_bins(Ctx& c, const double* pos) {
   cudaMemsetAsync(s.bin_cnt, 0, nbins * 4, c.stream);
   k_bins<<<(s.np + 127) / 128, 128, 0, c.stream>>>(P, pos, g, c.d_err, c.step + 1);
   k_bins_sort<<<int((nbins + 255) / 256), 256, 0, c.stream>>>(P, int(nbins));
+  return launch_status();
+}
+
+// flags and owners of the spheres at `pos` (every other cell fluid, no owner)
+static int compute_flags(Ctx& c, const double* pos, int8_t* flags) {
+  ParticleState& s = *c.part;
+  cudaMemsetAsync(flags, LBX_FLUID_FLUID, size_t(c.n), c.stream);
+  cudaMemsetAsync(s.owner, 0xFF, size_t(c.n) * 4, c.stream);
+  PDev P = pdev(c);
+  Geom g = geom(c);
+  k_stamp<<<s.np, 256, 0, c.stream>>>(P, pos, g);
+  k_stamp_flags<<<s.np, 256, 0, c.stream>>>(P, pos, g, flags);
   return launch_status();
 }
 
@@ -1214,10 +1342,8 @@ int particles_set(Ctx& c, int n, const double* h_x, const double* h_v, const dou
   int slot = 1 - c.fcur;
   int rc = rebuild_bins(c, s->pos[0]);
   if (rc) return rc;
-  LaunchDims d = cell_dims(c);
-  k_flags<<<d.grid, d.block, 0, c.stream>>>(pdev(c), s->pos[0], geom(c), c.flags[slot]);
+  rc = compute_flags(c, s->pos[0], c.flags[slot]);
   s->flags_last = slot;
-  rc = launch_status();
   if (!rc) rc = cudaStreamSynchronize(c.stream) == cudaSuccess ? 0 : LBX_ERR_CUDA;
   return rc;
 }
@@ -1247,8 +1373,8 @@ int particles_pre(Ctx& c) {
     C* rB = (C*)c.rho[1];
     C* phi = (C*)c.phi;
     int r0 = rebuild_bins(c, pc);
+    if (!r0) r0 = compute_flags(c, pc, c.flags[fn]);
     if (r0) return r0;
-    k_flags<<<d.grid, d.block, 0, c.stream>>>(P, pc, g, c.flags[fn]);
     k_drain<S><<<s.np, 256, 0, c.stream>>>(P, pc, po, s.acc, A, B, g, sh, c.flags[fo], c.flags[fn], rR, rB);
     if (c.fused != 2)
       k_rho_p<S><<<d.grid, d.block, 0, c.stream>>>(A, B, g, sh, c.flags[fo], c.flags[fn], phi, rR, rB, c.d_err, st);
@@ -1294,11 +1420,12 @@ int particles_post(Ctx& c) {
     C* rR = (C*)c.rho[0];
     C* rB = (C*)c.rho[1];
     k_bb<S><<<s.np, 256, 0, c.stream>>>(P, pc, s.acc, B, g, sh, L, c.flags[fn], rR, rB);
-    k_pairs<<<(s.np + 127) / 128, 128, 0, c.stream>>>(P, pc, s.acc, g);
+    const int warp_blocks = (s.np * 32 + 255) / 256;
+    k_pairs<<<warp_blocks, 256, 0, c.stream>>>(P, pc, s.acc, g);
     if (c.p.closure) {
       const int use_net = s.closure_ready;
       const double cut = fmax(double(c.p.closure_gap_max) * s.rdim, c.p.lubrication ? double(c.p.lubric_rmin) : 0.0);
-      k_pair_nbrs<<<(s.np + 127) / 128, 128, 0, c.stream>>>(P, pc, g, cut, s.nbr, s.nbr_cnt, c.d_err, st);
+      k_pair_nbrs<<<warp_blocks, 256, 0, c.stream>>>(P, pc, g, cut, s.nbr, s.nbr_cnt, c.d_err, st);
       size_t smem = sizeof(float) * (size_t(LBX_CLOSURE_NWEIGHTS) + 8 * 2 * H);
       int blocks = (s.np * NBCAP + 7) / 8;
       if (blocks > 148 * 4) blocks = 148 * 4;

@@ -148,9 +148,9 @@ def test_zero_network_changes_nothing():
 
 @pytest.mark.gpu
 def test_trained_closure_beats_plain_method_on_held_out_pairs():
-    """Small end-to-end run: R_hi = 8 in 48^3 resolves, R_lo = 4 in 24^3 does not."""
+    """Small end-to-end run: R_hi = 8 in 64^3 resolves, R_lo = 4 in 32^3 does not (gap/R up to 1.5)."""
     from lbcuda_b200 import closure
-    X, T, info = closure.generate(96, R_hi=8, L_hi=48, R_lo=4, steps_hi=160, seed=5)
+    X, T, info = closure.generate(96, R_hi=8, L_hi=64, R_lo=4, steps_hi=160, seed=5)
     ntr = 72
     w, loss = closure.train(X[:ntr], T[:ntr], epochs=300, lr=2e-3)
     pred = closure.infer(w, X[ntr:])
