@@ -196,6 +196,15 @@ int lbx_closure_train(float* weights, const float* X, const float* T, int32_t n,
 int lbx_closure_grad(const float* weights, const float* Xs, const float* Ts, int32_t n, float* grad);
 /* Batched inference on raw features: Y (n,12). */
 int lbx_closure_infer(const float* weights, const float* X, int32_t n, float* Y);
+/* lbx_closure_infer without any device allocation (no counterpart in the
+ * reference), for callers that must not allocate or free device memory:
+ * inputs and outputs go through one fixed device array per device
+ * (416,768 bytes).  n <= LBX_CLOSURE_NOALLOC_MAX, else LBX_ERR_ARG.  The
+ * first call on a device (that device current) looks the array up; make it
+ * before any stream capture.  Calls that overlap in time on one device share
+ * the array and race: serialise them.  Same results as lbx_closure_infer. */
+#define LBX_CLOSURE_NOALLOC_MAX 4096
+int lbx_closure_infer_noalloc(const float* weights, const float* X, int32_t n, float* Y);
 /* Attach trained weights to a particle context; with p->closure = 1 each
  * step then corrects every close pair inside the envelope (closure_gap_min
  * <= gap/R <= closure_gap_max, relative velocity and angular velocity

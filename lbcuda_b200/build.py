@@ -15,7 +15,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "liblbx.so")
 DRIVER = os.path.join(HERE, "lbx_run")
 
-SOURCES = ["lbx_api.cu", "lbx_fluid.cu", "lbx_fused.cu", "lbx_particles.cu", "lbx_closure.cu", "lbx_ensemble.cu"]
+SOURCES = ["lbx_api.cu", "lbx_fluid.cu", "lbx_fused.cu", "lbx_particles.cu", "lbx_closure.cu", "lbx_ensemble.cu", "lbx_noalloc.cu"]
 HOST_SOURCES = ["lbx_driver.cpp"]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

@@ -71,6 +71,7 @@ SIGNATURES = {
     "lbx_closure_train": (C.c_int, [_F, _F, _F, C.c_int32, C.c_int32, C.c_float, C.c_int32, _F]),
     "lbx_closure_grad": (C.c_int, [_F, _F, _F, C.c_int32, _F]),
     "lbx_closure_infer": (C.c_int, [_F, _F, C.c_int32, _F]),
+    "lbx_closure_infer_noalloc": (C.c_int, [_F, _F, C.c_int32, _F]),
     "lbx_closure_set": (C.c_int, [_P, _F]),
     "lbx_ensemble_create": (C.c_int, [C.c_int32, C.POINTER(LbxParams), _PP]),
     "lbx_ensemble_destroy": (C.c_int, [_P]),

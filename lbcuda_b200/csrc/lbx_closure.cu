@@ -228,6 +228,20 @@ __global__ void k_mlp_infer(const float* __restrict__ Wg, const float* __restric
   }
 }
 
+// Launch of k_mlp_infer on device buffers (weights, n x DIN features, n x
+// DOUT outputs) on the legacy default stream; used by entry points that
+// manage their own device memory.
+int closure_infer_launch(const float* dW, const float* dX, int n, float* dY) {
+  using L = MlpLayout;
+  const size_t smem = sizeof(float) * (size_t(L::TOTAL) + 8 * 2 * H);
+  if (cudaFuncSetAttribute(k_mlp_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess)
+    return LBX_ERR_CUDA;
+  int blocks = (n + 7) / 8;
+  if (blocks > 148 * 4) blocks = 148 * 4;
+  k_mlp_infer<<<blocks, 256, smem>>>(dW, dX, n, dY);
+  return cudaGetLastError() == cudaSuccess ? 0 : LBX_ERR_CUDA;
+}
+
 }  // namespace lbx
 
 // ---------------------------------------------------------------------------
