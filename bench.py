@@ -192,36 +192,63 @@ COLLOID_L = 256
 COLLOID_N = 1280
 
 
-def colloid_sim(storage, schedule=2):
+def small_colloid_positions(L=128, n=160, seed=5, min_dist=13.0):
+    """Seeded non-overlapping centres (centre distance >= 2r + 2 for r = 5.5) in an L^3 box:
+    the colloid workload's 5 % volume fraction at 1/8 of its size, for profiler captures."""
+    rng = np.random.default_rng(seed)
+    x = []
+    while len(x) < n:
+        c = rng.uniform(1, L, 3)
+        ok = True
+        for y in x:
+            d = c - y
+            d -= L * np.round(d / L)
+            if np.dot(d, d) < min_dist ** 2:
+                ok = False
+                break
+        if ok:
+            x.append(c)
+    return np.array(x)
+
+
+def colloid_sim(storage, schedule=2, small=False):
     """Colloid workload: 256^3 CG fluid with 1280 spheres of radius 5.5 (the first 1280 of the
-    reference's Tests/07-1280-Particle placement), density 1, neutral wetting, at rest."""
+    reference's Tests/07-1280-Particle placement), density 1, neutral wetting, at rest.
+    small=True: 128^3 with 160 seeded spheres moving at up to 0.01 (profiler captures)."""
     from lbcuda_b200 import LBSim, make_params
     from lbcuda_b200.inputs import read_input_xyz, seeded_noise_fields
-    deck = os.path.join(ROOT, "tests", "golden", "decks", "07-1280.input.xyz.256cube.r5.5")
-    x, _, q = read_input_xyz(deck, COLLOID_N, True)
-    L = COLLOID_L
+    if small:
+        L, n = 128, 160
+        x = small_colloid_positions(L, n)
+        v = np.random.default_rng(6).uniform(-0.01, 0.01, (n, 3))
+        q = None
+    else:
+        L, n = COLLOID_L, COLLOID_N
+        deck = os.path.join(ROOT, "tests", "golden", "decks", "07-1280.input.xyz.256cube.r5.5")
+        x, _, q = read_input_xyz(deck, n, True)
+        v = np.zeros_like(x)
     vol = 4.0 / 3.0 * np.pi * 5.5 ** 3
-    p = make_params(L, model="cg", storage=storage, sigma=SIGMA, beta=BETA, max_particles=COLLOID_N, radius=5.5,
+    p = make_params(L, model="cg", storage=storage, sigma=SIGMA, beta=BETA, max_particles=n, radius=5.5,
                     rmass=float(1.0 / vol), wetting="neutral", lrotate=1, max_vel=1.0)
     s = LBSim(p)
     s.set_schedule(schedule)
     rR, rB = seeded_noise_fields(L, L, L, seed=SEED)
     s.set_fields(rR, rB)
-    s.set_particles(x, np.zeros_like(x), None, q)
+    s.set_particles(x, v, None, q)
     return s
 
 
-def colloid_timing(storage, steps=50, warm=10):
-    s = colloid_sim(storage)
+def colloid_timing(storage, steps=50, warm=10, small=False):
+    s = colloid_sim(storage, small=small)
     s.step(warm)
     s.sync()
     tot, k, nl = s.time_steps(steps, kernel_timing=True)
     code = s.status()[0]
     s.close()
-    cells = COLLOID_L ** 3
+    cells = (128 if small else COLLOID_L) ** 3
     mlups = cells * steps / (tot * 1e-3) / 1e6
-    return {"storage": storage, "mlups": mlups, "ms_per_step": tot / steps, "steps": steps,
-            "achieved_gbs_at_basis": mlups * 1e6 * BYTES_PER_CELL[storage] / 1e9,
+    return {"storage": storage, "small": small, "fluid_kernel_us": k / nl * 1e3 if nl else None, "mlups": mlups,
+            "ms_per_step": tot / steps, "steps": steps, "achieved_gbs_at_basis": mlups * 1e6 * BYTES_PER_CELL[storage] / 1e9,
             "frac_at_basis": mlups * 1e6 * BYTES_PER_CELL[storage] / 1e9 / peaks()[0], "device_error": code}
 
 
@@ -231,7 +258,8 @@ def only_region(args, local):
     from lbcuda_b200 import LBSim, make_params
     from lbcuda_b200.inputs import seeded_noise_fields
     if args.only.startswith("colloid"):
-        r = colloid_timing(args.only.split("-")[1], steps=max(1, args.steps) * 5, warm=args.warmup)
+        r = colloid_timing(args.only.split("-")[1], steps=max(1, args.steps) * 5, warm=args.warmup,
+                           small=args.only.endswith("small"))
         print(json.dumps(r), flush=True)
         return 0
     rR, rB = seeded_noise_fields(L, L, L, seed=SEED)
@@ -256,7 +284,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-extras", action="store_true", help="skip the error runs, the colloid case and the CPU baseline")
-    ap.add_argument("--only", choices=["f16", "f32", "bf16", "f64", "colloid-f16", "colloid-f32"],
+    ap.add_argument("--only", choices=["f16", "f32", "bf16", "f64", "colloid-f16", "colloid-f32", "colloid-f16-small",
+                                       "colloid-f32-small"],
                     help="profiling aid: run one timed region only and print its timing")
     ap.add_argument("--lb-steps", type=int, default=LB_PER_STEP, help="lattice steps per bench step")
     ap.add_argument("--schedule", type=int, default=2, help="colour-gradient schedule (0, 1, 2)")

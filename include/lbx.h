@@ -147,9 +147,27 @@ int lbx_get_particles(void* ctx, double* xyz, double* vel, double* omega, double
  * bounce-back, pair forces and the particle integrator). */
 int lbx_step(void* ctx, int32_t nsteps);
 /* Kernel-level entries of the same step, for callers that drive the order
- * themselves (the reference's host does, main.CUF:130-271). */
-int lbx_init_rho(void* ctx);          /* init_rhoR_CG + init_rhoB_CG (+ periodic rho halo) */
-int lbx_time_step_cg(void* ctx);      /* time_step_CG + flipflop*Pop0 + stream*_CG (+ halos) */
+ * themselves (the reference's host does, main.CUF:130-271).  Fluid only:
+ * lbx_init_rho, lbx_time_step_cg (each lbx_time_step_cg completes a step).
+ * With spheres, one step is the sequence below, in this order, and gives
+ * the same state as lbx_step(ctx, 1); the step ends (every ping-pong index
+ * flips) in lbx_time_step_force_particles.  Streaming has no entry of its
+ * own: it is the periodic pull inside lbx_time_step_cg (the reference's
+ * flipflop*Pop0_CG, stream*_CG, stream_CG_x/_y/_z and halo copies,
+ * main.CUF:206-221).  The particle entries return LBX_ERR_STATE before
+ * lbx_set_particles. */
+int lbx_make_list_atoms(void* ctx);   /* makeListAtomsGPU (main.CUF:240, previous step's end) */
+int lbx_init_isfluid(void* ctx);      /* init_isfluid_CG + fixPeriodic_isfluid (main.CUF:130-131) */
+int lbx_del_fluid(void* ctx);         /* del_fluid_CG (main.CUF:132) */
+int lbx_init_rho(void* ctx);          /* init_rhoR_CG + init_rhoB_CG (+ periodic rho halo) (main.CUF:143-149) */
+int lbx_make_fluid(void* ctx);        /* make_fluid_CG (main.CUF:154) */
+int lbx_virtual_rho(void* ctx);       /* compute_virtual_rho / compute_densities_wall (main.CUF:164-165) */
+int lbx_time_step_cg(void* ctx);      /* time_step_CG + flipflop*Pop0 + stream*_CG (+ halos) (main.CUF:172-221) */
+int lbx_partbb(void* ctx);            /* partBB_CG: node -> particle momentum (main.CUF:179) */
+int lbx_partbb_p2n(void* ctx);        /* partBB_CG_p2n: bounce-back copy (main.CUF:184) */
+int lbx_partbb_p2n2(void* ctx);       /* partBB_CG_p2n2: moving-wall term (main.CUF:187) */
+int lbx_inter_force_particles(void* ctx);      /* inter_force_particles (+ closure) (main.CUF:224) */
+int lbx_time_step_force_particles(void* ctx);  /* time_step_force_particles + flips (main.CUF:230) */
 int lbx_time_step_bgk(void* ctx);     /* init_rho_isfluid_BGK + time_step_BGK + stream_BGK */
 
 /* ---- readback ---------------------------------------------------------- */

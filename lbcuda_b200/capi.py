@@ -58,6 +58,16 @@ SIGNATURES = {
     "lbx_set_pops": (C.c_int, [_P, _F, _F]),
     "lbx_step": (C.c_int, [_P, C.c_int32]),
     "lbx_init_rho": (C.c_int, [_P]),
+    "lbx_make_list_atoms": (C.c_int, [C.c_void_p]),
+    "lbx_init_isfluid": (C.c_int, [C.c_void_p]),
+    "lbx_del_fluid": (C.c_int, [C.c_void_p]),
+    "lbx_make_fluid": (C.c_int, [C.c_void_p]),
+    "lbx_virtual_rho": (C.c_int, [C.c_void_p]),
+    "lbx_partbb": (C.c_int, [C.c_void_p]),
+    "lbx_partbb_p2n": (C.c_int, [C.c_void_p]),
+    "lbx_partbb_p2n2": (C.c_int, [C.c_void_p]),
+    "lbx_inter_force_particles": (C.c_int, [C.c_void_p]),
+    "lbx_time_step_force_particles": (C.c_int, [C.c_void_p]),
     "lbx_time_step_cg": (C.c_int, [_P]),
     "lbx_time_step_bgk": (C.c_int, [_P]),
     "lbx_get_fields": (C.c_int, [_P, _F, _F, _F, _F]),

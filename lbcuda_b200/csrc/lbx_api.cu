@@ -22,6 +22,16 @@ void particles_destroy(Ctx& c);
 int particles_set(Ctx& c, int n, const double* x, const double* v, const double* om, const double* q);
 int particles_get(Ctx& c, double* x, double* v, double* om, double* q, double* f, double* t);
 int particles_step(Ctx& c);
+int particles_fluid(Ctx& c);
+int part_lists(Ctx& c);
+int part_flags(Ctx& c);
+int part_drain(Ctx& c);
+int part_rho(Ctx& c);
+int part_fill(Ctx& c);
+int part_virtual(Ctx& c);
+int part_bb(Ctx& c, int mode);
+int part_pairs(Ctx& c);
+int part_integrate(Ctx& c);
 int particles_set_closure(Ctx& c, const float* w);
 int particles_flags_slot(const Ctx& c);
 int particles_active(const Ctx& c);
@@ -202,16 +212,39 @@ int lbx_step(void* ctx, int32_t nsteps) {
 int lbx_init_rho(void* ctx) {
   Ctx* c = as_ctx(ctx);
   if (!c) return LBX_ERR_ARG;
+  if (lbx::particles_active(*c)) return lbx::part_rho(*c);
   return lbx::fluid_init_rho(*c);
 }
 
 int lbx_time_step_cg(void* ctx) {
   Ctx* c = as_ctx(ctx);
   if (!c) return LBX_ERR_ARG;
+  // with spheres the step ends in lbx_time_step_force_particles
+  if (lbx::particles_active(*c)) return c->ncomp == 2 ? lbx::particles_fluid(*c) : LBX_ERR_STATE;
   int rc = lbx::fluid_collide_stream(*c);
   if (!rc) c->step += 1;
   return rc;
 }
+
+// kernel-level particle stages (main.CUF:130-240)
+#define LBX_PART_STAGE(name, call)           \
+  int name(void* ctx) {                      \
+    Ctx* c = as_ctx(ctx);                    \
+    if (!c) return LBX_ERR_ARG;              \
+    if (!lbx::particles_active(*c)) return LBX_ERR_STATE; \
+    return call;                             \
+  }
+LBX_PART_STAGE(lbx_make_list_atoms, lbx::part_lists(*c))
+LBX_PART_STAGE(lbx_init_isfluid, lbx::part_flags(*c))
+LBX_PART_STAGE(lbx_del_fluid, lbx::part_drain(*c))
+LBX_PART_STAGE(lbx_make_fluid, lbx::part_fill(*c))
+LBX_PART_STAGE(lbx_virtual_rho, lbx::part_virtual(*c))
+LBX_PART_STAGE(lbx_partbb, lbx::part_bb(*c, 1))
+LBX_PART_STAGE(lbx_partbb_p2n, lbx::part_bb(*c, 2))
+LBX_PART_STAGE(lbx_partbb_p2n2, lbx::part_bb(*c, 4))
+LBX_PART_STAGE(lbx_inter_force_particles, lbx::part_pairs(*c))
+LBX_PART_STAGE(lbx_time_step_force_particles, lbx::part_integrate(*c))
+#undef LBX_PART_STAGE
 
 int lbx_time_step_bgk(void* ctx) {
   Ctx* c = as_ctx(ctx);

@@ -145,13 +145,24 @@ template <> struct SPair<__nv_bfloat16> {
 // element offset of direction l (both components) of a cell: 2 (l n + cell)
 __device__ __forceinline__ size_t poff(int64_t n, int l, int cell) { return (size_t(l) * size_t(n) + size_t(cell)) * 2; }
 
+// Direction plane l of a population buffer: its pair of cell c is at
+// plane(l)[2 c].  The plane base is the same for every thread, so each access
+// costs one 32-bit index scaled onto a uniform base.
+template <typename S>
+struct Planes {
+  S* p;
+  int64_t n2;  // 2 n elements per direction plane
+  __device__ __forceinline__ S* operator()(int l) const { return p + size_t(l) * size_t(n2); }
+};
+
 // clamped densities (Sum g + rho0, init_rho*_CG) of the pulled cell
 template <typename S, typename C>
 __device__ __forceinline__ void pull_rho(const S* __restrict__ A, int64_t n, const PullIdx& P, const LeanConst<C>& K,
                                          C& rR, C& rB) {
-  P2<C> s = SPair<S>::ld(A + poff(n, 0, P.src[0]));
+  const Planes<const S> Ap{A, 2 * n};
+  P2<C> s = SPair<S>::ld(Ap(0) + 2 * P.src[0]);
 #pragma unroll
-  for (int l = 1; l < Q; ++l) s = p_add(s, SPair<S>::ld(A + poff(n, l, P.src[l])));
+  for (int l = 1; l < Q; ++l) s = p_add(s, SPair<S>::ld(Ap(l) + 2 * P.src[l]));
   rR = s.x + K.rho0[0];
   rB = s.y + K.rho0[1];
 }
@@ -305,25 +316,29 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
 
   // clamped densities of cell (cx, cy, zz): pulled (fluid in both steps),
   // from the side arrays (new fluid, or the virtual density of a surface
-  // cell), zero for every other solid cell (init_rho*_CG's MINDENS)
+  // cell), zero for every other solid cell (init_rho*_CG's MINDENS).  The
+  // pull is issued together with the flag loads and discarded for the few
+  // cells that do not use it, so the flags add no round trip to the pull.
   auto densities = [&](int cx, int cy, int zz, bool check, C& rR, C& rB) {
     const int cell = cx + g.nx * (cy + g.ny * zz);
+    int8_t fn = LBX_FLUID_FLUID, fo = LBX_FLUID_FLUID;
     if (parts) {
-      const int8_t fn = PT.fnew[cell];
-      if (fn != LBX_FLUID_FLUID) {
-        if (fn == LBX_FLUID_SPHERELIST) { rR = PT.rhoR[cell]; rB = PT.rhoB[cell]; }
-        else { rR = C(0); rB = C(0); }
-        return false;
-      }
-      if (PT.fold[cell] != LBX_FLUID_FLUID) {
-        rR = PT.rhoR[cell];
-        rB = PT.rhoB[cell];
-        return false;
-      }
+      fn = PT.fnew[cell];
+      fo = PT.fold[cell];
     }
     PullIdx P;
     pull_idx(g, cx, cy, zz, P);
     pull_rho<S, C>(A, g.n, P, K, rR, rB);
+    if (parts && (fn != LBX_FLUID_FLUID || fo != LBX_FLUID_FLUID)) {
+      if (fn == LBX_FLUID_FLUID || fn == LBX_FLUID_SPHERELIST) {
+        rR = PT.rhoR[cell];
+        rB = PT.rhoB[cell];
+      } else {
+        rR = C(0);
+        rB = C(0);
+      }
+      return false;
+    }
     if (check && (rR < C(-10) || rR > C(10) || rB < C(-10) || rB > C(10)))
       raise_error(err, LBX_DEV_RHO_RANGE, step, cell);
     rR = clamp0(rR);
@@ -359,30 +374,31 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
       const int cell = x + g.nx * (y + g.ny * z);
       PullIdx P;
       pull_idx(g, x, y, z, P);
+      const Planes<const S> Ap{A, 2 * g.n};
+      const Planes<S> Bp{B, 2 * g.n};
       P2<C> gp[Q];
       bool collide = true;
+      int8_t fn = LBX_FLUID_FLUID, fo = LBX_FLUID_FLUID;
       if (parts) {
-        const int8_t fn = PT.fnew[cell], fo = PT.fold[cell];
+        fn = PT.fnew[cell];
+        fo = PT.fold[cell];
+      }
+      // the pull every fluid cell needs, issued with the flag loads
+#pragma unroll
+      for (int l = 0; l < Q; ++l) gp[l] = SPair<S>::ld(Ap(l) + 2 * P.src[l]);
+      if (parts) {
         collide = fn == LBX_FLUID_FLUID;
         if (collide && fo != LBX_FLUID_FLUID) {
           // make_fluid already wrote the new node's populations (stored form) into B
 #pragma unroll
-          for (int l = 0; l < Q; ++l) gp[l] = SPair<S>::ld(B + poff(g.n, l, cell));
+          for (int l = 0; l < Q; ++l) gp[l] = SPair<S>::ld(Bp(l) + 2 * cell);
         } else if (!collide) {
           // solid cell: streamed populations only; a spheredead source (previous
           // step) leaves the destination's stale value, which is B's entry
 #pragma unroll
-          for (int l = 0; l < Q; ++l) {
-            const bool dead = l > 0 && PT.fold[P.src[l]] == LBX_FLUID_SPHEREDEAD;
-            gp[l] = dead ? SPair<S>::ld(B + poff(g.n, l, cell)) : SPair<S>::ld(A + poff(g.n, l, P.src[l]));
-          }
-        } else {
-#pragma unroll
-          for (int l = 0; l < Q; ++l) gp[l] = SPair<S>::ld(A + poff(g.n, l, P.src[l]));
+          for (int l = 1; l < Q; ++l)
+            if (PT.fold[P.src[l]] == LBX_FLUID_SPHEREDEAD) gp[l] = SPair<S>::ld(Bp(l) + 2 * cell);
         }
-      } else {
-#pragma unroll
-        for (int l = 0; l < Q; ++l) gp[l] = SPair<S>::ld(A + poff(g.n, l, P.src[l]));
       }
       if (collide) {
         const C* pm = sphi[(z + 3) & 3];
@@ -402,7 +418,7 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
         collide_pair(K, gp, rRc, rBc, px, py, pz, Store<S>::shifted);
       }
 #pragma unroll
-      for (int l = 0; l < Q; ++l) SPair<S>::st(B + poff(g.n, l, cell), gp[l]);
+      for (int l = 0; l < Q; ++l) SPair<S>::st(Bp(l) + 2 * cell, gp[l]);
     }
     // slot (z+3)&3 read above is rewritten in iteration z+2; the barrier of
     // iteration z+1 orders that write after these reads

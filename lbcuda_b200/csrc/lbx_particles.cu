@@ -52,7 +52,7 @@ struct ParticleState {
   double* acc = nullptr;
   int8_t* tmpl = nullptr;
   int* offs = nullptr;        // packed template offsets (pack_off): solid cells, then the bounce-back list
-  int n_surf = 0, n_solid = 0, n_bb = 0;
+  int n_surf = 0, n_solid = 0, n_bb = 0, n_shell = 0, shell_r2 = 0;
   int* owner = nullptr;       // lowest index of the spheres whose template holds the cell, -1 if none
   int* bin_cnt = nullptr;
   int* bin_list = nullptr;
@@ -74,7 +74,8 @@ struct PDev {  // by-value kernel argument
   const int8_t* tmpl;
   const int* offs;     // [0, n_surf) surface offsets, [n_surf, n_solid) dead + centre
   const int* offs_bb;  // surface offsets, then the other offsets with d^2 < sphereMax
-  int n_surf, n_solid, n_bb;
+  const int* offs_shell;  // offsets with d^2 <= shell_r2 (the density shell)
+  int n_surf, n_solid, n_bb, n_shell, shell_r2;
   int* owner;
   int* bin_cnt;
   int* bin_list;
@@ -326,20 +327,6 @@ __device__ __forceinline__ void for_box(const PDev& P, const Geom& g, const int 
   }
 }
 
-// every cell of the box [c - m, c + m]^3 (periodic), once
-template <typename F>
-__device__ __forceinline__ void for_box_m(const Geom& g, const int c[3], int m, F&& fn) {
-  const int w = 2 * m + 1, tot = w * w * w;
-  for (int t = threadIdx.x; t < tot; t += blockDim.x) {
-    int dx = t % w - m, dy = (t / w) % w - m, dz = t / (w * w) - m;
-    // skip the images of a cell reached twice when the box exceeds the lattice
-    if (2 * m + 1 > g.nx && (dx < -(g.nx / 2) || dx >= g.nx - g.nx / 2)) continue;
-    if (2 * m + 1 > g.ny && (dy < -(g.ny / 2) || dy >= g.ny - g.ny / 2)) continue;
-    if (2 * m + 1 > g.nz && (dz < -(g.nz / 2) || dz >= g.nz - g.nz / 2)) continue;
-    fn(wrap1(c[0] + dx, g.nx), wrap1(c[1] + dy, g.ny), wrap1(c[2] + dz, g.nz), dx * dx + dy * dy + dz * dz);
-  }
-}
-
 __device__ __forceinline__ bool moved(const double* p0, const double* p1) {
   return nint_d(p0[0]) != nint_d(p1[0]) || nint_d(p0[1]) != nint_d(p1[1]) || nint_d(p0[2]) != nint_d(p1[2]);
 }
@@ -426,14 +413,55 @@ __global__ void __launch_bounds__(256) k_rho_p(const S* __restrict__ A, const S*
   phi[cell] = (rR - rB) / (rR + rB);
 }
 
+// both components of one direction and cell (adjacent in memory), one load
+__device__ __forceinline__ void ld_pair(const float* p, float, float, float& a, float& b) {
+  const float2 v = __ldg(reinterpret_cast<const float2*>(p));
+  a = v.x;
+  b = v.y;
+}
+__device__ __forceinline__ void ld_pair(const double* p, double, double, double& a, double& b) {
+  const double2 v = __ldg(reinterpret_cast<const double2*>(p));
+  a = v.x;
+  b = v.y;
+}
+__device__ __forceinline__ void ld_pair(const __half* p, float s0, float s1, float& a, float& b) {
+  const float2 v = __half22float2(__ldg(reinterpret_cast<const __half2*>(p)));
+  a = v.x + s0;
+  b = v.y + s1;
+}
+__device__ __forceinline__ void ld_pair(const __nv_bfloat16* p, float s0, float s1, float& a, float& b) {
+  const float2 v = __bfloat1622float2(__ldg(reinterpret_cast<const __nv_bfloat162*>(p)));
+  a = v.x + s0;
+  b = v.y + s1;
+}
+
+// clamped densities of a cell fluid in both steps, pulled (init_rho*_CG; a
+// cell fluid in the previous step has no spheredead source); the sums run
+// over the directions in order, as init_rhoR_CG / init_rhoB_CG do
+template <typename S, typename C = typename Store<S>::C>
+__device__ __forceinline__ void pulled_rho(const S* A, const Geom& g, const Shift<C>& sh, int i1, int j1, int k1,
+                                           C& rR, C& rB) {
+  Nbr b;
+  make_nbr(g, i1 - 1, j1 - 1, k1 - 1, b);
+  C fR[Q], fB[Q];
+#pragma unroll
+  for (int l = 0; l < Q; ++l)
+    ld_pair(A + pidx(g, 0, l, at(b, -ex(l), -ey(l), -ez(l))), sh.at(0, l), sh.at(1, l), fR[l], fB[l]);
+  rR = sum_q(fR);
+  rB = sum_q(fB);
+  rR = rR < C(0) ? C(0) : rR;
+  rB = rB < C(0) ? C(0) : rB;
+}
+
 // init_rho*_CG for the fluid cells around each sphere (single-pass schedule).
 // The particle kernels are the only readers of the densities of fluid cells
-// (the fluid kernel pulls its own): the fill and wetting kernels of this step
-// read them up to two cells beyond a template cell (the belts), the
-// bounce-back of this step at the fluid end of each surface link, the drain
-// of the next step at the cells the spheres then cover.  The box
-// [c - rmax - 2, c + rmax + 2]^3 covers all of them for spheres that move at
-// most one cell per step (MAX_PARTICLE_VEL <= 1).
+// (the fluid kernel pulls its own), and they read them within
+// (rdim + sqrt 3) of a sphere's centre: the bounce-back of this step at the
+// fluid end of each surface link, the wetting and fill kernels in the first
+// (D3Q27) belt of a surface or uncovered cell, the drain of the next step at
+// the cells the spheres then cover.  The shell is that ball around the
+// current centre and, for a sphere that changed cell, around the previous
+// one (its uncovered cells).  The rare second-belt fallbacks pull their own.
 template <typename S>
 __global__ void __launch_bounds__(256) k_rho_shell(PDev P, const double* __restrict__ pos_cur,
                                                    const double* __restrict__ pos_old, const S* A, Geom g,
@@ -443,22 +471,38 @@ __global__ void __launch_bounds__(256) k_rho_shell(PDev P, const double* __restr
   using C = typename Store<S>::C;
   const int a = blockIdx.x;
   const double* pc = pos_cur + size_t(a) * PS;
-  (void)pos_old;
-  const int m = P.rmax + 2;
-  const int c[3] = {nint_idx(pc[0], g.nx), nint_idx(pc[1], g.ny), nint_idx(pc[2], g.nz)};
-  for_box_m(g, c, m, [&](int i1, int j1, int k1, int) {
+  const double* po = pos_old + size_t(a) * PS;
+  const int cn[3] = {nint_idx(pc[0], g.nx), nint_idx(pc[1], g.ny), nint_idx(pc[2], g.nz)};
+  const int co[3] = {nint_idx(po[0], g.nx), nint_idx(po[1], g.ny), nint_idx(po[2], g.nz)};
+  const bool mv = moved(pc, po);
+  // old centre relative to the new one (minimum image)
+  const int nn[3] = {g.nx, g.ny, g.nz};
+  int sft[3];
+  for (int d = 0; d < 3; ++d) {
+    int v = co[d] - cn[d];
+    if (2 * v > nn[d]) v -= nn[d];
+    if (2 * v < -nn[d]) v += nn[d];
+    sft[d] = v;
+  }
+  const int tot = mv ? 2 * P.n_shell : P.n_shell;
+  for (int t = threadIdx.x; t < tot; t += blockDim.x) {
+    const bool second = t >= P.n_shell;
+    int dx, dy, dz, tv;
+    unpack_off(P.offs_shell[second ? t - P.n_shell : t], dx, dy, dz, tv);
+    const int* c0 = cn;
+    if (second) {  // around the old centre, minus what the new ball covers
+      const int ex_ = dx + sft[0], ey_ = dy + sft[1], ez_ = dz + sft[2];
+      if (ex_ * ex_ + ey_ * ey_ + ez_ * ez_ <= P.shell_r2) continue;
+      c0 = co;
+    }
+    const int i1 = wrap1(c0[0] + dx, g.nx), j1 = wrap1(c0[1] + dy, g.ny), k1 = wrap1(c0[2] + dz, g.nz);
     const int y = cell0(g, i1, j1, k1);
-    if (fnew[y] != LBX_FLUID_FLUID || fold[y] != LBX_FLUID_FLUID) return;
-    Nbr b;
-    make_nbr(g, i1 - 1, j1 - 1, k1 - 1, b);
-    C f[Q];
-    pull(A, g, b, 0, sh, f);
-    C rR = sum_q(f);
-    pull(A, g, b, 1, sh, f);
-    C rB = sum_q(f);
-    rhoR[y] = rR < C(0) ? C(0) : rR;
-    rhoB[y] = rB < C(0) ? C(0) : rB;
-  });
+    if (fnew[y] != LBX_FLUID_FLUID || fold[y] != LBX_FLUID_FLUID) continue;
+    C rR, rB;
+    pulled_rho(A, g, sh, i1, j1, k1, rR, rB);
+    rhoR[y] = rR;
+    rhoB[y] = rB;
+  }
 }
 
 // make_fluid: cells solid in the previous step and fluid now get the mean
@@ -507,7 +551,9 @@ __global__ void __launch_bounds__(256) k_fill(PDev P, const double* __restrict__
             int yi = wrap1(i1 + ii, g.nx), yj = wrap1(j1 + jj, g.ny), yk = wrap1(k1 + kk, g.nz);
             int y = cell0(g, yi, yj, yk);
             if (fnew[y] == LBX_FLUID_FLUID && fold[y] == LBX_FLUID_FLUID) {
-              Rs = Rs + rhoR[y]; Bs = Bs + rhoB[y]; ++D;
+              C qR, qB;
+              pulled_rho(A, g, sh, yi, yj, yk, qR, qB);  // beyond the density shell
+              Rs = Rs + qR; Bs = Bs + qB; ++D;
             }
           }
       if (D) { Rs = Rs / C(D); Bs = Bs / C(D); }
@@ -595,7 +641,9 @@ __global__ void __launch_bounds__(256) k_virtual(PDev P, const double* __restric
               int yi = wrap1(i1 + ii, g.nx), yj = wrap1(j1 + jj, g.ny), yk = wrap1(k1 + kk, g.nz);
               int y = cell0(g, yi, yj, yk);
               if (fnew[y] == LBX_FLUID_FLUID && fold[y] == LBX_FLUID_FLUID) {
-                Rs = Rs + rhoR[y]; Bs = Bs + rhoB[y]; ++D;
+                C qR, qB;
+                pulled_rho(A, g, sh, yi, yj, yk, qR, qB);  // beyond the density shell
+                Rs = Rs + qR; Bs = Bs + qB; ++D;
               }
             }
         // no fluid in either belt: the density stays at init_rho*_CG's zero
@@ -654,15 +702,30 @@ struct LinkGeo {
   double rv[3], ol[3];
 };
 
+// lab-frame angular velocity of a sphere (zero without rotation)
+__device__ __forceinline__ void lab_omega(const PDev& P, const double* pc, double ol[3]) {
+  ol[0] = ol[1] = ol[2] = 0;
+  if (P.lrotate) {
+    double om[3] = {pc[6], pc[7], pc[8]};
+    to_lab(pc, om, ol);
+  }
+}
+
 __device__ __forceinline__ void link_geo(const PDev& P, const Geom& g, const double* pc, int i1, int j1, int k1,
                                          LinkGeo& G) {
   G.rv[0] = G.rv[1] = G.rv[2] = 0;
-  G.ol[0] = G.ol[1] = G.ol[2] = 0;
-  if (P.lrotate) {
-    double om[3] = {pc[6], pc[7], pc[8]};
-    to_lab(pc, om, G.ol);
-    lever(g, pc, i1, j1, k1, true, P.rdim, G.rv);
-  }
+  lab_omega(P, pc, G.ol);
+  if (P.lrotate) lever(g, pc, i1, j1, k1, true, P.rdim, G.rv);
+}
+
+// the same with the sphere's lab angular velocity already known
+__device__ __forceinline__ void link_geo_ol(const PDev& P, const Geom& g, const double* pc, const double ol[3], int i1,
+                                            int j1, int k1, LinkGeo& G) {
+  G.rv[0] = G.rv[1] = G.rv[2] = 0;
+  G.ol[0] = ol[0];
+  G.ol[1] = ol[1];
+  G.ol[2] = ol[2];
+  if (P.lrotate) lever(g, pc, i1, j1, k1, true, P.rdim, G.rv);
 }
 
 __device__ __forceinline__ void wall_velocity(const PDev& P, const double* pc, const LinkGeo& G, int lr,
@@ -686,13 +749,17 @@ __device__ __forceinline__ void wall_velocity(const PDev& P, const double* pc, c
 // of this sphere; and, for the cell's owner only, the bounce-back copy and
 // the moving-wall corrections of every sphere in reach (ascending index, each
 // rounded to the storage type as a store and reload would), kept in
-// registers and stored once.
+// registers and stored once.  mode selects the phases (BB_N2P | BB_COPY |
+// BB_WALL; the step runs all three in one launch, the kernel-level entry
+// points one each, with the same results).
+constexpr int BB_N2P = 1, BB_COPY = 2, BB_WALL = 4, BB_ALL = 7;
+
 template <typename S>
 __global__ void __launch_bounds__(256) k_bb(PDev P, const double* __restrict__ pos, double* acc, S* B, Geom g,
                                             Shift<typename Store<S>::C> sh, LatticeT<typename Store<S>::C> L,
                                             const int8_t* __restrict__ fnew,
                                             const typename Store<S>::C* __restrict__ rhoR,
-                                            const typename Store<S>::C* __restrict__ rhoB) {
+                                            const typename Store<S>::C* __restrict__ rhoB, int mode) {
   using C = typename Store<S>::C;
   using St = Store<S>;
   const int a = blockIdx.x;
@@ -700,6 +767,8 @@ __global__ void __launch_bounds__(256) k_bb(PDev P, const double* __restrict__ p
   const int c[3] = {nint_idx(pc[0], g.nx), nint_idx(pc[1], g.ny), nint_idx(pc[2], g.nz)};
   const int nn3[3] = {g.nx, g.ny, g.nz};
   const C buz = C(2) / L.cssq;  // pref_bouzidi, dimensions_m.CUF:95
+  double ola[3];
+  lab_omega(P, pc, ola);
   double s[6] = {0, 0, 0, 0, 0, 0};
   for (int t = threadIdx.x; t < P.n_bb; t += blockDim.x) {
     int dx, dy, dz, tv, i1, j1, k1;
@@ -710,9 +779,9 @@ __global__ void __launch_bounds__(256) k_bb(PDev P, const double* __restrict__ p
     const int x0 = i1 - 1, y0 = j1 - 1, z0 = k1 - 1;
     const int ti = x0 / TILEX + 1, tj = y0 / TILEY + 1, tk = z0 / TILEZ + 1;
     // node -> particle momentum exchange for this sphere (atmDist < sphereMax)
-    const bool n2p = dx * dx + dy * dy + dz * dz < P.sphereMax &&
+    const bool n2p = (mode & BB_N2P) && dx * dx + dy * dy + dz * dz < P.sphereMax &&
                      (!P.exact_tiles || tile_covered(pc, nn3, P.rdim, ti, tj, tk));
-    const bool own = P.owner[cell] == a;
+    const bool own = (mode & (BB_COPY | BB_WALL)) && P.owner[cell] == a;
     if (!n2p && !own) continue;
     Nbr b;
     make_nbr(g, x0, y0, z0, b);
@@ -737,8 +806,10 @@ __global__ void __launch_bounds__(256) k_bb(PDev P, const double* __restrict__ p
       hR[it] = hB[it] = S(0.f);
       rR[it] = rB[it] = C(0);
       if (act >> it & 1) {
-        const int lf = (hib >> it & 1) ? 2 * it + 1 : 2 * it + 2;
-        const S* p = B + pidx(g, 0, lf, xf[it]);
+        const bool h = hib >> it & 1;
+        const int lf = h ? 2 * it + 1 : 2 * it + 2, lr = h ? 2 * it + 2 : 2 * it + 1;
+        // the fluid end's population, or (wall phase alone) the copy already in place
+        const S* p = (n2p || (mode & BB_COPY)) ? B + pidx(g, 0, lf, xf[it]) : B + pidx(g, 0, lr, cell);
         hR[it] = __ldg(p);
         hB[it] = __ldg(p + 1);
         rR[it] = rhoR[xf[it]];
@@ -747,7 +818,7 @@ __global__ void __launch_bounds__(256) k_bb(PDev P, const double* __restrict__ p
     }
     if (n2p) {
       LinkGeo G;
-      link_geo(P, g, pc, i1, j1, k1, G);
+      link_geo_ol(P, g, pc, ola, i1, j1, k1, G);
 #pragma unroll
       for (int it = 0; it < 9; ++it) {
         if (!(act >> it & 1)) continue;
@@ -775,7 +846,7 @@ __global__ void __launch_bounds__(256) k_bb(PDev P, const double* __restrict__ p
     // p2n phase 1: B(lr, cell) = B(lf, fluid end); lr and lf share their shift
     // p2n phase 2: moving-wall corrections of the spheres in reach
     const int bin = bin_of(P, x0, y0, z0);
-    const int nlist = min(P.bin_cnt[bin], BIN_CAP);
+    const int nlist = (mode & BB_WALL) ? min(P.bin_cnt[bin], BIN_CAP) : 0;
     const int* Lst = P.bin_list + size_t(bin) * BIN_CAP;
     for (int u = 0; u < nlist; ++u) {
       const int q = Lst[u];
@@ -786,7 +857,8 @@ __global__ void __launch_bounds__(256) k_bb(PDev P, const double* __restrict__ p
       if (ei * ei + ej * ej + ek * ek >= P.sphereMax) continue;
       if (P.exact_tiles && !tile_covered(pq, nn3, P.rdim, ti, tj, tk)) continue;
       LinkGeo G;
-      link_geo(P, g, pq, i1, j1, k1, G);
+      if (q == a) link_geo_ol(P, g, pq, ola, i1, j1, k1, G);
+      else link_geo(P, g, pq, i1, j1, k1, G);
 #pragma unroll
       for (int it = 0; it < 9; ++it) {
         if (!(act >> it & 1)) continue;
@@ -1148,6 +1220,9 @@ static PDev pdev(const Ctx& c) {
   d.n_surf = s.n_surf;
   d.n_solid = s.n_solid;
   d.n_bb = s.n_bb;
+  d.offs_shell = s.offs ? s.offs + s.n_solid + s.n_bb : nullptr;
+  d.n_shell = s.n_shell;
+  d.shell_r2 = s.shell_r2;
   d.owner = s.owner;
   d.bin_cnt = s.bin_cnt;
   d.bin_list = s.bin_list;
@@ -1250,6 +1325,16 @@ int particles_create(Ctx& c) {
         if (i * i + j * j + k * k < s->sphereMax && tv(i, j, k) != LBX_FLUID_SPHERELIST)
           offs.push_back(pack_off(i, j, k, tv(i, j, k)));
   s->n_bb = int(offs.size()) - s->n_solid;
+  // density shell: every offset within (rdim + sqrt 3) of the centre
+  const double rs = s->rdim + std::sqrt(3.0);
+  s->shell_r2 = int(std::floor(rs * rs));
+  const int RS = int(std::ceil(rs));
+  if (RS > 60) return LBX_ERR_ARG;  // offsets are packed in 8 bits
+  for (int k = -RS; k <= RS; ++k)
+    for (int j = -RS; j <= RS; ++j)
+      for (int i = -RS; i <= RS; ++i)
+        if (i * i + j * j + k * k <= s->shell_r2) offs.push_back(pack_off(i, j, k, 0));
+  s->n_shell = int(offs.size()) - s->n_solid - s->n_bb;
   if (!ok(cudaMalloc(&s->offs, offs.size() * 4))) return LBX_ERR_ALLOC;
   cudaMemcpyAsync(s->offs, offs.data(), offs.size() * 4, cudaMemcpyHostToDevice, c.stream);
   if (!ok(cudaMalloc(&s->owner, size_t(c.n) * 4))) return LBX_ERR_ALLOC;
@@ -1348,43 +1433,105 @@ int particles_set(Ctx& c, int n, const double* h_x, const double* h_v, const dou
   return rc;
 }
 
-// One step with particles, main.CUF:130-241, in three parts so that an
-// ensemble can put the fluid kernels of all its boxes into one launch:
-//   pre:   particle lists, flags, drain, (two-pass densities), fill, wetting
+// One step with particles, main.CUF:130-241, as the stages the reference
+// launches (each a kernel-level entry point of the C ABI as well):
+//   pre:   lists, flags, drain, densities, fill, wetting
 //   fluid: the colour-gradient step with flags
-//   post:  bounce-back, pair forces, closure, integrator, buffer swap
-int particles_pre(Ctx& c) {
-  ParticleState& s = *c.part;
-  Geom g = geom(c);
-  PDev P = pdev(c);
+//   post:  bounce-back (n2p, copy, wall), pair forces (+ closure), integrator
+//          and the buffer swap
+// particles_pre / particles_post group them so that an ensemble can put the
+// fluid kernels of all its boxes into one launch.
+namespace {
+struct Stage {  // the buffers and constants every stage launch needs
+  ParticleState& s;
+  Geom g;
+  PDev P;
+  int fo, fn;
+  const double* pc;
+  const double* po;
+  int64_t st;
+  explicit Stage(Ctx& c)
+      : s(*c.part), g(geom(c)), P(pdev(c)), fo(c.fcur), fn(1 - c.fcur), pc(c.part->pos[c.part->pcur]),
+        po(c.part->pos[1 - c.part->pcur]), st(c.step + 1) {}
+};
+}  // namespace
+
+int part_lists(Ctx& c) {
+  Stage t(c);
+  return rebuild_bins(c, t.pc);
+}
+
+int part_flags(Ctx& c) {
+  Stage t(c);
+  return compute_flags(c, t.pc, c.flags[t.fn]);
+}
+
+int part_drain(Ctx& c) {
+  Stage t(c);
+  return by_storage(c, [&](auto* tag) {
+    using S = std::remove_pointer_t<decltype(tag)>;
+    using C = typename Store<S>::C;
+    k_drain<S><<<t.s.np, 256, 0, c.stream>>>(t.P, t.pc, t.po, t.s.acc, (const S*)c.pops[c.cur],
+                                              (const S*)c.pops[1 - c.cur], t.g, make_shift<C>(c), c.flags[t.fo],
+                                              c.flags[t.fn], (const C*)c.rho[0], (const C*)c.rho[1]);
+    return launch_status();
+  });
+}
+
+// init_rho*_CG with flags: every cell (two-pass schedule) or only the fluid
+// cells the particle kernels read (single-pass schedule, whose fluid kernel
+// pulls its own densities)
+int part_rho(Ctx& c) {
+  Stage t(c);
   LaunchDims d = cell_dims(c);
-  const int fo = c.fcur, fn = 1 - c.fcur;
-  const double* pc = s.pos[s.pcur];
-  const double* po = s.pos[1 - s.pcur];
-  const int64_t st = c.step + 1;
   return by_storage(c, [&](auto* tag) {
     using S = std::remove_pointer_t<decltype(tag)>;
     using C = typename Store<S>::C;
     const S* A = (const S*)c.pops[c.cur];
     S* B = (S*)c.pops[1 - c.cur];
-    Shift<C> sh = make_shift<C>(c);
-    LatticeT<C> L = make_lattice<C>();
-    C* rR = (C*)c.rho[0];
-    C* rB = (C*)c.rho[1];
-    C* phi = (C*)c.phi;
-    int r0 = rebuild_bins(c, pc);
-    if (!r0) r0 = compute_flags(c, pc, c.flags[fn]);
-    if (r0) return r0;
-    k_drain<S><<<s.np, 256, 0, c.stream>>>(P, pc, po, s.acc, A, B, g, sh, c.flags[fo], c.flags[fn], rR, rB);
     if (c.fused != 2)
-      k_rho_p<S><<<d.grid, d.block, 0, c.stream>>>(A, B, g, sh, c.flags[fo], c.flags[fn], phi, rR, rB, c.d_err, st);
+      k_rho_p<S><<<d.grid, d.block, 0, c.stream>>>(A, B, t.g, make_shift<C>(c), c.flags[t.fo], c.flags[t.fn],
+                                                   (C*)c.phi, (C*)c.rho[0], (C*)c.rho[1], c.d_err, t.st);
     else
-      k_rho_shell<S><<<s.np, 256, 0, c.stream>>>(P, pc, po, A, g, sh, c.flags[fo], c.flags[fn], rR, rB);
-    k_fill<S><<<s.np, 256, 0, c.stream>>>(P, pc, po, s.acc, A, B, g, sh, L, c.flags[fo], c.flags[fn], rR, rB, phi);
-    k_virtual<S><<<s.np, 256, 0, c.stream>>>(P, pc, g, c.p.wetting == LBX_WET_NEUTRAL ? 1 : 0, A, sh, c.flags[fo],
-                                              c.flags[fn], rR, rB, phi, L);
+      k_rho_shell<S><<<t.s.np, 256, 0, c.stream>>>(t.P, t.pc, t.po, A, t.g, make_shift<C>(c), c.flags[t.fo],
+                                                    c.flags[t.fn], (C*)c.rho[0], (C*)c.rho[1]);
     return launch_status();
   });
+}
+
+int part_fill(Ctx& c) {
+  Stage t(c);
+  return by_storage(c, [&](auto* tag) {
+    using S = std::remove_pointer_t<decltype(tag)>;
+    using C = typename Store<S>::C;
+    k_fill<S><<<t.s.np, 256, 0, c.stream>>>(t.P, t.pc, t.po, t.s.acc, (const S*)c.pops[c.cur], (S*)c.pops[1 - c.cur],
+                                             t.g, make_shift<C>(c), make_lattice<C>(), c.flags[t.fo], c.flags[t.fn],
+                                             (C*)c.rho[0], (C*)c.rho[1], (C*)c.phi);
+    return launch_status();
+  });
+}
+
+int part_virtual(Ctx& c) {
+  Stage t(c);
+  return by_storage(c, [&](auto* tag) {
+    using S = std::remove_pointer_t<decltype(tag)>;
+    using C = typename Store<S>::C;
+    k_virtual<S><<<t.s.np, 256, 0, c.stream>>>(t.P, t.pc, t.g, c.p.wetting == LBX_WET_NEUTRAL ? 1 : 0,
+                                                (const S*)c.pops[c.cur], make_shift<C>(c), c.flags[t.fo],
+                                                c.flags[t.fn], (C*)c.rho[0], (C*)c.rho[1], (C*)c.phi,
+                                                make_lattice<C>());
+    return launch_status();
+  });
+}
+
+int particles_pre(Ctx& c) {
+  int rc = part_lists(c);
+  if (!rc) rc = part_flags(c);
+  if (!rc) rc = part_drain(c);
+  if (!rc) rc = part_rho(c);
+  if (!rc) rc = part_fill(c);
+  if (!rc) rc = part_virtual(c);
+  return rc;
 }
 
 int particles_fluid(Ctx& c) {
@@ -1404,45 +1551,61 @@ int particles_fluid(Ctx& c) {
   });
 }
 
-int particles_post(Ctx& c) {
-  ParticleState& s = *c.part;
-  Geom g = geom(c);
-  PDev P = pdev(c);
-  const int fn = 1 - c.fcur;
-  const double* pc = s.pos[s.pcur];
-  const int64_t st = c.step + 1;
-  int rc = by_storage(c, [&](auto* tag) {
+// partBB_CG (BB_N2P), partBB_CG_p2n (BB_COPY), partBB_CG_p2n2 (BB_WALL)
+int part_bb(Ctx& c, int mode) {
+  Stage t(c);
+  if (mode < 1 || mode > BB_ALL) return LBX_ERR_ARG;
+  return by_storage(c, [&](auto* tag) {
     using S = std::remove_pointer_t<decltype(tag)>;
     using C = typename Store<S>::C;
-    S* B = (S*)c.pops[1 - c.cur];
-    Shift<C> sh = make_shift<C>(c);
-    LatticeT<C> L = make_lattice<C>();
-    C* rR = (C*)c.rho[0];
-    C* rB = (C*)c.rho[1];
-    k_bb<S><<<s.np, 256, 0, c.stream>>>(P, pc, s.acc, B, g, sh, L, c.flags[fn], rR, rB);
-    const int warp_blocks = (s.np * 32 + 255) / 256;
-    k_pairs<<<warp_blocks, 256, 0, c.stream>>>(P, pc, s.acc, g);
-    if (c.p.closure) {
-      const int use_net = s.closure_ready;
-      const double cut = fmax(double(c.p.closure_gap_max) * s.rdim, c.p.lubrication ? double(c.p.lubric_rmin) : 0.0);
-      k_pair_nbrs<<<warp_blocks, 256, 0, c.stream>>>(P, pc, g, cut, s.nbr, s.nbr_cnt, c.d_err, st);
-      size_t smem = sizeof(float) * (size_t(LBX_CLOSURE_NWEIGHTS) + 8 * 2 * H);
-      int blocks = (s.np * NBCAP + 7) / 8;
-      if (blocks > 148 * 4) blocks = 148 * 4;
-      k_closure_pairs<<<blocks, 256, smem, c.stream>>>(P, pc, g, s.wclosure, use_net, s.nbr, s.nbr_cnt, s.corr);
-      k_closure_accum<<<(s.np + 127) / 128, 128, 0, c.stream>>>(P, s.nbr, s.nbr_cnt, s.corr, s.acc);
-    }
-    k_integrate<<<(s.np + 127) / 128, 128, 0, c.stream>>>(P, pc, s.pos[1 - s.pcur], s.frc[s.pcur],
-                                                          s.frc[1 - s.pcur], s.acc, g, c.d_err, st);
+    k_bb<S><<<t.s.np, 256, 0, c.stream>>>(t.P, t.pc, t.s.acc, (S*)c.pops[1 - c.cur], t.g, make_shift<C>(c),
+                                           make_lattice<C>(), c.flags[t.fn], (const C*)c.rho[0], (const C*)c.rho[1],
+                                           mode);
     return launch_status();
   });
+}
+
+// inter_force_particles: Hertz and analytic lubrication, then the closure
+int part_pairs(Ctx& c) {
+  Stage t(c);
+  ParticleState& s = t.s;
+  const int warp_blocks = (s.np * 32 + 255) / 256;
+  k_pairs<<<warp_blocks, 256, 0, c.stream>>>(t.P, t.pc, s.acc, t.g);
+  if (c.p.closure) {
+    const int use_net = s.closure_ready;
+    const double cut = fmax(double(c.p.closure_gap_max) * s.rdim, c.p.lubrication ? double(c.p.lubric_rmin) : 0.0);
+    k_pair_nbrs<<<warp_blocks, 256, 0, c.stream>>>(t.P, t.pc, t.g, cut, s.nbr, s.nbr_cnt, c.d_err, t.st);
+    size_t smem = sizeof(float) * (size_t(LBX_CLOSURE_NWEIGHTS) + 8 * 2 * H);
+    int blocks = (s.np * NBCAP + 7) / 8;
+    if (blocks > 148 * 4) blocks = 148 * 4;
+    k_closure_pairs<<<blocks, 256, smem, c.stream>>>(t.P, t.pc, t.g, s.wclosure, use_net, s.nbr, s.nbr_cnt, s.corr);
+    k_closure_accum<<<(s.np + 127) / 128, 128, 0, c.stream>>>(t.P, s.nbr, s.nbr_cnt, s.corr, s.acc);
+  }
+  return launch_status();
+}
+
+// time_step_force_particles, then the end of the step: every ping-pong
+// index (populations, flags, particle records) flips
+int part_integrate(Ctx& c) {
+  Stage t(c);
+  ParticleState& s = t.s;
+  k_integrate<<<(s.np + 127) / 128, 128, 0, c.stream>>>(t.P, t.pc, s.pos[1 - s.pcur], s.frc[s.pcur],
+                                                        s.frc[1 - s.pcur], s.acc, t.g, c.d_err, t.st);
+  int rc = launch_status();
   if (rc) return rc;
   c.cur = 1 - c.cur;
-  c.fcur = fn;
-  s.flags_last = fn;
+  c.fcur = t.fn;
+  s.flags_last = t.fn;
   s.pcur = 1 - s.pcur;
   c.step += 1;
   return 0;
+}
+
+int particles_post(Ctx& c) {
+  int rc = part_bb(c, BB_ALL);
+  if (!rc) rc = part_pairs(c);
+  if (!rc) rc = part_integrate(c);
+  return rc;
 }
 
 int particles_step(Ctx& c) {

@@ -40,3 +40,7 @@ def test_invalid_arguments_rejected_without_gpu():
     assert L.lbx_create(ctypes.byref(p), ctypes.byref(h)) == -2
     assert L.lbx_step(None, 1) == -2
     assert L.lbx_destroy(None) == -2
+    for name in ("lbx_make_list_atoms", "lbx_init_isfluid", "lbx_del_fluid", "lbx_make_fluid", "lbx_virtual_rho",
+                 "lbx_partbb", "lbx_partbb_p2n", "lbx_partbb_p2n2", "lbx_inter_force_particles",
+                 "lbx_time_step_force_particles"):
+        assert getattr(L, name)(None) == -2, name
