@@ -115,32 +115,48 @@ __device__ __forceinline__ double2 p_fma(double2 a, double2 b, double2 c) {
   return make_double2(fma(a.x, b.x, c.x), fma(a.y, b.y, c.y));
 }
 
-// storage pair <-> arithmetic pair
+// storage pair <-> arithmetic pair (R: the stored pair as one word)
 template <typename S> struct SPair;
 template <> struct SPair<float> {
-  static __device__ __forceinline__ float2 ld(const float* p) { return __ldg(reinterpret_cast<const float2*>(p)); }
+  using R = float2;
+  static __device__ __forceinline__ R ldr(const float* p) { return __ldg(reinterpret_cast<const float2*>(p)); }
+  static __device__ __forceinline__ float2 cvt(R r) { return r; }
+  static __device__ __forceinline__ float2 ld(const float* p) { return cvt(ldr(p)); }
   static __device__ __forceinline__ void st(float* p, float2 v) { *reinterpret_cast<float2*>(p) = v; }
 };
 template <> struct SPair<double> {
-  static __device__ __forceinline__ double2 ld(const double* p) { return __ldg(reinterpret_cast<const double2*>(p)); }
+  using R = double2;
+  static __device__ __forceinline__ R ldr(const double* p) { return __ldg(reinterpret_cast<const double2*>(p)); }
+  static __device__ __forceinline__ double2 cvt(R r) { return r; }
+  static __device__ __forceinline__ double2 ld(const double* p) { return cvt(ldr(p)); }
   static __device__ __forceinline__ void st(double* p, double2 v) { *reinterpret_cast<double2*>(p) = v; }
 };
 template <> struct SPair<__half> {
-  static __device__ __forceinline__ float2 ld(const __half* p) {
-    return __half22float2(__ldg(reinterpret_cast<const __half2*>(p)));
-  }
+  using R = __half2;
+  static __device__ __forceinline__ R ldr(const __half* p) { return __ldg(reinterpret_cast<const __half2*>(p)); }
+  static __device__ __forceinline__ float2 cvt(R r) { return __half22float2(r); }
+  static __device__ __forceinline__ float2 ld(const __half* p) { return cvt(ldr(p)); }
   static __device__ __forceinline__ void st(__half* p, float2 v) {
     *reinterpret_cast<__half2*>(p) = __float22half2_rn(v);
   }
 };
 template <> struct SPair<__nv_bfloat16> {
-  static __device__ __forceinline__ float2 ld(const __nv_bfloat16* p) {
-    return __bfloat1622float2(__ldg(reinterpret_cast<const __nv_bfloat162*>(p)));
+  using R = __nv_bfloat162;
+  static __device__ __forceinline__ R ldr(const __nv_bfloat16* p) {
+    return __ldg(reinterpret_cast<const __nv_bfloat162*>(p));
   }
+  static __device__ __forceinline__ float2 cvt(R r) { return __bfloat1622float2(r); }
+  static __device__ __forceinline__ float2 ld(const __nv_bfloat16* p) { return cvt(ldr(p)); }
   static __device__ __forceinline__ void st(__nv_bfloat16* p, float2 v) {
     *reinterpret_cast<__nv_bfloat162*>(p) = __float22bfloat162_rn(v);
   }
 };
+
+// 16-bit storage keeps the pulled pairs of its own cells in shared memory for
+// one iteration (4 bytes a pair); FP32 / FP64 pairs re-read them from L2,
+// which measured faster than a stage of 8 / 16-byte pairs.
+template <typename S>
+constexpr bool kStage = sizeof(typename SPair<S>::R) == 4;
 
 // element offset of direction l (both components) of a cell: 2 (l n + cell)
 __device__ __forceinline__ size_t poff(int64_t n, int l, int cell) { return (size_t(l) * size_t(n) + size_t(cell)) * 2; }
@@ -155,20 +171,34 @@ struct Planes {
   __device__ __forceinline__ S* operator()(int l) const { return p + size_t(l) * size_t(n2); }
 };
 
-// clamped densities (Sum g + rho0, init_rho*_CG) of the pulled cell
+// densities (Sum g + rho0, init_rho*_CG, before the clamp) of the pulled
+// cell; with a stage, the pulled pairs are also kept there (direction l at
+// st[l * stride]) for the collision of the same cell one plane later
 template <typename S, typename C>
 __device__ __forceinline__ void pull_rho(const S* __restrict__ A, int64_t n, const PullIdx& P, const LeanConst<C>& K,
-                                         C& rR, C& rB) {
+                                         C& rR, C& rB, typename SPair<S>::R* st = nullptr, int stride = 0) {
   const Planes<const S> Ap{A, 2 * n};
-  P2<C> s = SPair<S>::ld(Ap(0) + 2 * P.src[0]);
+  typename SPair<S>::R r = SPair<S>::ldr(Ap(0) + 2 * P.src[0]);
+  if (st) st[0] = r;
+  P2<C> s = SPair<S>::cvt(r);
 #pragma unroll
-  for (int l = 1; l < Q; ++l) s = p_add(s, SPair<S>::ld(Ap(l) + 2 * P.src[l]));
+  for (int l = 1; l < Q; ++l) {
+    r = SPair<S>::ldr(Ap(l) + 2 * P.src[l]);
+    if (st) st[l * stride] = r;
+    s = p_add(s, SPair<S>::cvt(r));
+  }
   rR = s.x + K.rho0[0];
   rB = s.y + K.rho0[1];
 }
 
 template <typename C>
 __device__ __forceinline__ C clamp0(C v) { return v < C(0) ? C(0) : v; }
+
+// a * b + c with one rounding.  This file is compiled without automatic
+// contraction (-fmad=false): every fused operation is written out, so each
+// kernel that inlines the collision rounds identically.
+template <typename C>
+__device__ __forceinline__ C fm(C a, C b, C c) { return fma(a, b, c); }
 
 // One colour-gradient collision (time_step_CG, kernels_fluid_CG.CUF:689-846)
 // on the component pairs g[l] = (g_R, g_B): stored form (f - shift) on entry,
@@ -184,7 +214,7 @@ __device__ __forceinline__ void collide_pair(const LeanConst<C>& K, P2<C> g[Q], 
   } else {
     const C ph = (rR - rB) / rs;
     const C visc = ONE / (HALF * (ONE + ph) * K.inv_viscR + HALF * (ONE - ph) * K.inv_viscB);
-    omega = ONE / (visc * K.inv_cssq + HALF);
+    omega = ONE / fm(visc, K.inv_cssq, HALF);
   }
   const C omm = ONE - omega;
   const C inv = ONE / rs;
@@ -200,7 +230,7 @@ __device__ __forceinline__ void collide_pair(const LeanConst<C>& K, P2<C> g[Q], 
   const C u = inv * (d[1] + d[4] - d[5] + d[6] - d[7]);
   const C v = inv * (d[2] + d[4] + d[5] + d[8] - d[9]);
   const C w = inv * (d[3] + d[6] + d[7] + d[8] + d[9]);
-  const C c0 = ONE - C(1.5) * (u * u + v * v + w * w);
+  const C c0 = fm(C(-1.5), fm(u, u, fm(v, v, w * w)), ONE);
   P2<C> Kc[3], ns[3];
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
@@ -217,7 +247,7 @@ __device__ __forceinline__ void collide_pair(const LeanConst<C>& K, P2<C> g[Q], 
   for (int p = 1; p <= 9; ++p) {
     const int l = 2 * p - 1, o = 2 * p, k = wclass(l);
     const C eu = edot(l, u, v, w);
-    const C P = c0 + C(4.5) * eu * eu;
+    const C P = fm(C(4.5) * eu, eu, c0);
     const C Qv = C(3) * eu;
     const C Ap = P + Qv, Am = P - Qv;
     const P2<C> fl = shifted ? p_fma(ns[k], NEG, g[l]) : g[l];
@@ -225,7 +255,7 @@ __device__ __forceinline__ void collide_pair(const LeanConst<C>& K, P2<C> g[Q], 
     g[l] = p_fma(fl, omm2, p_mul(Kc[k], pp(Ap, Ap)));
     g[o] = p_fma(fo, omm2, p_mul(Kc[k], pp(Am, Am)));
   }
-  const C psq = px * px + py * py + pz * pz;
+  const C psq = fm(px, px, fm(py, py, pz * pz));
   if (psq > C(1.e-20)) {
     const C pn = sqrt(psq);
     const C ipn = ONE / pn;
@@ -249,7 +279,7 @@ __device__ __forceinline__ void collide_pair(const LeanConst<C>& K, P2<C> g[Q], 
     for (int p = 1; p <= 9; ++p) {
       const int l = 2 * p - 1, o = 2 * p, k = wclass(l);
       const C ed = edot(l, px, py, pz);
-      const C pert = K1[k] * (ed * ed) - K0[k];
+      const C pert = fm(K1[k], ed * ed, -K0[k]);
       const C T = K3[k] * ed;
       const C fdp = g[l].x + g[l].y + pert;
       const C fdm = g[o].x + g[o].y + pert;
@@ -290,14 +320,36 @@ struct LeanPart {
   const C* __restrict__ rhoB;
 };
 
+// Shared memory of one CTA: the rolling phase-field window (4 planes of the
+// column and its ring) and, for 16-bit storage, the stage of pulled pairs (2
+// planes x Q directions x the column's cells: what a thread pulls for its own
+// cell one plane ahead it collides one iteration later, so that pull is not
+// repeated).
+template <typename S, int TX, int TY>
+struct LeanSmem {
+  using C = typename Store<S>::C;
+  using R = typename SPair<S>::R;
+  static constexpr size_t PHI = sizeof(C) * 4 * Ring<TX, TY>::CELLS;
+  static constexpr size_t BYTES = PHI + (kStage<S> ? sizeof(R) * 2 * Q * TX * TY : 0);
+  static_assert(PHI % 16 == 0, "stage alignment");
+  static __device__ __forceinline__ C (*phi(unsigned char* base))[Ring<TX, TY>::CELLS] {
+    return reinterpret_cast<C(*)[Ring<TX, TY>::CELLS]>(base);
+  }
+  static __device__ __forceinline__ R* stage(unsigned char* base) {
+    return kStage<S> ? reinterpret_cast<R*>(base + PHI) : nullptr;
+  }
+};
+
 // One column march: cells [x0, x0+TX) x [y0, y0+TY) x [z0, zend) of one box.
 template <typename S, int TX, int TY, bool PART>
 __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restrict__ B, const Geom& g,
                                             const LeanConst<typename Store<S>::C>& K, int x0, int y0, int z0,
                                             int zend, unsigned long long* err, int64_t step,
                                             const LeanPart<typename Store<S>::C>& PT,
-                                            typename Store<S>::C (*sphi)[Ring<TX, TY>::CELLS]) {
+                                            typename Store<S>::C (*sphi)[Ring<TX, TY>::CELLS],
+                                            typename SPair<S>::R* stage) {
   using C = typename Store<S>::C;
+  constexpr int NT = TX * TY;
   using R = Ring<TX, TY>;
   const bool parts = PART && PT.fnew != nullptr;  // a box of the ensemble may have no spheres
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
@@ -319,7 +371,7 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
   // cell), zero for every other solid cell (init_rho*_CG's MINDENS).  The
   // pull is issued together with the flag loads and discarded for the few
   // cells that do not use it, so the flags add no round trip to the pull.
-  auto densities = [&](int cx, int cy, int zz, bool check, C& rR, C& rB) {
+  auto densities = [&](int cx, int cy, int zz, bool check, C& rR, C& rB, typename SPair<S>::R* st) {
     const int cell = cx + g.nx * (cy + g.ny * zz);
     int8_t fn = LBX_FLUID_FLUID, fo = LBX_FLUID_FLUID;
     if (parts) {
@@ -328,7 +380,7 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
     }
     PullIdx P;
     pull_idx(g, cx, cy, zz, P);
-    pull_rho<S, C>(A, g.n, P, K, rR, rB);
+    pull_rho<S, C>(A, g.n, P, K, rR, rB, st, NT);
     if (parts && (fn != LBX_FLUID_FLUID || fo != LBX_FLUID_FLUID)) {
       if (fn == LBX_FLUID_FLUID || fn == LBX_FLUID_SPHERELIST) {
         rR = PT.rhoR[cell];
@@ -346,18 +398,19 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
     return true;
   };
 
-  // phase field of plane z (own cell and ring cell) into slot
+  // phase field of plane z (own cell and ring cell) into slot; with a stage,
+  // the own cell's pulled pairs into stage slot z & 1
   auto phase_plane = [&](int z, int slot, C& rRo, C& rBo) {
     const int zz = wrap0(z, g.nz);
     const bool owned = active && z >= z0 && z < zend;
     C rR, rB;
-    densities(x, y, zz, owned, rR, rB);
+    densities(x, y, zz, owned, rR, rB, kStage<S> ? stage + (z & 1) * (Q * NT) + tid : nullptr);
     rRo = rR;
     rBo = rB;
     sphi[slot][own] = (rR - rB) / (rR + rB);
     if (ringer) {
       C qR, qB;
-      densities(rxg, ryg, zz, false, qR, qB);
+      densities(rxg, ryg, zz, false, qR, qB, nullptr);
       sphi[slot][rslot] = (qR - qB) / (qR + qB);
     }
   };
@@ -383,9 +436,16 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
         fn = PT.fnew[cell];
         fo = PT.fold[cell];
       }
-      // the pull every fluid cell needs, issued with the flag loads
+      // the pull every fluid cell needs: staged one iteration ago, or issued
+      // here together with the flag loads
+      if constexpr (kStage<S>) {
+        const typename SPair<S>::R* sg = stage + (z & 1) * (Q * NT) + tid;
 #pragma unroll
-      for (int l = 0; l < Q; ++l) gp[l] = SPair<S>::ld(Ap(l) + 2 * P.src[l]);
+        for (int l = 0; l < Q; ++l) gp[l] = SPair<S>::cvt(sg[l * NT]);
+      } else {
+#pragma unroll
+        for (int l = 0; l < Q; ++l) gp[l] = SPair<S>::ld(Ap(l) + 2 * P.src[l]);
+      }
       if (parts) {
         collide = fn == LBX_FLUID_FLUID;
         if (collide && fo != LBX_FLUID_FLUID) {
@@ -411,9 +471,9 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
           const C* pl = dz < 0 ? pm : (dz > 0 ? ppl : p0);
           const C ps = pl[own + dy * R::RX + dx];
           const C a = K.a27[wclass27(l)];
-          if (dx) px = px + (dx > 0 ? a : -a) * ps;
-          if (dy) py = py + (dy > 0 ? a : -a) * ps;
-          if (dz) pz = pz + (dz > 0 ? a : -a) * ps;
+          if (dx) px = fm(dx > 0 ? a : -a, ps, px);
+          if (dy) py = fm(dy > 0 ? a : -a, ps, py);
+          if (dz) pz = fm(dz > 0 ? a : -a, ps, pz);
         }
         collide_pair(K, gp, rRc, rBc, px, py, pz, Store<S>::shifted);
       }
@@ -429,11 +489,11 @@ template <typename S, int TX, int TY, int MINB, bool PART>
 __global__ void __launch_bounds__(TX* TY, MINB)
     k_cg_lean(const S* __restrict__ A, S* __restrict__ B, Geom g, LeanConst<typename Store<S>::C> K, int zlen,
               unsigned long long* err, int64_t step, LeanPart<typename Store<S>::C> PT) {
-  using C = typename Store<S>::C;
-  __shared__ C sphi[4][Ring<TX, TY>::CELLS];
+  extern __shared__ __align__(16) unsigned char lean_smem[];
+  using M = LeanSmem<S, TX, TY>;
   const int z0 = blockIdx.z * zlen;
   lean_column<S, TX, TY, PART>(A, B, g, K, blockIdx.x * TX, blockIdx.y * TY, z0, min(z0 + zlen, g.nz), err, step,
-                               PT, sphi);
+                               PT, M::phi(lean_smem), M::stage(lean_smem));
 }
 
 // ---------------------------------------------------------------------------
@@ -460,12 +520,13 @@ __global__ void __launch_bounds__(TX* TY, MINB)
     k_cg_lean_multi(const BoxDesc<typename Store<S>::C>* __restrict__ boxes, const WorkItem* __restrict__ work,
                     int nwork, LeanConst<typename Store<S>::C> K) {
   using C = typename Store<S>::C;
-  __shared__ C sphi[4][Ring<TX, TY>::CELLS];
+  extern __shared__ __align__(16) unsigned char lean_smem[];
+  using M = LeanSmem<S, TX, TY>;
   for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
     const WorkItem it = work[w];
     const BoxDesc<C> bd = boxes[it.box];
     lean_column<S, TX, TY, PART>((const S*)bd.A, (S*)bd.B, bd.g, K, it.x0, it.y0, it.z0, it.zend, bd.err, bd.step,
-                                 bd.pt, sphi);
+                                 bd.pt, M::phi(lean_smem), M::stage(lean_smem));
     __syncthreads();  // the window is reused by the next item
   }
 }
@@ -480,14 +541,44 @@ static int lean_zlen(const Ctx& c, int tx, int ty, int per_sm) {
   return int((c.nz + segs - 1) / segs);
 }
 
+// Opt a kernel into its dynamic shared memory (beyond the default 48 KB), once
+// per device.  Called outside stream capture (the first eager launch, or when
+// an ensemble builds its tables).
+template <typename K>
+static int allow_smem(K* kernel, size_t bytes, unsigned long long& done_mask) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return LBX_ERR_CUDA;
+  const unsigned long long bit = 1ull << (dev & 63);
+  if (done_mask & bit) return 0;
+  if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)) != cudaSuccess)
+    return LBX_ERR_CUDA;
+  done_mask |= bit;
+  return 0;
+}
+
 template <typename S, int TX, int TY, int MINB, bool PART>
-static void launch_lean(Ctx& c, int zlen_override, LeanPart<typename Store<S>::C> pt) {
+static int prepare_lean() {
+  static unsigned long long done = 0;
+  return allow_smem(k_cg_lean<S, TX, TY, MINB, PART>, LeanSmem<S, TX, TY>::BYTES, done);
+}
+
+template <typename S, int TX, int TY, int MINB, bool PART>
+static int prepare_lean_multi() {
+  static unsigned long long done = 0;
+  return allow_smem(k_cg_lean_multi<S, TX, TY, MINB, PART>, LeanSmem<S, TX, TY>::BYTES, done);
+}
+
+template <typename S, int TX, int TY, int MINB, bool PART>
+static int launch_lean(Ctx& c, int zlen_override, LeanPart<typename Store<S>::C> pt) {
   using C = typename Store<S>::C;
+  const int rc = prepare_lean<S, TX, TY, MINB, PART>();
+  if (rc) return rc;
   int zlen = zlen_override > 0 ? zlen_override : lean_zlen(c, TX, TY, MINB);
   dim3 block(TX, TY, 1);
   dim3 grid((c.nx + TX - 1) / TX, (c.ny + TY - 1) / TY, (c.nz + zlen - 1) / zlen);
-  k_cg_lean<S, TX, TY, MINB, PART><<<grid, block, 0, c.stream>>>(
+  k_cg_lean<S, TX, TY, MINB, PART><<<grid, block, LeanSmem<S, TX, TY>::BYTES, c.stream>>>(
       (const S*)c.pops[c.cur], (S*)c.pops[1 - c.cur], geom(c), make_lean<C>(c), zlen, c.d_err, c.step + 1, pt);
+  return 0;
 }
 
 void kt_begin(Ctx& c);
@@ -500,14 +591,15 @@ int fluid_lean(Ctx& c) {
     using C = typename Store<S>::C;
     LeanPart<C> none{nullptr, nullptr, nullptr, nullptr};
     kt_begin(c);
+    int r = 0;
     if constexpr (std::is_same<S, double>::value) {
-      launch_lean<S, 32, 8, 1, false>(c, c.lean_zlen, none);
+      r = launch_lean<S, 32, 8, 1, false>(c, c.lean_zlen, none);
     } else {
-      if (c.lean_shape == 1) launch_lean<S, 32, 16, 1, false>(c, c.lean_zlen, none);
-      else launch_lean<S, 32, 8, 2, false>(c, c.lean_zlen, none);
+      if (c.lean_shape == 1) r = launch_lean<S, 32, 16, 1, false>(c, c.lean_zlen, none);
+      else r = launch_lean<S, 32, 8, 2, false>(c, c.lean_zlen, none);
     }
     kt_end(c);
-    return launch_status();
+    return r ? r : launch_status();
   });
   if (!rc) c.cur = 1 - c.cur;
   return rc;
@@ -520,10 +612,11 @@ int fluid_lean_particles(Ctx& c, int fo, int fn) {
     using C = typename Store<S>::C;
     LeanPart<C> pt{c.flags[fo], c.flags[fn], (C*)c.rho[0], (C*)c.rho[1]};
     kt_begin(c);
-    if constexpr (std::is_same<S, double>::value) launch_lean<S, 32, 8, 1, true>(c, c.lean_zlen, pt);
-    else launch_lean<S, 32, 8, 2, true>(c, c.lean_zlen, pt);
+    int r = 0;
+    if constexpr (std::is_same<S, double>::value) r = launch_lean<S, 32, 8, 1, true>(c, c.lean_zlen, pt);
+    else r = launch_lean<S, 32, 8, 2, true>(c, c.lean_zlen, pt);
     kt_end(c);
-    return launch_status();
+    return r ? r : launch_status();
   });
   return rc;  // the particle step swaps the buffers after its bounce-back
 }
@@ -566,6 +659,15 @@ int ensemble_launch(const std::vector<Ctx*>& boxes, int shape, const std::vector
       std::stable_sort(work.begin(), work.end(),
                        [](const WorkItem& a, const WorkItem& b) { return (a.zend - a.z0) > (b.zend - b.z0); });
       if (desc.size() * sizeof(BoxDesc<C>) > 512 * desc.size()) return LBX_ERR_STATE;
+      // shared-memory opt-in of every variant, before any capture
+      int rp = 0;
+      if constexpr (std::is_same<S, double>::value) {
+        rp = prepare_lean_multi<S, 32, 8, 1, true>();
+      } else {
+        rp = prepare_lean_multi<S, 32, 16, 1, true>();
+        if (!rp) rp = prepare_lean_multi<S, 32, 8, 2, true>();
+      }
+      if (rp) return rp;
       if (cudaMemcpy(d_desc, desc.data(), desc.size() * sizeof(BoxDesc<C>), cudaMemcpyHostToDevice) != cudaSuccess)
         return LBX_ERR_CUDA;
       if (cudaMemcpy(d_work, work.data(), work.size() * sizeof(WorkItem), cudaMemcpyHostToDevice) != cudaSuccess)
@@ -577,13 +679,14 @@ int ensemble_launch(const std::vector<Ctx*>& boxes, int shape, const std::vector
     const auto* W = (const WorkItem*)d_work;
     if constexpr (std::is_same<S, double>::value) {
       int grid = std::min(nwork, 148);
-      k_cg_lean_multi<S, 32, 8, 1, true><<<grid, dim3(32, 8), 0, stream>>>(D, W, nwork, K);
+      k_cg_lean_multi<S, 32, 8, 1, true><<<grid, dim3(32, 8), LeanSmem<S, 32, 8>::BYTES, stream>>>(D, W, nwork, K);
     } else if (shape == 1) {
       int grid = std::min(nwork, 148);
-      k_cg_lean_multi<S, 32, 16, 1, true><<<grid, dim3(32, 16), 0, stream>>>(D, W, nwork, K);
+      k_cg_lean_multi<S, 32, 16, 1, true><<<grid, dim3(32, 16), LeanSmem<S, 32, 16>::BYTES, stream>>>(D, W, nwork,
+                                                                                                      K);
     } else {
       int grid = std::min(nwork, 296);
-      k_cg_lean_multi<S, 32, 8, 2, true><<<grid, dim3(32, 8), 0, stream>>>(D, W, nwork, K);
+      k_cg_lean_multi<S, 32, 8, 2, true><<<grid, dim3(32, 8), LeanSmem<S, 32, 8>::BYTES, stream>>>(D, W, nwork, K);
     }
     return launch_status();
   });
