@@ -34,9 +34,12 @@ L = 128
 SEED = 1
 SIGMA, BETA = 0.02, 0.7
 LB_PER_STEP = 500
+# DRAM bytes (read + write) of one k_cg_lean launch at 128^3, from the ncu
+# captures summarised in profiles/ (None where no capture of that storage)
+TRAFFIC = {"f16": 298.1e6, "f32": None}
 BYTES_PER_CELL = {"f16": 160, "bf16": 160, "f32": 312, "f64": 616}  # algorithmic bytes per cell-step
 MINIMAL_BYTES = {"f16": 152, "bf16": 152, "f32": 304, "f64": 608}   # populations only (phi kept on chip)
-METRIC = "MLUPS (FP16-shifted storage, colour-gradient 128^3)"
+METRIC = "MLUPS & HBM GB/s, FP16-store vs FP32 LB at stated FP64 error, 1\u00d7B200"
 
 
 def peaks():
@@ -354,7 +357,9 @@ def main():
         alg = BYTES_PER_CELL[storage] * cells
         achieved = alg / (per_launch_ms * 1e-3) / 1e9
         return {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                "traffic": None, "peak_kind": peak_kind, "kernel": "k_cg_fused", "bytes_per_cell": BYTES_PER_CELL[storage],
+                "traffic": TRAFFIC.get(storage), "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, "
+                "one launch at 128^3 (profiles/)", "peak_kind": peak_kind, "kernel": "k_cg_lean",
+                "bytes_per_cell": BYTES_PER_CELL[storage],
                 "kernel_us_per_launch": per_launch_ms * 1e3,
                 "minimal_bytes_frac": MINIMAL_BYTES[storage] * cells / (per_launch_ms * 1e-3) / 1e9 / hbm}
 
@@ -402,7 +407,7 @@ def main():
         line = {
             "metric": METRIC, "value": mlups16, "unit": "MLUPS", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": tot16 / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f16 storage / f32 arithmetic", "data": "synthetic",
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": "colour-gradient spinodal 128^3 periodic, rho=0.5+U(-0.01,0.01) seed 1, "
                                    "tau=1, sigma=0.02, beta=0.7",
                        "lattice_steps_per_bench_step": LB_PER_STEP, "storage": "f16 shifted (f - w*0.5)",
@@ -414,8 +419,10 @@ def main():
             "fp16_over_fp32": mlups16 / mlups32,
             "clocks": clocks,
             "e2e": {"value": e2e_mlups, "unit": "MLUPS", "h2d_bytes_per_step": 2 * 4 * cells,
-                    "d2h_bytes_per_step": 6 * 4 * cells, "ms_per_step": e2e_ms / args.steps},
-            "gpu_launches": n16 + (n32 if True else 0) + args.steps * (LB_PER_STEP + 2),
+                    "d2h_bytes_per_step": 6 * 4 * cells, "ms_per_step": e2e_ms / args.steps,
+                    "timing": "host wall clock around the synchronous C-ABI calls, max over ranks",
+                    "gpu_launches_per_step": LB_PER_STEP + 2},
+            "gpu_launches": n16,
             "device_errors": [code16, code32],
         }
         line.update(extras)

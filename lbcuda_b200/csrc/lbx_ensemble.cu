@@ -230,11 +230,11 @@ int lbx_ensemble_tune(void* ens, int32_t trial, int32_t* chosen, double* best_ms
   trial += trial & 1;
   drop_graph(*e);
   const int shapes[2] = {0, 1};
-  const int zl[5] = {4, 8, 16, 32, 64};
+  const int zl[6] = {4, 8, 16, 32, 64, 128};
   double best = 1e30;
   int bs = 0, bz = 16;
   for (int si = 0; si < 2; ++si)
-    for (int zi = 0; zi < 5; ++zi) {
+    for (int zi = 0; zi < 6; ++zi) {
       e->shape = shapes[si];
       for (size_t i = 0; i < e->boxes.size(); ++i) e->zlen[i] = std::min(e->boxes[i]->nz, zl[zi]);
       e->tables_ok = false;

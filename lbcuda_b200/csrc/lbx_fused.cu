@@ -171,6 +171,38 @@ struct Planes {
   __device__ __forceinline__ S* operator()(int l) const { return p + size_t(l) * size_t(n2); }
 };
 
+// ---- asynchronous copies global -> shared (cp.async, 4-byte granules) --------
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// issue the 19 pulls of a cell as asynchronous copies into st[l * stride]
+template <typename S>
+__device__ __forceinline__ void pull_async(const S* __restrict__ A, int64_t n, const PullIdx& P,
+                                           typename SPair<S>::R* st, int stride) {
+  static_assert(sizeof(typename SPair<S>::R) == 4, "4-byte pairs");
+  const Planes<const S> Ap{A, 2 * n};
+#pragma unroll
+  for (int l = 0; l < Q; ++l) cp_async4(st + l * stride, Ap(l) + 2 * P.src[l]);
+}
+
+// densities (Sum g + rho0, before the clamp) from pairs already in shared memory
+template <typename S, typename C>
+__device__ __forceinline__ void stage_rho(const typename SPair<S>::R* st, int stride, const LeanConst<C>& K, C& rR,
+                                          C& rB) {
+  P2<C> s = SPair<S>::cvt(st[0]);
+#pragma unroll
+  for (int l = 1; l < Q; ++l) s = p_add(s, SPair<S>::cvt(st[l * stride]));
+  rR = s.x + K.rho0[0];
+  rB = s.y + K.rho0[1];
+}
+
 // densities (Sum g + rho0, init_rho*_CG, before the clamp) of the pulled
 // cell; with a stage, the pulled pairs are also kept there (direction l at
 // st[l * stride]) for the collision of the same cell one plane later
@@ -321,17 +353,21 @@ struct LeanPart {
 };
 
 // Shared memory of one CTA: the rolling phase-field window (4 planes of the
-// column and its ring) and, for 16-bit storage, the stage of pulled pairs (2
-// planes x Q directions x the column's cells: what a thread pulls for its own
-// cell one plane ahead it collides one iteration later, so that pull is not
-// repeated).
+// column and its ring) and, for 16-bit storage, the stage that the pulls land
+// in by cp.async: 3 planes x Q directions x the column's cells (a plane is
+// copied two iterations before its collision, summed into densities one
+// iteration before, and collided from the same copy), then 2 planes x Q x
+// the ring cells (summed only).
 template <typename S, int TX, int TY>
 struct LeanSmem {
   using C = typename Store<S>::C;
   using R = typename SPair<S>::R;
+  static constexpr int NT = TX * TY, RN = Ring<TX, TY>::N;
   static constexpr size_t PHI = sizeof(C) * 4 * Ring<TX, TY>::CELLS;
-  static constexpr size_t BYTES = PHI + (kStage<S> ? sizeof(R) * 2 * Q * TX * TY : 0);
-  static_assert(PHI % 16 == 0, "stage alignment");
+  static constexpr size_t OWN = kStage<S> ? sizeof(R) * 3 * Q * NT : 0;
+  static constexpr size_t RING = kStage<S> ? sizeof(R) * 2 * Q * RN : 0;
+  static constexpr size_t BYTES = PHI + OWN + RING;
+  static_assert(PHI % 16 == 0 && OWN % 16 == 0, "stage alignment");
   static __device__ __forceinline__ C (*phi(unsigned char* base))[Ring<TX, TY>::CELLS] {
     return reinterpret_cast<C(*)[Ring<TX, TY>::CELLS]>(base);
   }
@@ -366,21 +402,29 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
   const int rxg = wrap0(x0 + rx - 1, g.nx), ryg = wrap0(y0 + ry - 1, g.ny);
   const int rslot = ry * R::RX + rx;
 
+  using SR = typename SPair<S>::R;
+  constexpr int RN = R::N;
+  SR* const ring_stage = kStage<S> ? stage + 3 * Q * NT : nullptr;
+  const Planes<const S> Ap{A, 2 * g.n};
+  const Planes<S> Bp{B, 2 * g.n};
+
   // clamped densities of cell (cx, cy, zz): pulled (fluid in both steps),
   // from the side arrays (new fluid, or the virtual density of a surface
-  // cell), zero for every other solid cell (init_rho*_CG's MINDENS).  The
-  // pull is issued together with the flag loads and discarded for the few
-  // cells that do not use it, so the flags add no round trip to the pull.
-  auto densities = [&](int cx, int cy, int zz, bool check, C& rR, C& rB, typename SPair<S>::R* st) {
+  // cell), zero for every other solid cell (init_rho*_CG's MINDENS).  16-bit
+  // storage sums the pairs its copies brought into the stage (st, stride);
+  // wider types pull here.  The flags are loaded beside the pull and the pull
+  // is discarded for the few cells that do not use it.
+  // fl: the cell's flags (bits 0-7 this step, 8-15 the previous step)
+  auto densities = [&](int cx, int cy, int zz, bool check, C& rR, C& rB, const SR* st, int stride, unsigned fl) {
     const int cell = cx + g.nx * (cy + g.ny * zz);
-    int8_t fn = LBX_FLUID_FLUID, fo = LBX_FLUID_FLUID;
-    if (parts) {
-      fn = PT.fnew[cell];
-      fo = PT.fold[cell];
+    const int8_t fn = int8_t(fl & 255u), fo = int8_t((fl >> 8) & 255u);
+    if constexpr (kStage<S>) {
+      stage_rho<S, C>(st, stride, K, rR, rB);
+    } else {
+      PullIdx P;
+      pull_idx(g, cx, cy, zz, P);
+      pull_rho<S, C>(A, g.n, P, K, rR, rB);
     }
-    PullIdx P;
-    pull_idx(g, cx, cy, zz, P);
-    pull_rho<S, C>(A, g.n, P, K, rR, rB, st, NT);
     if (parts && (fn != LBX_FLUID_FLUID || fo != LBX_FLUID_FLUID)) {
       if (fn == LBX_FLUID_FLUID || fn == LBX_FLUID_SPHERELIST) {
         rR = PT.rhoR[cell];
@@ -398,48 +442,89 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
     return true;
   };
 
-  // phase field of plane z (own cell and ring cell) into slot; with a stage,
-  // the own cell's pulled pairs into stage slot z & 1
-  auto phase_plane = [&](int z, int slot, C& rRo, C& rBo) {
-    const int zz = wrap0(z, g.nz);
-    const bool owned = active && z >= z0 && z < zend;
+  // stage slots of plane p (p >= z0 - 1): own cells 3 deep, ring cells 2 deep
+  auto own_slot = [&](int p) { return stage + ((p - z0 + 1) % 3) * (Q * NT) + tid; };
+  auto ring_slot = [&](int p) { return ring_stage + ((p - z0 + 1) & 1) * (Q * RN) + tid; };
+
+  // Start plane p: 16-bit storage copies the pulls of the own and the ring
+  // cell into the stage (one copy group); with spheres, the flags of both
+  // cells are loaded here too and returned packed (own: bits 0-15, ring:
+  // 16-31; each this step | previous step << 8), two iterations before use.
+  constexpr unsigned FLUID2 = unsigned(LBX_FLUID_FLUID) | (unsigned(LBX_FLUID_FLUID) << 8);
+  auto issue = [&](int p) -> unsigned {
+    const int zz = wrap0(p, g.nz);
+    unsigned fl = FLUID2 | (FLUID2 << 16);
+    if (parts) {
+      const int co = x + g.nx * (y + g.ny * zz), cr = rxg + g.nx * (ryg + g.ny * zz);
+      fl = unsigned(uint8_t(PT.fnew[co])) | (unsigned(uint8_t(PT.fold[co])) << 8);
+      if (ringer) fl |= (unsigned(uint8_t(PT.fnew[cr])) << 16) | (unsigned(uint8_t(PT.fold[cr])) << 24);
+      else fl |= FLUID2 << 16;
+    }
+    if constexpr (kStage<S>) {
+      PullIdx P;
+      pull_idx(g, x, y, zz, P);
+      pull_async<S>(A, g.n, P, own_slot(p), NT);
+      if (ringer) {
+        pull_idx(g, rxg, ryg, zz, P);
+        pull_async<S>(A, g.n, P, ring_slot(p), RN);
+      }
+      cp_async_commit();
+    }
+    return fl;
+  };
+  auto settle = [&]() {  // every copy group but the newest has landed
+    if constexpr (kStage<S>) cp_async_wait<1>();
+  };
+
+  // phase field of plane p (own cell and ring cell) into its window slot
+  auto phase_plane = [&](int p, unsigned fl, C& rRo, C& rBo) {
+    const int zz = wrap0(p, g.nz);
+    const bool owned = active && p >= z0 && p < zend;
     C rR, rB;
-    densities(x, y, zz, owned, rR, rB, kStage<S> ? stage + (z & 1) * (Q * NT) + tid : nullptr);
+    densities(x, y, zz, owned, rR, rB, kStage<S> ? own_slot(p) : nullptr, NT, fl & 0xffffu);
     rRo = rR;
     rBo = rB;
-    sphi[slot][own] = (rR - rB) / (rR + rB);
+    sphi[p & 3][own] = (rR - rB) / (rR + rB);
     if (ringer) {
       C qR, qB;
-      densities(rxg, ryg, zz, false, qR, qB, nullptr);
-      sphi[slot][rslot] = (qR - qB) / (qR + qB);
+      densities(rxg, ryg, zz, false, qR, qB, kStage<S> ? ring_slot(p) : nullptr, RN, fl >> 16);
+      sphi[p & 3][rslot] = (qR - qB) / (qR + qB);
     }
   };
 
   C rRn, rBn, rRc, rBc;
-  phase_plane(z0 - 1, (z0 + 3) & 3, rRc, rBc);
-  phase_plane(z0, z0 & 3, rRn, rBn);
+  const unsigned flm = issue(z0 - 1);
+  unsigned flz = issue(z0);  // flags of plane z, then z+1 (loop carried)
+  settle();
+  phase_plane(z0 - 1, flm, rRc, rBc);
+  unsigned flz1 = issue(z0 + 1);
+  settle();
+  phase_plane(z0, flz, rRn, rBn);
   for (int z = z0; z < zend; ++z) {
     rRc = rRn;
     rBc = rBn;
-    phase_plane(z + 1, (z + 1) & 3, rRn, rBn);
+    // plane z+2 is copied while z+1 is summed and z collided; the copy into
+    // the slot of plane z-1 starts after this thread's last read of it
+    unsigned flz2 = FLUID2 | (FLUID2 << 16);
+    if (z + 2 <= zend) flz2 = issue(z + 2);
+    else if constexpr (kStage<S>) cp_async_commit();  // one group per iteration
+    settle();
+    phase_plane(z + 1, flz1, rRn, rBn);
     __syncthreads();
+    const unsigned flc = flz;
+    flz = flz1;
+    flz1 = flz2;
     if (active) {
       const int cell = x + g.nx * (y + g.ny * z);
-      PullIdx P;
-      pull_idx(g, x, y, z, P);
-      const Planes<const S> Ap{A, 2 * g.n};
-      const Planes<S> Bp{B, 2 * g.n};
       P2<C> gp[Q];
       bool collide = true;
-      int8_t fn = LBX_FLUID_FLUID, fo = LBX_FLUID_FLUID;
-      if (parts) {
-        fn = PT.fnew[cell];
-        fo = PT.fold[cell];
-      }
-      // the pull every fluid cell needs: staged one iteration ago, or issued
-      // here together with the flag loads
+      const int8_t fn = int8_t(flc & 255u), fo = int8_t((flc >> 8) & 255u);
+      PullIdx P;
+      pull_idx(g, x, y, z, P);
+      // the pull every fluid cell needs: in the stage since two iterations,
+      // or issued here together with the flag loads
       if constexpr (kStage<S>) {
-        const typename SPair<S>::R* sg = stage + (z & 1) * (Q * NT) + tid;
+        const SR* sg = own_slot(z);
 #pragma unroll
         for (int l = 0; l < Q; ++l) gp[l] = SPair<S>::cvt(sg[l * NT]);
       } else {
@@ -480,9 +565,10 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
 #pragma unroll
       for (int l = 0; l < Q; ++l) SPair<S>::st(Bp(l) + 2 * cell, gp[l]);
     }
-    // slot (z+3)&3 read above is rewritten in iteration z+2; the barrier of
-    // iteration z+1 orders that write after these reads
+    // window slot (z+3)&3 read above is rewritten in iteration z+2; the
+    // barrier of iteration z+1 orders that write after these reads
   }
+  if constexpr (kStage<S>) cp_async_wait<0>();  // nothing in flight when the stage is reused
 }
 
 template <typename S, int TX, int TY, int MINB, bool PART>
@@ -532,12 +618,21 @@ __global__ void __launch_bounds__(TX* TY, MINB)
 }
 
 // ---------------------------------------------------------------------------
-static int lean_zlen(const Ctx& c, int tx, int ty, int per_sm) {
-  long cols = long((c.nx + tx - 1) / tx) * long((c.ny + ty - 1) / ty);
-  long target = 148L * per_sm * 2;
-  long segs = (target + cols - 1) / cols;
-  if (segs < 1) segs = 1;
-  if (segs > c.nz) segs = c.nz;
+// z-segment length of the fluid kernel.  A segment costs two extra planes
+// (its halo in z), so segments should be long; neighbouring columns read each
+// other's edge cells (the ring) from L2, so the CTAs that run together should
+// march neighbouring columns over nearby planes, which many short waves of
+// equal segments do.  Segments of 32 planes, or, when that leaves the first
+// wave of resident CTAs short, as many equal segments per column as fit in
+// one wave.  Measured on B200 (FP16 / FP32 ms per step): 128^3, 4 segments
+// of 32: 0.127 / 0.168, against 10 of 13: 0.129 / 0.183, and 2 of 64:
+// 0.145 / 0.259; 256^3, segments of 32: 0.81 / 1.19, of 64: 0.81 / 1.27,
+// whole columns: 0.93 / 1.34.
+static int lean_zlen(const Ctx& c, int tx, int ty, int resident) {
+  const long cols = long((c.nx + tx - 1) / tx) * long((c.ny + ty - 1) / ty);
+  long segs = (c.nz + 31) / 32;
+  if (cols * segs <= resident) segs = std::max(segs, long(resident) / cols);
+  segs = std::max(1L, std::min<long>(segs, c.nz));
   return int((c.nz + segs - 1) / segs);
 }
 
@@ -556,10 +651,28 @@ static int allow_smem(K* kernel, size_t bytes, unsigned long long& done_mask) {
   return 0;
 }
 
+// Opt-in of k_cg_lean's shared memory and its resident CTAs per SM on this
+// device (the persistent grid), once per device.
 template <typename S, int TX, int TY, int MINB, bool PART>
-static int prepare_lean() {
+static int prepare_lean(int* resident) {
   static unsigned long long done = 0;
-  return allow_smem(k_cg_lean<S, TX, TY, MINB, PART>, LeanSmem<S, TX, TY>::BYTES, done);
+  static int per_sm[64] = {0}, sms[64] = {0};
+  int rc = allow_smem(k_cg_lean<S, TX, TY, MINB, PART>, LeanSmem<S, TX, TY>::BYTES, done);
+  if (rc) return rc;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return LBX_ERR_CUDA;
+  dev &= 63;
+  if (!per_sm[dev]) {
+    int nb = 0, nsm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_cg_lean<S, TX, TY, MINB, PART>, TX * TY,
+                                                      LeanSmem<S, TX, TY>::BYTES) != cudaSuccess ||
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || nb < 1 || nsm < 1)
+      return LBX_ERR_CUDA;
+    sms[dev] = nsm;
+    per_sm[dev] = nb;
+  }
+  *resident = per_sm[dev] * sms[dev];
+  return 0;
 }
 
 template <typename S, int TX, int TY, int MINB, bool PART>
@@ -571,9 +684,10 @@ static int prepare_lean_multi() {
 template <typename S, int TX, int TY, int MINB, bool PART>
 static int launch_lean(Ctx& c, int zlen_override, LeanPart<typename Store<S>::C> pt) {
   using C = typename Store<S>::C;
-  const int rc = prepare_lean<S, TX, TY, MINB, PART>();
+  int resident = 0;
+  const int rc = prepare_lean<S, TX, TY, MINB, PART>(&resident);
   if (rc) return rc;
-  int zlen = zlen_override > 0 ? zlen_override : lean_zlen(c, TX, TY, MINB);
+  const int zlen = zlen_override > 0 ? zlen_override : lean_zlen(c, TX, TY, resident);
   dim3 block(TX, TY, 1);
   dim3 grid((c.nx + TX - 1) / TX, (c.ny + TY - 1) / TY, (c.nz + zlen - 1) / zlen);
   k_cg_lean<S, TX, TY, MINB, PART><<<grid, block, LeanSmem<S, TX, TY>::BYTES, c.stream>>>(

@@ -55,7 +55,7 @@ def test_ensemble_tuner_keeps_results_consistent():
         if len(x):
             ens.boxes[i].set_particles(x, np.zeros_like(x))
     choice = ens.tune(trial=4)
-    assert choice["shape"] in ("32x8", "32x16") and choice["zlen"] in (4, 8, 16, 32, 64)
+    assert choice["shape"] in ("32x8", "32x16") and choice["zlen"] in (4, 8, 16, 32, 64, 128)
     ens.step(4)
     for b in ens.boxes:
         assert b.status()[0] == 0
