@@ -176,6 +176,15 @@ __device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
   const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
   asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
 }
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+template <typename C>
+__device__ __forceinline__ void cp_async_c(C* smem, const C* gmem) {
+  if constexpr (sizeof(C) == 4) cp_async4(smem, gmem);
+  else cp_async8(smem, gmem);
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() {
@@ -350,6 +359,7 @@ struct LeanPart {
   const int8_t* __restrict__ fnew;
   const C* __restrict__ rhoR;
   const C* __restrict__ rhoB;
+  const C* __restrict__ phi;  // phase field of the surface and new fluid cells
 };
 
 // Shared memory of one CTA: the rolling phase-field window (4 planes of the
@@ -358,21 +368,41 @@ struct LeanPart {
 // copied two iterations before its collision, summed into densities one
 // iteration before, and collided from the same copy), then 2 planes x Q x
 // the ring cells (summed only).
-template <typename S, int TX, int TY>
+//
+// The particle variant adds, per own / ring cell and plane, the side record
+// copied with the pulls: the 4-byte words holding the cell's flag of this and
+// of the previous step, and the phase field the wetting / fill kernels wrote
+// for it (3 planes deep for own cells, 2 for ring cells), and a 4-plane window
+// of previous-step flags of the column and its ring (spheredead sources).
+template <typename C>
+struct SideRec {
+  unsigned fnew_w, fold_w;  // aligned words containing the cell's flags
+  C phi;
+};
+
+template <typename S, int TX, int TY, bool PART>
 struct LeanSmem {
   using C = typename Store<S>::C;
   using R = typename SPair<S>::R;
-  static constexpr int NT = TX * TY, RN = Ring<TX, TY>::N;
-  static constexpr size_t PHI = sizeof(C) * 4 * Ring<TX, TY>::CELLS;
+  static constexpr int NT = TX * TY, RN = Ring<TX, TY>::N, CELLS = Ring<TX, TY>::CELLS;
+  static constexpr size_t PHI = sizeof(C) * 4 * CELLS;
   static constexpr size_t OWN = kStage<S> ? sizeof(R) * 3 * Q * NT : 0;
   static constexpr size_t RING = kStage<S> ? sizeof(R) * 2 * Q * RN : 0;
-  static constexpr size_t BYTES = PHI + OWN + RING;
-  static_assert(PHI % 16 == 0 && OWN % 16 == 0, "stage alignment");
-  static __device__ __forceinline__ C (*phi(unsigned char* base))[Ring<TX, TY>::CELLS] {
-    return reinterpret_cast<C(*)[Ring<TX, TY>::CELLS]>(base);
+  static constexpr size_t SIDE = PART ? (sizeof(SideRec<C>) * (3 * NT + 2 * RN) + 15) / 16 * 16 : 0;
+  static constexpr size_t FOLD = PART ? (4 * CELLS + 15) / 16 * 16 : 0;
+  static constexpr size_t BYTES = PHI + OWN + RING + SIDE + FOLD;
+  static_assert(PHI % 16 == 0 && OWN % 16 == 0 && RING % 16 == 0, "stage alignment");
+  static __device__ __forceinline__ C (*phi(unsigned char* base))[CELLS] {
+    return reinterpret_cast<C(*)[CELLS]>(base);
   }
   static __device__ __forceinline__ R* stage(unsigned char* base) {
     return kStage<S> ? reinterpret_cast<R*>(base + PHI) : nullptr;
+  }
+  static __device__ __forceinline__ SideRec<C>* side(unsigned char* base) {
+    return PART ? reinterpret_cast<SideRec<C>*>(base + PHI + OWN + RING) : nullptr;
+  }
+  static __device__ __forceinline__ int8_t (*fold(unsigned char* base))[CELLS] {
+    return PART ? reinterpret_cast<int8_t(*)[CELLS]>(base + PHI + OWN + RING + SIDE) : nullptr;
   }
 };
 
@@ -383,7 +413,8 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
                                             int zend, unsigned long long* err, int64_t step,
                                             const LeanPart<typename Store<S>::C>& PT,
                                             typename Store<S>::C (*sphi)[Ring<TX, TY>::CELLS],
-                                            typename SPair<S>::R* stage) {
+                                            typename SPair<S>::R* stage, SideRec<typename Store<S>::C>* side,
+                                            int8_t (*sfold)[Ring<TX, TY>::CELLS]) {
   using C = typename Store<S>::C;
   constexpr int NT = TX * TY;
   using R = Ring<TX, TY>;
@@ -404,61 +435,38 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
 
   using SR = typename SPair<S>::R;
   constexpr int RN = R::N;
+  constexpr bool ASYNC = kStage<S> || PART;  // copy groups in flight
   SR* const ring_stage = kStage<S> ? stage + 3 * Q * NT : nullptr;
+  SideRec<C>* const side_ring = PART ? side + 3 * NT : nullptr;
   const Planes<const S> Ap{A, 2 * g.n};
   const Planes<S> Bp{B, 2 * g.n};
 
-  // clamped densities of cell (cx, cy, zz): pulled (fluid in both steps),
-  // from the side arrays (new fluid, or the virtual density of a surface
-  // cell), zero for every other solid cell (init_rho*_CG's MINDENS).  16-bit
-  // storage sums the pairs its copies brought into the stage (st, stride);
-  // wider types pull here.  The flags are loaded beside the pull and the pull
-  // is discarded for the few cells that do not use it.
-  // fl: the cell's flags (bits 0-7 this step, 8-15 the previous step)
-  auto densities = [&](int cx, int cy, int zz, bool check, C& rR, C& rB, const SR* st, int stride, unsigned fl) {
-    const int cell = cx + g.nx * (cy + g.ny * zz);
-    const int8_t fn = int8_t(fl & 255u), fo = int8_t((fl >> 8) & 255u);
-    if constexpr (kStage<S>) {
-      stage_rho<S, C>(st, stride, K, rR, rB);
-    } else {
-      PullIdx P;
-      pull_idx(g, cx, cy, zz, P);
-      pull_rho<S, C>(A, g.n, P, K, rR, rB);
-    }
-    if (parts && (fn != LBX_FLUID_FLUID || fo != LBX_FLUID_FLUID)) {
-      if (fn == LBX_FLUID_FLUID || fn == LBX_FLUID_SPHERELIST) {
-        rR = PT.rhoR[cell];
-        rB = PT.rhoB[cell];
-      } else {
-        rR = C(0);
-        rB = C(0);
-      }
-      return false;
-    }
-    if (check && (rR < C(-10) || rR > C(10) || rB < C(-10) || rB > C(10)))
-      raise_error(err, LBX_DEV_RHO_RANGE, step, cell);
-    rR = clamp0(rR);
-    rB = clamp0(rB);
-    return true;
-  };
-
-  // stage slots of plane p (p >= z0 - 1): own cells 3 deep, ring cells 2 deep
-  auto own_slot = [&](int p) { return stage + ((p - z0 + 1) % 3) * (Q * NT) + tid; };
-  auto ring_slot = [&](int p) { return ring_stage + ((p - z0 + 1) & 1) * (Q * RN) + tid; };
+  // slots of plane p (p >= z0 - 1): own cells 3 deep, ring cells 2 deep
+  auto own_q = [&](int p) { return (p - z0 + 1) % 3; };
+  auto ring_q = [&](int p) { return (p - z0 + 1) & 1; };
+  auto own_slot = [&](int p) { return stage + own_q(p) * (Q * NT) + tid; };
+  auto ring_slot = [&](int p) { return ring_stage + ring_q(p) * (Q * RN) + tid; };
 
   // Start plane p: 16-bit storage copies the pulls of the own and the ring
-  // cell into the stage (one copy group); with spheres, the flags of both
-  // cells are loaded here too and returned packed (own: bits 0-15, ring:
-  // 16-31; each this step | previous step << 8), two iterations before use.
-  constexpr unsigned FLUID2 = unsigned(LBX_FLUID_FLUID) | (unsigned(LBX_FLUID_FLUID) << 8);
-  auto issue = [&](int p) -> unsigned {
+  // cell into the stage; with spheres, the flag words and the side phase
+  // field of both cells are copied too (all in one copy group).
+  auto issue = [&](int p) {
     const int zz = wrap0(p, g.nz);
-    unsigned fl = FLUID2 | (FLUID2 << 16);
-    if (parts) {
-      const int co = x + g.nx * (y + g.ny * zz), cr = rxg + g.nx * (ryg + g.ny * zz);
-      fl = unsigned(uint8_t(PT.fnew[co])) | (unsigned(uint8_t(PT.fold[co])) << 8);
-      if (ringer) fl |= (unsigned(uint8_t(PT.fnew[cr])) << 16) | (unsigned(uint8_t(PT.fold[cr])) << 24);
-      else fl |= FLUID2 << 16;
+    if constexpr (PART) {
+      if (parts) {
+        const int co = x + g.nx * (y + g.ny * zz);
+        SideRec<C>* so = side + own_q(p) * NT + tid;
+        cp_async4(&so->fnew_w, PT.fnew + (co & ~3));
+        cp_async4(&so->fold_w, PT.fold + (co & ~3));
+        cp_async_c(&so->phi, PT.phi + co);
+        if (ringer) {
+          const int cr = rxg + g.nx * (ryg + g.ny * zz);
+          SideRec<C>* sr = side_ring + ring_q(p) * RN + tid;
+          cp_async4(&sr->fnew_w, PT.fnew + (cr & ~3));
+          cp_async4(&sr->fold_w, PT.fold + (cr & ~3));
+          cp_async_c(&sr->phi, PT.phi + cr);
+        }
+      }
     }
     if constexpr (kStage<S>) {
       PullIdx P;
@@ -468,61 +476,115 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
         pull_idx(g, rxg, ryg, zz, P);
         pull_async<S>(A, g.n, P, ring_slot(p), RN);
       }
-      cp_async_commit();
     }
-    return fl;
+    if constexpr (ASYNC) cp_async_commit();
   };
   auto settle = [&]() {  // every copy group but the newest has landed
-    if constexpr (kStage<S>) cp_async_wait<1>();
+    if constexpr (ASYNC) cp_async_wait<1>();
+  };
+  // flags (this step, previous step) of a cell from its side record
+  auto flags_of = [&](const SideRec<C>* r, int cell, int8_t& fn, int8_t& fo) {
+    const int sh = 8 * (cell & 3);
+    fn = int8_t((r->fnew_w >> sh) & 255u);
+    fo = int8_t((r->fold_w >> sh) & 255u);
   };
 
-  // phase field of plane p (own cell and ring cell) into its window slot
-  auto phase_plane = [&](int p, unsigned fl, C& rRo, C& rBo) {
+  // Phase field (and, for the own cell, the clamped densities) of cell
+  // (cx, cy, zz).  Fluid in both steps: pulled densities (16-bit storage sums
+  // the pairs its copies brought into the stage, wider types pull here).
+  // With spheres, otherwise: a new fluid cell takes the fill kernel's
+  // densities, a surface cell the wetting kernel's phase field (both kernels
+  // store (rR - rB) / (rR + rB) of the densities they write), and every other
+  // solid cell densities 0 (init_rho*_CG's MINDENS).
+  auto cell_phase = [&](int cx, int cy, int zz, bool check, bool is_own, const SR* st, int stride,
+                        const SideRec<C>* rec, C& rR, C& rB) -> C {
+    const int cell = cx + g.nx * (cy + g.ny * zz);
+    if constexpr (PART) {
+      if (parts) {
+        int8_t fn, fo;
+        flags_of(rec, cell, fn, fo);
+        if (fn != LBX_FLUID_FLUID || fo != LBX_FLUID_FLUID) {
+          rR = C(0);
+          rB = C(0);
+          if (fn == LBX_FLUID_SPHERELIST) return rec->phi;
+          if (fn == LBX_FLUID_FLUID) {  // new fluid cell
+            if (!is_own) return rec->phi;
+            rR = PT.rhoR[cell];
+            rB = PT.rhoB[cell];
+          }
+          return (rR - rB) / (rR + rB);
+        }
+      }
+    }
+    if constexpr (kStage<S>) {
+      stage_rho<S, C>(st, stride, K, rR, rB);
+    } else {
+      PullIdx P;
+      pull_idx(g, cx, cy, zz, P);
+      pull_rho<S, C>(A, g.n, P, K, rR, rB);
+    }
+    if (check && (rR < C(-10) || rR > C(10) || rB < C(-10) || rB > C(10)))
+      raise_error(err, LBX_DEV_RHO_RANGE, step, cell);
+    rR = clamp0(rR);
+    rB = clamp0(rB);
+    return (rR - rB) / (rR + rB);
+  };
+
+  // phase field of plane p (own cell and ring cell) into its window slot, and
+  // with spheres the previous-step flags into the flag window
+  auto phase_plane = [&](int p, C& rRo, C& rBo) {
     const int zz = wrap0(p, g.nz);
     const bool owned = active && p >= z0 && p < zend;
-    C rR, rB;
-    densities(x, y, zz, owned, rR, rB, kStage<S> ? own_slot(p) : nullptr, NT, fl & 0xffffu);
-    rRo = rR;
-    rBo = rB;
-    sphi[p & 3][own] = (rR - rB) / (rR + rB);
+    const SideRec<C>* so = PART ? side + own_q(p) * NT + tid : nullptr;
+    sphi[p & 3][own] = cell_phase(x, y, zz, owned, true, kStage<S> ? own_slot(p) : nullptr, NT, so, rRo, rBo);
+    if constexpr (PART) {
+      if (parts) {
+        int8_t fn, fo;
+        flags_of(so, x + g.nx * (y + g.ny * zz), fn, fo);
+        sfold[p & 3][own] = fo;
+      }
+    }
     if (ringer) {
       C qR, qB;
-      densities(rxg, ryg, zz, false, qR, qB, kStage<S> ? ring_slot(p) : nullptr, RN, fl >> 16);
-      sphi[p & 3][rslot] = (qR - qB) / (qR + qB);
+      const SideRec<C>* sr = PART ? side_ring + ring_q(p) * RN + tid : nullptr;
+      sphi[p & 3][rslot] =
+          cell_phase(rxg, ryg, zz, false, false, kStage<S> ? ring_slot(p) : nullptr, RN, sr, qR, qB);
+      if constexpr (PART) {
+        if (parts) {
+          int8_t fn, fo;
+          flags_of(sr, rxg + g.nx * (ryg + g.ny * zz), fn, fo);
+          sfold[p & 3][rslot] = fo;
+        }
+      }
     }
   };
 
   C rRn, rBn, rRc, rBc;
-  const unsigned flm = issue(z0 - 1);
-  unsigned flz = issue(z0);  // flags of plane z, then z+1 (loop carried)
+  issue(z0 - 1);
+  issue(z0);
   settle();
-  phase_plane(z0 - 1, flm, rRc, rBc);
-  unsigned flz1 = issue(z0 + 1);
+  phase_plane(z0 - 1, rRc, rBc);
+  issue(z0 + 1);
   settle();
-  phase_plane(z0, flz, rRn, rBn);
+  phase_plane(z0, rRn, rBn);
   for (int z = z0; z < zend; ++z) {
     rRc = rRn;
     rBc = rBn;
-    // plane z+2 is copied while z+1 is summed and z collided; the copy into
-    // the slot of plane z-1 starts after this thread's last read of it
-    unsigned flz2 = FLUID2 | (FLUID2 << 16);
-    if (z + 2 <= zend) flz2 = issue(z + 2);
-    else if constexpr (kStage<S>) cp_async_commit();  // one group per iteration
+    // plane z+2 is copied while z+1 is summed and z collided; the copies into
+    // the slots of plane z-1 start after this thread's last read of them
+    if (z + 2 <= zend) issue(z + 2);
+    else if constexpr (ASYNC) cp_async_commit();  // one group per iteration
     settle();
-    phase_plane(z + 1, flz1, rRn, rBn);
+    phase_plane(z + 1, rRn, rBn);
     __syncthreads();
-    const unsigned flc = flz;
-    flz = flz1;
-    flz1 = flz2;
     if (active) {
       const int cell = x + g.nx * (y + g.ny * z);
       P2<C> gp[Q];
       bool collide = true;
-      const int8_t fn = int8_t(flc & 255u), fo = int8_t((flc >> 8) & 255u);
       PullIdx P;
       pull_idx(g, x, y, z, P);
       // the pull every fluid cell needs: in the stage since two iterations,
-      // or issued here together with the flag loads
+      // or issued here
       if constexpr (kStage<S>) {
         const SR* sg = own_slot(z);
 #pragma unroll
@@ -531,18 +593,24 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
 #pragma unroll
         for (int l = 0; l < Q; ++l) gp[l] = SPair<S>::ld(Ap(l) + 2 * P.src[l]);
       }
-      if (parts) {
-        collide = fn == LBX_FLUID_FLUID;
-        if (collide && fo != LBX_FLUID_FLUID) {
-          // make_fluid already wrote the new node's populations (stored form) into B
+      if constexpr (PART) {
+        if (parts) {
+          int8_t fn, fo;
+          flags_of(side + own_q(z) * NT + tid, cell, fn, fo);
+          collide = fn == LBX_FLUID_FLUID;
+          if (collide && fo != LBX_FLUID_FLUID) {
+            // make_fluid already wrote the new node's populations (stored form) into B
 #pragma unroll
-          for (int l = 0; l < Q; ++l) gp[l] = SPair<S>::ld(Bp(l) + 2 * cell);
-        } else if (!collide) {
-          // solid cell: streamed populations only; a spheredead source (previous
-          // step) leaves the destination's stale value, which is B's entry
+            for (int l = 0; l < Q; ++l) gp[l] = SPair<S>::ld(Bp(l) + 2 * cell);
+          } else if (!collide) {
+            // solid cell: streamed populations only; a spheredead source
+            // (previous step, from the flag window) leaves the destination's
+            // stale value, which is B's entry
 #pragma unroll
-          for (int l = 1; l < Q; ++l)
-            if (PT.fold[P.src[l]] == LBX_FLUID_SPHEREDEAD) gp[l] = SPair<S>::ld(Bp(l) + 2 * cell);
+            for (int l = 1; l < Q; ++l)
+              if (sfold[(z - ez(l)) & 3][own - ey(l) * R::RX - ex(l)] == LBX_FLUID_SPHEREDEAD)
+                gp[l] = SPair<S>::ld(Bp(l) + 2 * cell);
+          }
         }
       }
       if (collide) {
@@ -568,7 +636,7 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
     // window slot (z+3)&3 read above is rewritten in iteration z+2; the
     // barrier of iteration z+1 orders that write after these reads
   }
-  if constexpr (kStage<S>) cp_async_wait<0>();  // nothing in flight when the stage is reused
+  if constexpr (ASYNC) cp_async_wait<0>();  // nothing in flight when the shared memory is reused
 }
 
 template <typename S, int TX, int TY, int MINB, bool PART>
@@ -576,10 +644,11 @@ __global__ void __launch_bounds__(TX* TY, MINB)
     k_cg_lean(const S* __restrict__ A, S* __restrict__ B, Geom g, LeanConst<typename Store<S>::C> K, int zlen,
               unsigned long long* err, int64_t step, LeanPart<typename Store<S>::C> PT) {
   extern __shared__ __align__(16) unsigned char lean_smem[];
-  using M = LeanSmem<S, TX, TY>;
+  using M = LeanSmem<S, TX, TY, PART>;
   const int z0 = blockIdx.z * zlen;
   lean_column<S, TX, TY, PART>(A, B, g, K, blockIdx.x * TX, blockIdx.y * TY, z0, min(z0 + zlen, g.nz), err, step,
-                               PT, M::phi(lean_smem), M::stage(lean_smem));
+                               PT, M::phi(lean_smem), M::stage(lean_smem), M::side(lean_smem),
+                               M::fold(lean_smem));
 }
 
 // ---------------------------------------------------------------------------
@@ -607,12 +676,13 @@ __global__ void __launch_bounds__(TX* TY, MINB)
                     int nwork, LeanConst<typename Store<S>::C> K) {
   using C = typename Store<S>::C;
   extern __shared__ __align__(16) unsigned char lean_smem[];
-  using M = LeanSmem<S, TX, TY>;
+  using M = LeanSmem<S, TX, TY, PART>;
   for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
     const WorkItem it = work[w];
     const BoxDesc<C> bd = boxes[it.box];
     lean_column<S, TX, TY, PART>((const S*)bd.A, (S*)bd.B, bd.g, K, it.x0, it.y0, it.z0, it.zend, bd.err, bd.step,
-                                 bd.pt, M::phi(lean_smem), M::stage(lean_smem));
+                                 bd.pt, M::phi(lean_smem), M::stage(lean_smem), M::side(lean_smem),
+                                 M::fold(lean_smem));
     __syncthreads();  // the window is reused by the next item
   }
 }
@@ -657,7 +727,7 @@ template <typename S, int TX, int TY, int MINB, bool PART>
 static int prepare_lean(int* resident) {
   static unsigned long long done = 0;
   static int per_sm[64] = {0}, sms[64] = {0};
-  int rc = allow_smem(k_cg_lean<S, TX, TY, MINB, PART>, LeanSmem<S, TX, TY>::BYTES, done);
+  int rc = allow_smem(k_cg_lean<S, TX, TY, MINB, PART>, LeanSmem<S, TX, TY, PART>::BYTES, done);
   if (rc) return rc;
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return LBX_ERR_CUDA;
@@ -665,7 +735,7 @@ static int prepare_lean(int* resident) {
   if (!per_sm[dev]) {
     int nb = 0, nsm = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_cg_lean<S, TX, TY, MINB, PART>, TX * TY,
-                                                      LeanSmem<S, TX, TY>::BYTES) != cudaSuccess ||
+                                                      LeanSmem<S, TX, TY, PART>::BYTES) != cudaSuccess ||
         cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || nb < 1 || nsm < 1)
       return LBX_ERR_CUDA;
     sms[dev] = nsm;
@@ -678,7 +748,7 @@ static int prepare_lean(int* resident) {
 template <typename S, int TX, int TY, int MINB, bool PART>
 static int prepare_lean_multi() {
   static unsigned long long done = 0;
-  return allow_smem(k_cg_lean_multi<S, TX, TY, MINB, PART>, LeanSmem<S, TX, TY>::BYTES, done);
+  return allow_smem(k_cg_lean_multi<S, TX, TY, MINB, PART>, LeanSmem<S, TX, TY, PART>::BYTES, done);
 }
 
 template <typename S, int TX, int TY, int MINB, bool PART>
@@ -690,7 +760,7 @@ static int launch_lean(Ctx& c, int zlen_override, LeanPart<typename Store<S>::C>
   const int zlen = zlen_override > 0 ? zlen_override : lean_zlen(c, TX, TY, resident);
   dim3 block(TX, TY, 1);
   dim3 grid((c.nx + TX - 1) / TX, (c.ny + TY - 1) / TY, (c.nz + zlen - 1) / zlen);
-  k_cg_lean<S, TX, TY, MINB, PART><<<grid, block, LeanSmem<S, TX, TY>::BYTES, c.stream>>>(
+  k_cg_lean<S, TX, TY, MINB, PART><<<grid, block, LeanSmem<S, TX, TY, PART>::BYTES, c.stream>>>(
       (const S*)c.pops[c.cur], (S*)c.pops[1 - c.cur], geom(c), make_lean<C>(c), zlen, c.d_err, c.step + 1, pt);
   return 0;
 }
@@ -703,7 +773,7 @@ int fluid_lean(Ctx& c) {
   int rc = by_storage(c, [&](auto* tag) {
     using S = std::remove_pointer_t<decltype(tag)>;
     using C = typename Store<S>::C;
-    LeanPart<C> none{nullptr, nullptr, nullptr, nullptr};
+    LeanPart<C> none{nullptr, nullptr, nullptr, nullptr, nullptr};
     kt_begin(c);
     int r = 0;
     if constexpr (std::is_same<S, double>::value) {
@@ -724,7 +794,7 @@ int fluid_lean_particles(Ctx& c, int fo, int fn) {
   int rc = by_storage(c, [&](auto* tag) {
     using S = std::remove_pointer_t<decltype(tag)>;
     using C = typename Store<S>::C;
-    LeanPart<C> pt{c.flags[fo], c.flags[fn], (C*)c.rho[0], (C*)c.rho[1]};
+    LeanPart<C> pt{c.flags[fo], c.flags[fn], (C*)c.rho[0], (C*)c.rho[1], (C*)c.phi};
     kt_begin(c);
     int r = 0;
     if constexpr (std::is_same<S, double>::value) r = launch_lean<S, 32, 8, 1, true>(c, c.lean_zlen, pt);
@@ -762,7 +832,8 @@ int ensemble_launch(const std::vector<Ctx*>& boxes, int shape, const std::vector
         d.g = geom(c);
         const bool parts = particles_active(c) != 0;
         d.pt = LeanPart<C>{parts ? c.flags[parity] : nullptr, parts ? c.flags[1 - parity] : nullptr,
-                           parts ? (C*)c.rho[0] : nullptr, parts ? (C*)c.rho[1] : nullptr};
+                           parts ? (C*)c.rho[0] : nullptr, parts ? (C*)c.rho[1] : nullptr,
+                           parts ? (C*)c.phi : nullptr};
         d.err = c.d_err;
         d.step = c.step + 1;
         const int zl = std::max(1, zlen[b]);
@@ -793,14 +864,14 @@ int ensemble_launch(const std::vector<Ctx*>& boxes, int shape, const std::vector
     const auto* W = (const WorkItem*)d_work;
     if constexpr (std::is_same<S, double>::value) {
       int grid = std::min(nwork, 148);
-      k_cg_lean_multi<S, 32, 8, 1, true><<<grid, dim3(32, 8), LeanSmem<S, 32, 8>::BYTES, stream>>>(D, W, nwork, K);
+      k_cg_lean_multi<S, 32, 8, 1, true><<<grid, dim3(32, 8), LeanSmem<S, 32, 8, true>::BYTES, stream>>>(D, W, nwork, K);
     } else if (shape == 1) {
       int grid = std::min(nwork, 148);
-      k_cg_lean_multi<S, 32, 16, 1, true><<<grid, dim3(32, 16), LeanSmem<S, 32, 16>::BYTES, stream>>>(D, W, nwork,
+      k_cg_lean_multi<S, 32, 16, 1, true><<<grid, dim3(32, 16), LeanSmem<S, 32, 16, true>::BYTES, stream>>>(D, W, nwork,
                                                                                                       K);
     } else {
       int grid = std::min(nwork, 296);
-      k_cg_lean_multi<S, 32, 8, 2, true><<<grid, dim3(32, 8), LeanSmem<S, 32, 8>::BYTES, stream>>>(D, W, nwork, K);
+      k_cg_lean_multi<S, 32, 8, 2, true><<<grid, dim3(32, 8), LeanSmem<S, 32, 8, true>::BYTES, stream>>>(D, W, nwork, K);
     }
     return launch_status();
   });
