@@ -255,11 +255,61 @@ def colloid_timing(storage, steps=50, warm=10, small=False):
             "frac_at_basis": mlups * 1e6 * BYTES_PER_CELL[storage] / 1e9 / peaks()[0], "device_error": code}
 
 
+def ensemble_timing(steps=100, err_steps=200, seed=7):
+    """Ensemble workload: 48 boxes, edges uniform from {32, 48, 64, 96}, 0-40 spheres of radius 4 each
+    (seeded, min gap 1), FP16 storage, closure switched on without weights (every close pair takes the
+    analytic lubrication fallback), advanced together by the persistent kernel under a CUDA graph after
+    the autotuner.  Error: relative L2 of each box's velocity field against the same box advanced alone
+    with FP32 storage, after err_steps steps."""
+    from lbcuda_b200 import LBSim, make_params
+    from lbcuda_b200.ensemble import Ensemble, random_boxes
+    from lbcuda_b200.inputs import seeded_noise_fields
+    spec = random_boxes(48, seed=seed)
+
+    def params(L, n, storage):
+        return make_params(L, model="cg", storage=storage, sigma=SIGMA, beta=BETA, max_particles=max(n, 1),
+                           radius=4.0, wetting="neutral", lrotate=1, max_vel=1.0, exact_tiles=0,
+                           hz_rmin=8.5, hz_rcap=7.0, closure=1, lubrication=1, lubric_rmin=1.0, lubric_rcap=0.2)
+
+    def load(sim, i, L, x):
+        rR, rB = seeded_noise_fields(L, L, L, seed=100 + i)
+        sim.set_fields(rR, rB)
+        if len(x):
+            sim.set_particles(x, np.zeros_like(x))
+
+    ens = Ensemble([params(L, len(x), "f16") for L, x in spec])
+    for i, (L, x) in enumerate(spec):
+        load(ens.boxes[i], i, L, x)
+    tuned = ens.tune(trial=6)
+    for i, (L, x) in enumerate(spec):
+        load(ens.boxes[i], i, L, x)
+    ens.step(err_steps)
+    errs = []
+    for i, (L, x) in enumerate(spec):
+        ref = LBSim(params(L, len(x), "f32"))
+        load(ref, i, L, x)
+        ref.step(err_steps)
+        u16, u32 = ens.boxes[i].get_fields()[2], ref.get_fields()[2]
+        errs.append(float(np.linalg.norm(u16 - u32) / max(np.linalg.norm(u32), 1e-30)))
+        ref.close()
+    ens.step(10)
+    ms = ens.time(steps)
+    cells = ens.cells
+    spheres = int(sum(len(x) for _, x in spec))
+    ens.close()
+    return {"boxes": len(spec), "cells": cells, "spheres": spheres, "storage": "f16", "tuned": tuned,
+            "ms_per_step": ms / steps, "mlups": cells * steps / (ms * 1e-3) / 1e6,
+            "u_rel_l2_vs_f32_per_box": {"after_steps": err_steps, "max": max(errs), "median": float(np.median(errs))}}
+
+
 def only_region(args, local):
     import torch
     torch.cuda.set_device(local)
     from lbcuda_b200 import LBSim, make_params
     from lbcuda_b200.inputs import seeded_noise_fields
+    if args.only == "ensemble":
+        print(json.dumps(ensemble_timing()), flush=True)
+        return 0
     if args.only.startswith("colloid"):
         r = colloid_timing(args.only.split("-")[1], steps=max(1, args.steps) * 5, warm=args.warmup,
                            small=args.only.endswith("small"))
@@ -288,7 +338,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-extras", action="store_true", help="skip the error runs, the colloid case and the CPU baseline")
     ap.add_argument("--only", choices=["f16", "f32", "bf16", "f64", "colloid-f16", "colloid-f32", "colloid-f16-small",
-                                       "colloid-f32-small"],
+                                       "colloid-f32-small", "ensemble"],
                     help="profiling aid: run one timed region only and print its timing")
     ap.add_argument("--lb-steps", type=int, default=LB_PER_STEP, help="lattice steps per bench step")
     ap.add_argument("--schedule", type=int, default=2, help="colour-gradient schedule (0, 1, 2)")
@@ -401,6 +451,7 @@ def main():
     if rank == 0 and not args.no_extras:
         extras["error_vs_f64"] = error_vs_f64()
         extras["colloid_256_1280"] = {st: colloid_timing(st) for st in ("f16", "f32")}
+        extras["ensemble_48"] = ensemble_timing()
         extras["cpu_baseline"] = cpu_baseline_sample()
 
     if rank == 0:

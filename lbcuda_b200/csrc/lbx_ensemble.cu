@@ -3,12 +3,15 @@
 //
 // Every box is a full context (include/lbx.h), so its fields, spheres and
 // closure are set and read with the ordinary entry points.  A step of the
-// ensemble launches, on one stream: the sphere pre-kernels of every box with
-// spheres, ONE persistent colour-gradient kernel for the fluid of all boxes
+// ensemble forks from the ensemble stream to the stream of every box with
+// spheres, runs that box's sphere pre-kernels there, joins, launches ONE
+// persistent colour-gradient kernel for the fluid of all boxes
 // (k_cg_lean_multi: CTAs take (box, column, z-segment) work items, longest
-// first), then the sphere post-kernels.  Two consecutive steps (the
-// ping-pong parity) are captured once into a CUDA graph and replayed, so the
-// host issues one graph launch per two steps.  lbx_ensemble_tune times the
+// first) on the ensemble stream, then forks and joins again around the sphere
+// post-kernels.  The boxes' small sphere kernels thus run side by side
+// instead of one after the other.  Two consecutive steps (the ping-pong
+// parity) are captured once into a CUDA graph (the forks become parallel
+// branches) and replayed, so the host issues one graph launch per two steps.  lbx_ensemble_tune times the
 // candidate CTA shapes and z-segment lengths on the boxes themselves and
 // keeps the fastest.
 #include <algorithm>
@@ -40,6 +43,8 @@ namespace {
 struct Ensemble {
   std::vector<lbx::Ctx*> boxes;
   cudaStream_t stream = nullptr;
+  cudaEvent_t fork = nullptr;       // ensemble stream -> box streams
+  std::vector<cudaEvent_t> join;    // box stream -> ensemble stream
   int shape = 0;                 // 0: 32x8 CTAs, 1: 32x16
   std::vector<int> zlen;         // per box
   void* d_desc[2] = {nullptr, nullptr};
@@ -67,7 +72,26 @@ int build_tables(Ensemble& e) {
   return 0;
 }
 
-// one eager step of every box
+// run `part` (a sphere stage) of every box with spheres on the box's own
+// stream, between a fork from and a join into the ensemble stream
+template <typename F>
+int boxes_side_by_side(Ensemble& e, F&& part) {
+  if (cudaEventRecord(e.fork, e.stream) != cudaSuccess) return LBX_ERR_CUDA;
+  for (size_t b = 0; b < e.boxes.size(); ++b) {
+    lbx::Ctx* c = e.boxes[b];
+    if (!lbx::particles_active(*c)) continue;
+    if (cudaStreamWaitEvent(c->stream, e.fork, 0) != cudaSuccess) return LBX_ERR_CUDA;
+    int rc = part(*c);
+    if (rc) return rc;
+    if (cudaEventRecord(e.join[b], c->stream) != cudaSuccess ||
+        cudaStreamWaitEvent(e.stream, e.join[b], 0) != cudaSuccess)
+      return LBX_ERR_CUDA;
+  }
+  return 0;
+}
+
+// one step of every box (eager, or recorded while the ensemble stream is
+// being captured)
 int step_once(Ensemble& e) {
   if (!e.tables_ok) {
     int rc = build_tables(e);
@@ -76,23 +100,26 @@ int step_once(Ensemble& e) {
   const int parity = e.boxes[0]->cur;
   for (auto* c : e.boxes)
     if (c->cur != parity) return LBX_ERR_STATE;  // boxes must be stepped together
-  for (auto* c : e.boxes)
-    if (lbx::particles_active(*c)) {
-      int rc = lbx::particles_pre(*c);
-      if (rc) return rc;
-    }
-  int rc = lbx::ensemble_launch(e.boxes, e.shape, e.zlen, e.d_desc[parity], e.d_work[parity], e.nwork, e.stream, 0,
-                                parity);
+  int rc = boxes_side_by_side(e, [](lbx::Ctx& c) { return lbx::particles_pre(c); });
   if (rc) return rc;
-  for (auto* c : e.boxes) {
-    if (lbx::particles_active(*c)) {
-      rc = lbx::particles_post(*c);
-      if (rc) return rc;
-    } else {
+  rc = lbx::ensemble_launch(e.boxes, e.shape, e.zlen, e.d_desc[parity], e.d_work[parity], e.nwork, e.stream, 0,
+                            parity);
+  if (rc) return rc;
+  rc = boxes_side_by_side(e, [](lbx::Ctx& c) { return lbx::particles_post(c); });
+  if (rc) return rc;
+  for (auto* c : e.boxes)
+    if (!lbx::particles_active(*c)) {
       c->cur = 1 - c->cur;
       c->step += 1;
     }
-  }
+  return 0;
+}
+
+// host-side join: work the caller queued on a box (set / get calls) is done
+// before the ensemble stream (or a capture of it) starts a step
+int settle_boxes(Ensemble& e) {
+  for (auto* c : e.boxes)
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess) return LBX_ERR_CUDA;
   return 0;
 }
 
@@ -112,16 +139,18 @@ int lbx_ensemble_create(int32_t nbox, const lbx_params* params, void** out) {
   Ensemble* e = new (std::nothrow) Ensemble();
   if (!e) return LBX_ERR_ALLOC;
   int rc = cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) == cudaSuccess ? 0 : LBX_ERR_CUDA;
+  if (!rc && cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming) != cudaSuccess) rc = LBX_ERR_CUDA;
   for (int i = 0; i < nbox && !rc; ++i) {
     void* h = nullptr;
     rc = lbx_create(&params[i], &h);
     if (rc) break;
     auto* c = static_cast<lbx::Ctx*>(h);
-    cudaStreamDestroy(c->stream);  // every box runs on the ensemble's stream
-    c->stream = e->stream;
-    c->fused = 2;
+    c->fused = 2;  // each box keeps its own stream for its sphere kernels
     e->boxes.push_back(c);
     e->zlen.push_back(std::min(c->nz, 16));
+    cudaEvent_t ev = nullptr;
+    if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) rc = LBX_ERR_CUDA;
+    e->join.push_back(ev);
   }
   size_t desc_bytes = 512 * size_t(nbox), work_cap = 0;
   for (auto* c : e->boxes) work_cap += size_t((c->nx + 31) / 32) * ((c->ny + 7) / 8) * c->nz;
@@ -144,10 +173,10 @@ int lbx_ensemble_destroy(void* ens) {
   if (!e) return LBX_ERR_ARG;
   if (e->stream) cudaStreamSynchronize(e->stream);
   drop_graph(*e);
-  for (auto* c : e->boxes) {
-    c->stream = nullptr;  // owned by the ensemble
-    lbx_destroy(c);
-  }
+  for (auto* c : e->boxes) lbx_destroy(c);
+  for (auto ev : e->join)
+    if (ev) cudaEventDestroy(ev);
+  if (e->fork) cudaEventDestroy(e->fork);
   for (int p = 0; p < 2; ++p) {
     if (e->d_desc[p]) cudaFree(e->d_desc[p]);
     if (e->d_work[p]) cudaFree(e->d_work[p]);
@@ -168,7 +197,8 @@ int lbx_ensemble_box(void* ens, int32_t i, void** ctx) {
 int lbx_ensemble_step(void* ens, int32_t nsteps) {
   Ensemble* e = static_cast<Ensemble*>(ens);
   if (!e || nsteps < 0) return LBX_ERR_ARG;
-  int rc = 0;
+  int rc = settle_boxes(*e);
+  if (rc) return rc;
   int done = 0;
   if (nsteps >= 2 && e->boxes[0]->cur == 0) {
     if (!e->exec) {
@@ -198,6 +228,10 @@ int lbx_ensemble_step(void* ens, int32_t nsteps) {
   }
   for (; done < nsteps; ++done)
     if ((rc = step_once(*e))) return rc;
+  // later calls on a box (on its own stream) come after these steps
+  if (cudaEventRecord(e->fork, e->stream) != cudaSuccess) return LBX_ERR_CUDA;
+  for (auto* c : e->boxes)
+    if (cudaStreamWaitEvent(c->stream, e->fork, 0) != cudaSuccess) return LBX_ERR_CUDA;
   return 0;
 }
 
@@ -229,6 +263,8 @@ int lbx_ensemble_tune(void* ens, int32_t trial, int32_t* chosen, double* best_ms
   if (!e || trial < 2) return LBX_ERR_ARG;
   trial += trial & 1;
   drop_graph(*e);
+  int rs = settle_boxes(*e);
+  if (rs) return rs;
   const int shapes[2] = {0, 1};
   const int zl[6] = {4, 8, 16, 32, 64, 128};
   double best = 1e30;
@@ -264,6 +300,8 @@ int lbx_ensemble_tune(void* ens, int32_t trial, int32_t* chosen, double* best_ms
   for (size_t i = 0; i < e->boxes.size(); ++i) e->zlen[i] = std::min(e->boxes[i]->nz, bz);
   e->tables_ok = false;
   int rc = build_tables(*e);
+  if (!rc) rc = settle_boxes(*e);
+  if (!rc && cudaStreamSynchronize(e->stream) != cudaSuccess) rc = LBX_ERR_CUDA;
   if (chosen) {
     chosen[0] = bs;
     chosen[1] = bz;
