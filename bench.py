@@ -302,11 +302,59 @@ def ensemble_timing(steps=100, err_steps=200, seed=7):
             "u_rel_l2_vs_f32_per_box": {"after_steps": err_steps, "max": max(errs), "median": float(np.median(errs))}}
 
 
+def closure_experiment(n=1024, ntrain=896, R_hi=6, L_hi=48, R_lo=3, steps_hi=240, seed=11, epochs=300):
+    """Learned closure workload: two-sphere data from the method itself (R_hi resolved, R_lo under-resolved,
+    gap/R log-uniform in [0.05, 1.5], pair-frame velocities and angular velocities uniform in +-1e-3, static
+    force subtracted), training on the GPU by the library's kernels, held-out evaluation.  Errors are force
+    errors of the corrected R_lo pair against the scaled R_hi pair, relative, over the held-out pairs."""
+    from lbcuda_b200 import LBSim, closure, make_params
+    t0 = time.perf_counter()
+    X, T, info = closure.generate(n, R_hi=R_hi, L_hi=L_hi, R_lo=R_lo, steps_hi=steps_hi, seed=seed)
+    t_gen = time.perf_counter() - t0
+    w, loss = closure.train(X[:ntrain], T[:ntrain], epochs=epochs, lr=2e-3)
+    Xt, Tt, base = X[ntrain:], T[ntrain:], info["base"][ntrain:]
+    pred = closure.infer(w, Xt)
+    lub = closure.analytic_lubrication(Xt, float(R_lo))
+    fidx = [0, 1, 2, 6, 7, 8]  # the two forces, pair frame
+    hi = (base + Tt)[:, fidx]
+
+    def rel(corr):
+        err = (Tt - corr)[:, fidx]
+        per_pair = np.linalg.norm(err, axis=1) / np.maximum(np.linalg.norm(hi, axis=1), 1e-30)
+        return {"rel_l2": float(np.linalg.norm(err) / np.linalg.norm(hi)), "median_pair": float(np.median(per_pair)),
+                "pairs_within_5pct": float(np.mean(per_pair <= 0.05))}
+
+    # cost of a step at each resolution (same prescribed-motion pair runs)
+    costs = {}
+    for R, L in ((R_hi, L_hi), (R_lo, int(round(L_hi * R_lo / R_hi)))):
+        p = make_params(L, model="cg", storage="f32", max_particles=2, radius=float(R), kinematic=1, lrotate=1,
+                        wetting="neutral", max_vel=1.0, exact_tiles=0)
+        sim = LBSim(p)
+        one = np.ones((L, L, L), np.float32)
+        sim.set_fields(one, np.zeros_like(one))
+        c = np.full(3, (L + 1) / 2.0)
+        sim.set_particles(np.stack([c - [1.2 * R, 0, 0], c + [1.2 * R, 0, 0]]), np.zeros((2, 3)))
+        sim.step(10)
+        tot, _, _ = sim.time_steps(100, kernel_timing=False)
+        costs[R] = tot / 100
+        sim.close()
+    steps_lo = info["steps_lo"]
+    return {"samples": n, "train": ntrain, "held_out": n - ntrain, "R_hi": R_hi, "R_lo": R_lo, "L_hi": L_hi,
+            "steps_hi": steps_hi, "steps_lo": steps_lo, "generate_s": t_gen, "final_loss": float(loss[-1]),
+            "error_no_correction": rel(np.zeros_like(Tt)), "error_analytic_lubrication": rel(lub),
+            "error_closure": rel(pred),
+            "ms_per_step": {"R_hi": costs[R_hi], "R_lo": costs[R_lo]},
+            "cost_ratio_same_physical_time": costs[R_hi] * steps_hi / (costs[R_lo] * steps_lo)}
+
+
 def only_region(args, local):
     import torch
     torch.cuda.set_device(local)
     from lbcuda_b200 import LBSim, make_params
     from lbcuda_b200.inputs import seeded_noise_fields
+    if args.only == "closure":
+        print(json.dumps(closure_experiment()), flush=True)
+        return 0
     if args.only == "ensemble":
         print(json.dumps(ensemble_timing()), flush=True)
         return 0
@@ -338,7 +386,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-extras", action="store_true", help="skip the error runs, the colloid case and the CPU baseline")
     ap.add_argument("--only", choices=["f16", "f32", "bf16", "f64", "colloid-f16", "colloid-f32", "colloid-f16-small",
-                                       "colloid-f32-small", "ensemble"],
+                                       "colloid-f32-small", "ensemble", "closure"],
                     help="profiling aid: run one timed region only and print its timing")
     ap.add_argument("--lb-steps", type=int, default=LB_PER_STEP, help="lattice steps per bench step")
     ap.add_argument("--schedule", type=int, default=2, help="colour-gradient schedule (0, 1, 2)")
@@ -452,6 +500,7 @@ def main():
         extras["error_vs_f64"] = error_vs_f64()
         extras["colloid_256_1280"] = {st: colloid_timing(st) for st in ("f16", "f32")}
         extras["ensemble_48"] = ensemble_timing()
+        extras["closure"] = closure_experiment()
         extras["cpu_baseline"] = cpu_baseline_sample()
 
     if rank == 0:

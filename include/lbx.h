@@ -94,8 +94,10 @@ typedef struct lbx_params {
   float hz_k, hz_rmin, hz_rcap;             /* Hertz (dimensions_m.CUF:77-80) */
   int32_t lubrication;                      /* llubrication (dimensions_m.CUF:81) */
   float lubric_k, lubric_rmin, lubric_rcap; /* dimensions_m.CUF:82-84 */
-  int32_t kinematic;      /* 1: prescribed motion (force probes): centres move with the set
-                             velocity; velocity, angular velocity, orientation kept */
+  int32_t kinematic;      /* force probes, no counterpart in the reference.  1: prescribed
+                             motion: centres move with the set velocity; velocity, angular
+                             velocity, orientation kept.  2: frozen geometry: centres stay,
+                             the bounce-back walls move with the set velocities */
   int32_t closure;        /* 1: learned pair closure with analytic fallback (lbx_closure_*) */
   float closure_gap_min;  /* training envelope of the closure: gap / R in [min, max] */
   float closure_gap_max;

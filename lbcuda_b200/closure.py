@@ -3,13 +3,18 @@
 The closure corrects the force and torque of near-contact sphere pairs that
 the lattice resolves poorly (small radius).  Its training data come from the
 method itself: the same two-sphere configuration is run with prescribed
-sphere motion (``kinematic`` contexts) once well resolved (radius R_hi in an
+sphere motion (``kinematic`` contexts, frozen geometry) once well resolved (radius R_hi in an
 L_hi^3 box) and once at the deployment radius R_lo (box, gap and time scaled
 by s = R_lo/R_hi, s^2 for time; translational velocities equal, angular
 velocities scaled by s so that the surface velocities agree).  For such
 dynamically similar Stokes flows forces scale as mu R U and torques as
 mu R^2 U, so the target is F_hi s - F_lo and T_hi s^2 - T_lo, in the pair
-frame.  Training and
+frame.  Each force is the difference between the run with the sampled
+motion and the same configuration at rest: two spheres closer than a few
+cells hide some of each other's surface links, which leaves a static
+pressure imbalance of order w rho per hidden link that depends on how the
+pair sits on the lattice, not on the pair-frame inputs, and that no closure
+of those inputs can learn.  Training and
 inference run in the library's own kernels (lbx_closure_train /
 lbx_closure_infer); the analytic lubrication of the reference stays the
 fallback outside the training envelope and the judge of the gain.
@@ -42,9 +47,20 @@ def pair_frame(n):
     return t1, np.cross(n, t1)
 
 
+def nint(x):
+    """Fortran NINT (half away from zero), the rounding that places a sphere's template."""
+    x = np.asarray(x, np.float64)
+    return np.sign(x) * np.floor(np.abs(x) + 0.5)
+
+
 def features(xi, xj, vi, vj, oi, oj, R, box):
-    """The 11 closure inputs of pair (i, j) (lab angular velocities)."""
-    d = np.asarray(xj, np.float64) - np.asarray(xi, np.float64)
+    """The 11 closure inputs of pair (i, j) (lab angular velocities).
+
+    Gap and pair frame come from the rounded centres, where the spheres'
+    templates actually sit: an under-resolved pair's forces follow its
+    discrete geometry, which can differ from the nominal one by a cell.
+    """
+    d = nint(xj) - nint(xi)
     box = np.asarray(box, np.float64)
     d = d - box * np.round(d / box)
     r = np.linalg.norm(d)
@@ -67,33 +83,35 @@ def sample_configs(n, seed=0, gap_range=(0.05, 1.5), vmax=1e-3):
     return [dict(gap=g, n=d, dv=a, oi=b, oj=c) for g, d, a, b, c in zip(gaps, dirs, dv, oi, oj)]
 
 
-def run_pair(cfg, R, L, steps, average=0.25, storage="f32", lubrication=False, sim_cache=None):
+def run_pair(cfg, R, L, steps, average=0.25, storage="f32", lubrication=False, sim_cache=None, mult=1):
     """Forces / torques on both spheres of a prescribed-motion two-sphere run.
 
-    Spheres of radius R at distance 2R + gap*R along cfg['n'] around the box
-    centre, velocities -dv/2 and +dv/2 (pair frame -> lab), angular
-    velocities oi, oj (pair frame -> lab, body frame = lab, identity
-    orientation).  The spheres move with their set velocities; they start
-    displaced so that they pass through that configuration in the middle of
-    the averaging window.  Returns (F_i, T_i, F_j, T_j) in the lab frame,
+    Spheres of radius R on lattice sites, the second at mult * cfg['d'] (an
+    integer lattice vector) from the first, velocities -dv/2 and +dv/2 (pair
+    frame -> lab), angular velocities oi, oj (pair frame -> lab, body frame =
+    lab, identity orientation).  The geometry is frozen (kinematic = 2): the spheres keep
+    their place while their bounce-back walls move with the set velocities,
+    so the forces belong to this configuration and no cell is filled or
+    drained during the run.  Returns (F_i, T_i, F_j, T_j) in the lab frame,
     averaged over the last `average` fraction of the steps, and the
-    configuration (x, v, omega) the average belongs to.
+    configuration (x, v, omega).
     """
-    n = np.asarray(cfg["n"], np.float64)
+    d = np.asarray(cfg["d"], np.float64) * mult
+    n = d / np.linalg.norm(d)
     t1, t2 = pair_frame(n)
     Fm = np.stack([n, t1, t2])
     dv = Fm.T @ cfg["dv"]
     oi = Fm.T @ cfg["oi"]
     oj = Fm.T @ cfg["oj"]
-    c = np.full(3, (L + 1) / 2.0)
-    half = R + 0.5 * cfg["gap"] * R
-    x = np.stack([c - half * n, c + half * n])
+    c = np.full(3, float(L // 2))
+    xj = (c + d - 1.0) % L + 1.0
+    x = np.stack([c, xj])
     v = np.stack([-0.5 * dv, 0.5 * dv])
     om = np.stack([oi, oj])
     key = (R, L, storage, lubrication)
     sim = sim_cache.get(key) if sim_cache is not None else None
     if sim is None:
-        p = make_params(L, model="cg", storage=storage, max_particles=2, radius=float(R), kinematic=1,
+        p = make_params(L, model="cg", storage=storage, max_particles=2, radius=float(R), kinematic=2,
                         lrotate=1, wetting="neutral", max_vel=1.0,
                         hz_rmin=float(2 * R - 0.5), hz_rcap=float(2 * R - 2.0),
                         lubrication=1 if lubrication else 0, lubric_k=1.0 / 6.0, lubric_rmin=1.0,
@@ -104,7 +122,7 @@ def run_pair(cfg, R, L, steps, average=0.25, storage="f32", lubrication=False, s
     one = np.ones((L, L, L), np.float32)
     sim.set_fields(one, np.zeros_like(one))
     nav = max(1, int(round(steps * average)))
-    sim.set_particles(x - v * (steps - 0.5 * nav), v, om, None)
+    sim.set_particles(x, v, om, None)
     sim.step(steps - nav)
     acc = np.zeros((4, 3))
     for _ in range(nav):
@@ -114,7 +132,8 @@ def run_pair(cfg, R, L, steps, average=0.25, storage="f32", lubrication=False, s
     return acc / nav, x, v, om
 
 
-def generate(n_samples, R_hi=12, L_hi=128, R_lo=3, steps_hi=300, seed=0, progress=None, gap_range=(0.05, 1.5)):
+def generate(n_samples, R_hi=12, L_hi=128, R_lo=3, steps_hi=300, seed=0, progress=None, gap_range=(0.05, 1.5),
+             subtract_static=True):
     """(X, T, info): features at R_lo and targets (resolved - under-resolved, pair frame).
 
     The periodic box must keep each sphere's image farther away than its
@@ -126,15 +145,34 @@ def generate(n_samples, R_hi=12, L_hi=128, R_lo=3, steps_hi=300, seed=0, progres
     for L, R in ((L_hi, R_hi), (L_lo, R_lo)):
         if L < (4.0 + 2.0 * gap_range[1]) * R:
             raise ValueError(f"box {L} too small for radius {R} and gap/R up to {gap_range[1]}")
-    cfgs = sample_configs(n_samples, seed, gap_range=gap_range)
+    if abs(R_hi / R_lo - round(R_hi / R_lo)) > 1e-12:
+        raise ValueError("R_hi must be an integer multiple of R_lo")
+    mult = int(round(R_hi / R_lo))
+    # separations on the R_lo lattice (R_hi: the same vector times R_hi / R_lo),
+    # nearest to the sampled gap and direction, kept inside the gap range
+    cfgs = []
+    pool = sample_configs(8 * n_samples, seed, gap_range=gap_range)
+    for cfg in pool:
+        d = nint(np.asarray(cfg["n"]) * (2.0 + cfg["gap"]) * R_lo)
+        gap = np.linalg.norm(d) / R_lo - 2.0
+        if gap_range[0] <= gap <= gap_range[1]:
+            cfgs.append(dict(cfg, d=d, gap=gap, n=d / np.linalg.norm(d)))
+        if len(cfgs) == n_samples:
+            break
+    if len(cfgs) < n_samples:
+        raise ValueError("gap range admits too few lattice separations")
     X = np.zeros((n_samples, DIN))
     T = np.zeros((n_samples, DOUT))
     base = np.zeros((n_samples, DOUT))
     cache = {}
     for k, cfg in enumerate(cfgs):
         cfg_hi = dict(cfg, oi=np.asarray(cfg["oi"]) * s, oj=np.asarray(cfg["oj"]) * s)
-        hi, *_ = run_pair(cfg_hi, R_hi, L_hi, steps_hi, sim_cache=cache)
+        hi, *_ = run_pair(cfg_hi, R_hi, L_hi, steps_hi, sim_cache=cache, mult=mult)
         lo, x, v, om = run_pair(cfg, R_lo, L_lo, steps_lo, sim_cache=cache)
+        if subtract_static:
+            rest = dict(cfg, dv=np.zeros(3), oi=np.zeros(3), oj=np.zeros(3))
+            hi = hi - run_pair(rest, R_hi, L_hi, steps_hi, sim_cache=cache, mult=mult)[0]
+            lo = lo - run_pair(rest, R_lo, L_lo, steps_lo, sim_cache=cache)[0]
         feat, Fm = features(x[0], x[1], v[0], v[1], om[0], om[1], R_lo, (L_lo,) * 3)
         scale = np.array([s, s * s, s, s * s])[:, None]
         target = hi * scale - lo

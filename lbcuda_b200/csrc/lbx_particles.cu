@@ -1006,8 +1006,15 @@ __global__ void k_closure_pairs(PDev P, const double* __restrict__ pos, Geom g, 
     if (j < i) continue;
     const double* pi = pos + size_t(i) * PS;
     const double* pj = pos + size_t(j) * PS;
+    // the network sees the pair where the templates sit (rounded centres)
     double d[3];
-    min_image(g, pi, pj, d);
+    {
+      const int nn3[3] = {g.nx, g.ny, g.nz};
+      for (int k = 0; k < 3; ++k) {
+        double dk = double(nint_idx(pj[k], nn3[k]) - nint_idx(pi[k], nn3[k]));
+        d[k] = dk - double(nn3[k]) * double(nint_d(dk / nn3[k]));
+      }
+    }
     const double r = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
     const double n[3] = {d[0] / r, d[1] / r, d[2] / r};
     double t1[3], t2[3];
@@ -1043,16 +1050,21 @@ __global__ void k_closure_pairs(PDev P, const double* __restrict__ pos, Geom g, 
         for (int c = 0; c < 3; ++c)
           out[3 * q + c] = float(y[3 * q] * n[c] + y[3 * q + 1] * t1[c] + y[3 * q + 2] * t2[c]);
     } else if (P.lub) {
+      // the reference's lubrication on the centres themselves (addHertzian)
+      double dc[3];
+      min_image(g, pi, pj, dc);
+      const double rc = sqrt(dc[0] * dc[0] + dc[1] * dc[1] + dc[2] * dc[2]);
+      const double nc[3] = {dc[0] / rc, dc[1] / rc, dc[2] / rc};
       const double rpar = 2.0 * P.rdim, rparcut = rpar + P.lub_rmin, rparcap = rpar + P.lub_rcap;
-      if (r <= rparcut) {
+      if (rc <= rparcut) {
         const double lubfactor =
             P.lub_k * 6.0 * 3.141592653589793238462643383279502884 * pow(P.rdim * P.rdim, 2.0) / (rpar * rpar);
-        double rr = r <= rparcap ? rparcap : r;
-        double dotuv = n[0] * (pi[3] - pj[3]) + n[1] * (pi[4] - pj[4]) + n[2] * (pi[5] - pj[5]);
+        double rr = rc <= rparcap ? rparcap : rc;
+        double dotuv = nc[0] * (pi[3] - pj[3]) + nc[1] * (pi[4] - pj[4]) + nc[2] * (pi[5] - pj[5]);
         double cc = lubfactor * dotuv * (1.0 / (rr - rpar) - 1.0);
         for (int c = 0; c < 3; ++c) {
-          out[c] = float(-cc * n[c]);
-          out[6 + c] = float(cc * n[c]);
+          out[c] = float(-cc * nc[c]);
+          out[6 + c] = float(cc * nc[c]);
         }
       }
     }
@@ -1185,6 +1197,8 @@ __global__ void k_integrate(PDev P, const double* __restrict__ pos_cur, double* 
   for (int d = 0; d < 3; ++d) { pn[d] = xn[d]; pn[3 + d] = bv[d]; }
   if (P.kinematic)  // prescribed motion: the centre moves with the set velocity, v / omega / q are kept
     for (int k = 3; k < PS; ++k) pn[k] = pc[k];
+  if (P.kinematic == 2)  // frozen geometry: the centre stays, the wall still moves with v and omega
+    for (int d = 0; d < 3; ++d) pn[d] = pc[d];
   for (int d = 0; d < 3; ++d) {
     fo[d] = P.ext_f[d];
     fo[3 + d] = 0;
@@ -1573,7 +1587,9 @@ int part_pairs(Ctx& c) {
   k_pairs<<<warp_blocks, 256, 0, c.stream>>>(t.P, t.pc, s.acc, t.g);
   if (c.p.closure) {
     const int use_net = s.closure_ready;
-    const double cut = fmax(double(c.p.closure_gap_max) * s.rdim, c.p.lubrication ? double(c.p.lubric_rmin) : 0.0);
+    // the network's gap is that of the rounded centres, up to sqrt 3 closer
+    const double cut =
+        fmax(double(c.p.closure_gap_max) * s.rdim + 1.75, c.p.lubrication ? double(c.p.lubric_rmin) : 0.0);
     k_pair_nbrs<<<warp_blocks, 256, 0, c.stream>>>(t.P, t.pc, t.g, cut, s.nbr, s.nbr_cnt, c.d_err, t.st);
     size_t smem = sizeof(float) * (size_t(LBX_CLOSURE_NWEIGHTS) + 8 * 2 * H);
     int blocks = (s.np * NBCAP + 7) / 8;

@@ -919,6 +919,8 @@ class Oracle {
         for (int c = 6; c < 13; ++c) ps(o, a, c) = ps(b, a, c);
       if (prm.kinematic) /* prescribed motion: centre moves with the set velocity, v / omega / q kept */
         for (int c = 3; c < 13; ++c) ps(o, a, c) = ps(b, a, c);
+      if (prm.kinematic == 2) /* frozen geometry: centre stays, the wall still moves with v and omega */
+        for (int c = 0; c < 3; ++c) ps(o, a, c) = ps(b, a, c);
       /* reset the accumulators to the external force / torque */
       for (int d = 0; d < 3; ++d) {
         fa(o, a, d) = P(prm.ext_force[d]);

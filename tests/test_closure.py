@@ -47,10 +47,11 @@ def test_pair_frame_and_features():
         F = np.stack([n, t1, t2])
         assert np.allclose(F @ F.T, np.eye(3), atol=1e-12)
     x, F = features([10, 10, 10], [17.5, 10, 10], [0, 0, 0], [-1e-3, 0, 0], [0, 0, 0], [0, 0, 0], 3.0, (32,) * 3)
-    assert abs(x[0] - 0.5) < 1e-12 and abs(x[1] + 1e-3) < 1e-15 and x[10] == 3.0
-    # periodic image: the pair across the boundary
+    # the gap of the rounded centres (the templates sit at 10 and NINT(17.5) = 18)
+    assert abs(x[0] - 2.0 / 3.0) < 1e-12 and abs(x[1] + 1e-3) < 1e-15 and x[10] == 3.0
+    # periodic image: the pair across the boundary (NINT(31.5) = 32, one cell from 1)
     x, _ = features([1, 10, 10], [31.5, 10, 10], [0, 0, 0], [0, 0, 0], [0, 0, 0], [0, 0, 0], 3.0, (32,) * 3)
-    assert abs(x[0] - (1.5 - 6) / 3) < 1e-12
+    assert abs(x[0] - (1.0 - 6) / 3) < 1e-12
 
 
 def test_analytic_lubrication_is_repulsive_on_approach():
@@ -148,10 +149,10 @@ def test_zero_network_changes_nothing():
 
 @pytest.mark.gpu
 def test_trained_closure_beats_plain_method_on_held_out_pairs():
-    """Small end-to-end run: R_hi = 8 in 64^3 resolves, R_lo = 4 in 32^3 does not (gap/R up to 1.5)."""
+    """Small end-to-end run: R_hi = 6 in 48^3 resolves, R_lo = 3 in 24^3 does not (gap/R up to 1.5)."""
     from lbcuda_b200 import closure
-    X, T, info = closure.generate(96, R_hi=8, L_hi=64, R_lo=4, steps_hi=160, seed=5)
-    ntr = 72
+    X, T, info = closure.generate(192, R_hi=6, L_hi=48, R_lo=3, steps_hi=160, seed=5)
+    ntr = 160
     w, loss = closure.train(X[:ntr], T[:ntr], epochs=300, lr=2e-3)
     pred = closure.infer(w, X[ntr:])
     base_err = np.linalg.norm(T[ntr:])                      # plain method: no correction

@@ -121,12 +121,14 @@ def test_reference_deck_placement_flags():
     assert np.array_equal(g.get_flags(), o.get_flags())
 
 
-def test_kinematic_pair_parity():
-    """Prescribed-motion spheres (the closure's force probes) across the periodic boundary."""
+@pytest.mark.parametrize("kinematic", [1, 2])
+def test_kinematic_pair_parity(kinematic):
+    """Prescribed-motion (1) and frozen-geometry (2) spheres, the closure's force probes, across the
+    periodic boundary."""
     x = np.array([[4.0, 16.0, 16.0], [24.3, 16.5, 15.8]])   # periodic distance 11.71, gap 0.71
     v = np.array([[-0.01, 0.002, 0.0], [0.01, -0.002, 0.001]])
     om = np.array([[0.0, 0.0, 0.002], [0.001, 0.0, 0.0]])
-    g, o = make_pair(32, x, v, om, steps=20, wetting="neutral", kinematic=1, lrotate=1)
+    g, o = make_pair(32, x, v, om, steps=20, wetting="neutral", kinematic=kinematic, lrotate=1)
     gp, op = g.get_particles(), o.get_particles()
     assert np.array_equal(g.get_flags(), o.get_flags())
     assert np.abs(gp["x"] - op["x"]).max() < 1e-9

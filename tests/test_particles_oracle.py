@@ -80,3 +80,13 @@ def test_kinematic_sphere_moves_with_set_velocity():
     assert np.abs(d["x"][0] - [12.7, 16.35, 16.3]).max() < 1e-9
     assert np.array_equal(d["v"][0], [0.02, 0.01, 0.0])
     assert d["force"][0, 0] < 0 and d["force"][0, 1] < 0
+
+
+def test_frozen_geometry_sphere_keeps_its_centre():
+    """kinematic = 2: the centre stays while the wall moves with the set velocity (drag recorded)."""
+    o = _sim(32, [[12.2, 16.1, 16.3]], [[0.02, 0.0, 0.0]], wetting="neutral", kinematic=2)
+    o.step(20)
+    d = o.get_particles()
+    assert np.array_equal(d["x"][0], [12.2, 16.1, 16.3])
+    assert np.array_equal(d["v"][0], [0.02, 0.0, 0.0])
+    assert d["force"][0, 0] < 0
