@@ -70,6 +70,7 @@ extern "C" {
 #define LBX_DEV_POSITION 4        /* nve_lf, kernels_fluid_PART.CUF:1581-1598 */
 #define LBX_DEV_LIST_OVERFLOW 5   /* makeListAtomsGPU, kernels_fluid_PART.CUF:2436-2439 */
 #define LBX_DEV_BELT_RANGE 6      /* compute_onebelt_*, kernels_fluid_PART.CUF:800-803 */
+#define LBX_DEV_WAIT_TIMEOUT 7    /* a bounded in-kernel wait gave up (no counterpart in the reference) */
 
 /* ---- parameters -------------------------------------------------------- */
 /* The reference keeps these as compile-time `parameter`s (dimensions_m.CUF:

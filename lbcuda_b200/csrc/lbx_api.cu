@@ -384,6 +384,7 @@ const char* lbx_error_string(int code) {
     case LBX_DEV_POSITION: return "particle position outside the box (nve_lf)";
     case LBX_DEV_LIST_OVERFLOW: return "too many particles near one cell block";
     case LBX_DEV_BELT_RANGE: return "belt neighbour outside the lattice";
+    case LBX_DEV_WAIT_TIMEOUT: return "in-kernel wait timed out";
   }
   return "unknown error";
 }

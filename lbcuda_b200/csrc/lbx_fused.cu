@@ -191,6 +191,34 @@ __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
+// ---- split barrier of a plane (mbarrier in shared memory) -----------------
+// Every thread arrives once the phase field of plane z+1 is in the window and
+// waits only before its collision reads that plane, so the BGK half of the
+// collision runs while slower threads finish their copies.
+__device__ __forceinline__ void mbar_init(unsigned long long* m, unsigned count) {
+  const unsigned a = static_cast<unsigned>(__cvta_generic_to_shared(m));
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(a), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(unsigned long long* m) {
+  const unsigned a = static_cast<unsigned>(__cvta_generic_to_shared(m));
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(a) : "memory");
+}
+// wait for the completion of the phase of the given parity; false if the
+// bounded number of polls ran out (each poll may itself suspend a while)
+__device__ __forceinline__ bool mbar_wait(unsigned long long* m, unsigned parity) {
+  const unsigned a = static_cast<unsigned>(__cvta_generic_to_shared(m));
+  for (int i = 0; i < (1 << 22); ++i) {
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (ok) return true;
+  }
+  return false;
+}
+
 // issue the 19 pulls of a cell as asynchronous copies into st[l * stride]
 template <typename S>
 __device__ __forceinline__ void pull_async(const S* __restrict__ A, int64_t n, const PullIdx& P,
@@ -241,12 +269,35 @@ __device__ __forceinline__ C clamp0(C v) { return v < C(0) ? C(0) : v; }
 template <typename C>
 __device__ __forceinline__ C fm(C a, C b, C c) { return fma(a, b, c); }
 
+// reciprocal (FP32: the correctly rounded __frcp_rn, one multiply cheaper to
+// use than a division) and reciprocal square root (FP32: rsqrtf)
+template <typename C>
+__device__ __forceinline__ C rcp_c(C x) {
+  if constexpr (sizeof(C) == 4) return __frcp_rn(x);
+  else return C(1) / x;
+}
+template <typename C>
+__device__ __forceinline__ C rsqrt_c(C x) {
+  if constexpr (sizeof(C) == 4) return rsqrtf(x);
+  else return C(1) / sqrt(x);
+}
+// phase field (rR - rB) / (rR + rB)
+template <typename C>
+__device__ __forceinline__ C phase_of(C rR, C rB) { return (rR - rB) * rcp_c(rR + rB); }
+
 // One colour-gradient collision (time_step_CG, kernels_fluid_CG.CUF:689-846)
 // on the component pairs g[l] = (g_R, g_B): stored form (f - shift) on entry,
-// post-collision stored form on exit.  rR/rB: clamped densities.
+// post-collision stored form on exit.  rR/rB: clamped densities.  Two
+// halves: the BGK relaxation (no colour gradient needed), then the
+// perturbation and recolouring with the gradient (psi).
 template <typename C>
-__device__ __forceinline__ void collide_pair(const LeanConst<C>& K, P2<C> g[Q], C rR, C rB, C px, C py, C pz,
-                                             bool shifted) {
+struct CollideState {
+  C omega, inv;
+};
+
+template <typename C>
+__device__ __forceinline__ CollideState<C> collide_bgk(const LeanConst<C>& K, P2<C> g[Q], C rR, C rB,
+                                                       bool shifted) {
   const C ONE = C(1), HALF = C(0.5);
   const C rs = rR + rB;
   C omega;
@@ -258,7 +309,7 @@ __device__ __forceinline__ void collide_pair(const LeanConst<C>& K, P2<C> g[Q], 
     omega = ONE / fm(visc, K.inv_cssq, HALF);
   }
   const C omm = ONE - omega;
-  const C inv = ONE / rs;
+  const C inv = rcp_c(rs);
   // momentum from the opposite-pair differences (shifts cancel)
   const P2<C> NEG = pp(C(-1), C(-1));
   C d[10];
@@ -296,10 +347,20 @@ __device__ __forceinline__ void collide_pair(const LeanConst<C>& K, P2<C> g[Q], 
     g[l] = p_fma(fl, omm2, p_mul(Kc[k], pp(Ap, Ap)));
     g[o] = p_fma(fo, omm2, p_mul(Kc[k], pp(Am, Am)));
   }
+  return CollideState<C>{omega, inv};
+}
+
+template <typename C>
+__device__ __forceinline__ void collide_recolour(const LeanConst<C>& K, P2<C> g[Q], C rR, C rB, C px, C py, C pz,
+                                                 bool shifted, CollideState<C> cs) {
+  const C omega = cs.omega, inv = cs.inv;
+  P2<C> ns[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) ns[k] = pp(-K.s[0][k], -K.s[1][k]);  // minus the shift
   const C psq = fm(px, px, fm(py, py, pz * pz));
   if (psq > C(1.e-20)) {
-    const C pn = sqrt(psq);
-    const C ipn = ONE / pn;
+    const C ipn = rsqrt_c(psq);
+    const C pn = psq * ipn;
     const C acoeff = C(9) / C(4) * omega * K.sigma;
     const C coef = K.beta * rR * rB * inv * ipn;  // beta rR rB / (rs |psi|)
     const P2<C> kk = pp(rR * inv, rB * inv);
@@ -336,6 +397,13 @@ __device__ __forceinline__ void collide_pair(const LeanConst<C>& K, P2<C> g[Q], 
       g[2 * p] = p_add(g[2 * p], ns[k]);
     }
   }
+}
+
+template <typename C>
+__device__ __forceinline__ void collide_pair(const LeanConst<C>& K, P2<C> g[Q], C rR, C rB, C px, C py, C pz,
+                                             bool shifted) {
+  const CollideState<C> cs = collide_bgk(K, g, rR, rB, shifted);
+  collide_recolour(K, g, rR, rB, px, py, pz, shifted, cs);
 }
 
 template <int TX, int TY>
@@ -390,7 +458,8 @@ struct LeanSmem {
   static constexpr size_t RING = kStage<S> ? sizeof(R) * 2 * Q * RN : 0;
   static constexpr size_t SIDE = PART ? (sizeof(SideRec<C>) * (3 * NT + 2 * RN) + 15) / 16 * 16 : 0;
   static constexpr size_t FOLD = PART ? (4 * CELLS + 15) / 16 * 16 : 0;
-  static constexpr size_t BYTES = PHI + OWN + RING + SIDE + FOLD;
+  static constexpr size_t BAR = 16;  // the plane's split barrier
+  static constexpr size_t BYTES = PHI + OWN + RING + SIDE + FOLD + BAR;
   static_assert(PHI % 16 == 0 && OWN % 16 == 0 && RING % 16 == 0, "stage alignment");
   static __device__ __forceinline__ C (*phi(unsigned char* base))[CELLS] {
     return reinterpret_cast<C(*)[CELLS]>(base);
@@ -404,6 +473,13 @@ struct LeanSmem {
   static __device__ __forceinline__ int8_t (*fold(unsigned char* base))[CELLS] {
     return PART ? reinterpret_cast<int8_t(*)[CELLS]>(base + PHI + OWN + RING + SIDE) : nullptr;
   }
+  static __device__ __forceinline__ unsigned long long* bar(unsigned char* base) {
+    return reinterpret_cast<unsigned long long*>(base + PHI + OWN + RING + SIDE + FOLD);
+  }
+  // thread 0 sets up the barrier for the CTA's threads; the caller then syncs
+  static __device__ __forceinline__ void init(unsigned char* base) {
+    if (threadIdx.x == 0 && threadIdx.y == 0) mbar_init(bar(base), TX * TY);
+  }
 };
 
 // One column march: cells [x0, x0+TX) x [y0, y0+TY) x [z0, zend) of one box.
@@ -414,7 +490,8 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
                                             const LeanPart<typename Store<S>::C>& PT,
                                             typename Store<S>::C (*sphi)[Ring<TX, TY>::CELLS],
                                             typename SPair<S>::R* stage, SideRec<typename Store<S>::C>* side,
-                                            int8_t (*sfold)[Ring<TX, TY>::CELLS]) {
+                                            int8_t (*sfold)[Ring<TX, TY>::CELLS], unsigned long long* bar,
+                                            unsigned& bar_parity) {
   using C = typename Store<S>::C;
   constexpr int NT = TX * TY;
   using R = Ring<TX, TY>;
@@ -508,11 +585,13 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
           rB = C(0);
           if (fn == LBX_FLUID_SPHERELIST) return rec->phi;
           if (fn == LBX_FLUID_FLUID) {  // new fluid cell
-            if (!is_own) return rec->phi;
-            rR = PT.rhoR[cell];
-            rB = PT.rhoB[cell];
+            if (is_own) {
+              rR = PT.rhoR[cell];
+              rB = PT.rhoB[cell];
+            }
+            return rec->phi;
           }
-          return (rR - rB) / (rR + rB);
+          return phase_of(rR, rB);
         }
       }
     }
@@ -527,7 +606,7 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
       raise_error(err, LBX_DEV_RHO_RANGE, step, cell);
     rR = clamp0(rR);
     rB = clamp0(rB);
-    return (rR - rB) / (rR + rB);
+    return phase_of(rR, rB);
   };
 
   // phase field of plane p (own cell and ring cell) into its window slot, and
@@ -567,6 +646,7 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
   issue(z0 + 1);
   settle();
   phase_plane(z0, rRn, rBn);
+  __syncthreads();  // planes z0-1 and z0 of the window
   for (int z = z0; z < zend; ++z) {
     rRc = rRn;
     rBc = rBn;
@@ -576,12 +656,17 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
     else if constexpr (ASYNC) cp_async_commit();  // one group per iteration
     settle();
     phase_plane(z + 1, rRn, rBn);
-    __syncthreads();
+    mbar_arrive(bar);
+    // Until the wait below, only planes z-1 and z of the windows are read:
+    // every thread wrote them before arriving at the previous plane's barrier,
+    // and their slots are rewritten only after this plane's barrier.
+    const int cell = x + g.nx * (y + g.ny * z);
+    P2<C> gp[Q];
+    bool collide = true, solid = false;
+    C px = 0, py = 0, pz = 0;
+    CollideState<C> cst{C(0), C(0)};
+    PullIdx P;
     if (active) {
-      const int cell = x + g.nx * (y + g.ny * z);
-      P2<C> gp[Q];
-      bool collide = true;
-      PullIdx P;
       pull_idx(g, x, y, z, P);
       // the pull every fluid cell needs: in the stage since two iterations,
       // or issued here
@@ -598,43 +683,63 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
           int8_t fn, fo;
           flags_of(side + own_q(z) * NT + tid, cell, fn, fo);
           collide = fn == LBX_FLUID_FLUID;
+          solid = !collide;
           if (collide && fo != LBX_FLUID_FLUID) {
             // make_fluid already wrote the new node's populations (stored form) into B
 #pragma unroll
             for (int l = 0; l < Q; ++l) gp[l] = SPair<S>::ld(Bp(l) + 2 * cell);
-          } else if (!collide) {
-            // solid cell: streamed populations only; a spheredead source
-            // (previous step, from the flag window) leaves the destination's
-            // stale value, which is B's entry
-#pragma unroll
-            for (int l = 1; l < Q; ++l)
-              if (sfold[(z - ez(l)) & 3][own - ey(l) * R::RX - ex(l)] == LBX_FLUID_SPHEREDEAD)
-                gp[l] = SPair<S>::ld(Bp(l) + 2 * cell);
           }
         }
       }
       if (collide) {
+        // colour gradient from planes z-1 and z, then the BGK half
         const C* pm = sphi[(z + 3) & 3];
         const C* p0 = sphi[z & 3];
-        const C* ppl = sphi[(z + 1) & 3];
-        C px = 0, py = 0, pz = 0;
 #pragma unroll
         for (int l = 1; l < Q27; ++l) {
           const int dx = ex27(l), dy = ey27(l), dz = ez27(l);
-          const C* pl = dz < 0 ? pm : (dz > 0 ? ppl : p0);
+          if (dz > 0) continue;
+          const C* pl = dz < 0 ? pm : p0;
           const C ps = pl[own + dy * R::RX + dx];
           const C a = K.a27[wclass27(l)];
           if (dx) px = fm(dx > 0 ? a : -a, ps, px);
           if (dy) py = fm(dy > 0 ? a : -a, ps, py);
           if (dz) pz = fm(dz > 0 ? a : -a, ps, pz);
         }
-        collide_pair(K, gp, rRc, rBc, px, py, pz, Store<S>::shifted);
+        cst = collide_bgk(K, gp, rRc, rBc, Store<S>::shifted);
+      }
+    }
+    if (!mbar_wait(bar, bar_parity)) raise_error(err, LBX_DEV_WAIT_TIMEOUT, step, -1);
+    bar_parity ^= 1u;
+    if (active) {
+      if constexpr (PART) {
+        if (solid) {
+          // solid cell: streamed populations only; a spheredead source
+          // (previous step, from the flag window) leaves the destination's
+          // stale value, which is B's entry
+#pragma unroll
+          for (int l = 1; l < Q; ++l)
+            if (sfold[(z - ez(l)) & 3][own - ey(l) * R::RX - ex(l)] == LBX_FLUID_SPHEREDEAD)
+              gp[l] = SPair<S>::ld(Bp(l) + 2 * cell);
+        }
+      }
+      if (collide) {
+        const C* ppl = sphi[(z + 1) & 3];
+#pragma unroll
+        for (int l = 1; l < Q27; ++l) {
+          const int dx = ex27(l), dy = ey27(l), dz = ez27(l);
+          if (dz <= 0) continue;
+          const C ps = ppl[own + dy * R::RX + dx];
+          const C a = K.a27[wclass27(l)];
+          if (dx) px = fm(dx > 0 ? a : -a, ps, px);
+          if (dy) py = fm(dy > 0 ? a : -a, ps, py);
+          pz = fm(a, ps, pz);
+        }
+        collide_recolour(K, gp, rRc, rBc, px, py, pz, Store<S>::shifted, cst);
       }
 #pragma unroll
       for (int l = 0; l < Q; ++l) SPair<S>::st(Bp(l) + 2 * cell, gp[l]);
     }
-    // window slot (z+3)&3 read above is rewritten in iteration z+2; the
-    // barrier of iteration z+1 orders that write after these reads
   }
   if constexpr (ASYNC) cp_async_wait<0>();  // nothing in flight when the shared memory is reused
 }
@@ -645,10 +750,13 @@ __global__ void __launch_bounds__(TX* TY, MINB)
               unsigned long long* err, int64_t step, LeanPart<typename Store<S>::C> PT) {
   extern __shared__ __align__(16) unsigned char lean_smem[];
   using M = LeanSmem<S, TX, TY, PART>;
+  M::init(lean_smem);
+  __syncthreads();
+  unsigned parity = 0;
   const int z0 = blockIdx.z * zlen;
   lean_column<S, TX, TY, PART>(A, B, g, K, blockIdx.x * TX, blockIdx.y * TY, z0, min(z0 + zlen, g.nz), err, step,
                                PT, M::phi(lean_smem), M::stage(lean_smem), M::side(lean_smem),
-                               M::fold(lean_smem));
+                               M::fold(lean_smem), M::bar(lean_smem), parity);
 }
 
 // ---------------------------------------------------------------------------
@@ -677,12 +785,15 @@ __global__ void __launch_bounds__(TX* TY, MINB)
   using C = typename Store<S>::C;
   extern __shared__ __align__(16) unsigned char lean_smem[];
   using M = LeanSmem<S, TX, TY, PART>;
+  M::init(lean_smem);
+  __syncthreads();
+  unsigned parity = 0;
   for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
     const WorkItem it = work[w];
     const BoxDesc<C> bd = boxes[it.box];
     lean_column<S, TX, TY, PART>((const S*)bd.A, (S*)bd.B, bd.g, K, it.x0, it.y0, it.z0, it.zend, bd.err, bd.step,
                                  bd.pt, M::phi(lean_smem), M::stage(lean_smem), M::side(lean_smem),
-                                 M::fold(lean_smem));
+                                 M::fold(lean_smem), M::bar(lean_smem), parity);
     __syncthreads();  // the window is reused by the next item
   }
 }
