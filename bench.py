@@ -161,7 +161,7 @@ def cpu_baseline_sample():
             "sample": f"{n} lattice steps of the 128^3 workload (about 10 s), FP32, OpenMP"}
 
 
-def error_vs_f64(nsteps_list=(1000, 10000)):
+def error_vs_f64(nsteps_list=(100, 1000, 10000)):
     """Relative L2 error of |u| and phi of each storage against the FP64-storage run."""
     from lbcuda_b200 import LBSim, make_params
     from lbcuda_b200.inputs import seeded_noise_fields

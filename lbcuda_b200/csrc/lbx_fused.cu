@@ -152,11 +152,16 @@ template <> struct SPair<__nv_bfloat16> {
   }
 };
 
-// 16-bit storage keeps the pulled pairs of its own cells in shared memory for
-// one iteration (4 bytes a pair); FP32 / FP64 pairs re-read them from L2,
-// which measured faster than a stage of 8 / 16-byte pairs.
-template <typename S>
-constexpr bool kStage = sizeof(typename SPair<S>::R) == 4;
+// Which pulls land in shared memory by cp.async ("staged"): the 4-byte pairs
+// of 16-bit storage.  FP32 and FP64 pull synchronously and re-read the pairs
+// from L2 for the collision: a two-deep FP32 stage (109 KB per CTA, issued
+// once the collision has read a plane's pairs) measured 0.235 ms at 128^3
+// against 0.156 ms without it.  Own-cell pairs are 3 planes deep: plane z+2
+// is copied at the top of iteration z.
+template <typename S, bool PART>
+constexpr bool kStaged = sizeof(typename SPair<S>::R) == 4;
+template <typename S, bool PART>
+constexpr int kDepth = 3;
 
 // element offset of direction l (both components) of a cell: 2 (l n + cell)
 __device__ __forceinline__ size_t poff(int64_t n, int l, int cell) { return (size_t(l) * size_t(n) + size_t(cell)) * 2; }
@@ -223,10 +228,13 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long* m, unsigned parity
 template <typename S>
 __device__ __forceinline__ void pull_async(const S* __restrict__ A, int64_t n, const PullIdx& P,
                                            typename SPair<S>::R* st, int stride) {
-  static_assert(sizeof(typename SPair<S>::R) == 4, "4-byte pairs");
+  static_assert(sizeof(typename SPair<S>::R) == 4 || sizeof(typename SPair<S>::R) == 8, "4- or 8-byte pairs");
   const Planes<const S> Ap{A, 2 * n};
 #pragma unroll
-  for (int l = 0; l < Q; ++l) cp_async4(st + l * stride, Ap(l) + 2 * P.src[l]);
+  for (int l = 0; l < Q; ++l) {
+    if constexpr (sizeof(typename SPair<S>::R) == 4) cp_async4(st + l * stride, Ap(l) + 2 * P.src[l]);
+    else cp_async8(st + l * stride, Ap(l) + 2 * P.src[l]);
+  }
 }
 
 // densities (Sum g + rho0, before the clamp) from pairs already in shared memory
@@ -323,18 +331,19 @@ __device__ __forceinline__ CollideState<C> collide_bgk(const LeanConst<C>& K, P2
   const C v = inv * (d[2] + d[4] + d[5] + d[8] - d[9]);
   const C w = inv * (d[3] + d[6] + d[7] + d[8] + d[9]);
   const C c0 = fm(C(-1.5), fm(u, u, fm(v, v, w * w)), ONE);
-  P2<C> Kc[3], ns[3];
+  P2<C> Kc[3], os[3];
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
     Kc[k] = pp(omega * rR * K.w[k], omega * rB * K.w[k]);  // omega rho_k w
-    ns[k] = pp(-K.s[0][k], -K.s[1][k]);                      // minus the shift
+    os[k] = pp(-omega * K.s[0][k], -omega * K.s[1][k]);     // -omega times the shift
   }
   const P2<C> omm2 = pp(omm, omm);
-  // BGK: f' = f (1 - omega) + omega rho w A(u),  f = g + s
-  {
-    const P2<C> f = shifted ? p_fma(ns[0], NEG, g[0]) : g[0];
-    g[0] = p_fma(f, omm2, p_mul(Kc[0], pp(c0, c0)));
-  }
+  // BGK: f' = f (1 - omega) + omega rho w A(u).  Stored form g = f - s stays
+  // stored: g' = g (1 - omega) + omega rho w A(u) - omega s.
+  auto relax = [&](const P2<C>& gl, const P2<C>& kc, C a, const P2<C>& o) {
+    return shifted ? p_fma(gl, omm2, p_fma(kc, pp(a, a), o)) : p_fma(gl, omm2, p_mul(kc, pp(a, a)));
+  };
+  g[0] = relax(g[0], Kc[0], c0, os[0]);
 #pragma unroll
   for (int p = 1; p <= 9; ++p) {
     const int l = 2 * p - 1, o = 2 * p, k = wclass(l);
@@ -342,10 +351,8 @@ __device__ __forceinline__ CollideState<C> collide_bgk(const LeanConst<C>& K, P2
     const C P = fm(C(4.5) * eu, eu, c0);
     const C Qv = C(3) * eu;
     const C Ap = P + Qv, Am = P - Qv;
-    const P2<C> fl = shifted ? p_fma(ns[k], NEG, g[l]) : g[l];
-    const P2<C> fo = shifted ? p_fma(ns[k], NEG, g[o]) : g[o];
-    g[l] = p_fma(fl, omm2, p_mul(Kc[k], pp(Ap, Ap)));
-    g[o] = p_fma(fo, omm2, p_mul(Kc[k], pp(Am, Am)));
+    g[l] = relax(g[l], Kc[k], Ap, os[k]);
+    g[o] = relax(g[o], Kc[k], Am, os[k]);
   }
   return CollideState<C>{omega, inv};
 }
@@ -354,9 +361,14 @@ template <typename C>
 __device__ __forceinline__ void collide_recolour(const LeanConst<C>& K, P2<C> g[Q], C rR, C rB, C px, C py, C pz,
                                                  bool shifted, CollideState<C> cs) {
   const C omega = cs.omega, inv = cs.inv;
+  // g holds the relaxed populations in stored form; f_R + f_B = g_R + g_B + ss
   P2<C> ns[3];
+  C ss[3];
 #pragma unroll
-  for (int k = 0; k < 3; ++k) ns[k] = pp(-K.s[0][k], -K.s[1][k]);  // minus the shift
+  for (int k = 0; k < 3; ++k) {
+    ns[k] = pp(-K.s[0][k], -K.s[1][k]);  // minus the shift
+    ss[k] = K.s[0][k] + K.s[1][k];
+  }
   const C psq = fm(px, px, fm(py, py, pz * pz));
   if (psq > C(1.e-20)) {
     const C ipn = rsqrt_c(psq);
@@ -374,29 +386,22 @@ __device__ __forceinline__ void collide_recolour(const LeanConst<C>& K, P2<C> g[
     K3[1] = coef * K.w[1];
     K3[2] = coef * K.w[2] / K.sqrt2;
     {
-      const C fd = g[0].x + g[0].y - K0[0];
+      const C fd = g[0].x + g[0].y + (ss[0] - K0[0]);
       g[0] = p_fma(pp(fd, fd), kk, ns[0]);
     }
 #pragma unroll
     for (int p = 1; p <= 9; ++p) {
       const int l = 2 * p - 1, o = 2 * p, k = wclass(l);
       const C ed = edot(l, px, py, pz);
-      const C pert = fm(K1[k], ed * ed, -K0[k]);
+      const C pert = fm(K1[k], ed * ed, ss[k] - K0[k]);
       const C T = K3[k] * ed;
       const C fdp = g[l].x + g[l].y + pert;
       const C fdm = g[o].x + g[o].y + pert;
       g[l] = p_fma(pp(fdp, fdp), kk, p_add(pp(T, -T), ns[k]));
       g[o] = p_fma(pp(fdm, fdm), kk, p_add(pp(-T, T), ns[k]));
     }
-  } else if (shifted) {
-    g[0] = p_add(g[0], ns[0]);
-#pragma unroll
-    for (int p = 1; p <= 9; ++p) {
-      const int k = wclass(2 * p - 1);
-      g[2 * p - 1] = p_add(g[2 * p - 1], ns[k]);
-      g[2 * p] = p_add(g[2 * p], ns[k]);
-    }
   }
+  // without a colour gradient the relaxed populations are the result
 }
 
 template <typename C>
@@ -454,9 +459,10 @@ struct LeanSmem {
   using R = typename SPair<S>::R;
   static constexpr int NT = TX * TY, RN = Ring<TX, TY>::N, CELLS = Ring<TX, TY>::CELLS;
   static constexpr size_t PHI = sizeof(C) * 4 * CELLS;
-  static constexpr size_t OWN = kStage<S> ? sizeof(R) * 3 * Q * NT : 0;
-  static constexpr size_t RING = kStage<S> ? sizeof(R) * 2 * Q * RN : 0;
-  static constexpr size_t SIDE = PART ? (sizeof(SideRec<C>) * (3 * NT + 2 * RN) + 15) / 16 * 16 : 0;
+  static constexpr int D = kDepth<S, PART>;
+  static constexpr size_t OWN = kStaged<S, PART> ? sizeof(R) * D * Q * NT : 0;
+  static constexpr size_t RING = kStaged<S, PART> ? sizeof(R) * 2 * Q * RN : 0;
+  static constexpr size_t SIDE = PART ? (sizeof(SideRec<C>) * (D * NT + 2 * RN) + 15) / 16 * 16 : 0;
   static constexpr size_t FOLD = PART ? (4 * CELLS + 15) / 16 * 16 : 0;
   static constexpr size_t BAR = 16;  // the plane's split barrier
   static constexpr size_t BYTES = PHI + OWN + RING + SIDE + FOLD + BAR;
@@ -465,7 +471,7 @@ struct LeanSmem {
     return reinterpret_cast<C(*)[CELLS]>(base);
   }
   static __device__ __forceinline__ R* stage(unsigned char* base) {
-    return kStage<S> ? reinterpret_cast<R*>(base + PHI) : nullptr;
+    return kStaged<S, PART> ? reinterpret_cast<R*>(base + PHI) : nullptr;
   }
   static __device__ __forceinline__ SideRec<C>* side(unsigned char* base) {
     return PART ? reinterpret_cast<SideRec<C>*>(base + PHI + OWN + RING) : nullptr;
@@ -512,14 +518,16 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
 
   using SR = typename SPair<S>::R;
   constexpr int RN = R::N;
-  constexpr bool ASYNC = kStage<S> || PART;  // copy groups in flight
-  SR* const ring_stage = kStage<S> ? stage + 3 * Q * NT : nullptr;
-  SideRec<C>* const side_ring = PART ? side + 3 * NT : nullptr;
+  constexpr bool STAGED = kStaged<S, PART>;
+  constexpr int D = kDepth<S, PART>;
+  constexpr bool ASYNC = STAGED || PART;  // copy groups in flight
+  SR* const ring_stage = STAGED ? stage + D * Q * NT : nullptr;
+  SideRec<C>* const side_ring = PART ? side + D * NT : nullptr;
   const Planes<const S> Ap{A, 2 * g.n};
   const Planes<S> Bp{B, 2 * g.n};
 
-  // slots of plane p (p >= z0 - 1): own cells 3 deep, ring cells 2 deep
-  auto own_q = [&](int p) { return (p - z0 + 1) % 3; };
+  // slots of plane p (p >= z0 - 1): own cells D deep, ring cells 2 deep
+  auto own_q = [&](int p) { return (p - z0 + 1) % D; };
   auto ring_q = [&](int p) { return (p - z0 + 1) & 1; };
   auto own_slot = [&](int p) { return stage + own_q(p) * (Q * NT) + tid; };
   auto ring_slot = [&](int p) { return ring_stage + ring_q(p) * (Q * RN) + tid; };
@@ -545,7 +553,7 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
         }
       }
     }
-    if constexpr (kStage<S>) {
+    if constexpr (STAGED) {
       PullIdx P;
       pull_idx(g, x, y, zz, P);
       pull_async<S>(A, g.n, P, own_slot(p), NT);
@@ -595,7 +603,7 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
         }
       }
     }
-    if constexpr (kStage<S>) {
+    if constexpr (STAGED) {
       stage_rho<S, C>(st, stride, K, rR, rB);
     } else {
       PullIdx P;
@@ -615,7 +623,7 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
     const int zz = wrap0(p, g.nz);
     const bool owned = active && p >= z0 && p < zend;
     const SideRec<C>* so = PART ? side + own_q(p) * NT + tid : nullptr;
-    sphi[p & 3][own] = cell_phase(x, y, zz, owned, true, kStage<S> ? own_slot(p) : nullptr, NT, so, rRo, rBo);
+    sphi[p & 3][own] = cell_phase(x, y, zz, owned, true, STAGED ? own_slot(p) : nullptr, NT, so, rRo, rBo);
     if constexpr (PART) {
       if (parts) {
         int8_t fn, fo;
@@ -627,7 +635,7 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
       C qR, qB;
       const SideRec<C>* sr = PART ? side_ring + ring_q(p) * RN + tid : nullptr;
       sphi[p & 3][rslot] =
-          cell_phase(rxg, ryg, zz, false, false, kStage<S> ? ring_slot(p) : nullptr, RN, sr, qR, qB);
+          cell_phase(rxg, ryg, zz, false, false, STAGED ? ring_slot(p) : nullptr, RN, sr, qR, qB);
       if constexpr (PART) {
         if (parts) {
           int8_t fn, fo;
@@ -650,8 +658,8 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
   for (int z = z0; z < zend; ++z) {
     rRc = rRn;
     rBc = rBn;
-    // plane z+2 is copied while z+1 is summed and z collided; the copies into
-    // the slots of plane z-1 start after this thread's last read of them
+    // plane z+2 is copied while z+1 is summed and z collided; the copies
+    // into the slots of plane z-1 start after this thread's last read of them
     if (z + 2 <= zend) issue(z + 2);
     else if constexpr (ASYNC) cp_async_commit();  // one group per iteration
     settle();
@@ -670,7 +678,7 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
       pull_idx(g, x, y, z, P);
       // the pull every fluid cell needs: in the stage since two iterations,
       // or issued here
-      if constexpr (kStage<S>) {
+      if constexpr (STAGED) {
         const SR* sg = own_slot(z);
 #pragma unroll
         for (int l = 0; l < Q; ++l) gp[l] = SPair<S>::cvt(sg[l * NT]);
@@ -678,6 +686,8 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
 #pragma unroll
         for (int l = 0; l < Q; ++l) gp[l] = SPair<S>::ld(Ap(l) + 2 * P.src[l]);
       }
+    }
+    if (active) {
       if constexpr (PART) {
         if (parts) {
           int8_t fn, fo;

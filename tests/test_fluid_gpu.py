@@ -170,12 +170,13 @@ def test_equilibrium_and_uniform_flow_are_fixed_points():
         assert np.abs(vel - np.array([0.05, -0.02, 0.03])).max() < tol * 0.05 + 1e-7, storage
 
 
-@pytest.mark.parametrize("storage,tol", [("f32", 1e-6), ("f16", 1e-6), ("bf16", 1e-6), ("f64", 1e-12)])
+@pytest.mark.parametrize("storage,tol", [("f32", 1e-6), ("f16", 1e-6), ("bf16", 8e-6), ("f64", 1e-12)])
 def test_mass_conservation_full_size(storage, tol):
     """128^3 spinodal: FP64 sums of each component's mass are conserved by the step.
 
-    The 16-bit storages round each population, so their check compares the
-    FP64 sum after a step with the FP64 sum of the rounded state before it.
+    The arithmetic conserves mass; what drifts is the rounding of every stored
+    population, accumulated over the 50 steps.  BF16 keeps 8 significant bits
+    against FP16's 11, so its bound is 8 times FP16's.
     """
     n = 128
     p = make_params(n, model="cg", storage=storage, sigma=0.02, beta=0.7)
