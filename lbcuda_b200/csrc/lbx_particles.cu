@@ -497,9 +497,13 @@ __global__ void __launch_bounds__(256) k_rho_shell(PDev P, const double* __restr
     }
     const int i1 = wrap1(c0[0] + dx, g.nx), j1 = wrap1(c0[1] + dy, g.ny), k1 = wrap1(c0[2] + dz, g.nz);
     const int y = cell0(g, i1, j1, k1);
-    if (fnew[y] != LBX_FLUID_FLUID || fold[y] != LBX_FLUID_FLUID) continue;
+    // outside the sphere's own template the cell is nearly always fluid: the
+    // flags and the pull are loaded together, the pull dropped if unused
+    const int8_t fn = fnew[y], fo = fold[y];
+    if (tv != LBX_FLUID_FLUID && (fn != LBX_FLUID_FLUID || fo != LBX_FLUID_FLUID)) continue;
     C rR, rB;
     pulled_rho(A, g, sh, i1, j1, k1, rR, rB);
+    if (fn != LBX_FLUID_FLUID || fo != LBX_FLUID_FLUID) continue;
     rhoR[y] = rR;
     rhoB[y] = rB;
   }
@@ -775,16 +779,30 @@ __global__ void __launch_bounds__(256) k_bb(PDev P, const double* __restrict__ p
     unpack_off(P.offs_bb[t], dx, dy, dz, tv);
     if (!offset_cell(P, g, c, dx, dy, dz, i1, j1, k1)) continue;
     const int cell = cell0(g, i1, j1, k1);
-    if (fnew[cell] != LBX_FLUID_SPHERELIST) continue;
     const int x0 = i1 - 1, y0 = j1 - 1, z0 = k1 - 1;
+    Nbr b;
+    make_nbr(g, x0, y0, z0, b);
+    // bit l: neighbour l is fluid.  For the sphere's own surface offsets (a
+    // surface cell nearly always) the neighbours' flags are loaded together
+    // with the cell's flag and owner; for the other offsets only if needed.
+    auto nbr_fluid = [&]() {
+      unsigned m = 0;
+#pragma unroll
+      for (int l = 1; l < Q; ++l) m |= unsigned(fnew[at(b, ex(l), ey(l), ez(l))] == LBX_FLUID_FLUID) << l;
+      return m;
+    };
+    const bool likely = tv == LBX_FLUID_SPHERELIST;
+    const int8_t fc = fnew[cell];
+    const int ow = P.owner[cell];
+    unsigned fl = likely ? nbr_fluid() : 0u;
+    if (fc != LBX_FLUID_SPHERELIST) continue;
     const int ti = x0 / TILEX + 1, tj = y0 / TILEY + 1, tk = z0 / TILEZ + 1;
     // node -> particle momentum exchange for this sphere (atmDist < sphereMax)
     const bool n2p = (mode & BB_N2P) && dx * dx + dy * dy + dz * dz < P.sphereMax &&
                      (!P.exact_tiles || tile_covered(pc, nn3, P.rdim, ti, tj, tk));
-    const bool own = (mode & (BB_COPY | BB_WALL)) && P.owner[cell] == a;
+    const bool own = (mode & (BB_COPY | BB_WALL)) && ow == a;
     if (!n2p && !own) continue;
-    Nbr b;
-    make_nbr(g, x0, y0, z0, b);
+    if (!likely) fl = nbr_fluid();
     // link pair it = (lo, hi) = (2it+1, 2it+2) crosses when exactly one end is
     // fluid; hib: the fluid end is hi (then lf = lo, lr = hi), else lo
     int xf[9];
@@ -793,7 +811,7 @@ __global__ void __launch_bounds__(256) k_bb(PDev P, const double* __restrict__ p
     for (int it = 0; it < 9; ++it) {
       const int lo = 2 * it + 1, hi = 2 * it + 2;
       const int xi = at(b, ex(lo), ey(lo), ez(lo)), xo = at(b, ex(hi), ey(hi), ez(hi));
-      const bool fi = fnew[xi] == LBX_FLUID_FLUID, fo = fnew[xo] == LBX_FLUID_FLUID;
+      const bool fi = (fl >> lo) & 1u, fo = (fl >> hi) & 1u;
       xf[it] = fo ? xo : xi;
       act |= unsigned(fi != fo) << it;
       hib |= unsigned(fo) << it;
@@ -1344,10 +1362,15 @@ int particles_create(Ctx& c) {
   s->shell_r2 = int(std::floor(rs * rs));
   const int RS = int(std::ceil(rs));
   if (RS > 60) return LBX_ERR_ARG;  // offsets are packed in 8 bits
+  // (each with its template value: solid template cells are fluid only when
+  // the tile-list coverage left them out, so they are tested before pulling)
   for (int k = -RS; k <= RS; ++k)
     for (int j = -RS; j <= RS; ++j)
       for (int i = -RS; i <= RS; ++i)
-        if (i * i + j * j + k * k <= s->shell_r2) offs.push_back(pack_off(i, j, k, 0));
+        if (i * i + j * j + k * k <= s->shell_r2) {
+          const bool in_box = std::abs(i) <= R && std::abs(j) <= R && std::abs(k) <= R;
+          offs.push_back(pack_off(i, j, k, in_box ? tv(i, j, k) : LBX_FLUID_FLUID));
+        }
   s->n_shell = int(offs.size()) - s->n_solid - s->n_bb;
   if (!ok(cudaMalloc(&s->offs, offs.size() * 4))) return LBX_ERR_ALLOC;
   cudaMemcpyAsync(s->offs, offs.data(), offs.size() * 4, cudaMemcpyHostToDevice, c.stream);
