@@ -445,8 +445,7 @@ struct LeanPart {
 // The particle variant adds, per own / ring cell and plane, the side record
 // copied with the pulls: the 4-byte words holding the cell's flag of this and
 // of the previous step, and the phase field the wetting / fill kernels wrote
-// for it (3 planes deep for own cells, 2 for ring cells), and a 4-plane window
-// of previous-step flags of the column and its ring (spheredead sources).
+// for it (3 planes deep for own cells, 2 for ring cells).
 template <typename C>
 struct SideRec {
   unsigned fnew_w, fold_w;  // aligned words containing the cell's flags
@@ -463,9 +462,8 @@ struct LeanSmem {
   static constexpr size_t OWN = kStaged<S, PART> ? sizeof(R) * D * Q * NT : 0;
   static constexpr size_t RING = kStaged<S, PART> ? sizeof(R) * 2 * Q * RN : 0;
   static constexpr size_t SIDE = PART ? (sizeof(SideRec<C>) * (D * NT + 2 * RN) + 15) / 16 * 16 : 0;
-  static constexpr size_t FOLD = PART ? (4 * CELLS + 15) / 16 * 16 : 0;
   static constexpr size_t BAR = 16;  // the plane's split barrier
-  static constexpr size_t BYTES = PHI + OWN + RING + SIDE + FOLD + BAR;
+  static constexpr size_t BYTES = PHI + OWN + RING + SIDE + BAR;
   static_assert(PHI % 16 == 0 && OWN % 16 == 0 && RING % 16 == 0, "stage alignment");
   static __device__ __forceinline__ C (*phi(unsigned char* base))[CELLS] {
     return reinterpret_cast<C(*)[CELLS]>(base);
@@ -476,11 +474,8 @@ struct LeanSmem {
   static __device__ __forceinline__ SideRec<C>* side(unsigned char* base) {
     return PART ? reinterpret_cast<SideRec<C>*>(base + PHI + OWN + RING) : nullptr;
   }
-  static __device__ __forceinline__ int8_t (*fold(unsigned char* base))[CELLS] {
-    return PART ? reinterpret_cast<int8_t(*)[CELLS]>(base + PHI + OWN + RING + SIDE) : nullptr;
-  }
   static __device__ __forceinline__ unsigned long long* bar(unsigned char* base) {
-    return reinterpret_cast<unsigned long long*>(base + PHI + OWN + RING + SIDE + FOLD);
+    return reinterpret_cast<unsigned long long*>(base + PHI + OWN + RING + SIDE);
   }
   // thread 0 sets up the barrier for the CTA's threads; the caller then syncs
   static __device__ __forceinline__ void init(unsigned char* base) {
@@ -496,7 +491,7 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
                                             const LeanPart<typename Store<S>::C>& PT,
                                             typename Store<S>::C (*sphi)[Ring<TX, TY>::CELLS],
                                             typename SPair<S>::R* stage, SideRec<typename Store<S>::C>* side,
-                                            int8_t (*sfold)[Ring<TX, TY>::CELLS], unsigned long long* bar,
+                                            unsigned long long* bar,
                                             unsigned& bar_parity) {
   using C = typename Store<S>::C;
   constexpr int NT = TX * TY;
@@ -617,32 +612,17 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
     return phase_of(rR, rB);
   };
 
-  // phase field of plane p (own cell and ring cell) into its window slot, and
-  // with spheres the previous-step flags into the flag window
+  // phase field of plane p (own cell and ring cell) into its window slot
   auto phase_plane = [&](int p, C& rRo, C& rBo) {
     const int zz = wrap0(p, g.nz);
     const bool owned = active && p >= z0 && p < zend;
     const SideRec<C>* so = PART ? side + own_q(p) * NT + tid : nullptr;
     sphi[p & 3][own] = cell_phase(x, y, zz, owned, true, STAGED ? own_slot(p) : nullptr, NT, so, rRo, rBo);
-    if constexpr (PART) {
-      if (parts) {
-        int8_t fn, fo;
-        flags_of(so, x + g.nx * (y + g.ny * zz), fn, fo);
-        sfold[p & 3][own] = fo;
-      }
-    }
     if (ringer) {
       C qR, qB;
       const SideRec<C>* sr = PART ? side_ring + ring_q(p) * RN + tid : nullptr;
       sphi[p & 3][rslot] =
           cell_phase(rxg, ryg, zz, false, false, STAGED ? ring_slot(p) : nullptr, RN, sr, qR, qB);
-      if constexpr (PART) {
-        if (parts) {
-          int8_t fn, fo;
-          flags_of(sr, rxg + g.nx * (ryg + g.ny * zz), fn, fo);
-          sfold[p & 3][rslot] = fo;
-        }
-      }
     }
   };
 
@@ -670,7 +650,7 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
     // and their slots are rewritten only after this plane's barrier.
     const int cell = x + g.nx * (y + g.ny * z);
     P2<C> gp[Q];
-    bool collide = true, solid = false;
+    bool collide = true;
     C px = 0, py = 0, pz = 0;
     CollideState<C> cst{C(0), C(0)};
     PullIdx P;
@@ -692,8 +672,8 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
         if (parts) {
           int8_t fn, fo;
           flags_of(side + own_q(z) * NT + tid, cell, fn, fo);
+          // a solid cell keeps the plain pull (see below)
           collide = fn == LBX_FLUID_FLUID;
-          solid = !collide;
           if (collide && fo != LBX_FLUID_FLUID) {
             // make_fluid already wrote the new node's populations (stored form) into B
 #pragma unroll
@@ -722,17 +702,12 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
     if (!mbar_wait(bar, bar_parity)) raise_error(err, LBX_DEV_WAIT_TIMEOUT, step, -1);
     bar_parity ^= 1u;
     if (active) {
-      if constexpr (PART) {
-        if (solid) {
-          // solid cell: streamed populations only; a spheredead source
-          // (previous step, from the flag window) leaves the destination's
-          // stale value, which is B's entry
-#pragma unroll
-          for (int l = 1; l < Q; ++l)
-            if (sfold[(z - ez(l)) & 3][own - ey(l) * R::RX - ex(l)] == LBX_FLUID_SPHEREDEAD)
-              gp[l] = SPair<S>::ld(Bp(l) + 2 * cell);
-        }
-      }
+      // A solid cell stores its streamed populations as pulled.  The
+      // reference's push leaves a stale value behind a spheredead source
+      // instead; no fluid cell, force or moment ever reads a solid cell's
+      // populations (a fluid cell pulls from a solid one only along a link
+      // the bounce-back rewrote, and a cell that turns fluid is refilled), so
+      // only raw population dumps of solid cells differ.
       if (collide) {
         const C* ppl = sphi[(z + 1) & 3];
 #pragma unroll
@@ -766,7 +741,7 @@ __global__ void __launch_bounds__(TX* TY, MINB)
   const int z0 = blockIdx.z * zlen;
   lean_column<S, TX, TY, PART>(A, B, g, K, blockIdx.x * TX, blockIdx.y * TY, z0, min(z0 + zlen, g.nz), err, step,
                                PT, M::phi(lean_smem), M::stage(lean_smem), M::side(lean_smem),
-                               M::fold(lean_smem), M::bar(lean_smem), parity);
+                               M::bar(lean_smem), parity);
 }
 
 // ---------------------------------------------------------------------------
@@ -803,7 +778,7 @@ __global__ void __launch_bounds__(TX* TY, MINB)
     const BoxDesc<C> bd = boxes[it.box];
     lean_column<S, TX, TY, PART>((const S*)bd.A, (S*)bd.B, bd.g, K, it.x0, it.y0, it.z0, it.zend, bd.err, bd.step,
                                  bd.pt, M::phi(lean_smem), M::stage(lean_smem), M::side(lean_smem),
-                                 M::fold(lean_smem), M::bar(lean_smem), parity);
+                                 M::bar(lean_smem), parity);
     __syncthreads();  // the window is reused by the next item
   }
 }
