@@ -232,31 +232,35 @@ __device__ void block_sum(double v[NV], double* out /* NV, added */) {
 // ---------------------------------------------------------------------------
 // kernels
 // ---------------------------------------------------------------------------
-__global__ void k_bins(PDev P, const double* __restrict__ pos, Geom g, unsigned long long* err, int64_t step) {
-  int a = blockIdx.x * blockDim.x + threadIdx.x;
+// one warp per sphere: the distinct bins its box c - rmax .. c + rmax touches
+// along each axis (periodic; at most (2 rmax + 1) / BINW + 2 <= 17 for the
+// radii the 8-bit offset lists allow), then one list entry per bin triple,
+// spread over the lanes
+constexpr int MAXB = 20;
+__global__ void __launch_bounds__(256) k_bins(PDev P, const double* __restrict__ pos, Geom g,
+                                              unsigned long long* err, int64_t step) {
+  const int a = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
   if (a >= P.np) return;
   const double* p = pos + size_t(a) * PS;
   const int c[3] = {nint_idx(p[0], g.nx), nint_idx(p[1], g.ny), nint_idx(p[2], g.nz)};
   const int n[3] = {g.nx, g.ny, g.nz};
   const int nb[3] = {P.nbx, P.nby, P.nbz};
-  // distinct bins hit by the cells c - rmax .. c + rmax of each axis (periodic)
-  int bl[3][4], nbl[3] = {0, 0, 0};
+  int bl[3][MAXB], nbl[3] = {0, 0, 0};
   for (int d = 0; d < 3; ++d)
     for (int u = c[d] - P.rmax; u <= c[d] + P.rmax; ++u) {
       int bin = (wrap1(u, n[d]) - 1) / BINW;
       bool seen = false;
       for (int k = 0; k < nbl[d]; ++k) seen |= (bl[d][k] == bin);
-      if (!seen && nbl[d] < 4) bl[d][nbl[d]++] = bin;
-      (void)nb;
+      if (!seen && nbl[d] < MAXB) bl[d][nbl[d]++] = bin;
     }
-  for (int bk = 0; bk < nbl[2]; ++bk)
-    for (int bj = 0; bj < nbl[1]; ++bj)
-      for (int bi = 0; bi < nbl[0]; ++bi) {
-        int bin = bl[0][bi] + nb[0] * (bl[1][bj] + nb[1] * bl[2][bk]);
-        int slot = atomicAdd(P.bin_cnt + bin, 1);
-        if (slot < BIN_CAP) P.bin_list[size_t(bin) * BIN_CAP + slot] = a;
-        else raise_error(err, LBX_DEV_LIST_OVERFLOW, step, a);
-      }
+  const int total = nbl[0] * nbl[1] * nbl[2];
+  for (int t = lane; t < total; t += 32) {
+    const int bi = t % nbl[0], bj = (t / nbl[0]) % nbl[1], bk = t / (nbl[0] * nbl[1]);
+    const int bin = bl[0][bi] + nb[0] * (bl[1][bj] + nb[1] * bl[2][bk]);
+    const int slot = atomicAdd(P.bin_cnt + bin, 1);
+    if (slot < BIN_CAP) P.bin_list[size_t(bin) * BIN_CAP + slot] = a;
+    else raise_error(err, LBX_DEV_LIST_OVERFLOW, step, a);
+  }
 }
 
 // ascending particle order inside each bin (the first-match rules below then
@@ -309,6 +313,25 @@ __global__ void __launch_bounds__(256) k_stamp_flags(PDev P, const double* __res
     if (!offset_cell(P, g, c, dx, dy, dz, i1, j1, k1)) continue;
     const int cell = cell0(g, i1, j1, k1);
     if (P.owner[cell] == a) flags_new[cell] = int8_t(v);
+  }
+}
+
+// Undo a stamping: every solid template cell of the spheres at `pos` back to
+// fluid (flags) and to no owner.  Flags and owners are otherwise fluid / -1,
+// so clearing what the last stamping at these positions touched restores the
+// whole array without a full pass over the lattice.
+__global__ void __launch_bounds__(256) k_unstamp(PDev P, const double* __restrict__ pos, Geom g, int8_t* flags,
+                                                 int* owner) {
+  const int a = blockIdx.x;
+  const double* p = pos + size_t(a) * PS;
+  const int c[3] = {nint_idx(p[0], g.nx), nint_idx(p[1], g.ny), nint_idx(p[2], g.nz)};
+  for (int t = threadIdx.x; t < P.n_solid; t += blockDim.x) {
+    int dx, dy, dz, v, i1, j1, k1;
+    unpack_off(P.offs[t], dx, dy, dz, v);
+    if (!offset_cell(P, g, c, dx, dy, dz, i1, j1, k1)) continue;
+    const int cell = cell0(g, i1, j1, k1);
+    if (flags) flags[cell] = LBX_FLUID_FLUID;
+    if (owner) owner[cell] = -1;
   }
 }
 
@@ -1415,18 +1438,25 @@ static int rebuild_bins(Ctx& c, const double* pos) {
   Geom g = geom(c);
   size_t nbins = size_t(s.nbx) * s.nby * s.nbz;
   cudaMemsetAsync(s.bin_cnt, 0, nbins * 4, c.stream);
-  k_bins<<<(s.np + 127) / 128, 128, 0, c.stream>>>(P, pos, g, c.d_err, c.step + 1);
+  k_bins<<<(s.np * 32 + 255) / 256, 256, 0, c.stream>>>(P, pos, g, c.d_err, c.step + 1);
   k_bins_sort<<<int((nbins + 255) / 256), 256, 0, c.stream>>>(P, int(nbins));
   return launch_status();
 }
 
 // flags and owners of the spheres at `pos` (every other cell fluid, no owner)
-static int compute_flags(Ctx& c, const double* pos, int8_t* flags) {
+//   prev: positions of the last stamping of the owners (nullptr: clear the
+//   whole owner and flag arrays).  Otherwise `flags` must already be all
+//   fluid, which the end of the step before guarantees (k_unstamp).
+static int compute_flags(Ctx& c, const double* pos, int8_t* flags, const double* prev) {
   ParticleState& s = *c.part;
-  cudaMemsetAsync(flags, LBX_FLUID_FLUID, size_t(c.n), c.stream);
-  cudaMemsetAsync(s.owner, 0xFF, size_t(c.n) * 4, c.stream);
   PDev P = pdev(c);
   Geom g = geom(c);
+  if (prev) {
+    k_unstamp<<<s.np, 256, 0, c.stream>>>(P, prev, g, nullptr, s.owner);
+  } else {
+    cudaMemsetAsync(flags, LBX_FLUID_FLUID, size_t(c.n), c.stream);
+    cudaMemsetAsync(s.owner, 0xFF, size_t(c.n) * 4, c.stream);
+  }
   k_stamp<<<s.np, 256, 0, c.stream>>>(P, pos, g);
   k_stamp_flags<<<s.np, 256, 0, c.stream>>>(P, pos, g, flags);
   return launch_status();
@@ -1464,7 +1494,9 @@ int particles_set(Ctx& c, int n, const double* h_x, const double* h_v, const dou
   int slot = 1 - c.fcur;
   int rc = rebuild_bins(c, s->pos[0]);
   if (rc) return rc;
-  rc = compute_flags(c, s->pos[0], c.flags[slot]);
+  // both flag slots all fluid (the step-0 flags go into `slot`)
+  cudaMemsetAsync(c.flags[1 - slot], LBX_FLUID_FLUID, size_t(c.n), c.stream);
+  rc = compute_flags(c, s->pos[0], c.flags[slot], nullptr);
   s->flags_last = slot;
   if (!rc) rc = cudaStreamSynchronize(c.stream) == cudaSuccess ? 0 : LBX_ERR_CUDA;
   return rc;
@@ -1500,7 +1532,7 @@ int part_lists(Ctx& c) {
 
 int part_flags(Ctx& c) {
   Stage t(c);
-  return compute_flags(c, t.pc, c.flags[t.fn]);
+  return compute_flags(c, t.pc, c.flags[t.fn], t.po);
 }
 
 int part_drain(Ctx& c) {
@@ -1628,6 +1660,9 @@ int part_pairs(Ctx& c) {
 int part_integrate(Ctx& c) {
   Stage t(c);
   ParticleState& s = t.s;
+  // the previous step's flags (stamped at the previous positions) are not
+  // read again: clear them, so that the next step stamps into a fluid slot
+  k_unstamp<<<s.np, 256, 0, c.stream>>>(t.P, t.po, t.g, c.flags[t.fo], nullptr);
   k_integrate<<<(s.np + 127) / 128, 128, 0, c.stream>>>(t.P, t.pc, s.pos[1 - s.pcur], s.frc[s.pcur],
                                                         s.frc[1 - s.pcur], s.acc, t.g, c.d_err, t.st);
   int rc = launch_status();

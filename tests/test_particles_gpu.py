@@ -174,3 +174,19 @@ def test_kernel_level_entries_equal_step(sched):
     for k in da:
         assert np.array_equal(da[k], db[k]), k
     assert (np.rint(da["x"]) != np.rint(x)).any()   # a sphere changed cell: drain and fill ran
+
+
+def test_large_radius_spans_five_bins():
+    """r = 12.5: a sphere's box (27 cells) touches five 8-cell bins per axis; flags bit-exact and the
+    moving sphere's force and torque as in the oracle."""
+    x = np.array([[20.3, 21.1, 19.6]])
+    v = np.array([[0.02, -0.01, 0.015]])
+    om = np.array([[0.0, 0.004, -0.003]])
+    rR, rB = seeded_noise_fields(64, 64, 64, seed=8)
+    g, o = make_pair(64, x, v, om, steps=6, fields=(rR, rB), radius=12.5, lrotate=1, wetting="neutral",
+                     sigma=0.02, beta=0.7, rmass=1e-4)
+    assert g.status()[0] == 0 and o.status()[0] == 0
+    assert np.array_equal(g.get_flags(), o.get_flags())
+    gp, op = g.get_particles(), o.get_particles()
+    assert rel(gp["force"], op["force"]) < 1e-5
+    assert rel(gp["torque"], op["torque"]) < 1e-5
