@@ -102,6 +102,16 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def max_over_ranks(v, pg, device):
+    """The largest of every rank's value (timings are reported as the slowest rank's)."""
+    if pg is None:
+        return v
+    import torch
+    t = torch.tensor([float(v)], dtype=torch.float64, device=device)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
 def dist_env():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -438,11 +448,7 @@ def main():
     tot32, k32, n32, _, code32 = run_storage("f32", args.steps, args.warmup)
 
     def maxr(v):
-        if pg is None:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        return float(t.item())
+        return max_over_ranks(v, pg, "cuda")
 
     tot16, tot32 = maxr(tot16), maxr(tot32)
     cells = L ** 3
