@@ -1,23 +1,30 @@
 // lbx_fused.cu — single-pass colour-gradient step (time_step_CG + streaming,
 // kernels_fluid_CG.CUF:531-1141) for sm_100a, written for instruction
-// economy: the collision of the two components shares the velocity factors
-// of the equilibrium, opposite directions are processed as pairs (e_opp =
-// -e_l, so every odd power of e.u / e.psi changes sign and every even power
-// is shared), and all per-class products (omega rho_k w_l, the perturbation
-// and recolouring coefficients) are formed once per cell.
+// economy: the two components of a direction travel as one packed FP32 pair
+// (sm_100 add / mul / fma .f32x2), opposite directions are processed as pairs
+// (e_opp = -e_l, so every odd power of e.u / e.psi changes sign and every
+// even power is shared), and all per-class products (omega rho_k w_l, the
+// perturbation and recolouring coefficients) are formed once per cell.
 //
 // Schedule: a CTA of TX x TY threads owns the column [x0, x0+TX) x [y0, y0+TY)
-// and marches it along z over one segment.  In iteration z it
-//   1. pulls the populations of plane z+1 for its own cells and for the
-//      one-cell ring around the column, and writes their phase field into a
-//      rolling four-slot shared-memory window (only sums are formed, nothing
-//      is kept in registers);
-//   2. after one barrier, pulls the populations of plane z again (they are
-//      L1/L2 resident from step 1 of the previous iteration), computes the
-//      colour gradient from the window and collides, and stores the 38
-//      post-collision populations of each cell with aligned, coalesced writes.
+// and marches it along z over one segment (32 planes by default).  In
+// iteration z it
+//   1. starts the pulls of plane z+2 for its own cells and the one-cell ring
+//      around the column: 16-bit storage copies them into a three-plane
+//      shared-memory stage by cp.async (FP32 / FP64 pull synchronously in
+//      step 2 instead);
+//   2. sums the pulls of plane z+1 (landed one iteration ago) into densities
+//      and writes their phase field into a rolling four-slot window, then
+//      arrives at the plane's split barrier (an mbarrier);
+//   3. reads the pairs of plane z from the stage, takes the part of the
+//      colour gradient from planes z-1 and z, relaxes (BGK half), waits at the
+//      barrier, adds the plane z+1 part of the gradient, perturbs and
+//      recolours, and stores the 38 post-collision values of each cell with
+//      coalesced 4- or 8-byte writes.
 // The phase field never goes through global memory; the extra cost is the
-// ring and the two boundary planes of each segment, read from L2.
+// ring and the two boundary planes of each segment.  The particle variant
+// (PART) also copies each cell's flag words and side phase field with its
+// pulls and collides only fluid cells.
 #include "lbx_device.cuh"
 
 #include <algorithm>
