@@ -1,9 +1,12 @@
 // lbx_fused.cu — single-pass colour-gradient step (time_step_CG + streaming,
 // kernels_fluid_CG.CUF:531-1141) for sm_100a, written for instruction
-// economy: the two components of a direction travel as one packed FP32 pair
-// (sm_100 add / mul / fma .f32x2), opposite directions are processed as pairs
-// (e_opp = -e_l, so every odd power of e.u / e.psi changes sign and every
-// even power is shared), and all per-class products (omega rho_k w_l, the
+// economy: the two components of a direction are one 4- or 8-byte word in
+// memory, the collision relaxes their sum (the recolouring needs nothing
+// else when the colour gradient is non-zero), a direction and its opposite
+// form one packed FP32 pair for the sm_100 add / mul / fma .f32x2
+// instructions (e_opp = -e_l, so every odd power of e.u / e.psi changes sign
+// and every even power is shared), 16-bit values enter the FP32 sums by
+// mixed-precision adds, and all per-class products (omega rho w_l, the
 // perturbation and recolouring coefficients) are formed once per cell.
 //
 // Schedule: a CTA of TX x TY threads owns the column [x0, x0+TX) x [y0, y0+TY)
@@ -122,12 +125,26 @@ __device__ __forceinline__ double2 p_fma(double2 a, double2 b, double2 c) {
   return make_double2(fma(a.x, b.x, c.x), fma(a.y, b.y, c.y));
 }
 
+// a + c for a 16-bit a and an FP32 c, rounded once (sm_100 mixed-precision
+// add: the conversion of a is exact, so this equals float(a) + c)
+__device__ __forceinline__ float add_mixed(__half a, float c) {
+  float d;
+  asm("add.rn.f32.f16 %0, %1, %2;" : "=f"(d) : "h"(__half_as_ushort(a)), "f"(c));
+  return d;
+}
+__device__ __forceinline__ float add_mixed(__nv_bfloat16 a, float c) {
+  float d;
+  asm("add.rn.f32.bf16 %0, %1, %2;" : "=f"(d) : "h"(__bfloat16_as_ushort(a)), "f"(c));
+  return d;
+}
+
 // storage pair <-> arithmetic pair (R: the stored pair as one word)
 template <typename S> struct SPair;
 template <> struct SPair<float> {
   using R = float2;
   static __device__ __forceinline__ R ldr(const float* p) { return __ldg(reinterpret_cast<const float2*>(p)); }
   static __device__ __forceinline__ float2 cvt(R r) { return r; }
+  static __device__ __forceinline__ float sum(R r) { return r.x + r.y; }
   static __device__ __forceinline__ float2 ld(const float* p) { return cvt(ldr(p)); }
   static __device__ __forceinline__ void st(float* p, float2 v) { *reinterpret_cast<float2*>(p) = v; }
 };
@@ -135,6 +152,7 @@ template <> struct SPair<double> {
   using R = double2;
   static __device__ __forceinline__ R ldr(const double* p) { return __ldg(reinterpret_cast<const double2*>(p)); }
   static __device__ __forceinline__ double2 cvt(R r) { return r; }
+  static __device__ __forceinline__ double sum(R r) { return r.x + r.y; }
   static __device__ __forceinline__ double2 ld(const double* p) { return cvt(ldr(p)); }
   static __device__ __forceinline__ void st(double* p, double2 v) { *reinterpret_cast<double2*>(p) = v; }
 };
@@ -142,6 +160,7 @@ template <> struct SPair<__half> {
   using R = __half2;
   static __device__ __forceinline__ R ldr(const __half* p) { return __ldg(reinterpret_cast<const __half2*>(p)); }
   static __device__ __forceinline__ float2 cvt(R r) { return __half22float2(r); }
+  static __device__ __forceinline__ float sum(R r) { return add_mixed(r.y, __low2float(r)); }
   static __device__ __forceinline__ float2 ld(const __half* p) { return cvt(ldr(p)); }
   static __device__ __forceinline__ void st(__half* p, float2 v) {
     *reinterpret_cast<__half2*>(p) = __float22half2_rn(v);
@@ -153,6 +172,7 @@ template <> struct SPair<__nv_bfloat16> {
     return __ldg(reinterpret_cast<const __nv_bfloat162*>(p));
   }
   static __device__ __forceinline__ float2 cvt(R r) { return __bfloat1622float2(r); }
+  static __device__ __forceinline__ float sum(R r) { return add_mixed(r.y, __low2float(r)); }
   static __device__ __forceinline__ float2 ld(const __nv_bfloat16* p) { return cvt(ldr(p)); }
   static __device__ __forceinline__ void st(__nv_bfloat16* p, float2 v) {
     *reinterpret_cast<__nv_bfloat162*>(p) = __float22bfloat162_rn(v);
@@ -164,7 +184,9 @@ template <> struct SPair<__nv_bfloat16> {
 // from L2 for the collision: a two-deep FP32 stage (109 KB per CTA, issued
 // once the collision has read a plane's pairs) measured 0.235 ms at 128^3
 // against 0.156 ms without it.  Own-cell pairs are 3 planes deep: plane z+2
-// is copied at the top of iteration z.
+// is copied at the top of iteration z.  Copying one plane further ahead (4
+// planes, 100 KB per CTA) measured 0.165 ms against 0.107 at FP16 128^3: the
+// larger stage leaves the L1 too small for the pulls.
 template <typename S, bool PART>
 constexpr bool kStaged = sizeof(typename SPair<S>::R) == 4;
 template <typename S, bool PART>
@@ -181,6 +203,10 @@ struct Planes {
   S* p;
   int64_t n2;  // 2 n elements per direction plane
   __device__ __forceinline__ S* operator()(int l) const { return p + size_t(l) * size_t(n2); }
+  // pair i of direction plane l; the unsigned index keeps the per-thread part
+  // one 32 x 32 -> 64-bit multiply-add onto the plane base (a signed int
+  // index measured 84 more integer instructions per cell)
+  __device__ __forceinline__ S* at(int l, int i) const { return (*this)(l) + 2 * size_t(unsigned(i)); }
 };
 
 // ---- asynchronous copies global -> shared (cp.async, 4-byte granules) --------
@@ -239,18 +265,24 @@ __device__ __forceinline__ void pull_async(const S* __restrict__ A, int64_t n, c
   const Planes<const S> Ap{A, 2 * n};
 #pragma unroll
   for (int l = 0; l < Q; ++l) {
-    if constexpr (sizeof(typename SPair<S>::R) == 4) cp_async4(st + l * stride, Ap(l) + 2 * P.src[l]);
-    else cp_async8(st + l * stride, Ap(l) + 2 * P.src[l]);
+    if constexpr (sizeof(typename SPair<S>::R) == 4) cp_async4(st + l * stride, Ap.at(l, P.src[l]));
+    else cp_async8(st + l * stride, Ap.at(l, P.src[l]));
   }
 }
 
-// densities (Sum g + rho0, before the clamp) from pairs already in shared memory
+// densities (Sum g + rho0, before the clamp) from pairs already in shared
+// memory: each 16-bit value is added to the FP32 sums by one mixed-precision
+// add (same order and roundings as converting first)
 template <typename S, typename C>
 __device__ __forceinline__ void stage_rho(const typename SPair<S>::R* st, int stride, const LeanConst<C>& K, C& rR,
                                           C& rB) {
   P2<C> s = SPair<S>::cvt(st[0]);
 #pragma unroll
-  for (int l = 1; l < Q; ++l) s = p_add(s, SPair<S>::cvt(st[l * stride]));
+  for (int l = 1; l < Q; ++l) {
+    const typename SPair<S>::R r = st[l * stride];
+    s.x = add_mixed(r.x, s.x);
+    s.y = add_mixed(r.y, s.y);
+  }
   rR = s.x + K.rho0[0];
   rB = s.y + K.rho0[1];
 }
@@ -267,7 +299,7 @@ __device__ __forceinline__ void pull_rho(const S* __restrict__ A, int64_t n, con
   P2<C> s = SPair<S>::cvt(r);
 #pragma unroll
   for (int l = 1; l < Q; ++l) {
-    r = SPair<S>::ldr(Ap(l) + 2 * P.src[l]);
+    r = SPair<S>::ldr(Ap.at(l, P.src[l]));
     if (st) st[l * stride] = r;
     s = p_add(s, SPair<S>::cvt(r));
   }
@@ -301,20 +333,47 @@ template <typename C>
 __device__ __forceinline__ C phase_of(C rR, C rB) { return (rR - rB) * rcp_c(rR + rB); }
 
 // One colour-gradient collision (time_step_CG, kernels_fluid_CG.CUF:689-846)
-// on the component pairs g[l] = (g_R, g_B): stored form (f - shift) on entry,
-// post-collision stored form on exit.  rR/rB: clamped densities.  Two
-// halves: the BGK relaxation (no colour gradient needed), then the
-// perturbation and recolouring with the gradient (psi).
+// in two halves around the plane barrier, written on component SUMS.  When
+// the colour gradient is non-zero the recolouring needs, per direction, only
+// fd_l = f'_R,l + f'_B,l + perturbation (the BGK-relaxed sum) and the cell's
+// densities: the relaxed components themselves are never used.  So the BGK
+// half relaxes S_l = g_R,l + g_B,l (stored form; the shifts fold into one
+// constant per weight class),
+//   h_l = f'_R,l + f'_B,l = (1 - omega) S_l + omega rho w_l A_l(u) + (1 - omega) s_l,
+// and the recolouring half forms both outputs from h_l.  A direction pair
+// (l, opposite) is one packed FP32 pair: e_opp = -e_l, so (e.u, -e.u) and
+// (e.psi, -e.psi) give both directions' A, perturbation and recolouring term
+// from the same packed instructions.  A cell without a colour gradient
+// (|psi|^2 <= 1e-20) keeps the per-component BGK result (bgk_components).
 template <typename C>
-struct CollideState {
-  C omega, inv;
+struct Relaxed {
+  C h0;         // rest direction
+  P2<C> h[9];   // pair p: (h_{2p-1}, h_{2p})
+  C u, v, w, c0, omega, inv;
 };
 
+// packed pair (e.a, -e.a) of direction 2p-1 from the pairs (a_i, -a_i) and (-a_i, a_i)
 template <typename C>
-__device__ __forceinline__ CollideState<C> collide_bgk(const LeanConst<C>& K, P2<C> g[Q], C rR, C rB,
-                                                       bool shifted) {
+__device__ __forceinline__ P2<C> edot_pair(int l, const P2<C> pos[3], const P2<C> neg[3]) {
+  const int e[3] = {ex(l), ey(l), ez(l)};
+  P2<C> r = pp(C(0), C(0));
+  bool any = false;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    if (!e[i]) continue;
+    const P2<C> t = e[i] > 0 ? pos[i] : neg[i];
+    r = any ? p_add(r, t) : t;
+    any = true;
+  }
+  return r;
+}
+
+// BGK half: S[l] = g_R,l + g_B,l of the pulled (stored-form) pairs; rR/rB: clamped densities
+template <typename C>
+__device__ __forceinline__ Relaxed<C> relax_sums(const LeanConst<C>& K, const C S[Q], C rR, C rB, bool shifted) {
   const C ONE = C(1), HALF = C(0.5);
   const C rs = rR + rB;
+  Relaxed<C> X;
   C omega;
   if (K.omega >= C(0)) {
     omega = K.omega;
@@ -326,96 +385,110 @@ __device__ __forceinline__ CollideState<C> collide_bgk(const LeanConst<C>& K, P2
   const C omm = ONE - omega;
   const C inv = rcp_c(rs);
   // momentum from the opposite-pair differences (shifts cancel)
-  const P2<C> NEG = pp(C(-1), C(-1));
-  C d[10];
+  C mu = C(0), mv = C(0), mw = C(0);
 #pragma unroll
   for (int p = 1; p <= 9; ++p) {
-    const P2<C> t = p_fma(g[2 * p], NEG, g[2 * p - 1]);
-    d[p] = t.x + t.y;
+    const int l = 2 * p - 1;
+    const C d = S[l] - S[l + 1];
+    if (ex(l)) mu = ex(l) > 0 ? mu + d : mu - d;
+    if (ey(l)) mv = ey(l) > 0 ? mv + d : mv - d;
+    if (ez(l)) mw = ez(l) > 0 ? mw + d : mw - d;
   }
-  // pairs: 1 (+x) 2 (+y) 3 (+z) 4 (+x+y) 5 (-x+y) 6 (+x+z) 7 (-x+z) 8 (+y+z) 9 (-y+z)
-  const C u = inv * (d[1] + d[4] - d[5] + d[6] - d[7]);
-  const C v = inv * (d[2] + d[4] + d[5] + d[8] - d[9]);
-  const C w = inv * (d[3] + d[6] + d[7] + d[8] + d[9]);
+  const C u = inv * mu, v = inv * mv, w = inv * mw;
   const C c0 = fm(C(-1.5), fm(u, u, fm(v, v, w * w)), ONE);
-  P2<C> Kc[3], os[3];
+  // per weight class: omega rho w and the folded shift (1 - omega) (s_R + s_B)
+  C kc[3], hs[3];
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
-    Kc[k] = pp(omega * rR * K.w[k], omega * rB * K.w[k]);  // omega rho_k w
-    os[k] = pp(-omega * K.s[0][k], -omega * K.s[1][k]);     // -omega times the shift
+    kc[k] = omega * rs * K.w[k];
+    hs[k] = shifted ? omm * (K.s[0][k] + K.s[1][k]) : C(0);
   }
-  const P2<C> omm2 = pp(omm, omm);
-  // BGK: f' = f (1 - omega) + omega rho w A(u).  Stored form g = f - s stays
-  // stored: g' = g (1 - omega) + omega rho w A(u) - omega s.
-  auto relax = [&](const P2<C>& gl, const P2<C>& kc, C a, const P2<C>& o) {
-    return shifted ? p_fma(gl, omm2, p_fma(kc, pp(a, a), o)) : p_fma(gl, omm2, p_mul(kc, pp(a, a)));
-  };
-  g[0] = relax(g[0], Kc[0], c0, os[0]);
+  X.h0 = shifted ? fm(omm, S[0], fm(kc[0], c0, hs[0])) : fm(omm, S[0], kc[0] * c0);
+  const P2<C> pos[3] = {pp(u, -u), pp(v, -v), pp(w, -w)};
+  const P2<C> neg[3] = {pp(-u, u), pp(-v, v), pp(-w, w)};
+  const P2<C> OMM = pp(omm, omm), C0 = pp(c0, c0), F45 = pp(C(4.5), C(4.5)), THREE = pp(C(3), C(3));
 #pragma unroll
   for (int p = 1; p <= 9; ++p) {
-    const int l = 2 * p - 1, o = 2 * p, k = wclass(l);
-    const C eu = edot(l, u, v, w);
-    const C P = fm(C(4.5) * eu, eu, c0);
-    const C Qv = C(3) * eu;
-    const C Ap = P + Qv, Am = P - Qv;
-    g[l] = relax(g[l], Kc[k], Ap, os[k]);
-    g[o] = relax(g[o], Kc[k], Am, os[k]);
+    const int l = 2 * p - 1, k = wclass(l);
+    const P2<C> eu = edot_pair<C>(l, pos, neg);            // (e.u, -e.u)
+    const P2<C> P = p_fma(p_mul(F45, eu), eu, C0);        // 1 + 4.5 (e.u)^2 - 1.5 u^2
+    const P2<C> A = p_fma(THREE, eu, P);                  // + 3 e.u, - 3 e.u
+    const P2<C> Sv = pp(S[l], S[l + 1]);
+    const P2<C> KC = pp(kc[k], kc[k]);
+    X.h[p - 1] = shifted ? p_fma(OMM, Sv, p_fma(KC, A, pp(hs[k], hs[k]))) : p_fma(OMM, Sv, p_mul(KC, A));
   }
-  return CollideState<C>{omega, inv};
+  X.u = u;
+  X.v = v;
+  X.w = w;
+  X.c0 = c0;
+  X.omega = omega;
+  X.inv = inv;
+  return X;
 }
 
+// Recolouring half (perturbation + recolouring): the post-collision pairs
+// (stored form) into out[]; false, with out[] untouched, when the colour
+// gradient is below the reference's limit.
 template <typename C>
-__device__ __forceinline__ void collide_recolour(const LeanConst<C>& K, P2<C> g[Q], C rR, C rB, C px, C py, C pz,
-                                                 bool shifted, CollideState<C> cs) {
-  const C omega = cs.omega, inv = cs.inv;
-  // g holds the relaxed populations in stored form; f_R + f_B = g_R + g_B + ss
-  P2<C> ns[3];
-  C ss[3];
+__device__ __forceinline__ bool recolour_sums(const LeanConst<C>& K, const Relaxed<C>& X, C rR, C rB, C px, C py,
+                                              C pz, bool shifted, P2<C> out[Q]) {
+  const C psq = fm(px, px, fm(py, py, pz * pz));
+  if (!(psq > C(1.e-20))) return false;
+  const C ipn = rsqrt_c(psq);
+  const C pn = psq * ipn;
+  const C acoeff = C(9) / C(4) * X.omega * K.sigma;
+  const C coef = K.beta * rR * rB * X.inv * ipn;  // beta rR rB / (rs |psi|)
+  const C kR = rR * X.inv, kB = rB * X.inv;
+  C K1[3], K0[3], K3[3];
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
-    ns[k] = pp(-K.s[0][k], -K.s[1][k]);  // minus the shift
-    ss[k] = K.s[0][k] + K.s[1][k];
+    K1[k] = acoeff * K.w[k] * ipn;  // acoeff |psi| w / |psi|^2
+    K0[k] = acoeff * pn * K.b[k];
   }
-  const C psq = fm(px, px, fm(py, py, pz * pz));
-  if (psq > C(1.e-20)) {
-    const C ipn = rsqrt_c(psq);
-    const C pn = psq * ipn;
-    const C acoeff = C(9) / C(4) * omega * K.sigma;
-    const C coef = K.beta * rR * rB * inv * ipn;  // beta rR rB / (rs |psi|)
-    const P2<C> kk = pp(rR * inv, rB * inv);
-    C K1[3], K0[3], K3[3];
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-      K1[k] = acoeff * K.w[k] * ipn;  // acoeff |psi| w / |psi|^2
-      K0[k] = acoeff * pn * K.b[k];
-    }
-    K3[0] = C(0);
-    K3[1] = coef * K.w[1];
-    K3[2] = coef * K.w[2] / K.sqrt2;
-    {
-      const C fd = g[0].x + g[0].y + (ss[0] - K0[0]);
-      g[0] = p_fma(pp(fd, fd), kk, ns[0]);
-    }
-#pragma unroll
-    for (int p = 1; p <= 9; ++p) {
-      const int l = 2 * p - 1, o = 2 * p, k = wclass(l);
-      const C ed = edot(l, px, py, pz);
-      const C pert = fm(K1[k], ed * ed, ss[k] - K0[k]);
-      const C T = K3[k] * ed;
-      const C fdp = g[l].x + g[l].y + pert;
-      const C fdm = g[o].x + g[o].y + pert;
-      g[l] = p_fma(pp(fdp, fdp), kk, p_add(pp(T, -T), ns[k]));
-      g[o] = p_fma(pp(fdm, fdm), kk, p_add(pp(-T, T), ns[k]));
-    }
+  K3[0] = C(0);
+  K3[1] = coef * K.w[1];
+  K3[2] = coef * K.w[2] / K.sqrt2;
+  const P2<C> KK = pp(kR, kB);
+  {
+    const C fd = X.h0 - K0[0];
+    out[0] = shifted ? p_fma(pp(fd, fd), KK, pp(-K.s[0][0], -K.s[1][0])) : p_mul(pp(fd, fd), KK);
   }
-  // without a colour gradient the relaxed populations are the result
+  const P2<C> pos[3] = {pp(px, -px), pp(py, -py), pp(pz, -pz)};
+  const P2<C> neg[3] = {pp(-px, px), pp(-py, py), pp(-pz, pz)};
+  const P2<C> KR = pp(kR, kR), KB = pp(kB, kB), NEG = pp(C(-1), C(-1));
+#pragma unroll
+  for (int p = 1; p <= 9; ++p) {
+    const int l = 2 * p - 1, k = wclass(l);
+    const P2<C> ed = edot_pair<C>(l, pos, neg);                              // (e.psi, -e.psi)
+    const P2<C> pert = p_fma(pp(K1[k], K1[k]), p_mul(ed, ed), pp(-K0[k], -K0[k]));
+    const P2<C> T = p_mul(pp(K3[k], K3[k]), ed);                             // (T, -T)
+    const P2<C> fd = p_add(X.h[p - 1], pert);
+    const P2<C> cR = shifted ? p_add(T, pp(-K.s[0][k], -K.s[0][k])) : T;
+    const P2<C> cB = shifted ? p_fma(T, NEG, pp(-K.s[1][k], -K.s[1][k])) : p_mul(T, NEG);
+    const P2<C> oR = p_fma(KR, fd, cR);
+    const P2<C> oB = p_fma(KB, fd, cB);
+    out[l] = pp(oR.x, oB.x);
+    out[l + 1] = pp(oR.y, oB.y);
+  }
+  return true;
 }
 
+// BGK result per component (no colour gradient): g' = g (1 - omega) +
+// omega rho_k w A(u) - omega s_k, in place on the pulled pairs g[]
 template <typename C>
-__device__ __forceinline__ void collide_pair(const LeanConst<C>& K, P2<C> g[Q], C rR, C rB, C px, C py, C pz,
-                                             bool shifted) {
-  const CollideState<C> cs = collide_bgk(K, g, rR, rB, shifted);
-  collide_recolour(K, g, rR, rB, px, py, pz, shifted, cs);
+__device__ __forceinline__ void bgk_components(const LeanConst<C>& K, const Relaxed<C>& X, C rR, C rB, bool shifted,
+                                               P2<C> g[Q]) {
+  const C omega = X.omega, omm = C(1) - omega;
+  const P2<C> omm2 = pp(omm, omm);
+#pragma unroll
+  for (int l = 0; l < Q; ++l) {
+    const int k = wclass(l);
+    const C eu = edot(l, X.u, X.v, X.w);
+    const C a = fm(C(3), eu, fm(C(4.5) * eu, eu, X.c0));
+    const P2<C> kc = pp(omega * rR * K.w[k], omega * rB * K.w[k]);
+    g[l] = shifted ? p_fma(g[l], omm2, p_fma(kc, pp(a, a), pp(-omega * K.s[0][k], -omega * K.s[1][k])))
+                   : p_fma(g[l], omm2, p_mul(kc, pp(a, a)));
+  }
 }
 
 template <int TX, int TY>
@@ -423,6 +496,9 @@ struct Ring {
   static constexpr int RX = TX + 2, RY = TY + 2, CELLS = RX * RY, N = 2 * RX + 2 * TY, NT = TX * TY;
 };
 
+// periodic wrap of a plane index p in [-n, 2n) (the planes a segment touches,
+// z0 - 1 .. zend + 1, with n >= 3): two compares instead of a division
+__device__ __forceinline__ int wrap_plane(int p, int n) { return p < 0 ? p + n : (p >= n ? p - n : p); }
 __device__ __forceinline__ int wrap0(int v, int n) {
   v %= n;
   return v < 0 ? v + n : v;
@@ -538,7 +614,7 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
   // cell into the stage; with spheres, the flag words and the side phase
   // field of both cells are copied too (all in one copy group).
   auto issue = [&](int p) {
-    const int zz = wrap0(p, g.nz);
+    const int zz = wrap_plane(p, g.nz);
     if constexpr (PART) {
       if (parts) {
         const int co = x + g.nx * (y + g.ny * zz);
@@ -621,7 +697,7 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
 
   // phase field of plane p (own cell and ring cell) into its window slot
   auto phase_plane = [&](int p, C& rRo, C& rBo) {
-    const int zz = wrap0(p, g.nz);
+    const int zz = wrap_plane(p, g.nz);
     const bool owned = active && p >= z0 && p < zend;
     const SideRec<C>* so = PART ? side + own_q(p) * NT + tid : nullptr;
     sphi[p & 3][own] = cell_phase(x, y, zz, owned, true, STAGED ? own_slot(p) : nullptr, NT, so, rRo, rBo);
@@ -656,55 +732,55 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
     // every thread wrote them before arriving at the previous plane's barrier,
     // and their slots are rewritten only after this plane's barrier.
     const int cell = x + g.nx * (y + g.ny * z);
-    P2<C> gp[Q];
-    bool collide = true;
+    bool collide = true, fresh = false;
     C px = 0, py = 0, pz = 0;
-    CollideState<C> cst{C(0), C(0)};
+    Relaxed<C> rx;
     PullIdx P;
     if (active) {
-      pull_idx(g, x, y, z, P);
-      // the pull every fluid cell needs: in the stage since two iterations,
-      // or issued here
-      if constexpr (STAGED) {
-        const SR* sg = own_slot(z);
-#pragma unroll
-        for (int l = 0; l < Q; ++l) gp[l] = SPair<S>::cvt(sg[l * NT]);
-      } else {
-#pragma unroll
-        for (int l = 0; l < Q; ++l) gp[l] = SPair<S>::ld(Ap(l) + 2 * P.src[l]);
-      }
-    }
-    if (active) {
+      if constexpr (!STAGED) pull_idx(g, x, y, z, P);
       if constexpr (PART) {
         if (parts) {
           int8_t fn, fo;
           flags_of(side + own_q(z) * NT + tid, cell, fn, fo);
           // a solid cell keeps the plain pull (see below)
           collide = fn == LBX_FLUID_FLUID;
-          if (collide && fo != LBX_FLUID_FLUID) {
-            // make_fluid already wrote the new node's populations (stored form) into B
-#pragma unroll
-            for (int l = 0; l < Q; ++l) gp[l] = SPair<S>::ld(Bp(l) + 2 * cell);
-          }
+          // make_fluid already wrote a new node's populations (stored form) into B
+          fresh = collide && fo != LBX_FLUID_FLUID;
         }
       }
-      if (collide) {
-        // colour gradient from planes z-1 and z, then the BGK half
-        const C* pm = sphi[(z + 3) & 3];
-        const C* p0 = sphi[z & 3];
+    }
+    // Stored pairs of this cell: the pull (in the stage since two
+    // iterations, or issued here), or a new node's populations in B.
+    auto pulled = [&](int l) -> SR {
+      if constexpr (STAGED) return own_slot(z)[l * NT];
+      else return SPair<S>::ldr(Ap.at(l, P.src[l]));
+    };
+    auto refilled = [&](int l) -> SR { return SPair<S>::ldr(Bp.at(l, cell)); };
+    if (active && collide) {
+      // colour gradient from planes z-1 and z, then the BGK half
+      const C* pm = sphi[(z + 3) & 3];
+      const C* p0 = sphi[z & 3];
 #pragma unroll
-        for (int l = 1; l < Q27; ++l) {
-          const int dx = ex27(l), dy = ey27(l), dz = ez27(l);
-          if (dz > 0) continue;
-          const C* pl = dz < 0 ? pm : p0;
-          const C ps = pl[own + dy * R::RX + dx];
-          const C a = K.a27[wclass27(l)];
-          if (dx) px = fm(dx > 0 ? a : -a, ps, px);
-          if (dy) py = fm(dy > 0 ? a : -a, ps, py);
-          if (dz) pz = fm(dz > 0 ? a : -a, ps, pz);
-        }
-        cst = collide_bgk(K, gp, rRc, rBc, Store<S>::shifted);
+      for (int l = 1; l < Q27; ++l) {
+        const int dx = ex27(l), dy = ey27(l), dz = ez27(l);
+        if (dz > 0) continue;
+        const C* pl = dz < 0 ? pm : p0;
+        const C ps = pl[own + dy * R::RX + dx];
+        const C a = K.a27[wclass27(l)];
+        if (dx) px = fm(dx > 0 ? a : -a, ps, px);
+        if (dy) py = fm(dy > 0 ? a : -a, ps, py);
+        if (dz) pz = fm(dz > 0 ? a : -a, ps, pz);
       }
+      C Ssum[Q];
+#pragma unroll
+      for (int l = 0; l < Q; ++l) Ssum[l] = SPair<S>::sum(pulled(l));
+      if constexpr (PART) {
+        if (fresh) {
+#pragma unroll
+          for (int l = 0; l < Q; ++l) Ssum[l] = SPair<S>::sum(refilled(l));
+        }
+      }
+      rx = relax_sums(K, Ssum, rRc, rBc, Store<S>::shifted);
     }
     if (!mbar_wait(bar, bar_parity)) raise_error(err, LBX_DEV_WAIT_TIMEOUT, step, -1);
     bar_parity ^= 1u;
@@ -715,6 +791,8 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
       // populations (a fluid cell pulls from a solid one only along a link
       // the bounce-back rewrote, and a cell that turns fluid is refilled), so
       // only raw population dumps of solid cells differ.
+      P2<C> gp[Q];
+      bool done = false;
       if (collide) {
         const C* ppl = sphi[(z + 1) & 3];
 #pragma unroll
@@ -727,10 +805,21 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
           if (dy) py = fm(dy > 0 ? a : -a, ps, py);
           pz = fm(a, ps, pz);
         }
-        collide_recolour(K, gp, rRc, rBc, px, py, pz, Store<S>::shifted, cst);
+        done = recolour_sums(K, rx, rRc, rBc, px, py, pz, Store<S>::shifted, gp);
+      }
+      if (!done) {
+#pragma unroll
+        for (int l = 0; l < Q; ++l) gp[l] = SPair<S>::cvt(pulled(l));
+        if constexpr (PART) {
+          if (fresh) {
+#pragma unroll
+            for (int l = 0; l < Q; ++l) gp[l] = SPair<S>::cvt(refilled(l));
+          }
+        }
+        if (collide) bgk_components(K, rx, rRc, rBc, Store<S>::shifted, gp);
       }
 #pragma unroll
-      for (int l = 0; l < Q; ++l) SPair<S>::st(Bp(l) + 2 * cell, gp[l]);
+      for (int l = 0; l < Q; ++l) SPair<S>::st(Bp.at(l, cell), gp[l]);
     }
   }
   if constexpr (ASYNC) cp_async_wait<0>();  // nothing in flight when the shared memory is reused
