@@ -779,8 +779,8 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
     // plane's barrier, rewritten only after this one) and z+1 after it.
     const int cell = x + g.nx * (y + g.ny * z);
     bool collide = true, fresh = false;
-    Relaxed<C> rx;
     C px = 0, py = 0, pz = 0;
+    Relaxed<C> rx;
     PullIdx P;
     if (active) {
       if constexpr (!STAGED) pull_idx(g, x, y, z, P);
@@ -803,18 +803,8 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
     };
     auto refilled = [&](int l) -> SR { return SPair<S>::ldr(Bp.at(l, cell)); };
     if (active && collide) {
-      // the pulls (issued first: the gradient below overlaps their latency
-      // when they come from global memory), the gradient from planes z-1 and
-      // z (synchronous pulls only), then the BGK half
-      C Ssum[Q];
-#pragma unroll
-      for (int l = 0; l < Q; ++l) Ssum[l] = SPair<S>::sum(pulled(l));
-      if constexpr (PART) {
-        if (fresh) {
-#pragma unroll
-          for (int l = 0; l < Q; ++l) Ssum[l] = SPair<S>::sum(refilled(l));
-        }
-      }
+      // the colour gradient from planes z-1 and z (synchronous pulls only),
+      // then the BGK half
       if constexpr (!STAGED) {
         const C* pm = sphi[(z + 3) & 3];
         const C* p0 = sphi[z & 3];
@@ -828,6 +818,15 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
           if (dx) px = fm(dx > 0 ? a : -a, ps, px);
           if (dy) py = fm(dy > 0 ? a : -a, ps, py);
           if (dz) pz = fm(dz > 0 ? a : -a, ps, pz);
+        }
+      }
+      C Ssum[Q];
+#pragma unroll
+      for (int l = 0; l < Q; ++l) Ssum[l] = SPair<S>::sum(pulled(l));
+      if constexpr (PART) {
+        if (fresh) {
+#pragma unroll
+          for (int l = 0; l < Q; ++l) Ssum[l] = SPair<S>::sum(refilled(l));
         }
       }
       rx = relax_sums(K, Ssum, rRc, rBc, Store<S>::shifted);
@@ -853,20 +852,23 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
         }
         gm = g0;
         g0 = gpl;
-      } else if (collide) {  // plane z+1 of the colour gradient
-        const C* ppl = sphi[(z + 1) & 3];
-#pragma unroll
-        for (int l = 1; l < Q27; ++l) {
-          const int dx = ex27(l), dy = ey27(l), dz = ez27(l);
-          if (dz <= 0) continue;
-          const C ps = ppl[own + dy * R::RX + dx];
-          const C a = K.a27[wclass27(l)];
-          if (dx) px = fm(dx > 0 ? a : -a, ps, px);
-          if (dy) py = fm(dy > 0 ? a : -a, ps, py);
-          pz = fm(a, ps, pz);
-        }
       }
-      if (collide) done = recolour_sums(K, rx, rRc, rBc, px, py, pz, Store<S>::shifted, gp);
+      if (collide) {
+        if constexpr (!STAGED) {  // plane z+1 of the colour gradient
+          const C* ppl = sphi[(z + 1) & 3];
+#pragma unroll
+          for (int l = 1; l < Q27; ++l) {
+            const int dx = ex27(l), dy = ey27(l), dz = ez27(l);
+            if (dz <= 0) continue;
+            const C ps = ppl[own + dy * R::RX + dx];
+            const C a = K.a27[wclass27(l)];
+            if (dx) px = fm(dx > 0 ? a : -a, ps, px);
+            if (dy) py = fm(dy > 0 ? a : -a, ps, py);
+            pz = fm(a, ps, pz);
+          }
+        }
+        done = recolour_sums(K, rx, rRc, rBc, px, py, pz, Store<S>::shifted, gp);
+      }
       if (!done) {
 #pragma unroll
         for (int l = 0; l < Q; ++l) gp[l] = SPair<S>::cvt(pulled(l));
