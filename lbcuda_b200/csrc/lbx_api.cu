@@ -68,13 +68,27 @@ int sync_status(Ctx& c) {
 }
 
 // temporary device buffer for host<->device staging of one call
+// Device staging area of the context for host-buffer transfers: allocated
+// on first use and grown when a larger transfer comes, never per call (a
+// cudaMalloc / cudaFree pair per call cost milliseconds and synchronised the
+// device).
 struct DevBuf {
   void* p = nullptr;
-  explicit DevBuf(size_t bytes) {
-    if (bytes && cudaMalloc(&p, bytes) != cudaSuccess) p = nullptr;
-  }
-  ~DevBuf() {
-    if (p) cudaFree(p);
+  DevBuf(lbx::Ctx* c, size_t bytes) {
+    if (bytes > c->io_bytes) {
+      if (c->io) {
+        cudaStreamSynchronize(c->stream);
+        cudaFree(c->io);
+      }
+      c->io = nullptr;
+      c->io_bytes = 0;
+      if (cudaMalloc(&c->io, bytes) != cudaSuccess) {
+        c->io = nullptr;
+        return;
+      }
+      c->io_bytes = bytes;
+    }
+    p = c->io;
   }
 };
 
@@ -160,6 +174,7 @@ int lbx_destroy(void* ctx) {
   lbx::fluid_free(*c);
   for (auto e : c->kt_ev) cudaEventDestroy(e);
   if (c->d_err) cudaFree(c->d_err);
+  if (c->io) cudaFree(c->io);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return 0;
@@ -169,7 +184,7 @@ int lbx_set_fields(void* ctx, const float* rhoR, const float* rhoB, float vx, fl
   Ctx* c = as_ctx(ctx);
   if (!c || !rhoR || (c->ncomp == 2 && !rhoB)) return LBX_ERR_ARG;
   size_t bytes = size_t(c->n) * sizeof(float);
-  DevBuf buf(bytes * c->ncomp);
+  DevBuf buf(c, bytes * c->ncomp);
   if (!buf.p) return LBX_ERR_ALLOC;
   float* dR = static_cast<float*>(buf.p);
   float* dB = (c->ncomp == 2) ? dR + c->n : nullptr;
@@ -186,7 +201,7 @@ int lbx_set_pops(void* ctx, const float* popsR, const float* popsB) {
   Ctx* c = as_ctx(ctx);
   if (!c || !popsR || (c->ncomp == 2 && !popsB)) return LBX_ERR_ARG;
   size_t bytes = size_t(c->n) * lbx::Q * sizeof(float);
-  DevBuf buf(bytes * c->ncomp);
+  DevBuf buf(c, bytes * c->ncomp);
   if (!buf.p) return LBX_ERR_ALLOC;
   float* dR = static_cast<float*>(buf.p);
   float* dB = (c->ncomp == 2) ? dR + c->n * lbx::Q : nullptr;
@@ -257,7 +272,7 @@ int lbx_time_step_bgk(void* ctx) {
 static int get_fields_impl(Ctx* c, void* rR, void* rB, void* vel, void* phase, int f64) {
   size_t es = f64 ? 8 : 4;
   size_t nb = size_t(c->n) * es;
-  DevBuf buf(nb * 6);
+  DevBuf buf(c, nb * 6);
   if (!buf.p) return LBX_ERR_ALLOC;
   char* d = static_cast<char*>(buf.p);
   void* dR = rR ? d : nullptr;
@@ -289,7 +304,7 @@ int lbx_get_pops(void* ctx, float* popsR, float* popsB) {
   Ctx* c = as_ctx(ctx);
   if (!c) return LBX_ERR_ARG;
   size_t nb = size_t(c->n) * lbx::Q * sizeof(float);
-  DevBuf buf(nb * 2);
+  DevBuf buf(c, nb * 2);
   if (!buf.p) return LBX_ERR_ALLOC;
   float* dR = popsR ? static_cast<float*>(buf.p) : nullptr;
   float* dB = popsB ? static_cast<float*>(buf.p) + size_t(c->n) * lbx::Q : nullptr;
@@ -315,7 +330,7 @@ int lbx_get_flags(void* ctx, int8_t* flags) {
 int lbx_get_sums(void* ctx, double* mass, double* momentum) {
   Ctx* c = as_ctx(ctx);
   if (!c) return LBX_ERR_ARG;
-  DevBuf buf(5 * sizeof(double));
+  DevBuf buf(c, 5 * sizeof(double));
   if (!buf.p) return LBX_ERR_ALLOC;
   double h[5];
   int rc = lbx::fluid_get_sums(*c, static_cast<double*>(buf.p));

@@ -49,6 +49,10 @@ struct Ctx {
   double kt_ms = 0.0;
   int64_t kt_launches = 0;
   ParticleState* part = nullptr;
+  // staging buffer of the host-buffer entry points (lbx_set_fields,
+  // lbx_get_fields, ...), kept between calls and grown on demand
+  void* io = nullptr;
+  size_t io_bytes = 0;
 };
 
 // lbx_fluid.cu
