@@ -105,6 +105,16 @@ __device__ __forceinline__ void pull_idx(const Geom& g, int x, int y, int z, Pul
   for (int l = 0; l < Q; ++l) P.src[l] = X[1 - ex(l)] + Y[1 - ey(l)] + Z[1 - ez(l)];
 }
 
+// source offset of the pull of direction l alone (the same wrap as
+// pull_idx; a caller that needs all 19 at once lets the compiler share the
+// neighbour coordinates, and nothing stays live between two uses)
+__device__ __forceinline__ int pull_one(const Geom& g, int x, int y, int z, int l) {
+  const int sx = ex(l) == 0 ? x : (ex(l) > 0 ? (x == 0 ? g.nx - 1 : x - 1) : (x == g.nx - 1 ? 0 : x + 1));
+  const int sy = ey(l) == 0 ? y : (ey(l) > 0 ? (y == 0 ? g.ny - 1 : y - 1) : (y == g.ny - 1 ? 0 : y + 1));
+  const int sz = ez(l) == 0 ? z : (ez(l) > 0 ? (z == 0 ? g.nz - 1 : z - 1) : (z == g.nz - 1 ? 0 : z + 1));
+  return sx + g.nx * (sy + g.ny * sz);
+}
+
 // ---- component pairs ---------------------------------------------------------
 // The two components of one direction and cell are adjacent in memory, so one
 // load / store moves both; in registers they form one float2 on which the
@@ -474,20 +484,53 @@ __device__ __forceinline__ bool recolour_sums(const LeanConst<C>& K, const Relax
 }
 
 // BGK result per component (no colour gradient): g' = g (1 - omega) +
-// omega rho_k w A(u) - omega s_k, in place on the pulled pairs g[]
-template <typename C>
+// omega rho_k w A(u) - omega s_k, in place on the pulled pairs g[] (R, B of
+// each direction).  PACKED: a direction and its opposite packed per
+// component (used with staged 16-bit pulls; the FP32 / FP64 kernels, with
+// more state live at this point, keep the per-direction form and stay
+// within their registers without spilling).
+template <typename C, bool PACKED>
 __device__ __forceinline__ void bgk_components(const LeanConst<C>& K, const Relaxed<C>& X, C rR, C rB, bool shifted,
                                                P2<C> g[Q]) {
   const C omega = X.omega, omm = C(1) - omega;
-  const P2<C> omm2 = pp(omm, omm);
+  if constexpr (!PACKED) {
+    const P2<C> omm2 = pp(omm, omm);
 #pragma unroll
-  for (int l = 0; l < Q; ++l) {
-    const int k = wclass(l);
-    const C eu = edot(l, X.u, X.v, X.w);
-    const C a = fm(C(3), eu, fm(C(4.5) * eu, eu, X.c0));
-    const P2<C> kc = pp(omega * rR * K.w[k], omega * rB * K.w[k]);
-    g[l] = shifted ? p_fma(g[l], omm2, p_fma(kc, pp(a, a), pp(-omega * K.s[0][k], -omega * K.s[1][k])))
-                   : p_fma(g[l], omm2, p_mul(kc, pp(a, a)));
+    for (int l = 0; l < Q; ++l) {
+      const int k = wclass(l);
+      const C eu = edot(l, X.u, X.v, X.w);
+      const C a = fm(C(3), eu, fm(C(4.5) * eu, eu, X.c0));
+      const P2<C> kc = pp(omega * rR * K.w[k], omega * rB * K.w[k]);
+      g[l] = shifted ? p_fma(g[l], omm2, p_fma(kc, pp(a, a), pp(-omega * K.s[0][k], -omega * K.s[1][k])))
+                     : p_fma(g[l], omm2, p_mul(kc, pp(a, a)));
+    }
+    return;
+  }
+  const P2<C> OMM = pp(omm, omm), C0 = pp(X.c0, X.c0), F45 = pp(C(4.5), C(4.5)), THREE = pp(C(3), C(3));
+  const P2<C> pos[3] = {pp(X.u, -X.u), pp(X.v, -X.v), pp(X.w, -X.w)};
+  const P2<C> neg[3] = {pp(-X.u, X.u), pp(-X.v, X.v), pp(-X.w, X.w)};
+  {
+    const P2<C> kc = pp(omega * rR * K.w[0], omega * rB * K.w[0]);
+    g[0] = shifted ? p_fma(g[0], OMM, p_fma(kc, C0, pp(-omega * K.s[0][0], -omega * K.s[1][0])))
+                   : p_fma(g[0], OMM, p_mul(kc, C0));
+  }
+#pragma unroll
+  for (int p = 1; p <= 9; ++p) {
+    const int l = 2 * p - 1, k = wclass(l);
+    const P2<C> eu = edot_pair<C>(l, pos, neg);
+    const P2<C> A = p_fma(THREE, eu, p_fma(p_mul(F45, eu), eu, C0));  // (A_l, A_opp)
+    const C kR = omega * rR * K.w[k], kB = omega * rB * K.w[k];
+    const P2<C> Rv = pp(g[l].x, g[l + 1].x), Bv = pp(g[l].y, g[l + 1].y);
+    P2<C> oR, oB;
+    if (shifted) {
+      oR = p_fma(Rv, OMM, p_fma(pp(kR, kR), A, pp(-omega * K.s[0][k], -omega * K.s[0][k])));
+      oB = p_fma(Bv, OMM, p_fma(pp(kB, kB), A, pp(-omega * K.s[1][k], -omega * K.s[1][k])));
+    } else {
+      oR = p_fma(Rv, OMM, p_mul(pp(kR, kR), A));
+      oB = p_fma(Bv, OMM, p_mul(pp(kB, kB), A));
+    }
+    g[l] = pp(oR.x, oB.x);
+    g[l + 1] = pp(oR.y, oB.y);
   }
 }
 
@@ -781,9 +824,7 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
     bool collide = true, fresh = false;
     C px = 0, py = 0, pz = 0;
     Relaxed<C> rx;
-    PullIdx P;
     if (active) {
-      if constexpr (!STAGED) pull_idx(g, x, y, z, P);
       if constexpr (PART) {
         if (parts) {
           int8_t fn, fo;
@@ -799,7 +840,7 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
     // iterations, or issued here), or a new node's populations in B.
     auto pulled = [&](int l) -> SR {
       if constexpr (STAGED) return own_slot(z)[l * NT];
-      else return SPair<S>::ldr(Ap.at(l, P.src[l]));
+      else return SPair<S>::ldr(Ap.at(l, pull_one(g, x, y, z, l)));
     };
     auto refilled = [&](int l) -> SR { return SPair<S>::ldr(Bp.at(l, cell)); };
     if (active && collide) {
@@ -878,7 +919,7 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
             for (int l = 0; l < Q; ++l) gp[l] = SPair<S>::cvt(refilled(l));
           }
         }
-        if (collide) bgk_components(K, rx, rRc, rBc, Store<S>::shifted, gp);
+        if (collide) bgk_components<C, STAGED>(K, rx, rRc, rBc, Store<S>::shifted, gp);
       }
 #pragma unroll
       for (int l = 0; l < Q; ++l) SPair<S>::st(Bp.at(l, cell), gp[l]);
