@@ -38,6 +38,8 @@ extern "C" {
 /* ---- enumerations ------------------------------------------------------ */
 #define LBX_MODEL_BGK 0 /* single-component BGK (kernels_fluid_BGK.CUF)        */
 #define LBX_MODEL_CG 1  /* two-component colour gradient (kernels_fluid_CG.CUF) */
+#define LBX_MODEL_CG_DIFFDENS 2 /* colour gradient with two fluid densities (the DIFFDENS build,
+                                 kernels_fluid_CG.CUF:40-49,163-177,539-819): two-pass schedule */
 
 #define LBX_STORE_F32 0  /* FP32 populations (reference storage)            */
 #define LBX_STORE_F16 1  /* FP16 populations shifted by w_l * rho0           */
@@ -106,7 +108,9 @@ typedef struct lbx_params {
   int32_t exact_tiles;    /* 1 (default): a sphere acts on a cell only where the reference's 8x4x4
                              tile lists (makeListAtomsGPU) reach it; for integer radii those lists
                              miss template cells.  0: every cell of the sphere's template box */
-  int32_t reserved[2];
+  float densR, densB;     /* densities of the two fluids for LBX_MODEL_CG_DIFFDENS (namelist
+                             &fluid, main.CUF:343; SetConstants 1047-1083): both > 0, at least
+                             one equal to 1; ignored by the other models (default 1, 1) */
 } lbx_params;
 
 /* Fill the reference defaults for an nx*ny*nz periodic box: CG model, FP32
@@ -254,6 +258,7 @@ int lbx_ensemble_tune(void* ens, int32_t trial, int32_t* chosen, double* best_ms
 /* ---- measurement ------------------------------------------------------- */
 /* Colour-gradient schedule: 2 = lean single-pass kernel (default), 1 = the
  * first single-pass kernel, 0 = two passes (phase field, then collision).
+ * LBX_MODEL_CG_DIFFDENS runs on 0 only (other values: LBX_ERR_ARG).
  * The reference prints Mlup/s from CUDA events around the step loop
  * (main.CUF:274-292); these are the hooks the benchmark uses for the same. */
 int lbx_set_schedule(void* ctx, int32_t fused);

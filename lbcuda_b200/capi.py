@@ -5,7 +5,7 @@ import os
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB_PATH = os.path.join(_HERE, "liblbx.so")
 
-MODEL = {"bgk": 0, "cg": 1}
+MODEL = {"bgk": 0, "cg": 1, "cg-diffdens": 2}
 STORAGE = {"f32": 0, "f16": 1, "bf16": 2, "f64": 3}
 WETTING = {"janus": 0, "neutral": 1}
 
@@ -28,7 +28,7 @@ class LbxParams(C.Structure):
         ("lubric_k", C.c_float), ("lubric_rmin", C.c_float), ("lubric_rcap", C.c_float),
         ("kinematic", C.c_int32), ("closure", C.c_int32),
         ("closure_gap_min", C.c_float), ("closure_gap_max", C.c_float), ("closure_vmax", C.c_float),
-        ("exact_tiles", C.c_int32), ("reserved", C.c_int32 * 2),
+        ("exact_tiles", C.c_int32), ("densR", C.c_float), ("densB", C.c_float),
     ]
 
 

@@ -132,13 +132,19 @@ void lbx_default_params(lbx_params* p, int32_t nx, int32_t ny, int32_t nz) {
   p->closure_gap_max = 1.5f;
   p->closure_vmax = 1.0e-3f;
   p->exact_tiles = 1;
+  p->densR = 1.0f;  // noDIFFDENS values (SetConstants, main.CUF:1065-1066)
+  p->densB = 1.0f;
 }
 
 int lbx_create(const lbx_params* p, void** out) {
   if (!p || !out) return LBX_ERR_ARG;
   *out = nullptr;
   if (p->nx < 3 || p->ny < 3 || p->nz < 3) return LBX_ERR_ARG;
-  if (p->model != LBX_MODEL_BGK && p->model != LBX_MODEL_CG) return LBX_ERR_ARG;
+  if (p->model != LBX_MODEL_BGK && p->model != LBX_MODEL_CG && p->model != LBX_MODEL_CG_DIFFDENS) return LBX_ERR_ARG;
+  // SetConstants, main.CUF:1047-1061: at least one of the two densities is 1
+  if (p->model == LBX_MODEL_CG_DIFFDENS &&
+      (!(p->densR > 0.0f) || !(p->densB > 0.0f) || (p->densR != 1.0f && p->densB != 1.0f)))
+    return LBX_ERR_ARG;
   if (p->storage < LBX_STORE_F32 || p->storage > LBX_STORE_F64) return LBX_ERR_ARG;
   int64_t n = int64_t(p->nx) * p->ny * p->nz;
   if (n >= (int64_t(1) << 31)) return LBX_ERR_ARG;  // 32-bit cell indices
@@ -149,7 +155,9 @@ int lbx_create(const lbx_params* p, void** out) {
   c->ny = p->ny;
   c->nz = p->nz;
   c->n = n;
-  c->ncomp = (p->model == LBX_MODEL_CG) ? 2 : 1;
+  c->ncomp = (p->model == LBX_MODEL_BGK) ? 1 : 2;
+  // the DIFFDENS collision runs on the two-pass schedule only
+  if (p->model == LBX_MODEL_CG_DIFFDENS) c->fused = 0;
   c->storage = p->storage;
   c->elem = (p->storage == LBX_STORE_F32) ? 4 : (p->storage == LBX_STORE_F64 ? 8 : 2);
   int rc = cuda_rc(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
@@ -411,6 +419,7 @@ int lbx_set_schedule(void* ctx, int32_t fused) {
   Ctx* c = as_ctx(ctx);
   if (!c) return LBX_ERR_ARG;
   if (fused < 0 || fused > 2) return LBX_ERR_ARG;
+  if (c->p.model == LBX_MODEL_CG_DIFFDENS && fused != 0) return LBX_ERR_ARG;
   c->fused = fused;
   return 0;
 }

@@ -113,7 +113,21 @@ struct CGConst {
   LatticeT<C> L;
   C inv_viscR, inv_viscB;  // 1/viscR, 1/viscB
   C sigma, beta;
+  // two fluid densities (the DIFFDENS build): densR_d, densB_d, alphaCG_d and
+  // the phi / varphi / psi / xi tables per weight class (dimensions_m.CUF:231-261)
+  C densR, densB;
+  C alpha[2];
+  C phi[3], varphi[3], psi[3], xi[3];
 };
+
+// equilCG, kernels_fluid_CG.CUF:40-49 (component k = 0 R, 1 B), with the
+// velocity-square term hoisted like equil_u
+template <typename C>
+__device__ __forceinline__ C equil_cg(const CGConst<C>& K, C rho, C edu, C usq_term, int k, int l) {
+  const C uv = K.L.inv_cssq * edu;
+  const int c = wclass(l);
+  return rho * (K.phi[c] + K.varphi[c] * K.alpha[k] + K.L.w[c] * (uv + C(0.5) * (uv * uv) - usq_term));
+}
 
 // ---------------------------------------------------------------------------
 // time_step_CG at one fluid cell (kernels_fluid_CG.CUF:689-846).  fR/fB hold
@@ -166,6 +180,110 @@ __device__ __forceinline__ void cg_collide_cell(const CGConst<C>& K, C fR[Q], C 
       C t = coef * cosphi;
       fR[l] = fd * kR + t * feq;
       fB[l] = fd * kB - t * feq;
+    }
+  }
+}
+
+// time_step_CG of the DIFFDENS build at one fluid cell (kernels_fluid_CG.CUF:
+// 689-837 with DIFFDENS): the phase field scaled by the fluid densities, the
+// BGK step towards equilCG plus the viscous correction
+//   viscavg (psi_l u.grad(rho_k) + xi_l (G_k : e_l e_l)),  G_k = u grad(rho_k)^T + its transpose,
+// and the recolouring weighted by equilCG at rest.  psR / psB: D3Q27
+// gradients of the two densities; psi: gradient of the scaled phase field.
+template <typename C>
+__device__ __forceinline__ void cg_collide_cell_dd(const CGConst<C>& K, C fR[Q], C fB[Q], C rhoR, C rhoB, C psix,
+                                                   C psiy, C psiz, const C psR[3], const C psB[3]) {
+  const C ONE = 1, HALF = C(0.5), ZERO = 0;
+  const LatticeT<C>& L = K.L;
+  C rhosum = rhoR + rhoB;
+  C phase_field = (rhoR / K.densR - rhoB / K.densB) / (rhoR / K.densR + rhoB / K.densB);
+  C viscavg = ONE / (HALF * (ONE + phase_field) * K.inv_viscR + HALF * (ONE - phase_field) * K.inv_viscB);
+  C omega = ONE / (viscavg / L.cssq + HALF);
+  C omm = ONE - omega;
+  C invrho = ONE / rhosum;
+  C u = invrho * mx(fR) + invrho * mx(fB);
+  C v = invrho * my(fR) + invrho * my(fB);
+  C w = invrho * mz(fR) + invrho * mz(fB);
+  C usq = L.half_inv_cssq * (u * u + v * v + w * w);
+  const C vpR = u * psR[0] + v * psR[1] + w * psR[2];  // dot_product(myvel, psi_R)
+  const C vpB = u * psB[0] + v * psB[1] + w * psB[2];
+  const C uu[3] = {u, v, w};
+  C gR[3], gB[3];  // diagonal of tensor_product + its transpose
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    gR[i] = uu[i] * psR[i] + uu[i] * psR[i];
+    gB[i] = uu[i] * psB[i] + uu[i] * psB[i];
+  }
+#pragma unroll
+  for (int l = 0; l < Q; ++l) {
+    const int c = wclass(l);
+    const C e = edot(l, u, v, w);
+    const C cx = C(ex(l) * ex(l)), cy = C(ey(l) * ey(l)), cz = C(ez(l) * ez(l));  // cmat_d(i,i,l)
+    const C tR = gR[0] * cx + gR[1] * cy + gR[2] * cz;
+    const C tB = gB[0] * cx + gB[1] * cy + gB[2] * cz;
+    fR[l] = fR[l] * omm + (equil_cg(K, rhoR, e, usq, 0, l) + viscavg * (K.psi[c] * vpR + K.xi[c] * tR)) * omega;
+    fB[l] = fB[l] * omm + (equil_cg(K, rhoB, e, usq, 1, l) + viscavg * (K.psi[c] * vpB + K.xi[c] * tB)) * omega;
+  }
+  C psinorm_sq = psix * psix + psiy * psiy + psiz * psiz;
+  if (psinorm_sq > C(1.e-20)) {
+    C psinorm = sqrt(psinorm_sq);
+    C inv_psq = ONE / psinorm_sq;
+    C acoeff = C(9) / C(4) * omega * K.sigma;
+    C kR = rhoR * invrho, kB = rhoB * invrho;
+    C coef = K.beta * rhoR * rhoB * (invrho * invrho);
+    C inv_t1 = ONE / psinorm;
+    C inv_t2 = ONE / (L.rec[2] * psinorm);
+#pragma unroll
+    for (int l = 0; l < Q; ++l) {
+      C edp = edot(l, psix, psiy, psiz);
+      C temp = psinorm * (L.w[wclass(l)] * (edp * edp) * inv_psq - L.b[wclass(l)]);
+      C fd = fR[l] + fB[l] + acoeff * temp;
+      C feq = equil_cg(K, rhoR, ZERO, ZERO, 0, l) + equil_cg(K, rhoB, ZERO, ZERO, 1, l);
+      C cosphi;
+      if (l == 0) cosphi = C(0);
+      else {
+        C t1 = L.rec[wclass(l)] * psinorm;
+        cosphi = (t1 <= C(1.e-20)) ? C(0) : edp * (wclass(l) == 1 ? inv_t1 : inv_t2);
+      }
+      C t = coef * cosphi;
+      fR[l] = fd * kR + t * feq;
+      fB[l] = fd * kB - t * feq;
+    }
+  }
+}
+
+// DIFFDENS gradients from the neighbours' densities (rho_at returns the pair
+// (rhoR, rhoB) of neighbour (dx, dy, dz)): psi of the scaled phase field and
+// the gradients of the two densities (kernels_fluid_CG.CUF:720-741)
+template <typename C, typename F>
+__device__ __forceinline__ void grad27_dd(const CGConst<C>& K, F&& rho_at, C& psix, C& psiy, C& psiz, C psR[3],
+                                          C psB[3]) {
+  psix = C(0); psiy = C(0); psiz = C(0);
+#pragma unroll
+  for (int i = 0; i < 3; ++i) psR[i] = psB[i] = C(0);
+#pragma unroll
+  for (int l = 1; l < Q27; ++l) {
+    C rs, bs;
+    rho_at(ex27(l), ey27(l), ez27(l), rs, bs);
+    const C ps = (rs / K.densR - bs / K.densB) / (rs / K.densR + bs / K.densB);
+    const C a = K.L.a27[wclass27(l)];
+    if (ex27(l)) {
+      const C ax = ex27(l) > 0 ? a : -a;
+      psix = psix + ax * ps;
+      psR[0] = psR[0] + ax * rs;
+      psB[0] = psB[0] + ax * bs;
+    }
+    if (ey27(l)) {
+      const C ay = ey27(l) > 0 ? a : -a;
+      psiy = psiy + ay * ps;
+      psR[1] = psR[1] + ay * rs;
+      psB[1] = psB[1] + ay * bs;
+    }
+    if (ez27(l)) {
+      const C az = ez27(l) > 0 ? a : -a;
+      psiz = psiz + az * ps;
+      psR[2] = psR[2] + az * rs;
+      psB[2] = psB[2] + az * bs;
     }
   }
 }
@@ -223,6 +341,24 @@ inline CGConst<C> make_cg(const Ctx& c) {
   K.inv_viscB = C(1) / viscB;
   K.sigma = C(c.p.sigma);
   K.beta = C(c.p.beta);
+  // DIFFDENS constants (SetConstants, main.CUF:1047-1083; dimensions_m.CUF:231-261)
+  const bool dd = c.p.model == LBX_MODEL_CG_DIFFDENS;
+  const C ONE = C(1), TWO = C(2), FOUR = C(4), FIVE = C(5), SIX = C(6), EIGHT = C(8), TWELVE = C(12),
+          TWENTYFOUR = C(24);
+  K.densR = dd ? C(c.p.densR) : ONE;
+  K.densB = dd ? C(c.p.densB) : ONE;
+  const C p0 = K.L.w[0];
+  if (K.densR == ONE) {
+    K.alpha[0] = p0;
+    K.alpha[1] = (-ONE + K.alpha[0]) * (K.densR / K.densB) + ONE;
+  } else {  // as the reference writes it (not (1 - alpha_B) densB / densR)
+    K.alpha[1] = p0;
+    K.alpha[0] = (ONE / (-ONE + K.alpha[1])) * (K.densB / K.densR) + ONE;
+  }
+  K.phi[0] = C(0); K.phi[1] = ONE / TWELVE; K.phi[2] = ONE / TWENTYFOUR;
+  K.varphi[0] = ONE; K.varphi[1] = -ONE / TWELVE; K.varphi[2] = -ONE / TWENTYFOUR;
+  K.psi[0] = -FIVE / TWO; K.psi[1] = -ONE / SIX; K.psi[2] = ONE / TWENTYFOUR;
+  K.xi[0] = C(0); K.xi[1] = ONE / FOUR; K.xi[2] = ONE / EIGHT;
   return K;
 }
 

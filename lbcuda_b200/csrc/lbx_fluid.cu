@@ -34,12 +34,14 @@ namespace lbx {
 // ---------------------------------------------------------------------------
 // setupPops (kernels_fluid_CG.CUF:313-346) written in pull convention: the
 // stored buffer holds, at x, the populations that streaming moves to x + e_l,
-// so that the first step gathers exactly the equilibrium of the given fields.
-template <typename S>
+// so that the first step gathers exactly the equilibrium of the given fields
+// (equilCG with two fluid densities, kernels_fluid_CG.CUF:176-178).
+template <typename S, bool DD>
 __global__ void k_set_fields(S* __restrict__ A, S* __restrict__ B, Geom g, int ncomp, const float* __restrict__ rR,
                              const float* __restrict__ rB, float vx, float vy, float vz,
-                             LatticeT<typename Store<S>::C> L, Shift<typename Store<S>::C> sh) {
+                             CGConst<typename Store<S>::C> K, Shift<typename Store<S>::C> sh) {
   using C = typename Store<S>::C;
+  const LatticeT<C>& L = K.L;
   int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y, z = blockIdx.z;
   if (x >= g.nx || y >= g.ny) return;
   Nbr b;
@@ -52,7 +54,7 @@ __global__ void k_set_fields(S* __restrict__ A, S* __restrict__ B, Geom g, int n
 #pragma unroll
     for (int l = 0; l < Q; ++l) {
       C rho = C(r[at(b, ex(l), ey(l), ez(l))]);
-      C val = equil_u(L, rho, edot(l, u, v, w), usq, l);
+      C val = DD ? equil_cg(K, rho, edot(l, u, v, w), usq, comp, l) : equil_u(L, rho, edot(l, u, v, w), usq, l);
       Store<S>::st(A + pidx(g, comp, l, cell), val, sh.at(comp, l));
       Store<S>::st(B + pidx(g, comp, l, cell), C(0), sh.at(comp, l));
     }
@@ -105,11 +107,14 @@ __global__ void __launch_bounds__(256) k_cg_phi(const S* __restrict__ A, Geom g,
 }
 
 // time_step_CG + streaming, two-pass schedule: pull, densities, gradient from
-// the phase-field array, collision, aligned store.
-template <typename S>
+// the phase-field array (DD, two fluid densities: from the density arrays),
+// collision, aligned store.
+template <typename S, bool DD>
 __global__ void __launch_bounds__(256) k_cg_collide(const S* __restrict__ A, S* __restrict__ B, Geom g,
                                                      Shift<typename Store<S>::C> sh,
                                                      const typename Store<S>::C* __restrict__ phi,
+                                                     const typename Store<S>::C* __restrict__ rhoRa,
+                                                     const typename Store<S>::C* __restrict__ rhoBa,
                                                      CGConst<typename Store<S>::C> K) {
   using C = typename Store<S>::C;
   int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y, z = blockIdx.z;
@@ -124,8 +129,21 @@ __global__ void __launch_bounds__(256) k_cg_collide(const S* __restrict__ A, S* 
   if (rR < C(0)) rR = C(0);
   if (rB < C(0)) rB = C(0);
   C psix, psiy, psiz;
-  grad27(K.L, [&](int dx, int dy, int dz) { return __ldg(phi + at(b, dx, dy, dz)); }, psix, psiy, psiz);
-  cg_collide_cell(K, fR, fB, rR, rB, psix, psiy, psiz);
+  if constexpr (DD) {
+    C psR[3], psB[3];
+    grad27_dd(
+        K,
+        [&](int dx, int dy, int dz, C& rs, C& bs) {
+          const int y = at(b, dx, dy, dz);
+          rs = __ldg(rhoRa + y);
+          bs = __ldg(rhoBa + y);
+        },
+        psix, psiy, psiz, psR, psB);
+    cg_collide_cell_dd(K, fR, fB, rR, rB, psix, psiy, psiz, psR, psB);
+  } else {
+    grad27(K.L, [&](int dx, int dy, int dz) { return __ldg(phi + at(b, dx, dy, dz)); }, psix, psiy, psiz);
+    cg_collide_cell(K, fR, fB, rR, rB, psix, psiy, psiz);
+  }
   store_all(B, g, cell, 0, sh, fR);
   store_all(B, g, cell, 1, sh, fB);
 }
@@ -395,8 +413,12 @@ int fluid_set_fields(Ctx& c, const float* d_rR, const float* d_rB, float vx, flo
   return by_storage(c, [&](auto* tag) {
     using S = std::remove_pointer_t<decltype(tag)>;
     using C = typename Store<S>::C;
-    k_set_fields<S><<<d.grid, d.block, 0, c.stream>>>((S*)c.pops[0], (S*)c.pops[1], g, c.ncomp, d_rR, d_rB, vx, vy,
-                                                      vz, make_lattice<C>(), make_shift<C>(c));
+    if (c.p.model == LBX_MODEL_CG_DIFFDENS)
+      k_set_fields<S, true><<<d.grid, d.block, 0, c.stream>>>((S*)c.pops[0], (S*)c.pops[1], g, c.ncomp, d_rR, d_rB,
+                                                              vx, vy, vz, make_cg<C>(c), make_shift<C>(c));
+    else
+      k_set_fields<S, false><<<d.grid, d.block, 0, c.stream>>>((S*)c.pops[0], (S*)c.pops[1], g, c.ncomp, d_rR, d_rB,
+                                                               vx, vy, vz, make_cg<C>(c), make_shift<C>(c));
     return launch_status();
   });
 }
@@ -452,8 +474,14 @@ int fluid_collide_stream(Ctx& c) {
     using S = std::remove_pointer_t<decltype(tag)>;
     using C = typename Store<S>::C;
     kt_begin(c);
-    k_cg_collide<S><<<d.grid, d.block, 0, c.stream>>>((const S*)c.pops[c.cur], (S*)c.pops[1 - c.cur], g,
-                                                      make_shift<C>(c), (const C*)c.phi, make_cg<C>(c));
+    if (c.p.model == LBX_MODEL_CG_DIFFDENS)
+      k_cg_collide<S, true><<<d.grid, d.block, 0, c.stream>>>((const S*)c.pops[c.cur], (S*)c.pops[1 - c.cur], g,
+                                                              make_shift<C>(c), (const C*)c.phi, (const C*)c.rho[0],
+                                                              (const C*)c.rho[1], make_cg<C>(c));
+    else
+      k_cg_collide<S, false><<<d.grid, d.block, 0, c.stream>>>((const S*)c.pops[c.cur], (S*)c.pops[1 - c.cur], g,
+                                                               make_shift<C>(c), (const C*)c.phi, nullptr, nullptr,
+                                                               make_cg<C>(c));
     kt_end(c);
     c.cur = 1 - c.cur;
     return launch_status();

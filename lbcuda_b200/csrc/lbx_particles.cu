@@ -686,7 +686,7 @@ __global__ void __launch_bounds__(256) k_virtual(PDev P, const double* __restric
 
 // time_step_CG with flags (two-pass schedule): collision on fluid cells,
 // the streamed populations pass through unchanged elsewhere.
-template <typename S>
+template <typename S, bool DD>
 __global__ void __launch_bounds__(256) k_collide_p(const S* __restrict__ A, S* B, Geom g,
                                                    Shift<typename Store<S>::C> sh,
                                                    const typename Store<S>::C* __restrict__ phi,
@@ -715,8 +715,21 @@ __global__ void __launch_bounds__(256) k_collide_p(const S* __restrict__ A, S* B
   }
   if (fn == LBX_FLUID_FLUID) {
     C psix, psiy, psiz;
-    grad27(K.L, [&](int dx, int dy, int dz) { return phi[at(b, dx, dy, dz)]; }, psix, psiy, psiz);
-    cg_collide_cell(K, fR, fB, rhoR[cell], rhoB[cell], psix, psiy, psiz);
+    if constexpr (DD) {  // two fluid densities: gradients from the density arrays
+      C psR[3], psB[3];
+      grad27_dd(
+          K,
+          [&](int dx, int dy, int dz, C& rs, C& bs) {
+            const int y = at(b, dx, dy, dz);
+            rs = rhoR[y];
+            bs = rhoB[y];
+          },
+          psix, psiy, psiz, psR, psB);
+      cg_collide_cell_dd(K, fR, fB, rhoR[cell], rhoB[cell], psix, psiy, psiz, psR, psB);
+    } else {
+      grad27(K.L, [&](int dx, int dy, int dz) { return phi[at(b, dx, dy, dz)]; }, psix, psiy, psiz);
+      cg_collide_cell(K, fR, fB, rhoR[cell], rhoB[cell], psix, psiy, psiz);
+    }
   }
   store_all(B, g, cell, 0, sh, fR);
   store_all(B, g, cell, 1, sh, fB);
@@ -1612,9 +1625,16 @@ int particles_fluid(Ctx& c) {
     using S = std::remove_pointer_t<decltype(tag)>;
     using C = typename Store<S>::C;
     kt_begin(c);
-    k_collide_p<S><<<d.grid, d.block, 0, c.stream>>>((const S*)c.pops[c.cur], (S*)c.pops[1 - c.cur], g,
-                                                     make_shift<C>(c), (const C*)c.phi, (const C*)c.rho[0],
-                                                     (const C*)c.rho[1], c.flags[fo], c.flags[fn], make_cg<C>(c));
+    if (c.p.model == LBX_MODEL_CG_DIFFDENS)
+      k_collide_p<S, true><<<d.grid, d.block, 0, c.stream>>>((const S*)c.pops[c.cur], (S*)c.pops[1 - c.cur], g,
+                                                             make_shift<C>(c), (const C*)c.phi, (const C*)c.rho[0],
+                                                             (const C*)c.rho[1], c.flags[fo], c.flags[fn],
+                                                             make_cg<C>(c));
+    else
+      k_collide_p<S, false><<<d.grid, d.block, 0, c.stream>>>((const S*)c.pops[c.cur], (S*)c.pops[1 - c.cur], g,
+                                                              make_shift<C>(c), (const C*)c.phi, (const C*)c.rho[0],
+                                                              (const C*)c.rho[1], c.flags[fo], c.flags[fn],
+                                                              make_cg<C>(c));
     kt_end(c);
     return launch_status();
   });

@@ -173,8 +173,12 @@ def _grid(nx, ny, nz):
     return i.astype(np.float32), j.astype(np.float32), k.astype(np.float32)
 
 
-def initial_fields(init_type, nx, ny, nz, seed=0, path="."):
-    """(rhoR, rhoB) of initType 1, 2, 3, 5, 6 as float32 (nz, ny, nx) arrays."""
+def initial_fields(init_type, nx, ny, nz, seed=0, path=".", dens=None):
+    """(rhoR, rhoB) of initType 1, 2, 3, 5, 6 as float32 (nz, ny, nx) arrays.
+
+    dens = (densR, densB) for the two-density model: the droplet of initType
+    1 then carries densR inside and densB outside (setup2 with DIFFDENS,
+    kernels_fluid_CG.CUF:163-169); the other types ignore it, as there."""
     f = np.float32
     if init_type == 1:  # setup2: droplet of radius glz/8 at the centre
         i, j, k = _grid(nx, ny, nz)
@@ -184,6 +188,8 @@ def initial_fields(init_type, nx, ny, nz, seed=0, path="."):
         dz = k - f(nz // 2 + 0.5)
         r = np.sqrt(dx * dx + dy * dy + dz * dz).astype(f)
         t = _fcut(r, radius, radius + f(0.1))
+        if dens is not None:
+            return (t * f(dens[0])).astype(f), ((f(1.0) - t) * f(dens[1])).astype(f)
         return t, (f(1.0) - t).astype(f)
     if init_type == 2:  # setup2_zplanes: blue between glz/8 and 5glz/8
         i, j, k = _grid(nx, ny, nz)

@@ -46,7 +46,7 @@ class LBSim:
     def __init__(self, params):
         self.params = params
         self.nx, self.ny, self.nz = params.nx, params.ny, params.nz
-        self.ncomp = 2 if params.model == capi.MODEL["cg"] else 1
+        self.ncomp = 1 if params.model == capi.MODEL["bgk"] else 2
         self._L = capi.lib()
         h = C.c_void_p()
         check(self._L.lbx_create(C.byref(params), C.byref(h)), "lbx_create")

@@ -56,6 +56,7 @@ const int EZ27[Q27] = {0, 0, 0, 0, 0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1,
 template <typename T>
 struct Tables {
   T p[Q], b_l[Q], rec_fact[Q], a27[Q27], p27[Q27];
+  T phi[Q], varphi[Q], psi[Q], xi[Q]; /* DIFFDENS tables, dimensions_m.CUF:231-261 */
   T cssq;
   Tables() {
     /* all arithmetic in T, in the order the Fortran parameter expressions use */
@@ -79,6 +80,18 @@ struct Tables {
       p27[l] = w;
       a27[l] = (l == 0) ? T(0) : w / cssq;                        /* :292-298 */
     }
+    const T FOUR = 4, FIVE = 5, EIGHT = 8;
+    for (int l = 0; l < Q; ++l) {
+      const int c = (l == 0) ? 0 : (l <= 6 ? 1 : 2);
+      const T ph[3] = {T(0), ONE / TWELVE, ONE / TWENTYFOUR};
+      const T vph[3] = {ONE, -ONE / TWELVE, -ONE / TWENTYFOUR};
+      const T ps[3] = {-FIVE / TWO, -ONE / SIX, ONE / TWENTYFOUR};
+      const T x[3] = {T(0), ONE / FOUR, ONE / EIGHT};
+      phi[l] = ph[c];
+      varphi[l] = vph[c];
+      psi[l] = ps[c];
+      xi[l] = x[c];
+    }
   }
 };
 
@@ -88,6 +101,14 @@ inline T equil(const Tables<T>& tb, T rho, T u, T v, T w, int l) {
   const T ONE = 1, HALF = T(0.5);
   T uv = (ONE / tb.cssq) * (u * T(EX[l]) + v * T(EY[l]) + w * T(EZ[l]));
   return rho * tb.p[l] * (ONE + uv + HALF * (uv * uv) - (HALF / tb.cssq) * (u * u + v * v + w * w));
+}
+
+/* equilCG, kernels_fluid_CG.CUF:40-49 (alpha = alphaCG_d(k)) */
+template <typename T>
+inline T equil_cg(const Tables<T>& tb, T rho, T u, T v, T w, T alpha, int l) {
+  const T HALF = T(0.5);
+  T uv = (T(1) / tb.cssq) * (u * T(EX[l]) + v * T(EY[l]) + w * T(EZ[l]));
+  return rho * (tb.phi[l] + tb.varphi[l] * alpha + tb.p[l] * (uv + HALF * (uv * uv) - (HALF / tb.cssq) * (u * u + v * v + w * w)));
 }
 
 template <typename T>
@@ -113,13 +134,15 @@ class Oracle {
   int64_t err_where = 0;
   /* physical constants as the reference derives them (SetConstants) */
   T viscR, viscB, omega_bgk;
+  bool diffdens = false; /* LBX_MODEL_CG_DIFFDENS: the reference's DIFFDENS build */
+  T densR = 1, densB = 1, alphaCG[2] = {0, 0};
 
   Oracle(const lbx_params& p) : prm(p) {
     nx = p.nx; ny = p.ny; nz = p.nz;
     sx = nx + 2; sy = ny + 2; sz = nz + 2;
     ncell_pad = int64_t(sx) * sy * sz;
     model = p.model;
-    int ncomp = (model == LBX_MODEL_CG) ? 2 : 1;
+    int ncomp = (model != LBX_MODEL_BGK) ? 2 : 1;
     for (int c = 0; c < ncomp; ++c)
       for (int b = 0; b < 2; ++b) pops[c][b].assign(size_t(Q) * ncell_pad, T(0));
     for (int c = 0; c < 2; ++c) rho[c].assign(ncell_pad, T(0));
@@ -128,6 +151,18 @@ class Oracle {
     viscR = tb.cssq * (T(p.tauR) - HALF); /* main.CUF:1069-1071 */
     viscB = tb.cssq * (T(p.tauB) - HALF);
     omega_bgk = T(1) / T(p.tau);
+    /* SetConstants, main.CUF:1047-1083 */
+    diffdens = (model == LBX_MODEL_CG_DIFFDENS);
+    const T ONE = 1;
+    densR = diffdens ? T(p.densR) : ONE;
+    densB = diffdens ? T(p.densB) : ONE;
+    if (densR == ONE) {
+      alphaCG[0] = tb.p[0];
+      alphaCG[1] = (-ONE + alphaCG[0]) * (densR / densB) + ONE;
+    } else {
+      alphaCG[1] = tb.p[0];
+      alphaCG[0] = (ONE / (-ONE + alphaCG[1])) * (densB / densR) + ONE;
+    }
   }
 
   inline int64_t id(int i, int j, int k) const { return i + int64_t(sx) * (j + int64_t(sy) * k); }
@@ -156,7 +191,7 @@ class Oracle {
         }
   }
   void halo_pops(int b) {
-    int ncomp = (model == LBX_MODEL_CG) ? 2 : 1;
+    int ncomp = (model != LBX_MODEL_BGK) ? 2 : 1;
     for_halo([&](int64_t h, int64_t s) {
       for (int c = 0; c < ncomp; ++c)
         for (int l = 1; l < Q; ++l) f(c, b, l, h) = f(c, b, l, s);
@@ -171,7 +206,7 @@ class Oracle {
 
   /* ---- initial conditions: setupPops, kernels_fluid_CG.CUF:313-346 ------------- */
   void set_fields(const float* rR, const float* rB, float vx, float vy, float vz) {
-    int ncomp = (model == LBX_MODEL_CG) ? 2 : 1;
+    int ncomp = (model != LBX_MODEL_BGK) ? 2 : 1;
     flip = 0;
     step = 0;
     for (int c = 0; c < ncomp; ++c)
@@ -187,6 +222,11 @@ class Oracle {
           rho[0][x] = r0;
           rho[1][x] = r1;
           for (int l = 0; l < Q; ++l) {
+            if (diffdens) { /* setup2, kernels_fluid_CG.CUF:176-178 */
+              f(0, 0, l, x) = equil_cg(tb, r0, T(vx), T(vy), T(vz), alphaCG[0], l);
+              f(1, 0, l, x) = equil_cg(tb, r1, T(vx), T(vy), T(vz), alphaCG[1], l);
+              continue;
+            }
             f(0, 0, l, x) = equil(tb, r0, T(vx), T(vy), T(vz), l);
             if (ncomp == 2) f(1, 0, l, x) = equil(tb, r1, T(vx), T(vy), T(vz), l);
           }
@@ -201,7 +241,7 @@ class Oracle {
   }
 
   void set_pops(const float* pR, const float* pB) {
-    int ncomp = (model == LBX_MODEL_CG) ? 2 : 1;
+    int ncomp = (model != LBX_MODEL_BGK) ? 2 : 1;
     flip = 0;
     step = 0;
     int64_t n = int64_t(nx) * ny * nz;
@@ -252,12 +292,12 @@ class Oracle {
   static inline T mom_y(const T* q, T inv) { return inv * (q[3] - q[4] + q[7] - q[8] + q[9] - q[10] + q[15] - q[16] - q[17] + q[18]); }
   static inline T mom_z(const T* q, T inv) { return inv * (q[5] - q[6] + q[11] - q[12] + q[13] - q[14] + q[15] - q[16] + q[17] - q[18]); }
 
-  /* ---- time_step_CG, kernels_fluid_CG.CUF:531-848 (noDIFFDENS, HIGHGRAD) ------ */
+  /* ---- time_step_CG, kernels_fluid_CG.CUF:531-848 (HIGHGRAD; DIFFDENS when
+   * the model is LBX_MODEL_CG_DIFFDENS) --------------------------------------- */
   void time_step_cg() {
     const T ONE = 1, HALF = T(0.5), ZERO = 0, NINE = 9, FOUR = 4;
     const T mylimit = T(1.e-20);
     const T sigma = T(prm.sigma), beta = T(prm.beta);
-    const T densR = 1, densB = 1; /* noDIFFDENS: SetConstants main.CUF:1062-1067 */
     const int b = flip;
 #pragma omp parallel for schedule(static)
     for (int k = 1; k <= nz; ++k)
@@ -278,6 +318,7 @@ class Oracle {
           T v = mom_y(tR, invrho) + mom_y(tB, invrho);
           T w = mom_z(tR, invrho) + mom_z(tB, invrho);
           T psix = ZERO, psiy = ZERO, psiz = ZERO;
+          T psR[3] = {ZERO, ZERO, ZERO}, psB[3] = {ZERO, ZERO, ZERO};
           for (int l = 1; l < Q27; ++l) { /* HIGHGRAD, :720-741 */
             int64_t y = id(i + EX27[l], j + EY27[l], k + EZ27[l]);
             T rs = rho[0][y], bs = rho[1][y];
@@ -285,9 +326,40 @@ class Oracle {
             psix = psix + tb.a27[l] * T(EX27[l]) * ps;
             psiy = psiy + tb.a27[l] * T(EY27[l]) * ps;
             psiz = psiz + tb.a27[l] * T(EZ27[l]) * ps;
+            if (diffdens) {
+              psR[0] = psR[0] + tb.a27[l] * T(EX27[l]) * rs;
+              psR[1] = psR[1] + tb.a27[l] * T(EY27[l]) * rs;
+              psR[2] = psR[2] + tb.a27[l] * T(EZ27[l]) * rs;
+              psB[0] = psB[0] + tb.a27[l] * T(EX27[l]) * bs;
+              psB[1] = psB[1] + tb.a27[l] * T(EY27[l]) * bs;
+              psB[2] = psB[2] + tb.a27[l] * T(EZ27[l]) * bs;
+            }
           }
-          for (int l = 0; l < Q; ++l) tR[l] = tR[l] * oneminusomega + equil(tb, rhoR, u, v, w, l) * omega;
-          for (int l = 0; l < Q; ++l) tB[l] = tB[l] * oneminusomega + equil(tb, rhoB, u, v, w, l) * omega;
+          if (diffdens) { /* :743-786 */
+            const T vel[3] = {u, v, w};
+            T vR = vel[0] * psR[0] + vel[1] * psR[1] + vel[2] * psR[2];
+            T vB = vel[0] * psB[0] + vel[1] * psB[1] + vel[2] * psB[2];
+            T gR[3], gB[3]; /* diagonal of tensor_product(myvel, psi) + transpose */
+            for (int d = 0; d < 3; ++d) {
+              gR[d] = vel[d] * psR[d] + vel[d] * psR[d];
+              gB[d] = vel[d] * psB[d] + vel[d] * psB[d];
+            }
+            for (int l = 0; l < Q; ++l) {
+              const T cm[3] = {T(EX[l] * EX[l]), T(EY[l] * EY[l]), T(EZ[l] * EZ[l])}; /* cmat_d(d,d,l) */
+              T tc = gR[0] * cm[0] + gR[1] * cm[1] + gR[2] * cm[2];
+              tR[l] = tR[l] * oneminusomega +
+                      (equil_cg(tb, rhoR, u, v, w, alphaCG[0], l) + viscavg * (tb.psi[l] * vR + tb.xi[l] * tc)) * omega;
+            }
+            for (int l = 0; l < Q; ++l) {
+              const T cm[3] = {T(EX[l] * EX[l]), T(EY[l] * EY[l]), T(EZ[l] * EZ[l])};
+              T tc = gB[0] * cm[0] + gB[1] * cm[1] + gB[2] * cm[2];
+              tB[l] = tB[l] * oneminusomega +
+                      (equil_cg(tb, rhoB, u, v, w, alphaCG[1], l) + viscavg * (tb.psi[l] * vB + tb.xi[l] * tc)) * omega;
+            }
+          } else {
+            for (int l = 0; l < Q; ++l) tR[l] = tR[l] * oneminusomega + equil(tb, rhoR, u, v, w, l) * omega;
+            for (int l = 0; l < Q; ++l) tB[l] = tB[l] * oneminusomega + equil(tb, rhoB, u, v, w, l) * omega;
+          }
           T psinorm_sq = psix * psix + psiy * psiy + psiz * psiz;
           if (psinorm_sq > mylimit) { /* perturbation + recolouring, :803-837 */
             T psinorm = std::sqrt(psinorm_sq);
@@ -298,7 +370,9 @@ class Oracle {
               fd[l] = tR[l] + tB[l] + acoeff * temp;
             }
             for (int l = 0; l < Q; ++l) {
-              T feq = equil(tb, rhoR, ZERO, ZERO, ZERO, l) + equil(tb, rhoB, ZERO, ZERO, ZERO, l);
+              T feq = diffdens ? equil_cg(tb, rhoR, ZERO, ZERO, ZERO, alphaCG[0], l) +
+                                     equil_cg(tb, rhoB, ZERO, ZERO, ZERO, alphaCG[1], l)
+                               : equil(tb, rhoR, ZERO, ZERO, ZERO, l) + equil(tb, rhoB, ZERO, ZERO, ZERO, l);
               T edp = T(EX[l]) * psix + T(EY[l]) * psiy + T(EZ[l]) * psiz;
               T temp1 = tb.rec_fact[l] * psinorm;
               T cosphi = (temp1 <= mylimit) ? ZERO : edp / temp1;
@@ -340,7 +414,7 @@ class Oracle {
   /* ---- flipflop*Pop0_CG + stream*_CG + stream_CG_x/_y/_z, CG.CUF:851-1141 ---- */
   void stream() {
     const int b = flip, o = 1 - flip;
-    int ncomp = (model == LBX_MODEL_CG) ? 2 : 1;
+    int ncomp = (model != LBX_MODEL_BGK) ? 2 : 1;
     /* interior pushes; each target is written by exactly one source, so the
      * k-parallel loop is race-free */
 #pragma omp parallel for schedule(static)
@@ -1101,7 +1175,7 @@ class Oracle {
   void do_step() {
     if (np > 0) { do_step_particles(); return; }
     step += 1;
-    if (model == LBX_MODEL_CG) {
+    if (model != LBX_MODEL_BGK) {
       init_rho();
       time_step_cg();
     } else {
@@ -1118,7 +1192,7 @@ class Oracle {
     const int b = flip;
     const int bf = last_flags;
     const T ONE = 1, MINDENS = 0;
-    int ncomp = (model == LBX_MODEL_CG) ? 2 : 1;
+    int ncomp = (model != LBX_MODEL_BGK) ? 2 : 1;
     int64_t n = int64_t(nx) * ny * nz;
 #pragma omp parallel for schedule(static)
     for (int k = 1; k <= nz; ++k)
@@ -1152,7 +1226,7 @@ class Oracle {
 
   void get_pops(double* pR, double* pB) {
     const int b = flip;
-    int ncomp = (model == LBX_MODEL_CG) ? 2 : 1;
+    int ncomp = (model != LBX_MODEL_BGK) ? 2 : 1;
     int64_t n = int64_t(nx) * ny * nz;
 #pragma omp parallel for schedule(static)
     for (int k = 1; k <= nz; ++k)
@@ -1254,7 +1328,7 @@ int orc_status(void* h, int* code, int* step, int64_t* where) {
 }
 int orc_set_particles(void* h, int n, const double* x, const double* v, const double* om, const double* q) {
   return dispatch(h, [&](auto& o) {
-    if (o.model != LBX_MODEL_CG || n < 1) return int(LBX_ERR_ARG);
+    if (o.model == LBX_MODEL_BGK || n < 1) return int(LBX_ERR_ARG);
     if (o.nx % 8 || o.ny % 4 || o.nz % 4) return int(LBX_ERR_ARG); /* reference tile 8x4x4 */
     o.set_particles(n, x, v, om, q);
     return o.err_code;

@@ -61,7 +61,7 @@ class OracleSim:
     def __init__(self, params, mode="ref"):
         self.params = params
         self.nx, self.ny, self.nz = params.nx, params.ny, params.nz
-        self.ncomp = 2 if params.model == 1 else 1
+        self.ncomp = 1 if params.model == 0 else 2
         self._L = lib()
         self._h = self._L.orc_create(C.byref(params), MODES[mode])
         if not self._h:
