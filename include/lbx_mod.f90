@@ -22,7 +22,7 @@ module lbx_mod
   use iso_c_binding
   implicit none
 
-  integer(c_int32_t), parameter :: LBX_MODEL_BGK = 0, LBX_MODEL_CG = 1
+  integer(c_int32_t), parameter :: LBX_MODEL_BGK = 0, LBX_MODEL_CG = 1, LBX_MODEL_CG_DIFFDENS = 2
   integer(c_int32_t), parameter :: LBX_STORE_F32 = 0, LBX_STORE_F16 = 1, LBX_STORE_BF16 = 2, LBX_STORE_F64 = 3
   integer(c_int32_t), parameter :: LBX_WET_JANUS = 0, LBX_WET_NEUTRAL = 1
 
@@ -38,7 +38,7 @@ module lbx_mod
     integer(c_int32_t) :: kinematic, closure
     real(c_float) :: closure_gap_min, closure_gap_max, closure_vmax
     integer(c_int32_t) :: exact_tiles
-    integer(c_int32_t) :: reserved(2)
+    real(c_float) :: densR, densB   ! namelist &fluid (DIFFDENS build)
   end type lbx_params
 
   interface

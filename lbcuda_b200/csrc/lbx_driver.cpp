@@ -201,7 +201,10 @@ bool read_fortran_field(const char* path, int nx, int ny, int nz, float* out) {
 }
 
 // initial densities of initType 1, 2, 3, 5, 6 (setupRho_Pops, main.CUF:2531-2608)
-bool initial_fields(int type, int nx, int ny, int nz, unsigned seed, std::vector<float>& R, std::vector<float>& B) {
+// densR / densB: the two-density model's droplet (setup2 with DIFFDENS,
+// kernels_fluid_CG.CUF:163-169); 1, 1 otherwise
+bool initial_fields(int type, int nx, int ny, int nz, unsigned seed, std::vector<float>& R, std::vector<float>& B,
+                    float densR = 1.f, float densB = 1.f) {
   size_t n = size_t(nx) * ny * nz;
   R.assign(n, 0.f);
   B.assign(n, 0.f);
@@ -229,6 +232,10 @@ bool initial_fields(int type, int nx, int ny, int nz, unsigned seed, std::vector
         }
         R[h] = t;
         B[h] = 1.f - t;
+        if (type == 1) {
+          R[h] = t * densR;
+          B[h] = (1.f - t) * densB;
+        }
       }
   return true;
 }
@@ -301,6 +308,11 @@ int main(int argc, char** argv) {
       std::string t = nxt();
       p.storage = t == "f16" ? LBX_STORE_F16 : t == "bf16" ? LBX_STORE_BF16 : t == "f64" ? LBX_STORE_F64 : LBX_STORE_F32;
     } else if (s == "--bgk") p.model = LBX_MODEL_BGK;
+    else if (s == "--diffdens") {  // two fluid densities: --diffdens densR densB
+      p.model = LBX_MODEL_CG_DIFFDENS;
+      p.densR = float(std::atof(nxt()));
+      p.densB = float(std::atof(nxt()));
+    }
     else if (s == "--sigma") p.sigma = std::atof(nxt());
     else if (s == "--beta") p.beta = std::atof(nxt());
     else if (s == "--tau") p.tau = std::atof(nxt());
@@ -326,7 +338,7 @@ int main(int argc, char** argv) {
     for (int k = 0; k < 3; ++k) { p.ext_force[k] = d.ext_f[k]; p.ext_torque[k] = d.ext_t[k]; }
   }
   std::vector<float> R, B;
-  if (!initial_fields(d.initType, nx, ny, nz, seed, R, B)) return 2;
+  if (!initial_fields(d.initType, nx, ny, nz, seed, R, B, p.densR, p.densB)) return 2;
   void* ctx = nullptr;
   if (check(lbx_create(&p, &ctx), "lbx_create")) return 1;
   if (check(lbx_set_fields(ctx, R.data(), B.data(), d.vx, d.vy, d.vz), "lbx_set_fields")) return 1;

@@ -2,6 +2,9 @@
 
 * :func:`read_input_dat`  — the positional ``input.dat`` of readParameters
   (main.CUF:409-496), with the same validation and messages;
+* :func:`read_namelist_input` — the namelist deck of the NEWINPUT build
+  (groups &simulation, &fluid, &particle; main.CUF:341-345, 356-408), the
+  only input that carries the two fluid densities densR / densB;
 * :func:`read_input_xyz`  — ``input.xyz`` of read_input_atom
   (main.CUF:1230-1350), Euler angles -> quaternion by eul2q
   (main.CUF:1352-1370) with the reference's (eul1, eul3, eul2) argument order;
@@ -107,6 +110,67 @@ def read_input_dat(path):
         if wp and found < 9: msgs.append("lrotate not found")
         if lr and found < 10: msgs.append("ext_tqx,ext_tqy,ext_tqz not found")
         raise InputError("; ".join(msgs) or "input.dat incomplete")
+    return out
+
+
+_NAMELIST_GROUPS = {
+    "simulation": ("nIter", "nIterOut", "nIterVTK", "initType"),
+    "fluid": ("vx", "vy", "vz", "densR", "densB", "tauR", "tauB"),
+    "particle": ("withParticles", "numAtoms", "lrotate", "ext_fxx", "ext_fyy", "ext_fzz", "ext_tqx", "ext_tqy",
+                 "ext_tqz", "max_vel"),
+}
+
+
+def _namelist_value(text):
+    t = text.strip().rstrip(",").strip()
+    low = t.lower()
+    if low in (".true.", "t", ".t.", "true"):
+        return True
+    if low in (".false.", "f", ".f.", "false"):
+        return False
+    try:
+        return int(t)
+    except ValueError:
+        return float(t.lower().replace("d", "e"))
+
+
+def read_namelist_input(path):
+    """Read the namelist deck of the NEWINPUT build (main.CUF:341-345, 356-408).
+
+    The three groups are read in order (simulation, fluid, particle) with
+    list-directed namelist syntax: ``&group``, ``name=value`` entries
+    (several per line allowed, ``!`` comments), closed by ``/`` or ``&end``.
+    Names are matched without regard to case, as Fortran does; a name that
+    is not in its group raises InputError, as a namelist read fails.
+    Returns one dict of every name given (values int, float or bool); names
+    not given keep the caller's defaults (the reference initialises them
+    before the read: main.CUF:346-354).
+    """
+    with open(path) as fh:
+        text = fh.read()
+    out = {}
+    pos = 0
+    low = text.lower()
+    for group, names in _NAMELIST_GROUPS.items():
+        start = low.find("&" + group, pos)
+        if start < 0:
+            raise InputError(f"namelist group &{group} not found in {path}")
+        body_start = start + 1 + len(group)
+        ends = [e for e in (low.find("&end", body_start), low.find("/", body_start)) if e >= 0]
+        if not ends:
+            raise InputError(f"namelist group &{group} is not closed")
+        end = min(ends)
+        body = "\n".join(line.split("!")[0] for line in text[body_start:end].splitlines())
+        canon = {n.lower(): n for n in names}
+        for item in body.replace(",", " ").split():
+            if "=" not in item:
+                continue
+            key, _, val = item.partition("=")
+            key = key.strip().lower()
+            if key not in canon:
+                raise InputError(f"{key} is not in namelist &{group}")
+            out[canon[key]] = _namelist_value(val)
+        pos = end
     return out
 
 

@@ -2,7 +2,8 @@
 
     python tests/golden/make_decks.py /path/to/LBcuda
 
-The decks (Tests/*/input.dat, the small input.xyz files and the first 1280
+The decks (Tests/*/input.dat, the namelist deck Tests/CPC_Tab2_128/newinput.dat
+of the NEWINPUT build, the small input.xyz files and the first 1280
 particles of Tests/07-1280-Particle/input.xyz.256cube.5000.r5.5) are data the
 reference ships for its runs; the tests parse them with the host-side input
 readers and check the parser's verdicts (the stale 8-line decks 02-06 must be
@@ -22,6 +23,8 @@ def main(ref):
     for d in DECKS:
         src = os.path.join(ref, "Tests", d, "input.dat")
         shutil.copy(src, os.path.join(out, f"{d}.input.dat"))
+    shutil.copy(os.path.join(ref, "Tests", "CPC_Tab2_128", "newinput.dat"),
+                os.path.join(out, "CPC_Tab2_128.newinput.dat"))
     for d in ["05-1Particle", "06-12_Particle"]:
         shutil.copy(os.path.join(ref, "Tests", d, "input.xyz"), os.path.join(out, f"{d}.input.xyz"))
     for f in ["input_3a.dat", "input_3b.dat", "input_3c.dat"]:

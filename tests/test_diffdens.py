@@ -157,3 +157,34 @@ def test_diffdens_arguments():
         g.set_schedule(2)  # the two-density collision runs on the two-pass schedule
     g.set_schedule(0)
     g.close()
+
+
+def test_namelist_deck_gives_the_densities(tmp_path):
+    """The namelist deck (NEWINPUT build) is where densR / densB come from."""
+    from lbcuda_b200.inputs import InputError, read_namelist_input
+    deck = tmp_path / "deck.dat"
+    deck.write_text("&simulation\nnIter=200   ! steps\nnIterOut=20\nnIterVTK=100\ninitType=1\n&end\n"
+                    "&fluid\nDENSR=2.0\ndensB=1.0\nvx=0.0, vy=0.01, vz=0.0\ntauR=1.0\ntauB=1.0\n&end\n"
+                    "&particle\nwithParticles=.false.\nnumAtoms=1\nlrotate=.false.\nmax_vel=1.0\n/\n")
+    d = read_namelist_input(deck)
+    assert d["densR"] == 2.0 and d["densB"] == 1.0 and d["vy"] == 0.01 and d["initType"] == 1
+    assert d["withParticles"] is False and d["nIter"] == 200
+    p = dd_params(16, d["densR"], d["densB"], tauR=d["tauR"], tauB=d["tauB"])
+    assert p.densR == 2.0 and p.model == 2
+    bad = tmp_path / "bad.dat"
+    bad.write_text("&simulation\nnIter=1\nbogus=3\n&end\n&fluid\n&end\n&particle\n&end\n")
+    with pytest.raises(InputError):
+        read_namelist_input(bad)
+
+
+def test_reference_namelist_deck():
+    """The reference's own namelist deck (Tests/CPC_Tab2_128/newinput.dat):
+    a droplet (initType 1) of density 2 in a fluid of density 1."""
+    import os
+    from lbcuda_b200.inputs import read_namelist_input
+    deck = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "decks", "CPC_Tab2_128.newinput.dat")
+    d = read_namelist_input(deck)
+    assert (d["densR"], d["densB"]) == (2.0, 1.0)
+    assert d["initType"] == 1 and d["withParticles"] is False
+    assert (d["nIter"], d["nIterOut"]) == (5000, 500)
+    assert (d["tauR"], d["tauB"]) == (1.0, 1.0)
