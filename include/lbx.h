@@ -40,6 +40,11 @@ extern "C" {
 #define LBX_MODEL_CG 1  /* two-component colour gradient (kernels_fluid_CG.CUF) */
 #define LBX_MODEL_CG_DIFFDENS 2 /* colour gradient with two fluid densities (the DIFFDENS build,
                                  kernels_fluid_CG.CUF:40-49,163-177,539-819): two-pass schedule */
+#define LBX_MODEL_CG_D3Q27 3    /* colour gradient on the D3Q27 lattice (the D3Q27 build,
+                                   dimensions_m.CUF:117-198): 27 populations per component,
+                                   two-pass schedule, no spheres (the reference's bounce-back is
+                                   D3Q19 only, kernels_fluid_PART.CUF:1929-1941) */
+#define LBX_MODEL_CG_DIFFDENS_D3Q27 4 /* both builds together */
 
 #define LBX_STORE_F32 0  /* FP32 populations (reference storage)            */
 #define LBX_STORE_F16 1  /* FP16 populations shifted by w_l * rho0           */

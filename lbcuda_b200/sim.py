@@ -4,7 +4,8 @@ It plays the role of the reference's Fortran host for the hot path
 (main.CUF:125-308): it owns one ``lbx`` context, sets the initial fields,
 advances steps and reads moments back.  All arrays crossing the boundary are
 numpy arrays in the reference's Fortran layout (x fastest): a field is
-``(nz, ny, nx)`` in C order, populations ``(Q, nz, ny, nx)``.
+``(nz, ny, nx)`` in C order, populations ``(q, nz, ny, nx)`` (q = 19, or 27 for
+the D3Q27 models).
 """
 import ctypes as C
 
@@ -47,6 +48,7 @@ class LBSim:
         self.params = params
         self.nx, self.ny, self.nz = params.nx, params.ny, params.nz
         self.ncomp = 1 if params.model == capi.MODEL["bgk"] else 2
+        self.q = 27 if params.model in (capi.MODEL["cg-d3q27"], capi.MODEL["cg-diffdens-d3q27"]) else Q
         self._L = capi.lib()
         h = C.c_void_p()
         check(self._L.lbx_create(C.byref(params), C.byref(h)), "lbx_create")
@@ -82,8 +84,8 @@ class LBSim:
               "lbx_set_fields")
 
     def set_pops(self, popsR, popsB=None):
-        pR = np.ascontiguousarray(popsR, dtype=np.float32).reshape((Q,) + self.shape)
-        pB = None if popsB is None else np.ascontiguousarray(popsB, dtype=np.float32).reshape((Q,) + self.shape)
+        pR = np.ascontiguousarray(popsR, dtype=np.float32).reshape((self.q,) + self.shape)
+        pB = None if popsB is None else np.ascontiguousarray(popsB, dtype=np.float32).reshape((self.q,) + self.shape)
         check(self._L.lbx_set_pops(self._h, _fptr(pR), _fptr(pB)), "lbx_set_pops")
 
     def set_particles(self, x, v=None, omega=None, q=None):
@@ -149,8 +151,8 @@ class LBSim:
         return rR, rB, vel, ph
 
     def get_pops(self):
-        pR = np.empty((Q,) + self.shape, np.float32)
-        pB = np.empty((Q,) + self.shape, np.float32)
+        pR = np.empty((self.q,) + self.shape, np.float32)
+        pB = np.empty((self.q,) + self.shape, np.float32)
         check(self._L.lbx_get_pops(self._h, _fptr(pR), _fptr(pB)), "lbx_get_pops")
         return pR, (pB if self.ncomp == 2 else None)
 

@@ -45,52 +45,66 @@ constexpr int Q = 19;
 constexpr int Q27 = 27;
 
 /* ---- lattice tables, dimensions_m.CUF:201-300 (D3Q19, noD3Q27) ------------- */
-const int EX[Q] = {0, 1, -1, 0, 0, 0, 0, 1, -1, -1, 1, 1, -1, -1, 1, 0, 0, 0, 0};
-const int EY[Q] = {0, 0, 0, 1, -1, 0, 0, 1, -1, 1, -1, 0, 0, 0, 0, 1, -1, -1, 1};
-const int EZ[Q] = {0, 0, 0, 0, 0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1};
+/* directions 0..18 are D3Q19; the D3Q27 build (dimensions_m.CUF:117-198)
+ * appends the eight corners 19..26 in the same table order */
+const int EX[Q27] = {0, 1, -1, 0, 0, 0, 0, 1, -1, -1, 1, 1, -1, -1, 1, 0, 0, 0, 0, 1, -1, 1, -1, -1, 1, 1, -1};
+const int EY[Q27] = {0, 0, 0, 1, -1, 0, 0, 1, -1, 1, -1, 0, 0, 0, 0, 1, -1, -1, 1, 1, -1, 1, -1, 1, -1, -1, 1};
+const int EZ[Q27] = {0, 0, 0, 0, 0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1, 1, -1, -1, 1, 1, -1, 1, -1};
 /* D3Q27 neighbour set used by HIGHGRAD and the belts, dimensions_m.CUF:275-281 */
 const int EX27[Q27] = {0, 1, -1, 0, 0, 0, 0, 1, -1, -1, 1, 1, -1, -1, 1, 0, 0, 0, 0, 1, -1, 1, -1, -1, 1, 1, -1};
 const int EY27[Q27] = {0, 0, 0, 1, -1, 0, 0, 1, -1, 1, -1, 0, 0, 0, 0, 1, -1, -1, 1, 1, -1, 1, -1, 1, -1, -1, 1};
 const int EZ27[Q27] = {0, 0, 0, 0, 0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1, 1, -1, -1, 1, 1, -1, 1, -1};
 
+/* weight class of direction l: number of non-zero components (0..3) */
+inline int wcls(int l) { return (l == 0) ? 0 : (l <= 6 ? 1 : (l <= 18 ? 2 : 3)); }
+
 template <typename T>
 struct Tables {
-  T p[Q], b_l[Q], rec_fact[Q], a27[Q27], p27[Q27];
-  T phi[Q], varphi[Q], psi[Q], xi[Q]; /* DIFFDENS tables, dimensions_m.CUF:231-261 */
+  T p[Q27], b_l[Q27], rec_fact[Q27], a27[Q27], p27[Q27];
+  T phi[Q27], varphi[Q27], psi[Q27], xi[Q27]; /* DIFFDENS tables */
   T cssq;
-  Tables() {
+  int q; /* 19 or 27 populations */
+  explicit Tables(int nq = Q) : q(nq) {
     /* all arithmetic in T, in the order the Fortran parameter expressions use */
     const T ONE = 1, TWO = 2, THREE = 3, SIX = 6, TWELVE = 12, TWENTYFOUR = 24;
+    const T FOUR = 4, FIVE = 5, EIGHT = 8, NINE = 9, TEN = 10, TWENTYSEVEN = 27, FIFTYFOUR = 54;
     cssq = T(1.0) / T(3.0);                                   /* dimensions_m.CUF:94 */
-    const T p0 = T(1.0) / T(3.0), p1 = T(1.0) / T(18.0), p2 = T(1.0) / T(36.0); /* :208-210 */
-    for (int l = 0; l < Q; ++l) p[l] = (l == 0) ? p0 : (l <= 6 ? p1 : p2);
-    const T b_xi = T(0.5);                                    /* Leclaire, :222 */
-    const T b0 = -(TWO + TWO * b_xi) / (THREE * b_xi + TWELVE);
-    const T b1 = (b_xi) / (SIX * b_xi + TWENTYFOUR);
-    const T b2 = ONE / (SIX * b_xi + TWENTYFOUR);
-    for (int l = 0; l < Q; ++l) b_l[l] = (l == 0) ? b0 : (l <= 6 ? b1 : b2);
-    for (int l = 0; l < Q; ++l) /* SetConstants, main.CUF:1098 */
-      rec_fact[l] = std::sqrt(T(EX[l] * EX[l] + EY[l] * EY[l] + EZ[l] * EZ[l]));
     const T q0 = (TWO / THREE) * (TWO / THREE) * (TWO / THREE);   /* :283-286 */
     const T q1 = (TWO / THREE) * (TWO / THREE) * (ONE / SIX);
     const T q2 = (ONE / SIX) * (ONE / SIX) * (TWO / THREE);
     const T q3 = (ONE / SIX) * (ONE / SIX) * (ONE / SIX);
+    T pc[4], bc[4], phc[4], vpc[4], psc[4], xc[4];
+    if (q == Q) { /* D3Q19, :201-261 */
+      pc[0] = T(1.0) / T(3.0); pc[1] = T(1.0) / T(18.0); pc[2] = T(1.0) / T(36.0); pc[3] = 0;
+      const T b_xi = T(0.5);                                  /* Leclaire, :222 */
+      bc[0] = -(TWO + TWO * b_xi) / (THREE * b_xi + TWELVE);
+      bc[1] = (b_xi) / (SIX * b_xi + TWENTYFOUR);
+      bc[2] = ONE / (SIX * b_xi + TWENTYFOUR);
+      bc[3] = 0;
+      phc[0] = T(0); phc[1] = ONE / TWELVE; phc[2] = ONE / TWENTYFOUR; phc[3] = 0;
+      vpc[0] = ONE; vpc[1] = -ONE / TWELVE; vpc[2] = -ONE / TWENTYFOUR; vpc[3] = 0;
+      psc[0] = -FIVE / TWO; psc[1] = -ONE / SIX; psc[2] = ONE / TWENTYFOUR; psc[3] = 0;
+      xc[0] = T(0); xc[1] = ONE / FOUR; xc[2] = ONE / EIGHT; xc[3] = 0;
+    } else {      /* D3Q27, :117-198 */
+      pc[0] = q0; pc[1] = q1; pc[2] = q2; pc[3] = q3;
+      bc[0] = -(TEN / TWENTYSEVEN); bc[1] = TWO / TWENTYSEVEN; bc[2] = ONE / FIFTYFOUR; bc[3] = ONE / T(216.0);
+      phc[0] = T(0); phc[1] = TWO / T(19.0); phc[2] = ONE / T(38.0); phc[3] = ONE / T(152.0);
+      vpc[0] = ONE; vpc[1] = -TWO / T(19.0); vpc[2] = -ONE / T(38.0); vpc[3] = -ONE / T(152.0);
+      psc[0] = T(-20.0) / NINE; psc[1] = -TWO / NINE; psc[2] = ONE / T(36.0); psc[3] = ONE / T(36.0);
+      xc[0] = T(0); xc[1] = ONE / THREE; xc[2] = ONE / TWELVE; xc[3] = ONE / T(48.0);
+    }
     for (int l = 0; l < Q27; ++l) {
+      const int c = wcls(l);
+      p[l] = pc[c];
+      b_l[l] = bc[c];
+      phi[l] = phc[c];
+      varphi[l] = vpc[c];
+      psi[l] = psc[c];
+      xi[l] = xc[c];
+      rec_fact[l] = std::sqrt(T(EX[l] * EX[l] + EY[l] * EY[l] + EZ[l] * EZ[l])); /* SetConstants, main.CUF:1098 */
       T w = (l == 0) ? q0 : (l <= 6 ? q1 : (l <= 18 ? q2 : q3));
       p27[l] = w;
       a27[l] = (l == 0) ? T(0) : w / cssq;                        /* :292-298 */
-    }
-    const T FOUR = 4, FIVE = 5, EIGHT = 8;
-    for (int l = 0; l < Q; ++l) {
-      const int c = (l == 0) ? 0 : (l <= 6 ? 1 : 2);
-      const T ph[3] = {T(0), ONE / TWELVE, ONE / TWENTYFOUR};
-      const T vph[3] = {ONE, -ONE / TWELVE, -ONE / TWENTYFOUR};
-      const T ps[3] = {-FIVE / TWO, -ONE / SIX, ONE / TWENTYFOUR};
-      const T x[3] = {T(0), ONE / FOUR, ONE / EIGHT};
-      phi[l] = ph[c];
-      varphi[l] = vph[c];
-      psi[l] = ps[c];
-      xi[l] = x[c];
     }
   }
 };
@@ -123,6 +137,7 @@ class Oracle {
   int nx, ny, nz, sx, sy, sz;  /* interior and padded sizes */
   int64_t ncell_pad;
   Tables<T> tb;
+  int q = Q; /* populations per component: 19, or 27 for the D3Q27 models */
   int model;
   int flip = 0;  /* 0-based reference `flipflop - 1` */
   int64_t step = 0;
@@ -139,12 +154,14 @@ class Oracle {
 
   Oracle(const lbx_params& p) : prm(p) {
     nx = p.nx; ny = p.ny; nz = p.nz;
+    q = (p.model == LBX_MODEL_CG_D3Q27 || p.model == LBX_MODEL_CG_DIFFDENS_D3Q27) ? Q27 : Q;
+    tb = Tables<T>(q);
     sx = nx + 2; sy = ny + 2; sz = nz + 2;
     ncell_pad = int64_t(sx) * sy * sz;
     model = p.model;
     int ncomp = (model != LBX_MODEL_BGK) ? 2 : 1;
     for (int c = 0; c < ncomp; ++c)
-      for (int b = 0; b < 2; ++b) pops[c][b].assign(size_t(Q) * ncell_pad, T(0));
+      for (int b = 0; b < 2; ++b) pops[c][b].assign(size_t(q) * ncell_pad, T(0));
     for (int c = 0; c < 2; ++c) rho[c].assign(ncell_pad, T(0));
     for (int b = 0; b < 2; ++b) flags[b].assign(ncell_pad, int8_t(LBX_FLUID_FLUID));
     const T HALF = T(0.5);
@@ -152,7 +169,7 @@ class Oracle {
     viscB = tb.cssq * (T(p.tauB) - HALF);
     omega_bgk = T(1) / T(p.tau);
     /* SetConstants, main.CUF:1047-1083 */
-    diffdens = (model == LBX_MODEL_CG_DIFFDENS);
+    diffdens = (model == LBX_MODEL_CG_DIFFDENS || model == LBX_MODEL_CG_DIFFDENS_D3Q27);
     const T ONE = 1;
     densR = diffdens ? T(p.densR) : ONE;
     densB = diffdens ? T(p.densB) : ONE;
@@ -194,7 +211,7 @@ class Oracle {
     int ncomp = (model != LBX_MODEL_BGK) ? 2 : 1;
     for_halo([&](int64_t h, int64_t s) {
       for (int c = 0; c < ncomp; ++c)
-        for (int l = 1; l < Q; ++l) f(c, b, l, h) = f(c, b, l, s);
+        for (int l = 1; l < q; ++l) f(c, b, l, h) = f(c, b, l, s);
     });
   }
   void halo_rho() {
@@ -221,7 +238,7 @@ class Oracle {
           T r1 = (ncomp == 2 && rB) ? T(rB[h]) : T(0);
           rho[0][x] = r0;
           rho[1][x] = r1;
-          for (int l = 0; l < Q; ++l) {
+          for (int l = 0; l < q; ++l) {
             if (diffdens) { /* setup2, kernels_fluid_CG.CUF:176-178 */
               f(0, 0, l, x) = equil_cg(tb, r0, T(vx), T(vy), T(vz), alphaCG[0], l);
               f(1, 0, l, x) = equil_cg(tb, r1, T(vx), T(vy), T(vz), alphaCG[1], l);
@@ -251,7 +268,7 @@ class Oracle {
         for (int i = 1; i <= nx; ++i) {
           int64_t h = (i - 1) + int64_t(nx) * ((j - 1) + int64_t(ny) * (k - 1));
           int64_t x = id(i, j, k);
-          for (int l = 0; l < Q; ++l) {
+          for (int l = 0; l < q; ++l) {
             f(0, 0, l, x) = T(pR[h + n * l]);
             if (ncomp == 2) f(1, 0, l, x) = pB ? T(pB[h + n * l]) : T(0);
           }
@@ -275,7 +292,7 @@ class Oracle {
           for (int c = 0; c < 2; ++c) {
             if (flags[b][x] == LBX_FLUID_FLUID) {
               T r = f(c, b, 0, x);
-              for (int l = 1; l < Q; ++l) r = r + f(c, b, l, x); /* fixed order 0..18 */
+              for (int l = 1; l < q; ++l) r = r + f(c, b, l, x); /* fixed order 0..18 */
               if (r < minRho || r > maxRho) raise(LBX_DEV_RHO_RANGE, (i - 1) + int64_t(nx) * ((j - 1) + int64_t(ny) * (k - 1)));
               if (r < MINDENS) r = MINDENS;
               rho[c][x] = r;
@@ -288,9 +305,20 @@ class Oracle {
   }
 
   /* manual_u/v/w, kernels_fluid_CG.CUF:511-529 */
-  static inline T mom_x(const T* q, T inv) { return inv * (q[1] - q[2] + q[7] - q[8] - q[9] + q[10] + q[11] - q[12] - q[13] + q[14]); }
-  static inline T mom_y(const T* q, T inv) { return inv * (q[3] - q[4] + q[7] - q[8] + q[9] - q[10] + q[15] - q[16] - q[17] + q[18]); }
-  static inline T mom_z(const T* q, T inv) { return inv * (q[5] - q[6] + q[11] - q[12] + q[13] - q[14] + q[15] - q[16] + q[17] - q[18]); }
+  /* sum_l e_l,d f_l over the nonzero components in increasing l (the
+   * left-to-right order of manual_u/v/w, kernels_fluid_CG.CUF:511-529, and
+   * of the D3Q27 sums there); from zero, so the first term enters exactly */
+  T msum(const T* f_, const int* e) const {
+    T s = 0;
+    for (int l = 1; l < q; ++l) {
+      if (e[l] > 0) s = s + f_[l];
+      else if (e[l] < 0) s = s - f_[l];
+    }
+    return s;
+  }
+  T mom_x(const T* f_, T inv) const { return inv * msum(f_, EX); }
+  T mom_y(const T* f_, T inv) const { return inv * msum(f_, EY); }
+  T mom_z(const T* f_, T inv) const { return inv * msum(f_, EZ); }
 
   /* ---- time_step_CG, kernels_fluid_CG.CUF:531-848 (HIGHGRAD; DIFFDENS when
    * the model is LBX_MODEL_CG_DIFFDENS) --------------------------------------- */
@@ -305,8 +333,8 @@ class Oracle {
         for (int i = 1; i <= nx; ++i) {
           int64_t x = id(i, j, k);
           if (flags[b][x] != LBX_FLUID_FLUID) continue;
-          T tR[Q], tB[Q], fd[Q];
-          for (int l = 0; l < Q; ++l) { tR[l] = f(0, b, l, x); tB[l] = f(1, b, l, x); }
+          T tR[Q27], tB[Q27], fd[Q27];
+          for (int l = 0; l < q; ++l) { tR[l] = f(0, b, l, x); tB[l] = f(1, b, l, x); }
           T rhoR = rho[0][x], rhoB = rho[1][x];
           T rhosum = rhoR + rhoB;
           T phase_field = (rhoR / densR - rhoB / densB) / (rhoR / densR + rhoB / densB);
@@ -344,32 +372,32 @@ class Oracle {
               gR[d] = vel[d] * psR[d] + vel[d] * psR[d];
               gB[d] = vel[d] * psB[d] + vel[d] * psB[d];
             }
-            for (int l = 0; l < Q; ++l) {
+            for (int l = 0; l < q; ++l) {
               const T cm[3] = {T(EX[l] * EX[l]), T(EY[l] * EY[l]), T(EZ[l] * EZ[l])}; /* cmat_d(d,d,l) */
               T tc = gR[0] * cm[0] + gR[1] * cm[1] + gR[2] * cm[2];
               tR[l] = tR[l] * oneminusomega +
                       (equil_cg(tb, rhoR, u, v, w, alphaCG[0], l) + viscavg * (tb.psi[l] * vR + tb.xi[l] * tc)) * omega;
             }
-            for (int l = 0; l < Q; ++l) {
+            for (int l = 0; l < q; ++l) {
               const T cm[3] = {T(EX[l] * EX[l]), T(EY[l] * EY[l]), T(EZ[l] * EZ[l])};
               T tc = gB[0] * cm[0] + gB[1] * cm[1] + gB[2] * cm[2];
               tB[l] = tB[l] * oneminusomega +
                       (equil_cg(tb, rhoB, u, v, w, alphaCG[1], l) + viscavg * (tb.psi[l] * vB + tb.xi[l] * tc)) * omega;
             }
           } else {
-            for (int l = 0; l < Q; ++l) tR[l] = tR[l] * oneminusomega + equil(tb, rhoR, u, v, w, l) * omega;
-            for (int l = 0; l < Q; ++l) tB[l] = tB[l] * oneminusomega + equil(tb, rhoB, u, v, w, l) * omega;
+            for (int l = 0; l < q; ++l) tR[l] = tR[l] * oneminusomega + equil(tb, rhoR, u, v, w, l) * omega;
+            for (int l = 0; l < q; ++l) tB[l] = tB[l] * oneminusomega + equil(tb, rhoB, u, v, w, l) * omega;
           }
           T psinorm_sq = psix * psix + psiy * psiy + psiz * psiz;
           if (psinorm_sq > mylimit) { /* perturbation + recolouring, :803-837 */
             T psinorm = std::sqrt(psinorm_sq);
             T acoeff = NINE / FOUR * omega * sigma;
-            for (int l = 0; l < Q; ++l) {
+            for (int l = 0; l < q; ++l) {
               T edp = T(EX[l]) * psix + T(EY[l]) * psiy + T(EZ[l]) * psiz;
               T temp = psinorm * (tb.p[l] * (edp * edp) / psinorm_sq - tb.b_l[l]);
               fd[l] = tR[l] + tB[l] + acoeff * temp;
             }
-            for (int l = 0; l < Q; ++l) {
+            for (int l = 0; l < q; ++l) {
               T feq = diffdens ? equil_cg(tb, rhoR, ZERO, ZERO, ZERO, alphaCG[0], l) +
                                      equil_cg(tb, rhoB, ZERO, ZERO, ZERO, alphaCG[1], l)
                                : equil(tb, rhoR, ZERO, ZERO, ZERO, l) + equil(tb, rhoB, ZERO, ZERO, ZERO, l);
@@ -381,7 +409,7 @@ class Oracle {
               f(1, b, l, x) = fd[l] * rhoB / rhosum - temp * feq;
             }
           } else {
-            for (int l = 0; l < Q; ++l) { f(0, b, l, x) = tR[l]; f(1, b, l, x) = tB[l]; }
+            for (int l = 0; l < q; ++l) { f(0, b, l, x) = tR[l]; f(1, b, l, x) = tB[l]; }
           }
         }
     halo_pops(b); /* fixPeriodic(.true., .false.) */
@@ -425,13 +453,13 @@ class Oracle {
           for (int c = 0; c < ncomp; ++c) f(c, o, 0, x) = f(c, b, 0, x);
           if (flags[b][x] == LBX_FLUID_SPHEREDEAD) continue;
           for (int c = 0; c < ncomp; ++c)
-            for (int l = 1; l < Q; ++l) f(c, o, l, id(i + EX[l], j + EY[l], k + EZ[l])) = f(c, b, l, x);
+            for (int l = 1; l < q; ++l) f(c, o, l, id(i + EX[l], j + EY[l], k + EZ[l])) = f(c, b, l, x);
         }
     /* halo cells push into the interior (stream_CG_x, _y, _z) */
     auto halo_push = [&](int i, int j, int k) {
       int64_t x = id(i, j, k);
       if (flags[b][x] == LBX_FLUID_SPHEREDEAD) return;
-      for (int l = 1; l < Q; ++l) {
+      for (int l = 1; l < q; ++l) {
         int i1 = i + EX[l], j1 = j + EY[l], k1 = k + EZ[l];
         if (1 <= i1 && i1 <= nx && 1 <= j1 && j1 <= ny && 1 <= k1 && k1 <= nz)
           for (int c = 0; c < ncomp; ++c) f(c, o, l, id(i1, j1, k1)) = f(c, b, l, x);
@@ -1200,18 +1228,27 @@ class Oracle {
         for (int i = 1; i <= nx; ++i) {
           int64_t x = id(i, j, k);
           int64_t h = (i - 1) + int64_t(nx) * ((j - 1) + int64_t(ny) * (k - 1));
-          T pR[Q], pB[Q];
-          for (int l = 0; l < Q; ++l) { pR[l] = f(0, b, l, x); pB[l] = (ncomp == 2) ? f(1, b, l, x) : T(0); }
+          T pR[Q27], pB[Q27];
+          for (int l = 0; l < q; ++l) { pR[l] = f(0, b, l, x); pB[l] = (ncomp == 2) ? f(1, b, l, x) : T(0); }
           T lr = pR[0], lb = pB[0];
-          for (int l = 1; l < Q; ++l) { lr = lr + pR[l]; lb = lb + pB[l]; }
+          for (int l = 1; l < q; ++l) { lr = lr + pR[l]; lb = lb + pB[l]; }
           T rs = lr + lb;
           T inv = ONE / rs;
-          T u = inv * (pR[1] - pR[2] + pR[7] - pR[8] - pR[9] + pR[10] + pR[11] - pR[12] - pR[13] + pR[14] +
-                       pB[1] - pB[2] + pB[7] - pB[8] - pB[9] + pB[10] + pB[11] - pB[12] - pB[13] + pB[14]);
-          T v = inv * (pR[3] - pR[4] + pR[7] - pR[8] + pR[9] - pR[10] + pR[15] - pR[16] - pR[17] + pR[18] +
-                       pB[3] - pB[4] + pB[7] - pB[8] + pB[9] - pB[10] + pB[15] - pB[16] - pB[17] + pB[18]);
-          T w = inv * (pR[5] - pR[6] + pR[11] - pR[12] + pR[13] - pR[14] + pR[15] - pR[16] + pR[17] - pR[18] +
-                       pB[5] - pB[6] + pB[11] - pB[12] + pB[13] - pB[14] + pB[15] - pB[16] + pB[17] - pB[18]);
+          /* moments2Fl (write_output.f90:975-1041) sums the R terms, then the
+           * B terms, left to right; over all q directions (the reference's
+           * routine lists only the first 19, also in its D3Q27 build) */
+          T u = 0, v = 0, w = 0;
+          for (int c = 0; c < 2; ++c) {
+            const T* pp = c ? pB : pR;
+            for (int l = 1; l < q; ++l) {
+              if (EX[l]) u = EX[l] > 0 ? u + pp[l] : u - pp[l];
+              if (EY[l]) v = EY[l] > 0 ? v + pp[l] : v - pp[l];
+              if (EZ[l]) w = EZ[l] > 0 ? w + pp[l] : w - pp[l];
+            }
+          }
+          u = inv * u;
+          v = inv * v;
+          w = inv * w;
           bool ok = flags[bf][x] == LBX_FLUID_FLUID && rs > MINDENS;
           if (oR) oR[h] = ok ? double(lr) : 0.0;
           if (oB) oB[h] = ok ? double(lb) : 0.0;
@@ -1234,7 +1271,7 @@ class Oracle {
         for (int i = 1; i <= nx; ++i) {
           int64_t x = id(i, j, k);
           int64_t h = (i - 1) + int64_t(nx) * ((j - 1) + int64_t(ny) * (k - 1));
-          for (int l = 0; l < Q; ++l) {
+          for (int l = 0; l < q; ++l) {
             if (pR) pR[h + n * l] = double(f(0, b, l, x));
             if (pB) pB[h + n * l] = (ncomp == 2) ? double(f(1, b, l, x)) : 0.0;
           }

@@ -62,6 +62,7 @@ class OracleSim:
         self.params = params
         self.nx, self.ny, self.nz = params.nx, params.ny, params.nz
         self.ncomp = 1 if params.model == 0 else 2
+        self.q = 27 if params.model in (3, 4) else Q  # the D3Q27 models
         self._L = lib()
         self._h = self._L.orc_create(C.byref(params), MODES[mode])
         if not self._h:
@@ -105,8 +106,8 @@ class OracleSim:
         return rR, rB, vel, ph
 
     def get_pops(self):
-        pR = np.empty((Q,) + self.shape)
-        pB = np.empty((Q,) + self.shape)
+        pR = np.empty((self.q,) + self.shape)
+        pB = np.empty((self.q,) + self.shape)
         self._L.orc_get_pops(self._h, _p(pR, C.c_double), _p(pB, C.c_double))
         return pR, (pB if self.ncomp == 2 else None)
 
