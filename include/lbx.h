@@ -136,7 +136,8 @@ int lbx_destroy(void* ctx);
  * the BGK model rhoB is ignored (may be NULL).  Covers initType 1,2,3,5,6
  * once the host has built the density fields (main.CUF:2531-2608). */
 int lbx_set_fields(void* ctx, const float* rhoR, const float* rhoB, float vx, float vy, float vz);
-/* initType 4 (read_and_setPops, main.CUF:2489-2529): raw populations. */
+/* initType 4 (read_and_setPops, main.CUF:2489-2529): raw populations,
+ * q planes of nx*ny*nz per component (q = 19; 27 for the D3Q27 models). */
 int lbx_set_pops(void* ctx, const float* popsR, const float* popsB);
 
 /* ---- particles --------------------------------------------------------- */
@@ -189,7 +190,8 @@ int lbx_time_step_bgk(void* ctx);     /* init_rho_isfluid_BGK + time_step_BGK + 
 int lbx_get_fields(void* ctx, float* rhoR, float* rhoB, float* vel, float* phase);
 /* The same in FP64 (exact moments of the stored populations). */
 int lbx_get_fields_f64(void* ctx, double* rhoR, double* rhoB, double* vel, double* phase);
-/* Post-streaming populations (the reference's `flip` buffer after a step). */
+/* Post-streaming populations (the reference's `flip` buffer after a step),
+ * q planes of nx*ny*nz per component as for lbx_set_pops. */
 int lbx_get_pops(void* ctx, float* popsR, float* popsB);
 /* Cell flags of the last step (myfluid_d(:,:,:,flip)), int8 nx*ny*nz. */
 int lbx_get_flags(void* ctx, int8_t* flags);

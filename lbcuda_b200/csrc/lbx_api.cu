@@ -140,9 +140,13 @@ int lbx_create(const lbx_params* p, void** out) {
   if (!p || !out) return LBX_ERR_ARG;
   *out = nullptr;
   if (p->nx < 3 || p->ny < 3 || p->nz < 3) return LBX_ERR_ARG;
-  if (p->model != LBX_MODEL_BGK && p->model != LBX_MODEL_CG && p->model != LBX_MODEL_CG_DIFFDENS) return LBX_ERR_ARG;
+  if (p->model < LBX_MODEL_BGK || p->model > LBX_MODEL_CG_DIFFDENS_D3Q27) return LBX_ERR_ARG;
+  const bool two_dens = p->model == LBX_MODEL_CG_DIFFDENS || p->model == LBX_MODEL_CG_DIFFDENS_D3Q27;
+  const bool d3q27 = p->model == LBX_MODEL_CG_D3Q27 || p->model == LBX_MODEL_CG_DIFFDENS_D3Q27;
+  // the reference's sphere kernels are D3Q19 only (kernels_fluid_PART.CUF:1929-1941)
+  if (d3q27 && p->max_particles > 0) return LBX_ERR_ARG;
   // SetConstants, main.CUF:1047-1061: at least one of the two densities is 1
-  if (p->model == LBX_MODEL_CG_DIFFDENS &&
+  if (two_dens &&
       (!(p->densR > 0.0f) || !(p->densB > 0.0f) || (p->densR != 1.0f && p->densB != 1.0f)))
     return LBX_ERR_ARG;
   if (p->storage < LBX_STORE_F32 || p->storage > LBX_STORE_F64) return LBX_ERR_ARG;
@@ -156,8 +160,9 @@ int lbx_create(const lbx_params* p, void** out) {
   c->nz = p->nz;
   c->n = n;
   c->ncomp = (p->model == LBX_MODEL_BGK) ? 1 : 2;
-  // the DIFFDENS collision runs on the two-pass schedule only
-  if (p->model == LBX_MODEL_CG_DIFFDENS) c->fused = 0;
+  c->q = d3q27 ? lbx::Q27 : lbx::Q;
+  // the DIFFDENS collision and the D3Q27 lattice run on the two-pass schedule only
+  if (two_dens || d3q27) c->fused = 0;
   c->storage = p->storage;
   c->elem = (p->storage == LBX_STORE_F32) ? 4 : (p->storage == LBX_STORE_F64 ? 8 : 2);
   int rc = cuda_rc(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
@@ -208,11 +213,11 @@ int lbx_set_fields(void* ctx, const float* rhoR, const float* rhoB, float vx, fl
 int lbx_set_pops(void* ctx, const float* popsR, const float* popsB) {
   Ctx* c = as_ctx(ctx);
   if (!c || !popsR || (c->ncomp == 2 && !popsB)) return LBX_ERR_ARG;
-  size_t bytes = size_t(c->n) * lbx::Q * sizeof(float);
+  size_t bytes = size_t(c->n) * size_t(c->q) * sizeof(float);
   DevBuf buf(c, bytes * c->ncomp);
   if (!buf.p) return LBX_ERR_ALLOC;
   float* dR = static_cast<float*>(buf.p);
-  float* dB = (c->ncomp == 2) ? dR + c->n * lbx::Q : nullptr;
+  float* dB = (c->ncomp == 2) ? dR + c->n * c->q : nullptr;
   int rc = cuda_rc(cudaMemcpyAsync(dR, popsR, bytes, cudaMemcpyHostToDevice, c->stream));
   if (!rc && dB) rc = cuda_rc(cudaMemcpyAsync(dB, popsB, bytes, cudaMemcpyHostToDevice, c->stream));
   if (!rc) rc = lbx::fluid_set_pops(*c, dR, dB);
@@ -311,11 +316,11 @@ int lbx_get_fields_f64(void* ctx, double* rhoR, double* rhoB, double* vel, doubl
 int lbx_get_pops(void* ctx, float* popsR, float* popsB) {
   Ctx* c = as_ctx(ctx);
   if (!c) return LBX_ERR_ARG;
-  size_t nb = size_t(c->n) * lbx::Q * sizeof(float);
+  size_t nb = size_t(c->n) * size_t(c->q) * sizeof(float);
   DevBuf buf(c, nb * 2);
   if (!buf.p) return LBX_ERR_ALLOC;
   float* dR = popsR ? static_cast<float*>(buf.p) : nullptr;
-  float* dB = popsB ? static_cast<float*>(buf.p) + size_t(c->n) * lbx::Q : nullptr;
+  float* dB = popsB ? static_cast<float*>(buf.p) + size_t(c->n) * size_t(c->q) : nullptr;
   int rc = lbx::fluid_get_pops(*c, dR, dB);
   if (!rc && popsR) rc = cuda_rc(cudaMemcpyAsync(popsR, dR, nb, cudaMemcpyDeviceToHost, c->stream));
   if (!rc && popsB) {
@@ -419,7 +424,7 @@ int lbx_set_schedule(void* ctx, int32_t fused) {
   Ctx* c = as_ctx(ctx);
   if (!c) return LBX_ERR_ARG;
   if (fused < 0 || fused > 2) return LBX_ERR_ARG;
-  if (c->p.model == LBX_MODEL_CG_DIFFDENS && fused != 0) return LBX_ERR_ARG;
+  if (c->p.model >= LBX_MODEL_CG_DIFFDENS && fused != 0) return LBX_ERR_ARG;
   c->fused = fused;
   return 0;
 }

@@ -13,18 +13,19 @@ namespace lbx {
 constexpr int Q = 19;   // D3Q19, reference default (defines.h:8 `noD3Q27`)
 constexpr int Q27 = 27; // gradient / belt neighbourhood (dimensions_m.CUF:275-281)
 
-// Lattice velocities in the reference order (dimensions_m.CUF:211-218).  They
+// Lattice velocities in the reference order (dimensions_m.CUF:211-218, and
+// :130-135 for the D3Q27 build, whose first 19 directions are D3Q19's).  They
 // are compile-time constants here so that every unrolled loop folds them.
 __host__ __device__ constexpr int ex(int l) {
-  constexpr int t[Q] = {0, 1, -1, 0, 0, 0, 0, 1, -1, -1, 1, 1, -1, -1, 1, 0, 0, 0, 0};
+  constexpr int t[Q27] = {0, 1, -1, 0, 0, 0, 0, 1, -1, -1, 1, 1, -1, -1, 1, 0, 0, 0, 0, 1, -1, 1, -1, -1, 1, 1, -1};
   return t[l];
 }
 __host__ __device__ constexpr int ey(int l) {
-  constexpr int t[Q] = {0, 0, 0, 1, -1, 0, 0, 1, -1, 1, -1, 0, 0, 0, 0, 1, -1, -1, 1};
+  constexpr int t[Q27] = {0, 0, 0, 1, -1, 0, 0, 1, -1, 1, -1, 0, 0, 0, 0, 1, -1, -1, 1, 1, -1, 1, -1, 1, -1, -1, 1};
   return t[l];
 }
 __host__ __device__ constexpr int ez(int l) {
-  constexpr int t[Q] = {0, 0, 0, 0, 0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1};
+  constexpr int t[Q27] = {0, 0, 0, 0, 0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1, 1, -1, -1, 1, 1, -1, 1, -1};
   return t[l];
 }
 __host__ __device__ constexpr int ex27(int l) {
@@ -51,28 +52,31 @@ __host__ __device__ constexpr int opp(int l) { return l == 0 ? 0 : ((l & 1) ? l 
 // dimensions_m.CUF:201-300) and passed to kernels by value.
 template <typename C>
 struct LatticeT {
-  C w[3];        // p0, p1, p2
-  C b[3];        // b_l classes (Leclaire, b_xi = 0.5)
+  C w[4];        // p_l per weight class (class 3: D3Q27 corners)
+  C b[4];        // b_l classes (D3Q19: Leclaire, b_xi = 0.5; D3Q27: Saito)
   C a27[4];      // ad3q27 classes (0, p1/cssq, p2/cssq, p3/cssq)
   C p27[4];      // pd3q27 classes (D3Q27 weights, dimensions_m.CUF:283-290)
-  C rec[3];      // rec_fact classes: 0, 1, sqrt(2)
+  C rec[4];      // rec_fact classes: 0, 1, sqrt(2), sqrt(3)
   C cssq;        // 1/3
   C inv_cssq;    // 1/cssq
   C half_inv_cssq;  // HALF/cssq
 };
 
+// q = 19 (default, dimensions_m.CUF:201-261) or 27 (the D3Q27 build, :117-198)
 template <typename C>
-inline LatticeT<C> make_lattice() {
+inline LatticeT<C> make_lattice(int q = Q) {
   LatticeT<C> L;
   const C ONE = 1, TWO = 2, THREE = 3, SIX = 6, TWELVE = 12, TWENTYFOUR = 24;
   L.cssq = C(1.0) / C(3.0);
   L.w[0] = C(1.0) / C(3.0);
   L.w[1] = C(1.0) / C(18.0);
   L.w[2] = C(1.0) / C(36.0);
+  L.w[3] = C(0);
   const C b_xi = C(0.5);
   L.b[0] = -(TWO + TWO * b_xi) / (THREE * b_xi + TWELVE);
   L.b[1] = (b_xi) / (SIX * b_xi + TWENTYFOUR);
   L.b[2] = ONE / (SIX * b_xi + TWENTYFOUR);
+  L.b[3] = C(0);
   const C q1 = (TWO / THREE) * (TWO / THREE) * (ONE / SIX);
   const C q2 = (ONE / SIX) * (ONE / SIX) * (TWO / THREE);
   const C q3 = (ONE / SIX) * (ONE / SIX) * (ONE / SIX);
@@ -87,6 +91,14 @@ inline LatticeT<C> make_lattice() {
   L.rec[0] = 0;
   L.rec[1] = 1;
   L.rec[2] = sqrt(C(2));
+  L.rec[3] = sqrt(C(3));
+  if (q == Q27) {  // D3Q27 weights and Saito's b_l (dimensions_m.CUF:124-143)
+    for (int k = 0; k < 4; ++k) L.w[k] = L.p27[k];
+    L.b[0] = -(C(10) / C(27));
+    L.b[1] = TWO / C(27);
+    L.b[2] = ONE / C(54);
+    L.b[3] = ONE / C(216.0);
+  }
   L.inv_cssq = ONE / L.cssq;
   L.half_inv_cssq = C(0.5) / L.cssq;
   return L;
@@ -131,8 +143,8 @@ template <> struct Store<__nv_bfloat16> {
 // Shift of direction l of component c: w_l * rho0_c (zero for unshifted types).
 template <typename C>
 struct Shift {
-  C s[2][3];  // [component][weight class]
-  __device__ __forceinline__ C at(int c, int l) const { return s[c][wclass(l)]; }
+  C s[2][4];  // [component][weight class]
+  __device__ __forceinline__ C at(int c, int l) const { return s[c][wclass27(l)]; }
 };
 
 // ---- geometry ---------------------------------------------------------------

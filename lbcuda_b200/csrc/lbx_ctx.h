@@ -28,6 +28,7 @@ struct Ctx {
   int nx = 0, ny = 0, nz = 0;
   int64_t n = 0;            // interior cells
   int ncomp = 1;            // 1 (BGK) or 2 (CG)
+  int q = 19;               // populations per component: 19, or 27 for the D3Q27 models
   int storage = LBX_STORE_F32;
   size_t elem = 4;          // bytes per stored population
   void* pops[2] = {nullptr, nullptr};

@@ -50,34 +50,34 @@ __device__ __forceinline__ C edot(int l, C u, C v, C w) {
 template <typename C>
 __device__ __forceinline__ C equil_u(const LatticeT<C>& L, C rho, C edu, C usq_term, int l) {
   C uv = L.inv_cssq * edu;
-  return rho * L.w[wclass(l)] * (C(1) + uv + C(0.5) * (uv * uv) - usq_term);
+  return rho * L.w[wclass27(l)] * (C(1) + uv + C(0.5) * (uv * uv) - usq_term);
 }
 
 // gather the post-streaming populations of one component (pull of the push
 // streaming of stream*_CG + halo pushes)
-template <typename S, typename C>
+template <int QQ = Q, typename S, typename C>
 __device__ __forceinline__ void pull(const S* __restrict__ A, const Geom& g, const Nbr& b, int comp,
-                                     const Shift<C>& sh, C f[Q]) {
+                                     const Shift<C>& sh, C* f) {
 #pragma unroll
-  for (int l = 0; l < Q; ++l) f[l] = Store<S>::ld(A + pidx(g, comp, l, at(b, -ex(l), -ey(l), -ez(l))), sh.at(comp, l));
+  for (int l = 0; l < QQ; ++l) f[l] = Store<S>::ld(A + pidx(g, comp, l, at(b, -ex(l), -ey(l), -ez(l))), sh.at(comp, l));
 }
 
-template <typename S, typename C>
+template <int QQ = Q, typename S, typename C>
 __device__ __forceinline__ void store_all(S* __restrict__ B, const Geom& g, int cell, int comp, const Shift<C>& sh,
-                                          const C f[Q]) {
+                                          const C* f) {
 #pragma unroll
-  for (int l = 0; l < Q; ++l) Store<S>::st(B + pidx(g, comp, l, cell), f[l], sh.at(comp, l));
+  for (int l = 0; l < QQ; ++l) Store<S>::st(B + pidx(g, comp, l, cell), f[l], sh.at(comp, l));
 }
 
 // The post-streaming populations of a cell, pulled from the post-collision
 // state A; a spheredead source (flags of the previous step) leaves the
 // destination's stale value, which is B's entry.
-template <typename S, typename C>
+template <int QQ = Q, typename S, typename C>
 __device__ __forceinline__ void pull_dead(const S* __restrict__ A, const S* Bold, const Geom& g, const Nbr& b,
-                                          int comp, const Shift<C>& sh, const int8_t* __restrict__ fold, C f[Q]) {
+                                          int comp, const Shift<C>& sh, const int8_t* __restrict__ fold, C* f) {
   const int self = at(b, 0, 0, 0);
 #pragma unroll
-  for (int l = 0; l < Q; ++l) {
+  for (int l = 0; l < QQ; ++l) {
     int src = at(b, -ex(l), -ey(l), -ez(l));
     if (l > 0 && fold[src] == LBX_FLUID_SPHEREDEAD)
       f[l] = Store<S>::ld(Bold + pidx(g, comp, l, self), sh.at(comp, l));
@@ -87,24 +87,48 @@ __device__ __forceinline__ void pull_dead(const S* __restrict__ A, const S* Bold
 }
 
 // pull_dead when the flags of the previous step are given, plain pull otherwise
-template <typename S, typename C>
+template <int QQ = Q, typename S, typename C>
 __device__ __forceinline__ void pull_any(const S* __restrict__ A, const S* Bold, const Geom& g, const Nbr& b,
-                                         int comp, const Shift<C>& sh, const int8_t* __restrict__ fold, C f[Q]) {
-  if (fold) pull_dead(A, Bold, g, b, comp, sh, fold, f);
-  else pull(A, g, b, comp, sh, f);
+                                         int comp, const Shift<C>& sh, const int8_t* __restrict__ fold, C* f) {
+  if (fold) pull_dead<QQ>(A, Bold, g, b, comp, sh, fold, f);
+  else pull<QQ>(A, g, b, comp, sh, f);
 }
 
-template <typename C>
-__device__ __forceinline__ C sum_q(const C f[Q]) {
+template <int QQ = Q, typename C>
+__device__ __forceinline__ C sum_q(const C* f) {
   C r = f[0];
 #pragma unroll
-  for (int l = 1; l < Q; ++l) r = r + f[l];
+  for (int l = 1; l < QQ; ++l) r = r + f[l];
   return r;
 }
 // manual_u/v/w sums, kernels_fluid_CG.CUF:511-529 (without the 1/rho factor)
-template <typename C> __device__ __forceinline__ C mx(const C q[Q]) { return q[1] - q[2] + q[7] - q[8] - q[9] + q[10] + q[11] - q[12] - q[13] + q[14]; }
-template <typename C> __device__ __forceinline__ C my(const C q[Q]) { return q[3] - q[4] + q[7] - q[8] + q[9] - q[10] + q[15] - q[16] - q[17] + q[18]; }
-template <typename C> __device__ __forceinline__ C mz(const C q[Q]) { return q[5] - q[6] + q[11] - q[12] + q[13] - q[14] + q[15] - q[16] + q[17] - q[18]; }
+// (D3Q27: the same sums continued over the corners 19..26 in increasing l,
+// kernels_fluid_CG.CUF:511-523)
+template <int QQ, typename C>
+__device__ __forceinline__ C msum_q(const C* q, int axis) {
+  C s = C(0);
+  bool any = false;
+#pragma unroll
+  for (int l = 1; l < QQ; ++l) {
+    const int e = axis == 0 ? ex(l) : (axis == 1 ? ey(l) : ez(l));
+    if (!e) continue;
+    s = any ? (e > 0 ? s + q[l] : s - q[l]) : (e > 0 ? q[l] : -q[l]);
+    any = true;
+  }
+  return s;
+}
+template <int QQ = Q, typename C> __device__ __forceinline__ C mx(const C* q) {
+  if constexpr (QQ == Q) return q[1] - q[2] + q[7] - q[8] - q[9] + q[10] + q[11] - q[12] - q[13] + q[14];
+  else return msum_q<QQ>(q, 0);
+}
+template <int QQ = Q, typename C> __device__ __forceinline__ C my(const C* q) {
+  if constexpr (QQ == Q) return q[3] - q[4] + q[7] - q[8] + q[9] - q[10] + q[15] - q[16] - q[17] + q[18];
+  else return msum_q<QQ>(q, 1);
+}
+template <int QQ = Q, typename C> __device__ __forceinline__ C mz(const C* q) {
+  if constexpr (QQ == Q) return q[5] - q[6] + q[11] - q[12] + q[13] - q[14] + q[15] - q[16] + q[17] - q[18];
+  else return msum_q<QQ>(q, 2);
+}
 
 // Constants of the colour-gradient collision, derived on the host like
 // SetConstants (main.CUF:1043-1162).
@@ -117,7 +141,7 @@ struct CGConst {
   // the phi / varphi / psi / xi tables per weight class (dimensions_m.CUF:231-261)
   C densR, densB;
   C alpha[2];
-  C phi[3], varphi[3], psi[3], xi[3];
+  C phi[4], varphi[4], psi[4], xi[4];
 };
 
 // equilCG, kernels_fluid_CG.CUF:40-49 (component k = 0 R, 1 B), with the
@@ -125,7 +149,7 @@ struct CGConst {
 template <typename C>
 __device__ __forceinline__ C equil_cg(const CGConst<C>& K, C rho, C edu, C usq_term, int k, int l) {
   const C uv = K.L.inv_cssq * edu;
-  const int c = wclass(l);
+  const int c = wclass27(l);
   return rho * (K.phi[c] + K.varphi[c] * K.alpha[k] + K.L.w[c] * (uv + C(0.5) * (uv * uv) - usq_term));
 }
 
@@ -135,8 +159,8 @@ __device__ __forceinline__ C equil_cg(const CGConst<C>& K, C rho, C edu, C usq_t
 // rhoR/rhoB are the clamped densities of init_rho*_CG, psi the colour
 // gradient (HIGHGRAD, D3Q27 weights).
 // ---------------------------------------------------------------------------
-template <typename C>
-__device__ __forceinline__ void cg_collide_cell(const CGConst<C>& K, C fR[Q], C fB[Q], C rhoR, C rhoB, C psix,
+template <int QQ = Q, typename C>
+__device__ __forceinline__ void cg_collide_cell(const CGConst<C>& K, C* fR, C* fB, C rhoR, C rhoB, C psix,
                                                 C psiy, C psiz) {
   const C ONE = 1, HALF = C(0.5);
   const LatticeT<C>& L = K.L;
@@ -146,12 +170,12 @@ __device__ __forceinline__ void cg_collide_cell(const CGConst<C>& K, C fR[Q], C 
   C omega = ONE / (viscavg / L.cssq + HALF);
   C omm = ONE - omega;
   C invrho = ONE / rhosum;
-  C u = invrho * mx(fR) + invrho * mx(fB);
-  C v = invrho * my(fR) + invrho * my(fB);
-  C w = invrho * mz(fR) + invrho * mz(fB);
+  C u = invrho * mx<QQ>(fR) + invrho * mx<QQ>(fB);
+  C v = invrho * my<QQ>(fR) + invrho * my<QQ>(fB);
+  C w = invrho * mz<QQ>(fR) + invrho * mz<QQ>(fB);
   C usq = L.half_inv_cssq * (u * u + v * v + w * w);
 #pragma unroll
-  for (int l = 0; l < Q; ++l) {
+  for (int l = 0; l < QQ; ++l) {
     C e = edot(l, u, v, w);
     fR[l] = fR[l] * omm + equil_u(L, rhoR, e, usq, l) * omega;
     fB[l] = fB[l] * omm + equil_u(L, rhoB, e, usq, l) * omega;
@@ -165,17 +189,18 @@ __device__ __forceinline__ void cg_collide_cell(const CGConst<C>& K, C fR[Q], C 
     C coef = K.beta * rhoR * rhoB * (invrho * invrho);
     C inv_t1 = ONE / psinorm;                 // rec_fact = 1
     C inv_t2 = ONE / (L.rec[2] * psinorm);    // rec_fact = sqrt(2)
+    C inv_t3 = ONE / (L.rec[3] * psinorm);    // rec_fact = sqrt(3) (D3Q27 corners)
 #pragma unroll
-    for (int l = 0; l < Q; ++l) {
+    for (int l = 0; l < QQ; ++l) {
       C edp = edot(l, psix, psiy, psiz);
-      C temp = psinorm * (L.w[wclass(l)] * (edp * edp) * inv_psq - L.b[wclass(l)]);
+      C temp = psinorm * (L.w[wclass27(l)] * (edp * edp) * inv_psq - L.b[wclass27(l)]);
       C fd = fR[l] + fB[l] + acoeff * temp;
-      C feq = rhoR * L.w[wclass(l)] + rhoB * L.w[wclass(l)];
+      C feq = rhoR * L.w[wclass27(l)] + rhoB * L.w[wclass27(l)];
       C cosphi;
       if (l == 0) cosphi = C(0);
       else {
-        C t1 = L.rec[wclass(l)] * psinorm;
-        cosphi = (t1 <= C(1.e-20)) ? C(0) : edp * (wclass(l) == 1 ? inv_t1 : inv_t2);
+        C t1 = L.rec[wclass27(l)] * psinorm;
+        cosphi = (t1 <= C(1.e-20)) ? C(0) : edp * (wclass27(l) == 1 ? inv_t1 : (wclass27(l) == 2 ? inv_t2 : inv_t3));
       }
       C t = coef * cosphi;
       fR[l] = fd * kR + t * feq;
@@ -190,8 +215,8 @@ __device__ __forceinline__ void cg_collide_cell(const CGConst<C>& K, C fR[Q], C 
 //   viscavg (psi_l u.grad(rho_k) + xi_l (G_k : e_l e_l)),  G_k = u grad(rho_k)^T + its transpose,
 // and the recolouring weighted by equilCG at rest.  psR / psB: D3Q27
 // gradients of the two densities; psi: gradient of the scaled phase field.
-template <typename C>
-__device__ __forceinline__ void cg_collide_cell_dd(const CGConst<C>& K, C fR[Q], C fB[Q], C rhoR, C rhoB, C psix,
+template <int QQ = Q, typename C>
+__device__ __forceinline__ void cg_collide_cell_dd(const CGConst<C>& K, C* fR, C* fB, C rhoR, C rhoB, C psix,
                                                    C psiy, C psiz, const C psR[3], const C psB[3]) {
   const C ONE = 1, HALF = C(0.5), ZERO = 0;
   const LatticeT<C>& L = K.L;
@@ -201,9 +226,9 @@ __device__ __forceinline__ void cg_collide_cell_dd(const CGConst<C>& K, C fR[Q],
   C omega = ONE / (viscavg / L.cssq + HALF);
   C omm = ONE - omega;
   C invrho = ONE / rhosum;
-  C u = invrho * mx(fR) + invrho * mx(fB);
-  C v = invrho * my(fR) + invrho * my(fB);
-  C w = invrho * mz(fR) + invrho * mz(fB);
+  C u = invrho * mx<QQ>(fR) + invrho * mx<QQ>(fB);
+  C v = invrho * my<QQ>(fR) + invrho * my<QQ>(fB);
+  C w = invrho * mz<QQ>(fR) + invrho * mz<QQ>(fB);
   C usq = L.half_inv_cssq * (u * u + v * v + w * w);
   const C vpR = u * psR[0] + v * psR[1] + w * psR[2];  // dot_product(myvel, psi_R)
   const C vpB = u * psB[0] + v * psB[1] + w * psB[2];
@@ -215,8 +240,8 @@ __device__ __forceinline__ void cg_collide_cell_dd(const CGConst<C>& K, C fR[Q],
     gB[i] = uu[i] * psB[i] + uu[i] * psB[i];
   }
 #pragma unroll
-  for (int l = 0; l < Q; ++l) {
-    const int c = wclass(l);
+  for (int l = 0; l < QQ; ++l) {
+    const int c = wclass27(l);
     const C e = edot(l, u, v, w);
     const C cx = C(ex(l) * ex(l)), cy = C(ey(l) * ey(l)), cz = C(ez(l) * ez(l));  // cmat_d(i,i,l)
     const C tR = gR[0] * cx + gR[1] * cy + gR[2] * cz;
@@ -233,17 +258,18 @@ __device__ __forceinline__ void cg_collide_cell_dd(const CGConst<C>& K, C fR[Q],
     C coef = K.beta * rhoR * rhoB * (invrho * invrho);
     C inv_t1 = ONE / psinorm;
     C inv_t2 = ONE / (L.rec[2] * psinorm);
+    C inv_t3 = ONE / (L.rec[3] * psinorm);
 #pragma unroll
-    for (int l = 0; l < Q; ++l) {
+    for (int l = 0; l < QQ; ++l) {
       C edp = edot(l, psix, psiy, psiz);
-      C temp = psinorm * (L.w[wclass(l)] * (edp * edp) * inv_psq - L.b[wclass(l)]);
+      C temp = psinorm * (L.w[wclass27(l)] * (edp * edp) * inv_psq - L.b[wclass27(l)]);
       C fd = fR[l] + fB[l] + acoeff * temp;
       C feq = equil_cg(K, rhoR, ZERO, ZERO, 0, l) + equil_cg(K, rhoB, ZERO, ZERO, 1, l);
       C cosphi;
       if (l == 0) cosphi = C(0);
       else {
-        C t1 = L.rec[wclass(l)] * psinorm;
-        cosphi = (t1 <= C(1.e-20)) ? C(0) : edp * (wclass(l) == 1 ? inv_t1 : inv_t2);
+        C t1 = L.rec[wclass27(l)] * psinorm;
+        cosphi = (t1 <= C(1.e-20)) ? C(0) : edp * (wclass27(l) == 1 ? inv_t1 : (wclass27(l) == 2 ? inv_t2 : inv_t3));
       }
       C t = coef * cosphi;
       fR[l] = fd * kR + t * feq;
@@ -322,18 +348,18 @@ inline LaunchDims cell_dims(const Ctx& c) {
 template <typename C>
 inline Shift<C> make_shift(const Ctx& c) {
   Shift<C> s;
-  LatticeT<C> L = make_lattice<C>();
+  LatticeT<C> L = make_lattice<C>(c.q);
   bool shifted = (c.storage == LBX_STORE_F16 || c.storage == LBX_STORE_BF16);
   float r0[2] = {c.p.rho0R, c.p.rho0B};
   for (int comp = 0; comp < 2; ++comp)
-    for (int k = 0; k < 3; ++k) s.s[comp][k] = shifted ? C(L.w[k] * C(r0[comp])) : C(0);
+    for (int k = 0; k < 4; ++k) s.s[comp][k] = shifted ? C(L.w[k] * C(r0[comp])) : C(0);
   return s;
 }
 
 template <typename C>
 inline CGConst<C> make_cg(const Ctx& c) {
   CGConst<C> K;
-  K.L = make_lattice<C>();
+  K.L = make_lattice<C>(c.q);
   const C HALF = C(0.5);
   C viscR = K.L.cssq * (C(c.p.tauR) - HALF);  // SetConstants, main.CUF:1069-1070
   C viscB = K.L.cssq * (C(c.p.tauB) - HALF);
@@ -342,7 +368,7 @@ inline CGConst<C> make_cg(const Ctx& c) {
   K.sigma = C(c.p.sigma);
   K.beta = C(c.p.beta);
   // DIFFDENS constants (SetConstants, main.CUF:1047-1083; dimensions_m.CUF:231-261)
-  const bool dd = c.p.model == LBX_MODEL_CG_DIFFDENS;
+  const bool dd = c.p.model == LBX_MODEL_CG_DIFFDENS || c.p.model == LBX_MODEL_CG_DIFFDENS_D3Q27;
   const C ONE = C(1), TWO = C(2), FOUR = C(4), FIVE = C(5), SIX = C(6), EIGHT = C(8), TWELVE = C(12),
           TWENTYFOUR = C(24);
   K.densR = dd ? C(c.p.densR) : ONE;
@@ -355,10 +381,18 @@ inline CGConst<C> make_cg(const Ctx& c) {
     K.alpha[1] = p0;
     K.alpha[0] = (ONE / (-ONE + K.alpha[1])) * (K.densB / K.densR) + ONE;
   }
-  K.phi[0] = C(0); K.phi[1] = ONE / TWELVE; K.phi[2] = ONE / TWENTYFOUR;
-  K.varphi[0] = ONE; K.varphi[1] = -ONE / TWELVE; K.varphi[2] = -ONE / TWENTYFOUR;
-  K.psi[0] = -FIVE / TWO; K.psi[1] = -ONE / SIX; K.psi[2] = ONE / TWENTYFOUR;
-  K.xi[0] = C(0); K.xi[1] = ONE / FOUR; K.xi[2] = ONE / EIGHT;
+  if (c.q == Q27) {  // dimensions_m.CUF:145-191
+    const C NINE = C(9), THREE = C(3);
+    K.phi[0] = C(0); K.phi[1] = TWO / C(19.0); K.phi[2] = ONE / C(38.0); K.phi[3] = ONE / C(152.0);
+    K.varphi[0] = ONE; K.varphi[1] = -TWO / C(19.0); K.varphi[2] = -ONE / C(38.0); K.varphi[3] = -ONE / C(152.0);
+    K.psi[0] = C(-20.0) / NINE; K.psi[1] = -TWO / NINE; K.psi[2] = ONE / C(36.0); K.psi[3] = ONE / C(36.0);
+    K.xi[0] = C(0); K.xi[1] = ONE / THREE; K.xi[2] = ONE / TWELVE; K.xi[3] = ONE / C(48.0);
+  } else {
+    K.phi[0] = C(0); K.phi[1] = ONE / TWELVE; K.phi[2] = ONE / TWENTYFOUR; K.phi[3] = C(0);
+    K.varphi[0] = ONE; K.varphi[1] = -ONE / TWELVE; K.varphi[2] = -ONE / TWENTYFOUR; K.varphi[3] = C(0);
+    K.psi[0] = -FIVE / TWO; K.psi[1] = -ONE / SIX; K.psi[2] = ONE / TWENTYFOUR; K.psi[3] = C(0);
+    K.xi[0] = C(0); K.xi[1] = ONE / FOUR; K.xi[2] = ONE / EIGHT; K.xi[3] = C(0);
+  }
   return K;
 }
 

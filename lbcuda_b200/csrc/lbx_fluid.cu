@@ -36,7 +36,7 @@ namespace lbx {
 // stored buffer holds, at x, the populations that streaming moves to x + e_l,
 // so that the first step gathers exactly the equilibrium of the given fields
 // (equilCG with two fluid densities, kernels_fluid_CG.CUF:176-178).
-template <typename S, bool DD>
+template <typename S, bool DD, int QQ>
 __global__ void k_set_fields(S* __restrict__ A, S* __restrict__ B, Geom g, int ncomp, const float* __restrict__ rR,
                              const float* __restrict__ rB, float vx, float vy, float vz,
                              CGConst<typename Store<S>::C> K, Shift<typename Store<S>::C> sh) {
@@ -52,7 +52,7 @@ __global__ void k_set_fields(S* __restrict__ A, S* __restrict__ B, Geom g, int n
   for (int comp = 0; comp < ncomp; ++comp) {
     const float* r = comp ? rB : rR;
 #pragma unroll
-    for (int l = 0; l < Q; ++l) {
+    for (int l = 0; l < QQ; ++l) {
       C rho = C(r[at(b, ex(l), ey(l), ez(l))]);
       C val = DD ? equil_cg(K, rho, edot(l, u, v, w), usq, comp, l) : equil_u(L, rho, edot(l, u, v, w), usq, l);
       Store<S>::st(A + pidx(g, comp, l, cell), val, sh.at(comp, l));
@@ -62,7 +62,7 @@ __global__ void k_set_fields(S* __restrict__ A, S* __restrict__ B, Geom g, int n
 }
 
 // initType 4: raw post-streaming populations, stored in pull convention
-template <typename S>
+template <typename S, int QQ>
 __global__ void k_set_pops(S* __restrict__ A, Geom g, int ncomp, const float* __restrict__ pR,
                            const float* __restrict__ pB, Shift<typename Store<S>::C> sh) {
   using C = typename Store<S>::C;
@@ -74,7 +74,7 @@ __global__ void k_set_pops(S* __restrict__ A, Geom g, int ncomp, const float* __
   for (int comp = 0; comp < ncomp; ++comp) {
     const float* p = comp ? pB : pR;
 #pragma unroll
-    for (int l = 0; l < Q; ++l)
+    for (int l = 0; l < QQ; ++l)
       Store<S>::st(A + pidx(g, comp, l, cell), C(p[size_t(l) * size_t(g.n) + at(b, ex(l), ey(l), ez(l))]),
                    sh.at(comp, l));
   }
@@ -82,7 +82,7 @@ __global__ void k_set_pops(S* __restrict__ A, Geom g, int ncomp, const float* __
 
 // init_rhoR_CG + init_rhoB_CG (all cells fluid) producing the phase field of
 // the two-pass schedule and, optionally, the densities.
-template <typename S>
+template <typename S, int QQ>
 __global__ void __launch_bounds__(256) k_cg_phi(const S* __restrict__ A, Geom g, Shift<typename Store<S>::C> sh,
                                                  typename Store<S>::C* __restrict__ phi,
                                                  typename Store<S>::C* __restrict__ rhoR,
@@ -94,11 +94,11 @@ __global__ void __launch_bounds__(256) k_cg_phi(const S* __restrict__ A, Geom g,
   Nbr b;
   make_nbr(g, x, y, z, b);
   int cell = at(b, 0, 0, 0);
-  C f[Q];
-  pull(A, g, b, 0, sh, f);
-  C rR = sum_q(f);
-  pull(A, g, b, 1, sh, f);
-  C rB = sum_q(f);
+  C f[QQ];
+  pull<QQ>(A, g, b, 0, sh, f);
+  C rR = sum_q<QQ>(f);
+  pull<QQ>(A, g, b, 1, sh, f);
+  C rB = sum_q<QQ>(f);
   if (rR < C(-10) || rR > C(10) || rB < C(-10) || rB > C(10)) raise_error(err, LBX_DEV_RHO_RANGE, step, cell);
   if (rR < C(0)) rR = C(0);
   if (rB < C(0)) rB = C(0);
@@ -109,7 +109,7 @@ __global__ void __launch_bounds__(256) k_cg_phi(const S* __restrict__ A, Geom g,
 // time_step_CG + streaming, two-pass schedule: pull, densities, gradient from
 // the phase-field array (DD, two fluid densities: from the density arrays),
 // collision, aligned store.
-template <typename S, bool DD>
+template <typename S, bool DD, int QQ>
 __global__ void __launch_bounds__(256) k_cg_collide(const S* __restrict__ A, S* __restrict__ B, Geom g,
                                                      Shift<typename Store<S>::C> sh,
                                                      const typename Store<S>::C* __restrict__ phi,
@@ -122,10 +122,10 @@ __global__ void __launch_bounds__(256) k_cg_collide(const S* __restrict__ A, S* 
   Nbr b;
   make_nbr(g, x, y, z, b);
   int cell = at(b, 0, 0, 0);
-  C fR[Q], fB[Q];
-  pull(A, g, b, 0, sh, fR);
-  pull(A, g, b, 1, sh, fB);
-  C rR = sum_q(fR), rB = sum_q(fB);
+  C fR[QQ], fB[QQ];
+  pull<QQ>(A, g, b, 0, sh, fR);
+  pull<QQ>(A, g, b, 1, sh, fB);
+  C rR = sum_q<QQ>(fR), rB = sum_q<QQ>(fB);
   if (rR < C(0)) rR = C(0);
   if (rB < C(0)) rB = C(0);
   C psix, psiy, psiz;
@@ -139,13 +139,13 @@ __global__ void __launch_bounds__(256) k_cg_collide(const S* __restrict__ A, S* 
           bs = __ldg(rhoBa + y);
         },
         psix, psiy, psiz, psR, psB);
-    cg_collide_cell_dd(K, fR, fB, rR, rB, psix, psiy, psiz, psR, psB);
+    cg_collide_cell_dd<QQ>(K, fR, fB, rR, rB, psix, psiy, psiz, psR, psB);
   } else {
     grad27(K.L, [&](int dx, int dy, int dz) { return __ldg(phi + at(b, dx, dy, dz)); }, psix, psiy, psiz);
-    cg_collide_cell(K, fR, fB, rR, rB, psix, psiy, psiz);
+    cg_collide_cell<QQ>(K, fR, fB, rR, rB, psix, psiy, psiz);
   }
-  store_all(B, g, cell, 0, sh, fR);
-  store_all(B, g, cell, 1, sh, fB);
+  store_all<QQ>(B, g, cell, 0, sh, fR);
+  store_all<QQ>(B, g, cell, 1, sh, fB);
 }
 
 // ---------------------------------------------------------------------------
@@ -285,7 +285,7 @@ __global__ void __launch_bounds__(256) k_bgk(const S* __restrict__ A, S* __restr
 }
 
 // moments2Fl on the post-streaming populations (pulled from the state)
-template <typename S, typename O>
+template <typename S, typename O, int QQ>
 __global__ void k_fields(const S* __restrict__ A, const S* Bold, Geom g, int ncomp, Shift<typename Store<S>::C> sh,
                          const int8_t* __restrict__ flags, const int8_t* __restrict__ fold, O* rR, O* rB, O* vel,
                          O* phase) {
@@ -295,17 +295,17 @@ __global__ void k_fields(const S* __restrict__ A, const S* Bold, Geom g, int nco
   Nbr b;
   make_nbr(g, x, y, z, b);
   int cell = at(b, 0, 0, 0);
-  C fR[Q], fB[Q];
-  pull_any(A, Bold, g, b, 0, sh, fold, fR);
-  if (ncomp == 2) pull_any(A, Bold, g, b, 1, sh, fold, fB);
+  C fR[QQ], fB[QQ];
+  pull_any<QQ>(A, Bold, g, b, 0, sh, fold, fR);
+  if (ncomp == 2) pull_any<QQ>(A, Bold, g, b, 1, sh, fold, fB);
   else {
 #pragma unroll
-    for (int l = 0; l < Q; ++l) fB[l] = C(0);
+    for (int l = 0; l < QQ; ++l) fB[l] = C(0);
   }
-  C lr = sum_q(fR), lb = sum_q(fB);
+  C lr = sum_q<QQ>(fR), lb = sum_q<QQ>(fB);
   C rs = lr + lb;
   C inv = C(1) / rs;
-  C u = inv * (mx(fR) + mx(fB)), v = inv * (my(fR) + my(fB)), w = inv * (mz(fR) + mz(fB));
+  C u = inv * (mx<QQ>(fR) + mx<QQ>(fB)), v = inv * (my<QQ>(fR) + my<QQ>(fB)), w = inv * (mz<QQ>(fR) + mz<QQ>(fB));
   bool ok = (!flags || flags[cell] == LBX_FLUID_FLUID) && rs > C(0);
   if (rR) rR[cell] = ok ? O(lr) : O(0);
   if (rB) rB[cell] = ok ? O(lb) : O(0);
@@ -317,7 +317,7 @@ __global__ void k_fields(const S* __restrict__ A, const S* Bold, Geom g, int nco
   if (phase) phase[cell] = ok ? O((lr - lb) / (lr + lb)) : O(0);
 }
 
-template <typename S>
+template <typename S, int QQ>
 __global__ void k_get_pops(const S* __restrict__ A, const S* Bold, Geom g, int ncomp, Shift<typename Store<S>::C> sh,
                            const int8_t* __restrict__ fold, float* pR, float* pB) {
   using C = typename Store<S>::C;
@@ -326,19 +326,19 @@ __global__ void k_get_pops(const S* __restrict__ A, const S* Bold, Geom g, int n
   Nbr b;
   make_nbr(g, x, y, z, b);
   int cell = at(b, 0, 0, 0);
-  C f[Q];
+  C f[QQ];
   for (int comp = 0; comp < ncomp; ++comp) {
     float* out = comp ? pB : pR;
     if (!out) continue;
-    pull_any(A, Bold, g, b, comp, sh, fold, f);
+    pull_any<QQ>(A, Bold, g, b, comp, sh, fold, f);
 #pragma unroll
-    for (int l = 0; l < Q; ++l) out[size_t(l) * size_t(g.n) + cell] = float(f[l]);
+    for (int l = 0; l < QQ; ++l) out[size_t(l) * size_t(g.n) + cell] = float(f[l]);
   }
 }
 
 // FP64 mass (per component) and momentum of the post-streaming populations,
 // block partial sums combined with FP64 atomics.
-template <typename S>
+template <typename S, int QQ>
 __global__ void k_sums(const S* __restrict__ A, const S* Bold, Geom g, int ncomp, Shift<typename Store<S>::C> sh,
                        const int8_t* __restrict__ flags, const int8_t* __restrict__ fold, double* out) {
   using C = typename Store<S>::C;
@@ -349,16 +349,16 @@ __global__ void k_sums(const S* __restrict__ A, const S* Bold, Geom g, int ncomp
     make_nbr(g, x, y, z, b);
     int cell = at(b, 0, 0, 0);
     if (!flags || flags[cell] == LBX_FLUID_FLUID) {
-      C f[Q];
+      C f[QQ];
       for (int comp = 0; comp < ncomp; ++comp) {
-        pull_any(A, Bold, g, b, comp, sh, fold, f);
+        pull_any<QQ>(A, Bold, g, b, comp, sh, fold, f);
         double m = 0;
 #pragma unroll
-        for (int l = 0; l < Q; ++l) m += double(f[l]);
+        for (int l = 0; l < QQ; ++l) m += double(f[l]);
         acc[comp] = m;
-        acc[2] += double(mx(f));
-        acc[3] += double(my(f));
-        acc[4] += double(mz(f));
+        acc[2] += double(mx<QQ>(f));
+        acc[3] += double(my<QQ>(f));
+        acc[4] += double(mz<QQ>(f));
       }
     }
   }
@@ -373,7 +373,7 @@ __global__ void k_sums(const S* __restrict__ A, const S* Bold, Geom g, int ncomp
 // host side
 // ---------------------------------------------------------------------------
 int fluid_alloc(Ctx& c) {
-  size_t bytes = size_t(c.ncomp) * Q * size_t(c.n) * c.elem;
+  size_t bytes = size_t(c.ncomp) * size_t(c.q) * size_t(c.n) * c.elem;
   for (int i = 0; i < 2; ++i)
     if (cudaMalloc(&c.pops[i], bytes) != cudaSuccess) return LBX_ERR_ALLOC;
   size_t cb = (c.storage == LBX_STORE_F64) ? 8 : 4;
@@ -400,6 +400,16 @@ void fluid_free(Ctx& c) {
   c.phi = nullptr;
 }
 
+// fn(std::integral_constant<int, QQ>) with QQ = the context's populations per component
+template <typename F>
+static int by_lattice(const Ctx& c, F&& fn) {
+  if (c.q == Q27) return fn(std::integral_constant<int, Q27>{});
+  return fn(std::integral_constant<int, Q>{});
+}
+static bool two_densities(const Ctx& c) {
+  return c.p.model == LBX_MODEL_CG_DIFFDENS || c.p.model == LBX_MODEL_CG_DIFFDENS_D3Q27;
+}
+
 static void reset_flags(Ctx& c) {
   for (int i = 0; i < 2; ++i) cudaMemsetAsync(c.flags[i], LBX_FLUID_FLUID, size_t(c.n), c.stream);
   c.fcur = 0;
@@ -413,13 +423,16 @@ int fluid_set_fields(Ctx& c, const float* d_rR, const float* d_rB, float vx, flo
   return by_storage(c, [&](auto* tag) {
     using S = std::remove_pointer_t<decltype(tag)>;
     using C = typename Store<S>::C;
-    if (c.p.model == LBX_MODEL_CG_DIFFDENS)
-      k_set_fields<S, true><<<d.grid, d.block, 0, c.stream>>>((S*)c.pops[0], (S*)c.pops[1], g, c.ncomp, d_rR, d_rB,
-                                                              vx, vy, vz, make_cg<C>(c), make_shift<C>(c));
-    else
-      k_set_fields<S, false><<<d.grid, d.block, 0, c.stream>>>((S*)c.pops[0], (S*)c.pops[1], g, c.ncomp, d_rR, d_rB,
-                                                               vx, vy, vz, make_cg<C>(c), make_shift<C>(c));
-    return launch_status();
+    return by_lattice(c, [&](auto qt) {
+      constexpr int QQ = decltype(qt)::value;
+      if (two_densities(c))
+        k_set_fields<S, true, QQ><<<d.grid, d.block, 0, c.stream>>>((S*)c.pops[0], (S*)c.pops[1], g, c.ncomp, d_rR,
+                                                                    d_rB, vx, vy, vz, make_cg<C>(c), make_shift<C>(c));
+      else
+        k_set_fields<S, false, QQ><<<d.grid, d.block, 0, c.stream>>>((S*)c.pops[0], (S*)c.pops[1], g, c.ncomp, d_rR,
+                                                                     d_rB, vx, vy, vz, make_cg<C>(c), make_shift<C>(c));
+      return launch_status();
+    });
   });
 }
 
@@ -431,8 +444,11 @@ int fluid_set_pops(Ctx& c, const float* d_pR, const float* d_pB) {
   return by_storage(c, [&](auto* tag) {
     using S = std::remove_pointer_t<decltype(tag)>;
     using C = typename Store<S>::C;
-    k_set_pops<S><<<d.grid, d.block, 0, c.stream>>>((S*)c.pops[0], g, c.ncomp, d_pR, d_pB, make_shift<C>(c));
-    return launch_status();
+    return by_lattice(c, [&](auto qt) {
+      constexpr int QQ = decltype(qt)::value;
+      k_set_pops<S, QQ><<<d.grid, d.block, 0, c.stream>>>((S*)c.pops[0], g, c.ncomp, d_pR, d_pB, make_shift<C>(c));
+      return launch_status();
+    });
   });
 }
 
@@ -460,9 +476,12 @@ int fluid_init_rho(Ctx& c) {
   return by_storage(c, [&](auto* tag) {
     using S = std::remove_pointer_t<decltype(tag)>;
     using C = typename Store<S>::C;
-    k_cg_phi<S><<<d.grid, d.block, 0, c.stream>>>((const S*)c.pops[c.cur], g, make_shift<C>(c), (C*)c.phi,
-                                                  (C*)c.rho[0], (C*)c.rho[1], c.d_err, c.step + 1);
-    return launch_status();
+    return by_lattice(c, [&](auto qt) {
+      constexpr int QQ = decltype(qt)::value;
+      k_cg_phi<S, QQ><<<d.grid, d.block, 0, c.stream>>>((const S*)c.pops[c.cur], g, make_shift<C>(c), (C*)c.phi,
+                                                        (C*)c.rho[0], (C*)c.rho[1], c.d_err, c.step + 1);
+      return launch_status();
+    });
   });
 }
 
@@ -474,14 +493,19 @@ int fluid_collide_stream(Ctx& c) {
     using S = std::remove_pointer_t<decltype(tag)>;
     using C = typename Store<S>::C;
     kt_begin(c);
-    if (c.p.model == LBX_MODEL_CG_DIFFDENS)
-      k_cg_collide<S, true><<<d.grid, d.block, 0, c.stream>>>((const S*)c.pops[c.cur], (S*)c.pops[1 - c.cur], g,
-                                                              make_shift<C>(c), (const C*)c.phi, (const C*)c.rho[0],
-                                                              (const C*)c.rho[1], make_cg<C>(c));
-    else
-      k_cg_collide<S, false><<<d.grid, d.block, 0, c.stream>>>((const S*)c.pops[c.cur], (S*)c.pops[1 - c.cur], g,
-                                                               make_shift<C>(c), (const C*)c.phi, nullptr, nullptr,
-                                                               make_cg<C>(c));
+    by_lattice(c, [&](auto qt) {
+      constexpr int QQ = decltype(qt)::value;
+      if (two_densities(c))
+        k_cg_collide<S, true, QQ><<<d.grid, d.block, 0, c.stream>>>((const S*)c.pops[c.cur], (S*)c.pops[1 - c.cur], g,
+                                                                    make_shift<C>(c), (const C*)c.phi,
+                                                                    (const C*)c.rho[0], (const C*)c.rho[1],
+                                                                    make_cg<C>(c));
+      else
+        k_cg_collide<S, false, QQ><<<d.grid, d.block, 0, c.stream>>>((const S*)c.pops[c.cur], (S*)c.pops[1 - c.cur],
+                                                                     g, make_shift<C>(c), (const C*)c.phi, nullptr,
+                                                                     nullptr, make_cg<C>(c));
+      return 0;
+    });
     kt_end(c);
     c.cur = 1 - c.cur;
     return launch_status();
@@ -568,15 +592,18 @@ int fluid_get_fields(Ctx& c, void* rR, void* rB, void* vel, void* phase, int f64
     using C = typename Store<S>::C;
     const S* A = (const S*)c.pops[c.cur];
     const S* Bo = (const S*)c.pops[1 - c.cur];
-    if (f64)
-      k_fields<S, double><<<d.grid, d.block, 0, c.stream>>>(A, Bo, g, c.ncomp, make_shift<C>(c), mask_flags(c),
-                                                            dead_flags(c), (double*)rR, (double*)rB, (double*)vel,
-                                                            (double*)phase);
-    else
-      k_fields<S, float><<<d.grid, d.block, 0, c.stream>>>(A, Bo, g, c.ncomp, make_shift<C>(c), mask_flags(c),
-                                                           dead_flags(c), (float*)rR, (float*)rB, (float*)vel,
-                                                           (float*)phase);
-    return launch_status();
+    return by_lattice(c, [&](auto qt) {
+      constexpr int QQ = decltype(qt)::value;
+      if (f64)
+        k_fields<S, double, QQ><<<d.grid, d.block, 0, c.stream>>>(A, Bo, g, c.ncomp, make_shift<C>(c), mask_flags(c),
+                                                                  dead_flags(c), (double*)rR, (double*)rB,
+                                                                  (double*)vel, (double*)phase);
+      else
+        k_fields<S, float, QQ><<<d.grid, d.block, 0, c.stream>>>(A, Bo, g, c.ncomp, make_shift<C>(c), mask_flags(c),
+                                                                 dead_flags(c), (float*)rR, (float*)rB, (float*)vel,
+                                                                 (float*)phase);
+      return launch_status();
+    });
   });
 }
 
@@ -586,9 +613,12 @@ int fluid_get_pops(Ctx& c, float* pR, float* pB) {
   return by_storage(c, [&](auto* tag) {
     using S = std::remove_pointer_t<decltype(tag)>;
     using C = typename Store<S>::C;
-    k_get_pops<S><<<d.grid, d.block, 0, c.stream>>>((const S*)c.pops[c.cur], (const S*)c.pops[1 - c.cur], g,
-                                                    c.ncomp, make_shift<C>(c), dead_flags(c), pR, pB);
-    return launch_status();
+    return by_lattice(c, [&](auto qt) {
+      constexpr int QQ = decltype(qt)::value;
+      k_get_pops<S, QQ><<<d.grid, d.block, 0, c.stream>>>((const S*)c.pops[c.cur], (const S*)c.pops[1 - c.cur], g,
+                                                          c.ncomp, make_shift<C>(c), dead_flags(c), pR, pB);
+      return launch_status();
+    });
   });
 }
 
@@ -599,9 +629,12 @@ int fluid_get_sums(Ctx& c, double* d_out5) {
   return by_storage(c, [&](auto* tag) {
     using S = std::remove_pointer_t<decltype(tag)>;
     using C = typename Store<S>::C;
-    k_sums<S><<<d.grid, d.block, 0, c.stream>>>((const S*)c.pops[c.cur], (const S*)c.pops[1 - c.cur], g, c.ncomp,
-                                                make_shift<C>(c), mask_flags(c), dead_flags(c), d_out5);
-    return launch_status();
+    return by_lattice(c, [&](auto qt) {
+      constexpr int QQ = decltype(qt)::value;
+      k_sums<S, QQ><<<d.grid, d.block, 0, c.stream>>>((const S*)c.pops[c.cur], (const S*)c.pops[1 - c.cur], g,
+                                                      c.ncomp, make_shift<C>(c), mask_flags(c), dead_flags(c), d_out5);
+      return launch_status();
+    });
   });
 }
 

@@ -72,3 +72,86 @@ def test_d3q27_differs_from_d3q19():
         o.step(10)
         out.append(o.get_fields())
     assert rel(out[0][2], out[1][2]) > 1e-3
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("model,init", [("cg-d3q27", "droplet"), ("cg-d3q27", "noise"),
+                                        ("cg-diffdens-d3q27", "droplet")])
+def test_d3q27_f32_matches_oracle(model, init):
+    from lbcuda_b200 import LBSim
+    n = 32
+    dens = (2.0, 1.0) if "diffdens" in model else (1.0, 1.0)
+    p = make_params(n, model=model, storage="f32", sigma=0.05, beta=0.9, densR=dens[0], densB=dens[1])
+    if init == "droplet":
+        rR, rB = initial_fields(1, n, n, n, dens=dens)
+        vel = (0.02, -0.01, 0.01)
+    else:
+        rR, rB = seeded_noise_fields(n, n, n, seed=6)
+        vel = (0.0, 0.0, 0.0)
+    g = LBSim(p)
+    g.set_fields(rR, rB, vel)
+    g.step(30)
+    o = OracleSim(p, "ref")
+    o.set_fields(rR, rB, vel)
+    assert o.step(30) == 0
+    for name, a, b in zip(("rhoR", "rhoB", "vel", "phase"), g.get_fields(), o.get_fields()):
+        e = rel_l2(a, b) if name == "vel" else rel(a, b)
+        assert e <= (5e-5 if (name == "vel" and init == "noise") else 1e-5), (name, e)
+    pg, po = g.get_pops(), o.get_pops()
+    assert pg[0].shape[0] == 27
+    assert rel(pg[0], po[0]) <= 1e-5 and rel(pg[1], po[1]) <= 1e-5
+    assert g.status()[0] == 0
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("storage,tol", [("f64", 1e-12), ("f16", 1e-2)])
+def test_d3q27_other_storage(storage, tol):
+    """FP64 storage against the FP64 oracle (1e-12); FP16 shifted storage
+    against the FP64 oracle within its rounding (1e-2 on the phase field
+    after 20 steps of a droplet)."""
+    from lbcuda_b200 import LBSim
+    n = 24
+    p = make_params(n, model="cg-d3q27", storage=storage, sigma=0.05, beta=0.9)
+    rR, rB = initial_fields(1, n, n, n)
+    g = LBSim(p)
+    g.set_fields(rR, rB, (0.01, 0.02, 0.0))
+    g.step(20)
+    o = OracleSim(p, "f64")
+    o.set_fields(rR, rB, (0.01, 0.02, 0.0))
+    o.step(20)
+    gf, of = g.get_fields(f64=True), o.get_fields()
+    if storage == "f64":
+        for a, b in zip(gf, of):
+            assert rel(a, b) <= tol
+    else:
+        assert rel_l2(gf[3], of[3]) <= tol
+
+
+@pytest.mark.gpu
+def test_d3q27_rejects_spheres_and_single_pass():
+    from lbcuda_b200 import LBSim, LBXError
+    with pytest.raises(LBXError):
+        LBSim(make_params(32, model="cg-d3q27", storage="f32", max_particles=1))
+    g = LBSim(make_params(16, model="cg-d3q27", storage="f32"))
+    with pytest.raises(LBXError):
+        g.set_schedule(2)
+    g.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("storage,bound", [("f32", 2.5e-6), ("f64", 1e-12)])
+def test_d3q27_mass(storage, bound):
+    """FP64 sums of each component's mass over 20 steps.  The FP32 weights
+    of the D3Q27 build sum to 1 + 1.08e-7 (the D3Q19 ones to 1 + 1.5e-8), so
+    each BGK step at omega = 1 adds about 1.1e-7 of the mass in FP32, as the
+    reference's FP32 tables do; FP64 storage and tables conserve it."""
+    from lbcuda_b200 import LBSim
+    g = LBSim(make_params(16, model="cg-d3q27", storage=storage))
+    rR, rB = seeded_noise_fields(16, 16, 16, seed=1)
+    g.set_fields(rR, rB)
+    g.step(1)
+    m0, _ = g.get_sums()
+    g.step(20)
+    m1, _ = g.get_sums()
+    assert (np.abs(m1 - m0) / m0 <= bound).all(), np.abs(m1 - m0) / m0
+    g.close()
