@@ -265,6 +265,27 @@ def colloid_timing(storage, steps=50, warm=10, small=False):
             "frac_at_basis": mlups * 1e6 * BYTES_PER_CELL[storage] / 1e9 / peaks()[0], "device_error": code}
 
 
+def variants_timing(storage, steps=100, warm=20):
+    """The reference's compile-time variants as models (densR = 2, densB = 1 for the two-density ones,
+    as in its namelist deck): the spinodal workload at 128^3 on the two-pass schedule (phase field /
+    densities, then the collision), single density on D3Q19 beside them for scale."""
+    from lbcuda_b200 import LBSim, make_params
+    from lbcuda_b200.inputs import seeded_noise_fields
+    rR, rB = seeded_noise_fields(L, L, L, seed=SEED)
+    out = {"storage": storage, "densR": 2.0, "densB": 1.0, "schedule": "two-pass"}
+    for model in ("cg", "cg-diffdens", "cg-d3q27", "cg-diffdens-d3q27"):
+        s = LBSim(make_params(L, model=model, storage=storage, sigma=SIGMA, beta=BETA, densR=2.0, densB=1.0))
+        s.set_schedule(0)
+        s.set_fields((2.0 * rR).astype(np.float32) if "diffdens" in model else rR, rB)
+        s.step(warm)
+        s.sync()
+        tot, _, _ = s.time_steps(steps, kernel_timing=False)
+        out[model] = {"ms_per_step": tot / steps, "mlups": L ** 3 * steps / (tot * 1e-3) / 1e6,
+                      "device_error": s.status()[0]}
+        s.close()
+    return out
+
+
 def ensemble_timing(steps=100, err_steps=200, seed=7):
     """Ensemble workload: 48 boxes, edges uniform from {32, 48, 64, 96}, 0-40 spheres of radius 4 each
     (seeded, min gap 1), FP16 storage, closure switched on without weights (every close pair takes the
@@ -368,6 +389,9 @@ def only_region(args, local):
     if args.only == "ensemble":
         print(json.dumps(ensemble_timing()), flush=True)
         return 0
+    if args.only == "variants":
+        print(json.dumps({st: variants_timing(st) for st in ("f32", "f16")}), flush=True)
+        return 0
     if args.only.startswith("colloid"):
         r = colloid_timing(args.only.split("-")[1], steps=max(1, args.steps) * 5, warm=args.warmup,
                            small=args.only.endswith("small"))
@@ -396,7 +420,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-extras", action="store_true", help="skip the error runs, the colloid case and the CPU baseline")
     ap.add_argument("--only", choices=["f16", "f32", "bf16", "f64", "colloid-f16", "colloid-f32", "colloid-f16-small",
-                                       "colloid-f32-small", "ensemble", "closure"],
+                                       "colloid-f32-small", "ensemble", "closure", "variants"],
                     help="profiling aid: run one timed region only and print its timing")
     ap.add_argument("--lb-steps", type=int, default=LB_PER_STEP, help="lattice steps per bench step")
     ap.add_argument("--schedule", type=int, default=2, help="colour-gradient schedule (0, 1, 2)")
@@ -506,6 +530,7 @@ def main():
         extras["error_vs_f64"] = error_vs_f64()
         extras["colloid_256_1280"] = {st: colloid_timing(st) for st in ("f16", "f32")}
         extras["ensemble_48"] = ensemble_timing()
+        extras["variants_128"] = {st: variants_timing(st) for st in ("f32", "f16")}
         extras["closure"] = closure_experiment()
         extras["cpu_baseline"] = cpu_baseline_sample()
 

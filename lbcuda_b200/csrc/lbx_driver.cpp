@@ -309,9 +309,11 @@ int main(int argc, char** argv) {
       p.storage = t == "f16" ? LBX_STORE_F16 : t == "bf16" ? LBX_STORE_BF16 : t == "f64" ? LBX_STORE_F64 : LBX_STORE_F32;
     } else if (s == "--bgk") p.model = LBX_MODEL_BGK;
     else if (s == "--diffdens") {  // two fluid densities: --diffdens densR densB
-      p.model = LBX_MODEL_CG_DIFFDENS;
+      p.model = (p.model == LBX_MODEL_CG_D3Q27) ? LBX_MODEL_CG_DIFFDENS_D3Q27 : LBX_MODEL_CG_DIFFDENS;
       p.densR = float(std::atof(nxt()));
       p.densB = float(std::atof(nxt()));
+    } else if (s == "--d3q27") {  // the D3Q27 lattice (with --diffdens: both)
+      p.model = (p.model == LBX_MODEL_CG_DIFFDENS) ? LBX_MODEL_CG_DIFFDENS_D3Q27 : LBX_MODEL_CG_D3Q27;
     }
     else if (s == "--sigma") p.sigma = std::atof(nxt());
     else if (s == "--beta") p.beta = std::atof(nxt());
