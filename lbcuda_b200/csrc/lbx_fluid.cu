@@ -87,7 +87,8 @@ __global__ void __launch_bounds__(256) k_cg_phi(const S* __restrict__ A, Geom g,
                                                  typename Store<S>::C* __restrict__ phi,
                                                  typename Store<S>::C* __restrict__ rhoR,
                                                  typename Store<S>::C* __restrict__ rhoB,
-                                                 unsigned long long* err, int64_t step) {
+                                                 unsigned long long* err, int64_t step, typename Store<S>::C densR,
+                                                 typename Store<S>::C densB) {
   using C = typename Store<S>::C;
   int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y, z = blockIdx.z;
   if (x >= g.nx || y >= g.ny) return;
@@ -102,7 +103,9 @@ __global__ void __launch_bounds__(256) k_cg_phi(const S* __restrict__ A, Geom g,
   if (rR < C(-10) || rR > C(10) || rB < C(-10) || rB > C(10)) raise_error(err, LBX_DEV_RHO_RANGE, step, cell);
   if (rR < C(0)) rR = C(0);
   if (rB < C(0)) rB = C(0);
-  phi[cell] = (rR - rB) / (rR + rB);
+  // the phase field the gradient takes (psi_shifted, kernels_fluid_CG.CUF:
+  // 728-729: scaled by the fluid densities, 1 and 1 for a single density)
+  phi[cell] = (rR / densR - rB / densB) / (rR / densR + rB / densB);
   if (rhoR) { rhoR[cell] = rR; rhoB[cell] = rB; }
 }
 
@@ -130,15 +133,15 @@ __global__ void __launch_bounds__(256) k_cg_collide(const S* __restrict__ A, S* 
   if (rB < C(0)) rB = C(0);
   C psix, psiy, psiz;
   if constexpr (DD) {
-    C psR[3], psB[3];
-    grad27_dd(
-        K,
-        [&](int dx, int dy, int dz, C& rs, C& bs) {
-          const int y = at(b, dx, dy, dz);
-          rs = __ldg(rhoRa + y);
-          bs = __ldg(rhoBa + y);
-        },
-        psix, psiy, psiz, psR, psB);
+    // psi from the scaled phase field k_cg_phi stored (the same quotient per
+    // neighbour as psi_shifted), the two density gradients from the density
+    // arrays
+    C psR[3], psB[3], sx, sy, sz;
+    grad27(K.L, [&](int dx, int dy, int dz) { return __ldg(phi + at(b, dx, dy, dz)); }, psix, psiy, psiz);
+    grad27(K.L, [&](int dx, int dy, int dz) { return __ldg(rhoRa + at(b, dx, dy, dz)); }, sx, sy, sz);
+    psR[0] = sx; psR[1] = sy; psR[2] = sz;
+    grad27(K.L, [&](int dx, int dy, int dz) { return __ldg(rhoBa + at(b, dx, dy, dz)); }, sx, sy, sz);
+    psB[0] = sx; psB[1] = sy; psB[2] = sz;
     cg_collide_cell_dd<QQ>(K, fR, fB, rR, rB, psix, psiy, psiz, psR, psB);
   } else {
     grad27(K.L, [&](int dx, int dy, int dz) { return __ldg(phi + at(b, dx, dy, dz)); }, psix, psiy, psiz);
@@ -478,8 +481,10 @@ int fluid_init_rho(Ctx& c) {
     using C = typename Store<S>::C;
     return by_lattice(c, [&](auto qt) {
       constexpr int QQ = decltype(qt)::value;
+      const CGConst<C> K = make_cg<C>(c);
       k_cg_phi<S, QQ><<<d.grid, d.block, 0, c.stream>>>((const S*)c.pops[c.cur], g, make_shift<C>(c), (C*)c.phi,
-                                                        (C*)c.rho[0], (C*)c.rho[1], c.d_err, c.step + 1);
+                                                        (C*)c.rho[0], (C*)c.rho[1], c.d_err, c.step + 1, K.densR,
+                                                        K.densB);
       return launch_status();
     });
   });
