@@ -39,6 +39,7 @@ template <typename C>
 struct LeanConst {
   C w[3], b[3], a27[4];
   C sqrt2;
+  C w2_sqrt2;        // w_2 / sqrt 2 (recolouring weight of the face diagonals)
   C omega;           // uniform relaxation (tauR == tauB), else negative
   C inv_viscR, inv_viscB, inv_cssq;
   C sigma, beta;
@@ -53,6 +54,7 @@ LeanConst<C> make_lean(const Ctx& c) {
   for (int i = 0; i < 3; ++i) { K.w[i] = L.w[i]; K.b[i] = L.b[i]; }
   for (int i = 0; i < 4; ++i) K.a27[i] = L.a27[i];
   K.sqrt2 = L.rec[2];
+  K.w2_sqrt2 = K.w[2] / K.sqrt2;
   const C HALF = C(0.5);
   C viscR = L.cssq * (C(c.p.tauR) - HALF), viscB = L.cssq * (C(c.p.tauB) - HALF);
   K.inv_viscR = C(1) / viscR;
@@ -461,7 +463,7 @@ __device__ __forceinline__ bool recolour_sums(const LeanConst<C>& K, const Relax
   }
   K3[0] = C(0);
   K3[1] = coef * K.w[1];
-  K3[2] = coef * K.w[2] / K.sqrt2;
+  K3[2] = coef * K.w2_sqrt2;
   const P2<C> KK = pp(kR, kB);
   {
     const C fd = X.h0 - K0[0];
@@ -700,17 +702,18 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
     const int zz = wrap_plane(p, g.nz);
     if constexpr (PART) {
       if (parts) {
-        const int co = x + g.nx * (y + g.ny * zz);
+        // unsigned cell offsets: one 32 x 32 -> 64-bit multiply-add per address
+        const unsigned co = unsigned(x) + unsigned(g.nx) * (unsigned(y) + unsigned(g.ny) * unsigned(zz));
         SideRec<C>* so = side + own_q(p) * NT + tid;
-        cp_async4(&so->fnew_w, PT.fnew + (co & ~3));
-        cp_async4(&so->fold_w, PT.fold + (co & ~3));
-        cp_async_c(&so->phi, PT.phi + co);
+        cp_async4(&so->fnew_w, PT.fnew + size_t(co & ~3u));
+        cp_async4(&so->fold_w, PT.fold + size_t(co & ~3u));
+        cp_async_c(&so->phi, PT.phi + size_t(co));
         if (ringer) {
-          const int cr = rxg + g.nx * (ryg + g.ny * zz);
+          const unsigned cr = unsigned(rxg) + unsigned(g.nx) * (unsigned(ryg) + unsigned(g.ny) * unsigned(zz));
           SideRec<C>* sr = side_ring + ring_q(p) * RN + tid;
-          cp_async4(&sr->fnew_w, PT.fnew + (cr & ~3));
-          cp_async4(&sr->fold_w, PT.fold + (cr & ~3));
-          cp_async_c(&sr->phi, PT.phi + cr);
+          cp_async4(&sr->fnew_w, PT.fnew + size_t(cr & ~3u));
+          cp_async4(&sr->fold_w, PT.fold + size_t(cr & ~3u));
+          cp_async_c(&sr->phi, PT.phi + size_t(cr));
         }
       }
     }
@@ -755,8 +758,8 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
           if (fn == LBX_FLUID_SPHERELIST) return rec->phi;
           if (fn == LBX_FLUID_FLUID) {  // new fluid cell
             if (is_own) {
-              rR = PT.rhoR[cell];
-              rB = PT.rhoB[cell];
+              rR = PT.rhoR[size_t(unsigned(cell))];
+              rB = PT.rhoB[size_t(unsigned(cell))];
             }
             return rec->phi;
           }
