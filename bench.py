@@ -36,7 +36,7 @@ SIGMA, BETA = 0.02, 0.7
 LB_PER_STEP = 500
 # DRAM bytes (read + write) of one k_cg_lean launch at 128^3, from the ncu
 # captures summarised in profiles/ (None where no capture of that storage)
-TRAFFIC = {"f16": 291.2e6, "f32": 623.7e6}
+TRAFFIC = {"f16": 292.7e6, "f32": 622.6e6}
 BYTES_PER_CELL = {"f16": 160, "bf16": 160, "f32": 312, "f64": 616}  # algorithmic bytes per cell-step
 MINIMAL_BYTES = {"f16": 152, "bf16": 152, "f32": 304, "f64": 608}   # populations only (phi kept on chip)
 METRIC = "MLUPS & HBM GB/s, FP16-store vs FP32 LB at stated FP64 error, 1\u00d7B200"
