@@ -17,13 +17,15 @@
 //      shared-memory stage by cp.async (FP32 / FP64 pull synchronously in
 //      step 2 instead);
 //   2. sums the pulls of plane z+1 (landed one iteration ago) into densities
-//      and writes their phase field into a rolling four-slot window, then
-//      arrives at the plane's split barrier (an mbarrier);
-//   3. reads the pairs of plane z from the stage, takes the part of the
-//      colour gradient from planes z-1 and z, relaxes (BGK half), waits at the
-//      barrier, adds the plane z+1 part of the gradient, perturbs and
-//      recolours, and stores the 38 post-collision values of each cell with
-//      coalesced 4- or 8-byte writes.
+//      and writes their phase field into a rolling window (two planes with
+//      staged pulls, four otherwise), then arrives at the plane's split
+//      barrier (an mbarrier);
+//   3. reads the pairs of plane z from the stage and relaxes their component
+//      sums (BGK half), waits at the barrier, takes the colour gradient
+//      (staged: the in-plane sums of plane z+1 from the window, those of z-1
+//      and z kept in registers; otherwise the 26-point sum, its planes z-1
+//      and z before the wait), perturbs and recolours, and stores the 38
+//      post-collision values of each cell with coalesced 4- or 8-byte writes.
 // The phase field never goes through global memory; the extra cost is the
 // ring and the two boundary planes of each segment.  The particle variant
 // (PART) also copies each cell's flag words and side phase field with its
