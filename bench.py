@@ -171,16 +171,25 @@ def cpu_baseline_sample():
             "sample": f"{n} lattice steps of the 128^3 workload (about 10 s), FP32, OpenMP"}
 
 
-def error_vs_f64(nsteps_list=(100, 1000, 10000)):
-    """Relative L2 error of |u| and phi of each storage against the FP64-storage run."""
+def error_vs_f64(nsteps_list=(100, 1000, 10000), workload="spinodal"):
+    """Relative L2 error of |u| and phi of each storage against the FP64-storage run.
+
+    workload "spinodal": the bench's own field (chaotic: every storage decorrelates from FP64 with
+    time); "droplet": the reference's initType-1 droplet (radius L/8) in a uniform flow
+    u0 = (0.02, 0.01, 0.005), a smooth problem whose error grows with rounding only."""
     from lbcuda_b200 import LBSim, make_params
-    from lbcuda_b200.inputs import seeded_noise_fields
-    rR, rB = seeded_noise_fields(L, L, L, seed=SEED)
-    out = {}
+    from lbcuda_b200.inputs import initial_fields, seeded_noise_fields
+    vel = (0.0, 0.0, 0.0)
+    if workload == "droplet":
+        rR, rB = initial_fields(1, L, L, L)
+        vel = (0.02, 0.01, 0.005)
+    else:
+        rR, rB = seeded_noise_fields(L, L, L, seed=SEED)
+    out = {"workload": workload}
     sims = {}
     for st in ("f64", "f32", "f16", "bf16"):
         s = LBSim(make_params(L, model="cg", storage=st, sigma=SIGMA, beta=BETA))
-        s.set_fields(rR, rB)
+        s.set_fields(rR, rB, vel)
         sims[st] = s
     done = 0
     for n in nsteps_list:
@@ -389,6 +398,10 @@ def only_region(args, local):
     if args.only == "ensemble":
         print(json.dumps(ensemble_timing()), flush=True)
         return 0
+    if args.only == "errors":
+        print(json.dumps({"spinodal": error_vs_f64((100, 1000)),
+                          "droplet": error_vs_f64((100, 1000), workload="droplet")}), flush=True)
+        return 0
     if args.only == "variants":
         print(json.dumps({st: variants_timing(st) for st in ("f32", "f16")}), flush=True)
         return 0
@@ -420,7 +433,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-extras", action="store_true", help="skip the error runs, the colloid case and the CPU baseline")
     ap.add_argument("--only", choices=["f16", "f32", "bf16", "f64", "colloid-f16", "colloid-f32", "colloid-f16-small",
-                                       "colloid-f32-small", "ensemble", "closure", "variants"],
+                                       "colloid-f32-small", "ensemble", "closure", "variants", "errors"],
                     help="profiling aid: run one timed region only and print its timing")
     ap.add_argument("--lb-steps", type=int, default=LB_PER_STEP, help="lattice steps per bench step")
     ap.add_argument("--schedule", type=int, default=2, help="colour-gradient schedule (0, 1, 2)")
@@ -528,6 +541,7 @@ def main():
     extras = {}
     if rank == 0 and not args.no_extras:
         extras["error_vs_f64"] = error_vs_f64()
+        extras["error_vs_f64_droplet"] = error_vs_f64((100, 1000), workload="droplet")
         extras["colloid_256_1280"] = {st: colloid_timing(st) for st in ("f16", "f32")}
         extras["ensemble_48"] = ensemble_timing()
         extras["variants_128"] = {st: variants_timing(st) for st in ("f32", "f16")}
