@@ -155,3 +155,46 @@ def test_d3q27_mass(storage, bound):
     m1, _ = g.get_sums()
     assert (np.abs(m1 - m0) / m0 <= bound).all(), np.abs(m1 - m0) / m0
     g.close()
+
+
+@pytest.mark.gpu
+def test_d3q27_noncubic_unequal_tau_matches_oracle():
+    """A non-cubic box (48 x 20 x 16) with tauR != tauB and two densities."""
+    from lbcuda_b200 import LBSim
+    nx, ny, nz = 48, 20, 16
+    p = make_params(nx, ny, nz, model="cg-diffdens-d3q27", storage="f32", tauR=0.8, tauB=1.3, sigma=0.05,
+                    beta=0.9, densR=1.0, densB=0.5)
+    rR, rB = seeded_noise_fields(nx, ny, nz, seed=12)
+    rB = (0.5 * rB).astype(np.float32)
+    g = LBSim(p)
+    g.set_fields(rR, rB, (0.01, -0.02, 0.0))
+    g.step(25)
+    o = OracleSim(p, "ref")
+    o.set_fields(rR, rB, (0.01, -0.02, 0.0))
+    assert o.step(25) == 0
+    for name, a, b in zip(("rhoR", "rhoB", "vel", "phase"), g.get_fields(), o.get_fields()):
+        e = rel_l2(a, b) if name == "vel" else rel(a, b)
+        assert e <= (5e-5 if name == "vel" else 1e-5), (name, e)
+
+
+@pytest.mark.gpu
+def test_d3q27_set_pops_roundtrip_bf16_shift():
+    """27-plane population transfer both ways; BF16 storage keeps the D3Q27
+    corner class's shift (w_3 rho0) in the round trip of an equilibrium."""
+    from lbcuda_b200 import LBSim
+    n = 12
+    g = LBSim(make_params(n, model="cg-d3q27", storage="f32"))
+    rng = np.random.default_rng(3)
+    pR = rng.uniform(0.0, 0.1, (27, n, n, n)).astype(np.float32)
+    pB = rng.uniform(0.0, 0.1, (27, n, n, n)).astype(np.float32)
+    g.set_pops(pR, pB)
+    a, b = g.get_pops()
+    assert np.array_equal(a, pR) and np.array_equal(b, pB)
+    g.close()
+    g = LBSim(make_params(n, model="cg-d3q27", storage="bf16"))
+    r = np.full((n, n, n), 0.5, np.float32)
+    g.set_fields(r, r)
+    a, b = g.get_pops()
+    w = np.array([8 / 27] + [2 / 27] * 6 + [1 / 54] * 12 + [1 / 216] * 8)
+    assert np.abs(a[:, 0, 0, 0] - 0.5 * w).max() < 1e-7
+    g.close()
