@@ -342,27 +342,37 @@ def ensemble_timing(steps=100, err_steps=200, seed=7):
             "u_rel_l2_vs_f32_per_box": {"after_steps": err_steps, "max": max(errs), "median": float(np.median(errs))}}
 
 
-def closure_experiment(n=1024, ntrain=896, R_hi=6, L_hi=48, R_lo=3, steps_hi=240, seed=11, epochs=300):
-    """Learned closure workload: two-sphere data from the method itself (R_hi resolved, R_lo under-resolved,
-    gap/R log-uniform in [0.05, 1.5], pair-frame velocities and angular velocities uniform in +-1e-3, static
-    force subtracted), training on the GPU by the library's kernels, held-out evaluation.  Errors are force
-    errors of the corrected R_lo pair against the scaled R_hi pair, relative, over the held-out pairs."""
+def closure_experiment(R_hi=6, L_hi=48, R_lo=3, steps_hi=240, m=256, epochs=100, n_direct=64, seed=11):
+    """Learned closure workload.  Training data: the resistance of every lattice class of R_lo pairs with
+    gap/R in [0.05, 1.5] (121 classes at R_lo = 3; R_hi resolved in L_hi^3, R_lo in the box scaled by
+    R_lo / R_hi; a rest run and nine unit pair-frame velocity runs per class and resolution, static force
+    subtracted), m velocity vectors per class uniform in +-1e-3 (pair frame), training on the GPU by the
+    library's kernels.  Held out: n_direct pairs run directly (gap/R log-uniform, random orientation,
+    random velocities) and fresh velocities for every class.  Errors: relative L2 of the R_lo pair forces,
+    corrected or not, against the scaled R_hi forces."""
     from lbcuda_b200 import LBSim, closure, make_params
     t0 = time.perf_counter()
-    X, T, info = closure.generate(n, R_hi=R_hi, L_hi=L_hi, R_lo=R_lo, steps_hi=steps_hi, seed=seed)
-    t_gen = time.perf_counter() - t0
-    w, loss = closure.train(X[:ntrain], T[:ntrain], epochs=epochs, lr=2e-3)
-    Xt, Tt, base = X[ntrain:], T[ntrain:], info["base"][ntrain:]
-    pred = closure.infer(w, Xt)
-    lub = closure.analytic_lubrication(Xt, float(R_lo))
+    res = closure.resistance(R_hi=R_hi, L_hi=L_hi, R_lo=R_lo, steps_hi=steps_hi)
+    t_res = time.perf_counter() - t0
+    X, T, _ = closure.synthesize(res, m, seed=seed)
+    t0 = time.perf_counter()
+    w, loss = closure.train(X, T, epochs=epochs, lr=2e-3)
+    t_train = time.perf_counter() - t0
+    Xd, Td, info = closure.generate(n_direct, R_hi=R_hi, L_hi=L_hi, R_lo=R_lo, steps_hi=steps_hi, seed=seed + 1)
+    Xv, Tv, bv = closure.synthesize(res, 16, seed=seed + 2)
     fidx = [0, 1, 2, 6, 7, 8]  # the two forces, pair frame
-    hi = (base + Tt)[:, fidx]
 
-    def rel(corr):
+    def rel(Tt, base, corr):
+        hi = (base + Tt)[:, fidx]
         err = (Tt - corr)[:, fidx]
         per_pair = np.linalg.norm(err, axis=1) / np.maximum(np.linalg.norm(hi, axis=1), 1e-30)
         return {"rel_l2": float(np.linalg.norm(err) / np.linalg.norm(hi)), "median_pair": float(np.median(per_pair)),
                 "pairs_within_5pct": float(np.mean(per_pair <= 0.05))}
+
+    def errors(Xt, Tt, base):
+        return {"none": rel(Tt, base, np.zeros_like(Tt)),
+                "analytic_lubrication": rel(Tt, base, closure.analytic_lubrication(Xt, float(R_lo))),
+                "closure": rel(Tt, base, closure.infer(w, Xt))}
 
     # cost of a step at each resolution (same prescribed-motion pair runs)
     costs = {}
@@ -379,10 +389,11 @@ def closure_experiment(n=1024, ntrain=896, R_hi=6, L_hi=48, R_lo=3, steps_hi=240
         costs[R] = tot / 100
         sim.close()
     steps_lo = info["steps_lo"]
-    return {"samples": n, "train": ntrain, "held_out": n - ntrain, "R_hi": R_hi, "R_lo": R_lo, "L_hi": L_hi,
-            "steps_hi": steps_hi, "steps_lo": steps_lo, "generate_s": t_gen, "final_loss": float(loss[-1]),
-            "error_no_correction": rel(np.zeros_like(Tt)), "error_analytic_lubrication": rel(lub),
-            "error_closure": rel(pred),
+    return {"R_hi": R_hi, "R_lo": R_lo, "L_hi": L_hi, "steps_hi": steps_hi, "steps_lo": steps_lo,
+            "classes": int(len(res["gap"])), "train_samples": int(len(X)), "epochs": epochs,
+            "resistance_s": t_res, "train_s": t_train, "final_loss": float(loss[-1]),
+            "held_out_direct_pairs": n_direct, "error_direct": errors(Xd, Td, info["base"]),
+            "error_fresh_velocities": errors(Xv, Tv, bv),
             "ms_per_step": {"R_hi": costs[R_hi], "R_lo": costs[R_lo]},
             "cost_ratio_same_physical_time": costs[R_hi] * steps_hi / (costs[R_lo] * steps_lo)}
 
@@ -394,6 +405,9 @@ def only_region(args, local):
     from lbcuda_b200.inputs import seeded_noise_fields
     if args.only == "closure":
         print(json.dumps(closure_experiment()), flush=True)
+        return 0
+    if args.only == "closure12":
+        print(json.dumps(closure_experiment(R_hi=12, L_hi=96, steps_hi=960)), flush=True)
         return 0
     if args.only == "ensemble":
         print(json.dumps(ensemble_timing()), flush=True)
@@ -433,7 +447,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-extras", action="store_true", help="skip the error runs, the colloid case and the CPU baseline")
     ap.add_argument("--only", choices=["f16", "f32", "bf16", "f64", "colloid-f16", "colloid-f32", "colloid-f16-small",
-                                       "colloid-f32-small", "ensemble", "closure", "variants", "errors"],
+                                       "colloid-f32-small", "ensemble", "closure", "closure12", "variants", "errors"],
                     help="profiling aid: run one timed region only and print its timing")
     ap.add_argument("--lb-steps", type=int, default=LB_PER_STEP, help="lattice steps per bench step")
     ap.add_argument("--schedule", type=int, default=2, help="colour-gradient schedule (0, 1, 2)")

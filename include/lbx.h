@@ -208,19 +208,26 @@ const char* lbx_error_string(int code);
 int lbx_get_step(void* ctx, int64_t* step);
 
 /* ---- learned pair closure (no counterpart in the reference) ------------ */
-/* MLP 11 -> 64 -> 64 -> 64 -> 12 (SiLU, FP32) correcting the pair force and
+/* MLP 13 -> 64 -> 64 -> 64 -> 12 (SiLU, FP32) correcting the pair force and
  * torque of near-contact spheres; the reference's analytic lubrication
  * (addHertzian, kernels_fluid_PART.CUF:1463-1501) is the fallback outside
- * the training envelope.  The weights travel as one flat blob of
- * LBX_CLOSURE_NWEIGHTS floats: W0[64][11] b0 W1[64][64] b1 W2[64][64] b2
- * W3[12][64] b3, then the input mean[11], std[11] and output mean[12],
+ * the training envelope.  Inputs per pair i < j, in the lattice-fixed pair
+ * frame E (first axis n = (x_j - x_i)/|x_j - x_i|, transverse axes fixed by
+ * the cubic symmetry class of n, s = +-1 the sign of that class map):
+ * gap/R, E(v_j - v_i), s E omega_i, s E omega_j, R, nc_1, nc_2 (nc: |n|
+ * sorted descending).  Outputs: force and torque on i, then on j, in E
+ * (torques times s).  The weights travel as one flat blob of
+ * LBX_CLOSURE_NWEIGHTS floats: W0[64][13] b0 W1[64][64] b1 W2[64][64] b2
+ * W3[12][64] b3, then the input mean[13], std[13] and output mean[12],
  * std[12] used to standardise. */
-#define LBX_CLOSURE_NWEIGHTS 9914
+#define LBX_CLOSURE_NWEIGHTS 10046
 /* Glorot-uniform initial weights, identity standardisation. */
 int lbx_closure_init(float* weights, int32_t seed);
 /* Train on the GPU (one fused forward/backward/Adam kernel for all epochs):
- * X (n,11), T (n,12) raw features and targets, standardised with the
- * statistics in the blob; weights updated in place; loss[epochs] optional. */
+ * X (n,13), T (n,12) raw features and targets, standardised with the
+ * statistics in the blob; weights updated in place; loss[epochs] optional.
+ * Minibatches of 64, Adam with the step size decaying from lr to 0 as a half
+ * cosine over all epochs. */
 int lbx_closure_train(float* weights, const float* X, const float* T, int32_t n, int32_t epochs, float lr,
                       int32_t seed, float* loss);
 /* Gradient of the mean-squared error over the first min(n,128) standardised
@@ -231,7 +238,7 @@ int lbx_closure_infer(const float* weights, const float* X, int32_t n, float* Y)
 /* lbx_closure_infer without any device allocation (no counterpart in the
  * reference), for callers that must not allocate or free device memory:
  * inputs and outputs go through one fixed device array per device
- * (416,768 bytes).  n <= LBX_CLOSURE_NOALLOC_MAX, else LBX_ERR_ARG.  The
+ * (449,792 bytes).  n <= LBX_CLOSURE_NOALLOC_MAX, else LBX_ERR_ARG.  The
  * first call on a device (that device current) looks the array up; make it
  * before any stream capture.  Calls that overlap in time on one device share
  * the array and race: serialise them.  Same results as lbx_closure_infer. */

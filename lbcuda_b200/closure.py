@@ -3,21 +3,31 @@
 The closure corrects the force and torque of near-contact sphere pairs that
 the lattice resolves poorly (small radius).  Its training data come from the
 method itself: the same two-sphere configuration is run with prescribed
-sphere motion (``kinematic`` contexts, frozen geometry) once well resolved (radius R_hi in an
-L_hi^3 box) and once at the deployment radius R_lo (box, gap and time scaled
-by s = R_lo/R_hi, s^2 for time; translational velocities equal, angular
-velocities scaled by s so that the surface velocities agree).  For such
-dynamically similar Stokes flows forces scale as mu R U and torques as
-mu R^2 U, so the target is F_hi s - F_lo and T_hi s^2 - T_lo, in the pair
-frame.  Each force is the difference between the run with the sampled
-motion and the same configuration at rest: two spheres closer than a few
-cells hide some of each other's surface links, which leaves a static
-pressure imbalance of order w rho per hidden link that depends on how the
-pair sits on the lattice, not on the pair-frame inputs, and that no closure
-of those inputs can learn.  Training and
-inference run in the library's own kernels (lbx_closure_train /
-lbx_closure_infer); the analytic lubrication of the reference stays the
-fallback outside the training envelope and the judge of the gain.
+sphere motion (``kinematic`` contexts, frozen geometry) once well resolved
+(radius R_hi in an L_hi^3 box) and once at the deployment radius R_lo (box,
+gap and time scaled by s = R_lo/R_hi, s^2 for time; translational
+velocities equal, angular velocities scaled by s so that the surface
+velocities agree).  For such dynamically similar Stokes flows forces scale
+as mu R U and torques as mu R^2 U, so the target is F_hi s - F_lo and
+T_hi s^2 - T_lo.  Each force is the difference between the run with the
+sampled motion and the same configuration at rest: two spheres closer than
+a few cells hide some of each other's surface links, which leaves a static
+pressure imbalance that does not depend on the motion.
+
+Pairs are described in a pair frame fixed to the lattice (lattice_frame):
+the lattice and a sphere template centred on a site are invariant under the
+48 signed axis permutations, so every pair whose separation vector is one of
+a class under that group has the same forces in that frame.  At R_lo the
+rounded centres put every pair on one of finitely many classes (121 for
+gap/R in [0.05, 1.5] at R_lo = 3); the flow is linear in the sphere
+velocities at these Reynolds numbers, so per class a rest run and nine
+unit-velocity runs at each resolution give the whole correction as a 12 x 9
+matrix (resistance), from which training samples for any velocities follow
+(synthesize).  Held-out pairs are run directly (generate) in random
+orientations.  Training and inference run in the library's own kernels
+(lbx_closure_train / lbx_closure_infer); the analytic lubrication of the
+reference stays the fallback outside the training envelope and the judge of
+the gain.
 """
 import ctypes as C
 
@@ -26,9 +36,9 @@ import numpy as np
 from . import capi
 from .sim import LBSim, make_params
 
-DIN, H, DOUT = 11, 64, 12
-NW = 9914
-NPARAM = 9868
+DIN, H, DOUT = 13, 64, 12  # inputs: gap/R, pair-frame dv, w_i, w_j, R, nc_1, nc_2
+NW = 10046
+NPARAM = 9996
 XMU, XSD, YMU, YSD = NPARAM, NPARAM + DIN, NPARAM + 2 * DIN, NPARAM + 2 * DIN + DOUT
 
 
@@ -53,22 +63,66 @@ def nint(x):
     return np.sign(x) * np.floor(np.abs(x) + 0.5)
 
 
-def features(xi, xj, vi, vj, oi, oj, R, box):
-    """The 11 closure inputs of pair (i, j) (lab angular velocities).
+def lattice_frame(n):
+    """(E, sign, nc): the closure's pair frame, fixed to the lattice (lattice_frame, lbx_closure.h).
 
-    Gap and pair frame come from the rounded centres, where the spheres'
+    P, the signed axis permutation (stable order by descending |n|, ties to
+    the lower axis, sign + for n_k >= 0) that takes n to nc = P n in the
+    cubic fundamental domain; rows of E: n, P^T t1(nc), P^T t2(nc); sign =
+    det P.  Pair-frame components: E v for velocities and forces, sign * E w
+    for angular velocities and torques.
+    """
+    n = np.asarray(n, np.float64)
+    a = np.abs(n)
+    o = sorted(range(3), key=lambda k: (-a[k], k))
+    sg = np.where(n >= 0.0, 1.0, -1.0)
+    nc = a[o]
+    t1, t2 = pair_frame(nc)
+    E = np.zeros((3, 3))
+    E[0] = n
+    for r, k in enumerate(o):
+        E[1, k] = sg[k] * t1[r]
+        E[2, k] = sg[k] * t2[r]
+    inv = int(o[0] > o[1]) + int(o[0] > o[2]) + int(o[1] > o[2])
+    return E, (-1.0 if inv & 1 else 1.0) * sg[0] * sg[1] * sg[2], nc
+
+
+def to_pair(out, E, sign):
+    """(F_i, T_i, F_j, T_j) lab (4, 3) -> the 12 pair-frame components."""
+    out = np.asarray(out, np.float64)
+    return np.concatenate([E @ out[0], sign * (E @ out[1]), E @ out[2], sign * (E @ out[3])])
+
+
+def features(xi, xj, vi, vj, oi, oj, R, box):
+    """The 13 closure inputs of pair (i, j) (lab angular velocities) and (E, sign).
+
+    Gap and frame come from the rounded centres, where the spheres'
     templates actually sit: an under-resolved pair's forces follow its
     discrete geometry, which can differ from the nominal one by a cell.
     """
     d = nint(xj) - nint(xi)
     box = np.asarray(box, np.float64)
-    d = d - box * np.round(d / box)
+    d = d - box * nint(d / box)
     r = np.linalg.norm(d)
-    n = d / r
-    t1, t2 = pair_frame(n)
-    F = np.stack([n, t1, t2])
-    dv = F @ (np.asarray(vj) - np.asarray(vi))
-    return np.concatenate([[(r - 2 * R) / R], dv, F @ np.asarray(oi), F @ np.asarray(oj), [R]]), F
+    E, sign, nc = lattice_frame(d / r)
+    dv = E @ (np.asarray(vj, np.float64) - np.asarray(vi, np.float64))
+    x = np.concatenate([[(r - 2 * R) / R], dv, sign * (E @ np.asarray(oi, np.float64)),
+                        sign * (E @ np.asarray(oj, np.float64)), [R], nc[1:]])
+    return x, (E, sign)
+
+
+def lattice_classes(R, gap_range=(0.05, 1.5)):
+    """Separation vectors a >= b >= c >= 0 (one per lattice class) with gap/R in the range, by |d|."""
+    hi = (2.0 + gap_range[1]) * R
+    m = int(np.floor(hi)) + 1
+    out = []
+    for a in range(m + 1):
+        for b in range(a + 1):
+            for c in range(b + 1):
+                g = np.sqrt(a * a + b * b + c * c) / R - 2.0
+                if gap_range[0] <= g <= gap_range[1]:
+                    out.append((a, b, c))
+    return sorted(out, key=lambda t: (t[0] ** 2 + t[1] ** 2 + t[2] ** 2, t))
 
 
 def sample_configs(n, seed=0, gap_range=(0.05, 1.5), vmax=1e-3):
@@ -87,22 +141,20 @@ def run_pair(cfg, R, L, steps, average=0.25, storage="f32", lubrication=False, s
     """Forces / torques on both spheres of a prescribed-motion two-sphere run.
 
     Spheres of radius R on lattice sites, the second at mult * cfg['d'] (an
-    integer lattice vector) from the first, velocities -dv/2 and +dv/2 (pair
-    frame -> lab), angular velocities oi, oj (pair frame -> lab, body frame =
-    lab, identity orientation).  The geometry is frozen (kinematic = 2): the spheres keep
-    their place while their bounce-back walls move with the set velocities,
-    so the forces belong to this configuration and no cell is filled or
-    drained during the run.  Returns (F_i, T_i, F_j, T_j) in the lab frame,
-    averaged over the last `average` fraction of the steps, and the
-    configuration (x, v, omega).
+    integer lattice vector) from the first, velocities -dv/2 and +dv/2 and
+    angular velocities oi, oj, all given in the lattice pair frame of d
+    (body frame = lab, identity orientation).  The geometry is frozen
+    (kinematic = 2): the spheres keep their place while their bounce-back
+    walls move with the set velocities, so the forces belong to this
+    configuration and no cell is filled or drained during the run.  Returns
+    (F_i, T_i, F_j, T_j) in the lab frame, averaged over the last `average`
+    fraction of the steps, and the configuration (x, v, omega).
     """
     d = np.asarray(cfg["d"], np.float64) * mult
-    n = d / np.linalg.norm(d)
-    t1, t2 = pair_frame(n)
-    Fm = np.stack([n, t1, t2])
-    dv = Fm.T @ cfg["dv"]
-    oi = Fm.T @ cfg["oi"]
-    oj = Fm.T @ cfg["oj"]
+    E, sign, _ = lattice_frame(d / np.linalg.norm(d))
+    dv = E.T @ np.asarray(cfg["dv"], np.float64)
+    oi = sign * (E.T @ np.asarray(cfg["oi"], np.float64))
+    oj = sign * (E.T @ np.asarray(cfg["oj"], np.float64))
     c = np.full(3, float(L // 2))
     xj = (c + d - 1.0) % L + 1.0
     x = np.stack([c, xj])
@@ -132,13 +184,7 @@ def run_pair(cfg, R, L, steps, average=0.25, storage="f32", lubrication=False, s
     return acc / nav, x, v, om
 
 
-def generate(n_samples, R_hi=12, L_hi=128, R_lo=3, steps_hi=300, seed=0, progress=None, gap_range=(0.05, 1.5),
-             subtract_static=True):
-    """(X, T, info): features at R_lo and targets (resolved - under-resolved, pair frame).
-
-    The periodic box must keep each sphere's image farther away than its
-    partner: L >= (4 + 2 gap_max) R, checked at both resolutions.
-    """
+def _scales(R_hi, L_hi, R_lo, steps_hi, gap_range):
     s = R_lo / R_hi
     L_lo = int(round(L_hi * s))
     steps_lo = max(8, int(round(steps_hi * s * s)))
@@ -147,7 +193,26 @@ def generate(n_samples, R_hi=12, L_hi=128, R_lo=3, steps_hi=300, seed=0, progres
             raise ValueError(f"box {L} too small for radius {R} and gap/R up to {gap_range[1]}")
     if abs(R_hi / R_lo - round(R_hi / R_lo)) > 1e-12:
         raise ValueError("R_hi must be an integer multiple of R_lo")
-    mult = int(round(R_hi / R_lo))
+    if L_hi % 8 or L_lo % 8:
+        raise ValueError(f"boxes {L_hi} and {L_lo} must be multiples of 8 (the particle tile grid)")
+    return s, L_lo, steps_lo, int(round(R_hi / R_lo))
+
+
+# force and torque scaling from R_hi to R_lo (F_i, T_i, F_j, T_j in the 12 components)
+def _out_scale(s):
+    return np.repeat([s, s * s, s, s * s], 3)
+
+
+def generate(n_samples, R_hi=12, L_hi=128, R_lo=3, steps_hi=300, seed=0, progress=None, gap_range=(0.05, 1.5),
+             subtract_static=True):
+    """(X, T, info) from direct runs: random pairs, features at R_lo and targets (resolved - under-resolved).
+
+    Gap/R log-uniform in the range, separation direction uniform (so every
+    lattice orientation occurs), velocities uniform in +-1e-3 in the pair
+    frame.  The periodic box must keep each sphere's image farther away than
+    its partner: L >= (4 + 2 gap_max) R, checked at both resolutions.
+    """
+    s, L_lo, steps_lo, mult = _scales(R_hi, L_hi, R_lo, steps_hi, gap_range)
     # separations on the R_lo lattice (R_hi: the same vector times R_hi / R_lo),
     # nearest to the sampled gap and direction, kept inside the gap range
     cfgs = []
@@ -173,17 +238,72 @@ def generate(n_samples, R_hi=12, L_hi=128, R_lo=3, steps_hi=300, seed=0, progres
             rest = dict(cfg, dv=np.zeros(3), oi=np.zeros(3), oj=np.zeros(3))
             hi = hi - run_pair(rest, R_hi, L_hi, steps_hi, sim_cache=cache, mult=mult)[0]
             lo = lo - run_pair(rest, R_lo, L_lo, steps_lo, sim_cache=cache)[0]
-        feat, Fm = features(x[0], x[1], v[0], v[1], om[0], om[1], R_lo, (L_lo,) * 3)
-        scale = np.array([s, s * s, s, s * s])[:, None]
-        target = hi * scale - lo
+        feat, (E, sign) = features(x[0], x[1], v[0], v[1], om[0], om[1], R_lo, (L_lo,) * 3)
         X[k] = feat
-        T[k] = (target @ Fm.T).ravel()          # pair frame
-        base[k] = (lo @ Fm.T).ravel()
+        T[k] = to_pair(hi, E, sign) * _out_scale(s) - to_pair(lo, E, sign)
+        base[k] = to_pair(lo, E, sign)
         if progress and (k + 1) % progress == 0:
             print(f"closure data {k + 1}/{n_samples}", flush=True)
     for sim in cache.values():
         sim.close()
     return X, T, dict(base=base, cfgs=cfgs, steps_hi=steps_hi, steps_lo=steps_lo, L_lo=L_lo)
+
+
+def resistance(R_hi=12, L_hi=96, R_lo=3, steps_hi=960, gap_range=(0.05, 1.5), amp=1e-3, progress=None):
+    """Per lattice class: the pair-frame response of both resolutions to unit sphere velocities.
+
+    For each class (lattice_classes, separation in the fundamental domain,
+    so its frame needs no sign) a rest run and nine runs with one pair-frame
+    velocity component (dv, w_i, w_j) set to amp, at R_lo and at R_hi
+    (angular components times s there).  Returns dict with 'classes' (C, 3),
+    'gap' (C,), 'M_lo' and 'M_hi' (C, 12, 9): pair-frame force and torque per
+    unit R_lo-frame velocity, M_hi already scaled to R_lo units, so that a
+    pair with velocities q has target (M_hi - M_lo) q.
+    """
+    s, L_lo, steps_lo, mult = _scales(R_hi, L_hi, R_lo, steps_hi, gap_range)
+    classes = lattice_classes(R_lo, gap_range)
+    C = len(classes)
+    M_lo = np.zeros((C, DOUT, 9))
+    M_hi = np.zeros((C, DOUT, 9))
+    cache = {}
+    z = np.zeros(3)
+    for c, dcl in enumerate(classes):
+        d = np.asarray(dcl, np.float64)
+        E, sign, _ = lattice_frame(d / np.linalg.norm(d))
+        rest = dict(d=d, dv=z, oi=z, oj=z)
+        r_lo = to_pair(run_pair(rest, R_lo, L_lo, steps_lo, sim_cache=cache)[0], E, sign)
+        r_hi = to_pair(run_pair(rest, R_hi, L_hi, steps_hi, sim_cache=cache, mult=mult)[0], E, sign)
+        for k in range(9):
+            e = np.zeros(9)
+            e[k] = amp
+            lo = run_pair(dict(d=d, dv=e[:3], oi=e[3:6], oj=e[6:]), R_lo, L_lo, steps_lo, sim_cache=cache)[0]
+            hi = run_pair(dict(d=d, dv=e[:3], oi=e[3:6] * s, oj=e[6:] * s), R_hi, L_hi, steps_hi,
+                          sim_cache=cache, mult=mult)[0]
+            M_lo[c, :, k] = (to_pair(lo, E, sign) - r_lo) / amp
+            M_hi[c, :, k] = (to_pair(hi, E, sign) - r_hi) / amp * _out_scale(s)
+        if progress and (c + 1) % progress == 0:
+            print(f"closure classes {c + 1}/{C}", flush=True)
+    for sim in cache.values():
+        sim.close()
+    gap = np.array([np.linalg.norm(d) / R_lo - 2.0 for d in classes])
+    return dict(classes=np.array(classes, np.float64), gap=gap, M_lo=M_lo, M_hi=M_hi, R_lo=float(R_lo),
+                R_hi=float(R_hi), steps_hi=steps_hi, steps_lo=steps_lo, L_lo=L_lo)
+
+
+def synthesize(res, m, seed=0, vmax=1e-3):
+    """(X, T, base): m samples per class, pair-frame velocities uniform in +-vmax, targets from the matrices."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    C = len(res["gap"])
+    Q = rng.uniform(-vmax, vmax, (C, m, 9))
+    X = np.zeros((C, m, DIN))
+    X[:, :, 0] = res["gap"][:, None]
+    X[:, :, 1:10] = Q
+    X[:, :, 10] = res["R_lo"]
+    nc = res["classes"] / np.linalg.norm(res["classes"], axis=1, keepdims=True)
+    X[:, :, 11:13] = nc[:, None, 1:3]
+    T = np.einsum("cij,cmj->cmi", res["M_hi"] - res["M_lo"], Q)
+    base = np.einsum("cij,cmj->cmi", res["M_lo"], Q)
+    return X.reshape(C * m, DIN), T.reshape(C * m, DOUT), base.reshape(C * m, DOUT)
 
 
 def init_weights(X, T, seed=0):

@@ -3,13 +3,17 @@
 // analytic lubrication branch sits, addHertzian, kernels_fluid_PART.CUF:
 // 1463-1501, which stays the fallback and the judge).
 //
-// Network: 11 -> 64 -> 64 -> 64 -> 12, SiLU, FP32.  Inputs (pair frame of
-// spheres i < j, n = (x_j - x_i)/|x_j - x_i|, t1 = unit(n x e_k) with e_k the
-// axis least aligned with n, t2 = n x t1):
-//   gap/R, (v_j - v_i).{n,t1,t2}, omega_i.{n,t1,t2}, omega_j.{n,t1,t2}, R
-// (angular velocities in the lab frame).  Outputs: force and torque
-// corrections on i and on j in the same frame.  Inputs and outputs are
-// standardised with the mean / std stored after the weights.
+// Network: 13 -> 64 -> 64 -> 64 -> 12, SiLU, FP32.  Inputs, in the
+// lattice-fixed pair frame E of spheres i < j (lattice_frame in
+// lbx_closure.h: first axis n = (x_j - x_i)/|x_j - x_i|, transverse axes
+// fixed by the cubic symmetry class of n, sign s = det of that class map):
+//   gap/R, E (v_j - v_i), s E omega_i, s E omega_j, R, nc_1, nc_2
+// (angular velocities in the lab frame; nc the sorted |n| components, which
+// with the gap name the pair's lattice class).  Outputs: force and torque
+// corrections on i and on j in the same frame (torques carry s).  Inputs and
+// outputs are standardised with the mean / std stored after the weights.
+// Training decays the Adam step size from lr to 0 as a half cosine over the
+// optimiser steps of all epochs.
 //
 // Kernels
 //   k_mlp_train  one CTA runs every epoch of minibatch Adam on the whole data
@@ -192,13 +196,14 @@ __global__ void __launch_bounds__(TT) k_mlp_train(TrainArgs a) {
       // Adam
       ++t_adam;
       const float c1 = 1.0f - powf(a.beta1, float(t_adam)), c2 = 1.0f - powf(a.beta2, float(t_adam));
+      const float lr_t = 0.5f * a.lr * (1.0f + cospif(float(t_adam - 1) / float(a.epochs * nb)));
       for (int i = threadIdx.x; i < L::NPARAM; i += TT) {
         float gi = G[i];
         float mi = a.beta1 * a.m[i] + (1.0f - a.beta1) * gi;
         float vi = a.beta2 * a.v[i] + (1.0f - a.beta2) * gi * gi;
         a.m[i] = mi;
         a.v[i] = vi;
-        W[i] -= a.lr * (mi / c1) / (sqrtf(vi / c2) + a.eps);
+        W[i] -= lr_t * (mi / c1) / (sqrtf(vi / c2) + a.eps);
       }
       __syncthreads();
     }

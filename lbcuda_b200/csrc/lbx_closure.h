@@ -1,14 +1,14 @@
 // lbx_closure.h — the learned pair closure shared by its training/inference
 // kernels (lbx_closure.cu) and the particle step (lbx_particles.cu):
 // network dimensions, the weight-blob layout, the warp-level forward pass and
-// the pair frame.
+// the lattice-fixed pair frame.
 #pragma once
 #include <cuda_runtime.h>
 
 #include "../../include/lbx.h"
 
 namespace lbx {
-constexpr int DIN = 11, H = 64, DOUT = 12;
+constexpr int DIN = 13, H = 64, DOUT = 12;
 
 // parameter offsets in the flat weight blob
 struct MlpLayout {
@@ -92,6 +92,43 @@ __host__ __device__ inline void pair_frame(const double n[3], double t1[3], doub
   t2[0] = n[1] * t1[2] - n[2] * t1[1];
   t2[1] = n[2] * t1[0] - n[0] * t1[2];
   t2[2] = n[0] * t1[1] - n[1] * t1[0];
+}
+
+// The closure's pair frame, fixed to the lattice.  D3Q19 and a sphere
+// template centred on a lattice site are invariant under the 48 signed axis
+// permutations of the cubic group, so a pair and its image under any of them
+// have the same forces, mapped by the same operation (angular velocities and
+// torques as pseudovectors).  P is the one (stable order by descending |n|,
+// ties to the lower axis; sign + for n_k >= 0) that takes n into the
+// fundamental domain nc = P n, nc_0 >= nc_1 >= nc_2 >= 0; the frame is
+// pair_frame(nc) carried back by P^T: rows E[0] = n, E[1] = P^T t1(nc),
+// E[2] = P^T t2(nc).  Returns det P (+-1): the pair-frame components are
+// E dv for velocities and det P * E w for angular velocities, and forces
+// and torques come back as E^T y and det P * E^T y.  Every pair of one
+// lattice class (one separation vector up to the group) then has the same
+// gap, nc and frame, and the same forces for the same pair-frame inputs.
+__host__ __device__ inline double lattice_frame(const double n[3], double E[3][3], double nc[3]) {
+  const double a[3] = {fabs(n[0]), fabs(n[1]), fabs(n[2])};
+  int o[3] = {0, 1, 2};
+  auto sw = [](int& x, int& y) { int t = x; x = y; y = t; };
+  if (a[o[1]] > a[o[0]]) sw(o[0], o[1]);
+  if (a[o[2]] > a[o[1]]) {
+    sw(o[1], o[2]);
+    if (a[o[1]] > a[o[0]]) sw(o[0], o[1]);
+  }
+  double sg[3];
+  for (int k = 0; k < 3; ++k) sg[k] = n[k] >= 0.0 ? 1.0 : -1.0;
+  for (int r = 0; r < 3; ++r) nc[r] = a[o[r]];
+  double t1[3], t2[3];
+  pair_frame(nc, t1, t2);
+  for (int r = 0; r < 3; ++r) {
+    E[0][o[r]] = n[o[r]];
+    E[1][o[r]] = sg[o[r]] * t1[r];
+    E[2][o[r]] = sg[o[r]] * t2[r];
+  }
+  // det P = parity of the permutation o times the product of the signs
+  const int inv = (o[0] > o[1]) + (o[0] > o[2]) + (o[1] > o[2]);
+  return ((inv & 1) ? -1.0 : 1.0) * sg[0] * sg[1] * sg[2];
 }
 
 }  // namespace lbx

@@ -10,8 +10,8 @@
 //
 //   capacity:  LBX_CLOSURE_NOALLOC_MAX pairs (4096); larger n is rejected
 //              with LBX_ERR_ARG before any device work
-//   scratch:   weights (LBX_CLOSURE_NWEIGHTS floats, padded to 9984), then
-//              X (MAX x 11), then Y (MAX x 12): 416,768 bytes per device
+//   scratch:   weights (LBX_CLOSURE_NWEIGHTS floats, padded to 10048), then
+//              X (MAX x 13), then Y (MAX x 12): 449,792 bytes per device
 //   zeroing:   none needed; every call overwrites the weights and the n
 //              feature rows it uses, and the kernel writes every output row
 //              that is copied back
@@ -31,8 +31,8 @@ int closure_infer_launch(const float* dW, const float* dX, int n, float* dY);
 
 namespace {
 
-constexpr int kWPad = 9984;  // LBX_CLOSURE_NWEIGHTS rounded up to 256 bytes
-constexpr int kDin = 11, kDout = 12;
+constexpr int kWPad = 10048;  // LBX_CLOSURE_NWEIGHTS rounded up to 256 bytes
+constexpr int kDin = 13, kDout = 12;
 constexpr size_t kScratchFloats = size_t(kWPad) + size_t(LBX_CLOSURE_NOALLOC_MAX) * (kDin + kDout);
 static_assert(LBX_CLOSURE_NWEIGHTS <= kWPad, "weight blob exceeds its scratch slot");
 

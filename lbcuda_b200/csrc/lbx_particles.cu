@@ -1071,8 +1071,8 @@ __global__ void k_closure_pairs(PDev P, const double* __restrict__ pos, Geom g, 
     }
     const double r = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
     const double n[3] = {d[0] / r, d[1] / r, d[2] / r};
-    double t1[3], t2[3];
-    pair_frame(n, t1, t2);
+    double E[3][3], nc[3];
+    const double sgn = lattice_frame(n, E, nc);
     const double dv[3] = {pj[3] - pi[3], pj[4] - pi[4], pj[5] - pi[5]};
     double oi[3] = {0, 0, 0}, oj[3] = {0, 0, 0};
     {
@@ -1080,15 +1080,13 @@ __global__ void k_closure_pairs(PDev P, const double* __restrict__ pos, Geom g, 
       to_lab(pi, bi, oi);
       to_lab(pj, bj, oj);
     }
-    auto proj = [&](const double v[3], double o[3]) {
-      o[0] = v[0] * n[0] + v[1] * n[1] + v[2] * n[2];
-      o[1] = v[0] * t1[0] + v[1] * t1[1] + v[2] * t1[2];
-      o[2] = v[0] * t2[0] + v[1] * t2[1] + v[2] * t2[2];
+    auto proj = [&](const double v[3], double f, double o[3]) {
+      for (int a = 0; a < 3; ++a) o[a] = f * (v[0] * E[a][0] + v[1] * E[a][1] + v[2] * E[a][2]);
     };
     double fv[3], fi[3], fj[3];
-    proj(dv, fv);
-    proj(oi, fi);
-    proj(oj, fj);
+    proj(dv, 1.0, fv);
+    proj(oi, sgn, fi);
+    proj(oj, sgn, fj);
     const double gapR = (r - 2.0 * P.rdim) / P.rdim;
     bool inside = use_net && gapR >= P.cl_gmin && gapR <= P.cl_gmax;
     for (int c = 0; c < 3 && inside; ++c)
@@ -1096,13 +1094,17 @@ __global__ void k_closure_pairs(PDev P, const double* __restrict__ pos, Geom g, 
     float out[12];
     for (int c = 0; c < 12; ++c) out[c] = 0.f;
     if (inside) {
-      float x[DIN] = {float(gapR), float(fv[0]), float(fv[1]), float(fv[2]), float(fi[0]), float(fi[1]),
-                      float(fi[2]), float(fj[0]), float(fj[1]), float(fj[2]), float(P.rdim)};
+      float x[DIN] = {float(gapR),  float(fv[0]), float(fv[1]),   float(fv[2]), float(fi[0]),
+                      float(fi[1]), float(fi[2]), float(fj[0]),   float(fj[1]), float(fj[2]),
+                      float(P.rdim), float(nc[1]), float(nc[2])};
       float y[DOUT];
       mlp_warp(W, x, y, buf);
-      for (int q = 0; q < 4; ++q)
+      // forces back by E^T, torques (rows 3..5, 9..11) by det P * E^T
+      for (int q = 0; q < 4; ++q) {
+        const double f = (q & 1) ? sgn : 1.0;
         for (int c = 0; c < 3; ++c)
-          out[3 * q + c] = float(y[3 * q] * n[c] + y[3 * q + 1] * t1[c] + y[3 * q + 2] * t2[c]);
+          out[3 * q + c] = float(f * (y[3 * q] * E[0][c] + y[3 * q + 1] * E[1][c] + y[3 * q + 2] * E[2][c]));
+      }
     } else if (P.lub) {
       // the reference's lubrication on the centres themselves (addHertzian)
       double dc[3];

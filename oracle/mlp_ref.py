@@ -9,7 +9,7 @@ in tests/test_closure.py.
 """
 import numpy as np
 
-DIN, H, DOUT = 11, 64, 12
+DIN, H, DOUT = 13, 64, 12
 
 
 def layout():

@@ -11,10 +11,10 @@ import numpy as np
 import pytest
 
 from lbcuda_b200 import capi
+from lbcuda_b200.closure import DIN, DOUT, NPARAM, NW
 
 pytestmark = pytest.mark.gpu
 
-DIN, DOUT = 11, 12
 NMAX = 4096
 
 
@@ -23,10 +23,10 @@ def _fp(a):
 
 
 def _weights(seed):
-    w = np.zeros(9914, np.float32)                                # LBX_CLOSURE_NWEIGHTS
+    w = np.zeros(NW, np.float32)                                  # LBX_CLOSURE_NWEIGHTS
     assert capi.lib().lbx_closure_init(_fp(w), seed) == 0
     rng = np.random.default_rng(seed)
-    npar = 9868
+    npar = NPARAM
     w[npar:npar + DIN] = rng.normal(0, 0.5, DIN)                  # feature means
     w[npar + DIN:npar + 2 * DIN] = rng.uniform(0.5, 2.0, DIN)     # feature scales
     w[npar + 2 * DIN:npar + 2 * DIN + DOUT] = rng.normal(0, 0.1, DOUT)
