@@ -264,9 +264,10 @@ int lbx_ensemble_destroy(void* ens);
 int lbx_ensemble_box(void* ens, int32_t i, void** ctx);
 int lbx_ensemble_step(void* ens, int32_t nsteps);
 int lbx_ensemble_time(void* ens, int32_t nsteps, double* ms);
-/* Autotuner: times every (CTA shape, z-segment length) candidate for
- * `trial` steps on the boxes themselves (this advances them) and keeps the
- * fastest; chosen = {shape, zlen}, best_ms = per-step time. */
+/* Autotuner: times the fused fluid kernel of every (CTA shape, z-segment
+ * length) candidate over `trial` steps on the boxes themselves (this
+ * advances them) and keeps the fastest; chosen = {shape, zlen}, best_ms =
+ * that kernel's time per step. */
 int lbx_ensemble_tune(void* ens, int32_t trial, int32_t* chosen, double* best_ms);
 
 /* ---- measurement ------------------------------------------------------- */

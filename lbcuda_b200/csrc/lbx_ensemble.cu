@@ -12,8 +12,8 @@
 // instead of one after the other.  Two consecutive steps (the ping-pong
 // parity) are captured once into a CUDA graph (the forks become parallel
 // branches) and replayed, so the host issues one graph launch per two steps.  lbx_ensemble_tune times the
-// candidate CTA shapes and z-segment lengths on the boxes themselves and
-// keeps the fastest.
+// fused fluid kernel of each candidate CTA shape and z-segment length on the
+// boxes themselves and keeps the fastest.
 #include <algorithm>
 #include <new>
 #include <vector>
@@ -92,7 +92,9 @@ int boxes_side_by_side(Ensemble& e, F&& part) {
 
 // one step of every box (eager, or recorded while the ensemble stream is
 // being captured)
-int step_once(Ensemble& e) {
+// ta / tb (optional): events recorded on the ensemble stream around the
+// fused fluid launch, the only part of a step the tuner's choice changes
+int step_once(Ensemble& e, cudaEvent_t ta = nullptr, cudaEvent_t tb = nullptr) {
   if (!e.tables_ok) {
     int rc = build_tables(e);
     if (rc) return rc;
@@ -102,8 +104,10 @@ int step_once(Ensemble& e) {
     if (c->cur != parity) return LBX_ERR_STATE;  // boxes must be stepped together
   int rc = boxes_side_by_side(e, [](lbx::Ctx& c) { return lbx::particles_pre(c); });
   if (rc) return rc;
+  if (ta) cudaEventRecord(ta, e.stream);
   rc = lbx::ensemble_launch(e.boxes, e.shape, e.zlen, e.d_desc[parity], e.d_work[parity], e.nwork, e.stream, 0,
                             parity);
+  if (tb) cudaEventRecord(tb, e.stream);
   if (rc) return rc;
   rc = boxes_side_by_side(e, [](lbx::Ctx& c) { return lbx::particles_post(c); });
   if (rc) return rc;
@@ -278,15 +282,21 @@ int lbx_ensemble_tune(void* ens, int32_t trial, int32_t* chosen, double* best_ms
       if (rc) return rc;
       for (int w = 0; w < 2; ++w)
         if ((rc = step_once(*e))) return rc;
+      // fused-kernel time only: the sphere kernels around it do not depend
+      // on the candidate, and their eager launch overhead would swamp the
+      // differences between candidates
       cudaEvent_t a, b;
       cudaEventCreate(&a);
       cudaEventCreate(&b);
-      cudaEventRecord(a, e->stream);
-      for (int s = 0; s < trial && !rc; ++s) rc = step_once(*e);
-      cudaEventRecord(b, e->stream);
-      cudaEventSynchronize(b);
       float t = 0.f;
-      cudaEventElapsedTime(&t, a, b);
+      for (int s = 0; s < trial && !rc; ++s) {
+        rc = step_once(*e, a, b);
+        if (rc) break;
+        if (cudaEventSynchronize(b) != cudaSuccess) rc = LBX_ERR_CUDA;
+        float ts = 0.f;
+        if (!rc && cudaEventElapsedTime(&ts, a, b) != cudaSuccess) rc = LBX_ERR_CUDA;
+        t += ts;
+      }
       cudaEventDestroy(a);
       cudaEventDestroy(b);
       if (rc) return rc;

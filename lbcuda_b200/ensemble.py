@@ -52,7 +52,7 @@ class Ensemble:
         ch = (C.c_int32 * 2)()
         best = C.c_double()
         check(self._L.lbx_ensemble_tune(self._h, int(trial), ch, C.byref(best)), "lbx_ensemble_tune")
-        return {"shape": "32x16" if ch[0] == 1 else "32x8", "zlen": int(ch[1]), "ms_per_step": best.value}
+        return {"shape": "32x16" if ch[0] == 1 else "32x8", "zlen": int(ch[1]), "fused_kernel_ms": best.value}
 
     def close(self):
         if getattr(self, "_h", None) and self._h.value:
