@@ -36,9 +36,9 @@ SIGMA, BETA = 0.02, 0.7
 LB_PER_STEP = 500
 # DRAM bytes (read + write) of one k_cg_lean launch at 128^3, from the ncu
 # captures summarised in profiles/ (None where no capture of that storage)
-TRAFFIC = {"f16": 292.7e6, "f32": 622.6e6}
-BYTES_PER_CELL = {"f16": 160, "bf16": 160, "f32": 312, "f64": 616}  # algorithmic bytes per cell-step
-MINIMAL_BYTES = {"f16": 152, "bf16": 152, "f32": 304, "f64": 608}   # populations only (phi kept on chip)
+TRAFFIC = {"f16": 292.7e6, "f16sd": 292.0e6, "f32": 622.6e6}
+BYTES_PER_CELL = {"f16": 160, "bf16": 160, "f16sd": 160, "f32": 312, "f64": 616}  # algorithmic bytes per cell-step
+MINIMAL_BYTES = {"f16": 152, "bf16": 152, "f16sd": 152, "f32": 304, "f64": 608}   # populations only (phi on chip)
 METRIC = "MLUPS & HBM GB/s, FP16-store vs FP32 LB at stated FP64 error, 1\u00d7B200"
 
 
@@ -187,7 +187,7 @@ def error_vs_f64(nsteps_list=(100, 1000, 10000), workload="spinodal"):
         rR, rB = seeded_noise_fields(L, L, L, seed=SEED)
     out = {"workload": workload}
     sims = {}
-    for st in ("f64", "f32", "f16", "bf16"):
+    for st in ("f64", "f32", "f16", "bf16", "f16sd", "bf16sd"):
         s = LBSim(make_params(L, model="cg", storage=st, sigma=SIGMA, beta=BETA))
         s.set_fields(rR, rB, vel)
         sims[st] = s
@@ -200,7 +200,7 @@ def error_vs_f64(nsteps_list=(100, 1000, 10000), workload="spinodal"):
         done = n
         u64, p64 = res["f64"][2], res["f64"][3]
         m64 = res["f64"][0].sum() + res["f64"][1].sum()
-        for st in ("f32", "f16", "bf16"):
+        for st in ("f32", "f16", "bf16", "f16sd", "bf16sd"):
             eu = float(np.linalg.norm(res[st][2] - u64) / np.linalg.norm(u64))
             ep = float(np.linalg.norm(res[st][3] - p64) / np.linalg.norm(p64))
             out.setdefault(st, {})[f"after_{n}"] = {"u_rel_l2": eu, "phi_rel_l2": ep}
@@ -446,7 +446,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-extras", action="store_true", help="skip the error runs, the colloid case and the CPU baseline")
-    ap.add_argument("--only", choices=["f16", "f32", "bf16", "f64", "colloid-f16", "colloid-f32", "colloid-f16-small",
+    ap.add_argument("--only", choices=["f16", "f32", "bf16", "f64", "f16sd", "bf16sd", "colloid-f16", "colloid-f32", "colloid-f16-small",
                                        "colloid-f32-small", "ensemble", "closure", "closure12", "variants", "errors"],
                     help="profiling aid: run one timed region only and print its timing")
     ap.add_argument("--lb-steps", type=int, default=LB_PER_STEP, help="lattice steps per bench step")
@@ -494,18 +494,21 @@ def main():
         s.close()
         return total_ms, kernel_ms, launches, clocks, code
 
-    # headline: FP16 shifted storage
-    tot16, k16, n16, clocks, code16 = run_storage("f16", args.steps, args.warmup)
+    # headline: FP16 storage as sum / difference pairs (R + B - w (rho0R + rho0B), R - B); beside it the
+    # FP16 (R, B) pairs the sphere path stores, and FP32
+    tot16, k16, n16, clocks, code16 = run_storage("f16sd", args.steps, args.warmup)
     tot32, k32, n32, _, code32 = run_storage("f32", args.steps, args.warmup)
+    totrb, krb, nrb, _, coderb = run_storage("f16", args.steps, args.warmup)
 
     def maxr(v):
         return max_over_ranks(v, pg, "cuda")
 
-    tot16, tot32 = maxr(tot16), maxr(tot32)
+    tot16, tot32, totrb = maxr(tot16), maxr(tot32), maxr(totrb)
     cells = L ** 3
     lb_steps = args.steps * LB_PER_STEP
     mlups16 = ws * cells * lb_steps / (tot16 * 1e-3) / 1e6
     mlups32 = ws * cells * lb_steps / (tot32 * 1e-3) / 1e6
+    mlupsrb = ws * cells * lb_steps / (totrb * 1e-3) / 1e6
 
     def roofline(storage, kernel_ms, launches):
         per_launch_ms = kernel_ms / max(launches, 1)
@@ -524,7 +527,7 @@ def main():
     hR, hB = pin((L, L, L)), pin((L, L, L))
     hR[...] = rR
     hB[...] = rB
-    s = LBSim(make_params(L, model="cg", storage="f16", sigma=SIGMA, beta=BETA))
+    s = LBSim(make_params(L, model="cg", storage="f16sd", sigma=SIGMA, beta=BETA))
     import ctypes
     fp = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
     oR, oB, oV, oP = pin((L, L, L)), pin((L, L, L)), pin((L, L, L, 3)), pin((L, L, L))
@@ -569,20 +572,24 @@ def main():
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": "colour-gradient spinodal 128^3 periodic, rho=0.5+U(-0.01,0.01) seed 1, "
                                    "tau=1, sigma=0.02, beta=0.7",
-                       "lattice_steps_per_bench_step": LB_PER_STEP, "storage": "f16 shifted (f - w*0.5)",
+                       "lattice_steps_per_bench_step": LB_PER_STEP,
+                       "storage": "f16 sum / difference pairs (f_R + f_B - w*1, f_R - f_B), FP32 arithmetic",
                        "cells": cells, "l2": "inputs larger than L2 (2 x 160 MB population buffers)",
                        "parallelism": "replicas" if ws > 1 else "single"},
-            "roofline": roofline("f16", k16, n16),
+            "roofline": roofline("f16sd", k16, n16),
             "fp32_storage": {"value": mlups32, "unit": "MLUPS", "ms_per_step": tot32 / args.steps,
                              "roofline": roofline("f32", k32, n32)},
             "fp16_over_fp32": mlups16 / mlups32,
+            "f16_component_pairs": {"value": mlupsrb, "unit": "MLUPS", "ms_per_step": totrb / args.steps,
+                                    "storage": "f16 (R - w rho0R, B - w rho0B) pairs, the sphere path's storage",
+                                    "roofline": roofline("f16", krb, nrb), "over_fp32": mlupsrb / mlups32},
             "clocks": clocks,
             "e2e": {"value": e2e_mlups, "unit": "MLUPS", "h2d_bytes_per_step": 2 * 4 * cells,
                     "d2h_bytes_per_step": 6 * 4 * cells, "ms_per_step": e2e_ms / args.steps,
                     "timing": "host wall clock around the synchronous C-ABI calls, max over ranks",
                     "gpu_launches_per_step": LB_PER_STEP + 2},
             "gpu_launches": n16,
-            "device_errors": [code16, code32],
+            "device_errors": [code16, code32, coderb],
         }
         line.update(extras)
         print(json.dumps(line), flush=True)

@@ -50,6 +50,19 @@ extern "C" {
 #define LBX_STORE_F16 1  /* FP16 populations shifted by w_l * rho0           */
 #define LBX_STORE_BF16 2 /* BF16 populations shifted by w_l * rho0           */
 #define LBX_STORE_F64 3  /* FP64 populations and FP64 arithmetic (error runs) */
+/* 16-bit sum / difference pairs (no counterpart in the reference): per
+ * direction and cell the pair (f_R + f_B - w_l (rho0R + rho0B),
+ * f_R - f_B - w_l (rho0R - rho0B)) instead of (f_R - w_l rho0R,
+ * f_B - w_l rho0B).  The total population carries the momentum and sits near
+ * w_l rho, so its shifted value is small and keeps more bits; rounding then
+ * moves the velocity far less.  FP32 arithmetic as for LBX_STORE_F16.
+ * Colour-gradient model (LBX_MODEL_CG) on the single-pass schedule without
+ * spheres; lbx_create rejects it with particles or another model, and
+ * lbx_set_schedule / the ensemble reject it on the other schedules.
+ * lbx_set_pops / lbx_get_pops and the field calls convert, so callers still
+ * see f_R and f_B. */
+#define LBX_STORE_F16_SD 4
+#define LBX_STORE_BF16_SD 5
 
 #define LBX_WET_JANUS 0   /* compute_virtual_rho, kernels_fluid_PART.CUF:299-352 */
 #define LBX_WET_NEUTRAL 1 /* compute_densities_wall, kernels_fluid_PART.CUF:267-297 */

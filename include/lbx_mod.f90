@@ -25,6 +25,7 @@ module lbx_mod
   integer(c_int32_t), parameter :: LBX_MODEL_BGK = 0, LBX_MODEL_CG = 1, LBX_MODEL_CG_DIFFDENS = 2
   integer(c_int32_t), parameter :: LBX_MODEL_CG_D3Q27 = 3, LBX_MODEL_CG_DIFFDENS_D3Q27 = 4
   integer(c_int32_t), parameter :: LBX_STORE_F32 = 0, LBX_STORE_F16 = 1, LBX_STORE_BF16 = 2, LBX_STORE_F64 = 3
+  integer(c_int32_t), parameter :: LBX_STORE_F16_SD = 4, LBX_STORE_BF16_SD = 5
   integer(c_int32_t), parameter :: LBX_WET_JANUS = 0, LBX_WET_NEUTRAL = 1
 
   type, bind(C) :: lbx_params

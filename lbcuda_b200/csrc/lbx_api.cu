@@ -149,7 +149,10 @@ int lbx_create(const lbx_params* p, void** out) {
   if (two_dens &&
       (!(p->densR > 0.0f) || !(p->densB > 0.0f) || (p->densR != 1.0f && p->densB != 1.0f)))
     return LBX_ERR_ARG;
-  if (p->storage < LBX_STORE_F32 || p->storage > LBX_STORE_F64) return LBX_ERR_ARG;
+  if (p->storage < LBX_STORE_F32 || p->storage > LBX_STORE_BF16_SD) return LBX_ERR_ARG;
+  const bool sd = p->storage == LBX_STORE_F16_SD || p->storage == LBX_STORE_BF16_SD;
+  // sum / difference pairs: the single-pass colour-gradient kernel without spheres only
+  if (sd && (p->model != LBX_MODEL_CG || p->max_particles > 0)) return LBX_ERR_ARG;
   int64_t n = int64_t(p->nx) * p->ny * p->nz;
   if (n >= (int64_t(1) << 31)) return LBX_ERR_ARG;  // 32-bit cell indices
   Ctx* c = new (std::nothrow) Ctx();
@@ -164,6 +167,8 @@ int lbx_create(const lbx_params* p, void** out) {
   // the DIFFDENS collision and the D3Q27 lattice run on the two-pass schedule only
   if (two_dens || d3q27) c->fused = 0;
   c->storage = p->storage;
+  c->sd = sd;
+  if (sd) c->fused = 2;
   c->elem = (p->storage == LBX_STORE_F32) ? 4 : (p->storage == LBX_STORE_F64 ? 8 : 2);
   int rc = cuda_rc(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
   if (!rc) rc = cuda_rc(cudaMalloc(&c->d_err, sizeof(unsigned long long)));
@@ -425,6 +430,7 @@ int lbx_set_schedule(void* ctx, int32_t fused) {
   if (!c) return LBX_ERR_ARG;
   if (fused < 0 || fused > 2) return LBX_ERR_ARG;
   if (c->p.model >= LBX_MODEL_CG_DIFFDENS && fused != 0) return LBX_ERR_ARG;
+  if (c->sd && fused != 2) return LBX_ERR_ARG;  // sum / difference pairs: lean kernel only
   c->fused = fused;
   return 0;
 }

@@ -144,6 +144,7 @@ template <> struct Store<__nv_bfloat16> {
 template <typename C>
 struct Shift {
   C s[2][4];  // [component][weight class]
+  int sd = 0;  // sum / difference pairs: component 0 holds R + B, 1 holds R - B (s: their shifts)
   __device__ __forceinline__ C at(int c, int l) const { return s[c][wclass27(l)]; }
 };
 

@@ -30,6 +30,7 @@ struct Ctx {
   int ncomp = 1;            // 1 (BGK) or 2 (CG)
   int q = 19;               // populations per component: 19, or 27 for the D3Q27 models
   int storage = LBX_STORE_F32;
+  bool sd = false;  // LBX_STORE_F16_SD / LBX_STORE_BF16_SD: sum / difference pairs
   size_t elem = 4;          // bytes per stored population
   void* pops[2] = {nullptr, nullptr};
   int cur = 0;              // buffer holding the current state

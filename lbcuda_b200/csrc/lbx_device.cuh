@@ -94,6 +94,28 @@ __device__ __forceinline__ void pull_any(const S* __restrict__ A, const S* Bold,
   else pull<QQ>(A, g, b, comp, sh, f);
 }
 
+// Sum / difference pairs (Shift::sd): what the per-component pulls gave
+// (R + B and R - B, shifts removed) into the components, and back before
+// the per-component stores.
+template <int QQ = Q, typename C>
+__device__ __forceinline__ void sd_to_rb(C* f0, C* f1) {
+#pragma unroll
+  for (int l = 0; l < QQ; ++l) {
+    const C s = f0[l], d = f1[l];
+    f0[l] = C(0.5) * (s + d);
+    f1[l] = C(0.5) * (s - d);
+  }
+}
+template <int QQ = Q, typename C>
+__device__ __forceinline__ void rb_to_sd(C* f0, C* f1) {
+#pragma unroll
+  for (int l = 0; l < QQ; ++l) {
+    const C r = f0[l], b = f1[l];
+    f0[l] = r + b;
+    f1[l] = r - b;
+  }
+}
+
 template <int QQ = Q, typename C>
 __device__ __forceinline__ C sum_q(const C* f) {
   C r = f[0];
@@ -349,8 +371,14 @@ template <typename C>
 inline Shift<C> make_shift(const Ctx& c) {
   Shift<C> s;
   LatticeT<C> L = make_lattice<C>(c.q);
-  bool shifted = (c.storage == LBX_STORE_F16 || c.storage == LBX_STORE_BF16);
+  bool shifted = c.storage != LBX_STORE_F32 && c.storage != LBX_STORE_F64;
   float r0[2] = {c.p.rho0R, c.p.rho0B};
+  s.sd = c.sd ? 1 : 0;
+  // sum / difference pairs: the shifts of R + B and of R - B
+  if (c.sd) {
+    r0[0] = c.p.rho0R + c.p.rho0B;
+    r0[1] = c.p.rho0R - c.p.rho0B;
+  }
   for (int comp = 0; comp < 2; ++comp)
     for (int k = 0; k < 4; ++k) s.s[comp][k] = shifted ? C(L.w[k] * C(r0[comp])) : C(0);
   return s;
@@ -402,8 +430,10 @@ template <typename F>
 inline int by_storage(const Ctx& c, F&& fn) {
   switch (c.storage) {
     case LBX_STORE_F32: return fn((float*)nullptr);
-    case LBX_STORE_F16: return fn((__half*)nullptr);
-    case LBX_STORE_BF16: return fn((__nv_bfloat16*)nullptr);
+    case LBX_STORE_F16:
+    case LBX_STORE_F16_SD: return fn((__half*)nullptr);
+    case LBX_STORE_BF16:
+    case LBX_STORE_BF16_SD: return fn((__nv_bfloat16*)nullptr);
     case LBX_STORE_F64: return fn((double*)nullptr);
   }
   return LBX_ERR_ARG;

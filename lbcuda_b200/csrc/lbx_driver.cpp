@@ -3,7 +3,7 @@
 //
 //   lbx_run [options] [input.dat]
 //     -L n | --nx n --ny n --nz n   lattice (the reference's MYDIMESION)
-//     --storage f32|f16|bf16|f64    population storage
+//     --storage f32|f16|bf16|f64|f16sd|bf16sd    population storage
 //     --bgk                         single-component BGK instead of CG
 //     --sigma s --beta b --tauR t --tauB t --tau t
 //     --radius r --rmass m --neutral (wetting) --xyz file
@@ -306,7 +306,8 @@ int main(int argc, char** argv) {
     else if (s == "--nz") nz = std::atoi(nxt());
     else if (s == "--storage") {
       std::string t = nxt();
-      p.storage = t == "f16" ? LBX_STORE_F16 : t == "bf16" ? LBX_STORE_BF16 : t == "f64" ? LBX_STORE_F64 : LBX_STORE_F32;
+      p.storage = t == "f16" ? LBX_STORE_F16 : t == "bf16" ? LBX_STORE_BF16 : t == "f64" ? LBX_STORE_F64
+                : t == "f16sd" ? LBX_STORE_F16_SD : t == "bf16sd" ? LBX_STORE_BF16_SD : LBX_STORE_F32;
     } else if (s == "--bgk") p.model = LBX_MODEL_BGK;
     else if (s == "--diffdens") {  // two fluid densities: --diffdens densR densB
       p.model = (p.model == LBX_MODEL_CG_D3Q27) ? LBX_MODEL_CG_DIFFDENS_D3Q27 : LBX_MODEL_CG_DIFFDENS;

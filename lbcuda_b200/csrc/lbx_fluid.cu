@@ -49,6 +49,22 @@ __global__ void k_set_fields(S* __restrict__ A, S* __restrict__ B, Geom g, int n
   int cell = at(b, 0, 0, 0);
   C u = C(vx), v = C(vy), w = C(vz);
   C usq = L.half_inv_cssq * (u * u + v * v + w * w);
+  if (sh.sd) {  // sum / difference pairs (single density, D3Q19)
+    C f0[Q], f1[Q];
+#pragma unroll
+    for (int l = 0; l < Q; ++l) {
+      f0[l] = equil_u(L, C(rR[at(b, ex(l), ey(l), ez(l))]), edot(l, u, v, w), usq, l);
+      f1[l] = equil_u(L, C(rB[at(b, ex(l), ey(l), ez(l))]), edot(l, u, v, w), usq, l);
+    }
+    rb_to_sd(f0, f1);
+    store_all(A, g, cell, 0, sh, f0);
+    store_all(A, g, cell, 1, sh, f1);
+#pragma unroll
+    for (int l = 0; l < Q; ++l) f0[l] = f1[l] = C(0);
+    store_all(B, g, cell, 0, sh, f0);
+    store_all(B, g, cell, 1, sh, f1);
+    return;
+  }
   for (int comp = 0; comp < ncomp; ++comp) {
     const float* r = comp ? rB : rR;
 #pragma unroll
@@ -71,6 +87,18 @@ __global__ void k_set_pops(S* __restrict__ A, Geom g, int ncomp, const float* __
   Nbr b;
   make_nbr(g, x, y, z, b);
   int cell = at(b, 0, 0, 0);
+  if (sh.sd) {  // sum / difference pairs (D3Q19)
+    C f0[Q], f1[Q];
+#pragma unroll
+    for (int l = 0; l < Q; ++l) {
+      f0[l] = C(pR[size_t(l) * size_t(g.n) + at(b, ex(l), ey(l), ez(l))]);
+      f1[l] = C(pB[size_t(l) * size_t(g.n) + at(b, ex(l), ey(l), ez(l))]);
+    }
+    rb_to_sd(f0, f1);
+    store_all(A, g, cell, 0, sh, f0);
+    store_all(A, g, cell, 1, sh, f1);
+    return;
+  }
   for (int comp = 0; comp < ncomp; ++comp) {
     const float* p = comp ? pB : pR;
 #pragma unroll
@@ -305,6 +333,7 @@ __global__ void k_fields(const S* __restrict__ A, const S* Bold, Geom g, int nco
 #pragma unroll
     for (int l = 0; l < QQ; ++l) fB[l] = C(0);
   }
+  if (sh.sd) sd_to_rb<QQ>(fR, fB);
   C lr = sum_q<QQ>(fR), lb = sum_q<QQ>(fB);
   C rs = lr + lb;
   C inv = C(1) / rs;
@@ -330,6 +359,18 @@ __global__ void k_get_pops(const S* __restrict__ A, const S* Bold, Geom g, int n
   make_nbr(g, x, y, z, b);
   int cell = at(b, 0, 0, 0);
   C f[QQ];
+  if (sh.sd) {  // both halves of each pair are needed for either component
+    C f1[QQ];
+    pull_any<QQ>(A, Bold, g, b, 0, sh, fold, f);
+    pull_any<QQ>(A, Bold, g, b, 1, sh, fold, f1);
+    sd_to_rb<QQ>(f, f1);
+#pragma unroll
+    for (int l = 0; l < QQ; ++l) {
+      if (pR) pR[size_t(l) * size_t(g.n) + cell] = float(f[l]);
+      if (pB) pB[size_t(l) * size_t(g.n) + cell] = float(f1[l]);
+    }
+    return;
+  }
   for (int comp = 0; comp < ncomp; ++comp) {
     float* out = comp ? pB : pR;
     if (!out) continue;
@@ -352,9 +393,21 @@ __global__ void k_sums(const S* __restrict__ A, const S* Bold, Geom g, int ncomp
     make_nbr(g, x, y, z, b);
     int cell = at(b, 0, 0, 0);
     if (!flags || flags[cell] == LBX_FLUID_FLUID) {
-      C f[QQ];
+      C f[QQ], f1[QQ];
+      if (sh.sd) {
+        pull_any<QQ>(A, Bold, g, b, 0, sh, fold, f);
+        pull_any<QQ>(A, Bold, g, b, 1, sh, fold, f1);
+        sd_to_rb<QQ>(f, f1);
+      }
       for (int comp = 0; comp < ncomp; ++comp) {
-        pull_any<QQ>(A, Bold, g, b, comp, sh, fold, f);
+        if (sh.sd) {
+          if (comp == 1) {
+#pragma unroll
+            for (int l = 0; l < QQ; ++l) f[l] = f1[l];
+          }
+        } else {
+          pull_any<QQ>(A, Bold, g, b, comp, sh, fold, f);
+        }
         double m = 0;
 #pragma unroll
         for (int l = 0; l < QQ; ++l) m += double(f[l]);

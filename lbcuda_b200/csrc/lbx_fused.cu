@@ -47,6 +47,10 @@ struct LeanConst {
   C sigma, beta;
   C rho0[2];         // shift densities of the stored populations (0 when unshifted)
   C s[2][3];         // shift of each weight class, w_cls * rho0
+  // sum / difference pairs (LBX_STORE_F16_SD, _BF16_SD): the stored pair is
+  // (R + B, R - B) less these shifts
+  C rho0sd[2];       // rho0R + rho0B, rho0R - rho0B
+  C ssd[2][3];       // w_cls * rho0sd
 };
 
 template <typename C>
@@ -65,11 +69,16 @@ LeanConst<C> make_lean(const Ctx& c) {
   K.omega = (c.p.tauR == c.p.tauB) ? C(1) / (viscR / L.cssq + HALF) : C(-1);
   K.sigma = C(c.p.sigma);
   K.beta = C(c.p.beta);
-  bool shifted = (c.storage == LBX_STORE_F16 || c.storage == LBX_STORE_BF16);
+  bool shifted = c.storage != LBX_STORE_F32 && c.storage != LBX_STORE_F64;
   K.rho0[0] = shifted ? C(c.p.rho0R) : C(0);
   K.rho0[1] = shifted ? C(c.p.rho0B) : C(0);
+  K.rho0sd[0] = K.rho0[0] + K.rho0[1];
+  K.rho0sd[1] = K.rho0[0] - K.rho0[1];
   for (int comp = 0; comp < 2; ++comp)
-    for (int k = 0; k < 3; ++k) K.s[comp][k] = K.w[k] * K.rho0[comp];
+    for (int k = 0; k < 3; ++k) {
+      K.s[comp][k] = K.w[k] * K.rho0[comp];
+      K.ssd[comp][k] = K.w[k] * K.rho0sd[comp];
+    }
   return K;
 }
 
@@ -159,6 +168,7 @@ template <> struct SPair<float> {
   static __device__ __forceinline__ R ldr(const float* p) { return __ldg(reinterpret_cast<const float2*>(p)); }
   static __device__ __forceinline__ float2 cvt(R r) { return r; }
   static __device__ __forceinline__ float sum(R r) { return r.x + r.y; }
+  static __device__ __forceinline__ float first(R r) { return r.x; }
   static __device__ __forceinline__ float2 ld(const float* p) { return cvt(ldr(p)); }
   static __device__ __forceinline__ void st(float* p, float2 v) { *reinterpret_cast<float2*>(p) = v; }
 };
@@ -167,6 +177,7 @@ template <> struct SPair<double> {
   static __device__ __forceinline__ R ldr(const double* p) { return __ldg(reinterpret_cast<const double2*>(p)); }
   static __device__ __forceinline__ double2 cvt(R r) { return r; }
   static __device__ __forceinline__ double sum(R r) { return r.x + r.y; }
+  static __device__ __forceinline__ double first(R r) { return r.x; }
   static __device__ __forceinline__ double2 ld(const double* p) { return cvt(ldr(p)); }
   static __device__ __forceinline__ void st(double* p, double2 v) { *reinterpret_cast<double2*>(p) = v; }
 };
@@ -175,6 +186,7 @@ template <> struct SPair<__half> {
   static __device__ __forceinline__ R ldr(const __half* p) { return __ldg(reinterpret_cast<const __half2*>(p)); }
   static __device__ __forceinline__ float2 cvt(R r) { return __half22float2(r); }
   static __device__ __forceinline__ float sum(R r) { return add_mixed(r.y, __low2float(r)); }
+  static __device__ __forceinline__ float first(R r) { return __low2float(r); }
   static __device__ __forceinline__ float2 ld(const __half* p) { return cvt(ldr(p)); }
   static __device__ __forceinline__ void st(__half* p, float2 v) {
     *reinterpret_cast<__half2*>(p) = __float22half2_rn(v);
@@ -187,6 +199,7 @@ template <> struct SPair<__nv_bfloat16> {
   }
   static __device__ __forceinline__ float2 cvt(R r) { return __bfloat1622float2(r); }
   static __device__ __forceinline__ float sum(R r) { return add_mixed(r.y, __low2float(r)); }
+  static __device__ __forceinline__ float first(R r) { return __low2float(r); }
   static __device__ __forceinline__ float2 ld(const __nv_bfloat16* p) { return cvt(ldr(p)); }
   static __device__ __forceinline__ void st(__nv_bfloat16* p, float2 v) {
     *reinterpret_cast<__nv_bfloat162*>(p) = __float22bfloat162_rn(v);
@@ -286,8 +299,9 @@ __device__ __forceinline__ void pull_async(const S* __restrict__ A, int64_t n, c
 
 // densities (Sum g + rho0, before the clamp) from pairs already in shared
 // memory: each 16-bit value is added to the FP32 sums by one mixed-precision
-// add (same order and roundings as converting first)
-template <typename S, typename C>
+// add (same order and roundings as converting first).  SD: the pairs are
+// (R + B, R - B), whose sums give rho and rhoR - rhoB.
+template <typename S, typename C, bool SD = false>
 __device__ __forceinline__ void stage_rho(const typename SPair<S>::R* st, int stride, const LeanConst<C>& K, C& rR,
                                           C& rB) {
   P2<C> s = SPair<S>::cvt(st[0]);
@@ -297,8 +311,14 @@ __device__ __forceinline__ void stage_rho(const typename SPair<S>::R* st, int st
     s.x = add_mixed(r.x, s.x);
     s.y = add_mixed(r.y, s.y);
   }
-  rR = s.x + K.rho0[0];
-  rB = s.y + K.rho0[1];
+  if constexpr (SD) {
+    const C rho = s.x + K.rho0sd[0], dif = s.y + K.rho0sd[1];
+    rR = C(0.5) * (rho + dif);
+    rB = C(0.5) * (rho - dif);
+  } else {
+    rR = s.x + K.rho0[0];
+    rB = s.y + K.rho0[1];
+  }
 }
 
 // densities (Sum g + rho0, init_rho*_CG, before the clamp) of the pulled
@@ -446,8 +466,10 @@ __device__ __forceinline__ Relaxed<C> relax_sums(const LeanConst<C>& K, const C 
 
 // Recolouring half (perturbation + recolouring): the post-collision pairs
 // (stored form) into out[]; false, with out[] untouched, when the colour
-// gradient is below the reference's limit.
-template <typename C>
+// gradient is below the reference's limit.  SD: the pairs (R + B, R - B)
+// less their shifts; R + B is the perturbed total itself (kR + kB = 1 up to
+// rounding, the recolouring terms cancel) and R - B = (kR - kB) f + 2 T.
+template <typename C, bool SD = false>
 __device__ __forceinline__ bool recolour_sums(const LeanConst<C>& K, const Relaxed<C>& X, C rR, C rB, C px, C py,
                                               C pz, bool shifted, P2<C> out[Q]) {
   const C psq = fm(px, px, fm(py, py, pz * pz));
@@ -467,6 +489,28 @@ __device__ __forceinline__ bool recolour_sums(const LeanConst<C>& K, const Relax
   K3[1] = coef * K.w[1];
   K3[2] = coef * K.w2_sqrt2;
   const P2<C> KK = pp(kR, kB);
+  if constexpr (SD) {
+    const C kD = kR - kB;
+    const C fd = X.h0 - K0[0];
+    out[0] = pp(fd - K.ssd[0][0], fm(kD, fd, -K.ssd[1][0]));
+    const P2<C> pos[3] = {pp(px, -px), pp(py, -py), pp(pz, -pz)};
+    const P2<C> neg[3] = {pp(-px, px), pp(-py, py), pp(-pz, pz)};
+    const P2<C> KD = pp(kD, kD);
+#pragma unroll
+    for (int p = 1; p <= 9; ++p) {
+      const int l = 2 * p - 1, k = wclass(l);
+      const P2<C> ed = edot_pair<C>(l, pos, neg);                              // (e.psi, -e.psi)
+      const P2<C> pert = p_fma(pp(K1[k], K1[k]), p_mul(ed, ed), pp(-K0[k], -K0[k]));
+      const C t2 = C(2) * K3[k];
+      const P2<C> cD = p_fma(pp(t2, t2), ed, pp(-K.ssd[1][k], -K.ssd[1][k]));  // (2T, -2T) - s_D
+      const P2<C> fd = p_add(X.h[p - 1], pert);
+      const P2<C> oS = p_add(fd, pp(-K.ssd[0][k], -K.ssd[0][k]));
+      const P2<C> oD = p_fma(KD, fd, cD);
+      out[l] = pp(oS.x, oD.x);
+      out[l + 1] = pp(oS.y, oD.y);
+    }
+    return true;
+  }
   {
     const C fd = X.h0 - K0[0];
     out[0] = shifted ? p_fma(pp(fd, fd), KK, pp(-K.s[0][0], -K.s[1][0])) : p_mul(pp(fd, fd), KK);
@@ -497,9 +541,13 @@ __device__ __forceinline__ bool recolour_sums(const LeanConst<C>& K, const Relax
 // component (used with staged 16-bit pulls; the FP32 / FP64 kernels, with
 // more state live at this point, keep the per-direction form and stay
 // within their registers without spilling).
-template <typename C, bool PACKED>
+template <typename C, bool PACKED, bool SD = false>
 __device__ __forceinline__ void bgk_components(const LeanConst<C>& K, const Relaxed<C>& X, C rR, C rB, bool shifted,
                                                P2<C> g[Q]) {
+  // SD: g holds (R + B, R - B) pairs, rR / rB are rho and rhoR - rhoB, and
+  // the same BGK step (linear in the populations and the densities) applies
+  // with the shifts of the sum and the difference
+  const C(&sh)[2][3] = SD ? K.ssd : K.s;
   const C omega = X.omega, omm = C(1) - omega;
   if constexpr (!PACKED) {
     const P2<C> omm2 = pp(omm, omm);
@@ -509,7 +557,7 @@ __device__ __forceinline__ void bgk_components(const LeanConst<C>& K, const Rela
       const C eu = edot(l, X.u, X.v, X.w);
       const C a = fm(C(3), eu, fm(C(4.5) * eu, eu, X.c0));
       const P2<C> kc = pp(omega * rR * K.w[k], omega * rB * K.w[k]);
-      g[l] = shifted ? p_fma(g[l], omm2, p_fma(kc, pp(a, a), pp(-omega * K.s[0][k], -omega * K.s[1][k])))
+      g[l] = shifted ? p_fma(g[l], omm2, p_fma(kc, pp(a, a), pp(-omega * sh[0][k], -omega * sh[1][k])))
                      : p_fma(g[l], omm2, p_mul(kc, pp(a, a)));
     }
     return;
@@ -519,7 +567,7 @@ __device__ __forceinline__ void bgk_components(const LeanConst<C>& K, const Rela
   const P2<C> neg[3] = {pp(-X.u, X.u), pp(-X.v, X.v), pp(-X.w, X.w)};
   {
     const P2<C> kc = pp(omega * rR * K.w[0], omega * rB * K.w[0]);
-    g[0] = shifted ? p_fma(g[0], OMM, p_fma(kc, C0, pp(-omega * K.s[0][0], -omega * K.s[1][0])))
+    g[0] = shifted ? p_fma(g[0], OMM, p_fma(kc, C0, pp(-omega * sh[0][0], -omega * sh[1][0])))
                    : p_fma(g[0], OMM, p_mul(kc, C0));
   }
 #pragma unroll
@@ -531,8 +579,8 @@ __device__ __forceinline__ void bgk_components(const LeanConst<C>& K, const Rela
     const P2<C> Rv = pp(g[l].x, g[l + 1].x), Bv = pp(g[l].y, g[l + 1].y);
     P2<C> oR, oB;
     if (shifted) {
-      oR = p_fma(Rv, OMM, p_fma(pp(kR, kR), A, pp(-omega * K.s[0][k], -omega * K.s[0][k])));
-      oB = p_fma(Bv, OMM, p_fma(pp(kB, kB), A, pp(-omega * K.s[1][k], -omega * K.s[1][k])));
+      oR = p_fma(Rv, OMM, p_fma(pp(kR, kR), A, pp(-omega * sh[0][k], -omega * sh[0][k])));
+      oB = p_fma(Bv, OMM, p_fma(pp(kB, kB), A, pp(-omega * sh[1][k], -omega * sh[1][k])));
     } else {
       oR = p_fma(Rv, OMM, p_mul(pp(kR, kR), A));
       oB = p_fma(Bv, OMM, p_mul(pp(kB, kB), A));
@@ -653,7 +701,8 @@ struct LeanSmem {
 };
 
 // One column march: cells [x0, x0+TX) x [y0, y0+TY) x [z0, zend) of one box.
-template <typename S, int TX, int TY, bool PART>
+// SD: the stored pairs are sum / difference pairs (16-bit storage, no spheres).
+template <typename S, int TX, int TY, bool PART, bool SD = false>
 __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restrict__ B, const Geom& g,
                                             const LeanConst<typename Store<S>::C>& K, int x0, int y0, int z0,
                                             int zend, unsigned long long* err, int64_t step,
@@ -665,6 +714,7 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
   using C = typename Store<S>::C;
   constexpr int NT = TX * TY;
   using R = Ring<TX, TY>;
+  static_assert(!SD || (!PART && sizeof(typename SPair<S>::R) == 4), "sum / difference pairs: 16-bit, no spheres");
   const bool parts = PART && PT.fnew != nullptr;  // a box of the ensemble may have no spheres
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
   const bool active = (x0 + tx < g.nx) && (y0 + ty < g.ny);
@@ -770,7 +820,7 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
       }
     }
     if constexpr (STAGED) {
-      stage_rho<S, C>(st, stride, K, rR, rB);
+      stage_rho<S, C, SD>(st, stride, K, rR, rB);
     } else {
       PullIdx P;
       pull_idx(g, cx, cy, zz, P);
@@ -872,7 +922,7 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
       }
       C Ssum[Q];
 #pragma unroll
-      for (int l = 0; l < Q; ++l) Ssum[l] = SPair<S>::sum(pulled(l));
+      for (int l = 0; l < Q; ++l) Ssum[l] = SD ? SPair<S>::first(pulled(l)) : SPair<S>::sum(pulled(l));
       if constexpr (PART) {
         if (fresh) {
 #pragma unroll
@@ -917,7 +967,7 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
             pz = fm(a, ps, pz);
           }
         }
-        done = recolour_sums(K, rx, rRc, rBc, px, py, pz, Store<S>::shifted, gp);
+        done = recolour_sums<C, SD>(K, rx, rRc, rBc, px, py, pz, Store<S>::shifted, gp);
       }
       if (!done) {
 #pragma unroll
@@ -928,7 +978,10 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
             for (int l = 0; l < Q; ++l) gp[l] = SPair<S>::cvt(refilled(l));
           }
         }
-        if (collide) bgk_components<C, STAGED>(K, rx, rRc, rBc, Store<S>::shifted, gp);
+        if (collide) {
+          if constexpr (SD) bgk_components<C, STAGED, true>(K, rx, rRc + rBc, rRc - rBc, Store<S>::shifted, gp);
+          else bgk_components<C, STAGED>(K, rx, rRc, rBc, Store<S>::shifted, gp);
+        }
       }
 #pragma unroll
       for (int l = 0; l < Q; ++l) SPair<S>::st(Bp.at(l, cell), gp[l]);
@@ -937,7 +990,7 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
   if constexpr (ASYNC) cp_async_wait<0>();  // nothing in flight when the shared memory is reused
 }
 
-template <typename S, int TX, int TY, int MINB, bool PART>
+template <typename S, int TX, int TY, int MINB, bool PART, bool SD = false>
 __global__ void __launch_bounds__(TX* TY, MINB)
     k_cg_lean(const S* __restrict__ A, S* __restrict__ B, Geom g, LeanConst<typename Store<S>::C> K, int zlen,
               unsigned long long* err, int64_t step, LeanPart<typename Store<S>::C> PT) {
@@ -947,7 +1000,7 @@ __global__ void __launch_bounds__(TX* TY, MINB)
   __syncthreads();
   unsigned parity = 0;
   const int z0 = blockIdx.z * zlen;
-  lean_column<S, TX, TY, PART>(A, B, g, K, blockIdx.x * TX, blockIdx.y * TY, z0, min(z0 + zlen, g.nz), err, step,
+  lean_column<S, TX, TY, PART, SD>(A, B, g, K, blockIdx.x * TX, blockIdx.y * TY, z0, min(z0 + zlen, g.nz), err, step,
                                PT, M::phi(lean_smem), M::stage(lean_smem), M::side(lean_smem),
                                M::bar(lean_smem), parity);
 }
@@ -1027,18 +1080,18 @@ static int allow_smem(K* kernel, size_t bytes, unsigned long long& done_mask) {
 
 // Opt-in of k_cg_lean's shared memory and its resident CTAs per SM on this
 // device (the persistent grid), once per device.
-template <typename S, int TX, int TY, int MINB, bool PART>
+template <typename S, int TX, int TY, int MINB, bool PART, bool SD = false>
 static int prepare_lean(int* resident) {
   static unsigned long long done = 0;
   static int per_sm[64] = {0}, sms[64] = {0};
-  int rc = allow_smem(k_cg_lean<S, TX, TY, MINB, PART>, LeanSmem<S, TX, TY, PART>::BYTES, done);
+  int rc = allow_smem(k_cg_lean<S, TX, TY, MINB, PART, SD>, LeanSmem<S, TX, TY, PART>::BYTES, done);
   if (rc) return rc;
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return LBX_ERR_CUDA;
   dev &= 63;
   if (!per_sm[dev]) {
     int nb = 0, nsm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_cg_lean<S, TX, TY, MINB, PART>, TX * TY,
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_cg_lean<S, TX, TY, MINB, PART, SD>, TX * TY,
                                                       LeanSmem<S, TX, TY, PART>::BYTES) != cudaSuccess ||
         cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || nb < 1 || nsm < 1)
       return LBX_ERR_CUDA;
@@ -1055,16 +1108,16 @@ static int prepare_lean_multi() {
   return allow_smem(k_cg_lean_multi<S, TX, TY, MINB, PART>, LeanSmem<S, TX, TY, PART>::BYTES, done);
 }
 
-template <typename S, int TX, int TY, int MINB, bool PART>
+template <typename S, int TX, int TY, int MINB, bool PART, bool SD = false>
 static int launch_lean(Ctx& c, int zlen_override, LeanPart<typename Store<S>::C> pt) {
   using C = typename Store<S>::C;
   int resident = 0;
-  const int rc = prepare_lean<S, TX, TY, MINB, PART>(&resident);
+  const int rc = prepare_lean<S, TX, TY, MINB, PART, SD>(&resident);
   if (rc) return rc;
   const int zlen = zlen_override > 0 ? zlen_override : lean_zlen(c, TX, TY, resident);
   dim3 block(TX, TY, 1);
   dim3 grid((c.nx + TX - 1) / TX, (c.ny + TY - 1) / TY, (c.nz + zlen - 1) / zlen);
-  k_cg_lean<S, TX, TY, MINB, PART><<<grid, block, LeanSmem<S, TX, TY, PART>::BYTES, c.stream>>>(
+  k_cg_lean<S, TX, TY, MINB, PART, SD><<<grid, block, LeanSmem<S, TX, TY, PART>::BYTES, c.stream>>>(
       (const S*)c.pops[c.cur], (S*)c.pops[1 - c.cur], geom(c), make_lean<C>(c), zlen, c.d_err, c.step + 1, pt);
   return 0;
 }
@@ -1082,6 +1135,12 @@ int fluid_lean(Ctx& c) {
     int r = 0;
     if constexpr (std::is_same<S, double>::value) {
       r = launch_lean<S, 32, 8, 1, false>(c, c.lean_zlen, none);
+    } else if constexpr (std::is_same<S, float>::value) {
+      if (c.lean_shape == 1) r = launch_lean<S, 32, 16, 1, false>(c, c.lean_zlen, none);
+      else r = launch_lean<S, 32, 8, 2, false>(c, c.lean_zlen, none);
+    } else if (c.sd) {  // sum / difference pairs
+      if (c.lean_shape == 1) r = launch_lean<S, 32, 16, 1, false, true>(c, c.lean_zlen, none);
+      else r = launch_lean<S, 32, 8, 2, false, true>(c, c.lean_zlen, none);
     } else {
       if (c.lean_shape == 1) r = launch_lean<S, 32, 16, 1, false>(c, c.lean_zlen, none);
       else r = launch_lean<S, 32, 8, 2, false>(c, c.lean_zlen, none);

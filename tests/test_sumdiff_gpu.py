@@ -1,0 +1,155 @@
+"""16-bit sum / difference storage (LBX_STORE_F16_SD, LBX_STORE_BF16_SD).
+
+Each stored pair is (f_R + f_B - w_l (rho0R + rho0B), f_R - f_B - w_l (rho0R - rho0B)): the total population
+carries the momentum and sits near w_l rho, so it keeps more bits than either component.  The storage has
+no counterpart in the reference; these tests hold it to the same algorithm as the (f_R, f_B) storage (the
+first step agrees with FP16 pairs within FP16 rounding), to the FP64 run (errors well below the FP16 pairs'
+on the same run), to conservation, and to the argument checks that keep it on the single-pass
+colour-gradient kernel without spheres.
+"""
+import ctypes as C
+import re
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from lbcuda_b200 import capi
+
+LBX_ERR_ARG = -2  # include/lbx.h
+
+
+def test_storage_codes_match_the_header():
+    h = (Path(__file__).resolve().parents[1] / "include" / "lbx.h").read_text()
+    for name, key in (("LBX_STORE_F16_SD", "f16sd"), ("LBX_STORE_BF16_SD", "bf16sd")):
+        assert int(re.search(rf"#define {name} (\d+)", h).group(1)) == capi.STORAGE[key]
+
+
+def _create(**kw):
+    from lbcuda_b200 import make_params
+    p = make_params(32, **kw)
+    h = C.c_void_p()
+    rc = capi.lib().lbx_create(C.byref(p), C.byref(h))
+    if rc == 0:
+        capi.lib().lbx_destroy(h)
+    return rc
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("storage", ["f16sd", "bf16sd"])
+def test_rejected_outside_the_single_pass_kernel(storage):
+    from lbcuda_b200 import LBSim, make_params
+    from lbcuda_b200.ensemble import Ensemble
+    assert _create(model="cg", storage=storage) == 0
+    assert _create(model="bgk", storage=storage) == LBX_ERR_ARG
+    assert _create(model="cg-diffdens", storage=storage) == LBX_ERR_ARG
+    assert _create(model="cg", storage=storage, max_particles=2, radius=3.0) == LBX_ERR_ARG
+    g = LBSim(make_params(32, model="cg", storage=storage))
+    for fused in (0, 1):
+        assert capi.lib().lbx_set_schedule(g._h, fused) == LBX_ERR_ARG
+    assert capi.lib().lbx_set_schedule(g._h, 2) == 0
+    g.close()
+    with pytest.raises(capi.LBXError):
+        Ensemble([make_params(32, model="cg", storage=storage)] * 2)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("storage,tol", [("f16sd", 2e-3), ("bf16sd", 1.6e-2)])
+def test_populations_round_trip(storage, tol):
+    """set_pops / get_pops convert to and from the pairs: f_R, f_B back within the 16-bit rounding of R + B and
+    R - B (absolute, relative to the largest population)."""
+    from lbcuda_b200 import LBSim, make_params
+    n = 32
+    rng = np.random.default_rng(0)
+    w = np.array([1 / 3] + [1 / 18] * 6 + [1 / 36] * 12, np.float32)[:, None, None, None]
+    pR = (w * rng.uniform(0.0, 1.0, (19, n, n, n))).astype(np.float32)
+    pB = (w * rng.uniform(0.0, 1.0, (19, n, n, n))).astype(np.float32)
+    g = LBSim(make_params(n, model="cg", storage=storage))
+    g.set_pops(pR, pB)
+    a, b = g.get_pops()
+    assert np.abs(a - pR).max() <= tol * pR.max() and np.abs(b - pB).max() <= tol * pB.max()
+    g.close()
+
+
+@pytest.mark.gpu
+def test_equilibrium_and_uniform_flow_are_fixed_points():
+    from lbcuda_b200 import LBSim, make_params
+    n = 32
+    g = LBSim(make_params(n, model="cg", storage="f16sd"))
+    r = np.full((n, n, n), 0.5, np.float32)
+    g.set_fields(r, r, (0.05, -0.02, 0.03))
+    g.step(10)
+    rR, rB, vel, ph = g.get_fields(f64=True)
+    assert np.abs(rR - 0.5).max() < 1e-3 and np.abs(rB - 0.5).max() < 1e-3
+    assert np.abs(vel - np.array([0.05, -0.02, 0.03])).max() < 1e-4
+    g.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("storage", ["f16sd", "bf16sd"])
+def test_first_step_agrees_with_component_pairs(storage):
+    """One step of the same spinodal field: the sum / difference pairs and the (R, B) pairs of the same 16-bit
+    type agree to the type's rounding (densities relative to their largest value, velocity and phase field
+    absolute)."""
+    from lbcuda_b200 import LBSim, make_params
+    from lbcuda_b200.inputs import seeded_noise_fields
+    n = 48
+    rR, rB = seeded_noise_fields(n, n, n, seed=3)
+    out = {}
+    for st in (storage, storage[:-2]):
+        g = LBSim(make_params(n, model="cg", storage=st, sigma=0.02, beta=0.7))
+        g.set_fields(rR, rB)
+        g.step(1)
+        out[st] = g.get_fields(f64=True)
+        g.close()
+    eps = 2e-3 if storage == "f16sd" else 1.6e-2
+    a, b = out[storage], out[storage[:-2]]
+    for k in (0, 1):
+        assert np.abs(a[k] - b[k]).max() <= eps * np.abs(b[k]).max(), (storage, k)
+    assert np.abs(a[2] - b[2]).max() <= 0.1 * eps, storage
+    assert np.abs(a[3] - b[3]).max() <= eps, storage
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("storage,tol", [("f16sd", 1e-6), ("bf16sd", 8e-6)])
+def test_mass_conservation_full_size(storage, tol):
+    """128^3 spinodal, 50 steps: FP64 sums of each component's mass (what drifts is the rounding of the
+    stored pairs)."""
+    from lbcuda_b200 import LBSim, make_params
+    from lbcuda_b200.inputs import seeded_noise_fields
+    n = 128
+    rR, rB = seeded_noise_fields(n, n, n, seed=1)
+    g = LBSim(make_params(n, model="cg", storage=storage, sigma=0.02, beta=0.7))
+    g.set_fields(rR, rB)
+    g.step(1)
+    m0, _ = g.get_sums()
+    g.step(50)
+    m1, _ = g.get_sums()
+    drift = np.abs(m1 - m0) / m0
+    print(f"{storage}: mass drift {drift}")
+    assert (drift <= tol).all(), (storage, drift)
+    g.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("pair,bound_u", [(("f16sd", "f16"), 1e-3), (("bf16sd", "bf16"), 1e-2)])
+def test_error_vs_f64_below_component_pairs(pair, bound_u):
+    """48^3 spinodal, 100 steps: relative L2 error of u against the FP64 run, sum / difference pairs against
+    (R, B) pairs of the same type; the pairs' point is a several times smaller velocity error."""
+    from lbcuda_b200 import LBSim, make_params
+    from lbcuda_b200.inputs import seeded_noise_fields
+    n = 48
+    rR, rB = seeded_noise_fields(n, n, n, seed=2)
+    res = {}
+    for st in ("f64",) + pair:
+        g = LBSim(make_params(n, model="cg", storage=st, sigma=0.02, beta=0.7))
+        g.set_fields(rR, rB)
+        g.step(100)
+        res[st] = g.get_fields(f64=True)
+        g.close()
+    u64, p64 = res["f64"][2], res["f64"][3]
+    eu = {st: np.linalg.norm(res[st][2] - u64) / np.linalg.norm(u64) for st in pair}
+    ep = {st: np.linalg.norm(res[st][3] - p64) / np.linalg.norm(p64) for st in pair}
+    print(f"rel L2 err u {eu} phi {ep}")
+    assert eu[pair[0]] <= bound_u and eu[pair[0]] < eu[pair[1]] / 3
+    assert ep[pair[0]] < 2 * ep[pair[1]] + 1e-4
