@@ -260,6 +260,31 @@ def colloid_sim(storage, schedule=2, small=False):
     return s
 
 
+def colloid_error_vs_f64(steps=(100, 1000)):
+    """Colloid workload at 128^3 (160 spheres r = 5.5 moving at up to 0.01): relative L2 error of the velocity
+    field, relative max and L2 errors of the particle forces and the largest position difference of each
+    storage against the FP64 run of the same kernels."""
+    sims = {st: colloid_sim(st, small=True) for st in ("f64", "f32", "f16", "f16sd")}
+    out, done = {}, 0
+    for n in steps:
+        res = {}
+        for st, sm in sims.items():
+            sm.step(n - done)
+            res[st] = (sm.get_fields(f64=True)[2], sm.get_particles())
+        done = n
+        u64, p64 = res["f64"]
+        for st in ("f32", "f16", "f16sd"):
+            u, pp = res[st]
+            out.setdefault(st, {})[f"after_{n}"] = {
+                "u_rel_l2": float(np.linalg.norm(u - u64) / np.linalg.norm(u64)),
+                "force_rel_max": float(np.abs(pp["force"] - p64["force"]).max() / np.abs(p64["force"]).max()),
+                "force_rel_l2": float(np.linalg.norm(pp["force"] - p64["force"]) / np.linalg.norm(p64["force"])),
+                "x_abs_max": float(np.abs(pp["x"] - p64["x"]).max())}
+    for sm in sims.values():
+        sm.close()
+    return out
+
+
 def colloid_timing(storage, steps=50, warm=10, small=False):
     s = colloid_sim(storage, small=small)
     s.step(warm)
@@ -414,7 +439,8 @@ def only_region(args, local):
         return 0
     if args.only == "errors":
         print(json.dumps({"spinodal": error_vs_f64((100, 1000)),
-                          "droplet": error_vs_f64((100, 1000), workload="droplet")}), flush=True)
+                          "droplet": error_vs_f64((100, 1000), workload="droplet"),
+                          "colloid": colloid_error_vs_f64()}), flush=True)
         return 0
     if args.only == "variants":
         print(json.dumps({st: variants_timing(st) for st in ("f32", "f16")}), flush=True)
@@ -446,7 +472,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-extras", action="store_true", help="skip the error runs, the colloid case and the CPU baseline")
-    ap.add_argument("--only", choices=["f16", "f32", "bf16", "f64", "f16sd", "bf16sd", "colloid-f16", "colloid-f32", "colloid-f16-small",
+    ap.add_argument("--only", choices=["f16", "f32", "bf16", "f64", "f16sd", "bf16sd", "colloid-f16", "colloid-f32", "colloid-f16-small", "colloid-f16sd",
                                        "colloid-f32-small", "ensemble", "closure", "closure12", "variants", "errors"],
                     help="profiling aid: run one timed region only and print its timing")
     ap.add_argument("--lb-steps", type=int, default=LB_PER_STEP, help="lattice steps per bench step")
@@ -559,7 +585,8 @@ def main():
     if rank == 0 and not args.no_extras:
         extras["error_vs_f64"] = error_vs_f64()
         extras["error_vs_f64_droplet"] = error_vs_f64((100, 1000), workload="droplet")
-        extras["colloid_256_1280"] = {st: colloid_timing(st) for st in ("f16", "f32")}
+        extras["colloid_256_1280"] = {st: colloid_timing(st) for st in ("f16sd", "f16", "f32")}
+        extras["colloid_error_vs_f64"] = colloid_error_vs_f64()
         extras["ensemble_48"] = ensemble_timing()
         extras["variants_128"] = {st: variants_timing(st) for st in ("f32", "f16")}
         extras["closure"] = closure_experiment()

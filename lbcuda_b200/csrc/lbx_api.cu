@@ -151,8 +151,8 @@ int lbx_create(const lbx_params* p, void** out) {
     return LBX_ERR_ARG;
   if (p->storage < LBX_STORE_F32 || p->storage > LBX_STORE_BF16_SD) return LBX_ERR_ARG;
   const bool sd = p->storage == LBX_STORE_F16_SD || p->storage == LBX_STORE_BF16_SD;
-  // sum / difference pairs: the single-pass colour-gradient kernel without spheres only
-  if (sd && (p->model != LBX_MODEL_CG || p->max_particles > 0)) return LBX_ERR_ARG;
+  // sum / difference pairs: the single-pass colour-gradient kernel (with or without spheres) only
+  if (sd && p->model != LBX_MODEL_CG) return LBX_ERR_ARG;
   int64_t n = int64_t(p->nx) * p->ny * p->nz;
   if (n >= (int64_t(1) << 31)) return LBX_ERR_ARG;  // 32-bit cell indices
   Ctx* c = new (std::nothrow) Ctx();

@@ -714,7 +714,7 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
   using C = typename Store<S>::C;
   constexpr int NT = TX * TY;
   using R = Ring<TX, TY>;
-  static_assert(!SD || (!PART && sizeof(typename SPair<S>::R) == 4), "sum / difference pairs: 16-bit, no spheres");
+  static_assert(!SD || sizeof(typename SPair<S>::R) == 4, "sum / difference pairs: 16-bit storage");
   const bool parts = PART && PT.fnew != nullptr;  // a box of the ensemble may have no spheres
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
   const bool active = (x0 + tx < g.nx) && (y0 + ty < g.ny);
@@ -926,7 +926,7 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
       if constexpr (PART) {
         if (fresh) {
 #pragma unroll
-          for (int l = 0; l < Q; ++l) Ssum[l] = SPair<S>::sum(refilled(l));
+          for (int l = 0; l < Q; ++l) Ssum[l] = SD ? SPair<S>::first(refilled(l)) : SPair<S>::sum(refilled(l));
         }
       }
       rx = relax_sums(K, Ssum, rRc, rBc, Store<S>::shifted);
@@ -1161,6 +1161,8 @@ int fluid_lean_particles(Ctx& c, int fo, int fn) {
     kt_begin(c);
     int r = 0;
     if constexpr (std::is_same<S, double>::value) r = launch_lean<S, 32, 8, 1, true>(c, c.lean_zlen, pt);
+    else if constexpr (std::is_same<S, float>::value) r = launch_lean<S, 32, 8, 2, true>(c, c.lean_zlen, pt);
+    else if (c.sd) r = launch_lean<S, 32, 8, 2, true, true>(c, c.lean_zlen, pt);
     else r = launch_lean<S, 32, 8, 2, true>(c, c.lean_zlen, pt);
     kt_end(c);
     return r ? r : launch_status();

@@ -384,6 +384,7 @@ __global__ void __launch_bounds__(256) k_drain(PDev P, const double* __restrict_
     C qR[Q], qB[Q];
     pull_dead(A, Bold, g, b, 0, sh, fold, qR);
     pull_dead(A, Bold, g, b, 1, sh, fold, qB);
+    if (sh.sd) sd_to_rb(qR, qB);  // sum / difference pairs: the components' momenta below
     C rR = rhoR[cell], rB = rhoB[cell];
     C invrho = C(1) / (rR + rB);
     C u = invrho * mx(qR) + invrho * mx(qB);
@@ -427,6 +428,11 @@ __global__ void __launch_bounds__(256) k_rho_p(const S* __restrict__ A, const S*
     rR = sum_q(f);
     pull_dead(A, Bold, g, b, 1, sh, fold, f);
     rB = sum_q(f);
+    if (sh.sd) {  // sum / difference pairs: rho and rhoR - rhoB
+      const C t = rR;
+      rR = C(0.5) * (t + rB);
+      rB = C(0.5) * (t - rB);
+    }
     if (rR < C(-10) || rR > C(10) || rB < C(-10) || rB > C(10)) raise_error(err, LBX_DEV_RHO_RANGE, step, cell);
     if (rR < C(0)) rR = C(0);
     if (rB < C(0)) rB = C(0);
@@ -472,6 +478,11 @@ __device__ __forceinline__ void pulled_rho(const S* A, const Geom& g, const Shif
     ld_pair(A + pidx(g, 0, l, at(b, -ex(l), -ey(l), -ez(l))), sh.at(0, l), sh.at(1, l), fR[l], fB[l]);
   rR = sum_q(fR);
   rB = sum_q(fB);
+  if (sh.sd) {  // sum / difference pairs: rho and rhoR - rhoB
+    const C t = rR;
+    rR = C(0.5) * (t + rB);
+    rB = C(0.5) * (t - rB);
+  }
   rR = rR < C(0) ? C(0) : rR;
   rB = rB < C(0) ? C(0) : rB;
 }
@@ -592,7 +603,8 @@ __global__ void __launch_bounds__(256) k_fill(PDev P, const double* __restrict__
     phi[cell] = (Rs - Bs) / (Rs + Bs);
     C usq = L.half_inv_cssq * (u * u + v * v + w * w);
     for (int comp = 0; comp < 2; ++comp) {
-      C r = comp ? Bs : Rs;
+      // sum / difference pairs store the equilibria of rho and rhoR - rhoB
+      C r = sh.sd ? (comp ? Rs - Bs : Rs + Bs) : (comp ? Bs : Rs);
 #pragma unroll
       for (int l = 0; l < Q; ++l)
         Store<S>::st(B + pidx(g, comp, l, cell), equil_u(L, r, edot(l, u, v, w), usq, l), sh.at(comp, l));
@@ -868,6 +880,11 @@ __global__ void __launch_bounds__(256) k_bb(PDev P, const double* __restrict__ p
         hB[it] = __ldg(p + 1);
         rR[it] = rhoR[xf[it]];
         rB[it] = rhoB[xf[it]];
+        if (sh.sd) {  // sum / difference pairs: the wall term of each half is linear in its density
+          const C t = rR[it];
+          rR[it] = t + rB[it];
+          rB[it] = t - rB[it];
+        }
       }
     }
     if (n2p) {
@@ -884,7 +901,7 @@ __global__ void __launch_bounds__(256) k_bb(PDev P, const double* __restrict__ p
         C w = L.w[wclass(lf)];
         C f2pR = C(2) * St::dec(hR[it], sh.at(0, lf)) - w * buz * rR[it] * ev;
         C f2pB = C(2) * St::dec(hB[it], sh.at(1, lf)) - w * buz * rB[it] * ev;
-        C f2p = f2pR + f2pB;
+        C f2p = sh.sd ? f2pR : f2pR + f2pB;  // sum / difference pairs: the total is the first half
         double ft[3] = {double(f2p * C(ex(lf))), double(f2p * C(ey(lf))), double(f2p * C(ez(lf)))};
         s[0] += ft[0]; s[1] += ft[1]; s[2] += ft[2];
         if (P.lrotate) {
