@@ -701,7 +701,7 @@ struct LeanSmem {
 };
 
 // One column march: cells [x0, x0+TX) x [y0, y0+TY) x [z0, zend) of one box.
-// SD: the stored pairs are sum / difference pairs (16-bit storage, no spheres).
+// SD: the stored pairs are sum / difference pairs (16-bit storage).
 template <typename S, int TX, int TY, bool PART, bool SD = false>
 __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restrict__ B, const Geom& g,
                                             const LeanConst<typename Store<S>::C>& K, int x0, int y0, int z0,
