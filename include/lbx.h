@@ -56,10 +56,9 @@ extern "C" {
  * f_B - w_l rho0B).  The total population carries the momentum and sits near
  * w_l rho, so its shifted value is small and keeps more bits; rounding then
  * moves the velocity far less.  FP32 arithmetic as for LBX_STORE_F16.
- * Colour-gradient model (LBX_MODEL_CG) on the single-pass schedule, with or
- * without spheres; lbx_create rejects it with another model, and
- * lbx_set_schedule / lbx_ensemble_create reject it on the other schedules
- * and in the ensemble.
+ * Colour-gradient model (LBX_MODEL_CG) on the single-pass schedule (one box
+ * or the ensemble), with or without spheres; lbx_create rejects it with
+ * another model, lbx_set_schedule on the other schedules.
  * lbx_set_pops / lbx_get_pops and the field calls convert, so callers still
  * see f_R and f_B. */
 #define LBX_STORE_F16_SD 4

@@ -1024,7 +1024,7 @@ struct WorkItem {
   int box, x0, y0, z0, zend;
 };
 
-template <typename S, int TX, int TY, int MINB, bool PART>
+template <typename S, int TX, int TY, int MINB, bool PART, bool SD = false>
 __global__ void __launch_bounds__(TX* TY, MINB)
     k_cg_lean_multi(const BoxDesc<typename Store<S>::C>* __restrict__ boxes, const WorkItem* __restrict__ work,
                     int nwork, LeanConst<typename Store<S>::C> K) {
@@ -1037,8 +1037,8 @@ __global__ void __launch_bounds__(TX* TY, MINB)
   for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
     const WorkItem it = work[w];
     const BoxDesc<C> bd = boxes[it.box];
-    lean_column<S, TX, TY, PART>((const S*)bd.A, (S*)bd.B, bd.g, K, it.x0, it.y0, it.z0, it.zend, bd.err, bd.step,
-                                 bd.pt, M::phi(lean_smem), M::stage(lean_smem), M::side(lean_smem),
+    lean_column<S, TX, TY, PART, SD>((const S*)bd.A, (S*)bd.B, bd.g, K, it.x0, it.y0, it.z0, it.zend, bd.err,
+                                     bd.step, bd.pt, M::phi(lean_smem), M::stage(lean_smem), M::side(lean_smem),
                                  M::bar(lean_smem), parity);
     __syncthreads();  // the window is reused by the next item
   }
@@ -1102,10 +1102,10 @@ static int prepare_lean(int* resident) {
   return 0;
 }
 
-template <typename S, int TX, int TY, int MINB, bool PART>
+template <typename S, int TX, int TY, int MINB, bool PART, bool SD = false>
 static int prepare_lean_multi() {
   static unsigned long long done = 0;
-  return allow_smem(k_cg_lean_multi<S, TX, TY, MINB, PART>, LeanSmem<S, TX, TY, PART>::BYTES, done);
+  return allow_smem(k_cg_lean_multi<S, TX, TY, MINB, PART, SD>, LeanSmem<S, TX, TY, PART>::BYTES, done);
 }
 
 template <typename S, int TX, int TY, int MINB, bool PART, bool SD = false>
@@ -1213,6 +1213,12 @@ int ensemble_launch(const std::vector<Ctx*>& boxes, int shape, const std::vector
       int rp = 0;
       if constexpr (std::is_same<S, double>::value) {
         rp = prepare_lean_multi<S, 32, 8, 1, true>();
+      } else if constexpr (std::is_same<S, float>::value) {
+        rp = prepare_lean_multi<S, 32, 16, 1, true>();
+        if (!rp) rp = prepare_lean_multi<S, 32, 8, 2, true>();
+      } else if (c0.sd) {
+        rp = prepare_lean_multi<S, 32, 16, 1, true, true>();
+        if (!rp) rp = prepare_lean_multi<S, 32, 8, 2, true, true>();
       } else {
         rp = prepare_lean_multi<S, 32, 16, 1, true>();
         if (!rp) rp = prepare_lean_multi<S, 32, 8, 2, true>();
@@ -1230,13 +1236,28 @@ int ensemble_launch(const std::vector<Ctx*>& boxes, int shape, const std::vector
     if constexpr (std::is_same<S, double>::value) {
       int grid = std::min(nwork, 148);
       k_cg_lean_multi<S, 32, 8, 1, true><<<grid, dim3(32, 8), LeanSmem<S, 32, 8, true>::BYTES, stream>>>(D, W, nwork, K);
-    } else if (shape == 1) {
-      int grid = std::min(nwork, 148);
-      k_cg_lean_multi<S, 32, 16, 1, true><<<grid, dim3(32, 16), LeanSmem<S, 32, 16, true>::BYTES, stream>>>(D, W, nwork,
-                                                                                                      K);
     } else {
-      int grid = std::min(nwork, 296);
-      k_cg_lean_multi<S, 32, 8, 2, true><<<grid, dim3(32, 8), LeanSmem<S, 32, 8, true>::BYTES, stream>>>(D, W, nwork, K);
+      bool launched = false;
+      if constexpr (!std::is_same<S, float>::value) {
+        if (c0.sd) {  // sum / difference pairs
+          if (shape == 1)
+            k_cg_lean_multi<S, 32, 16, 1, true, true>
+                <<<std::min(nwork, 148), dim3(32, 16), LeanSmem<S, 32, 16, true>::BYTES, stream>>>(D, W, nwork, K);
+          else
+            k_cg_lean_multi<S, 32, 8, 2, true, true>
+                <<<std::min(nwork, 296), dim3(32, 8), LeanSmem<S, 32, 8, true>::BYTES, stream>>>(D, W, nwork, K);
+          launched = true;
+        }
+      }
+      if (!launched && shape == 1) {
+        int grid = std::min(nwork, 148);
+        k_cg_lean_multi<S, 32, 16, 1, true><<<grid, dim3(32, 16), LeanSmem<S, 32, 16, true>::BYTES, stream>>>(
+            D, W, nwork, K);
+      } else if (!launched) {
+        int grid = std::min(nwork, 296);
+        k_cg_lean_multi<S, 32, 8, 2, true><<<grid, dim3(32, 8), LeanSmem<S, 32, 8, true>::BYTES, stream>>>(D, W,
+                                                                                                          nwork, K);
+      }
     }
     return launch_status();
   });

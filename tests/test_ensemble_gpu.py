@@ -17,7 +17,7 @@ def _params(L, n, storage="f32"):
                        hz_rmin=7.5, hz_rcap=6.0)
 
 
-@pytest.mark.parametrize("storage", ["f32", "f16"])
+@pytest.mark.parametrize("storage", ["f32", "f16", "f16sd"])
 def test_ensemble_equals_boxes_alone(storage):
     spec = random_boxes(6, seed=3, edges=(32, 48), max_spheres=6)
     params = [_params(L, len(x), storage) for L, x in spec]

@@ -5,7 +5,7 @@ carries the momentum and sits near w_l rho, so it keeps more bits than either co
 no counterpart in the reference; these tests hold it to the same algorithm as the (f_R, f_B) storage (the
 first step agrees with FP16 pairs within FP16 rounding), to the FP64 run (errors well below the FP16 pairs'
 on the same run, with and without moving spheres), to conservation, and to the argument checks that keep it
-on the single-pass colour-gradient kernel.
+on the single-pass colour-gradient kernels (one box, or the ensemble: `tests/test_ensemble_gpu.py`).
 """
 import ctypes as C
 import re
@@ -38,9 +38,8 @@ def _create(**kw):
 @pytest.mark.gpu
 @pytest.mark.parametrize("storage", ["f16sd", "bf16sd"])
 def test_rejected_outside_the_single_pass_kernel(storage):
-    """Other models, the other schedules and the ensemble (which reads (R, B) pairs) refuse the format."""
+    """Other models and the other schedules refuse the format (spheres and the ensemble take it)."""
     from lbcuda_b200 import LBSim, make_params
-    from lbcuda_b200.ensemble import Ensemble
     assert _create(model="cg", storage=storage) == 0
     assert _create(model="bgk", storage=storage) == LBX_ERR_ARG
     assert _create(model="cg-diffdens", storage=storage) == LBX_ERR_ARG
@@ -50,8 +49,6 @@ def test_rejected_outside_the_single_pass_kernel(storage):
         assert capi.lib().lbx_set_schedule(g._h, fused) == LBX_ERR_ARG
     assert capi.lib().lbx_set_schedule(g._h, 2) == 0
     g.close()
-    with pytest.raises(capi.LBXError):
-        Ensemble([make_params(32, model="cg", storage=storage)] * 2)
 
 
 @pytest.mark.gpu
