@@ -367,7 +367,8 @@ def ensemble_timing(steps=100, err_steps=200, seed=7):
             "u_rel_l2_vs_f32_per_box": {"after_steps": err_steps, "max": max(errs), "median": float(np.median(errs))}}
 
 
-def closure_experiment(R_hi=6, L_hi=48, R_lo=3, steps_hi=240, m=256, epochs=100, n_direct=64, seed=11):
+def closure_experiment(R_hi=6, L_hi=48, R_lo=3, steps_hi=240, m=256, epochs=100, n_direct=64, seed=11,
+                       return_weights=False):
     """Learned closure workload.  Training data: the resistance of every lattice class of R_lo pairs with
     gap/R in [0.05, 1.5] (121 classes at R_lo = 3; R_hi resolved in L_hi^3, R_lo in the box scaled by
     R_lo / R_hi; a rest run and nine unit pair-frame velocity runs per class and resolution, static force
@@ -414,13 +415,67 @@ def closure_experiment(R_hi=6, L_hi=48, R_lo=3, steps_hi=240, m=256, epochs=100,
         costs[R] = tot / 100
         sim.close()
     steps_lo = info["steps_lo"]
-    return {"R_hi": R_hi, "R_lo": R_lo, "L_hi": L_hi, "steps_hi": steps_hi, "steps_lo": steps_lo,
+    out = {"R_hi": R_hi, "R_lo": R_lo, "L_hi": L_hi, "steps_hi": steps_hi, "steps_lo": steps_lo,
             "classes": int(len(res["gap"])), "train_samples": int(len(X)), "epochs": epochs,
             "resistance_s": t_res, "train_s": t_train, "final_loss": float(loss[-1]),
             "held_out_direct_pairs": n_direct, "error_direct": errors(Xd, Td, info["base"]),
             "error_fresh_velocities": errors(Xv, Tv, bv),
             "ms_per_step": {"R_hi": costs[R_hi], "R_lo": costs[R_lo]},
             "cost_ratio_same_physical_time": costs[R_hi] * steps_hi / (costs[R_lo] * steps_lo)}
+    return (out, w) if return_weights else out
+
+
+def suspension_positions(L, n, r, seed=9, min_gap=0.1):
+    """Seeded non-overlapping centres (centre distance >= 2r + min_gap) in a periodic L^3 box."""
+    rng = np.random.default_rng(seed)
+    x = np.zeros((0, 3))
+    while len(x) < n:
+        c = rng.uniform(1, L, 3)
+        d = x - c
+        d -= L * np.round(d / L)
+        if not len(x) or (d * d).sum(1).min() >= (2 * r + min_gap) ** 2:
+            x = np.vstack([x, c])
+    return x
+
+
+def closure_suspension(w, L=256, n=4000, r=3.0, steps=50, warm=10, seed=9):
+    """The trained closure deployed: L^3 one-colour fluid with n spheres of radius r (seeded, gaps >= 0.1),
+    velocities uniform in +-5e-4 (pair-frame relative velocities inside the training envelope), FP16 sum /
+    difference pairs.  ms per step with the network on every close pair inside its envelope (analytic
+    lubrication outside it) and with the analytic lubrication alone."""
+    import ctypes
+    from lbcuda_b200 import LBSim, capi, make_params
+    x = suspension_positions(L, n, r, seed)
+    v = np.random.default_rng(seed + 1).uniform(-5e-4, 5e-4, (n, 3))
+    vol = 4.0 / 3.0 * np.pi * r ** 3
+    close = 0
+    for i0 in range(0, n, 500):
+        d = x[i0:i0 + 500, None, :] - x[None, :, :]
+        d -= L * np.round(d / L)
+        dist = np.sqrt((d * d).sum(-1))
+        close += int(((dist > 0) & (dist <= (2.0 + 1.5) * r)).sum())
+    close //= 2
+    out = {"box": L, "spheres": n, "radius": r, "volume_fraction": n * vol / L ** 3, "pairs_gap_le_1.5R": close}
+    for name, on in (("closure", 1), ("analytic_only", 0)):
+        p = make_params(L, model="cg", storage="f16sd", max_particles=n, radius=r, rmass=float(1.0 / vol),
+                        wetting="neutral", lrotate=1, max_vel=1.0, exact_tiles=0, hz_rmin=float(2 * r - 0.5),
+                        hz_rcap=float(2 * r - 2.0), closure=on, lubrication=1, lubric_k=1.0 / 6.0, lubric_rmin=1.0,
+                        lubric_rcap=float(0.05 * r))
+        s = LBSim(p)
+        if on:
+            wf = np.ascontiguousarray(w, np.float32)
+            capi.check(capi.lib().lbx_closure_set(s._h, wf.ctypes.data_as(ctypes.POINTER(ctypes.c_float))),
+                       "lbx_closure_set")
+        one = np.ones((L, L, L), np.float32)
+        s.set_fields(one, np.zeros_like(one))
+        s.set_particles(x, v)
+        s.step(warm)
+        s.sync()
+        tot, _, _ = s.time_steps(steps, kernel_timing=False)
+        out[name] = {"ms_per_step": tot / steps, "device_error": s.status()[0]}
+        s.close()
+    out["closure_overhead"] = out["closure"]["ms_per_step"] / out["analytic_only"]["ms_per_step"] - 1.0
+    return out
 
 
 def only_region(args, local):
@@ -429,7 +484,9 @@ def only_region(args, local):
     from lbcuda_b200 import LBSim, make_params
     from lbcuda_b200.inputs import seeded_noise_fields
     if args.only == "closure":
-        print(json.dumps(closure_experiment()), flush=True)
+        res, w = closure_experiment(return_weights=True)
+        res["suspension"] = closure_suspension(w)
+        print(json.dumps(res), flush=True)
         return 0
     if args.only == "closure12":
         print(json.dumps(closure_experiment(R_hi=12, L_hi=96, steps_hi=960)), flush=True)
@@ -589,7 +646,8 @@ def main():
         extras["colloid_error_vs_f64"] = colloid_error_vs_f64()
         extras["ensemble_48"] = ensemble_timing()
         extras["variants_128"] = {st: variants_timing(st) for st in ("f32", "f16")}
-        extras["closure"] = closure_experiment()
+        extras["closure"], w = closure_experiment(return_weights=True)
+        extras["closure"]["suspension"] = closure_suspension(w)
         extras["cpu_baseline"] = cpu_baseline_sample()
 
     if rank == 0:

@@ -20,8 +20,9 @@
 //                set: forward, backward and update fused, activations in
 //                shared memory, gradients reduced in a fixed order.
 //   k_mlp_infer  one warp per sample (pair), weights in shared memory.
-//   k_pair_nbrs / k_closure_pairs / k_closure_accum: per step, the close
-//                pairs of each sphere (ascending index), the closure (or the
+//   k_pairs (lbx_particles.cu) / k_closure_pairs / k_closure_accum: per
+//                step, the close pairs of each sphere (ascending index, listed
+//                by the all-pairs force pass), the closure (or the
 //                analytic lubrication when the pair leaves the training
 //                envelope) and a fixed-order accumulation per sphere.
 #include "lbx_device.cuh"

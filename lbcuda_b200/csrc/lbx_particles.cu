@@ -962,8 +962,12 @@ __global__ void __launch_bounds__(256) k_bb(PDev P, const double* __restrict__ p
 // lanes take every 32nd partner and the warp sums their shares in a fixed
 // order.  With lubrication on, the analytic squeeze force is added as well
 // (the reference writes it into a total that its integrator then
-// overwrites; here it reaches the integrator).
-__global__ void __launch_bounds__(256) k_pairs(PDev P, const double* __restrict__ pos, double* acc, Geom g) {
+// overwrites; here it reaches the integrator).  With the learned closure the
+// same pass lists each sphere's close partners for it (nbr, cnt), so the
+// closure costs no second all-pairs pass.
+__global__ void __launch_bounds__(256) k_pairs(PDev P, const double* __restrict__ pos, double* acc, Geom g,
+                                               double gap_cut, int* nbr, int* cnt, unsigned long long* err,
+                                               int64_t step) {
   const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
   if (i >= P.np) return;
   const double rsqcut = P.hz_rmin * P.hz_rmin;
@@ -973,35 +977,53 @@ __global__ void __launch_bounds__(256) k_pairs(PDev P, const double* __restrict_
   const double rparcut = rpar + P.lub_rmin;
   const double mxrsqcut = fmax(rparcut * rparcut, rsqcut);
   const double rparcap = rpar + P.lub_rcap;
+  // closure neighbour list (nbr != nullptr): partners with gap below gap_cut,
+  // ascending (32 partners per pass, hits appended in lane order)
+  const double nbr_pre = (2.0 * P.rdim + gap_cut + 1.0) * (2.0 * P.rdim + gap_cut + 1.0);
   double f[3] = {0, 0, 0}, fl[3] = {0, 0, 0};
-  for (int j = lane; j < P.np; j += 32) {
-    if (j == i) continue;
-    // pair (lo, hi) with d = x_hi - x_lo as in addHertzian(lo, hi)
-    const int lo = min(i, j), hi = max(i, j);
-    const double* pl = pos + size_t(lo) * PS;
-    const double* ph = pos + size_t(hi) * PS;
-    double xdf = ph[0] - pl[0], ydf = ph[1] - pl[1], zdf = ph[2] - pl[2];
-    xdf = xdf - double(g.nx * nint_d(xdf / g.nx));
-    ydf = ydf - double(g.ny * nint_d(ydf / g.ny));
-    zdf = zdf - double(g.nz * nint_d(zdf / g.nz));
-    double rsq = xdf * xdf + ydf * ydf + zdf * zdf;
-    if (rsq > mxrsqcut) continue;
-    double rrr = sqrt(rsq);
-    double sgn = (i == lo) ? -1.0 : 1.0;
-    if (rrr <= P.hz_rmin) {
-      double ggg = (rrr <= P.hz_rcap) ? gmin : 5.0 * 0.5 * P.hz_k * pow(P.hz_rmin - rrr, 1.5);
-      f[0] += sgn * (ggg * xdf / rrr);
-      f[1] += sgn * (ggg * ydf / rrr);
-      f[2] += sgn * (ggg * zdf / rrr);
+  int c = 0;
+  for (int j0 = 0; j0 < P.np; j0 += 32) {
+    const int j = j0 + lane;
+    bool hit = false;
+    if (j < P.np && j != i) {
+      // pair (lo, hi) with d = x_hi - x_lo as in addHertzian(lo, hi)
+      const int lo = min(i, j), hi = max(i, j);
+      const double* pl = pos + size_t(lo) * PS;
+      const double* ph = pos + size_t(hi) * PS;
+      double xdf = ph[0] - pl[0], ydf = ph[1] - pl[1], zdf = ph[2] - pl[2];
+      xdf = xdf - double(g.nx * nint_d(xdf / g.nx));
+      ydf = ydf - double(g.ny * nint_d(ydf / g.ny));
+      zdf = zdf - double(g.nz * nint_d(zdf / g.nz));
+      double rsq = xdf * xdf + ydf * ydf + zdf * zdf;
+      if (nbr && rsq < nbr_pre) hit = sqrt(rsq) - 2.0 * P.rdim < gap_cut;
+      if (rsq <= mxrsqcut) {
+        double rrr = sqrt(rsq);
+        double sgn = (i == lo) ? -1.0 : 1.0;
+        if (rrr <= P.hz_rmin) {
+          double ggg = (rrr <= P.hz_rcap) ? gmin : 5.0 * 0.5 * P.hz_k * pow(P.hz_rmin - rrr, 1.5);
+          f[0] += sgn * (ggg * xdf / rrr);
+          f[1] += sgn * (ggg * ydf / rrr);
+          f[2] += sgn * (ggg * zdf / rrr);
+        }
+        if (P.lub && !P.closure && rrr <= rparcut) {
+          double ux = xdf / rrr, uy = ydf / rrr, uz = zdf / rrr;
+          if (rrr <= rparcap) rrr = rparcap;
+          double dotuv = ux * (pl[3] - ph[3]) + uy * (pl[4] - ph[4]) + uz * (pl[5] - ph[5]);
+          double cc = lubfactor * dotuv * (1.0 / (rrr - rpar) - 1.0);
+          fl[0] += sgn * (cc * ux);
+          fl[1] += sgn * (cc * uy);
+          fl[2] += sgn * (cc * uz);
+        }
+      }
     }
-    if (P.lub && !P.closure && rrr <= rparcut) {
-      double ux = xdf / rrr, uy = ydf / rrr, uz = zdf / rrr;
-      if (rrr <= rparcap) rrr = rparcap;
-      double dotuv = ux * (pl[3] - ph[3]) + uy * (pl[4] - ph[4]) + uz * (pl[5] - ph[5]);
-      double cc = lubfactor * dotuv * (1.0 / (rrr - rpar) - 1.0);
-      fl[0] += sgn * (cc * ux);
-      fl[1] += sgn * (cc * uy);
-      fl[2] += sgn * (cc * uz);
+    if (nbr) {
+      const unsigned m = __ballot_sync(0xffffffffu, hit);
+      const int slot = c + __popc(m & ((1u << lane) - 1u));
+      if (hit) {
+        if (slot < NBCAP) nbr[size_t(i) * NBCAP + slot] = j;
+        else raise_error(err, LBX_DEV_LIST_OVERFLOW, step, i);
+      }
+      c += __popc(m);
     }
   }
 #pragma unroll
@@ -1010,11 +1032,13 @@ __global__ void __launch_bounds__(256) k_pairs(PDev P, const double* __restrict_
       f[d] += __shfl_down_sync(0xffffffffu, f[d], o);
       fl[d] += __shfl_down_sync(0xffffffffu, fl[d], o);
     }
-  if (lane == 0)
+  if (lane == 0) {
     for (int d = 0; d < 3; ++d) {
       acc[size_t(i) * AS + 6 + d] += f[d];
       acc[size_t(i) * AS + 12 + d] += fl[d];
     }
+    if (nbr) cnt[i] = min(c, NBCAP);
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -1027,35 +1051,6 @@ __device__ __forceinline__ void min_image(const Geom& g, const double* pl, const
   d[0] = d[0] - double(g.nx * nint_d(d[0] / g.nx));
   d[1] = d[1] - double(g.ny * nint_d(d[1] / g.ny));
   d[2] = d[2] - double(g.nz * nint_d(d[2] / g.nz));
-}
-
-// close neighbours of each sphere in ascending index (gap below the cut):
-// one warp per sphere tests 32 partners at a time and appends the hits in
-// lane order
-__global__ void __launch_bounds__(256) k_pair_nbrs(PDev P, const double* __restrict__ pos, Geom g, double gap_cut,
-                                                   int* nbr, int* cnt, unsigned long long* err, int64_t step) {
-  const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-  if (i >= P.np) return;
-  const double* pi = pos + size_t(i) * PS;
-  int c = 0;
-  for (int j0 = 0; j0 < P.np; j0 += 32) {
-    const int j = j0 + lane;
-    bool hit = false;
-    if (j < P.np && j != i) {
-      double d[3];
-      min_image(g, pi, pos + size_t(j) * PS, d);
-      double r = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
-      hit = r - 2.0 * P.rdim < gap_cut;
-    }
-    const unsigned m = __ballot_sync(0xffffffffu, hit);
-    const int slot = c + __popc(m & ((1u << lane) - 1u));
-    if (hit) {
-      if (slot < NBCAP) nbr[size_t(i) * NBCAP + slot] = j;
-      else raise_error(err, LBX_DEV_LIST_OVERFLOW, step, i);
-    }
-    c += __popc(m);
-  }
-  if (lane == 0) cnt[i] = min(c, NBCAP);
 }
 
 // one warp per close pair (i < j): the network inside its training envelope,
@@ -1678,13 +1673,16 @@ int part_pairs(Ctx& c) {
   Stage t(c);
   ParticleState& s = t.s;
   const int warp_blocks = (s.np * 32 + 255) / 256;
-  k_pairs<<<warp_blocks, 256, 0, c.stream>>>(t.P, t.pc, s.acc, t.g);
+  // with the closure, the same all-pairs pass lists each sphere's close
+  // partners; the network's gap is that of the rounded centres, up to
+  // sqrt 3 closer than the centres' own
+  const double cut = c.p.closure ? fmax(double(c.p.closure_gap_max) * s.rdim + 1.75,
+                                        c.p.lubrication ? double(c.p.lubric_rmin) : 0.0)
+                                 : 0.0;
+  k_pairs<<<warp_blocks, 256, 0, c.stream>>>(t.P, t.pc, s.acc, t.g, cut, c.p.closure ? s.nbr : nullptr, s.nbr_cnt,
+                                              c.d_err, t.st);
   if (c.p.closure) {
     const int use_net = s.closure_ready;
-    // the network's gap is that of the rounded centres, up to sqrt 3 closer
-    const double cut =
-        fmax(double(c.p.closure_gap_max) * s.rdim + 1.75, c.p.lubrication ? double(c.p.lubric_rmin) : 0.0);
-    k_pair_nbrs<<<warp_blocks, 256, 0, c.stream>>>(t.P, t.pc, t.g, cut, s.nbr, s.nbr_cnt, c.d_err, t.st);
     size_t smem = sizeof(float) * (size_t(LBX_CLOSURE_NWEIGHTS) + 8 * 2 * H);
     int blocks = (s.np * NBCAP + 7) / 8;
     if (blocks > 148 * 4) blocks = 148 * 4;
