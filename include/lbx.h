@@ -252,9 +252,12 @@ int lbx_closure_infer(const float* weights, const float* X, int32_t n, float* Y)
  * reference), for callers that must not allocate or free device memory:
  * inputs and outputs go through one fixed device array per device
  * (449,792 bytes).  n <= LBX_CLOSURE_NOALLOC_MAX, else LBX_ERR_ARG.  The
- * first call on a device (that device current) looks the array up; make it
- * before any stream capture.  Calls that overlap in time on one device share
- * the array and race: serialise them.  Same results as lbx_closure_infer. */
+ * first call on a device (that device current) looks the array up; with lazy
+ * module loading that is also when the array gets its device memory, so make
+ * the first call before reserving device memory up front and before any
+ * stream capture.  Not valid after cudaDeviceReset in the same process.
+ * Calls that overlap in time on one device share the array and race:
+ * serialise them.  Same results as lbx_closure_infer. */
 #define LBX_CLOSURE_NOALLOC_MAX 4096
 int lbx_closure_infer_noalloc(const float* weights, const float* X, int32_t n, float* Y);
 /* Attach trained weights to a particle context; with p->closure = 1 each

@@ -16,8 +16,15 @@
 //              feature rows it uses, and the kernel writes every output row
 //              that is copied back
 //   setup:     the first call on a device, with that device current, looks
-//              up the array's address (cudaGetSymbolAddress) and keeps it;
-//              make that first call before any stream capture
+//              up the array's address (cudaGetSymbolAddress) and keeps it.
+//              With lazy module loading (the CUDA default) that lookup is
+//              also where the library's module, and with it this array, gets
+//              its device memory, so make the first call on each device
+//              before reserving device memory up front and before any stream
+//              capture
+//   lifetime:  the kept address belongs to the device's primary context;
+//              after cudaDeviceReset the entry point is not valid any more in
+//              this process (the address would be stale)
 //   races:     calls share the array of their device; calls that overlap in
 //              time on one device (several host threads) race, so such
 //              callers serialise them
@@ -71,6 +78,9 @@ int lbx_closure_infer_noalloc(const float* weights, const float* X, int32_t n, f
   float* dW = base;
   float* dX = base + kWPad;
   float* dY = dX + size_t(LBX_CLOSURE_NOALLOC_MAX) * kDin;
+  // The copies and the launch all go to the legacy default stream, so the
+  // blocking copy of Y back waits for the kernel without a separate
+  // synchronise; a move of the launch to another stream needs one.
   rc = rc_of(cudaMemcpy(dW, weights, size_t(LBX_CLOSURE_NWEIGHTS) * 4, cudaMemcpyHostToDevice));
   if (!rc) rc = rc_of(cudaMemcpy(dX, X, size_t(n) * kDin * 4, cudaMemcpyHostToDevice));
   if (!rc) rc = lbx::closure_infer_launch(dW, dX, n, dY);

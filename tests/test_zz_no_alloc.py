@@ -56,6 +56,23 @@ def test_two_calls_in_a_row_match_the_allocating_entry_point():
         assert np.array_equal(Y, ref)
 
 
+def test_calls_leave_free_device_memory_unchanged():
+    """After one warm-up call (module load, first lookup) the entry point must
+    not allocate: the device's free memory stays the same over more calls."""
+    import torch
+    w = _weights(4)
+    X = np.random.default_rng(4).normal(size=(NMAX, DIN)).astype(np.float32)
+    rc, _ = _infer("lbx_closure_infer_noalloc", w, X)
+    assert rc == 0
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    for n in (NMAX, 1, 513, NMAX):
+        rc, Y = _infer("lbx_closure_infer_noalloc", w, X[:n])
+        assert rc == 0 and np.isfinite(Y).all()
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free0
+
+
 def test_sizes_beyond_the_scratch_are_rejected():
     w = _weights(3)
     X = np.zeros((NMAX + 1, DIN), np.float32)
