@@ -119,15 +119,24 @@ def dist_env():
     return ws, rank, local
 
 
+WORKLOAD = ("colour-gradient spinodal 128^3 periodic, rho=0.5+U(-0.01,0.01) seed 1, tau=1, sigma=0.02, beta=0.7, "
+            "10,000 lattice steps")
+
+
+def workload_config():
+    """The `config` object both arms print (the timed sample of each arm is described beside it)."""
+    return {"workload": WORKLOAD, "cells": L ** 3, "lattice_steps_total": 20 * LB_PER_STEP,
+            "l2": "inputs larger than L2 (2 x 160 MB population buffers at FP16, 2 x 320 MB at FP32)"}
+
+
 def reference_arm(args, ws, rank):
-    """The oracle (CPU restatement of the reference) on all host cores."""
+    """The oracle (CPU restatement of the reference) on all host cores; it imports nothing of the
+    product package, only oracle/."""
     if rank != 0:
         return 0
-    from oracle.orc import OracleSim, num_threads
-    from lbcuda_b200 import make_params
-    from lbcuda_b200.inputs import seeded_noise_fields
-    p = make_params(L, model="cg", storage="f32", sigma=SIGMA, beta=BETA)
-    rR, rB = seeded_noise_fields(L, L, L, seed=SEED)
+    from oracle.orc import OracleSim, default_params, noise_fields, num_threads
+    p = default_params(L, model="cg", sigma=SIGMA, beta=BETA)
+    rR, rB = noise_fields(L, L, L, seed=SEED)
     o = OracleSim(p, "ref")
     o.set_fields(rR, rB)
     per = 2  # lattice steps per bench step: a bounded sample of the workload
@@ -142,8 +151,8 @@ def reference_arm(args, ws, rank):
         "impl": "reference", "metric": METRIC, "value": mlups, "unit": "MLUPS", "n_gpus": ws,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "colour-gradient spinodal 128^3, sigma=0.02, beta=0.7, tau=1",
-                   "lattice_steps_per_bench_step": per, "storage": "f32"},
+        "config": workload_config(),
+        "storage": "f32 (the reference's only storage)", "lattice_steps_per_bench_step": per,
         "cpu_baseline": {"value": mlups, "unit": "MLUPS", "cores": num_threads(), "kind": "port",
                          "sample": f"{args.steps} x {per} lattice steps of 128^3 after {args.warmup} x {per} warm-up"},
         "e2e": {"value": mlups, "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -153,11 +162,9 @@ def reference_arm(args, ws, rank):
 
 
 def cpu_baseline_sample():
-    from oracle.orc import OracleSim, num_threads
-    from lbcuda_b200 import make_params
-    from lbcuda_b200.inputs import seeded_noise_fields
-    p = make_params(L, model="cg", storage="f32", sigma=SIGMA, beta=BETA)
-    rR, rB = seeded_noise_fields(L, L, L, seed=SEED)
+    from oracle.orc import OracleSim, default_params, noise_fields, num_threads
+    p = default_params(L, model="cg", sigma=SIGMA, beta=BETA)
+    rR, rB = noise_fields(L, L, L, seed=SEED)
     o = OracleSim(p, "ref")
     o.set_fields(rR, rB)
     o.step(1)
@@ -169,6 +176,26 @@ def cpu_baseline_sample():
     dt = time.perf_counter() - t0
     return {"value": n * L ** 3 / dt / 1e6, "unit": "MLUPS", "cores": num_threads(), "kind": "port",
             "sample": f"{n} lattice steps of the 128^3 workload (about 10 s), FP32, OpenMP"}
+
+
+def bgk_timing(Lb, steps, warm=20):
+    """Plain BGK (D3Q19, FP32, tau = 1, rho = 1 + U(-1e-3, 1e-3) from seed 1, u = 0), one k_bgk launch
+    per lattice step: ms per step, MLUPS and the kernel's HBM fraction at 152 B per cell-step."""
+    from lbcuda_b200 import LBSim, make_params
+    from lbcuda_b200.inputs import seeded_noise_fields
+    rho = seeded_noise_fields(Lb, Lb, Lb, mean=1.0, amp=1e-3, seed=SEED, ncomp=1)[0]
+    s = LBSim(make_params(Lb, model="bgk", storage="f32", tau=1.0))
+    s.set_fields(rho, None)
+    s.step(warm)
+    s.sync()
+    tot, k, nl = s.time_steps(steps, kernel_timing=True)
+    code = s.status()[0]
+    s.close()
+    per_us = k / nl * 1e3
+    gbs = 152 * Lb ** 3 / (per_us * 1e-6) / 1e9
+    return {"box": Lb, "steps": steps, "ms_per_step": tot / steps, "mlups": Lb ** 3 * steps / (tot * 1e-3) / 1e6,
+            "kernel": "k_bgk", "kernel_us": per_us, "achieved_gbs": gbs, "frac": gbs / peaks()[0],
+            "l2_resident": bool(152 * Lb ** 3 < 126e6), "device_error": code}
 
 
 def error_vs_f64(nsteps_list=(100, 1000, 10000), workload="spinodal"):
@@ -478,6 +505,32 @@ def closure_suspension(w, L=256, n=4000, r=3.0, steps=50, warm=10, seed=9):
     return out
 
 
+def summary(line):
+    """The key figures of every workload in a few hundred bytes, printed last."""
+    c = line["colloid_256_1280"]
+    e = line["error_vs_f64"]
+    r3 = lambda v: float(f"{v:.3g}")
+    out = {
+        "spinodal_128_f16sd": {"mlups": r3(line["value"]), "frac": r3(line["roofline"]["frac"]),
+                               "fp16_over_fp32": r3(line["fp16_over_fp32"]),
+                               "u_err_vs_f64_100": r3(e["f16sd"]["after_100"]["u_rel_l2"]),
+                               "u_err_vs_f64_1000": r3(e["f16sd"]["after_1000"]["u_rel_l2"])},
+        "colloid_256_1280_f16sd": {"ms_per_step": r3(c["f16sd"]["ms_per_step"]),
+                                   "frac_at_160B": r3(c["f16sd"]["frac_at_basis"]),
+                                   "over_fp32": r3(c["f32"]["ms_per_step"] / c["f16sd"]["ms_per_step"]),
+                                   "u_err_vs_f64_100": r3(line["colloid_error_vs_f64"]["f16sd"]["after_100"]["u_rel_l2"])},
+        "bgk_f32": {k: {"mlups": r3(v["mlups"]), "frac": r3(v["frac"])} for k, v in line["bgk"].items()},
+        "ensemble_48": {"mlups": r3(line["ensemble_48"]["mlups"]),
+                        "u_err_vs_f32_max": r3(line["ensemble_48"]["u_rel_l2_vs_f32_per_box"]["max"])},
+    }
+    cl = line.get("closure")
+    if cl:
+        out["closure"] = {"R_hi": cl["R_hi"], "rel_l2": r3(cl["error_direct"]["closure"]["rel_l2"]),
+                          "within_5pct": r3(cl["error_direct"]["closure"]["pairs_within_5pct"]),
+                          "cost_ratio": r3(cl["cost_ratio_same_physical_time"])}
+    return out
+
+
 def only_region(args, local):
     import torch
     torch.cuda.set_device(local)
@@ -490,6 +543,13 @@ def only_region(args, local):
         return 0
     if args.only == "closure12":
         print(json.dumps(closure_experiment(R_hi=12, L_hi=96, steps_hi=960)), flush=True)
+        return 0
+    if args.only == "bgk":
+        print(json.dumps({"64": bgk_timing(64, 2000), "256": bgk_timing(256, 200), "512": bgk_timing(512, 40)}),
+              flush=True)
+        return 0
+    if args.only == "bgk-256":
+        print(json.dumps(bgk_timing(256, max(1, args.steps) * 5, warm=args.warmup)), flush=True)
         return 0
     if args.only == "ensemble":
         print(json.dumps(ensemble_timing()), flush=True)
@@ -530,7 +590,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-extras", action="store_true", help="skip the error runs, the colloid case and the CPU baseline")
     ap.add_argument("--only", choices=["f16", "f32", "bf16", "f64", "f16sd", "bf16sd", "colloid-f16", "colloid-f32", "colloid-f16-small", "colloid-f16sd",
-                                       "colloid-f32-small", "ensemble", "closure", "closure12", "variants", "errors"],
+                                       "colloid-f32-small", "ensemble", "closure", "closure12", "variants", "errors", "bgk",
+                                       "bgk-256"],
                     help="profiling aid: run one timed region only and print its timing")
     ap.add_argument("--lb-steps", type=int, default=LB_PER_STEP, help="lattice steps per bench step")
     ap.add_argument("--schedule", type=int, default=2, help="colour-gradient schedule (0, 1, 2)")
@@ -604,34 +665,33 @@ def main():
                 "kernel_us_per_launch": per_launch_ms * 1e3,
                 "minimal_bytes_frac": MINIMAL_BYTES[storage] * cells / (per_launch_ms * 1e-3) / 1e9 / hbm}
 
-    # e2e through the public API with host buffers: upload the fields from
-    # pinned memory, run one bench step of lattice steps, read the fields back
-    pin = lambda shape: torch.empty(shape, dtype=torch.float32, pin_memory=True).numpy()
-    hR, hB = pin((L, L, L)), pin((L, L, L))
-    hR[...] = rR
-    hB[...] = rB
-    s = LBSim(make_params(L, model="cg", storage="f16sd", sigma=SIGMA, beta=BETA))
+    # e2e through the public API with host buffers, one continuous trajectory:
+    # each bench step uploads the full population state from pinned host
+    # memory (lbx_set_pops), runs one bench step of lattice steps and reads
+    # the state back (lbx_get_pops), which the next step uploads again
     import ctypes
+    pin = lambda shape: torch.empty(shape, dtype=torch.float32, pin_memory=True).numpy()
+    s = LBSim(make_params(L, model="cg", storage="f16sd", sigma=SIGMA, beta=BETA))
+    s.set_fields(rR, rB)
+    hR, hB = pin((19, L, L, L)), pin((19, L, L, L))
     fp = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
-    oR, oB, oV, oP = pin((L, L, L)), pin((L, L, L)), pin((L, L, L, 3)), pin((L, L, L))
     lib = s._L
+    if lib.lbx_get_pops(s._h, fp(hR), fp(hB)):
+        raise RuntimeError("lbx_get_pops")
 
     def e2e_step():
-        lib.lbx_set_fields(s._h, fp(hR), fp(hB), 0.0, 0.0, 0.0)
-        lib.lbx_step(s._h, LB_PER_STEP)
-        rc = lib.lbx_get_fields(s._h, fp(oR), fp(oB), fp(oV), fp(oP))
+        rc = lib.lbx_set_pops(s._h, fp(hR), fp(hB))
+        rc = rc or lib.lbx_step(s._h, LB_PER_STEP)
+        rc = rc or lib.lbx_get_pops(s._h, fp(hR), fp(hB))
         if rc:
-            raise RuntimeError(f"lbx_get_fields {rc}")
+            raise RuntimeError(f"e2e step: lbx status {rc}")
 
     for _ in range(args.warmup):
         e2e_step()
     barrier()
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     t0 = time.perf_counter()
-    ev0.record()
     for _ in range(args.steps):
         e2e_step()
-    ev1.record()
     barrier()
     e2e_wall = time.perf_counter() - t0
     e2e_ms = maxr(e2e_wall * 1e3)
@@ -642,6 +702,7 @@ def main():
     if rank == 0 and not args.no_extras:
         extras["error_vs_f64"] = error_vs_f64()
         extras["error_vs_f64_droplet"] = error_vs_f64((100, 1000), workload="droplet")
+        extras["bgk"] = {"64": bgk_timing(64, 2000), "256": bgk_timing(256, 200), "512": bgk_timing(512, 40)}
         extras["colloid_256_1280"] = {st: colloid_timing(st) for st in ("f16sd", "f16", "f32")}
         extras["colloid_error_vs_f64"] = colloid_error_vs_f64()
         extras["ensemble_48"] = ensemble_timing()
@@ -655,28 +716,29 @@ def main():
             "metric": METRIC, "value": mlups16, "unit": "MLUPS", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": tot16 / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "colour-gradient spinodal 128^3 periodic, rho=0.5+U(-0.01,0.01) seed 1, "
-                                   "tau=1, sigma=0.02, beta=0.7",
-                       "lattice_steps_per_bench_step": LB_PER_STEP,
-                       "storage": "f16 sum / difference pairs (f_R + f_B - w*1, f_R - f_B), FP32 arithmetic",
-                       "cells": cells, "l2": "inputs larger than L2 (2 x 160 MB population buffers)",
-                       "parallelism": "replicas" if ws > 1 else "single"},
+            "config": workload_config(),
+            "storage": "f16 sum / difference pairs (f_R + f_B - w*1, f_R - f_B), FP32 arithmetic",
+            "lattice_steps_per_bench_step": LB_PER_STEP,
+            "parallelism": "replicas" if ws > 1 else "single",
             "roofline": roofline("f16sd", k16, n16),
             "fp32_storage": {"value": mlups32, "unit": "MLUPS", "ms_per_step": tot32 / args.steps,
                              "roofline": roofline("f32", k32, n32)},
             "fp16_over_fp32": mlups16 / mlups32,
             "f16_component_pairs": {"value": mlupsrb, "unit": "MLUPS", "ms_per_step": totrb / args.steps,
-                                    "storage": "f16 (R - w rho0R, B - w rho0B) pairs, the sphere path's storage",
+                                    "storage": "f16 (R - w rho0R, B - w rho0B) pairs",
                                     "roofline": roofline("f16", krb, nrb), "over_fp32": mlupsrb / mlups32},
             "clocks": clocks,
-            "e2e": {"value": e2e_mlups, "unit": "MLUPS", "h2d_bytes_per_step": 2 * 4 * cells,
-                    "d2h_bytes_per_step": 6 * 4 * cells, "ms_per_step": e2e_ms / args.steps,
-                    "timing": "host wall clock around the synchronous C-ABI calls, max over ranks",
+            "e2e": {"value": e2e_mlups, "unit": "MLUPS", "h2d_bytes_per_step": 2 * 19 * 4 * cells,
+                    "d2h_bytes_per_step": 2 * 19 * 4 * cells, "ms_per_step": e2e_ms / args.steps,
+                    "timing": "host wall clock around the synchronous C-ABI calls (lbx_set_pops, lbx_step, "
+                              "lbx_get_pops of the full FP32 state, one continuous trajectory), max over ranks",
                     "gpu_launches_per_step": LB_PER_STEP + 2},
             "gpu_launches": n16,
             "device_errors": [code16, code32, coderb],
         }
         line.update(extras)
+        if extras:
+            line["summary"] = summary(line)
         print(json.dumps(line), flush=True)
     if pg is not None:
         pg.destroy_process_group()

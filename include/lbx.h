@@ -208,6 +208,18 @@ int lbx_get_fields_f64(void* ctx, double* rhoR, double* rhoB, double* vel, doubl
 int lbx_get_pops(void* ctx, float* popsR, float* popsB);
 /* Cell flags of the last step (myfluid_d(:,:,:,flip)), int8 nx*ny*nz. */
 int lbx_get_flags(void* ctx, int8_t* flags);
+/* The boundary links of the particle bounce-back at the flags lbx_get_flags
+ * returns (those of the last step; before the first step, those of
+ * lbx_set_particles), at the sphere positions that stamped them: every
+ * (sphere, surface cell, direction) for which node_to_particle_bounce_back_bc2
+ * (kernels_fluid_PART.CUF:1874-2113, pair loop 1929-1941) exchanges momentum:
+ * a spherelist cell within the sphere's reach (d^2 < rmax^2, on the sphere's
+ * tile list) and an opposite pair (2i-1, 2i) with exactly one fluid end.
+ * cell = x + nx*(y + ny*z) of the surface cell, dir = the direction (1..18,
+ * reference order) from it towards the fluid end, sphere = 0-based index.
+ * Sorted by (sphere, cell, dir).  *n receives the total; at most cap entries
+ * are written (cap = 0 queries the count).  LBX_ERR_STATE without spheres. */
+int lbx_get_links(void* ctx, int32_t* cell, int8_t* dir, int32_t* sphere, int64_t cap, int64_t* n);
 /* FP64 global sums: mass[2] (red, blue) and momentum[3], over fluid cells. */
 int lbx_get_sums(void* ctx, double* mass, double* momentum);
 

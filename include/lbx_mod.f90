@@ -95,6 +95,14 @@ module lbx_mod
       type(c_ptr), value :: ctx
       integer(c_int8_t), intent(out) :: flags(*)
     end function
+    integer(c_int) function lbx_get_links(ctx, cell, dir, sphere, cap, n) bind(C, name="lbx_get_links")
+      import :: c_int, c_ptr, c_int8_t, c_int32_t, c_int64_t
+      type(c_ptr), value :: ctx
+      integer(c_int32_t), intent(out) :: cell(*), sphere(*)
+      integer(c_int8_t), intent(out) :: dir(*)
+      integer(c_int64_t), value :: cap
+      integer(c_int64_t), intent(out) :: n
+    end function
     integer(c_int) function lbx_get_particles(ctx, xyz, vel, omega, q, force, torque) bind(C, name="lbx_get_particles")
       import :: c_int, c_ptr, c_double
       type(c_ptr), value :: ctx

@@ -29,8 +29,10 @@ NVCC_FLAGS = [
 ]
 # The single-pass fluid kernels write every fused multiply-add explicitly and
 # are compiled without contraction, so each kernel that inlines them (one box,
-# particle box, ensemble) performs the same roundings.
-FILE_FLAGS = {"lbx_fused.cu": ["-fmad=false"]}
+# particle box, ensemble) performs the same roundings.  The BGK and two-pass
+# kernels follow the reference's expression order and are compiled without
+# contraction as well, so they round as the reference's FP32 arithmetic does.
+FILE_FLAGS = {"lbx_fused.cu": ["-fmad=false"], "lbx_fluid.cu": ["-fmad=false"]}
 
 
 def nvcc():

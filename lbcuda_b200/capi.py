@@ -75,6 +75,7 @@ SIGNATURES = {
     "lbx_get_pops": (C.c_int, [_P, _F, _F]),
     "lbx_get_flags": (C.c_int, [_P, _I8]),
     "lbx_get_sums": (C.c_int, [_P, _D, _D]),
+    "lbx_get_links": (C.c_int, [_P, _I32, _I8, _I32, C.c_int64, _I64]),
     "lbx_set_particles": (C.c_int, [_P, C.c_int32, _D, _D, _D, _D]),
     "lbx_get_particles": (C.c_int, [_P, _D, _D, _D, _D, _D, _D]),
     "lbx_closure_init": (C.c_int, [_F, C.c_int32]),

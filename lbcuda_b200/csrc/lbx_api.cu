@@ -34,6 +34,7 @@ int part_pairs(Ctx& c);
 int part_integrate(Ctx& c);
 int particles_set_closure(Ctx& c, const float* w);
 int particles_flags_slot(const Ctx& c);
+int particles_links(Ctx& c, int32_t* cell, int8_t* dir, int32_t* sph, int64_t cap, int64_t* n);
 int particles_active(const Ctx& c);
 }  // namespace lbx
 
@@ -341,6 +342,14 @@ int lbx_get_flags(void* ctx, int8_t* flags) {
   if (!c || !flags) return LBX_ERR_ARG;
   int rc = cuda_rc(cudaMemcpyAsync(flags, c->flags[lbx::particles_flags_slot(*c)], size_t(c->n),
                                    cudaMemcpyDeviceToHost, c->stream));
+  if (!rc) rc = sync_status(*c);
+  return rc;
+}
+
+int lbx_get_links(void* ctx, int32_t* cell, int8_t* dir, int32_t* sphere, int64_t cap, int64_t* n) {
+  Ctx* c = as_ctx(ctx);
+  if (!c) return LBX_ERR_ARG;
+  int rc = lbx::particles_links(*c, cell, dir, sphere, cap, n);
   if (!rc) rc = sync_status(*c);
   return rc;
 }

@@ -29,6 +29,7 @@
 #include "lbx_device.cuh"
 #include "lbx_closure.h"
 
+#include <algorithm>
 #include <cmath>
 #include <vector>
 
@@ -958,6 +959,47 @@ __global__ void __launch_bounds__(256) k_bb(PDev P, const double* __restrict__ p
     for (int d = 0; d < 6; ++d) acc[size_t(a) * AS + d] += out[d];
 }
 
+// The crossing links of the bounce-back: for every surface cell within a
+// sphere's reach (the node -> particle predicates of k_bb: flag spherelist,
+// d^2 < sphereMax, the tile-list coverage), each opposite pair with exactly
+// one fluid end, as (sphere, surface cell, direction from the cell towards
+// its fluid end).  This is the link set node_to_particle_bounce_back_bc2
+// visits (kernels_fluid_PART.CUF:1929-1941, its DEBUG_N2P record); a
+// readback kernel, not part of the step.  Entries past `cap` are counted,
+// not written.
+__global__ void __launch_bounds__(256) k_links(PDev P, const double* __restrict__ pos, Geom g,
+                                               const int8_t* __restrict__ fnew, unsigned long long* count,
+                                               long long cap, int* lcell, int8_t* ldir, int* lsph) {
+  const int a = blockIdx.x;
+  const double* pc = pos + size_t(a) * PS;
+  const int c[3] = {nint_idx(pc[0], g.nx), nint_idx(pc[1], g.ny), nint_idx(pc[2], g.nz)};
+  const int nn3[3] = {g.nx, g.ny, g.nz};
+  for (int t = threadIdx.x; t < P.n_bb; t += blockDim.x) {
+    int dx, dy, dz, tv, i1, j1, k1;
+    unpack_off(P.offs_bb[t], dx, dy, dz, tv);
+    if (dx * dx + dy * dy + dz * dz >= P.sphereMax) continue;
+    if (!offset_cell(P, g, c, dx, dy, dz, i1, j1, k1)) continue;
+    const int cell = cell0(g, i1, j1, k1);
+    if (fnew[cell] != LBX_FLUID_SPHERELIST) continue;
+    const int x0 = i1 - 1, y0 = j1 - 1, z0 = k1 - 1;
+    if (P.exact_tiles && !tile_covered(pc, nn3, P.rdim, x0 / TILEX + 1, y0 / TILEY + 1, z0 / TILEZ + 1)) continue;
+    Nbr b;
+    make_nbr(g, x0, y0, z0, b);
+    for (int it = 0; it < 9; ++it) {
+      const int lo = 2 * it + 1, hi = 2 * it + 2;
+      const bool fi = fnew[at(b, ex(lo), ey(lo), ez(lo))] == LBX_FLUID_FLUID;
+      const bool fo = fnew[at(b, ex(hi), ey(hi), ez(hi))] == LBX_FLUID_FLUID;
+      if (fi == fo) continue;
+      const unsigned long long k = atomicAdd(count, 1ull);
+      if ((long long)k < cap) {
+        lcell[k] = cell;
+        ldir[k] = int8_t(fo ? hi : lo);
+        lsph[k] = a;
+      }
+    }
+  }
+}
+
 // inter_force_particles / addHertzian: all pairs; one warp per sphere, the
 // lanes take every 32nd partner and the warp sums their shares in a fixed
 // order.  With lubrication on, the analytic squeeze force is added as well
@@ -1763,6 +1805,73 @@ int particles_set_closure(Ctx& c, const float* h_w) {
   }
   s->closure_ready = 1;
   return cudaStreamSynchronize(c.stream) == cudaSuccess ? 0 : LBX_ERR_CUDA;
+}
+
+// The bounce-back links of the flags lbx_get_flags reports (those of the last
+// step, or of lbx_set_particles before the first step) at the positions that
+// stamped them; sorted by (sphere, cell, direction).
+int particles_links(Ctx& c, int32_t* h_cell, int8_t* h_dir, int32_t* h_sph, int64_t cap, int64_t* h_n) {
+  ParticleState* s = c.part;
+  if (!s || !s->active) return LBX_ERR_STATE;
+  if (!h_n || cap < 0 || (cap > 0 && (!h_cell || !h_dir || !h_sph))) return LBX_ERR_ARG;
+  // after a step pos[pcur] holds the new positions and pos[1 - pcur] those
+  // of the step; lbx_set_particles wrote both slots
+  const double* pos = s->pos[1 - s->pcur];
+  const int8_t* fl = c.flags[s->flags_last];
+  PDev P = pdev(c);
+  Geom g = geom(c);
+  unsigned long long* d_count = nullptr;
+  if (cudaMalloc(&d_count, sizeof(*d_count)) != cudaSuccess) return LBX_ERR_ALLOC;
+  cudaMemsetAsync(d_count, 0, sizeof(*d_count), c.stream);
+  k_links<<<s->np, 256, 0, c.stream>>>(P, pos, g, fl, d_count, 0, nullptr, nullptr, nullptr);
+  unsigned long long total = 0;
+  cudaMemcpyAsync(&total, d_count, sizeof(total), cudaMemcpyDeviceToHost, c.stream);
+  if (cudaStreamSynchronize(c.stream) != cudaSuccess) {
+    cudaFree(d_count);
+    return LBX_ERR_CUDA;
+  }
+  *h_n = int64_t(total);
+  int rc = 0;
+  if (cap > 0 && total > 0) {
+    const size_t nt = size_t(total);
+    int *d_cell = nullptr, *d_sph = nullptr;
+    int8_t* d_dir = nullptr;
+    if (cudaMalloc(&d_cell, nt * 4) != cudaSuccess || cudaMalloc(&d_sph, nt * 4) != cudaSuccess ||
+        cudaMalloc(&d_dir, nt) != cudaSuccess) {
+      rc = LBX_ERR_ALLOC;
+    } else {
+      cudaMemsetAsync(d_count, 0, sizeof(*d_count), c.stream);
+      k_links<<<s->np, 256, 0, c.stream>>>(P, pos, g, fl, d_count, (long long)nt, d_cell, d_dir, d_sph);
+      std::vector<int> cell(nt), sph(nt);
+      std::vector<int8_t> dir(nt);
+      cudaMemcpyAsync(cell.data(), d_cell, nt * 4, cudaMemcpyDeviceToHost, c.stream);
+      cudaMemcpyAsync(sph.data(), d_sph, nt * 4, cudaMemcpyDeviceToHost, c.stream);
+      cudaMemcpyAsync(dir.data(), d_dir, nt, cudaMemcpyDeviceToHost, c.stream);
+      if (cudaStreamSynchronize(c.stream) != cudaSuccess) {
+        rc = LBX_ERR_CUDA;
+      } else {
+        std::vector<size_t> ord(nt);
+        for (size_t i = 0; i < nt; ++i) ord[i] = i;
+        std::sort(ord.begin(), ord.end(), [&](size_t x, size_t y) {
+          if (sph[x] != sph[y]) return sph[x] < sph[y];
+          if (cell[x] != cell[y]) return cell[x] < cell[y];
+          return dir[x] < dir[y];
+        });
+        const size_t m = std::min(nt, size_t(cap));
+        for (size_t i = 0; i < m; ++i) {
+          h_cell[i] = cell[ord[i]];
+          h_dir[i] = dir[ord[i]];
+          h_sph[i] = sph[ord[i]];
+        }
+      }
+    }
+    if (d_cell) cudaFree(d_cell);
+    if (d_sph) cudaFree(d_sph);
+    if (d_dir) cudaFree(d_dir);
+  }
+  cudaFree(d_count);
+  if (!rc) rc = launch_status();
+  return rc;
 }
 
 int particles_flags_slot(const Ctx& c) { return c.part ? c.part->flags_last : c.fcur; }

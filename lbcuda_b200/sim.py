@@ -161,6 +161,19 @@ class LBSim:
         check(self._L.lbx_get_flags(self._h, _fptr(f, C.c_int8)), "lbx_get_flags")
         return f
 
+    def get_links(self):
+        """Boundary links of the last step's bounce-back: int32 (n, 3) rows of
+        (sphere, cell, direction), sorted (lbx_get_links)."""
+        n = C.c_int64()
+        check(self._L.lbx_get_links(self._h, None, None, None, 0, C.byref(n)), "lbx_get_links")
+        m = n.value
+        cell = np.empty(max(m, 1), np.int32)
+        sph = np.empty(max(m, 1), np.int32)
+        d = np.empty(max(m, 1), np.int8)
+        check(self._L.lbx_get_links(self._h, _fptr(cell, C.c_int32), _fptr(d, C.c_int8), _fptr(sph, C.c_int32),
+                                    m, C.byref(n)), "lbx_get_links")
+        return np.stack([sph[:m], cell[:m], d[:m].astype(np.int32)], axis=1)
+
     def get_sums(self):
         m = np.zeros(2, np.float64)
         mom = np.zeros(3, np.float64)

@@ -33,6 +33,7 @@
 #include <cstring>
 #include <vector>
 #include <algorithm>
+#include <array>
 #ifdef _OPENMP
 #include <omp.h>
 #endif
@@ -844,6 +845,23 @@ class Oracle {
     v[2] = ps(b, a, 5) + c[2];
   }
 
+  /* links visited by the last step's n2p, one list per OpenMP thread */
+  bool record_links = false;
+  std::vector<std::vector<std::array<int64_t, 3>>> link_rec;
+  void clear_links() {
+#ifdef _OPENMP
+    link_rec.assign(size_t(omp_get_max_threads()), {});
+#else
+    link_rec.assign(1, {});
+#endif
+  }
+  std::vector<std::array<int64_t, 3>> links_sorted() const {
+    std::vector<std::array<int64_t, 3>> all;
+    for (const auto& v : link_rec) all.insert(all.end(), v.begin(), v.end());
+    std::sort(all.begin(), all.end());
+    return all;
+  }
+
   /* node_to_particle_bounce_back_bc2, kernels_fluid_PART.CUF:1874-2113 */
   void n2p(int b, int a, int i, int j, int k) {
     P rv[3] = {0, 0, 0}, ol[3] = {0, 0, 0};
@@ -862,6 +880,17 @@ class Oracle {
         int lf = side ? lo : hi;            /* direction of the population read at xf */
         int lr = side ? hi : lo;            /* direction towards xf */
         if (!(flags[b][xf] == LBX_FLUID_FLUID && flags[b][xs] != LBX_FLUID_FLUID)) continue;
+        if (record_links) {
+          /* the link this pair crosses: (sphere, surface cell, direction
+           * towards the fluid end), the DEBUG_N2P record of the reference */
+          const int64_t cell = (i - 1) + int64_t(nx) * ((j - 1) + int64_t(ny) * (k - 1));
+#ifdef _OPENMP
+          auto& out = link_rec[size_t(omp_get_thread_num())];
+#else
+          auto& out = link_rec[0];
+#endif
+          out.push_back({int64_t(a), cell, int64_t(lr)});
+        }
         P v[3] = {ps(b, a, 3), ps(b, a, 4), ps(b, a, 5)};
         P rt[3] = {0, 0, 0};
         if (lrotate) {
@@ -1158,6 +1187,7 @@ class Oracle {
   /* ---- one step with particles, main.CUF:130-241 --------------------------- */
   void do_step_particles() {
     step += 1;
+    clear_links();
     const int b = flip;
     init_isfluid(b);
     for_cells_with_tile_atoms([&](int a, int i, int j, int k) {
@@ -1404,6 +1434,45 @@ int orc_template(void* h, int* rmax, int8_t* out) {
   return dispatch(h, [&](auto& o) {
     if (rmax) *rmax = o.rmax;
     if (out) for (size_t i = 0; i < o.issub.size(); ++i) out[i] = o.issub[i];
+    return 0;
+  });
+}
+/* the reference defaults of lbx_params (dimensions_m.CUF:50-99): the
+ * compile-time parameters of the reference, restated for the oracle's own
+ * callers */
+void orc_default_params(lbx_params* p, int32_t nx, int32_t ny, int32_t nz) {
+  std::memset(p, 0, sizeof(*p));
+  p->nx = nx; p->ny = ny; p->nz = nz;
+  p->model = LBX_MODEL_CG;
+  p->storage = LBX_STORE_F32;
+  p->wetting = LBX_WET_JANUS;
+  p->tau = 1.0f;
+  p->tauR = 1.0f; p->tauB = 1.0f;       /* dimensions_m.CUF:98-99 */
+  p->sigma = 0.1f; p->beta = 0.999f;    /* dimensions_m.CUF:50 */
+  p->rho0R = 0.5f; p->rho0B = 0.5f;
+  p->radius = 5.5f;                     /* dimensions_m.CUF:59 */
+  p->rmass = 1.0f / 1500.0f;            /* dimensions_m.CUF:60 */
+  p->hz_k = 10.0f; p->hz_rmin = 10.5f; p->hz_rcap = 9.0f;               /* :77-80 */
+  p->lubric_k = 10.0f; p->lubric_rmin = 10.0f; p->lubric_rcap = 9.0f;  /* :81-84 */
+  p->closure_gap_min = 0.05f; p->closure_gap_max = 1.5f; p->closure_vmax = 1.0e-3f;
+  p->exact_tiles = 1;
+  p->densR = 1.0f; p->densB = 1.0f;     /* noDIFFDENS, main.CUF:1065-1066 */
+}
+
+/* the boundary links of the last step's bounce-back (record_links on), as
+ * (sphere, cell, direction) sorted; *n = total, at most cap written */
+int orc_record_links(void* h, int on) {
+  return dispatch(h, [&](auto& o) { o.record_links = on != 0; if (on) o.clear_links(); return 0; });
+}
+int orc_get_links(void* h, int32_t* cell, int8_t* dir, int32_t* sph, int64_t cap, int64_t* n) {
+  return dispatch(h, [&](auto& o) {
+    auto all = o.links_sorted();
+    *n = int64_t(all.size());
+    for (size_t i = 0; i < all.size() && int64_t(i) < cap; ++i) {
+      sph[i] = int32_t(all[i][0]);
+      cell[i] = int32_t(all[i][1]);
+      dir[i] = int8_t(all[i][2]);
+    }
     return 0;
   });
 }

@@ -9,8 +9,6 @@ import os
 
 import numpy as np
 
-from lbcuda_b200.capi import LbxParams
-
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB = os.path.join(_HERE, "liblbx_oracle.so")
 Q = 19
@@ -27,7 +25,8 @@ def lib():
         L = C.CDLL(_LIB)
         P = C.c_void_p
         L.orc_create.restype = P
-        L.orc_create.argtypes = [C.POINTER(LbxParams), C.c_int]
+        L.orc_create.argtypes = [C.POINTER(Params), C.c_int]
+        L.orc_default_params.argtypes = [C.POINTER(Params), C.c_int32, C.c_int32, C.c_int32]
         L.orc_destroy.argtypes = [P]
         L.orc_set_fields.argtypes = [P, C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_float, C.c_float, C.c_float]
         L.orc_set_pops.argtypes = [P, C.POINTER(C.c_float), C.POINTER(C.c_float)]
@@ -43,8 +42,73 @@ def lib():
         L.orc_get_accumulators.argtypes = [P, D, D, D, D]
         L.orc_get_rho.argtypes = [P, D, D]
         L.orc_template.argtypes = [P, C.POINTER(C.c_int), C.POINTER(C.c_int8)]
+        L.orc_record_links.argtypes = [P, C.c_int]
+        L.orc_get_links.argtypes = [P, C.POINTER(C.c_int32), C.POINTER(C.c_int8), C.POINTER(C.c_int32), C.c_int64,
+                                    C.POINTER(C.c_int64)]
         _lib = L
     return _lib
+
+
+class Params(C.Structure):
+    """lbx_params of include/lbx.h, mirrored here so that the oracle needs
+    nothing of the product package (a CPU test checks both mirrors agree)."""
+    _fields_ = [
+        ("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32),
+        ("model", C.c_int32), ("storage", C.c_int32), ("wetting", C.c_int32),
+        ("lrotate", C.c_int32), ("max_particles", C.c_int32),
+        ("tau", C.c_float), ("tauR", C.c_float), ("tauB", C.c_float),
+        ("sigma", C.c_float), ("beta", C.c_float),
+        ("rho0R", C.c_float), ("rho0B", C.c_float),
+        ("radius", C.c_float), ("rmass", C.c_float), ("max_vel", C.c_float),
+        ("ext_force", C.c_float * 3), ("ext_torque", C.c_float * 3),
+        ("hz_k", C.c_float), ("hz_rmin", C.c_float), ("hz_rcap", C.c_float),
+        ("lubrication", C.c_int32),
+        ("lubric_k", C.c_float), ("lubric_rmin", C.c_float), ("lubric_rcap", C.c_float),
+        ("kinematic", C.c_int32), ("closure", C.c_int32),
+        ("closure_gap_min", C.c_float), ("closure_gap_max", C.c_float), ("closure_vmax", C.c_float),
+        ("exact_tiles", C.c_int32), ("densR", C.c_float), ("densB", C.c_float),
+    ]
+
+
+MODEL = {"bgk": 0, "cg": 1, "cg-diffdens": 2, "cg-d3q27": 3, "cg-diffdens-d3q27": 4}
+WETTING = {"janus": 0, "neutral": 1}
+
+
+def default_params(nx, ny=None, nz=None, model="cg", **kw):
+    """The reference defaults (dimensions_m.CUF:50-99, restated by orc_default_params) with kw applied."""
+    ny = nx if ny is None else ny
+    nz = nx if nz is None else nz
+    p = Params()
+    lib().orc_default_params(C.byref(p), nx, ny, nz)
+    p.model = MODEL[model] if isinstance(model, str) else int(model)
+    for k, v in kw.items():
+        if k == "wetting" and isinstance(v, str):
+            v = WETTING[v]
+        if k in ("ext_force", "ext_torque"):
+            getattr(p, k)[:] = list(v)
+            continue
+        if not hasattr(p, k):
+            raise KeyError(k)
+        setattr(p, k, v)
+    return p
+
+
+def noise_fields(nx, ny, nz, mean=0.5, amp=0.01, seed=0, ncomp=2):
+    """rho_k = mean + U(-amp, amp) per cell and component from numpy's PCG64
+    with the given seed: the same fields the product's input helpers make."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    return [(np.float32(mean) + rng.uniform(-amp, amp, size=(nz, ny, nx))).astype(np.float32) for _ in range(ncomp)]
+
+
+def _as_params(p):
+    """Any structure with lbx_params' layout, as this module's Params."""
+    if isinstance(p, Params):
+        return p
+    q = Params()
+    if C.sizeof(p) != C.sizeof(q):
+        raise TypeError("not an lbx_params layout")
+    C.memmove(C.byref(q), C.byref(p), C.sizeof(q))
+    return q
 
 
 def num_threads():
@@ -59,6 +123,7 @@ class OracleSim:
     """Same surface as lbcuda_b200.LBSim, computed by the CPU restatement."""
 
     def __init__(self, params, mode="ref"):
+        params = _as_params(params)
         self.params = params
         self.nx, self.ny, self.nz = params.nx, params.ny, params.nz
         self.ncomp = 1 if params.model == 0 else 2
@@ -140,6 +205,21 @@ class OracleSim:
         rR, rB = np.empty(self.shape), np.empty(self.shape)
         self._L.orc_get_rho(self._h, _p(rR, C.c_double), _p(rB, C.c_double))
         return rR, rB
+
+    def record_links(self, on=True):
+        """Record the bounce-back links of each particle step (off by default)."""
+        self._L.orc_record_links(self._h, 1 if on else 0)
+
+    def get_links(self):
+        """Links of the last particle step: int32 (n, 3) rows (sphere, cell, direction), sorted."""
+        n = C.c_int64()
+        self._L.orc_get_links(self._h, None, None, None, 0, C.byref(n))
+        m = n.value
+        cell = np.empty(max(m, 1), np.int32)
+        sph = np.empty(max(m, 1), np.int32)
+        d = np.empty(max(m, 1), np.int8)
+        self._L.orc_get_links(self._h, _p(cell, C.c_int32), _p(d, C.c_int8), _p(sph, C.c_int32), m, C.byref(n))
+        return np.stack([sph[:m], cell[:m], d[:m].astype(np.int32)], axis=1)
 
     def template(self):
         rm = C.c_int()

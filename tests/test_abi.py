@@ -44,3 +44,5 @@ def test_invalid_arguments_rejected_without_gpu():
                  "lbx_partbb", "lbx_partbb_p2n", "lbx_partbb_p2n2", "lbx_inter_force_particles",
                  "lbx_time_step_force_particles"):
         assert getattr(L, name)(None) == -2, name
+    n = ctypes.c_int64(-1)
+    assert L.lbx_get_links(None, None, None, None, 0, ctypes.byref(n)) == -2

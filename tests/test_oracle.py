@@ -4,6 +4,7 @@ PARITY UNPINNED: the reference ships no golden outputs and cannot be built
 here (CUDA Fortran), so the oracle is checked against analytic invariants of
 the method and against identities between its own code paths.
 """
+import ctypes
 import os
 
 import numpy as np
@@ -136,3 +137,18 @@ def test_initial_fields_shapes():
         assert np.allclose(rR + rB, 1.0, atol=1e-6)
     rR, _ = inputs.initial_fields(1, 32, 32, 32)
     assert rR[16, 16, 16] == 1.0 and rR[0, 0, 0] == 0.0  # droplet radius glz/8 at the centre
+
+
+def test_oracle_binding_is_independent_of_the_product():
+    """The oracle's params mirror, defaults and noise fields equal the product's,
+    so the CPU arm of the benchmark needs nothing from lbcuda_b200."""
+    from lbcuda_b200 import capi, make_params
+    from lbcuda_b200.inputs import seeded_noise_fields
+    from oracle import orc
+    assert [f[0] for f in orc.Params._fields_] == [f[0] for f in capi.LbxParams._fields_]
+    assert ctypes.sizeof(orc.Params) == ctypes.sizeof(capi.LbxParams)
+    a = orc.default_params(24, 16, 8, model="bgk", tau=0.8, wetting="neutral")
+    b = make_params(24, 16, 8, model="bgk", tau=0.8, wetting="neutral")
+    assert bytes(a) == bytes(b)
+    for x, y in zip(orc.noise_fields(8, 6, 4, seed=3), seeded_noise_fields(8, 6, 4, seed=3)):
+        assert np.array_equal(x, y)

@@ -90,3 +90,50 @@ def test_frozen_geometry_sphere_keeps_its_centre():
     assert np.array_equal(d["x"][0], [12.2, 16.1, 16.3])
     assert np.array_equal(d["v"][0], [0.02, 0.0, 0.0])
     assert d["force"][0, 0] < 0
+
+
+# D3Q19 directions 1..18 in the reference order (dimensions_m.CUF:211-218)
+E19 = [(1, 0, 0), (-1, 0, 0), (0, 1, 0), (0, -1, 0), (0, 0, 1), (0, 0, -1), (1, 1, 0), (-1, -1, 0), (-1, 1, 0),
+       (1, -1, 0), (1, 0, 1), (-1, 0, -1), (-1, 0, 1), (1, 0, -1), (0, 1, 1), (0, -1, -1), (0, -1, 1), (0, 1, -1)]
+
+
+def independent_links(flags, owner_of):
+    """The bounce-back link set restated from the flags with numpy: every
+    surface cell and opposite pair (2i-1, 2i) with exactly one fluid end,
+    as (sphere, cell, direction towards the fluid end)."""
+    nz, ny, nx = flags.shape
+    fluid = flags == 1
+    rows = []
+    zz, yy, xx = np.nonzero(flags == 2)
+    for z, y, x in zip(zz, yy, xx):
+        cell = x + nx * (y + ny * z)
+        for it in range(9):
+            lo, hi = 2 * it + 1, 2 * it + 2
+            (ax, ay, az), (bx, by, bz) = E19[lo - 1], E19[hi - 1]
+            fi = fluid[(z + az) % nz, (y + ay) % ny, (x + ax) % nx]
+            fo = fluid[(z + bz) % nz, (y + by) % ny, (x + bx) % nx]
+            if fi != fo:
+                rows.append((owner_of(x, y, z), cell, hi if fo else lo))
+    return np.array(sorted(rows), np.int64).reshape(-1, 3)
+
+
+def test_oracle_links_match_independent_restatement():
+    """Two spheres apart (one across the periodic edge): the links the oracle's
+    node_to_particle_bounce_back_bc2 visits in a step are exactly the set
+    restated from its flags."""
+    n = 32
+    x = np.array([[9.3, 10.6, 12.2], [24.7, 22.1, 1.4]])
+    o = _sim(n, x, np.zeros((2, 3)), radius=5.5)
+    o.record_links(True)
+    assert o.step(1) == 0
+    f = o.get_flags()
+
+    def owner_of(cx, cy, cz):
+        d = np.array([cx + 1, cy + 1, cz + 1], float) - x        # 1-based cell coordinates
+        d -= n * np.round(d / n)
+        return int(np.argmin((d * d).sum(axis=1)))
+
+    ind = independent_links(f, owner_of)
+    got = o.get_links().astype(np.int64)
+    assert len(got) > 2 * 400
+    assert np.array_equal(got, ind)
