@@ -9,6 +9,13 @@
 //     --radius r --rmass m --neutral (wetting) --xyz file
 //     --out dir                     VTI/VTK output directory (default output)
 //     --seed s                      seed of initType 6
+//     --restart-out dir             after the last step, write the restart
+//                                   files of initType 4 (rhoR/rhoB.init.bin,
+//                                   popR/popB.NNNNNN.init.bin) into dir
+//
+// initType 3 reads rhoR.init.bin / rhoB.init.bin and initType 4 also the
+// per-direction population files popR/popB.NNNNNN.init.bin (read_and_setPops,
+// main.CUF:2444-2529) from the working directory.
 //
 // input.dat is read with the rules of readParameters (main.CUF:409-496);
 // input.xyz with those of read_input_atom (main.CUF:1230-1350).  Every
@@ -200,6 +207,60 @@ bool read_fortran_field(const char* path, int nx, int ny, int nz, float* out) {
   return bool(in) && m0 == m1;
 }
 
+// Fortran unformatted sequential record pair of the *.init.bin files: a
+// header record (1, nx, 1, ny, 1, nz) and the nx*ny*nz float32 block
+bool write_fortran_field(const std::string& path, int nx, int ny, int nz, const float* a) {
+  FILE* f = std::fopen(path.c_str(), "wb");
+  if (!f) return false;
+  const int32_t n0 = 24, hdr[6] = {1, nx, 1, ny, 1, nz};
+  const int32_t m = int32_t(size_t(nx) * ny * nz * 4);
+  bool ok = std::fwrite(&n0, 4, 1, f) == 1 && std::fwrite(hdr, 4, 6, f) == 6 && std::fwrite(&n0, 4, 1, f) == 1 &&
+            std::fwrite(&m, 4, 1, f) == 1 && std::fwrite(a, 4, size_t(nx) * ny * nz, f) == size_t(nx) * ny * nz &&
+            std::fwrite(&m, 4, 1, f) == 1;
+  return std::fclose(f) == 0 && ok;
+}
+
+// write_fmtnumb (write_output.f90:858-875): six digits, zero-padded
+std::string fmtnumb(int l) {
+  char b[16];
+  std::snprintf(b, sizeof b, "%06d", l);
+  return b;
+}
+
+// read_and_setPops (main.CUF:2489-2529): q files popR.NNNNNN.init.bin and
+// popB.NNNNNN.init.bin (direction l = 0 .. q-1) in directory dir, each one
+// direction's nx*ny*nz populations; pR, pB get q planes of nx*ny*nz
+bool read_init_pops(const std::string& dir, int q, int nx, int ny, int nz, std::vector<float>& pR,
+                    std::vector<float>& pB) {
+  const size_t n = size_t(nx) * ny * nz;
+  pR.assign(size_t(q) * n, 0.f);
+  pB.assign(size_t(q) * n, 0.f);
+  for (int l = 0; l < q; ++l) {
+    const std::string fr = dir + "/popR." + fmtnumb(l) + ".init.bin", fb = dir + "/popB." + fmtnumb(l) + ".init.bin";
+    if (!read_fortran_field(fr.c_str(), nx, ny, nz, pR.data() + size_t(l) * n) ||
+        !read_fortran_field(fb.c_str(), nx, ny, nz, pB.data() + size_t(l) * n)) {
+      std::fprintf(stderr, "Wrong start pops file %s / %s\n", fr.c_str(), fb.c_str());
+      return false;
+    }
+  }
+  return true;
+}
+
+// the restart files of initType 4 (and 3): rhoR/rhoB.init.bin and the
+// population files read_and_setPops reads, from the current state
+bool write_restart(void* ctx, const std::string& dir, int q, int nx, int ny, int nz) {
+  const size_t n = size_t(nx) * ny * nz;
+  std::vector<float> pR(size_t(q) * n), pB(size_t(q) * n), R(n), B(n);
+  if (lbx_get_pops(ctx, pR.data(), pB.data()) || lbx_get_fields(ctx, R.data(), B.data(), nullptr, nullptr))
+    return false;
+  bool ok = write_fortran_field(dir + "/rhoR.init.bin", nx, ny, nz, R.data()) &&
+            write_fortran_field(dir + "/rhoB.init.bin", nx, ny, nz, B.data());
+  for (int l = 0; ok && l < q; ++l)
+    ok = write_fortran_field(dir + "/popR." + fmtnumb(l) + ".init.bin", nx, ny, nz, pR.data() + size_t(l) * n) &&
+         write_fortran_field(dir + "/popB." + fmtnumb(l) + ".init.bin", nx, ny, nz, pB.data() + size_t(l) * n);
+  return ok;
+}
+
 // initial densities of initType 1, 2, 3, 5, 6 (setupRho_Pops, main.CUF:2531-2608)
 // densR / densB: the two-density model's droplet (setup2 with DIFFDENS,
 // kernels_fluid_CG.CUF:163-169); 1, 1 otherwise
@@ -208,8 +269,14 @@ bool initial_fields(int type, int nx, int ny, int nz, unsigned seed, std::vector
   size_t n = size_t(nx) * ny * nz;
   R.assign(n, 0.f);
   B.assign(n, 0.f);
-  if (type == 3) return read_fortran_field("rhoR.init.bin", nx, ny, nz, R.data()) &&
-                        read_fortran_field("rhoB.init.bin", nx, ny, nz, B.data());
+  // initType 3 starts from these densities; initType 4 reads them as well
+  // (read_and_setRed_Blue) before its populations
+  if (type == 3 || type == 4) {
+    const bool ok = read_fortran_field("rhoR.init.bin", nx, ny, nz, R.data()) &&
+                    read_fortran_field("rhoB.init.bin", nx, ny, nz, B.data());
+    if (!ok) std::fprintf(stderr, "Wrong start rho file rhoR.init.bin / rhoB.init.bin\n");
+    return ok;
+  }
   std::mt19937_64 rng(seed);
   std::uniform_real_distribution<float> U(0.f, 1.f);
   for (int k = 1; k <= nz; ++k)
@@ -295,6 +362,7 @@ int main(int argc, char** argv) {
   const char* xyz_path = "input.xyz";
   std::string out = "output";
   unsigned seed = 1;
+  std::string restart_out;
   lbx_params p;
   lbx_default_params(&p, nx, ny, nz);
   for (int a = 1; a < argc; ++a) {
@@ -327,6 +395,7 @@ int main(int argc, char** argv) {
     else if (s == "--xyz") xyz_path = nxt();
     else if (s == "--out") out = nxt();
     else if (s == "--seed") seed = unsigned(std::atoi(nxt()));
+    else if (s == "--restart-out") restart_out = nxt();
     else deck_path = argv[a];
   }
   p.nx = nx; p.ny = ny; p.nz = nz;
@@ -345,6 +414,12 @@ int main(int argc, char** argv) {
   void* ctx = nullptr;
   if (check(lbx_create(&p, &ctx), "lbx_create")) return 1;
   if (check(lbx_set_fields(ctx, R.data(), B.data(), d.vx, d.vy, d.vz), "lbx_set_fields")) return 1;
+  const int npop = (p.model == LBX_MODEL_CG_D3Q27 || p.model == LBX_MODEL_CG_DIFFDENS_D3Q27) ? 27 : 19;
+  if (d.initType == 4) {
+    std::vector<float> pR, pB;
+    if (!read_init_pops(".", npop, nx, ny, nz, pR, pB)) return 2;
+    if (check(lbx_set_pops(ctx, pR.data(), p.model == LBX_MODEL_BGK ? nullptr : pB.data()), "lbx_set_pops")) return 1;
+  }
   if (d.withParticles && check(lbx_set_particles(ctx, d.numAtoms, x.data(), v.data(), nullptr, q.data()),
                                "lbx_set_particles"))
     return 1;
@@ -381,6 +456,14 @@ int main(int argc, char** argv) {
         std::snprintf(fn, sizeof fn, "%s/particle_0.%08d.vtk", out.c_str(), step);
         write_particles_vtk(fn, d.numAtoms, x, v, q);
       }
+    }
+  }
+  if (!restart_out.empty()) {
+    mkdir(restart_out.c_str(), 0755);
+    if (!write_restart(ctx, restart_out, npop, nx, ny, nz)) {
+      std::fprintf(stderr, "restart files not written to %s\n", restart_out.c_str());
+      lbx_destroy(ctx);
+      return 1;
     }
   }
   int32_t code = 0, st = 0;

@@ -14,6 +14,10 @@
 * :func:`read_fortran_field` / :func:`write_fortran_field` — the
   Fortran-unformatted ``rhoR.init.bin`` layout (header record
   minx,maxx,miny,maxy,minz,maxz then one FP32 record, main.CUF:2448-2470);
+* :func:`read_init_pops` / :func:`write_init_pops` — initType 4's
+  per-direction population files ``popR.NNNNNN.init.bin`` /
+  ``popB.NNNNNN.init.bin`` (read_and_setPops, main.CUF:2489-2529), the
+  restart set of a run;
 * :func:`seeded_noise_fields` — the seeded synthetic inputs that stand in for
   the reference's unseeded Fortran RNG.
 """
@@ -260,7 +264,7 @@ def initial_fields(init_type, nx, ny, nz, seed=0, path=".", dens=None):
         blue = (nz * 1 // 8 < k) & (k < nz * 5 // 8)
         t = np.where(blue, f(0.0), f(1.0)).astype(f)
         return t, (f(1.0) - t).astype(f)
-    if init_type == 3:  # read_and_setRed_Blue
+    if init_type in (3, 4):  # read_and_setRed_Blue (initType 4 reads them before its populations)
         rR = read_fortran_field(os.path.join(path, "rhoR.init.bin"), nx, ny, nz)
         rB = read_fortran_field(os.path.join(path, "rhoB.init.bin"), nx, ny, nz)
         return rR, rB
@@ -325,3 +329,28 @@ def write_fortran_field(path, a):
         for rec in (hdr, body):
             n = np.array([len(rec)], np.int32).tobytes()
             fh.write(n + rec + n)
+
+
+def pops_file(comp, l):
+    """File name of direction l of one component in the initType-4 set: popR.NNNNNN.init.bin
+    (write_fmtnumb's six zero-padded digits, write_output.f90:858-875)."""
+    return f"pop{'RB'[comp]}.{l:06d}.init.bin"
+
+
+def read_init_pops(path, nx, ny, nz, q=19):
+    """initType 4 (read_and_setPops, main.CUF:2489-2529): the q per-direction files of each
+    component in `path`, as float32 (q, nz, ny, nx) arrays (popsR, popsB)."""
+    return tuple(np.stack([read_fortran_field(os.path.join(path, pops_file(c, l)), nx, ny, nz) for l in range(q)])
+                 for c in (0, 1))
+
+
+def write_init_pops(path, popsR, popsB, rhoR=None, rhoB=None):
+    """The initType-4 restart set: popR/popB.NNNNNN.init.bin per direction ((q, nz, ny, nx) arrays)
+    and, when given, rhoR/rhoB.init.bin, which the reference reads alongside (read_and_setRed_Blue)."""
+    os.makedirs(path, exist_ok=True)
+    for c, pops in enumerate((popsR, popsB)):
+        for l in range(pops.shape[0]):
+            write_fortran_field(os.path.join(path, pops_file(c, l)), pops[l])
+    if rhoR is not None:
+        write_fortran_field(os.path.join(path, "rhoR.init.bin"), rhoR)
+        write_fortran_field(os.path.join(path, "rhoB.init.bin"), rhoB)

@@ -152,3 +152,16 @@ def test_oracle_binding_is_independent_of_the_product():
     assert bytes(a) == bytes(b)
     for x, y in zip(orc.noise_fields(8, 6, 4, seed=3), seeded_noise_fields(8, 6, 4, seed=3)):
         assert np.array_equal(x, y)
+
+
+def test_init_pops_roundtrip(tmp_path):
+    """initType 4's per-direction files: six-digit names (write_fmtnumb) and a lossless round trip."""
+    rng = np.random.default_rng(0)
+    pR = rng.normal(size=(19, 4, 3, 5)).astype(np.float32)
+    pB = rng.normal(size=(19, 4, 3, 5)).astype(np.float32)
+    inputs.write_init_pops(str(tmp_path), pR, pB, pR.sum(0), pB.sum(0))
+    assert (tmp_path / "popR.000000.init.bin").exists() and (tmp_path / "popB.000018.init.bin").exists()
+    a, b = inputs.read_init_pops(str(tmp_path), 5, 3, 4)
+    assert np.array_equal(a, pR) and np.array_equal(b, pB)
+    rR, rB = inputs.initial_fields(4, 5, 3, 4, path=str(tmp_path))
+    assert np.array_equal(rR, pR.sum(0))
