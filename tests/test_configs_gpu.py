@@ -106,6 +106,7 @@ def test_cg_spinodal_128cube_100_steps(flow):
         tol_l2 = 5e-5 if (name == "vel" and not any(flow)) else TOL
         assert l2 <= tol_l2, f"{name}: rel L2 {l2:.2e}"
         mx, env = rel(a, b), envelope(b, c)
+        print(f"spinodal flow={flow} {name}: rel L2 {l2:.2e}, max-norm {mx:.2e}, FP32 envelope {env:.2e}")
         assert mx <= max(TOL, 2 * env), f"{name}: max-norm {mx:.2e}, FP32 envelope {env:.2e}"
 
 
@@ -144,10 +145,12 @@ def test_colloid_256cube_1280_spheres_5_steps():
         l2 = rel_l2(gp[key], op[key])
         assert l2 <= TOL, f"{key}: rel L2 {l2:.2e}"
         mx, env = rel(gp[key], op[key]), envelope(op[key], p64[key])
+        print(f"colloid {key}: rel L2 {l2:.2e}, max-norm {mx:.2e}, FP32 envelope {env:.2e}")
         assert mx <= max(TOL, 2 * env), f"{key}: max-norm {mx:.2e}, FP32 envelope {env:.2e}"
     gf, f64 = g.get_fields(), res["f64"][3]
     for k, name in enumerate(("rhoR", "rhoB", "vel", "phase")):
         l2 = rel_l2(gf[k], ofl[k])
         assert l2 <= (5e-5 if name == "vel" else TOL), f"{name}: rel L2 {l2:.2e}"
         mx, env = rel(gf[k], ofl[k]), envelope(ofl[k], f64[k])
+        print(f"colloid {name}: rel L2 {l2:.2e}, max-norm {mx:.2e}, FP32 envelope {env:.2e}")
         assert mx <= max(TOL, 2 * env), f"{name}: max-norm {mx:.2e}, FP32 envelope {env:.2e}"
