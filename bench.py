@@ -37,7 +37,7 @@ LB_PER_STEP = 500
 # DRAM bytes (read + write) of one k_cg_lean launch at 128^3, from the ncu
 # captures summarised in profiles/ (None where no capture of that storage)
 TRAFFIC = {"f16": 292.7e6, "f16sd": 292.0e6, "f32": 622.6e6}
-BYTES_PER_CELL = {"f16": 160, "bf16": 160, "f16sd": 160, "f32": 312, "f64": 616}  # algorithmic bytes per cell-step
+BYTES_PER_CELL = {"f16": 160, "bf16": 160, "f16sd": 160, "bf16sd": 160, "f32": 312, "f64": 616}  # algorithmic bytes per cell-step
 MINIMAL_BYTES = {"f16": 152, "bf16": 152, "f16sd": 152, "f32": 304, "f64": 608}   # populations only (phi on chip)
 METRIC = "MLUPS & HBM GB/s, FP16-store vs FP32 LB at stated FP64 error, 1\u00d7B200"
 
@@ -312,8 +312,9 @@ def colloid_error_vs_f64(steps=(100, 1000)):
     return out
 
 
-def colloid_timing(storage, steps=50, warm=10, small=False):
+def colloid_timing(storage, steps=50, warm=10, small=False, bulk=True):
     s = colloid_sim(storage, small=small)
+    s.set_lean_copies(bulk)
     s.step(warm)
     s.sync()
     tot, k, nl = s.time_steps(steps, kernel_timing=True)
@@ -564,20 +565,25 @@ def only_region(args, local):
         return 0
     if args.only.startswith("colloid"):
         r = colloid_timing(args.only.split("-")[1], steps=max(1, args.steps) * 5, warm=args.warmup,
-                           small=args.only.endswith("small"))
+                           small=args.only.endswith("small"), bulk=not args.per_thread_copies)
         print(json.dumps(r), flush=True)
         return 0
-    rR, rB = seeded_noise_fields(L, L, L, seed=SEED)
-    s = LBSim(make_params(L, model="cg", storage=args.only, sigma=SIGMA, beta=BETA))
+    Lb = args.box
+    rR, rB = seeded_noise_fields(Lb, Lb, Lb, seed=SEED)
+    s = LBSim(make_params(Lb, model="cg", storage=args.only, sigma=SIGMA, beta=BETA))
     s.set_schedule(args.schedule)
+    s.set_lean_copies(not args.per_thread_copies)
     s.set_fields(rR, rB)
     s.step(args.warmup * args.lb_steps)
     s.sync()
     tot, k, nl = s.time_steps(args.steps * args.lb_steps, kernel_timing=args.schedule != 0)
     n = args.steps * args.lb_steps
-    print(json.dumps({"only": args.only, "schedule": args.schedule, "ms_per_lattice_step": tot / n,
-                      "mlups": L ** 3 * n / (tot * 1e-3) / 1e6, "kernel_us": (k / nl * 1e3) if nl else None}),
-          flush=True)
+    kus = (k / nl * 1e3) if nl else None
+    print(json.dumps({"only": args.only, "box": Lb, "schedule": args.schedule,
+                      "copies": "per-thread" if args.per_thread_copies else "bulk", "ms_per_lattice_step": tot / n,
+                      "mlups": Lb ** 3 * n / (tot * 1e-3) / 1e6, "kernel_us": kus,
+                      "frac_at_basis": (BYTES_PER_CELL[args.only] * Lb ** 3 / (kus * 1e-6) / 1e9 / peaks()[0])
+                      if kus else None}), flush=True)
     s.close()
     return 0
 
@@ -595,6 +601,9 @@ def main():
                     help="profiling aid: run one timed region only and print its timing")
     ap.add_argument("--lb-steps", type=int, default=LB_PER_STEP, help="lattice steps per bench step")
     ap.add_argument("--schedule", type=int, default=2, help="colour-gradient schedule (0, 1, 2)")
+    ap.add_argument("--box", type=int, default=L, help="lattice edge of the --only storage runs")
+    ap.add_argument("--per-thread-copies", action="store_true",
+                    help="lean kernel: per-thread cp.async pulls instead of bulk row copies")
     args = ap.parse_args()
     ws, rank, local = dist_env()
     if args.impl == "reference":

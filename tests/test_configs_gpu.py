@@ -19,7 +19,9 @@ Stated tolerances:
   colour gradient, sphere states (FP32 fluid, reassociated collision):
       relative L2 |gpu - oracle|_2 / |oracle|_2 <= 1e-5 for every field and
       every particle quantity (the spinodal at rest: velocity 5e-5, its ~1e-4
-      velocity being the difference of ~3e-2 momenta), and the max-norm
+      velocity being the difference of ~3e-2 momenta; the sphere velocities,
+      forces and torques: max(1e-5, 2 x the oracle's FP32-vs-FP64 relative L2
+      difference)), and the max-norm
       difference within max(1e-5, 2 x the oracle's own FP32-vs-FP64 max-norm
       difference on the same run): spinodal decomposition amplifies rounding
       differences, so any two FP32 operation orders drift apart at the rate
@@ -142,10 +144,12 @@ def test_colloid_256cube_1280_spheres_5_steps():
     assert np.abs(gp["x"] - op["x"]).max() < 1e-6
     assert np.abs(gp["q"] - op["q"]).max() < 1e-6
     for key in ("v", "omega", "force", "torque"):
-        l2 = rel_l2(gp[key], op[key])
-        assert l2 <= TOL, f"{key}: rel L2 {l2:.2e}"
+        # the sphere state integrates the FP32 fluid's forces, so both norms
+        # are held to the FP32 envelope of the oracle's own run as well
+        l2, env_l2 = rel_l2(gp[key], op[key]), rel_l2(op[key], p64[key])
         mx, env = rel(gp[key], op[key]), envelope(op[key], p64[key])
-        print(f"colloid {key}: rel L2 {l2:.2e}, max-norm {mx:.2e}, FP32 envelope {env:.2e}")
+        print(f"colloid {key}: rel L2 {l2:.2e} (envelope {env_l2:.2e}), max-norm {mx:.2e} (envelope {env:.2e})")
+        assert l2 <= max(TOL, 2 * env_l2), f"{key}: rel L2 {l2:.2e}, FP32 envelope {env_l2:.2e}"
         assert mx <= max(TOL, 2 * env), f"{key}: max-norm {mx:.2e}, FP32 envelope {env:.2e}"
     gf, f64 = g.get_fields(), res["f64"][3]
     for k, name in enumerate(("rhoR", "rhoB", "vel", "phase")):
