@@ -16,9 +16,13 @@
 // optimiser steps of all epochs.
 //
 // Kernels
-//   k_mlp_train  one CTA runs every epoch of minibatch Adam on the whole data
-//                set: forward, backward and update fused, activations in
-//                shared memory, gradients reduced in a fixed order.
+//   k_mlp_train  one thread-block cluster of 8 CTAs runs every epoch of
+//                minibatch Adam on the whole data set: each CTA takes 8 of
+//                the 64 samples of a minibatch (forward, backward, its
+//                gradient in shared memory), the gradient is summed over the
+//                cluster in rank order through distributed shared memory,
+//                each CTA updates one slice of the parameters and writes it
+//                into every CTA's copy.
 //   k_mlp_infer  one warp per sample (pair), weights in shared memory.
 //   k_pairs (lbx_particles.cu) / k_closure_pairs / k_closure_accum: per
 //                step, the close pairs of each sphere (ascending index, listed
@@ -28,24 +32,27 @@
 #include "lbx_device.cuh"
 #include "lbx_closure.h"
 
+#include <cooperative_groups.h>
 #include <cmath>
 #include <vector>
 
 namespace lbx {
 
 // ---------------------------------------------------------------------------
-// training: one CTA of 256 threads, minibatch B
+// training: a thread-block cluster of NCL CTAs, minibatch TB split over them
 // ---------------------------------------------------------------------------
-constexpr int TB = 64;    // minibatch (shared-memory bound)
-constexpr int TT = 256;   // threads
+constexpr int TB = 64;              // minibatch
+constexpr int TT = 256;             // threads per CTA
+constexpr int NCL = 8;              // CTAs of the cluster (portable cluster size)
+constexpr int TBC = TB / NCL;       // samples of a minibatch per CTA
+constexpr int NP4 = (MlpLayout::NPARAM + 3) / 4 * 4;
+constexpr int SLICE = (MlpLayout::NPARAM + NCL - 1) / NCL;  // parameters each CTA reduces and updates
 
 struct TrainArgs {
   const float* X;   // n x DIN, standardised
   const float* T;   // n x DOUT, standardised
   int n;
   float* w;         // NPARAM (updated)
-  float* m;         // Adam moments
-  float* v;
   float* loss;      // per epoch (may be null)
   float* grad_out;  // grad-only mode: NPARAM gradient of the first minibatch
   int epochs;
@@ -53,10 +60,10 @@ struct TrainArgs {
   unsigned seed;
 };
 
-// Z[b][o] = sum_k A[b][k] W[o][k] + bias[o]   (A: TB x K in smem, W: O x K in smem)
+// Z[b][o] = sum_k A[b][k] W[o][k] + bias[o] for the CTA's TBC samples
 __device__ void dense_fwd(const float* A, int K, const float* W, const float* bias, int O, float* Z) {
-  for (int idx = threadIdx.x; idx < TB * O; idx += TT) {
-    int b = idx / O, o = idx % O;
+  for (int idx = threadIdx.x; idx < TBC * O; idx += TT) {
+    const int b = idx / O, o = idx % O;
     const float* a = A + b * K;
     const float* wr = W + o * K;
     float s = bias[o];
@@ -65,21 +72,69 @@ __device__ void dense_fwd(const float* A, int K, const float* W, const float* bi
   }
 }
 
-__global__ void __launch_bounds__(TT) k_mlp_train(TrainArgs a) {
+// G[W][o][k] = sum_b dZ[b][o] A[b][k], G[bias][o] = sum_b dZ[b][o] (this CTA's samples, in order)
+__device__ void dense_grad(const float* dZ, int O, const float* A, int K, float* GW, float* GB) {
+  for (int idx = threadIdx.x; idx < O * K; idx += TT) {
+    const int o = idx / K, k = idx % K;
+    float s = 0.f;
+#pragma unroll
+    for (int b = 0; b < TBC; ++b) s = fmaf(dZ[b * O + o], A[b * K + k], s);
+    GW[idx] = s;
+  }
+  for (int o = threadIdx.x; o < O; o += TT) {
+    float s = 0.f;
+#pragma unroll
+    for (int b = 0; b < TBC; ++b) s += dZ[b * O + o];
+    GB[o] = s;
+  }
+}
+
+// dZp[b][k] = (sum_o dZ[b][o] W[o][k]) * silu'(Zp[b][k])
+__device__ void dense_back(const float* dZ, int O, const float* W, const float* Zp, int K, float* dZp) {
+  for (int idx = threadIdx.x; idx < TBC * K; idx += TT) {
+    const int b = idx / K, k = idx % K;
+    float s = 0.f;
+    for (int o = 0; o < O; ++o) s = fmaf(dZ[b * O + o], W[o * K + k], s);
+    dZp[idx] = s * dsilu(Zp[idx]);
+  }
+}
+
+// Every epoch of minibatch Adam on the whole data set in one launch of one
+// cluster.  Each CTA holds the weights, runs forward and backward for its
+// TBC samples of the minibatch and keeps their gradient in its shared
+// memory; after a cluster barrier CTA r sums slice r of the gradient over the
+// CTAs in rank order (distributed shared memory reads), updates that slice
+// with Adam (its moments stay in its shared memory) and writes the new
+// values into every CTA's weights; a second barrier ends the step.  The
+// minibatches, their order and the update are those of a single CTA running
+// all TB samples; only the summation order of the gradient differs.
+__global__ void __cluster_dims__(NCL, 1, 1) __launch_bounds__(TT) k_mlp_train(TrainArgs a) {
+  namespace cg = cooperative_groups;
   using L = MlpLayout;
+  cg::cluster_group cl = cg::this_cluster();
+  const int rank = int(cl.block_rank());
   extern __shared__ float sm[];
-  float* W = sm;                       // NPARAM
-  float* X0 = W + L::NPARAM;           // TB x DIN
-  float* Z1 = X0 + TB * DIN;           // TB x H (pre-activations)
-  float* Z2 = Z1 + TB * H;
-  float* Z3 = Z2 + TB * H;
-  float* Y = Z3 + TB * H;              // TB x DOUT
-  float* D = Y + TB * DOUT;            // TB x H   (gradient w.r.t. the current layer's pre-activation)
-  float* E = D + TB * H;               // TB x H   (scratch: activations / next gradient)
-  float* G = E + TB * H;               // NPARAM gradient of the minibatch
+  float* W = sm;                       // NPARAM (replicated)
+  float* G = W + NP4;                  // NPARAM: gradient of this CTA's samples
+  float* Mo = G + NP4;                 // SLICE: Adam moments of this CTA's slice
+  float* Vo = Mo + SLICE;
+  float* X0 = Vo + SLICE;              // TBC x DIN
+  float* Z1 = X0 + TBC * DIN;          // TBC x H pre-activations
+  float* Z2 = Z1 + TBC * H;
+  float* Z3 = Z2 + TBC * H;
+  float* A1 = Z3 + TBC * H;            // TBC x H activations
+  float* A2 = A1 + TBC * H;
+  float* A3 = A2 + TBC * H;
+  float* Y = A3 + TBC * H;             // TBC x DOUT
+  float* D = Y + TBC * DOUT;           // TBC x DOUT: dL/dY
+  float* E = D + TBC * DOUT;           // TBC x H: dL/dZ of the current layer
+  float* F = E + TBC * H;              // TBC x H: dL/dZ of the layer below
   __shared__ float red[TT];
-  __shared__ int idxs[TB];
+  __shared__ int idxs[TBC];
+  __shared__ float part_loss;
   for (int i = threadIdx.x; i < L::NPARAM; i += TT) W[i] = a.w[i];
+  for (int i = threadIdx.x; i < SLICE; i += TT) Mo[i] = Vo[i] = 0.f;
+  const int lo = rank * SLICE, hi = min(L::NPARAM, lo + SLICE);
   __syncthreads();
   const int nb = (a.n + TB - 1) / TB;
   const bool grad_only = a.grad_out != nullptr;
@@ -98,119 +153,87 @@ __global__ void __launch_bounds__(TT) k_mlp_train(TrainArgs a) {
     float ep_loss = 0.f;
     for (int bi = 0; bi < (grad_only ? 1 : nb); ++bi) {
       const int cnt = min(TB, a.n - bi * TB);
-      for (int b = threadIdx.x; b < TB; b += TT)
-        idxs[b] = grad_only ? min(b, a.n - 1) : int((long long)(bi * TB + min(b, cnt - 1)) * stride % a.n + off) % a.n;
+      for (int b = threadIdx.x; b < TBC; b += TT) {
+        const int gb = rank * TBC + b;  // sample of the minibatch
+        idxs[b] = grad_only ? min(gb, a.n - 1)
+                            : int((long long)(bi * TB + min(gb, cnt - 1)) * stride % a.n + off) % a.n;
+      }
       __syncthreads();
-      for (int i = threadIdx.x; i < TB * DIN; i += TT) X0[i] = a.X[size_t(idxs[i / DIN]) * DIN + i % DIN];
+      for (int i = threadIdx.x; i < TBC * DIN; i += TT) X0[i] = a.X[size_t(idxs[i / DIN]) * DIN + i % DIN];
       __syncthreads();
       // forward
       dense_fwd(X0, DIN, W + L::W0, W + L::B0, H, Z1);
       __syncthreads();
-      for (int i = threadIdx.x; i < TB * H; i += TT) E[i] = silu(Z1[i]);
+      for (int i = threadIdx.x; i < TBC * H; i += TT) A1[i] = silu(Z1[i]);
       __syncthreads();
-      dense_fwd(E, H, W + L::W1, W + L::B1, H, Z2);
+      dense_fwd(A1, H, W + L::W1, W + L::B1, H, Z2);
       __syncthreads();
-      for (int i = threadIdx.x; i < TB * H; i += TT) E[i] = silu(Z2[i]);
+      for (int i = threadIdx.x; i < TBC * H; i += TT) A2[i] = silu(Z2[i]);
       __syncthreads();
-      dense_fwd(E, H, W + L::W2, W + L::B2, H, Z3);
+      dense_fwd(A2, H, W + L::W2, W + L::B2, H, Z3);
       __syncthreads();
-      for (int i = threadIdx.x; i < TB * H; i += TT) E[i] = silu(Z3[i]);
+      for (int i = threadIdx.x; i < TBC * H; i += TT) A3[i] = silu(Z3[i]);
       __syncthreads();
-      dense_fwd(E, H, W + L::W3, W + L::B3, DOUT, Y);
+      dense_fwd(A3, H, W + L::W3, W + L::B3, DOUT, Y);
       __syncthreads();
-      // loss = mean over valid samples and outputs of (y - t)^2; dY in D (TB x DOUT)
+      // loss = mean over the minibatch's valid samples and outputs of (y - t)^2
       float part = 0.f;
       const float scale = 2.0f / float(cnt * DOUT);
-      for (int i = threadIdx.x; i < TB * DOUT; i += TT) {
-        int b = i / DOUT;
-        float d = (b < cnt) ? Y[i] - a.T[size_t(idxs[b]) * DOUT + i % DOUT] : 0.f;
+      for (int i = threadIdx.x; i < TBC * DOUT; i += TT) {
+        const int b = i / DOUT;
+        const float d = (rank * TBC + b < cnt) ? Y[i] - a.T[size_t(idxs[b]) * DOUT + i % DOUT] : 0.f;
         part += d * d;
         D[i] = d * scale;
       }
       red[threadIdx.x] = part;
       __syncthreads();
-      for (int s = TT / 2; s > 0; s >>= 1) {
-        if (threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
+      for (int st = TT / 2; st > 0; st >>= 1) {
+        if (threadIdx.x < st) red[threadIdx.x] += red[threadIdx.x + st];
         __syncthreads();
       }
-      if (threadIdx.x == 0) ep_loss += red[0];
-      // layer 3: G[W3] = dY^T A3 (A3 = silu(Z3) is in E), G[B3] = sum dY
-      for (int idx = threadIdx.x; idx < DOUT * H; idx += TT) {
-        int o = idx / H, k = idx % H;
-        float s = 0.f;
-        for (int b = 0; b < TB; ++b) s = fmaf(D[b * DOUT + o], E[b * H + k], s);
-        G[L::W3 + idx] = s;
-      }
-      for (int o = threadIdx.x; o < DOUT; o += TT) {
-        float s = 0.f;
-        for (int b = 0; b < TB; ++b) s += D[b * DOUT + o];
-        G[L::B3 + o] = s;
-      }
+      if (threadIdx.x == 0) part_loss = red[0];
+      // backward: output layer, then the three hidden layers
+      dense_grad(D, DOUT, A3, H, G + L::W3, G + L::B3);
+      dense_back(D, DOUT, W + L::W3, Z3, H, E);
       __syncthreads();
-      // dA3 = dY W3 -> dZ3 = dA3 * silu'(Z3), into E (A3 no longer needed)
-      for (int idx = threadIdx.x; idx < TB * H; idx += TT) {
-        int b = idx / H, k = idx % H;
-        float s = 0.f;
-        for (int o = 0; o < DOUT; ++o) s = fmaf(D[b * DOUT + o], W[L::W3 + o * H + k], s);
-        E[idx] = s * dsilu(Z3[idx]);
-      }
+      dense_grad(E, H, A2, H, G + L::W2, G + L::B2);
+      dense_back(E, H, W + L::W2, Z2, H, F);
       __syncthreads();
-      // hidden layers 2 and 1 (and the input layer): dZ in E, A_prev = silu(Z_prev)
-      const float* Zs[3] = {Z2, Z1, nullptr};
-      const int Wo[3] = {L::W2, L::W1, L::W0}, Bo[3] = {L::B2, L::B1, L::B0};
-      for (int layer = 0; layer < 3; ++layer) {
-        const float* Zp = Zs[layer];
-        const int K = Zp ? H : DIN;
-        for (int idx = threadIdx.x; idx < H * K; idx += TT) {
-          int o = idx / K, k = idx % K;
-          float s = 0.f;
-          if (Zp)
-            for (int b = 0; b < TB; ++b) s = fmaf(E[b * H + o], silu(Zp[b * H + k]), s);
-          else
-            for (int b = 0; b < TB; ++b) s = fmaf(E[b * H + o], X0[b * DIN + k], s);
-          G[Wo[layer] + idx] = s;
-        }
-        for (int o = threadIdx.x; o < H; o += TT) {
-          float s = 0.f;
-          for (int b = 0; b < TB; ++b) s += E[b * H + o];
-          G[Bo[layer] + o] = s;
-        }
-        __syncthreads();
-        if (Zp) {
-          // dZ_prev = (dZ W) * silu'(Z_prev) into D, then swap into E
-          for (int idx = threadIdx.x; idx < TB * H; idx += TT) {
-            int b = idx / H, k = idx % H;
-            float s = 0.f;
-            for (int o = 0; o < H; ++o) s = fmaf(E[b * H + o], W[Wo[layer] + o * H + k], s);
-            D[idx] = s * dsilu(Zp[idx]);
-          }
-          __syncthreads();
-          for (int idx = threadIdx.x; idx < TB * H; idx += TT) E[idx] = D[idx];
-          __syncthreads();
-        }
-      }
+      dense_grad(F, H, A1, H, G + L::W1, G + L::B1);
+      dense_back(F, H, W + L::W1, Z1, H, E);
+      __syncthreads();
+      dense_grad(E, H, X0, DIN, G + L::W0, G + L::B0);
+      cl.sync();  // every CTA's gradient and loss share are complete
+      if (rank == 0 && threadIdx.x == 0)
+        for (int r = 0; r < NCL; ++r) ep_loss += *cl.map_shared_rank(&part_loss, r);
       if (grad_only) {
-        for (int i = threadIdx.x; i < L::NPARAM; i += TT) a.grad_out[i] = G[i];
-        __syncthreads();
+        for (int i = lo + int(threadIdx.x); i < hi; i += TT) {
+          float g = 0.f;
+          for (int r = 0; r < NCL; ++r) g += cl.map_shared_rank(G, r)[i];
+          a.grad_out[i] = g;
+        }
+        cl.sync();
         break;
       }
-      // Adam
+      // Adam on this CTA's slice; the new weights go to every CTA
       ++t_adam;
       const float c1 = 1.0f - powf(a.beta1, float(t_adam)), c2 = 1.0f - powf(a.beta2, float(t_adam));
       const float lr_t = 0.5f * a.lr * (1.0f + cospif(float(t_adam - 1) / float(a.epochs * nb)));
-      for (int i = threadIdx.x; i < L::NPARAM; i += TT) {
-        float gi = G[i];
-        float mi = a.beta1 * a.m[i] + (1.0f - a.beta1) * gi;
-        float vi = a.beta2 * a.v[i] + (1.0f - a.beta2) * gi * gi;
-        a.m[i] = mi;
-        a.v[i] = vi;
-        W[i] -= lr_t * (mi / c1) / (sqrtf(vi / c2) + a.eps);
+      for (int i = lo + int(threadIdx.x); i < hi; i += TT) {
+        float gi = 0.f;
+        for (int r = 0; r < NCL; ++r) gi += cl.map_shared_rank(G, r)[i];
+        const float mi = a.beta1 * Mo[i - lo] + (1.0f - a.beta1) * gi;
+        const float vi = a.beta2 * Vo[i - lo] + (1.0f - a.beta2) * gi * gi;
+        Mo[i - lo] = mi;
+        Vo[i - lo] = vi;
+        const float wi = W[i] - lr_t * (mi / c1) / (sqrtf(vi / c2) + a.eps);
+        for (int r = 0; r < NCL; ++r) cl.map_shared_rank(W, r)[i] = wi;
       }
-      __syncthreads();
+      cl.sync();  // new weights everywhere; gradients free for the next step
     }
-    if (threadIdx.x == 0 && a.loss && !grad_only) a.loss[ep] = ep_loss / float(a.n * DOUT);
+    if (rank == 0 && threadIdx.x == 0 && a.loss && !grad_only) a.loss[ep] = ep_loss / float(a.n * DOUT);
   }
-  if (!grad_only)
+  if (!grad_only && rank == 0)
     for (int i = threadIdx.x; i < L::NPARAM; i += TT) a.w[i] = W[i];
 }
 
@@ -264,8 +287,8 @@ struct Dev {
   }
 };
 size_t train_smem() {
-  using L = lbx::MlpLayout;
-  return sizeof(float) * (2 * size_t(L::NPARAM) + lbx::TB * lbx::DIN + 5 * lbx::TB * lbx::H + lbx::TB * lbx::DOUT);
+  return sizeof(float) * (2 * size_t(lbx::NP4) + 2 * size_t(lbx::SLICE) + lbx::TBC * lbx::DIN + 6 * lbx::TBC * lbx::H +
+                          2 * lbx::TBC * lbx::DOUT + 2 * lbx::TBC * lbx::H);
 }
 int rc_of(cudaError_t e) { return e == cudaSuccess ? 0 : LBX_ERR_CUDA; }
 }  // namespace
@@ -300,9 +323,8 @@ int lbx_closure_train(float* weights, const float* X, const float* T, int32_t n,
   using L = lbx::MlpLayout;
   if (!weights || !X || !T || n < 1 || epochs < 1) return LBX_ERR_ARG;
   const size_t nx = size_t(n) * lbx::DIN, nt = size_t(n) * lbx::DOUT;
-  Dev dX(nx * 4), dT(nt * 4), dW(size_t(L::TOTAL) * 4), dM(size_t(L::NPARAM) * 4), dV(size_t(L::NPARAM) * 4),
-      dL(size_t(epochs) * 4);
-  if (!dX.p || !dT.p || !dW.p || !dM.p || !dV.p || !dL.p) return LBX_ERR_ALLOC;
+  Dev dX(nx * 4), dT(nt * 4), dW(size_t(L::TOTAL) * 4), dL(size_t(epochs) * 4);
+  if (!dX.p || !dT.p || !dW.p || !dL.p) return LBX_ERR_ALLOC;
   // standardise with the statistics stored in the blob
   std::vector<float> Xs(nx), Ts(nt);
   for (size_t i = 0; i < nx; ++i) Xs[i] = (X[i] - weights[L::XMU + i % lbx::DIN]) / weights[L::XSD + i % lbx::DIN];
@@ -310,15 +332,13 @@ int lbx_closure_train(float* weights, const float* X, const float* T, int32_t n,
   int rc = rc_of(cudaMemcpy(dX.p, Xs.data(), nx * 4, cudaMemcpyHostToDevice));
   if (!rc) rc = rc_of(cudaMemcpy(dT.p, Ts.data(), nt * 4, cudaMemcpyHostToDevice));
   if (!rc) rc = rc_of(cudaMemcpy(dW.p, weights, size_t(L::TOTAL) * 4, cudaMemcpyHostToDevice));
-  if (!rc) rc = rc_of(cudaMemset(dM.p, 0, size_t(L::NPARAM) * 4));
-  if (!rc) rc = rc_of(cudaMemset(dV.p, 0, size_t(L::NPARAM) * 4));
   if (rc) return rc;
-  lbx::TrainArgs a{(const float*)dX.p, (const float*)dT.p, n, (float*)dW.p, (float*)dM.p, (float*)dV.p,
-                   (float*)dL.p, nullptr, epochs, lr, 0.9f, 0.999f, 1e-8f, unsigned(seed)};
+  lbx::TrainArgs a{(const float*)dX.p, (const float*)dT.p, n, (float*)dW.p, (float*)dL.p, nullptr, epochs, lr,
+                   0.9f, 0.999f, 1e-8f, unsigned(seed)};
   size_t smem = train_smem();
   rc = rc_of(cudaFuncSetAttribute(lbx::k_mlp_train, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
   if (rc) return rc;
-  lbx::k_mlp_train<<<1, lbx::TT, smem>>>(a);
+  lbx::k_mlp_train<<<lbx::NCL, lbx::TT, smem>>>(a);  // one cluster
   rc = rc_of(cudaGetLastError());
   if (!rc) rc = rc_of(cudaDeviceSynchronize());
   if (!rc) rc = rc_of(cudaMemcpy(weights, dW.p, size_t(L::NPARAM) * 4, cudaMemcpyDeviceToHost));
@@ -336,12 +356,12 @@ int lbx_closure_grad(const float* weights, const float* Xs, const float* Ts, int
   if (!rc) rc = rc_of(cudaMemcpy(dT.p, Ts, nt * 4, cudaMemcpyHostToDevice));
   if (!rc) rc = rc_of(cudaMemcpy(dW.p, weights, size_t(L::TOTAL) * 4, cudaMemcpyHostToDevice));
   if (rc) return rc;
-  lbx::TrainArgs a{(const float*)dX.p, (const float*)dT.p, n, (float*)dW.p, nullptr, nullptr, nullptr,
-                   (float*)dG.p, 1, 0.f, 0.9f, 0.999f, 1e-8f, 0u};
+  lbx::TrainArgs a{(const float*)dX.p, (const float*)dT.p, n, (float*)dW.p, nullptr, (float*)dG.p, 1, 0.f,
+                   0.9f, 0.999f, 1e-8f, 0u};
   size_t smem = train_smem();
   rc = rc_of(cudaFuncSetAttribute(lbx::k_mlp_train, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
   if (rc) return rc;
-  lbx::k_mlp_train<<<1, lbx::TT, smem>>>(a);
+  lbx::k_mlp_train<<<lbx::NCL, lbx::TT, smem>>>(a);  // one cluster
   rc = rc_of(cudaGetLastError());
   if (!rc) rc = rc_of(cudaDeviceSynchronize());
   if (!rc) rc = rc_of(cudaMemcpy(grad, dG.p, size_t(L::NPARAM) * 4, cudaMemcpyDeviceToHost));

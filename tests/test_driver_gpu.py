@@ -97,14 +97,14 @@ def test_droplet_deck(tmp_path):
 
 def test_particle_deck(tmp_path):
     """Tests/07-1280-Particle's deck (rotation, MAX_PARTICLE_VEL) with 16 spheres of its placement in a
-    64^3 box: particle VTK and fluid VTI after 6 steps against LBSim."""
-    n = 64
+    128^3 box: particle VTK and fluid VTI after 6 steps against LBSim."""
+    n = 128
     x, v, q = read_input_xyz(os.path.join(DECKS, "07-1280.input.xyz.256cube.r5.5"), 1280, True)
-    # spheres of the placement inside [7, 57)^3: no periodic image of one
-    # comes near another in the 64^3 box
+    # spheres of the placement inside [7, n - 7)^3: no periodic image of one
+    # comes near another in the n^3 box
     keep = np.nonzero(((x >= 7) & (x < n - 7)).all(axis=1))[0][:16]
     k = len(keep)
-    assert k >= 8
+    assert k == 16
     src = open(os.path.join(DECKS, "07-1280.input.xyz.256cube.r5.5")).read().splitlines()
     with open(tmp_path / "input.xyz", "w") as fh:
         fh.write("\n".join([str(k), src[1]] + [src[2 + i] for i in keep]) + "\n")
