@@ -312,9 +312,8 @@ def colloid_error_vs_f64(steps=(100, 1000)):
     return out
 
 
-def colloid_timing(storage, steps=50, warm=10, small=False, bulk=True):
+def colloid_timing(storage, steps=50, warm=10, small=False):
     s = colloid_sim(storage, small=small)
-    s.set_lean_copies(bulk)
     s.step(warm)
     s.sync()
     tot, k, nl = s.time_steps(steps, kernel_timing=True)
@@ -348,13 +347,15 @@ def variants_timing(storage, steps=100, warm=20):
     return out
 
 
-def ensemble_timing(steps=100, err_steps=200, seed=7):
+def ensemble_timing(steps=100, err_steps=200, seed=7, weights=None):
     """Ensemble workload: 48 boxes, edges uniform from {32, 48, 64, 96}, 0-40 spheres of radius 4 each
-    (seeded, min gap 1), FP16 sum / difference pairs, closure switched on without weights (every close pair takes the
-    analytic lubrication fallback), advanced together by the persistent kernel under a CUDA graph after
-    the autotuner.  Error: relative L2 of each box's velocity field against the same box advanced alone
-    with FP32 storage, after err_steps steps."""
-    from lbcuda_b200 import LBSim, make_params
+    (seeded, min gap 1), FP16 sum / difference pairs, the learned closure on (with `weights`, trained for
+    radius 4; without them every close pair takes the analytic lubrication fallback), advanced together
+    by the persistent kernel under a CUDA graph after the autotuner.  Error: relative L2 of each box's
+    velocity field against the same box advanced alone with FP32 storage (same closure), after err_steps
+    steps."""
+    import ctypes
+    from lbcuda_b200 import LBSim, capi, make_params
     from lbcuda_b200.ensemble import Ensemble, random_boxes
     from lbcuda_b200.inputs import seeded_noise_fields
     spec = random_boxes(48, seed=seed)
@@ -364,11 +365,16 @@ def ensemble_timing(steps=100, err_steps=200, seed=7):
                            radius=4.0, wetting="neutral", lrotate=1, max_vel=1.0, exact_tiles=0,
                            hz_rmin=8.5, hz_rcap=7.0, closure=1, lubrication=1, lubric_rmin=1.0, lubric_rcap=0.2)
 
+    wf = None if weights is None else np.ascontiguousarray(weights, np.float32)
+
     def load(sim, i, L, x):
         rR, rB = seeded_noise_fields(L, L, L, seed=100 + i)
         sim.set_fields(rR, rB)
         if len(x):
             sim.set_particles(x, np.zeros_like(x))
+            if wf is not None:
+                capi.check(capi.lib().lbx_closure_set(sim._h, wf.ctypes.data_as(ctypes.POINTER(ctypes.c_float))),
+                           "lbx_closure_set")
 
     ens = Ensemble([params(L, len(x), "f16sd") for L, x in spec])
     for i, (L, x) in enumerate(spec):
@@ -391,6 +397,7 @@ def ensemble_timing(steps=100, err_steps=200, seed=7):
     spheres = int(sum(len(x) for _, x in spec))
     ens.close()
     return {"boxes": len(spec), "cells": cells, "spheres": spheres, "storage": "f16sd", "tuned": tuned,
+            "closure": "trained weights (R_lo = 4)" if weights is not None else "analytic fallback only",
             "ms_per_step": ms / steps, "mlups": cells * steps / (ms * 1e-3) / 1e6,
             "u_rel_l2_vs_f32_per_box": {"after_steps": err_steps, "max": max(errs), "median": float(np.median(errs))}}
 
@@ -526,9 +533,14 @@ def summary(line):
     }
     cl = line.get("closure")
     if cl:
-        out["closure"] = {"R_hi": cl["R_hi"], "rel_l2": r3(cl["error_direct"]["closure"]["rel_l2"]),
-                          "within_5pct": r3(cl["error_direct"]["closure"]["pairs_within_5pct"]),
-                          "cost_ratio": r3(cl["cost_ratio_same_physical_time"])}
+        out["closure"] = {"R_hi": cl["R_hi"], "pair_rel_l2": r3(cl["error_direct"]["closure"]["rel_l2"]),
+                          "pairs_within_5pct": r3(cl["error_direct"]["closure"]["pairs_within_5pct"]),
+                          "pair_cost_ratio": r3(cl["cost_ratio_same_physical_time"])}
+        win = cl.get("window")
+        if win:
+            out["closure"]["window_force_rel_l2"] = {k: r3(win[k]["force_rel_l2"]) for k in
+                                                     ("plain", "analytic_lubrication", "closure")}
+            out["closure"]["window_cost_ratio"] = r3(win["cost_ratio_same_physical_time"])
     return out
 
 
@@ -543,7 +555,16 @@ def only_region(args, local):
         print(json.dumps(res), flush=True)
         return 0
     if args.only == "closure12":
-        print(json.dumps(closure_experiment(R_hi=12, L_hi=96, steps_hi=960)), flush=True)
+        from lbcuda_b200 import closure as _cl
+        res, w = closure_experiment(R_hi=12, L_hi=96, steps_hi=960, return_weights=True)
+        res["window"] = _cl.window_score(w)
+        print(json.dumps(res), flush=True)
+        return 0
+    if args.only == "ensemble-closure":
+        r4, w4 = closure_experiment(R_hi=8, L_hi=64, R_lo=4, steps_hi=432, n_direct=32, return_weights=True)
+        res = ensemble_timing(weights=w4)
+        res["closure_r4"] = r4
+        print(json.dumps(res), flush=True)
         return 0
     if args.only == "bgk":
         print(json.dumps({"64": bgk_timing(64, 2000), "256": bgk_timing(256, 200), "512": bgk_timing(512, 40)}),
@@ -565,14 +586,13 @@ def only_region(args, local):
         return 0
     if args.only.startswith("colloid"):
         r = colloid_timing(args.only.split("-")[1], steps=max(1, args.steps) * 5, warm=args.warmup,
-                           small=args.only.endswith("small"), bulk=not args.per_thread_copies)
+                           small=args.only.endswith("small"))
         print(json.dumps(r), flush=True)
         return 0
     Lb = args.box
     rR, rB = seeded_noise_fields(Lb, Lb, Lb, seed=SEED)
     s = LBSim(make_params(Lb, model="cg", storage=args.only, sigma=SIGMA, beta=BETA))
     s.set_schedule(args.schedule)
-    s.set_lean_copies(not args.per_thread_copies)
     s.set_fields(rR, rB)
     s.step(args.warmup * args.lb_steps)
     s.sync()
@@ -580,7 +600,7 @@ def only_region(args, local):
     n = args.steps * args.lb_steps
     kus = (k / nl * 1e3) if nl else None
     print(json.dumps({"only": args.only, "box": Lb, "schedule": args.schedule,
-                      "copies": "per-thread" if args.per_thread_copies else "bulk", "ms_per_lattice_step": tot / n,
+                      "ms_per_lattice_step": tot / n,
                       "mlups": Lb ** 3 * n / (tot * 1e-3) / 1e6, "kernel_us": kus,
                       "frac_at_basis": (BYTES_PER_CELL[args.only] * Lb ** 3 / (kus * 1e-6) / 1e9 / peaks()[0])
                       if kus else None}), flush=True)
@@ -596,14 +616,12 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-extras", action="store_true", help="skip the error runs, the colloid case and the CPU baseline")
     ap.add_argument("--only", choices=["f16", "f32", "bf16", "f64", "f16sd", "bf16sd", "colloid-f16", "colloid-f32", "colloid-f16-small", "colloid-f16sd",
-                                       "colloid-f32-small", "ensemble", "closure", "closure12", "variants", "errors", "bgk",
+                                       "colloid-f32-small", "ensemble", "ensemble-closure", "closure", "closure12", "variants", "errors", "bgk",
                                        "bgk-256"],
                     help="profiling aid: run one timed region only and print its timing")
     ap.add_argument("--lb-steps", type=int, default=LB_PER_STEP, help="lattice steps per bench step")
     ap.add_argument("--schedule", type=int, default=2, help="colour-gradient schedule (0, 1, 2)")
     ap.add_argument("--box", type=int, default=L, help="lattice edge of the --only storage runs")
-    ap.add_argument("--per-thread-copies", action="store_true",
-                    help="lean kernel: per-thread cp.async pulls instead of bulk row copies")
     args = ap.parse_args()
     ws, rank, local = dist_env()
     if args.impl == "reference":
@@ -714,10 +732,17 @@ def main():
         extras["bgk"] = {"64": bgk_timing(64, 2000), "256": bgk_timing(256, 200), "512": bgk_timing(512, 40)}
         extras["colloid_256_1280"] = {st: colloid_timing(st) for st in ("f16sd", "f16", "f32")}
         extras["colloid_error_vs_f64"] = colloid_error_vs_f64()
-        extras["ensemble_48"] = ensemble_timing()
         extras["variants_128"] = {st: variants_timing(st) for st in ("f32", "f16")}
-        extras["closure"], w = closure_experiment(return_weights=True)
+        from lbcuda_b200 import closure as _cl
+        # the task's closure: radius-3 pairs against radius-12 resolved ones
+        extras["closure"], w = closure_experiment(R_hi=12, L_hi=96, steps_hi=960, return_weights=True)
+        extras["closure"]["window"] = _cl.window_score(w)
         extras["closure"]["suspension"] = closure_suspension(w)
+        # the ensemble's spheres have radius 4: its closure is trained at R_lo = 4 against R_hi = 8
+        r4, w4 = closure_experiment(R_hi=8, L_hi=64, R_lo=4, steps_hi=432, n_direct=32, return_weights=True)
+        extras["ensemble_48"] = ensemble_timing(weights=w4)
+        extras["ensemble_48"]["closure_r4"] = {k: r4[k] for k in ("R_hi", "R_lo", "classes", "train_samples",
+                                                                  "error_direct", "resistance_s", "train_s")}
         extras["cpu_baseline"] = cpu_baseline_sample()
 
     if rank == 0:

@@ -308,10 +308,6 @@ int lbx_set_schedule(void* ctx, int32_t fused);
 /* Lean single-pass kernel shape: 0 = 32x8 cells per CTA, 1 = 32x16; zlen =
  * lattice planes per z-segment (0 = automatic). */
 int lbx_set_lean_shape(void* ctx, int32_t shape, int32_t zlen);
-/* How the lean kernel moves 16-bit pulls into shared memory: 1 (default) =
- * bulk row copies on the TMA engine, one warp per plane, when nx % 4 == 0
- * (else as 0); 0 = per-thread 4-byte cp.async.  Both give the same bits. */
-int lbx_set_lean_copies(void* ctx, int32_t bulk);
 /* Enqueue nsteps steps bracketed by CUDA events on the context stream and
  * wait: total device ms, and the summed duration / launch count of the
  * step's dominant kernel (NULL kernel_ms disables per-kernel events). */

@@ -137,6 +137,28 @@ def sample_configs(n, seed=0, gap_range=(0.05, 1.5), vmax=1e-3):
     return [dict(gap=g, n=d, dv=a, oi=b, oj=c) for g, d, a, b, c in zip(gaps, dirs, dv, oi, oj)]
 
 
+def _pair_params(R, L, storage="f32", lubrication=False):
+    """lbx_params of the closure's two-sphere runs: frozen geometry (kinematic = 2), rotation, neutral
+    wetting, every template cell placed (exact_tiles = 0), Hertz only on overlap."""
+    return make_params(L, model="cg", storage=storage, max_particles=2, radius=float(R), kinematic=2,
+                       lrotate=1, wetting="neutral", max_vel=1.0,
+                       hz_rmin=float(2 * R - 0.5), hz_rcap=float(2 * R - 2.0),
+                       lubrication=1 if lubrication else 0, lubric_k=1.0 / 6.0, lubric_rmin=1.0,
+                       lubric_rcap=float(0.05 * R), exact_tiles=0)
+
+
+def _pair_state(cfg, L, mult=1):
+    """Centres, velocities and angular velocities (lab frame) of a pair configuration."""
+    d = np.asarray(cfg["d"], np.float64) * mult
+    E, sign, _ = lattice_frame(d / np.linalg.norm(d))
+    dv = E.T @ np.asarray(cfg["dv"], np.float64)
+    oi = sign * (E.T @ np.asarray(cfg["oi"], np.float64))
+    oj = sign * (E.T @ np.asarray(cfg["oj"], np.float64))
+    c = np.full(3, float(L // 2))
+    xj = (c + d - 1.0) % L + 1.0
+    return np.stack([c, xj]), np.stack([-0.5 * dv, 0.5 * dv]), np.stack([oi, oj])
+
+
 def run_pair(cfg, R, L, steps, average=0.25, storage="f32", lubrication=False, sim_cache=None, mult=1):
     """Forces / torques on both spheres of a prescribed-motion two-sphere run.
 
@@ -150,25 +172,11 @@ def run_pair(cfg, R, L, steps, average=0.25, storage="f32", lubrication=False, s
     (F_i, T_i, F_j, T_j) in the lab frame, averaged over the last `average`
     fraction of the steps, and the configuration (x, v, omega).
     """
-    d = np.asarray(cfg["d"], np.float64) * mult
-    E, sign, _ = lattice_frame(d / np.linalg.norm(d))
-    dv = E.T @ np.asarray(cfg["dv"], np.float64)
-    oi = sign * (E.T @ np.asarray(cfg["oi"], np.float64))
-    oj = sign * (E.T @ np.asarray(cfg["oj"], np.float64))
-    c = np.full(3, float(L // 2))
-    xj = (c + d - 1.0) % L + 1.0
-    x = np.stack([c, xj])
-    v = np.stack([-0.5 * dv, 0.5 * dv])
-    om = np.stack([oi, oj])
+    x, v, om = _pair_state(cfg, L, mult)
     key = (R, L, storage, lubrication)
     sim = sim_cache.get(key) if sim_cache is not None else None
     if sim is None:
-        p = make_params(L, model="cg", storage=storage, max_particles=2, radius=float(R), kinematic=2,
-                        lrotate=1, wetting="neutral", max_vel=1.0,
-                        hz_rmin=float(2 * R - 0.5), hz_rcap=float(2 * R - 2.0),
-                        lubrication=1 if lubrication else 0, lubric_k=1.0 / 6.0, lubric_rmin=1.0,
-                        lubric_rcap=float(0.05 * R), exact_tiles=0)
-        sim = LBSim(p)
+        sim = LBSim(_pair_params(R, L, storage, lubrication))
         if sim_cache is not None:
             sim_cache[key] = sim
     one = np.ones((L, L, L), np.float32)
@@ -182,6 +190,40 @@ def run_pair(cfg, R, L, steps, average=0.25, storage="f32", lubrication=False, s
         d = sim.get_particles()
         acc += np.stack([d["force"][0], d["torque"][0], d["force"][1], d["torque"][1]])
     return acc / nav, x, v, om
+
+
+def run_pairs(cfgs, R, L, steps, average=0.25, storage="f32", mult=1, mem_bytes=60e9):
+    """run_pair for many configurations: their boxes advance together, as many at a time as fit in
+    mem_bytes of device memory, in one ensemble (one persistent fluid kernel per step, the sphere
+    kernels of the boxes side by side); each box gives the bits of its own run_pair.  Returns the list
+    of (forces (4, 3), x, v, omega)."""
+    from .ensemble import Ensemble
+    nav = max(1, int(round(steps * average)))
+    per_box = L ** 3 * (19 * 2 * {"f32": 4, "f64": 8}.get(storage, 2) * 2 + 40)
+    batch = max(1, min(len(cfgs), int(mem_bytes // per_box)))
+    p = _pair_params(R, L, storage)
+    one = np.ones((L, L, L), np.float32)
+    zero = np.zeros_like(one)
+    out = []
+    for b0 in range(0, len(cfgs), batch):
+        chunk = cfgs[b0:b0 + batch]
+        ens = Ensemble([p] * len(chunk))
+        states = []
+        for box, cfg in zip(ens.boxes, chunk):
+            x, v, om = _pair_state(cfg, L, mult)
+            box.set_fields(one, zero)
+            box.set_particles(x, v, om, None)
+            states.append((x, v, om))
+        ens.step(steps - nav)
+        acc = np.zeros((len(chunk), 4, 3))
+        for _ in range(nav):
+            ens.step(1)
+            for i, box in enumerate(ens.boxes):
+                d = box.get_particles()
+                acc[i] += np.stack([d["force"][0], d["torque"][0], d["force"][1], d["torque"][1]])
+        ens.close()
+        out.extend((acc[i] / nav,) + states[i] for i in range(len(chunk)))
+    return out
 
 
 def _scales(R_hi, L_hi, R_lo, steps_hi, gap_range):
@@ -229,23 +271,23 @@ def generate(n_samples, R_hi=12, L_hi=128, R_lo=3, steps_hi=300, seed=0, progres
     X = np.zeros((n_samples, DIN))
     T = np.zeros((n_samples, DOUT))
     base = np.zeros((n_samples, DOUT))
-    cache = {}
+    z = np.zeros(3)
+    cfg_hi = [dict(c, oi=np.asarray(c["oi"]) * s, oj=np.asarray(c["oj"]) * s) for c in cfgs]
+    rest = [dict(c, dv=z, oi=z, oj=z) for c in cfgs]
+    hi = run_pairs(cfg_hi + (rest if subtract_static else []), R_hi, L_hi, steps_hi, mult=mult)
+    lo = run_pairs(cfgs + (rest if subtract_static else []), R_lo, L_lo, steps_lo)
     for k, cfg in enumerate(cfgs):
-        cfg_hi = dict(cfg, oi=np.asarray(cfg["oi"]) * s, oj=np.asarray(cfg["oj"]) * s)
-        hi, *_ = run_pair(cfg_hi, R_hi, L_hi, steps_hi, sim_cache=cache, mult=mult)
-        lo, x, v, om = run_pair(cfg, R_lo, L_lo, steps_lo, sim_cache=cache)
+        f_hi, f_lo = hi[k][0], lo[k][0]
+        x, v, om = lo[k][1:]
         if subtract_static:
-            rest = dict(cfg, dv=np.zeros(3), oi=np.zeros(3), oj=np.zeros(3))
-            hi = hi - run_pair(rest, R_hi, L_hi, steps_hi, sim_cache=cache, mult=mult)[0]
-            lo = lo - run_pair(rest, R_lo, L_lo, steps_lo, sim_cache=cache)[0]
+            f_hi = f_hi - hi[n_samples + k][0]
+            f_lo = f_lo - lo[n_samples + k][0]
         feat, (E, sign) = features(x[0], x[1], v[0], v[1], om[0], om[1], R_lo, (L_lo,) * 3)
         X[k] = feat
-        T[k] = to_pair(hi, E, sign) * _out_scale(s) - to_pair(lo, E, sign)
-        base[k] = to_pair(lo, E, sign)
+        T[k] = to_pair(f_hi, E, sign) * _out_scale(s) - to_pair(f_lo, E, sign)
+        base[k] = to_pair(f_lo, E, sign)
         if progress and (k + 1) % progress == 0:
             print(f"closure data {k + 1}/{n_samples}", flush=True)
-    for sim in cache.values():
-        sim.close()
     return X, T, dict(base=base, cfgs=cfgs, steps_hi=steps_hi, steps_lo=steps_lo, L_lo=L_lo)
 
 
@@ -265,26 +307,30 @@ def resistance(R_hi=12, L_hi=96, R_lo=3, steps_hi=960, gap_range=(0.05, 1.5), am
     C = len(classes)
     M_lo = np.zeros((C, DOUT, 9))
     M_hi = np.zeros((C, DOUT, 9))
-    cache = {}
     z = np.zeros(3)
-    for c, dcl in enumerate(classes):
+    # per class: the rest run and the nine unit-velocity runs, every class's runs advanced together
+    lo_cfgs, hi_cfgs = [], []
+    for dcl in classes:
         d = np.asarray(dcl, np.float64)
-        E, sign, _ = lattice_frame(d / np.linalg.norm(d))
-        rest = dict(d=d, dv=z, oi=z, oj=z)
-        r_lo = to_pair(run_pair(rest, R_lo, L_lo, steps_lo, sim_cache=cache)[0], E, sign)
-        r_hi = to_pair(run_pair(rest, R_hi, L_hi, steps_hi, sim_cache=cache, mult=mult)[0], E, sign)
+        lo_cfgs.append(dict(d=d, dv=z, oi=z, oj=z))
+        hi_cfgs.append(dict(d=d, dv=z, oi=z, oj=z))
         for k in range(9):
             e = np.zeros(9)
             e[k] = amp
-            lo = run_pair(dict(d=d, dv=e[:3], oi=e[3:6], oj=e[6:]), R_lo, L_lo, steps_lo, sim_cache=cache)[0]
-            hi = run_pair(dict(d=d, dv=e[:3], oi=e[3:6] * s, oj=e[6:] * s), R_hi, L_hi, steps_hi,
-                          sim_cache=cache, mult=mult)[0]
-            M_lo[c, :, k] = (to_pair(lo, E, sign) - r_lo) / amp
-            M_hi[c, :, k] = (to_pair(hi, E, sign) - r_hi) / amp * _out_scale(s)
+            lo_cfgs.append(dict(d=d, dv=e[:3], oi=e[3:6], oj=e[6:]))
+            hi_cfgs.append(dict(d=d, dv=e[:3], oi=e[3:6] * s, oj=e[6:] * s))
+    lo = run_pairs(lo_cfgs, R_lo, L_lo, steps_lo)
+    hi = run_pairs(hi_cfgs, R_hi, L_hi, steps_hi, mult=mult)
+    for c, dcl in enumerate(classes):
+        d = np.asarray(dcl, np.float64)
+        E, sign, _ = lattice_frame(d / np.linalg.norm(d))
+        r_lo = to_pair(lo[10 * c][0], E, sign)
+        r_hi = to_pair(hi[10 * c][0], E, sign)
+        for k in range(9):
+            M_lo[c, :, k] = (to_pair(lo[10 * c + 1 + k][0], E, sign) - r_lo) / amp
+            M_hi[c, :, k] = (to_pair(hi[10 * c + 1 + k][0], E, sign) - r_hi) / amp * _out_scale(s)
         if progress and (c + 1) % progress == 0:
             print(f"closure classes {c + 1}/{C}", flush=True)
-    for sim in cache.values():
-        sim.close()
     gap = np.array([np.linalg.norm(d) / R_lo - 2.0 for d in classes])
     return dict(classes=np.array(classes, np.float64), gap=gap, M_lo=M_lo, M_hi=M_hi, R_lo=float(R_lo),
                 R_hi=float(R_hi), steps_hi=steps_hi, steps_lo=steps_lo, L_lo=L_lo)
@@ -359,4 +405,106 @@ def analytic_lubrication(X, R, mu=1.0 / 6.0, rcut_gap=1.0, rcap_gap=None):
     f = np.where(h <= rcut_gap, lubfactor * (-dvn) * (1.0 / hh - 1.0), 0.0)
     out[:, 0] = -f
     out[:, 6] = f
+    return out
+
+
+def window_positions(L, n, R, seed=0, min_gap=0.05, tries=200000):
+    """n sphere centres of radius R on lattice sites of a periodic L^3 box, every centre distance at least
+    (2 + min_gap) R (random sequential placement)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    dmin2 = ((2.0 + min_gap) * R) ** 2
+    x = np.zeros((0, 3))
+    for _ in range(tries):
+        if len(x) == n:
+            break
+        c = rng.integers(1, L + 1, 3).astype(np.float64)
+        d = x - c
+        d -= L * np.round(d / L)
+        if not len(x) or (d * d).sum(1).min() >= dmin2:
+            x = np.vstack([x, c])
+    return x
+
+
+def _window_run(x, v, om, R, L, steps, average=0.25, closure=0, lubrication=0, weights=None):
+    """Frozen-geometry suspension run: the spheres' forces and torques averaged over the last steps,
+    and the ms per step."""
+    n = len(x)
+    p = make_params(L, model="cg", storage="f32", max_particles=n, radius=float(R), kinematic=2, lrotate=1,
+                    wetting="neutral", max_vel=1.0, hz_rmin=float(2 * R - 0.5), hz_rcap=float(2 * R - 2.0),
+                    lubrication=lubrication, lubric_k=1.0 / 6.0, lubric_rmin=1.0, lubric_rcap=float(0.05 * R),
+                    exact_tiles=0, closure=closure)
+    sim = LBSim(p)
+    if weights is not None:
+        wf = np.ascontiguousarray(weights, np.float32)
+        capi.check(capi.lib().lbx_closure_set(sim._h, _fp(wf)), "lbx_closure_set")
+    one = np.ones((L, L, L), np.float32)
+    sim.set_fields(one, np.zeros_like(one))
+    sim.set_particles(x, v, om, None)
+    nav = max(1, int(round(steps * average)))
+    sim.step(1)
+    sim.sync()
+    ms, _, _ = sim.time_steps(steps - nav - 1, kernel_timing=False)
+    F = np.zeros((n, 3))
+    T = np.zeros((n, 3))
+    for _ in range(nav):
+        sim.step(1)
+        d = sim.get_particles()
+        F += d["force"]
+        T += d["torque"]
+    code = sim.status()[0]
+    sim.close()
+    return F / nav, T / nav, ms / max(1, steps - nav - 1), code
+
+
+def window_score(w, L_lo=64, R_lo=3, scale=4, n=460, steps_lo=60, vmax=5e-4, seed=21, gap_max=1.5):
+    """A many-body check of the closure on a suspension window: n spheres of radius R_lo on lattice
+    sites of an L_lo^3 box (volume fraction about 0.2, gaps from 0.05 R), translational and angular
+    velocities uniform in +-vmax (frozen geometry, walls moving), and the same system resolved at
+    R_hi = scale * R_lo: centres times scale in a (scale L_lo)^3 box, scale^2 times the steps, angular
+    velocities divided by scale.  Each sphere's force and torque with motion minus those at rest,
+    resolved and scaled to R_lo (F s, T s^2, s = 1/scale), is the target; the R_lo run is scored plain,
+    with the reference's analytic lubrication, and with the closure (analytic outside its envelope).
+    Returns relative L2 errors over all spheres and over the spheres with a partner within gap_max R,
+    the median per-sphere error, the share within 5 %, and the cost of both resolutions."""
+    s = 1.0 / scale
+    rng = np.random.Generator(np.random.PCG64(seed + 1))
+    x = window_positions(L_lo, n, R_lo, seed)
+    n = len(x)
+    v = rng.uniform(-vmax, vmax, (n, 3))
+    om = rng.uniform(-vmax, vmax, (n, 3))
+    L_hi, R_hi, steps_hi = L_lo * scale, R_lo * scale, steps_lo * scale * scale
+    xh = scale * x
+    z = np.zeros_like(v)
+    Fm, Tm, ms_hi, c1 = _window_run(xh, v, om * s, R_hi, L_hi, steps_hi)
+    Fr, Tr, _, c2 = _window_run(xh, z, z, R_hi, L_hi, steps_hi)
+    tgt = np.concatenate([(Fm - Fr) * s, (Tm - Tr) * s * s], axis=1)
+    F0, T0, _, c3 = _window_run(x, z, z, R_lo, L_lo, steps_lo)
+    d = x[:, None, :] - x[None, :, :]
+    d -= L_lo * np.round(d / L_lo)
+    gap = np.sqrt((d * d).sum(-1)) / R_lo - 2.0
+    np.fill_diagonal(gap, np.inf)
+    close = (gap <= gap_max).any(axis=1)
+    out = {"box_lo": L_lo, "R_lo": R_lo, "box_hi": L_hi, "R_hi": R_hi, "spheres": n,
+           "volume_fraction": n * 4.0 / 3.0 * np.pi * R_lo ** 3 / L_lo ** 3, "steps_lo": steps_lo,
+           "steps_hi": steps_hi, "spheres_with_close_partner": int(close.sum()),
+           "close_pairs": int((gap[np.triu_indices(n, 1)] <= gap_max).sum()), "device_errors": [c1, c2, c3]}
+
+    def score(pred):
+        err = pred - tgt
+        per = np.linalg.norm(err[:, :3], axis=1) / np.maximum(np.linalg.norm(tgt[:, :3], axis=1), 1e-30)
+        return {"force_rel_l2": float(np.linalg.norm(err[:, :3]) / np.linalg.norm(tgt[:, :3])),
+                "force_rel_l2_close": float(np.linalg.norm(err[close, :3]) / np.linalg.norm(tgt[close, :3])),
+                "torque_rel_l2": float(np.linalg.norm(err[:, 3:]) / np.linalg.norm(tgt[:, 3:])),
+                "median_sphere": float(np.median(per)), "spheres_within_5pct": float(np.mean(per <= 0.05))}
+
+    runs = {"plain": dict(), "analytic_lubrication": dict(lubrication=1),
+            "closure": dict(closure=1, lubrication=1, weights=w)}
+    ms_lo = {}
+    for name, kw in runs.items():
+        F, T, ms, code = _window_run(x, v, om, R_lo, L_lo, steps_lo, **kw)
+        out[name] = score(np.concatenate([F - F0, T - T0], axis=1))
+        out[name]["device_error"] = code
+        ms_lo[name] = ms
+    out["ms_per_step"] = {"R_hi": ms_hi, "R_lo_closure": ms_lo["closure"], "R_lo_plain": ms_lo["plain"]}
+    out["cost_ratio_same_physical_time"] = ms_hi * steps_hi / (ms_lo["closure"] * steps_lo)
     return out

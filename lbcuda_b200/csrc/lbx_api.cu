@@ -454,13 +454,6 @@ int lbx_set_lean_shape(void* ctx, int32_t shape, int32_t zlen) {
   return 0;
 }
 
-int lbx_set_lean_copies(void* ctx, int32_t bulk) {
-  Ctx* c = as_ctx(ctx);
-  if (!c || bulk < 0 || bulk > 1) return LBX_ERR_ARG;
-  c->lean_bulk = bulk;
-  return 0;
-}
-
 /* Time nsteps steps on the context stream with CUDA events: total device
  * time in ms, and the summed duration of the step's dominant kernel (the
  * fused collide-stream kernel) with its launch count. */

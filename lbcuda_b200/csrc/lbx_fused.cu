@@ -1006,432 +1006,6 @@ __global__ void __launch_bounds__(TX* TY, MINB)
 }
 
 // ---------------------------------------------------------------------------
-// The same column march with the 16-bit pulls moved by the TMA engine.
-//
-// Every thread of lean_column computes 19 source addresses and issues 19
-// 4-byte cp.async per cell (and again for its ring cell): about an eighth of
-// the kernel's instructions.  Here one warp fills a plane's stage with bulk
-// copies (cp.async.bulk, completion on an mbarrier by transaction bytes): for
-// each direction l and each of the TY + 2 rows of the column and its ring, the
-// source row y - e_ly of direction plane l at z - e_lz, window
-// [x0 - 4, x0 + TX + 4) (16-byte aligned; split at the periodic x edge, so
-// the box needs nx % 4 == 0).  A thread finds direction l of its cell (cx, cy)
-// at row cy + 1, column cx + 4 - e_lx of that direction's box, so each pull is
-// a shared-memory load at a constant offset from one base address.
-//
-// Stage: three planes.  A plane is copied one iteration before it is summed
-// into densities and two before its collision; the last warp to finish the
-// collision of plane z (a shared counter) refills its slot with plane z + 3,
-// so no warp waits for a producer.  Each thread waits on the slot's mbarrier
-// (bounded, parity per slot) before its first read of a plane.  The densities
-// are summed in the order of lean_column, so both give the same bits.
-// ---------------------------------------------------------------------------
-template <int TX, int TY>
-struct BulkLayout {
-  static constexpr int RY = TY + 2;          // rows of a box: the column and its ring
-  static constexpr int PITCH = TX + 8;       // pairs per row: window [x0 - 4, x0 + TX + 4)
-  static constexpr int DIR = RY * PITCH;     // pairs per direction box
-  static constexpr int SLOT = Q * DIR;       // pairs per plane
-  static constexpr unsigned SLOT_BYTES = unsigned(SLOT) * 4u;
-  static constexpr int SLOTS = 3;
-  static constexpr int PER = 32 / RY;        // direction boxes per pass of the issuing warp
-  static_assert(TX % 4 == 0 && PER >= 1, "bulk rows: 16-byte windows, at most 32 rows per box");
-};
-
-__device__ __forceinline__ unsigned smem_u32(const void* p) { return static_cast<unsigned>(__cvta_generic_to_shared(p)); }
-__device__ __forceinline__ void mbar_arrive_expect_tx(unsigned long long* m, unsigned bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(m)), "r"(bytes) : "memory");
-}
-// bulk copy global -> this CTA's shared memory, completing on mbarrier m
-__device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned bytes, unsigned long long* m) {
-  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
-                   smem_u32(dst)),
-               "l"(src), "r"(bytes), "r"(smem_u32(m))
-               : "memory");
-}
-__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
-__device__ __forceinline__ unsigned long long globaltimer_ns() {
-  unsigned long long t;
-  asm volatile("mov.u64 %0, %%globaltimer;\n" : "=l"(t));
-  return t;
-}
-// wait for the completion of the phase of the given parity, at most about
-// limit_ns of wall time; false when the time ran out
-__device__ __forceinline__ bool mbar_wait_for(unsigned long long* m, unsigned parity, unsigned long long limit_ns) {
-  const unsigned a = smem_u32(m);
-  unsigned long long t0 = 0;
-  for (unsigned i = 1;; ++i) {
-    unsigned ok;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(ok)
-        : "r"(a), "r"(parity)
-        : "memory");
-    if (ok) return true;
-    if ((i & 31u) == 0u) {
-      const unsigned long long t = globaltimer_ns();
-      if (!t0) t0 = t;
-      else if (t - t0 > limit_ns) return false;
-    }
-  }
-}
-constexpr unsigned long long kWaitNs = 200000000ull;  // 200 ms: a stage or plane wait never takes this long
-__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory"); }
-
-// Shared memory of the bulk variant: phase-field window (2 planes), the
-// three-plane stage, the particle side records (as in LeanSmem, copied by
-// cp.async), the plane barrier, one completion barrier per stage slot and the
-// counter of warps done with a plane.
-template <typename S, int TX, int TY, bool PART>
-struct LeanSmemB {
-  using C = typename Store<S>::C;
-  using R = typename SPair<S>::R;
-  using BL = BulkLayout<TX, TY>;
-  static constexpr int NT = TX * TY, RN = Ring<TX, TY>::N, CELLS = Ring<TX, TY>::CELLS;
-  static constexpr size_t PHI = (sizeof(C) * 2 * CELLS + 15) / 16 * 16;
-  static constexpr size_t STG = size_t(BL::SLOTS) * BL::SLOT_BYTES;
-  static constexpr size_t SIDE = PART ? (sizeof(SideRec<C>) * (3 * NT + 2 * RN) + 15) / 16 * 16 : 0;
-  static constexpr size_t BAR = 64;
-  static constexpr size_t BYTES = PHI + STG + SIDE + BAR;
-  static_assert(sizeof(R) == 4 && STG % 16 == 0, "16-bit pairs");
-  static __device__ __forceinline__ C (*phi(unsigned char* base))[CELLS] { return reinterpret_cast<C(*)[CELLS]>(base); }
-  static __device__ __forceinline__ R* stage(unsigned char* base) { return reinterpret_cast<R*>(base + PHI); }
-  static __device__ __forceinline__ SideRec<C>* side(unsigned char* base) {
-    return PART ? reinterpret_cast<SideRec<C>*>(base + PHI + STG) : nullptr;
-  }
-  static __device__ __forceinline__ unsigned long long* bars(unsigned char* base) {
-    return reinterpret_cast<unsigned long long*>(base + PHI + STG + SIDE);  // [0] plane, [1..3] slots
-  }
-  static __device__ __forceinline__ int* counter(unsigned char* base) {
-    return reinterpret_cast<int*>(base + PHI + STG + SIDE + 32);
-  }
-  static __device__ __forceinline__ void init(unsigned char* base) {
-    if (threadIdx.x == 0 && threadIdx.y == 0) {
-      mbar_init(bars(base), TX * TY);
-      for (int s = 0; s < BL::SLOTS; ++s) mbar_init(bars(base) + 1 + s, 1);
-      *counter(base) = 0;
-      fence_mbar_init();
-    }
-  }
-};
-
-// densities (Sum g + rho0, before the clamp) of one cell from a bulk stage:
-// direction l at base[l * DIR - e_lx]; the order and roundings of stage_rho
-template <typename S, typename C, int DIR, bool SD>
-__device__ __forceinline__ void stage_rho_b(const typename SPair<S>::R* base, const LeanConst<C>& K, C& rR, C& rB) {
-  P2<C> s = SPair<S>::cvt(base[0]);
-#pragma unroll
-  for (int l = 1; l < Q; ++l) {
-    const typename SPair<S>::R r = base[l * DIR - ex(l)];
-    s.x = add_mixed(r.x, s.x);
-    s.y = add_mixed(r.y, s.y);
-  }
-  if constexpr (SD) {
-    const C rho = s.x + K.rho0sd[0], dif = s.y + K.rho0sd[1];
-    rR = C(0.5) * (rho + dif);
-    rB = C(0.5) * (rho - dif);
-  } else {
-    rR = s.x + K.rho0[0];
-    rB = s.y + K.rho0[1];
-  }
-}
-
-// One warp copies plane p (every direction box) into stage slot `dst` and
-// arms barrier `fb` with the plane's bytes.  All 32 lanes call it.
-template <typename S, int TX, int TY>
-__device__ __forceinline__ void bulk_plane(const S* __restrict__ A, const Geom& g, int x0, int y0, int p,
-                                           typename SPair<S>::R* dst, unsigned long long* fb) {
-  using BL = BulkLayout<TX, TY>;
-  const int lane = threadIdx.x & 31;
-  if (lane == 0) mbar_arrive_expect_tx(fb, BL::SLOT_BYTES);
-  __syncwarp();
-  fence_proxy_async();
-  const int sub = lane / BL::RY, r = lane - sub * BL::RY;
-  const size_t plane = size_t(g.nx) * size_t(g.ny);
-#pragma unroll
-  for (int l0 = 0; l0 < Q; l0 += BL::PER) {
-    // direction l0 + sub, its offsets chosen among compile-time constants
-    int l = l0, dx = ex(l0), dy = ey(l0), dz = ez(l0);
-#pragma unroll
-    for (int k = 1; k < BL::PER; ++k)
-      if (sub == k && l0 + k < Q) {
-        l = l0 + k;
-        dx = ex(l0 + k);
-        dy = ey(l0 + k);
-        dz = ez(l0 + k);
-      }
-    (void)dx;
-    if (sub >= BL::PER || l0 + sub >= Q) continue;
-    const int sy = wrap0(y0 - 1 - dy + r, g.ny);
-    const int sz = wrap_plane(p - dz, g.nz);
-    const S* row = A + 2 * (size_t(l) * size_t(g.n) + size_t(sz) * plane + size_t(sy) * size_t(g.nx));
-    typename SPair<S>::R* d = dst + l * BL::DIR + r * BL::PITCH;
-    int x = x0 - 4, off = 0;
-    while (off < BL::PITCH) {  // periodic x edge: at most a few segments
-      const int xm = wrap0(x, g.nx);
-      const int len = min(BL::PITCH - off, g.nx - xm);
-      bulk_load(d + off, row + 2 * size_t(xm), unsigned(len) * 4u, fb);
-      off += len;
-      x += len;
-    }
-  }
-}
-
-template <typename S, int TX, int TY, bool PART, bool SD = false>
-__device__ __forceinline__ void lean_column_bulk(const S* __restrict__ A, S* __restrict__ B, const Geom& g,
-                                                 const LeanConst<typename Store<S>::C>& K, int x0, int y0, int z0,
-                                                 int zend, unsigned long long* err, int64_t step,
-                                                 const LeanPart<typename Store<S>::C>& PT,
-                                                 typename Store<S>::C (*sphi)[Ring<TX, TY>::CELLS],
-                                                 typename SPair<S>::R* stage, SideRec<typename Store<S>::C>* side,
-                                                 unsigned long long* bars, int* done, unsigned& bar_parity,
-                                                 unsigned& slot_parity) {
-  using C = typename Store<S>::C;
-  using SR = typename SPair<S>::R;
-  using BL = BulkLayout<TX, TY>;
-  constexpr int NT = TX * TY;
-  constexpr int NW = NT / 32;
-  using R = Ring<TX, TY>;
-  constexpr int RN = R::N;
-  unsigned long long* const bar = bars;
-  unsigned long long* const full = bars + 1;
-  const bool parts = PART && PT.fnew != nullptr;
-  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
-  const int warp = tid >> 5, lane = tid & 31;
-  const bool active = (x0 + tx < g.nx) && (y0 + ty < g.ny);
-  const int x = wrap0(x0 + tx, g.nx), y = wrap0(y0 + ty, g.ny);
-  const int own = (ty + 1) * R::RX + (tx + 1);
-  int rx = 0, ry = 0;
-  const bool ringer = tid < R::N;
-  if (tid < R::RX) { rx = tid; ry = 0; }
-  else if (tid < 2 * R::RX) { rx = tid - R::RX; ry = R::RY - 1; }
-  else if (tid < 2 * R::RX + TY) { rx = 0; ry = 1 + tid - 2 * R::RX; }
-  else { rx = R::RX - 1; ry = 1 + tid - 2 * R::RX - TY; }
-  const int rxg = wrap0(x0 + rx - 1, g.nx), ryg = wrap0(y0 + ry - 1, g.ny);
-  const int rslot = ry * R::RX + rx;
-  SideRec<C>* const side_ring = PART ? side + 3 * NT : nullptr;
-  const Planes<S> Bp{B, 2 * g.n};
-
-  auto slot_of = [&](int p) { return (p - z0 + 1) % BL::SLOTS; };
-  // this thread's cell and ring cell in the box of direction 0 of plane p
-  auto own_base = [&](int p) { return stage + slot_of(p) * BL::SLOT + (ty + 1) * BL::PITCH + tx + 4; };
-  auto ring_base = [&](int p) { return stage + slot_of(p) * BL::SLOT + ry * BL::PITCH + rx + 3; };
-  auto own_q = [&](int p) { return (p - z0 + 1) % 3; };
-  auto ring_q = [&](int p) { return (p - z0 + 1) & 1; };
-
-  auto copy_plane = [&](int p) {  // by one whole warp
-    const int s = slot_of(p);
-    bulk_plane<S, TX, TY>(A, g, x0, y0, p, stage + s * BL::SLOT, full + s);
-  };
-  // particle side records of plane p (per thread, cp.async, one group per call)
-  auto issue_side = [&](int p) {
-    if constexpr (PART) {
-      if (parts) {
-        const int zz = wrap_plane(p, g.nz);
-        const unsigned co = unsigned(x) + unsigned(g.nx) * (unsigned(y) + unsigned(g.ny) * unsigned(zz));
-        SideRec<C>* so = side + own_q(p) * NT + tid;
-        cp_async4(&so->fnew_w, PT.fnew + size_t(co & ~3u));
-        cp_async4(&so->fold_w, PT.fold + size_t(co & ~3u));
-        cp_async_c(&so->phi, PT.phi + size_t(co));
-        if (ringer) {
-          const unsigned cr = unsigned(rxg) + unsigned(g.nx) * (unsigned(ryg) + unsigned(g.ny) * unsigned(zz));
-          SideRec<C>* sr = side_ring + ring_q(p) * RN + tid;
-          cp_async4(&sr->fnew_w, PT.fnew + size_t(cr & ~3u));
-          cp_async4(&sr->fold_w, PT.fold + size_t(cr & ~3u));
-          cp_async_c(&sr->phi, PT.phi + size_t(cr));
-        }
-      }
-      cp_async_commit();
-    }
-  };
-  // before the first read of plane p: its bulk copies (and the side records
-  // of every plane but the newest group) have landed
-  // after a wait that ran out (an error already raised) the others are skipped,
-  // so the kernel ends promptly with the error word set
-  bool dead = false;
-  auto land = [&](int p) {
-    if constexpr (PART) cp_async_wait<1>();
-    const int s = slot_of(p);
-    if (!dead && !mbar_wait_for(full + s, (slot_parity >> s) & 1u, kWaitNs)) {
-      dead = true;
-      raise_error(err, LBX_DEV_WAIT_TIMEOUT, step, -1);
-    }
-    slot_parity ^= 1u << s;
-  };
-  auto flags_of = [&](const SideRec<C>* r, int cell, int8_t& fn, int8_t& fo) {
-    const int sh = 8 * (cell & 3);
-    fn = int8_t((r->fnew_w >> sh) & 255u);
-    fo = int8_t((r->fold_w >> sh) & 255u);
-  };
-  auto cell_phase = [&](int cx, int cy, int zz, bool check, bool is_own, const SR* base, const SideRec<C>* rec,
-                        C& rR, C& rB) -> C {
-    const int cell = cx + g.nx * (cy + g.ny * zz);
-    if constexpr (PART) {
-      if (parts) {
-        int8_t fn, fo;
-        flags_of(rec, cell, fn, fo);
-        if (fn != LBX_FLUID_FLUID || fo != LBX_FLUID_FLUID) {
-          rR = C(0);
-          rB = C(0);
-          if (fn == LBX_FLUID_SPHERELIST) return rec->phi;
-          if (fn == LBX_FLUID_FLUID) {
-            if (is_own) {
-              rR = PT.rhoR[size_t(unsigned(cell))];
-              rB = PT.rhoB[size_t(unsigned(cell))];
-            }
-            return rec->phi;
-          }
-          return phase_of(rR, rB);
-        }
-      }
-    }
-    stage_rho_b<S, C, BL::DIR, SD>(base, K, rR, rB);
-    if (check && (rR < C(-10) || rR > C(10) || rB < C(-10) || rB > C(10)))
-      raise_error(err, LBX_DEV_RHO_RANGE, step, cell);
-    rR = clamp0(rR);
-    rB = clamp0(rB);
-    return phase_of(rR, rB);
-  };
-  auto phase_plane = [&](int p, C& rRo, C& rBo) {
-    const int zz = wrap_plane(p, g.nz);
-    const bool owned = active && p >= z0 && p < zend;
-    const SideRec<C>* so = PART ? side + own_q(p) * NT + tid : nullptr;
-    sphi[p & 1][own] = cell_phase(x, y, zz, owned, true, own_base(p), so, rRo, rBo);
-    if (ringer) {
-      C qR, qB;
-      const SideRec<C>* sr = PART ? side_ring + ring_q(p) * RN + tid : nullptr;
-      sphi[p & 1][rslot] = cell_phase(rxg, ryg, zz, false, false, ring_base(p), sr, qR, qB);
-    }
-  };
-
-  // prologue: planes z0 - 1, z0, z0 + 1 into the three slots
-  if (warp == 0) {
-    copy_plane(z0 - 1);
-    copy_plane(z0);
-    if (z0 + 1 <= zend) copy_plane(z0 + 1);
-  }
-  issue_side(z0 - 1);
-  issue_side(z0);
-  C rRn, rBn, rRc, rBc;
-  land(z0 - 1);
-  phase_plane(z0 - 1, rRc, rBc);
-  issue_side(z0 + 1);
-  land(z0);
-  phase_plane(z0, rRn, rBn);
-  __syncthreads();  // planes z0-1 and z0 of the window; slot of z0 - 1 free
-  PlaneGrad<C> gm{}, g0{};
-  if (active) {
-    gm = plane_grad<C, R::RX>(sphi[(z0 + 1) & 1], own);
-    g0 = plane_grad<C, R::RX>(sphi[z0 & 1], own);
-  }
-  if (warp == 0 && z0 + 2 <= zend) copy_plane(z0 + 2);
-  __syncthreads();  // the window slot of plane z0-1 is rewritten in the first iteration
-  for (int z = z0; z < zend; ++z) {
-    rRc = rRn;
-    rBc = rBn;
-    if (z + 2 <= zend) issue_side(z + 2);
-    else if constexpr (PART) cp_async_commit();
-    land(z + 1);
-    phase_plane(z + 1, rRn, rBn);
-    mbar_arrive(bar);
-    const int cell = x + g.nx * (y + g.ny * z);
-    bool collide = true, fresh = false;
-    C px = 0, py = 0, pz = 0;
-    Relaxed<C> rlx;
-    if (active) {
-      if constexpr (PART) {
-        if (parts) {
-          int8_t fn, fo;
-          flags_of(side + own_q(z) * NT + tid, cell, fn, fo);
-          collide = fn == LBX_FLUID_FLUID;
-          fresh = collide && fo != LBX_FLUID_FLUID;
-        }
-      }
-    }
-    const SR* ob = own_base(z);
-    auto pulled = [&](int l) -> SR { return ob[l * BL::DIR - ex(l)]; };
-    auto refilled = [&](int l) -> SR { return SPair<S>::ldr(Bp.at(l, cell)); };
-    if (active && collide) {
-      C Ssum[Q];
-#pragma unroll
-      for (int l = 0; l < Q; ++l) Ssum[l] = SD ? SPair<S>::first(pulled(l)) : SPair<S>::sum(pulled(l));
-      if constexpr (PART) {
-        if (fresh) {
-#pragma unroll
-          for (int l = 0; l < Q; ++l) Ssum[l] = SD ? SPair<S>::first(refilled(l)) : SPair<S>::sum(refilled(l));
-        }
-      }
-      rlx = relax_sums(K, Ssum, rRc, rBc, Store<S>::shifted);
-    }
-    if (!dead && !mbar_wait_for(bar, bar_parity, kWaitNs)) {
-      dead = true;
-      raise_error(err, LBX_DEV_WAIT_TIMEOUT, step, -1);
-    }
-    bar_parity ^= 1u;
-    if (active) {
-      P2<C> gp[Q];
-      bool fin = false;
-      const PlaneGrad<C> gpl = plane_grad<C, R::RX>(sphi[(z + 1) & 1], own);
-      if (collide) {
-        const C H0 = C(1) / C(3), H1 = C(1) / C(12), HALF = C(0.5);
-        px = fm(H0, g0.gx, H1 * (gm.gx + gpl.gx));
-        py = fm(H0, g0.gy, H1 * (gm.gy + gpl.gy));
-        pz = HALF * (gpl.m - gm.m);
-      }
-      gm = g0;
-      g0 = gpl;
-      if (collide) fin = recolour_sums<C, SD>(K, rlx, rRc, rBc, px, py, pz, Store<S>::shifted, gp);
-      if (!fin) {
-#pragma unroll
-        for (int l = 0; l < Q; ++l) gp[l] = SPair<S>::cvt(pulled(l));
-        if constexpr (PART) {
-          if (fresh) {
-#pragma unroll
-            for (int l = 0; l < Q; ++l) gp[l] = SPair<S>::cvt(refilled(l));
-          }
-        }
-        if (collide) {
-          if constexpr (SD) bgk_components<C, true, true>(K, rlx, rRc + rBc, rRc - rBc, Store<S>::shifted, gp);
-          else bgk_components<C, true>(K, rlx, rRc, rBc, Store<S>::shifted, gp);
-        }
-      }
-#pragma unroll
-      for (int l = 0; l < Q; ++l) SPair<S>::st(Bp.at(l, cell), gp[l]);
-    }
-    // this warp is done with the stage slot of plane z; the last warp to be
-    // done refills it with plane z + 3
-    __syncwarp();
-    int last = 0;
-    if (lane == 0) {
-      __threadfence_block();
-      last = atomicAdd(done, 1) == NW - 1;
-      if (last) {
-        atomicExch(done, 0);
-        __threadfence_block();
-      }
-    }
-    last = __shfl_sync(0xffffffffu, last, 0);
-    if (last && z + 3 <= zend) copy_plane(z + 3);
-  }
-  if constexpr (PART) cp_async_wait<0>();  // nothing in flight when the shared memory is reused
-}
-
-template <typename S, int TX, int TY, int MINB, bool PART, bool SD = false>
-__global__ void __launch_bounds__(TX* TY, MINB)
-    k_cg_lean_bulk(const S* __restrict__ A, S* __restrict__ B, Geom g, LeanConst<typename Store<S>::C> K, int zlen,
-                   unsigned long long* err, int64_t step, LeanPart<typename Store<S>::C> PT) {
-  extern __shared__ __align__(16) unsigned char lean_smem[];
-  using M = LeanSmemB<S, TX, TY, PART>;
-  M::init(lean_smem);
-  __syncthreads();
-  unsigned parity = 0, slots = 0;
-  const int z0 = blockIdx.z * zlen;
-  lean_column_bulk<S, TX, TY, PART, SD>(A, B, g, K, blockIdx.x * TX, blockIdx.y * TY, z0, min(z0 + zlen, g.nz), err,
-                                        step, PT, M::phi(lean_smem), M::stage(lean_smem), M::side(lean_smem),
-                                        M::bars(lean_smem), M::counter(lean_smem), parity, slots);
-}
-
-// ---------------------------------------------------------------------------
 // Several independent boxes in one persistent launch: each CTA takes work
 // items (box, column, z-segment) from a table, longest first, and marches
 // them like k_cg_lean.  Used by the ensemble of uneven boxes.
@@ -1548,48 +1122,6 @@ static int launch_lean(Ctx& c, int zlen_override, LeanPart<typename Store<S>::C>
   return 0;
 }
 
-template <typename S, int TX, int TY, int MINB, bool PART, bool SD = false>
-static int prepare_lean_bulk(int* resident) {
-  static unsigned long long done = 0;
-  static int per_sm[64] = {0}, sms[64] = {0};
-  int rc = allow_smem(k_cg_lean_bulk<S, TX, TY, MINB, PART, SD>, LeanSmemB<S, TX, TY, PART>::BYTES, done);
-  if (rc) return rc;
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess) return LBX_ERR_CUDA;
-  dev &= 63;
-  if (!per_sm[dev]) {
-    int nb = 0, nsm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_cg_lean_bulk<S, TX, TY, MINB, PART, SD>, TX * TY,
-                                                      LeanSmemB<S, TX, TY, PART>::BYTES) != cudaSuccess ||
-        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || nb < 1 || nsm < 1)
-      return LBX_ERR_CUDA;
-    sms[dev] = nsm;
-    per_sm[dev] = nb;
-  }
-  *resident = per_sm[dev] * sms[dev];
-  return 0;
-}
-
-// the bulk-copy variant for 16-bit pairs: its 16-byte row windows need nx % 4 == 0
-template <typename S>
-static bool use_bulk(const Ctx& c) {
-  return sizeof(typename SPair<S>::R) == 4 && c.nx % 4 == 0 && c.lean_bulk;
-}
-
-template <typename S, int TX, int TY, int MINB, bool PART, bool SD = false>
-static int launch_lean_bulk(Ctx& c, int zlen_override, LeanPart<typename Store<S>::C> pt) {
-  using C = typename Store<S>::C;
-  int resident = 0;
-  const int rc = prepare_lean_bulk<S, TX, TY, MINB, PART, SD>(&resident);
-  if (rc) return rc;
-  const int zlen = zlen_override > 0 ? zlen_override : lean_zlen(c, TX, TY, resident);
-  dim3 block(TX, TY, 1);
-  dim3 grid((c.nx + TX - 1) / TX, (c.ny + TY - 1) / TY, (c.nz + zlen - 1) / zlen);
-  k_cg_lean_bulk<S, TX, TY, MINB, PART, SD><<<grid, block, LeanSmemB<S, TX, TY, PART>::BYTES, c.stream>>>(
-      (const S*)c.pops[c.cur], (S*)c.pops[1 - c.cur], geom(c), make_lean<C>(c), zlen, c.d_err, c.step + 1, pt);
-  return 0;
-}
-
 void kt_begin(Ctx& c);
 void kt_end(Ctx& c);
 
@@ -1606,9 +1138,6 @@ int fluid_lean(Ctx& c) {
     } else if constexpr (std::is_same<S, float>::value) {
       if (c.lean_shape == 1) r = launch_lean<S, 32, 16, 1, false>(c, c.lean_zlen, none);
       else r = launch_lean<S, 32, 8, 2, false>(c, c.lean_zlen, none);
-    } else if (use_bulk<S>(c) && c.lean_shape == 0) {  // 16-bit pairs moved by bulk copies
-      if (c.sd) r = launch_lean_bulk<S, 32, 8, 2, false, true>(c, c.lean_zlen, none);
-      else r = launch_lean_bulk<S, 32, 8, 2, false>(c, c.lean_zlen, none);
     } else if (c.sd) {  // sum / difference pairs
       if (c.lean_shape == 1) r = launch_lean<S, 32, 16, 1, false, true>(c, c.lean_zlen, none);
       else r = launch_lean<S, 32, 8, 2, false, true>(c, c.lean_zlen, none);
@@ -1633,8 +1162,6 @@ int fluid_lean_particles(Ctx& c, int fo, int fn) {
     int r = 0;
     if constexpr (std::is_same<S, double>::value) r = launch_lean<S, 32, 8, 1, true>(c, c.lean_zlen, pt);
     else if constexpr (std::is_same<S, float>::value) r = launch_lean<S, 32, 8, 2, true>(c, c.lean_zlen, pt);
-    else if (use_bulk<S>(c) && c.sd) r = launch_lean_bulk<S, 32, 8, 2, true, true>(c, c.lean_zlen, pt);
-    else if (use_bulk<S>(c)) r = launch_lean_bulk<S, 32, 8, 2, true>(c, c.lean_zlen, pt);
     else if (c.sd) r = launch_lean<S, 32, 8, 2, true, true>(c, c.lean_zlen, pt);
     else r = launch_lean<S, 32, 8, 2, true>(c, c.lean_zlen, pt);
     kt_end(c);

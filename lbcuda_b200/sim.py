@@ -122,10 +122,6 @@ class LBSim:
     def set_lean_shape(self, shape, zlen=0):
         check(self._L.lbx_set_lean_shape(self._h, int(shape), int(zlen)), "lbx_set_lean_shape")
 
-    def set_lean_copies(self, bulk):
-        """16-bit pulls of the lean kernel by bulk copies (True, default) or per-thread cp.async (False)."""
-        check(self._L.lbx_set_lean_copies(self._h, 1 if bulk else 0), "lbx_set_lean_copies")
-
     def time_steps(self, n, kernel_timing=True):
         """(total_ms, kernel_ms, kernel_launches) of n steps, CUDA events on the context stream."""
         t = C.c_double()

@@ -286,3 +286,17 @@ def test_trained_closure_beats_plain_method_on_held_out_pairs():
     net = np.linalg.norm((Th - closure.infer(w, Xh))[:, f]) / hi
     print(f"held-out pair-force error: none {none:.3f} analytic {lub:.3f} closure {net:.3f}; loss {loss[-1]:.2e}")
     assert net < 0.5 * min(none, lub)
+
+
+@pytest.mark.gpu
+def test_batched_pair_runs_equal_single_runs():
+    """run_pairs (boxes advanced together in one ensemble) gives each configuration the bits of run_pair."""
+    from lbcuda_b200 import closure
+    z = np.zeros(3)
+    cfgs = [dict(d=np.array([7.0, 1.0, 0.0]), dv=np.array([1e-3, 0, 0]), oi=z, oj=z),
+            dict(d=np.array([6.0, 3.0, 2.0]), dv=z, oi=np.array([0, 5e-4, 0]), oj=z),
+            dict(d=np.array([8.0, 0.0, 0.0]), dv=z, oi=z, oj=z)]
+    batched = closure.run_pairs(cfgs, 3, 24, 40)
+    for cfg, b in zip(cfgs, batched):
+        single = closure.run_pair(cfg, 3, 24, 40)
+        assert np.array_equal(b[0], single[0])
