@@ -37,8 +37,9 @@ LB_PER_STEP = 500
 # DRAM bytes (read + write) of one k_cg_lean launch at 128^3, from the ncu
 # captures summarised in profiles/ (None where no capture of that storage)
 TRAFFIC = {"f16": 292.7e6, "f16sd": 292.0e6, "f32": 622.6e6}
-BYTES_PER_CELL = {"f16": 160, "bf16": 160, "f16sd": 160, "bf16sd": 160, "f32": 312, "f64": 616}  # algorithmic bytes per cell-step
-MINIMAL_BYTES = {"f16": 152, "bf16": 152, "f16sd": 152, "f32": 304, "f64": 608}   # populations only (phi on chip)
+BYTES_PER_CELL = {"f16": 160, "bf16": 160, "f16sd": 160, "bf16sd": 160, "f16sdp": 160, "bf16sdp": 160, "f32": 312,
+                  "f64": 616}  # algorithmic bytes per cell-step
+MINIMAL_BYTES = {"f16": 152, "bf16": 152, "f16sd": 152, "f16sdp": 160, "f32": 304, "f64": 608}  # bytes the kernel must move
 METRIC = "MLUPS & HBM GB/s, FP16-store vs FP32 LB at stated FP64 error, 1\u00d7B200"
 
 
@@ -214,7 +215,7 @@ def error_vs_f64(nsteps_list=(100, 1000, 10000), workload="spinodal"):
         rR, rB = seeded_noise_fields(L, L, L, seed=SEED)
     out = {"workload": workload}
     sims = {}
-    for st in ("f64", "f32", "f16", "bf16", "f16sd", "bf16sd"):
+    for st in ("f64", "f32", "f16", "bf16", "f16sd", "bf16sd", "f16sdp", "bf16sdp"):
         s = LBSim(make_params(L, model="cg", storage=st, sigma=SIGMA, beta=BETA))
         s.set_fields(rR, rB, vel)
         sims[st] = s
@@ -227,7 +228,7 @@ def error_vs_f64(nsteps_list=(100, 1000, 10000), workload="spinodal"):
         done = n
         u64, p64 = res["f64"][2], res["f64"][3]
         m64 = res["f64"][0].sum() + res["f64"][1].sum()
-        for st in ("f32", "f16", "bf16", "f16sd", "bf16sd"):
+        for st in ("f32", "f16", "bf16", "f16sd", "bf16sd", "f16sdp", "bf16sdp"):
             eu = float(np.linalg.norm(res[st][2] - u64) / np.linalg.norm(u64))
             ep = float(np.linalg.norm(res[st][3] - p64) / np.linalg.norm(p64))
             out.setdefault(st, {})[f"after_{n}"] = {"u_rel_l2": eu, "phi_rel_l2": ep}
@@ -615,7 +616,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-extras", action="store_true", help="skip the error runs, the colloid case and the CPU baseline")
-    ap.add_argument("--only", choices=["f16", "f32", "bf16", "f64", "f16sd", "bf16sd", "colloid-f16", "colloid-f32", "colloid-f16-small", "colloid-f16sd",
+    ap.add_argument("--only", choices=["f16", "f32", "bf16", "f64", "f16sd", "bf16sd", "f16sdp", "bf16sdp", "colloid-f16", "colloid-f32", "colloid-f16-small", "colloid-f16sd",
                                        "colloid-f32-small", "ensemble", "ensemble-closure", "closure", "closure12", "variants", "errors", "bgk",
                                        "bgk-256"],
                     help="profiling aid: run one timed region only and print its timing")
@@ -670,16 +671,18 @@ def main():
     tot16, k16, n16, clocks, code16 = run_storage("f16sd", args.steps, args.warmup)
     tot32, k32, n32, _, code32 = run_storage("f32", args.steps, args.warmup)
     totrb, krb, nrb, _, coderb = run_storage("f16", args.steps, args.warmup)
+    totsp, ksp, nsp, _, codesp = run_storage("f16sdp", args.steps, args.warmup)
 
     def maxr(v):
         return max_over_ranks(v, pg, "cuda")
 
-    tot16, tot32, totrb = maxr(tot16), maxr(tot32), maxr(totrb)
+    tot16, tot32, totrb, totsp = maxr(tot16), maxr(tot32), maxr(totrb), maxr(totsp)
     cells = L ** 3
     lb_steps = args.steps * LB_PER_STEP
     mlups16 = ws * cells * lb_steps / (tot16 * 1e-3) / 1e6
     mlups32 = ws * cells * lb_steps / (tot32 * 1e-3) / 1e6
     mlupsrb = ws * cells * lb_steps / (totrb * 1e-3) / 1e6
+    mlupssp = ws * cells * lb_steps / (totsp * 1e-3) / 1e6
 
     def roofline(storage, kernel_ms, launches):
         per_launch_ms = kernel_ms / max(launches, 1)
@@ -761,6 +764,10 @@ def main():
             "f16_component_pairs": {"value": mlupsrb, "unit": "MLUPS", "ms_per_step": totrb / args.steps,
                                     "storage": "f16 (R - w rho0R, B - w rho0B) pairs",
                                     "roofline": roofline("f16", krb, nrb), "over_fp32": mlupsrb / mlups32},
+            "f16_predicted_split": {"value": mlupssp, "unit": "MLUPS", "ms_per_step": totsp / args.steps,
+                                    "storage": "f16 (total, colour difference less the receiving cell's predicted "
+                                               "split) pairs + an FP32 phase field per cell",
+                                    "roofline": roofline("f16sdp", ksp, nsp), "over_fp32": mlupssp / mlups32},
             "clocks": clocks,
             "e2e": {"value": e2e_mlups, "unit": "MLUPS", "h2d_bytes_per_step": 2 * 19 * 4 * cells,
                     "d2h_bytes_per_step": 2 * 19 * 4 * cells, "ms_per_step": e2e_ms / args.steps,
@@ -768,7 +775,7 @@ def main():
                               "lbx_get_pops of the full FP32 state, one continuous trajectory), max over ranks",
                     "gpu_launches_per_step": LB_PER_STEP + 2},
             "gpu_launches": n16,
-            "device_errors": [code16, code32, coderb],
+            "device_errors": [code16, code32, coderb, codesp],
         }
         line.update(extras)
         if extras:

@@ -63,6 +63,18 @@ extern "C" {
  * see f_R and f_B. */
 #define LBX_STORE_F16_SD 4
 #define LBX_STORE_BF16_SD 5
+/* 16-bit sum / predicted-split pairs (no counterpart in the reference): the
+ * total as in LBX_STORE_F16_SD, and in place of the colour difference
+ * D = f_R - f_B its deviation from the split the receiving cell predicts,
+ * E = D - phi_y (f_R + f_B), phi_y the phase field of the cell y that will
+ * pull the pair, from the step in which the pair was written (an FP32 value
+ * per cell, kept beside each population buffer).  In the bulk of either
+ * fluid E is only the small recolouring term, so its rounding no longer
+ * stirs the flow.  Colour-gradient model on the single-pass schedule without
+ * spheres (lbx_create rejects max_particles > 0, the ensemble rejects it);
+ * the population and field calls convert as for the other formats. */
+#define LBX_STORE_F16_SDP 6
+#define LBX_STORE_BF16_SDP 7
 
 #define LBX_WET_JANUS 0   /* compute_virtual_rho, kernels_fluid_PART.CUF:299-352 */
 #define LBX_WET_NEUTRAL 1 /* compute_densities_wall, kernels_fluid_PART.CUF:267-297 */

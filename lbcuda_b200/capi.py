@@ -6,7 +6,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB_PATH = os.path.join(_HERE, "liblbx.so")
 
 MODEL = {"bgk": 0, "cg": 1, "cg-diffdens": 2, "cg-d3q27": 3, "cg-diffdens-d3q27": 4}
-STORAGE = {"f32": 0, "f16": 1, "bf16": 2, "f64": 3, "f16sd": 4, "bf16sd": 5}
+STORAGE = {"f32": 0, "f16": 1, "bf16": 2, "f64": 3, "f16sd": 4, "bf16sd": 5, "f16sdp": 6, "bf16sdp": 7}
 WETTING = {"janus": 0, "neutral": 1}
 
 FLUID_WALL, FLUID_FLUID, FLUID_SPHERELIST, FLUID_SPHEREDEAD, FLUID_PARTICLECM = 0, 1, 2, 4, 5

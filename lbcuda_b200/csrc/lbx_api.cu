@@ -150,10 +150,13 @@ int lbx_create(const lbx_params* p, void** out) {
   if (two_dens &&
       (!(p->densR > 0.0f) || !(p->densB > 0.0f) || (p->densR != 1.0f && p->densB != 1.0f)))
     return LBX_ERR_ARG;
-  if (p->storage < LBX_STORE_F32 || p->storage > LBX_STORE_BF16_SD) return LBX_ERR_ARG;
-  const bool sd = p->storage == LBX_STORE_F16_SD || p->storage == LBX_STORE_BF16_SD;
-  // sum / difference pairs: the single-pass colour-gradient kernel (with or without spheres) only
+  if (p->storage < LBX_STORE_F32 || p->storage > LBX_STORE_BF16_SDP) return LBX_ERR_ARG;
+  const bool sdp = p->storage == LBX_STORE_F16_SDP || p->storage == LBX_STORE_BF16_SDP;
+  const bool sd = sdp || p->storage == LBX_STORE_F16_SD || p->storage == LBX_STORE_BF16_SD;
+  // sum / difference pairs: the single-pass colour-gradient kernel (with or without spheres) only;
+  // sum / predicted-split pairs: without spheres
   if (sd && p->model != LBX_MODEL_CG) return LBX_ERR_ARG;
+  if (sdp && p->max_particles > 0) return LBX_ERR_ARG;
   int64_t n = int64_t(p->nx) * p->ny * p->nz;
   if (n >= (int64_t(1) << 31)) return LBX_ERR_ARG;  // 32-bit cell indices
   Ctx* c = new (std::nothrow) Ctx();
@@ -169,6 +172,7 @@ int lbx_create(const lbx_params* p, void** out) {
   if (two_dens || d3q27) c->fused = 0;
   c->storage = p->storage;
   c->sd = sd;
+  c->sdp = sdp;
   if (sd) c->fused = 2;
   c->elem = (p->storage == LBX_STORE_F32) ? 4 : (p->storage == LBX_STORE_F64 ? 8 : 2);
   int rc = cuda_rc(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));

@@ -145,6 +145,9 @@ template <typename C>
 struct Shift {
   C s[2][4];  // [component][weight class]
   int sd = 0;  // sum / difference pairs: component 0 holds R + B, 1 holds R - B (s: their shifts)
+  // sum / predicted-split pairs: component 1 holds E = (R - B) - split[y] (R + B) for the cell y
+  // that pulls the pair; split is the phase field of each cell, or nullptr for the other formats
+  const float* split = nullptr;
   __device__ __forceinline__ C at(int c, int l) const { return s[c][wclass27(l)]; }
 };
 

@@ -12,6 +12,8 @@
 //             (only the two-pass colour-gradient path and the particle path).
 //   rho[2]    FP32/FP64 densities (particle path, readback).
 //   flags[2]  int8 cell flags of the current and previous step.
+//   split[2]  (sum / predicted-split storage) per cell, the phase field that
+//             the pairs of pops[i] pulled by that cell were encoded against.
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -31,6 +33,8 @@ struct Ctx {
   int q = 19;               // populations per component: 19, or 27 for the D3Q27 models
   int storage = LBX_STORE_F32;
   bool sd = false;  // LBX_STORE_F16_SD / LBX_STORE_BF16_SD: sum / difference pairs
+  bool sdp = false;  // LBX_STORE_F16_SDP / _BF16_SDP: sum / predicted-split pairs (sd is set too)
+  float* split[2] = {nullptr, nullptr};  // sdp: phase field each cell decodes the pairs of pops[i] it pulls with
   size_t elem = 4;          // bytes per stored population
   void* pops[2] = {nullptr, nullptr};
   int cur = 0;              // buffer holding the current state

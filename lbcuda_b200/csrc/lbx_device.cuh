@@ -106,6 +106,13 @@ __device__ __forceinline__ void sd_to_rb(C* f0, C* f1) {
     f1[l] = C(0.5) * (s - d);
   }
 }
+// Sum / predicted-split pairs: the pulled (total, E) pairs of a cell back to
+// (total, R - B) with the phase field ph the pairs were encoded against.
+template <int QQ = Q, typename C>
+__device__ __forceinline__ void split_decode(C ph, const C* f0, C* f1) {
+#pragma unroll
+  for (int l = 0; l < QQ; ++l) f1[l] = f1[l] + ph * f0[l];
+}
 template <int QQ = Q, typename C>
 __device__ __forceinline__ void rb_to_sd(C* f0, C* f1) {
 #pragma unroll
@@ -374,11 +381,13 @@ inline Shift<C> make_shift(const Ctx& c) {
   bool shifted = c.storage != LBX_STORE_F32 && c.storage != LBX_STORE_F64;
   float r0[2] = {c.p.rho0R, c.p.rho0B};
   s.sd = c.sd ? 1 : 0;
-  // sum / difference pairs: the shifts of R + B and of R - B
+  // sum / difference pairs: the shifts of R + B and of R - B (the predicted
+  // split's deviation E is stored unshifted)
   if (c.sd) {
     r0[0] = c.p.rho0R + c.p.rho0B;
-    r0[1] = c.p.rho0R - c.p.rho0B;
+    r0[1] = c.sdp ? 0.0f : c.p.rho0R - c.p.rho0B;
   }
+  s.split = c.sdp ? c.split[c.cur] : nullptr;
   for (int comp = 0; comp < 2; ++comp)
     for (int k = 0; k < 4; ++k) s.s[comp][k] = shifted ? C(L.w[k] * C(r0[comp])) : C(0);
   return s;
@@ -431,9 +440,11 @@ inline int by_storage(const Ctx& c, F&& fn) {
   switch (c.storage) {
     case LBX_STORE_F32: return fn((float*)nullptr);
     case LBX_STORE_F16:
-    case LBX_STORE_F16_SD: return fn((__half*)nullptr);
+    case LBX_STORE_F16_SD:
+    case LBX_STORE_F16_SDP: return fn((__half*)nullptr);
     case LBX_STORE_BF16:
-    case LBX_STORE_BF16_SD: return fn((__nv_bfloat16*)nullptr);
+    case LBX_STORE_BF16_SD:
+    case LBX_STORE_BF16_SDP: return fn((__nv_bfloat16*)nullptr);
     case LBX_STORE_F64: return fn((double*)nullptr);
   }
   return LBX_ERR_ARG;

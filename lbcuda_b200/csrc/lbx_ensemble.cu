@@ -140,6 +140,8 @@ int lbx_ensemble_create(int32_t nbox, const lbx_params* params, void** out) {
         params[i].beta != params[0].beta || params[i].rho0R != params[0].rho0R || params[i].rho0B != params[0].rho0B)
       return LBX_ERR_ARG;  // one fluid kernel (and its constants) for every box
   if (params[0].model != LBX_MODEL_CG) return LBX_ERR_ARG;
+  // sum / predicted-split pairs: single boxes without spheres only
+  if (params[0].storage == LBX_STORE_F16_SDP || params[0].storage == LBX_STORE_BF16_SDP) return LBX_ERR_ARG;
   Ensemble* e = new (std::nothrow) Ensemble();
   if (!e) return LBX_ERR_ALLOC;
   int rc = cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) == cudaSuccess ? 0 : LBX_ERR_CUDA;

@@ -57,6 +57,10 @@ __global__ void k_set_fields(S* __restrict__ A, S* __restrict__ B, Geom g, int n
       f1[l] = equil_u(L, C(rB[at(b, ex(l), ey(l), ez(l))]), edot(l, u, v, w), usq, l);
     }
     rb_to_sd(f0, f1);
+    if (sh.split) {  // predicted split: against the phase field of the cell that pulls the pair
+#pragma unroll
+      for (int l = 0; l < Q; ++l) f1[l] = f1[l] - C(sh.split[at(b, ex(l), ey(l), ez(l))]) * f0[l];
+    }
     store_all(A, g, cell, 0, sh, f0);
     store_all(A, g, cell, 1, sh, f1);
 #pragma unroll
@@ -77,6 +81,30 @@ __global__ void k_set_fields(S* __restrict__ A, S* __restrict__ B, Geom g, int n
   }
 }
 
+// Sum / predicted-split storage: the phase field each cell decodes its pulled
+// pairs with, for a state given as densities (set_fields) or as populations
+// (set_pops: the phase of each cell's pulled populations).
+__global__ void k_split_of_fields(Geom g, const float* __restrict__ rR, const float* __restrict__ rB, float* split) {
+  const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= g.n) return;
+  const float r = fmaxf(rR[i], 0.f), b = fmaxf(rB[i], 0.f);
+  split[i] = (r + b > 0.f) ? (r - b) / (r + b) : 0.f;
+}
+template <int QQ>
+__global__ void k_split_of_pops(Geom g, const float* __restrict__ pR, const float* __restrict__ pB, float* split) {
+  const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= g.n) return;
+  float r = 0.f, b = 0.f;
+#pragma unroll
+  for (int l = 0; l < QQ; ++l) {
+    r += pR[size_t(l) * size_t(g.n) + size_t(i)];
+    b += pB[size_t(l) * size_t(g.n) + size_t(i)];
+  }
+  r = fmaxf(r, 0.f);
+  b = fmaxf(b, 0.f);
+  split[i] = (r + b > 0.f) ? (r - b) / (r + b) : 0.f;
+}
+
 // initType 4: raw post-streaming populations, stored in pull convention
 template <typename S, int QQ>
 __global__ void k_set_pops(S* __restrict__ A, Geom g, int ncomp, const float* __restrict__ pR,
@@ -95,6 +123,10 @@ __global__ void k_set_pops(S* __restrict__ A, Geom g, int ncomp, const float* __
       f1[l] = C(pB[size_t(l) * size_t(g.n) + at(b, ex(l), ey(l), ez(l))]);
     }
     rb_to_sd(f0, f1);
+    if (sh.split) {  // predicted split: against the phase field of the cell that pulls the pair
+#pragma unroll
+      for (int l = 0; l < Q; ++l) f1[l] = f1[l] - C(sh.split[at(b, ex(l), ey(l), ez(l))]) * f0[l];
+    }
     store_all(A, g, cell, 0, sh, f0);
     store_all(A, g, cell, 1, sh, f1);
     return;
@@ -333,6 +365,7 @@ __global__ void k_fields(const S* __restrict__ A, const S* Bold, Geom g, int nco
 #pragma unroll
     for (int l = 0; l < QQ; ++l) fB[l] = C(0);
   }
+  if (sh.split) split_decode<QQ>(C(sh.split[cell]), fR, fB);
   if (sh.sd) sd_to_rb<QQ>(fR, fB);
   C lr = sum_q<QQ>(fR), lb = sum_q<QQ>(fB);
   C rs = lr + lb;
@@ -363,6 +396,7 @@ __global__ void k_get_pops(const S* __restrict__ A, const S* Bold, Geom g, int n
     C f1[QQ];
     pull_any<QQ>(A, Bold, g, b, 0, sh, fold, f);
     pull_any<QQ>(A, Bold, g, b, 1, sh, fold, f1);
+    if (sh.split) split_decode<QQ>(C(sh.split[cell]), f, f1);
     sd_to_rb<QQ>(f, f1);
 #pragma unroll
     for (int l = 0; l < QQ; ++l) {
@@ -397,6 +431,7 @@ __global__ void k_sums(const S* __restrict__ A, const S* Bold, Geom g, int ncomp
       if (sh.sd) {
         pull_any<QQ>(A, Bold, g, b, 0, sh, fold, f);
         pull_any<QQ>(A, Bold, g, b, 1, sh, fold, f1);
+        if (sh.split) split_decode<QQ>(C(sh.split[cell]), f, f1);
         sd_to_rb<QQ>(f, f1);
       }
       for (int comp = 0; comp < ncomp; ++comp) {
@@ -442,6 +477,11 @@ int fluid_alloc(Ctx& c) {
   }
   cudaMemsetAsync(c.pops[0], 0, bytes, c.stream);
   cudaMemsetAsync(c.pops[1], 0, bytes, c.stream);
+  if (c.sdp)
+    for (int i = 0; i < 2; ++i) {
+      if (cudaMalloc(&c.split[i], size_t(c.n) * 4) != cudaSuccess) return LBX_ERR_ALLOC;
+      cudaMemsetAsync(c.split[i], 0, size_t(c.n) * 4, c.stream);
+    }
   return launch_status();
 }
 
@@ -454,6 +494,10 @@ void fluid_free(Ctx& c) {
   }
   if (c.phi) cudaFree(c.phi);
   c.phi = nullptr;
+  for (int i = 0; i < 2; ++i) {
+    if (c.split[i]) cudaFree(c.split[i]);
+    c.split[i] = nullptr;
+  }
 }
 
 // fn(std::integral_constant<int, QQ>) with QQ = the context's populations per component
@@ -479,6 +523,8 @@ int fluid_set_fields(Ctx& c, const float* d_rR, const float* d_rB, float vx, flo
   return by_storage(c, [&](auto* tag) {
     using S = std::remove_pointer_t<decltype(tag)>;
     using C = typename Store<S>::C;
+    if (c.sdp)
+      k_split_of_fields<<<int((c.n + 255) / 256), 256, 0, c.stream>>>(g, d_rR, d_rB, c.split[0]);
     return by_lattice(c, [&](auto qt) {
       constexpr int QQ = decltype(qt)::value;
       if (two_densities(c))
@@ -502,6 +548,7 @@ int fluid_set_pops(Ctx& c, const float* d_pR, const float* d_pB) {
     using C = typename Store<S>::C;
     return by_lattice(c, [&](auto qt) {
       constexpr int QQ = decltype(qt)::value;
+      if (c.sdp) k_split_of_pops<QQ><<<int((c.n + 255) / 256), 256, 0, c.stream>>>(g, d_pR, d_pB, c.split[0]);
       k_set_pops<S, QQ><<<d.grid, d.block, 0, c.stream>>>((S*)c.pops[0], g, c.ncomp, d_pR, d_pB, make_shift<C>(c));
       return launch_status();
     });

@@ -73,7 +73,7 @@ LeanConst<C> make_lean(const Ctx& c) {
   K.rho0[0] = shifted ? C(c.p.rho0R) : C(0);
   K.rho0[1] = shifted ? C(c.p.rho0B) : C(0);
   K.rho0sd[0] = K.rho0[0] + K.rho0[1];
-  K.rho0sd[1] = K.rho0[0] - K.rho0[1];
+  K.rho0sd[1] = c.sdp ? C(0) : K.rho0[0] - K.rho0[1];  // the predicted split's deviation is stored unshifted
   for (int comp = 0; comp < 2; ++comp)
     for (int k = 0; k < 3; ++k) {
       K.s[comp][k] = K.w[k] * K.rho0[comp];
@@ -301,9 +301,9 @@ __device__ __forceinline__ void pull_async(const S* __restrict__ A, int64_t n, c
 // memory: each 16-bit value is added to the FP32 sums by one mixed-precision
 // add (same order and roundings as converting first).  SD: the pairs are
 // (R + B, R - B), whose sums give rho and rhoR - rhoB.
-template <typename S, typename C, bool SD = false>
+template <typename S, typename C, bool SD = false, bool SDP = false>
 __device__ __forceinline__ void stage_rho(const typename SPair<S>::R* st, int stride, const LeanConst<C>& K, C& rR,
-                                          C& rB) {
+                                          C& rB, C split = C(0)) {
   P2<C> s = SPair<S>::cvt(st[0]);
 #pragma unroll
   for (int l = 1; l < Q; ++l) {
@@ -312,7 +312,8 @@ __device__ __forceinline__ void stage_rho(const typename SPair<S>::R* st, int st
     s.y = add_mixed(r.y, s.y);
   }
   if constexpr (SD) {
-    const C rho = s.x + K.rho0sd[0], dif = s.y + K.rho0sd[1];
+    // predicted split: Sum (R - B) = Sum E + split Sum (R + B)
+    const C rho = s.x + K.rho0sd[0], dif = SDP ? fma(split, rho, s.y) : s.y + K.rho0sd[1];
     rR = C(0.5) * (rho + dif);
     rB = C(0.5) * (rho - dif);
   } else {
@@ -469,9 +470,10 @@ __device__ __forceinline__ Relaxed<C> relax_sums(const LeanConst<C>& K, const C 
 // gradient is below the reference's limit.  SD: the pairs (R + B, R - B)
 // less their shifts; R + B is the perturbed total itself (kR + kB = 1 up to
 // rounding, the recolouring terms cancel) and R - B = (kR - kB) f + 2 T.
-template <typename C, bool SD = false>
+template <typename C, bool SD = false, bool SDP = false, int RXW = 0>
 __device__ __forceinline__ bool recolour_sums(const LeanConst<C>& K, const Relaxed<C>& X, C rR, C rB, C px, C py,
-                                              C pz, bool shifted, P2<C> out[Q]) {
+                                              C pz, bool shifted, P2<C> out[Q], const C* const* win = nullptr,
+                                              int own = 0) {
   const C psq = fm(px, px, fm(py, py, pz * pz));
   if (!(psq > C(1.e-20))) return false;
   const C ipn = rsqrt_c(psq);
@@ -492,7 +494,11 @@ __device__ __forceinline__ bool recolour_sums(const LeanConst<C>& K, const Relax
   if constexpr (SD) {
     const C kD = kR - kB;
     const C fd = X.h0 - K0[0];
-    out[0] = pp(fd - K.ssd[0][0], fm(kD, fd, -K.ssd[1][0]));
+    // predicted split: the difference is stored as its deviation from the
+    // split of the receiving cell x + e_l (its phase field, win[1 + e_lz]
+    // at own + e_ly RX + e_lx), i.e. with the coefficient kD - phi_dest
+    auto dest = [&](int l) -> C { return win[1 + ez(l)][own + ey(l) * RXW + ex(l)]; };
+    out[0] = pp(fd - K.ssd[0][0], fm(SDP ? kD - dest(0) : kD, fd, -K.ssd[1][0]));
     const P2<C> pos[3] = {pp(px, -px), pp(py, -py), pp(pz, -pz)};
     const P2<C> neg[3] = {pp(-px, px), pp(-py, py), pp(-pz, pz)};
     const P2<C> KD = pp(kD, kD);
@@ -505,7 +511,7 @@ __device__ __forceinline__ bool recolour_sums(const LeanConst<C>& K, const Relax
       const P2<C> cD = p_fma(pp(t2, t2), ed, pp(-K.ssd[1][k], -K.ssd[1][k]));  // (2T, -2T) - s_D
       const P2<C> fd = p_add(X.h[p - 1], pert);
       const P2<C> oS = p_add(fd, pp(-K.ssd[0][k], -K.ssd[0][k]));
-      const P2<C> oD = p_fma(KD, fd, cD);
+      const P2<C> oD = p_fma(SDP ? p_add(KD, pp(-dest(l), -dest(l + 1))) : KD, fd, cD);
       out[l] = pp(oS.x, oD.x);
       out[l + 1] = pp(oS.y, oD.y);
     }
@@ -668,19 +674,23 @@ struct SideRec {
   C phi;
 };
 
-template <typename S, int TX, int TY, bool PART>
+template <typename S, int TX, int TY, bool PART, bool SDP = false>
 struct LeanSmem {
   using C = typename Store<S>::C;
   using R = typename SPair<S>::R;
   static constexpr int NT = TX * TY, RN = Ring<TX, TY>::N, CELLS = Ring<TX, TY>::CELLS;
-  static constexpr int WIN = kStaged<S, PART> ? 2 : 4;  // window planes
+  // window planes (the predicted split reads the phase field of every
+  // destination, planes z - 1 .. z + 1, after the plane barrier)
+  static constexpr int WIN = (kStaged<S, PART> && !SDP) ? 2 : 4;
   static constexpr size_t PHI = (sizeof(C) * WIN * CELLS + 15) / 16 * 16;
   static constexpr int D = kDepth<S, PART>;
   static constexpr size_t OWN = kStaged<S, PART> ? sizeof(R) * D * Q * NT : 0;
   static constexpr size_t RING = kStaged<S, PART> ? sizeof(R) * 2 * Q * RN : 0;
   static constexpr size_t SIDE = PART ? (sizeof(SideRec<C>) * (D * NT + 2 * RN) + 15) / 16 * 16 : 0;
+  // predicted split: each own / ring cell's phase field of the last step, copied with its pulls
+  static constexpr size_t SPL = SDP ? (4 * (D * NT + 2 * RN) + 15) / 16 * 16 : 0;
   static constexpr size_t BAR = 16;  // the plane's split barrier
-  static constexpr size_t BYTES = PHI + OWN + RING + SIDE + BAR;
+  static constexpr size_t BYTES = PHI + OWN + RING + SIDE + SPL + BAR;
   static_assert(PHI % 16 == 0 && OWN % 16 == 0 && RING % 16 == 0, "stage alignment");
   static __device__ __forceinline__ C (*phi(unsigned char* base))[CELLS] {
     return reinterpret_cast<C(*)[CELLS]>(base);
@@ -691,8 +701,11 @@ struct LeanSmem {
   static __device__ __forceinline__ SideRec<C>* side(unsigned char* base) {
     return PART ? reinterpret_cast<SideRec<C>*>(base + PHI + OWN + RING) : nullptr;
   }
+  static __device__ __forceinline__ float* spl(unsigned char* base) {
+    return SDP ? reinterpret_cast<float*>(base + PHI + OWN + RING + SIDE) : nullptr;
+  }
   static __device__ __forceinline__ unsigned long long* bar(unsigned char* base) {
-    return reinterpret_cast<unsigned long long*>(base + PHI + OWN + RING + SIDE);
+    return reinterpret_cast<unsigned long long*>(base + PHI + OWN + RING + SIDE + SPL);
   }
   // thread 0 sets up the barrier for the CTA's threads; the caller then syncs
   static __device__ __forceinline__ void init(unsigned char* base) {
@@ -702,7 +715,7 @@ struct LeanSmem {
 
 // One column march: cells [x0, x0+TX) x [y0, y0+TY) x [z0, zend) of one box.
 // SD: the stored pairs are sum / difference pairs (16-bit storage).
-template <typename S, int TX, int TY, bool PART, bool SD = false>
+template <typename S, int TX, int TY, bool PART, bool SD = false, bool SDP = false>
 __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restrict__ B, const Geom& g,
                                             const LeanConst<typename Store<S>::C>& K, int x0, int y0, int z0,
                                             int zend, unsigned long long* err, int64_t step,
@@ -710,11 +723,14 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
                                             typename Store<S>::C (*sphi)[Ring<TX, TY>::CELLS],
                                             typename SPair<S>::R* stage, SideRec<typename Store<S>::C>* side,
                                             unsigned long long* bar,
-                                            unsigned& bar_parity) {
+                                            unsigned& bar_parity, float* spl = nullptr,
+                                            const float* __restrict__ split_in = nullptr,
+                                            float* __restrict__ split_out = nullptr) {
   using C = typename Store<S>::C;
   constexpr int NT = TX * TY;
   using R = Ring<TX, TY>;
   static_assert(!SD || sizeof(typename SPair<S>::R) == 4, "sum / difference pairs: 16-bit storage");
+  static_assert(!SDP || (SD && !PART), "predicted split: sum / difference pairs without spheres");
   const bool parts = PART && PT.fnew != nullptr;  // a box of the ensemble may have no spheres
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
   const bool active = (x0 + tx < g.nx) && (y0 + ty < g.ny);
@@ -735,7 +751,7 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
   constexpr bool STAGED = kStaged<S, PART>;
   constexpr int D = kDepth<S, PART>;
   constexpr bool ASYNC = STAGED || PART;  // copy groups in flight
-  constexpr int WM = LeanSmem<S, TX, TY, PART>::WIN - 1;  // window slot of plane p: p & WM
+  constexpr int WM = LeanSmem<S, TX, TY, PART, SDP>::WIN - 1;  // window slot of plane p: p & WM
   SR* const ring_stage = STAGED ? stage + D * Q * NT : nullptr;
   SideRec<C>* const side_ring = PART ? side + D * NT : nullptr;
   const Planes<const S> Ap{A, 2 * g.n};
@@ -778,6 +794,14 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
         pull_async<S>(A, g.n, P, ring_slot(p), RN);
       }
     }
+    if constexpr (SDP) {  // the phase field the pulled pairs were encoded against
+      const unsigned co = unsigned(x) + unsigned(g.nx) * (unsigned(y) + unsigned(g.ny) * unsigned(zz));
+      cp_async4(spl + own_q(p) * NT + tid, split_in + size_t(co));
+      if (ringer) {
+        const unsigned cr = unsigned(rxg) + unsigned(g.nx) * (unsigned(ryg) + unsigned(g.ny) * unsigned(zz));
+        cp_async4(spl + D * NT + ring_q(p) * RN + tid, split_in + size_t(cr));
+      }
+    }
     if constexpr (ASYNC) cp_async_commit();
   };
   auto settle = [&]() {  // every copy group but the newest has landed
@@ -798,7 +822,7 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
   // store (rR - rB) / (rR + rB) of the densities they write), and every other
   // solid cell densities 0 (init_rho*_CG's MINDENS).
   auto cell_phase = [&](int cx, int cy, int zz, bool check, bool is_own, const SR* st, int stride,
-                        const SideRec<C>* rec, C& rR, C& rB) -> C {
+                        const SideRec<C>* rec, C& rR, C& rB, C split) -> C {
     const int cell = cx + g.nx * (cy + g.ny * zz);
     if constexpr (PART) {
       if (parts) {
@@ -820,7 +844,7 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
       }
     }
     if constexpr (STAGED) {
-      stage_rho<S, C, SD>(st, stride, K, rR, rB);
+      stage_rho<S, C, SD, SDP>(st, stride, K, rR, rB, split);
     } else {
       PullIdx P;
       pull_idx(g, cx, cy, zz, P);
@@ -838,12 +862,13 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
     const int zz = wrap_plane(p, g.nz);
     const bool owned = active && p >= z0 && p < zend;
     const SideRec<C>* so = PART ? side + own_q(p) * NT + tid : nullptr;
-    sphi[p & WM][own] = cell_phase(x, y, zz, owned, true, STAGED ? own_slot(p) : nullptr, NT, so, rRo, rBo);
+    sphi[p & WM][own] = cell_phase(x, y, zz, owned, true, STAGED ? own_slot(p) : nullptr, NT, so, rRo, rBo,
+                                   SDP ? C(spl[own_q(p) * NT + tid]) : C(0));
     if (ringer) {
       C qR, qB;
       const SideRec<C>* sr = PART ? side_ring + ring_q(p) * RN + tid : nullptr;
-      sphi[p & WM][rslot] =
-          cell_phase(rxg, ryg, zz, false, false, STAGED ? ring_slot(p) : nullptr, RN, sr, qR, qB);
+      sphi[p & WM][rslot] = cell_phase(rxg, ryg, zz, false, false, STAGED ? ring_slot(p) : nullptr, RN, sr, qR, qB,
+                                       SDP ? C(spl[D * NT + ring_q(p) * RN + tid]) : C(0));
     }
   };
 
@@ -859,8 +884,8 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
   PlaneGrad<C> gm{}, g0{};
   if constexpr (STAGED) {
     if (active) {
-      gm = plane_grad<C, R::RX>(sphi[(z0 + 1) & 1], own);
-      g0 = plane_grad<C, R::RX>(sphi[z0 & 1], own);
+      gm = plane_grad<C, R::RX>(sphi[(z0 - 1) & WM], own);
+      g0 = plane_grad<C, R::RX>(sphi[z0 & WM], own);
     }
     __syncthreads();  // the slot of plane z0-1 is rewritten in the first iteration
   }
@@ -933,6 +958,8 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
     }
     if (!mbar_wait(bar, bar_parity)) raise_error(err, LBX_DEV_WAIT_TIMEOUT, step, -1);
     bar_parity ^= 1u;
+    const C* const win[3] = {sphi[(z - 1) & WM], sphi[z & WM], sphi[(z + 1) & WM]};  // planes z - 1 .. z + 1
+    (void)win;
     if (active) {
       // A solid cell stores its streamed populations as pulled.  The
       // reference's push leaves a stale value behind a spheredead source
@@ -943,7 +970,7 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
       P2<C> gp[Q];
       bool done = false;
       if constexpr (STAGED) {
-        const PlaneGrad<C> gpl = plane_grad<C, R::RX>(sphi[(z + 1) & 1], own);
+        const PlaneGrad<C> gpl = plane_grad<C, R::RX>(sphi[(z + 1) & WM], own);
         if (collide) {
           const C H0 = C(1) / C(3), H1 = C(1) / C(12), HALF = C(0.5);  // W / 2
           px = fm(H0, g0.gx, H1 * (gm.gx + gpl.gx));
@@ -967,11 +994,16 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
             pz = fm(a, ps, pz);
           }
         }
-        done = recolour_sums<C, SD>(K, rx, rRc, rBc, px, py, pz, Store<S>::shifted, gp);
+        done = recolour_sums<C, SD, SDP, R::RX>(K, rx, rRc, rBc, px, py, pz, Store<S>::shifted, gp, win, own);
       }
       if (!done) {
 #pragma unroll
         for (int l = 0; l < Q; ++l) gp[l] = SPair<S>::cvt(pulled(l));
+        if constexpr (SDP) {  // (total, E) -> (total, R - B) with this cell's split of the last step
+          const C ph = spl[own_q(z) * NT + tid];
+#pragma unroll
+          for (int l = 0; l < Q; ++l) gp[l].y = fm(ph, gp[l].x + K.ssd[0][wclass(l)], gp[l].y);
+        }
         if constexpr (PART) {
           if (fresh) {
 #pragma unroll
@@ -982,27 +1014,34 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
           if constexpr (SD) bgk_components<C, STAGED, true>(K, rx, rRc + rBc, rRc - rBc, Store<S>::shifted, gp);
           else bgk_components<C, STAGED>(K, rx, rRc, rBc, Store<S>::shifted, gp);
         }
+        if constexpr (SDP) {  // R - B -> E against the split of each receiving cell
+#pragma unroll
+          for (int l = 0; l < Q; ++l)
+            gp[l].y = fm(-win[1 + ez(l)][own + ey(l) * R::RX + ex(l)], gp[l].x + K.ssd[0][wclass(l)], gp[l].y);
+        }
       }
 #pragma unroll
       for (int l = 0; l < Q; ++l) SPair<S>::st(Bp.at(l, cell), gp[l]);
+      if constexpr (SDP) split_out[size_t(unsigned(cell))] = sphi[z & WM][own];  // what the receivers decode with
     }
   }
   if constexpr (ASYNC) cp_async_wait<0>();  // nothing in flight when the shared memory is reused
 }
 
-template <typename S, int TX, int TY, int MINB, bool PART, bool SD = false>
+template <typename S, int TX, int TY, int MINB, bool PART, bool SD = false, bool SDP = false>
 __global__ void __launch_bounds__(TX* TY, MINB)
     k_cg_lean(const S* __restrict__ A, S* __restrict__ B, Geom g, LeanConst<typename Store<S>::C> K, int zlen,
-              unsigned long long* err, int64_t step, LeanPart<typename Store<S>::C> PT) {
+              unsigned long long* err, int64_t step, LeanPart<typename Store<S>::C> PT,
+              const float* __restrict__ split_in, float* __restrict__ split_out) {
   extern __shared__ __align__(16) unsigned char lean_smem[];
-  using M = LeanSmem<S, TX, TY, PART>;
+  using M = LeanSmem<S, TX, TY, PART, SDP>;
   M::init(lean_smem);
   __syncthreads();
   unsigned parity = 0;
   const int z0 = blockIdx.z * zlen;
-  lean_column<S, TX, TY, PART, SD>(A, B, g, K, blockIdx.x * TX, blockIdx.y * TY, z0, min(z0 + zlen, g.nz), err, step,
-                               PT, M::phi(lean_smem), M::stage(lean_smem), M::side(lean_smem),
-                               M::bar(lean_smem), parity);
+  lean_column<S, TX, TY, PART, SD, SDP>(A, B, g, K, blockIdx.x * TX, blockIdx.y * TY, z0, min(z0 + zlen, g.nz), err,
+                                        step, PT, M::phi(lean_smem), M::stage(lean_smem), M::side(lean_smem),
+                                        M::bar(lean_smem), parity, M::spl(lean_smem), split_in, split_out);
 }
 
 // ---------------------------------------------------------------------------
@@ -1080,19 +1119,19 @@ static int allow_smem(K* kernel, size_t bytes, unsigned long long& done_mask) {
 
 // Opt-in of k_cg_lean's shared memory and its resident CTAs per SM on this
 // device (the persistent grid), once per device.
-template <typename S, int TX, int TY, int MINB, bool PART, bool SD = false>
+template <typename S, int TX, int TY, int MINB, bool PART, bool SD = false, bool SDP = false>
 static int prepare_lean(int* resident) {
   static unsigned long long done = 0;
   static int per_sm[64] = {0}, sms[64] = {0};
-  int rc = allow_smem(k_cg_lean<S, TX, TY, MINB, PART, SD>, LeanSmem<S, TX, TY, PART>::BYTES, done);
+  int rc = allow_smem(k_cg_lean<S, TX, TY, MINB, PART, SD, SDP>, LeanSmem<S, TX, TY, PART, SDP>::BYTES, done);
   if (rc) return rc;
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return LBX_ERR_CUDA;
   dev &= 63;
   if (!per_sm[dev]) {
     int nb = 0, nsm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_cg_lean<S, TX, TY, MINB, PART, SD>, TX * TY,
-                                                      LeanSmem<S, TX, TY, PART>::BYTES) != cudaSuccess ||
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_cg_lean<S, TX, TY, MINB, PART, SD, SDP>, TX * TY,
+                                                      LeanSmem<S, TX, TY, PART, SDP>::BYTES) != cudaSuccess ||
         cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || nb < 1 || nsm < 1)
       return LBX_ERR_CUDA;
     sms[dev] = nsm;
@@ -1108,17 +1147,18 @@ static int prepare_lean_multi() {
   return allow_smem(k_cg_lean_multi<S, TX, TY, MINB, PART, SD>, LeanSmem<S, TX, TY, PART>::BYTES, done);
 }
 
-template <typename S, int TX, int TY, int MINB, bool PART, bool SD = false>
+template <typename S, int TX, int TY, int MINB, bool PART, bool SD = false, bool SDP = false>
 static int launch_lean(Ctx& c, int zlen_override, LeanPart<typename Store<S>::C> pt) {
   using C = typename Store<S>::C;
   int resident = 0;
-  const int rc = prepare_lean<S, TX, TY, MINB, PART, SD>(&resident);
+  const int rc = prepare_lean<S, TX, TY, MINB, PART, SD, SDP>(&resident);
   if (rc) return rc;
   const int zlen = zlen_override > 0 ? zlen_override : lean_zlen(c, TX, TY, resident);
   dim3 block(TX, TY, 1);
   dim3 grid((c.nx + TX - 1) / TX, (c.ny + TY - 1) / TY, (c.nz + zlen - 1) / zlen);
-  k_cg_lean<S, TX, TY, MINB, PART, SD><<<grid, block, LeanSmem<S, TX, TY, PART>::BYTES, c.stream>>>(
-      (const S*)c.pops[c.cur], (S*)c.pops[1 - c.cur], geom(c), make_lean<C>(c), zlen, c.d_err, c.step + 1, pt);
+  k_cg_lean<S, TX, TY, MINB, PART, SD, SDP><<<grid, block, LeanSmem<S, TX, TY, PART, SDP>::BYTES, c.stream>>>(
+      (const S*)c.pops[c.cur], (S*)c.pops[1 - c.cur], geom(c), make_lean<C>(c), zlen, c.d_err, c.step + 1, pt,
+      SDP ? c.split[c.cur] : nullptr, SDP ? c.split[1 - c.cur] : nullptr);
   return 0;
 }
 
@@ -1138,6 +1178,8 @@ int fluid_lean(Ctx& c) {
     } else if constexpr (std::is_same<S, float>::value) {
       if (c.lean_shape == 1) r = launch_lean<S, 32, 16, 1, false>(c, c.lean_zlen, none);
       else r = launch_lean<S, 32, 8, 2, false>(c, c.lean_zlen, none);
+    } else if (c.sdp) {  // sum / predicted-split pairs
+      r = launch_lean<S, 32, 8, 2, false, true, true>(c, c.lean_zlen, none);
     } else if (c.sd) {  // sum / difference pairs
       if (c.lean_shape == 1) r = launch_lean<S, 32, 16, 1, false, true>(c, c.lean_zlen, none);
       else r = launch_lean<S, 32, 8, 2, false, true>(c, c.lean_zlen, none);
