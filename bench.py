@@ -567,6 +567,37 @@ def only_region(args, local):
         res["closure_r4"] = r4
         print(json.dumps(res), flush=True)
         return 0
+    if args.only == "ensemble-profile":
+        # the ensemble workload's 48 boxes (FP16 sum / difference pairs), a few eager steps: profiler captures
+        from lbcuda_b200.ensemble import Ensemble, random_boxes
+        spec = random_boxes(48, seed=7)
+        ens = Ensemble([make_params(Lb, model="cg", storage="f16sd", sigma=SIGMA, beta=BETA, max_particles=max(len(x), 1),
+                                    radius=4.0, wetting="neutral", lrotate=1, max_vel=1.0, exact_tiles=0,
+                                    hz_rmin=8.5, hz_rcap=7.0) for Lb, x in spec])
+        for i, (Lb, x) in enumerate(spec):
+            rR, rB = seeded_noise_fields(Lb, Lb, Lb, seed=100 + i)
+            ens.boxes[i].set_fields(rR, rB)
+            if len(x):
+                ens.boxes[i].set_particles(x, np.zeros_like(x))
+        ms = ens.time(max(1, args.steps) * 2)
+        print(json.dumps({"only": args.only, "cells": ens.cells, "ms_per_step": ms / (max(1, args.steps) * 2)}),
+              flush=True)
+        ens.close()
+        return 0
+    if args.only == "mlp-profile":
+        # a short training and one inference batch of the closure network: profiler captures
+        from lbcuda_b200 import closure as _cl
+        rng = np.random.default_rng(0)
+        X = rng.uniform(-1, 1, (2048, _cl.DIN)).astype(np.float32)
+        T = np.tanh(X[:, :_cl.DOUT]).astype(np.float32)
+        t0 = time.perf_counter()
+        w, loss = _cl.train(X, T, epochs=max(1, args.steps), lr=2e-3)
+        t1 = time.perf_counter()
+        Y = _cl.infer(w, np.repeat(X, 2, axis=0))
+        t2 = time.perf_counter()
+        print(json.dumps({"only": args.only, "train_s": t1 - t0, "infer_s": t2 - t1, "loss": float(loss[-1]),
+                          "finite": bool(np.isfinite(Y).all())}), flush=True)
+        return 0
     if args.only == "bgk":
         print(json.dumps({"64": bgk_timing(64, 2000), "256": bgk_timing(256, 200), "512": bgk_timing(512, 40)}),
               flush=True)
@@ -617,7 +648,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-extras", action="store_true", help="skip the error runs, the colloid case and the CPU baseline")
     ap.add_argument("--only", choices=["f16", "f32", "bf16", "f64", "f16sd", "bf16sd", "f16sdp", "bf16sdp", "colloid-f16", "colloid-f32", "colloid-f16-small", "colloid-f16sd",
-                                       "colloid-f32-small", "ensemble", "ensemble-closure", "closure", "closure12", "variants", "errors", "bgk",
+                                       "colloid-f32-small", "ensemble", "ensemble-closure", "ensemble-profile", "mlp-profile", "closure",
+                                       "closure12", "variants", "errors", "bgk",
                                        "bgk-256"],
                     help="profiling aid: run one timed region only and print its timing")
     ap.add_argument("--lb-steps", type=int, default=LB_PER_STEP, help="lattice steps per bench step")
