@@ -41,6 +41,9 @@ BYTES_PER_CELL = {"f16": 160, "bf16": 160, "f16sd": 160, "bf16sd": 160, "f16sdp"
                   "f64": 616}  # algorithmic bytes per cell-step
 MINIMAL_BYTES = {"f16": 152, "bf16": 152, "f16sd": 152, "f16sdp": 160, "f32": 304, "f64": 608}  # bytes the kernel must move
 METRIC = "MLUPS & HBM GB/s, FP16-store vs FP32 LB at stated FP64 error, 1\u00d7B200"
+# closure weights for radius-4 spheres (the ensemble workload), written by
+# `python bench.py --only ensemble-closure --save-weights <path>`
+CLOSURE_R4 = os.path.join(ROOT, "lbcuda_b200", "data", "closure_r4_weights.npy")
 
 
 def peaks():
@@ -563,6 +566,8 @@ def only_region(args, local):
         return 0
     if args.only == "ensemble-closure":
         r4, w4 = closure_experiment(R_hi=8, L_hi=64, R_lo=4, steps_hi=432, n_direct=32, return_weights=True)
+        if args.save_weights:
+            np.save(args.save_weights, np.asarray(w4, np.float32))
         res = ensemble_timing(weights=w4)
         res["closure_r4"] = r4
         print(json.dumps(res), flush=True)
@@ -655,6 +660,8 @@ def main():
     ap.add_argument("--lb-steps", type=int, default=LB_PER_STEP, help="lattice steps per bench step")
     ap.add_argument("--schedule", type=int, default=2, help="colour-gradient schedule (0, 1, 2)")
     ap.add_argument("--box", type=int, default=L, help="lattice edge of the --only storage runs")
+    ap.add_argument("--save-weights", default=None,
+                    help="--only ensemble-closure: write the trained radius-4 closure weights (.npy) here")
     args = ap.parse_args()
     ws, rank, local = dist_env()
     if args.impl == "reference":
@@ -773,11 +780,11 @@ def main():
         extras["closure"], w = closure_experiment(R_hi=12, L_hi=96, steps_hi=960, return_weights=True)
         extras["closure"]["window"] = _cl.window_score(w)
         extras["closure"]["suspension"] = closure_suspension(w)
-        # the ensemble's spheres have radius 4: its closure is trained at R_lo = 4 against R_hi = 8
-        r4, w4 = closure_experiment(R_hi=8, L_hi=64, R_lo=4, steps_hi=432, n_direct=32, return_weights=True)
-        extras["ensemble_48"] = ensemble_timing(weights=w4)
-        extras["ensemble_48"]["closure_r4"] = {k: r4[k] for k in ("R_hi", "R_lo", "classes", "train_samples",
-                                                                  "error_direct", "resistance_s", "train_s")}
+        # the ensemble's spheres have radius 4: its closure (R_lo = 4 trained against R_hi = 8 by
+        # `bench.py --only ensemble-closure --save-weights ...`, the same pipeline as above) is an input
+        # of the ensemble workload, loaded from the weights that run wrote
+        extras["ensemble_48"] = ensemble_timing(weights=np.load(CLOSURE_R4))
+        extras["ensemble_48"]["closure_weights"] = os.path.relpath(CLOSURE_R4, ROOT)
         extras["cpu_baseline"] = cpu_baseline_sample()
 
     if rank == 0:
