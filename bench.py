@@ -36,7 +36,7 @@ SIGMA, BETA = 0.02, 0.7
 LB_PER_STEP = 500
 # DRAM bytes (read + write) of one k_cg_lean launch at 128^3, from the ncu
 # captures summarised in profiles/ (None where no capture of that storage)
-TRAFFIC = {"f16": 292.7e6, "f16sd": 292.0e6, "f32": 622.6e6}
+TRAFFIC = {"f16": 292.7e6, "f16sd": 292.0e6, "f16sdp": 310.8e6, "f32": 622.6e6}
 BYTES_PER_CELL = {"f16": 160, "bf16": 160, "f16sd": 160, "bf16sd": 160, "f16sdp": 160, "bf16sdp": 160, "f32": 312,
                   "f64": 616}  # algorithmic bytes per cell-step
 MINIMAL_BYTES = {"f16": 152, "bf16": 152, "f16sd": 152, "f16sdp": 160, "f32": 304, "f64": 608}  # bytes the kernel must move
