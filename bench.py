@@ -575,15 +575,21 @@ def only_region(args, local):
     if args.only == "ensemble-profile":
         # the ensemble workload's 48 boxes (FP16 sum / difference pairs), a few eager steps: profiler captures
         from lbcuda_b200.ensemble import Ensemble, random_boxes
+        import ctypes
+        from lbcuda_b200 import capi
         spec = random_boxes(48, seed=7)
         ens = Ensemble([make_params(Lb, model="cg", storage="f16sd", sigma=SIGMA, beta=BETA, max_particles=max(len(x), 1),
                                     radius=4.0, wetting="neutral", lrotate=1, max_vel=1.0, exact_tiles=0,
-                                    hz_rmin=8.5, hz_rcap=7.0) for Lb, x in spec])
+                                    hz_rmin=8.5, hz_rcap=7.0, closure=1, lubrication=1, lubric_rmin=1.0,
+                                    lubric_rcap=0.2) for Lb, x in spec])
+        wf = np.ascontiguousarray(np.load(CLOSURE_R4), np.float32)
         for i, (Lb, x) in enumerate(spec):
             rR, rB = seeded_noise_fields(Lb, Lb, Lb, seed=100 + i)
             ens.boxes[i].set_fields(rR, rB)
             if len(x):
                 ens.boxes[i].set_particles(x, np.zeros_like(x))
+                capi.check(capi.lib().lbx_closure_set(ens.boxes[i]._h, wf.ctypes.data_as(ctypes.POINTER(ctypes.c_float))),
+                           "lbx_closure_set")
         ms = ens.time(max(1, args.steps) * 2)
         print(json.dumps({"only": args.only, "cells": ens.cells, "ms_per_step": ms / (max(1, args.steps) * 2)}),
               flush=True)
@@ -630,13 +636,15 @@ def only_region(args, local):
     rR, rB = seeded_noise_fields(Lb, Lb, Lb, seed=SEED)
     s = LBSim(make_params(Lb, model="cg", storage=args.only, sigma=SIGMA, beta=BETA))
     s.set_schedule(args.schedule)
+    if args.zlen:
+        s.set_lean_shape(0, args.zlen)
     s.set_fields(rR, rB)
     s.step(args.warmup * args.lb_steps)
     s.sync()
     tot, k, nl = s.time_steps(args.steps * args.lb_steps, kernel_timing=args.schedule != 0)
     n = args.steps * args.lb_steps
     kus = (k / nl * 1e3) if nl else None
-    print(json.dumps({"only": args.only, "box": Lb, "schedule": args.schedule,
+    print(json.dumps({"only": args.only, "box": Lb, "schedule": args.schedule, "zlen": args.zlen or "auto",
                       "ms_per_lattice_step": tot / n,
                       "mlups": Lb ** 3 * n / (tot * 1e-3) / 1e6, "kernel_us": kus,
                       "frac_at_basis": (BYTES_PER_CELL[args.only] * Lb ** 3 / (kus * 1e-6) / 1e9 / peaks()[0])
@@ -660,6 +668,8 @@ def main():
     ap.add_argument("--lb-steps", type=int, default=LB_PER_STEP, help="lattice steps per bench step")
     ap.add_argument("--schedule", type=int, default=2, help="colour-gradient schedule (0, 1, 2)")
     ap.add_argument("--box", type=int, default=L, help="lattice edge of the --only storage runs")
+    ap.add_argument("--zlen", type=int, default=0,
+                    help="--only storage runs: equal z-segments of this length (0: automatic plan)")
     ap.add_argument("--save-weights", default=None,
                     help="--only ensemble-closure: write the trained radius-4 closure weights (.npy) here")
     args = ap.parse_args()

@@ -498,6 +498,8 @@ void fluid_free(Ctx& c) {
     if (c.split[i]) cudaFree(c.split[i]);
     c.split[i] = nullptr;
   }
+  if (c.lean_plan) cudaFree(c.lean_plan);
+  c.lean_plan = nullptr;
 }
 
 // fn(std::integral_constant<int, QQ>) with QQ = the context's populations per component

@@ -1032,16 +1032,25 @@ template <typename S, int TX, int TY, int MINB, bool PART, bool SD = false, bool
 __global__ void __launch_bounds__(TX* TY, MINB)
     k_cg_lean(const S* __restrict__ A, S* __restrict__ B, Geom g, LeanConst<typename Store<S>::C> K, int zlen,
               unsigned long long* err, int64_t step, LeanPart<typename Store<S>::C> PT,
-              const float* __restrict__ split_in, float* __restrict__ split_out) {
+              const float* __restrict__ split_in, float* __restrict__ split_out, const int4* __restrict__ plan) {
   extern __shared__ __align__(16) unsigned char lean_smem[];
   using M = LeanSmem<S, TX, TY, PART, SDP>;
   M::init(lean_smem);
   __syncthreads();
   unsigned parity = 0;
-  const int z0 = blockIdx.z * zlen;
-  lean_column<S, TX, TY, PART, SD, SDP>(A, B, g, K, blockIdx.x * TX, blockIdx.y * TY, z0, min(z0 + zlen, g.nz), err,
-                                        step, PT, M::phi(lean_smem), M::stage(lean_smem), M::side(lean_smem),
-                                        M::bar(lean_smem), parity, M::spl(lean_smem), split_in, split_out);
+  // the column and z-segment of this CTA: from the grid (equal segments) or
+  // from the launch's plan (x0, y0, z0, zend per CTA)
+  int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY, z0 = blockIdx.z * zlen, z1 = min(z0 + zlen, g.nz);
+  if (plan) {
+    const int4 w = plan[blockIdx.x];
+    x0 = w.x;
+    y0 = w.y;
+    z0 = w.z;
+    z1 = w.w;
+  }
+  lean_column<S, TX, TY, PART, SD, SDP>(A, B, g, K, x0, y0, z0, z1, err, step, PT, M::phi(lean_smem),
+                                        M::stage(lean_smem), M::side(lean_smem), M::bar(lean_smem), parity,
+                                        M::spl(lean_smem), split_in, split_out);
 }
 
 // ---------------------------------------------------------------------------
@@ -1102,6 +1111,51 @@ static int lean_zlen(const Ctx& c, int tx, int ty, int resident) {
   return int((c.nz + segs - 1) / segs);
 }
 
+// Paired segment plan.  When four equal z-segments per column leave resident
+// CTA slots empty and five would need a second wave (128^3 with 32 x 8
+// columns: 256 CTAs for 296 slots, so 40 SMs run one CTA and the kernel takes
+// as long as two 32-plane segments on the others), some columns are cut into
+// one segment of nz/4 planes and four of the rest's quarter, the others into
+// four of nz/4, and all long segments are launched before the short ones:
+// the scheduler then gives each SM one long and one short segment (at 128^3:
+// 37 columns of 32 + 4 x 24 planes, 27 of 4 x 32; 145 long, 148 short).
+// Returns the device table (x0, y0, z0, zend per CTA) kept in the context, or
+// nullptr when the equal segments are used.
+static const int4* paired_plan(Ctx& c, int TX, int TY, int resident, int* n) {
+  const int ncx = (c.nx + TX - 1) / TX, ncy = (c.ny + TY - 1) / TY, cols = ncx * ncy;
+  const int b = std::min(cols, std::min(resident / 8, resident - 4 * cols));  // columns cut 1 + 4
+  if (c.nz < 64 || 4 * cols >= resident || 5 * cols <= resident || b <= 0) return nullptr;
+  const int key = resident * 4096 + TX * 64 + TY;
+  if (c.lean_plan && c.lean_plan_key == key) {
+    *n = c.lean_plan_n;
+    return static_cast<const int4*>(c.lean_plan);
+  }
+  std::vector<int4> lng, sht;
+  const int L1 = c.nz / 4, rest = c.nz - L1;
+  for (int col = 0; col < cols; ++col) {
+    const int x0 = (col % ncx) * TX, y0 = (col / ncx) * TY;
+    const bool cut = (long(col) * b) / cols != (long(col + 1) * b) / cols;  // b columns spread over all
+    if (!cut) {
+      for (int k = 0; k < 4; ++k) lng.push_back(make_int4(x0, y0, k * c.nz / 4, (k + 1) * c.nz / 4));
+    } else {
+      lng.push_back(make_int4(x0, y0, 0, L1));
+      for (int k = 0; k < 4; ++k) sht.push_back(make_int4(x0, y0, L1 + k * rest / 4, L1 + (k + 1) * rest / 4));
+    }
+  }
+  lng.insert(lng.end(), sht.begin(), sht.end());
+  if (c.lean_plan) cudaFree(c.lean_plan);
+  c.lean_plan = nullptr;
+  if (cudaMalloc(&c.lean_plan, lng.size() * sizeof(int4)) != cudaSuccess) {
+    c.lean_plan = nullptr;
+    return nullptr;
+  }
+  cudaMemcpy(c.lean_plan, lng.data(), lng.size() * sizeof(int4), cudaMemcpyHostToDevice);
+  c.lean_plan_n = int(lng.size());
+  c.lean_plan_key = key;
+  *n = c.lean_plan_n;
+  return static_cast<const int4*>(c.lean_plan);
+}
+
 // Opt a kernel into its dynamic shared memory (beyond the default 48 KB), once
 // per device.  Called outside stream capture (the first eager launch, or when
 // an ensemble builds its tables).
@@ -1156,9 +1210,12 @@ static int launch_lean(Ctx& c, int zlen_override, LeanPart<typename Store<S>::C>
   const int zlen = zlen_override > 0 ? zlen_override : lean_zlen(c, TX, TY, resident);
   dim3 block(TX, TY, 1);
   dim3 grid((c.nx + TX - 1) / TX, (c.ny + TY - 1) / TY, (c.nz + zlen - 1) / zlen);
+  int nplan = 0;
+  const int4* plan = zlen_override > 0 ? nullptr : paired_plan(c, TX, TY, resident, &nplan);
+  if (plan) grid = dim3(unsigned(nplan), 1, 1);
   k_cg_lean<S, TX, TY, MINB, PART, SD, SDP><<<grid, block, LeanSmem<S, TX, TY, PART, SDP>::BYTES, c.stream>>>(
       (const S*)c.pops[c.cur], (S*)c.pops[1 - c.cur], geom(c), make_lean<C>(c), zlen, c.d_err, c.step + 1, pt,
-      SDP ? c.split[c.cur] : nullptr, SDP ? c.split[1 - c.cur] : nullptr);
+      SDP ? c.split[c.cur] : nullptr, SDP ? c.split[1 - c.cur] : nullptr, plan);
   return 0;
 }
 
