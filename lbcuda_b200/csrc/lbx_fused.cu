@@ -1210,8 +1210,11 @@ static int launch_lean(Ctx& c, int zlen_override, LeanPart<typename Store<S>::C>
   const int zlen = zlen_override > 0 ? zlen_override : lean_zlen(c, TX, TY, resident);
   dim3 block(TX, TY, 1);
   dim3 grid((c.nx + TX - 1) / TX, (c.ny + TY - 1) / TY, (c.nz + zlen - 1) / zlen);
+  // the paired plan only for the staged 16-bit kernels: FP32 / FP64 re-read
+  // their pairs from L2, which neighbouring columns out of step in z defeat
+  // (FP32 128^3: 185 us with the plan, 148 us without; FP16 96 against 101)
   int nplan = 0;
-  const int4* plan = zlen_override > 0 ? nullptr : paired_plan(c, TX, TY, resident, &nplan);
+  const int4* plan = (zlen_override > 0 || !kStaged<S, PART>) ? nullptr : paired_plan(c, TX, TY, resident, &nplan);
   if (plan) grid = dim3(unsigned(nplan), 1, 1);
   k_cg_lean<S, TX, TY, MINB, PART, SD, SDP><<<grid, block, LeanSmem<S, TX, TY, PART, SDP>::BYTES, c.stream>>>(
       (const S*)c.pops[c.cur], (S*)c.pops[1 - c.cur], geom(c), make_lean<C>(c), zlen, c.d_err, c.step + 1, pt,
