@@ -638,6 +638,7 @@ def only_region(args, local):
     s.set_schedule(args.schedule)
     if args.zlen:
         s.set_lean_shape(0, args.zlen)
+    s.set_lean_copies(args.lean_copies)
     s.set_fields(rR, rB)
     s.step(args.warmup * args.lb_steps)
     s.sync()
@@ -645,6 +646,7 @@ def only_region(args, local):
     n = args.steps * args.lb_steps
     kus = (k / nl * 1e3) if nl else None
     print(json.dumps({"only": args.only, "box": Lb, "schedule": args.schedule, "zlen": args.zlen or "auto",
+                      "lean_copies": args.lean_copies,
                       "ms_per_lattice_step": tot / n,
                       "mlups": Lb ** 3 * n / (tot * 1e-3) / 1e6, "kernel_us": kus,
                       "frac_at_basis": (BYTES_PER_CELL[args.only] * Lb ** 3 / (kus * 1e-6) / 1e9 / peaks()[0])
@@ -670,6 +672,8 @@ def main():
     ap.add_argument("--box", type=int, default=L, help="lattice edge of the --only storage runs")
     ap.add_argument("--zlen", type=int, default=0,
                     help="--only storage runs: equal z-segments of this length (0: automatic plan)")
+    ap.add_argument("--lean-copies", type=int, default=1,
+                    help="--only storage runs: 16-bit pulls as box granules (1) or one copy per pull (0)")
     ap.add_argument("--save-weights", default=None,
                     help="--only ensemble-closure: write the trained radius-4 closure weights (.npy) here")
     args = ap.parse_args()

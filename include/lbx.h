@@ -320,6 +320,10 @@ int lbx_set_schedule(void* ctx, int32_t fused);
 /* Lean single-pass kernel shape: 0 = 32x8 cells per CTA, 1 = 32x16; zlen =
  * lattice planes per z-segment (0 = automatic). */
 int lbx_set_lean_shape(void* ctx, int32_t shape, int32_t zlen);
+/* How the lean kernel stages 16-bit pulls in shared memory: 1 = 16-byte
+ * granules of a box of rows per direction (default; used when nx is a
+ * multiple of 4), 0 = one 4-byte copy per pull.  Both give the same bits. */
+int lbx_set_lean_copies(void* ctx, int32_t mode);
 /* Enqueue nsteps steps bracketed by CUDA events on the context stream and
  * wait: total device ms, and the summed duration / launch count of the
  * step's dominant kernel (NULL kernel_ms disables per-kernel events). */

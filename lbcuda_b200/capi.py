@@ -96,6 +96,7 @@ SIGNATURES = {
     "lbx_get_step": (C.c_int, [_P, _I64]),
     "lbx_set_schedule": (C.c_int, [_P, C.c_int32]),
     "lbx_set_lean_shape": (C.c_int, [_P, C.c_int32, C.c_int32]),
+    "lbx_set_lean_copies": (C.c_int, [_P, C.c_int32]),
     "lbx_time_steps": (C.c_int, [_P, C.c_int32, _D, _D, _I64]),
 }
 

@@ -458,6 +458,14 @@ int lbx_set_lean_shape(void* ctx, int32_t shape, int32_t zlen) {
   return 0;
 }
 
+/* Staging of the lean kernel's 16-bit pulls: 1 = box granules, 0 = one copy per pull. */
+int lbx_set_lean_copies(void* ctx, int32_t mode) {
+  Ctx* c = as_ctx(ctx);
+  if (!c || mode < 0 || mode > 1) return LBX_ERR_ARG;
+  c->lean_copies = mode;
+  return 0;
+}
+
 /* Time nsteps steps on the context stream with CUDA events: total device
  * time in ms, and the summed duration of the step's dominant kernel (the
  * fused collide-stream kernel) with its launch count. */

@@ -48,6 +48,7 @@ struct Ctx {
   int fused = 2;            // colour-gradient schedule: 0 two passes, 1 first single-pass kernel, 2 lean single pass
   int lean_shape = 0;       // lean kernel CTA: 0 = 32x8 (2 per SM), 1 = 32x16
   int lean_zlen = 0;        // z-segment length of the lean kernel (0 = automatic)
+  int lean_copies = 1;      // 16-bit pulls: 1 = 16-byte box granules (when nx % 4 == 0), 0 = one copy per pull
   void* lean_plan = nullptr;  // device table of the lean kernel's paired segments (int4 per CTA), or null
   int lean_plan_n = 0, lean_plan_key = 0;
   // timing of the dominant kernel (opt-in)

@@ -33,9 +33,27 @@
 #include "lbx_device.cuh"
 
 #include <algorithm>
+#include <type_traits>
+#include <utility>
 #include <vector>
 
 namespace lbx {
+
+// f(std::integral_constant<int, l>) for the even / odd directions l of D3Q19,
+// each with its direction as a compile-time constant
+template <typename F, int... I>
+__device__ __forceinline__ void unroll_dirs(F& f, int first, std::integer_sequence<int, I...>) {
+  (void)first;
+  (f(std::integral_constant<int, 2 * I>{}), ...);
+}
+template <typename F, int... I>
+__device__ __forceinline__ void unroll_dirs_odd(F& f, std::integer_sequence<int, I...>) {
+  (f(std::integral_constant<int, 2 * I + 1>{}), ...);
+}
+template <typename F>
+__device__ __forceinline__ void unroll_even(F& f) { unroll_dirs(f, 0, std::make_integer_sequence<int, 10>{}); }
+template <typename F>
+__device__ __forceinline__ void unroll_odd(F& f) { unroll_dirs_odd(f, std::make_integer_sequence<int, 9>{}); }
 
 template <typename C>
 struct LeanConst {
@@ -250,6 +268,11 @@ __device__ __forceinline__ void cp_async_c(C* smem, const C* gmem) {
   if constexpr (sizeof(C) == 4) cp_async4(smem, gmem);
   else cp_async8(smem, gmem);
 }
+// 16-byte granule, L2 -> shared memory without an L1 allocation
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() {
@@ -267,6 +290,12 @@ __device__ __forceinline__ void mbar_init(unsigned long long* m, unsigned count)
 __device__ __forceinline__ void mbar_arrive(unsigned long long* m) {
   const unsigned a = static_cast<unsigned>(__cvta_generic_to_shared(m));
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(a) : "memory");
+}
+// arrive on the barrier once every cp.async this thread has issued so far has
+// landed (the barrier's expected count includes this arrival)
+__device__ __forceinline__ void mbar_arrive_cp_async(unsigned long long* m) {
+  const unsigned a = static_cast<unsigned>(__cvta_generic_to_shared(m));
+  asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];\n" ::"r"(a) : "memory");
 }
 // wait for the completion of the phase of the given parity; false if the
 // bounded number of polls ran out (each poll may itself suspend a while)
@@ -301,13 +330,13 @@ __device__ __forceinline__ void pull_async(const S* __restrict__ A, int64_t n, c
 // memory: each 16-bit value is added to the FP32 sums by one mixed-precision
 // add (same order and roundings as converting first).  SD: the pairs are
 // (R + B, R - B), whose sums give rho and rhoR - rhoB.
-template <typename S, typename C, bool SD = false, bool SDP = false>
-__device__ __forceinline__ void stage_rho(const typename SPair<S>::R* st, int stride, const LeanConst<C>& K, C& rR,
-                                          C& rB, C split = C(0)) {
-  P2<C> s = SPair<S>::cvt(st[0]);
+// at(l): the staged pair of direction l
+template <typename S, typename C, bool SD = false, bool SDP = false, typename F>
+__device__ __forceinline__ void stage_rho(F&& at, const LeanConst<C>& K, C& rR, C& rB, C split = C(0)) {
+  P2<C> s = SPair<S>::cvt(at(0));
 #pragma unroll
   for (int l = 1; l < Q; ++l) {
-    const typename SPair<S>::R r = st[l * stride];
+    const typename SPair<S>::R r = at(l);
     s.x = add_mixed(r.x, s.x);
     s.y = add_mixed(r.y, s.y);
   }
@@ -674,22 +703,48 @@ struct SideRec {
   C phi;
 };
 
-template <typename S, int TX, int TY, bool PART, bool SDP = false>
+// Staged pulls in boxes (BOX, 16-bit storage with nx a multiple of 4): per
+// plane and direction l, the rows y0 - 1 - e_ly .. y0 + TY - e_ly and the
+// columns x0 - 4 .. x0 + TX + 3 of direction plane l at z - e_lz, copied by
+// 16-byte cp.async granules (a granule starts on a multiple of 4 cells, so
+// the periodic wrap moves whole granules).  Own cell (tx, ty) finds its pull
+// of direction l at box row ty + 1, column tx + 4 - e_lx; ring cell (rx, ry)
+// at row ry, column rx + 3 - e_lx: one per-thread base and a constant offset
+// per direction.  Each plane slot has a FULL barrier (every thread arrives
+// once its copies have landed, cp.async.mbarrier.arrive) and an EMPTY
+// barrier (every thread arrives after its last read of the plane), since a
+// thread now reads what other threads copied.
+template <int TX, int TY>
+struct LeanBox {
+  static constexpr int BW = TX + 8, ROWS = TY + 2, ELEMS = BW * ROWS;  // 4-byte pairs per direction box
+  static constexpr int GR = BW / 4;                                    // granules per row
+  static constexpr int POS = ROWS * GR;                                // granule positions per box
+  static constexpr int NT = TX * TY;
+  static constexpr int G = NT / POS;  // copy groups: group k copies directions k, k + G, ...
+  static_assert(G == 2, "box copies are written for two groups (even / odd directions)");
+  static constexpr int COPIERS = G * POS;
+};
+
+template <typename S, int TX, int TY, bool PART, bool SDP = false, bool BOX = false>
 struct LeanSmem {
   using C = typename Store<S>::C;
   using R = typename SPair<S>::R;
   static constexpr int NT = TX * TY, RN = Ring<TX, TY>::N, CELLS = Ring<TX, TY>::CELLS;
+  static constexpr bool BOXED = BOX && kStaged<S, PART>;
   // window planes (the predicted split reads the phase field of every
   // destination, planes z - 1 .. z + 1, after the plane barrier)
   static constexpr int WIN = (kStaged<S, PART> && !SDP) ? 2 : 4;
   static constexpr size_t PHI = (sizeof(C) * WIN * CELLS + 15) / 16 * 16;
   static constexpr int D = kDepth<S, PART>;
-  static constexpr size_t OWN = kStaged<S, PART> ? sizeof(R) * D * Q * NT : 0;
-  static constexpr size_t RING = kStaged<S, PART> ? sizeof(R) * 2 * Q * RN : 0;
+  static constexpr size_t OWN = !kStaged<S, PART> ? 0
+                                : BOXED          ? sizeof(R) * D * Q * LeanBox<TX, TY>::ELEMS
+                                                 : sizeof(R) * D * Q * NT;
+  static constexpr size_t RING = (kStaged<S, PART> && !BOXED) ? sizeof(R) * 2 * Q * RN : 0;
   static constexpr size_t SIDE = PART ? (sizeof(SideRec<C>) * (D * NT + 2 * RN) + 15) / 16 * 16 : 0;
   // predicted split: each own / ring cell's phase field of the last step, copied with its pulls
   static constexpr size_t SPL = SDP ? (4 * (D * NT + 2 * RN) + 15) / 16 * 16 : 0;
-  static constexpr size_t BAR = 16;  // the plane's split barrier
+  // the plane's split barrier; with boxes also FULL[D] and EMPTY[D]
+  static constexpr size_t BAR = BOXED ? 8 * (1 + 2 * D + 1) : 16;
   static constexpr size_t BYTES = PHI + OWN + RING + SIDE + SPL + BAR;
   static_assert(PHI % 16 == 0 && OWN % 16 == 0 && RING % 16 == 0, "stage alignment");
   static __device__ __forceinline__ C (*phi(unsigned char* base))[CELLS] {
@@ -707,15 +762,28 @@ struct LeanSmem {
   static __device__ __forceinline__ unsigned long long* bar(unsigned char* base) {
     return reinterpret_cast<unsigned long long*>(base + PHI + OWN + RING + SIDE + SPL);
   }
-  // thread 0 sets up the barrier for the CTA's threads; the caller then syncs
+  static __device__ __forceinline__ unsigned long long* full(unsigned char* base) { return bar(base) + 1; }
+  static __device__ __forceinline__ unsigned long long* empty(unsigned char* base) { return bar(base) + 1 + D; }
+  // thread 0 sets up the barriers for the CTA's threads; the caller then syncs
   static __device__ __forceinline__ void init(unsigned char* base) {
-    if (threadIdx.x == 0 && threadIdx.y == 0) mbar_init(bar(base), TX * TY);
+    if (threadIdx.x == 0 && threadIdx.y == 0) {
+      mbar_init(bar(base), TX * TY);
+      if constexpr (BOXED)
+        for (int q = 0; q < 2 * D; ++q) mbar_init(bar(base) + 1 + q, TX * TY);
+    }
   }
+};
+
+// Barrier phases a CTA has gone through (kept across the columns a
+// persistent CTA marches): the plane barrier's parity and, per stage slot,
+// the parity of the next FULL / EMPTY phase (bit q)
+struct LeanSync {
+  unsigned bar = 0, full = 0, empty = 0;
 };
 
 // One column march: cells [x0, x0+TX) x [y0, y0+TY) x [z0, zend) of one box.
 // SD: the stored pairs are sum / difference pairs (16-bit storage).
-template <typename S, int TX, int TY, bool PART, bool SD = false, bool SDP = false>
+template <typename S, int TX, int TY, bool PART, bool SD = false, bool SDP = false, bool BOX = false>
 __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restrict__ B, const Geom& g,
                                             const LeanConst<typename Store<S>::C>& K, int x0, int y0, int z0,
                                             int zend, unsigned long long* err, int64_t step,
@@ -723,7 +791,7 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
                                             typename Store<S>::C (*sphi)[Ring<TX, TY>::CELLS],
                                             typename SPair<S>::R* stage, SideRec<typename Store<S>::C>* side,
                                             unsigned long long* bar,
-                                            unsigned& bar_parity, float* spl = nullptr,
+                                            LeanSync& sy, float* spl = nullptr,
                                             const float* __restrict__ split_in = nullptr,
                                             float* __restrict__ split_out = nullptr) {
   using C = typename Store<S>::C;
@@ -749,30 +817,76 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
   using SR = typename SPair<S>::R;
   constexpr int RN = R::N;
   constexpr bool STAGED = kStaged<S, PART>;
+  constexpr bool BOXED = LeanSmem<S, TX, TY, PART, SDP, BOX>::BOXED;
   constexpr int D = kDepth<S, PART>;
   constexpr bool ASYNC = STAGED || PART;  // copy groups in flight
-  constexpr int WM = LeanSmem<S, TX, TY, PART, SDP>::WIN - 1;  // window slot of plane p: p & WM
-  SR* const ring_stage = STAGED ? stage + D * Q * NT : nullptr;
+  constexpr int WM = LeanSmem<S, TX, TY, PART, SDP, BOX>::WIN - 1;  // window slot of plane p: p & WM
+  SR* const ring_stage = (STAGED && !BOXED) ? stage + D * Q * NT : nullptr;
   SideRec<C>* const side_ring = PART ? side + D * NT : nullptr;
   const Planes<const S> Ap{A, 2 * g.n};
   const Planes<S> Bp{B, 2 * g.n};
 
   // slots of plane p (p >= z0 - 1): own cells D deep, ring cells 2 deep
-  auto own_q = [&](int p) { return (p - z0 + 1) % D; };
+  // (the own slot q of a plane is passed along: plane z0 - 1 + k has slot
+  // k % D, and the march advances it by one per plane without a division)
   auto ring_q = [&](int p) { return (p - z0 + 1) & 1; };
-  auto own_slot = [&](int p) { return stage + own_q(p) * (Q * NT) + tid; };
+  auto own_slot = [&](int q) { return stage + q * (Q * NT) + tid; };
   auto ring_slot = [&](int p) { return ring_stage + ring_q(p) * (Q * RN) + tid; };
+
+  // Boxes: the slot of plane p holds Q direction boxes of LeanBox::ELEMS
+  // pairs; the own / ring cell's pull of direction l is at its base minus e_lx
+  using BX = LeanBox<TX, TY>;
+  const int obase = (ty + 1) * BX::BW + tx + 4, rbase = ry * BX::BW + rx + 3;
+  auto box_slot = [&](int q) { return stage + q * (Q * BX::ELEMS); };
+  unsigned long long* const fullb = bar + 1;
+  unsigned long long* const emptyb = bar + 1 + D;
+  // this thread's granule position: copier threads are the last COPIERS of
+  // the CTA (the ring cells sit on the first threads); copier k takes box
+  // row r, granule c of the directions of parity grp
+  const int ci = tid - (NT - BX::COPIERS);
+  const bool copier = BOXED && ci >= 0;
+  const int cgrp = ci >= BX::POS ? 1 : 0, cpos = ci - cgrp * BX::POS;
+  const int crow = cpos / BX::GR, ccol = cpos - crow * BX::GR;
+  // first cell of the granule in its plane for e_ly = +1, 0, -1: row
+  // y0 - 1 - e_ly + crow, column x0 - 4 + 4 ccol (periodic; nx % 4 == 0 keeps
+  // a granule inside one row)
+  unsigned cyx[3] = {0, 0, 0};
+  if constexpr (BOXED) {
+    if (copier) {
+      const int cxg = wrap0(x0 - 4 + 4 * ccol, g.nx);
+#pragma unroll
+      for (int k = 0; k < 3; ++k) cyx[k] = unsigned(wrap0(y0 - 1 - (1 - k) + crow, g.ny) * g.nx + cxg);  // k = 1 - e_ly
+    }
+  }
+  const unsigned plane_cells = unsigned(g.nx) * unsigned(g.ny);
+  // the copies of plane p: direction boxes of one parity, one granule each
+  auto issue_boxes = [&](int p, int q) {
+    SR* const dst = box_slot(q) + crow * BX::BW + 4 * ccol;
+    unsigned zo[3];  // plane offsets for e_lz = +1, 0, -1
+#pragma unroll
+    for (int k = 0; k < 3; ++k) zo[k] = unsigned(wrap_plane(p - (1 - k), g.nz)) * plane_cells;
+    auto one = [&](auto lc) {
+      constexpr int l = decltype(lc)::value;
+      const unsigned cell = zo[1 - ez(l)] + cyx[1 - ey(l)];
+      cp_async16(dst + l * BX::ELEMS, Ap.at(l, int(cell)));
+    };
+    if (cgrp == 0) {
+      unroll_even(one);
+    } else {
+      unroll_odd(one);
+    }
+  };
 
   // Start plane p: 16-bit storage copies the pulls of the own and the ring
   // cell into the stage; with spheres, the flag words and the side phase
   // field of both cells are copied too (all in one copy group).
-  auto issue = [&](int p) {
+  auto issue = [&](int p, int q) {
     const int zz = wrap_plane(p, g.nz);
     if constexpr (PART) {
       if (parts) {
         // unsigned cell offsets: one 32 x 32 -> 64-bit multiply-add per address
         const unsigned co = unsigned(x) + unsigned(g.nx) * (unsigned(y) + unsigned(g.ny) * unsigned(zz));
-        SideRec<C>* so = side + own_q(p) * NT + tid;
+        SideRec<C>* so = side + q * NT + tid;
         cp_async4(&so->fnew_w, PT.fnew + size_t(co & ~3u));
         cp_async4(&so->fold_w, PT.fold + size_t(co & ~3u));
         cp_async_c(&so->phi, PT.phi + size_t(co));
@@ -785,10 +899,12 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
         }
       }
     }
-    if constexpr (STAGED) {
+    if constexpr (BOXED) {
+      if (copier) issue_boxes(p, q);
+    } else if constexpr (STAGED) {
       PullIdx P;
       pull_idx(g, x, y, zz, P);
-      pull_async<S>(A, g.n, P, own_slot(p), NT);
+      pull_async<S>(A, g.n, P, own_slot(q), NT);
       if (ringer) {
         pull_idx(g, rxg, ryg, zz, P);
         pull_async<S>(A, g.n, P, ring_slot(p), RN);
@@ -796,16 +912,37 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
     }
     if constexpr (SDP) {  // the phase field the pulled pairs were encoded against
       const unsigned co = unsigned(x) + unsigned(g.nx) * (unsigned(y) + unsigned(g.ny) * unsigned(zz));
-      cp_async4(spl + own_q(p) * NT + tid, split_in + size_t(co));
+      cp_async4(spl + q * NT + tid, split_in + size_t(co));
       if (ringer) {
         const unsigned cr = unsigned(rxg) + unsigned(g.nx) * (unsigned(ryg) + unsigned(g.ny) * unsigned(zz));
         cp_async4(spl + D * NT + ring_q(p) * RN + tid, split_in + size_t(cr));
       }
     }
-    if constexpr (ASYNC) cp_async_commit();
+    if constexpr (BOXED) mbar_arrive_cp_async(fullb + q);
+    else if constexpr (ASYNC) cp_async_commit();
   };
   auto settle = [&]() {  // every copy group but the newest has landed
-    if constexpr (ASYNC) cp_async_wait<1>();
+    if constexpr (ASYNC && !BOXED) cp_async_wait<1>();
+  };
+  // boxes: every thread's copies of plane p have landed
+  auto full_wait = [&](int q) {
+    if constexpr (BOXED) {
+      if (!mbar_wait(fullb + q, (sy.full >> q) & 1u)) raise_error(err, LBX_DEV_WAIT_TIMEOUT, step, -2);
+      sy.full ^= 1u << q;
+    }
+  };
+  // boxes: this thread has read plane p for the last time / every thread has
+  // (the round of the slot this thread arrived at last)
+  auto empty_arrive = [&](int q) {
+    if constexpr (BOXED) {
+      mbar_arrive(emptyb + q);
+      sy.empty ^= 1u << q;
+    }
+  };
+  auto empty_wait = [&](int q) {
+    if constexpr (BOXED) {
+      if (!mbar_wait(emptyb + q, ((sy.empty >> q) & 1u) ^ 1u)) raise_error(err, LBX_DEV_WAIT_TIMEOUT, step, -3);
+    }
   };
   // flags (this step, previous step) of a cell from its side record
   auto flags_of = [&](const SideRec<C>* r, int cell, int8_t& fn, int8_t& fo) {
@@ -821,8 +958,8 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
   // densities, a surface cell the wetting kernel's phase field (both kernels
   // store (rR - rB) / (rR + rB) of the densities they write), and every other
   // solid cell densities 0 (init_rho*_CG's MINDENS).
-  auto cell_phase = [&](int cx, int cy, int zz, bool check, bool is_own, const SR* st, int stride,
-                        const SideRec<C>* rec, C& rR, C& rB, C split) -> C {
+  auto cell_phase = [&](int cx, int cy, int zz, bool check, bool is_own, auto&& at, const SideRec<C>* rec, C& rR,
+                        C& rB, C split) -> C {
     const int cell = cx + g.nx * (cy + g.ny * zz);
     if constexpr (PART) {
       if (parts) {
@@ -844,7 +981,7 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
       }
     }
     if constexpr (STAGED) {
-      stage_rho<S, C, SD, SDP>(st, stride, K, rR, rB, split);
+      stage_rho<S, C, SD, SDP>(at, K, rR, rB, split);
     } else {
       PullIdx P;
       pull_idx(g, cx, cy, zz, P);
@@ -858,28 +995,40 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
   };
 
   // phase field of plane p (own cell and ring cell) into its window slot
-  auto phase_plane = [&](int p, C& rRo, C& rBo) {
+  auto phase_plane = [&](int p, int q, C& rRo, C& rBo) {
     const int zz = wrap_plane(p, g.nz);
     const bool owned = active && p >= z0 && p < zend;
-    const SideRec<C>* so = PART ? side + own_q(p) * NT + tid : nullptr;
-    sphi[p & WM][own] = cell_phase(x, y, zz, owned, true, STAGED ? own_slot(p) : nullptr, NT, so, rRo, rBo,
-                                   SDP ? C(spl[own_q(p) * NT + tid]) : C(0));
+    const SideRec<C>* so = PART ? side + q * NT + tid : nullptr;
+    const SR* const ob = BOXED ? box_slot(q) + obase : (STAGED ? own_slot(q) : nullptr);
+    auto own_at = [&](int l) -> SR {
+      if constexpr (BOXED) return ob[l * BX::ELEMS - ex(l)];
+      else return ob[l * NT];
+    };
+    sphi[p & WM][own] = cell_phase(x, y, zz, owned, true, own_at, so, rRo, rBo,
+                                   SDP ? C(spl[q * NT + tid]) : C(0));
     if (ringer) {
       C qR, qB;
       const SideRec<C>* sr = PART ? side_ring + ring_q(p) * RN + tid : nullptr;
-      sphi[p & WM][rslot] = cell_phase(rxg, ryg, zz, false, false, STAGED ? ring_slot(p) : nullptr, RN, sr, qR, qB,
+      const SR* const rb = BOXED ? box_slot(q) + rbase : (STAGED ? ring_slot(p) : nullptr);
+      auto ring_at = [&](int l) -> SR {
+        if constexpr (BOXED) return rb[l * BX::ELEMS - ex(l)];
+        else return rb[l * RN];
+      };
+      sphi[p & WM][rslot] = cell_phase(rxg, ryg, zz, false, false, ring_at, sr, qR, qB,
                                        SDP ? C(spl[D * NT + ring_q(p) * RN + tid]) : C(0));
     }
   };
 
   C rRn, rBn, rRc, rBc;
-  issue(z0 - 1);
-  issue(z0);
+  issue(z0 - 1, 0);
+  issue(z0, 1);
   settle();
-  phase_plane(z0 - 1, rRc, rBc);
-  issue(z0 + 1);
+  full_wait(0);
+  phase_plane(z0 - 1, 0, rRc, rBc);
+  issue(z0 + 1, 2 % D);
   settle();
-  phase_plane(z0, rRn, rBn);
+  full_wait(1);
+  phase_plane(z0, 1, rRn, rBn);
   __syncthreads();  // planes z0-1 and z0 of the window
   PlaneGrad<C> gm{}, g0{};
   if constexpr (STAGED) {
@@ -889,15 +1038,24 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
     }
     __syncthreads();  // the slot of plane z0-1 is rewritten in the first iteration
   }
+  int qz = 1;  // own slot of plane z
   for (int z = z0; z < zend; ++z) {
     rRc = rRn;
     rBc = rBn;
+    const int q1 = qz == D - 1 ? 0 : qz + 1;  // plane z+1
+    const int q2 = q1 == D - 1 ? 0 : q1 + 1;  // plane z+2, the slot of plane z-1
     // plane z+2 is copied while z+1 is summed and z collided; the copies
     // into the slots of plane z-1 start after this thread's last read of them
-    if (z + 2 <= zend) issue(z + 2);
-    else if constexpr (ASYNC) cp_async_commit();  // one group per iteration
+    // (boxes: after every thread's; plane z0-1 was read in the prologue only)
+    if (z + 2 <= zend) {
+      if (z > z0) empty_wait(q2);
+      issue(z + 2, q2);
+    } else if constexpr (ASYNC && !BOXED) {
+      cp_async_commit();  // one group per iteration
+    }
     settle();
-    phase_plane(z + 1, rRn, rBn);
+    full_wait(q1);
+    phase_plane(z + 1, q1, rRn, rBn);
     mbar_arrive(bar);
     // Window reads: with staged pulls, plane z+1 after the wait below (its
     // other slot, plane z+2, is written in the next iteration, after every
@@ -912,7 +1070,7 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
       if constexpr (PART) {
         if (parts) {
           int8_t fn, fo;
-          flags_of(side + own_q(z) * NT + tid, cell, fn, fo);
+          flags_of(side + qz * NT + tid, cell, fn, fo);
           // a solid cell keeps the plain pull (see below)
           collide = fn == LBX_FLUID_FLUID;
           // make_fluid already wrote a new node's populations (stored form) into B
@@ -922,8 +1080,10 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
     }
     // Stored pairs of this cell: the pull (in the stage since two
     // iterations, or issued here), or a new node's populations in B.
+    const SR* const zb = BOXED ? box_slot(qz) + obase : nullptr;
     auto pulled = [&](int l) -> SR {
-      if constexpr (STAGED) return own_slot(z)[l * NT];
+      if constexpr (BOXED) return zb[l * BX::ELEMS - ex(l)];
+      else if constexpr (STAGED) return own_slot(qz)[l * NT];
       else return SPair<S>::ldr(Ap.at(l, pull_one(g, x, y, z, l)));
     };
     auto refilled = [&](int l) -> SR { return SPair<S>::ldr(Bp.at(l, cell)); };
@@ -956,8 +1116,8 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
       }
       rx = relax_sums(K, Ssum, rRc, rBc, Store<S>::shifted);
     }
-    if (!mbar_wait(bar, bar_parity)) raise_error(err, LBX_DEV_WAIT_TIMEOUT, step, -1);
-    bar_parity ^= 1u;
+    if (!mbar_wait(bar, sy.bar)) raise_error(err, LBX_DEV_WAIT_TIMEOUT, step, -1);
+    sy.bar ^= 1u;
     const C* const win[3] = {sphi[(z - 1) & WM], sphi[z & WM], sphi[(z + 1) & WM]};  // planes z - 1 .. z + 1
     (void)win;
     if (active) {
@@ -969,6 +1129,10 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
       // only raw population dumps of solid cells differ.
       P2<C> gp[Q];
       bool done = false;
+      auto store_all = [&](const P2<C>* v) {
+#pragma unroll
+        for (int l = 0; l < Q; ++l) SPair<S>::st(Bp.at(l, cell), v[l]);
+      };
       if constexpr (STAGED) {
         const PlaneGrad<C> gpl = plane_grad<C, R::RX>(sphi[(z + 1) & WM], own);
         if (collide) {
@@ -995,12 +1159,17 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
           }
         }
         done = recolour_sums<C, SD, SDP, R::RX>(K, rx, rRc, rBc, px, py, pz, Store<S>::shifted, gp, win, own);
+        // stored on each path by itself: one set of values per path, no
+        // register copies to merge the two (with spheres, where more state is
+        // live, the persistent multi-box kernel would spill: one store there)
+        if constexpr (!PART)
+          if (done) store_all(gp);
       }
       if (!done) {
 #pragma unroll
         for (int l = 0; l < Q; ++l) gp[l] = SPair<S>::cvt(pulled(l));
         if constexpr (SDP) {  // (total, E) -> (total, R - B) with this cell's split of the last step
-          const C ph = spl[own_q(z) * NT + tid];
+          const C ph = spl[qz * NT + tid];
 #pragma unroll
           for (int l = 0; l < Q; ++l) gp[l].y = fm(ph, gp[l].x + K.ssd[0][wclass(l)], gp[l].y);
         }
@@ -1019,25 +1188,28 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
           for (int l = 0; l < Q; ++l)
             gp[l].y = fm(-win[1 + ez(l)][own + ey(l) * R::RX + ex(l)], gp[l].x + K.ssd[0][wclass(l)], gp[l].y);
         }
+        if constexpr (!PART) store_all(gp);
       }
-#pragma unroll
-      for (int l = 0; l < Q; ++l) SPair<S>::st(Bp.at(l, cell), gp[l]);
+      if constexpr (PART) store_all(gp);
       if constexpr (SDP) split_out[size_t(unsigned(cell))] = sphi[z & WM][own];  // what the receivers decode with
     }
+    // boxes: plane z is not read again; its slot takes plane z+3 next iteration
+    if (z + 3 <= zend) empty_arrive(qz);
+    qz = q1;
   }
   if constexpr (ASYNC) cp_async_wait<0>();  // nothing in flight when the shared memory is reused
 }
 
-template <typename S, int TX, int TY, int MINB, bool PART, bool SD = false, bool SDP = false>
+template <typename S, int TX, int TY, int MINB, bool PART, bool SD = false, bool SDP = false, bool BOX = false>
 __global__ void __launch_bounds__(TX* TY, MINB)
     k_cg_lean(const S* __restrict__ A, S* __restrict__ B, Geom g, LeanConst<typename Store<S>::C> K, int zlen,
               unsigned long long* err, int64_t step, LeanPart<typename Store<S>::C> PT,
               const float* __restrict__ split_in, float* __restrict__ split_out, const int4* __restrict__ plan) {
   extern __shared__ __align__(16) unsigned char lean_smem[];
-  using M = LeanSmem<S, TX, TY, PART, SDP>;
+  using M = LeanSmem<S, TX, TY, PART, SDP, BOX>;
   M::init(lean_smem);
   __syncthreads();
-  unsigned parity = 0;
+  LeanSync sy;
   // the column and z-segment of this CTA: from the grid (equal segments) or
   // from the launch's plan (x0, y0, z0, zend per CTA)
   int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY, z0 = blockIdx.z * zlen, z1 = min(z0 + zlen, g.nz);
@@ -1048,9 +1220,9 @@ __global__ void __launch_bounds__(TX* TY, MINB)
     z0 = w.z;
     z1 = w.w;
   }
-  lean_column<S, TX, TY, PART, SD, SDP>(A, B, g, K, x0, y0, z0, z1, err, step, PT, M::phi(lean_smem),
-                                        M::stage(lean_smem), M::side(lean_smem), M::bar(lean_smem), parity,
-                                        M::spl(lean_smem), split_in, split_out);
+  lean_column<S, TX, TY, PART, SD, SDP, BOX>(A, B, g, K, x0, y0, z0, z1, err, step, PT, M::phi(lean_smem),
+                                             M::stage(lean_smem), M::side(lean_smem), M::bar(lean_smem), sy,
+                                             M::spl(lean_smem), split_in, split_out);
 }
 
 // ---------------------------------------------------------------------------
@@ -1072,23 +1244,23 @@ struct WorkItem {
   int box, x0, y0, z0, zend;
 };
 
-template <typename S, int TX, int TY, int MINB, bool PART, bool SD = false>
+template <typename S, int TX, int TY, int MINB, bool PART, bool SD = false, bool BOX = false>
 __global__ void __launch_bounds__(TX* TY, MINB)
     k_cg_lean_multi(const BoxDesc<typename Store<S>::C>* __restrict__ boxes, const WorkItem* __restrict__ work,
                     int nwork, LeanConst<typename Store<S>::C> K) {
   using C = typename Store<S>::C;
   extern __shared__ __align__(16) unsigned char lean_smem[];
-  using M = LeanSmem<S, TX, TY, PART>;
+  using M = LeanSmem<S, TX, TY, PART, false, BOX>;
   M::init(lean_smem);
   __syncthreads();
-  unsigned parity = 0;
+  LeanSync sy;
   for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
     const WorkItem it = work[w];
     const BoxDesc<C> bd = boxes[it.box];
-    lean_column<S, TX, TY, PART, SD>((const S*)bd.A, (S*)bd.B, bd.g, K, it.x0, it.y0, it.z0, it.zend, bd.err,
-                                     bd.step, bd.pt, M::phi(lean_smem), M::stage(lean_smem), M::side(lean_smem),
-                                 M::bar(lean_smem), parity);
-    __syncthreads();  // the window is reused by the next item
+    lean_column<S, TX, TY, PART, SD, false, BOX>((const S*)bd.A, (S*)bd.B, bd.g, K, it.x0, it.y0, it.z0, it.zend,
+                                                bd.err, bd.step, bd.pt, M::phi(lean_smem), M::stage(lean_smem),
+                                                M::side(lean_smem), M::bar(lean_smem), sy);
+    __syncthreads();  // the window and the stage are reused by the next item
   }
 }
 
@@ -1173,19 +1345,20 @@ static int allow_smem(K* kernel, size_t bytes, unsigned long long& done_mask) {
 
 // Opt-in of k_cg_lean's shared memory and its resident CTAs per SM on this
 // device (the persistent grid), once per device.
-template <typename S, int TX, int TY, int MINB, bool PART, bool SD = false, bool SDP = false>
+template <typename S, int TX, int TY, int MINB, bool PART, bool SD = false, bool SDP = false, bool BOX = false>
 static int prepare_lean(int* resident) {
   static unsigned long long done = 0;
   static int per_sm[64] = {0}, sms[64] = {0};
-  int rc = allow_smem(k_cg_lean<S, TX, TY, MINB, PART, SD, SDP>, LeanSmem<S, TX, TY, PART, SDP>::BYTES, done);
+  using M = LeanSmem<S, TX, TY, PART, SDP, BOX>;
+  int rc = allow_smem(k_cg_lean<S, TX, TY, MINB, PART, SD, SDP, BOX>, M::BYTES, done);
   if (rc) return rc;
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return LBX_ERR_CUDA;
   dev &= 63;
   if (!per_sm[dev]) {
     int nb = 0, nsm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_cg_lean<S, TX, TY, MINB, PART, SD, SDP>, TX * TY,
-                                                      LeanSmem<S, TX, TY, PART, SDP>::BYTES) != cudaSuccess ||
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_cg_lean<S, TX, TY, MINB, PART, SD, SDP, BOX>, TX * TY,
+                                                      M::BYTES) != cudaSuccess ||
         cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || nb < 1 || nsm < 1)
       return LBX_ERR_CUDA;
     sms[dev] = nsm;
@@ -1195,17 +1368,22 @@ static int prepare_lean(int* resident) {
   return 0;
 }
 
-template <typename S, int TX, int TY, int MINB, bool PART, bool SD = false>
+template <typename S, int TX, int TY, int MINB, bool PART, bool SD = false, bool BOX = false>
 static int prepare_lean_multi() {
   static unsigned long long done = 0;
-  return allow_smem(k_cg_lean_multi<S, TX, TY, MINB, PART, SD>, LeanSmem<S, TX, TY, PART>::BYTES, done);
+  return allow_smem(k_cg_lean_multi<S, TX, TY, MINB, PART, SD, BOX>, LeanSmem<S, TX, TY, PART, false, BOX>::BYTES,
+                    done);
 }
 
-template <typename S, int TX, int TY, int MINB, bool PART, bool SD = false, bool SDP = false>
-static int launch_lean(Ctx& c, int zlen_override, LeanPart<typename Store<S>::C> pt) {
+// Box copies (16-bit storage): when nx is a multiple of 4 (a 16-byte granule
+// then never straddles the periodic x edge) unless switched off
+static bool use_boxes(const Ctx& c) { return c.lean_copies == 1 && c.nx % 4 == 0; }
+
+template <typename S, int TX, int TY, int MINB, bool PART, bool SD = false, bool SDP = false, bool BOX = false>
+static int launch_lean_as(Ctx& c, int zlen_override, LeanPart<typename Store<S>::C> pt) {
   using C = typename Store<S>::C;
   int resident = 0;
-  const int rc = prepare_lean<S, TX, TY, MINB, PART, SD, SDP>(&resident);
+  const int rc = prepare_lean<S, TX, TY, MINB, PART, SD, SDP, BOX>(&resident);
   if (rc) return rc;
   const int zlen = zlen_override > 0 ? zlen_override : lean_zlen(c, TX, TY, resident);
   dim3 block(TX, TY, 1);
@@ -1216,10 +1394,19 @@ static int launch_lean(Ctx& c, int zlen_override, LeanPart<typename Store<S>::C>
   int nplan = 0;
   const int4* plan = (zlen_override > 0 || !kStaged<S, PART>) ? nullptr : paired_plan(c, TX, TY, resident, &nplan);
   if (plan) grid = dim3(unsigned(nplan), 1, 1);
-  k_cg_lean<S, TX, TY, MINB, PART, SD, SDP><<<grid, block, LeanSmem<S, TX, TY, PART, SDP>::BYTES, c.stream>>>(
-      (const S*)c.pops[c.cur], (S*)c.pops[1 - c.cur], geom(c), make_lean<C>(c), zlen, c.d_err, c.step + 1, pt,
-      SDP ? c.split[c.cur] : nullptr, SDP ? c.split[1 - c.cur] : nullptr, plan);
+  k_cg_lean<S, TX, TY, MINB, PART, SD, SDP, BOX>
+      <<<grid, block, LeanSmem<S, TX, TY, PART, SDP, BOX>::BYTES, c.stream>>>(
+          (const S*)c.pops[c.cur], (S*)c.pops[1 - c.cur], geom(c), make_lean<C>(c), zlen, c.d_err, c.step + 1, pt,
+          SDP ? c.split[c.cur] : nullptr, SDP ? c.split[1 - c.cur] : nullptr, plan);
   return 0;
+}
+
+template <typename S, int TX, int TY, int MINB, bool PART, bool SD = false, bool SDP = false>
+static int launch_lean(Ctx& c, int zlen_override, LeanPart<typename Store<S>::C> pt) {
+  if constexpr (kStaged<S, PART>) {
+    if (use_boxes(c)) return launch_lean_as<S, TX, TY, MINB, PART, SD, SDP, true>(c, zlen_override, pt);
+  }
+  return launch_lean_as<S, TX, TY, MINB, PART, SD, SDP, false>(c, zlen_override, pt);
 }
 
 void kt_begin(Ctx& c);
@@ -1285,6 +1472,11 @@ int ensemble_launch(const std::vector<Ctx*>& boxes, int shape, const std::vector
   if (boxes.empty()) return LBX_ERR_ARG;
   const Ctx& c0 = *boxes[0];
   const int TX = 32, TY = shape == 1 ? 16 : 8;
+  // The persistent kernel keeps each work item's box descriptor in
+  // registers, which leaves no room for the box copies' per-thread state
+  // without spills (measured: 8-16 bytes per thread), so it stages its 16-bit
+  // pulls one copy per pull.
+  const bool boxed = false;
   return by_storage(c0, [&](auto* tag) -> int {
     using S = std::remove_pointer_t<decltype(tag)>;
     using C = typename Store<S>::C;
@@ -1313,18 +1505,22 @@ int ensemble_launch(const std::vector<Ctx*>& boxes, int shape, const std::vector
       if (desc.size() * sizeof(BoxDesc<C>) > 512 * desc.size()) return LBX_ERR_STATE;
       // shared-memory opt-in of every variant, before any capture
       int rp = 0;
-      if constexpr (std::is_same<S, double>::value) {
-        rp = prepare_lean_multi<S, 32, 8, 1, true>();
-      } else if constexpr (std::is_same<S, float>::value) {
-        rp = prepare_lean_multi<S, 32, 16, 1, true>();
-        if (!rp) rp = prepare_lean_multi<S, 32, 8, 2, true>();
-      } else if (c0.sd) {
-        rp = prepare_lean_multi<S, 32, 16, 1, true, true>();
-        if (!rp) rp = prepare_lean_multi<S, 32, 8, 2, true, true>();
-      } else {
-        rp = prepare_lean_multi<S, 32, 16, 1, true>();
-        if (!rp) rp = prepare_lean_multi<S, 32, 8, 2, true>();
-      }
+      auto prep = [&](auto box_tag) {
+        constexpr bool BX = decltype(box_tag)::value;
+        if constexpr (std::is_same<S, double>::value) {
+          rp = prepare_lean_multi<S, 32, 8, 1, true>();
+        } else if constexpr (std::is_same<S, float>::value) {
+          rp = prepare_lean_multi<S, 32, 16, 1, true>();
+          if (!rp) rp = prepare_lean_multi<S, 32, 8, 2, true>();
+        } else if (c0.sd) {
+          rp = prepare_lean_multi<S, 32, 16, 1, true, true, BX>();
+          if (!rp) rp = prepare_lean_multi<S, 32, 8, 2, true, true, BX>();
+        } else {
+          rp = prepare_lean_multi<S, 32, 16, 1, true, false, BX>();
+          if (!rp) rp = prepare_lean_multi<S, 32, 8, 2, true, false, BX>();
+        }
+      };
+      prep(std::false_type{});
       if (rp) return rp;
       if (cudaMemcpy(d_desc, desc.data(), desc.size() * sizeof(BoxDesc<C>), cudaMemcpyHostToDevice) != cudaSuccess)
         return LBX_ERR_CUDA;
@@ -1338,28 +1534,28 @@ int ensemble_launch(const std::vector<Ctx*>& boxes, int shape, const std::vector
     if constexpr (std::is_same<S, double>::value) {
       int grid = std::min(nwork, 148);
       k_cg_lean_multi<S, 32, 8, 1, true><<<grid, dim3(32, 8), LeanSmem<S, 32, 8, true>::BYTES, stream>>>(D, W, nwork, K);
+    } else if constexpr (std::is_same<S, float>::value) {
+      if (shape == 1)
+        k_cg_lean_multi<S, 32, 16, 1, true><<<std::min(nwork, 148), dim3(32, 16), LeanSmem<S, 32, 16, true>::BYTES,
+                                                stream>>>(D, W, nwork, K);
+      else
+        k_cg_lean_multi<S, 32, 8, 2, true><<<std::min(nwork, 296), dim3(32, 8), LeanSmem<S, 32, 8, true>::BYTES,
+                                               stream>>>(D, W, nwork, K);
     } else {
-      bool launched = false;
-      if constexpr (!std::is_same<S, float>::value) {
-        if (c0.sd) {  // sum / difference pairs
-          if (shape == 1)
-            k_cg_lean_multi<S, 32, 16, 1, true, true>
-                <<<std::min(nwork, 148), dim3(32, 16), LeanSmem<S, 32, 16, true>::BYTES, stream>>>(D, W, nwork, K);
-          else
-            k_cg_lean_multi<S, 32, 8, 2, true, true>
-                <<<std::min(nwork, 296), dim3(32, 8), LeanSmem<S, 32, 8, true>::BYTES, stream>>>(D, W, nwork, K);
-          launched = true;
-        }
-      }
-      if (!launched && shape == 1) {
-        int grid = std::min(nwork, 148);
-        k_cg_lean_multi<S, 32, 16, 1, true><<<grid, dim3(32, 16), LeanSmem<S, 32, 16, true>::BYTES, stream>>>(
-            D, W, nwork, K);
-      } else if (!launched) {
-        int grid = std::min(nwork, 296);
-        k_cg_lean_multi<S, 32, 8, 2, true><<<grid, dim3(32, 8), LeanSmem<S, 32, 8, true>::BYTES, stream>>>(D, W,
-                                                                                                          nwork, K);
-      }
+      auto go = [&](auto sd_tag, auto box_tag) {
+        constexpr bool SDV = decltype(sd_tag)::value, BX = decltype(box_tag)::value;
+        if (shape == 1)
+          k_cg_lean_multi<S, 32, 16, 1, true, SDV, BX>
+              <<<std::min(nwork, 148), dim3(32, 16), LeanSmem<S, 32, 16, true, false, BX>::BYTES, stream>>>(D, W,
+                                                                                                         nwork, K);
+        else
+          k_cg_lean_multi<S, 32, 8, 2, true, SDV, BX>
+              <<<std::min(nwork, 296), dim3(32, 8), LeanSmem<S, 32, 8, true, false, BX>::BYTES, stream>>>(D, W, nwork,
+                                                                                                        K);
+      };
+      (void)boxed;
+      if (c0.sd) go(std::true_type{}, std::false_type{});
+      else go(std::false_type{}, std::false_type{});
     }
     return launch_status();
   });

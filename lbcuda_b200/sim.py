@@ -122,6 +122,10 @@ class LBSim:
     def set_lean_shape(self, shape, zlen=0):
         check(self._L.lbx_set_lean_shape(self._h, int(shape), int(zlen)), "lbx_set_lean_shape")
 
+    def set_lean_copies(self, mode):
+        """16-bit pulls of the lean kernel: 1 = 16-byte box granules (default), 0 = one copy per pull."""
+        check(self._L.lbx_set_lean_copies(self._h, int(mode)), "lbx_set_lean_copies")
+
     def time_steps(self, n, kernel_timing=True):
         """(total_ms, kernel_ms, kernel_launches) of n steps, CUDA events on the context stream."""
         t = C.c_double()
