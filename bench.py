@@ -636,8 +636,8 @@ def only_region(args, local):
     rR, rB = seeded_noise_fields(Lb, Lb, Lb, seed=SEED)
     s = LBSim(make_params(Lb, model="cg", storage=args.only, sigma=SIGMA, beta=BETA))
     s.set_schedule(args.schedule)
-    if args.zlen:
-        s.set_lean_shape(0, args.zlen)
+    if args.zlen or args.shape:
+        s.set_lean_shape(args.shape, args.zlen)
     s.set_lean_copies(args.lean_copies)
     s.set_fields(rR, rB)
     s.step(args.warmup * args.lb_steps)
@@ -646,7 +646,7 @@ def only_region(args, local):
     n = args.steps * args.lb_steps
     kus = (k / nl * 1e3) if nl else None
     print(json.dumps({"only": args.only, "box": Lb, "schedule": args.schedule, "zlen": args.zlen or "auto",
-                      "lean_copies": args.lean_copies,
+                      "lean_copies": args.lean_copies, "shape": args.shape,
                       "ms_per_lattice_step": tot / n,
                       "mlups": Lb ** 3 * n / (tot * 1e-3) / 1e6, "kernel_us": kus,
                       "frac_at_basis": (BYTES_PER_CELL[args.only] * Lb ** 3 / (kus * 1e-6) / 1e9 / peaks()[0])
@@ -662,7 +662,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-extras", action="store_true", help="skip the error runs, the colloid case and the CPU baseline")
-    ap.add_argument("--only", choices=["f16", "f32", "bf16", "f64", "f16sd", "bf16sd", "f16sdp", "bf16sdp", "colloid-f16", "colloid-f32", "colloid-f16-small", "colloid-f16sd",
+    ap.add_argument("--only", choices=["f16", "f32", "bf16", "f64", "f16sd", "bf16sd", "f16sdp", "bf16sdp", "colloid-f16", "colloid-f32", "colloid-f16-small", "colloid-f16sd", "colloid-f16sd-small",
                                        "colloid-f32-small", "ensemble", "ensemble-closure", "ensemble-profile", "mlp-profile", "closure",
                                        "closure12", "variants", "errors", "bgk",
                                        "bgk-256"],
@@ -672,6 +672,7 @@ def main():
     ap.add_argument("--box", type=int, default=L, help="lattice edge of the --only storage runs")
     ap.add_argument("--zlen", type=int, default=0,
                     help="--only storage runs: equal z-segments of this length (0: automatic plan)")
+    ap.add_argument("--shape", type=int, default=0, help="--only storage runs: lean kernel CTA, 0 = 32x8, 1 = 32x16")
     ap.add_argument("--lean-copies", type=int, default=1,
                     help="--only storage runs: 16-bit pulls as box granules (1) or one copy per pull (0)")
     ap.add_argument("--save-weights", default=None,

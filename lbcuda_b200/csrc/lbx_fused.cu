@@ -723,6 +723,13 @@ struct LeanBox {
   static constexpr int G = NT / POS;  // copy groups: group k copies directions k, k + G, ...
   static_assert(G == 2, "box copies are written for two groups (even / odd directions)");
   static constexpr int COPIERS = G * POS;
+  // particle variant: the flag bytes of this and of the previous step (rows
+  // y0 - 1 .. y0 + TY, bytes x0 - 16 .. x0 + TX + 15: 16-byte granules at
+  // multiples of 16 cells, so nx % 16 == 0), copied by group 0, and the side
+  // phase field (the pull box's rows and columns, e = 0), copied by group 1
+  static constexpr int FBW = TX + 32, FGR = FBW / 16, FB = ROWS * FBW;  // bytes per row / granules / per array
+  static constexpr int FPOS = 2 * ROWS * FGR;
+  static_assert(FPOS <= POS, "flag granules: one per copier of group 0");
 };
 
 template <typename S, int TX, int TY, bool PART, bool SDP = false, bool BOX = false>
@@ -740,13 +747,15 @@ struct LeanSmem {
                                 : BOXED          ? sizeof(R) * D * Q * LeanBox<TX, TY>::ELEMS
                                                  : sizeof(R) * D * Q * NT;
   static constexpr size_t RING = (kStaged<S, PART> && !BOXED) ? sizeof(R) * 2 * Q * RN : 0;
-  static constexpr size_t SIDE = PART ? (sizeof(SideRec<C>) * (D * NT + 2 * RN) + 15) / 16 * 16 : 0;
+  static constexpr size_t SIDE = !PART ? 0
+                                 : BOXED ? size_t(D) * (2 * LeanBox<TX, TY>::FB + sizeof(C) * LeanBox<TX, TY>::ELEMS)
+                                         : (sizeof(SideRec<C>) * (D * NT + 2 * RN) + 15) / 16 * 16;
   // predicted split: each own / ring cell's phase field of the last step, copied with its pulls
   static constexpr size_t SPL = SDP ? (4 * (D * NT + 2 * RN) + 15) / 16 * 16 : 0;
   // the plane's split barrier; with boxes also FULL[D] and EMPTY[D]
   static constexpr size_t BAR = BOXED ? 8 * (1 + 2 * D + 1) : 16;
   static constexpr size_t BYTES = PHI + OWN + RING + SIDE + SPL + BAR;
-  static_assert(PHI % 16 == 0 && OWN % 16 == 0 && RING % 16 == 0, "stage alignment");
+  static_assert(PHI % 16 == 0 && OWN % 16 == 0 && RING % 16 == 0 && SIDE % 16 == 0, "stage alignment");
   static __device__ __forceinline__ C (*phi(unsigned char* base))[CELLS] {
     return reinterpret_cast<C(*)[CELLS]>(base);
   }
@@ -820,6 +829,7 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
   constexpr bool BOXED = LeanSmem<S, TX, TY, PART, SDP, BOX>::BOXED;
   constexpr int D = kDepth<S, PART>;
   constexpr bool ASYNC = STAGED || PART;  // copy groups in flight
+  constexpr bool SPLIT_STORE = !PART;  // see the stores below
   constexpr int WM = LeanSmem<S, TX, TY, PART, SDP, BOX>::WIN - 1;  // window slot of plane p: p & WM
   SR* const ring_stage = (STAGED && !BOXED) ? stage + D * Q * NT : nullptr;
   SideRec<C>* const side_ring = PART ? side + D * NT : nullptr;
@@ -851,13 +861,28 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
   // y0 - 1 - e_ly + crow, column x0 - 4 + 4 ccol (periodic; nx % 4 == 0 keeps
   // a granule inside one row)
   unsigned cyx[3] = {0, 0, 0};
+  // particle variant, group 0: the flag granule of this copier (array fnew /
+  // fold, its first cell in the plane, its place in the flag box)
+  unsigned fyx = 0;
+  int fdst = -1;
   if constexpr (BOXED) {
     if (copier) {
       const int cxg = wrap0(x0 - 4 + 4 * ccol, g.nx);
 #pragma unroll
       for (int k = 0; k < 3; ++k) cyx[k] = unsigned(wrap0(y0 - 1 - (1 - k) + crow, g.ny) * g.nx + cxg);  // k = 1 - e_ly
+      if (PART && cgrp == 0 && cpos < BX::FPOS) {
+        const int arr = cpos / (BX::ROWS * BX::FGR), rem = cpos - arr * (BX::ROWS * BX::FGR);
+        const int frow = rem / BX::FGR, fgr = rem - frow * BX::FGR;
+        fyx = unsigned(wrap0(y0 - 1 + frow, g.ny) * g.nx + wrap0(x0 - 16 + 16 * fgr, g.nx));
+        fdst = arr * BX::FB + frow * BX::FBW + 16 * fgr;
+      }
     }
   }
+  // particle boxes of slot q: flags [2][FB] bytes (this step, previous step),
+  // then the side phase field [ELEMS]
+  unsigned char* const fbox = (PART && BOXED) ? reinterpret_cast<unsigned char*>(side) : nullptr;
+  C* const pbox = (PART && BOXED) ? reinterpret_cast<C*>(fbox + D * 2 * BX::FB) : nullptr;
+  const int ofb = (ty + 1) * BX::FBW + tx + 16, rfb = ry * BX::FBW + rx + 15;  // own / ring cell's flag byte
   const unsigned plane_cells = unsigned(g.nx) * unsigned(g.ny);
   // the copies of plane p: direction boxes of one parity, one granule each
   auto issue_boxes = [&](int p, int q) {
@@ -875,6 +900,14 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
     } else {
       unroll_odd(one);
     }
+    if constexpr (PART) {
+      if (parts) {
+        if (cgrp == 1)
+          cp_async16(pbox + q * BX::ELEMS + crow * BX::BW + 4 * ccol, PT.phi + size_t(zo[1] + cyx[1]));
+        else if (fdst >= 0)
+          cp_async16(fbox + q * 2 * BX::FB + fdst, (fdst >= BX::FB ? PT.fold : PT.fnew) + size_t(zo[1] + fyx));
+      }
+    }
   };
 
   // Start plane p: 16-bit storage copies the pulls of the own and the ring
@@ -882,7 +915,7 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
   // field of both cells are copied too (all in one copy group).
   auto issue = [&](int p, int q) {
     const int zz = wrap_plane(p, g.nz);
-    if constexpr (PART) {
+    if constexpr (PART && !BOXED) {
       if (parts) {
         // unsigned cell offsets: one 32 x 32 -> 64-bit multiply-add per address
         const unsigned co = unsigned(x) + unsigned(g.nx) * (unsigned(y) + unsigned(g.ny) * unsigned(zz));
@@ -958,23 +991,24 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
   // densities, a surface cell the wetting kernel's phase field (both kernels
   // store (rR - rB) / (rR + rB) of the densities they write), and every other
   // solid cell densities 0 (init_rho*_CG's MINDENS).
-  auto cell_phase = [&](int cx, int cy, int zz, bool check, bool is_own, auto&& at, const SideRec<C>* rec, C& rR,
-                        C& rB, C split) -> C {
+  // side(cell, fn, fo) gives the cell's flags, side_phi() its side phase field
+  auto cell_phase = [&](int cx, int cy, int zz, bool check, bool is_own, auto&& at, auto&& side, auto&& side_phi,
+                        C& rR, C& rB, C split) -> C {
     const int cell = cx + g.nx * (cy + g.ny * zz);
     if constexpr (PART) {
       if (parts) {
         int8_t fn, fo;
-        flags_of(rec, cell, fn, fo);
+        side(cell, fn, fo);
         if (fn != LBX_FLUID_FLUID || fo != LBX_FLUID_FLUID) {
           rR = C(0);
           rB = C(0);
-          if (fn == LBX_FLUID_SPHERELIST) return rec->phi;
+          if (fn == LBX_FLUID_SPHERELIST) return side_phi();
           if (fn == LBX_FLUID_FLUID) {  // new fluid cell
             if (is_own) {
               rR = PT.rhoR[size_t(unsigned(cell))];
               rB = PT.rhoB[size_t(unsigned(cell))];
             }
-            return rec->phi;
+            return side_phi();
           }
           return phase_of(rR, rB);
         }
@@ -998,23 +1032,47 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
   auto phase_plane = [&](int p, int q, C& rRo, C& rBo) {
     const int zz = wrap_plane(p, g.nz);
     const bool owned = active && p >= z0 && p < zend;
-    const SideRec<C>* so = PART ? side + q * NT + tid : nullptr;
+    const SideRec<C>* so = (PART && !BOXED) ? side + q * NT + tid : nullptr;
     const SR* const ob = BOXED ? box_slot(q) + obase : (STAGED ? own_slot(q) : nullptr);
     auto own_at = [&](int l) -> SR {
       if constexpr (BOXED) return ob[l * BX::ELEMS - ex(l)];
       else return ob[l * NT];
     };
-    sphi[p & WM][own] = cell_phase(x, y, zz, owned, true, own_at, so, rRo, rBo,
+    auto own_side = [&](int cell, int8_t& fn, int8_t& fo) {
+      if constexpr (BOXED) {
+        fn = int8_t(fbox[q * 2 * BX::FB + ofb]);
+        fo = int8_t(fbox[q * 2 * BX::FB + BX::FB + ofb]);
+      } else {
+        flags_of(so, cell, fn, fo);
+      }
+    };
+    auto own_sphi = [&]() -> C {
+      if constexpr (BOXED) return pbox[q * BX::ELEMS + obase];
+      else return so->phi;
+    };
+    sphi[p & WM][own] = cell_phase(x, y, zz, owned, true, own_at, own_side, own_sphi, rRo, rBo,
                                    SDP ? C(spl[q * NT + tid]) : C(0));
     if (ringer) {
       C qR, qB;
-      const SideRec<C>* sr = PART ? side_ring + ring_q(p) * RN + tid : nullptr;
+      const SideRec<C>* sr = (PART && !BOXED) ? side_ring + ring_q(p) * RN + tid : nullptr;
       const SR* const rb = BOXED ? box_slot(q) + rbase : (STAGED ? ring_slot(p) : nullptr);
       auto ring_at = [&](int l) -> SR {
         if constexpr (BOXED) return rb[l * BX::ELEMS - ex(l)];
         else return rb[l * RN];
       };
-      sphi[p & WM][rslot] = cell_phase(rxg, ryg, zz, false, false, ring_at, sr, qR, qB,
+      auto ring_side = [&](int cell, int8_t& fn, int8_t& fo) {
+        if constexpr (BOXED) {
+          fn = int8_t(fbox[q * 2 * BX::FB + rfb]);
+          fo = int8_t(fbox[q * 2 * BX::FB + BX::FB + rfb]);
+        } else {
+          flags_of(sr, cell, fn, fo);
+        }
+      };
+      auto ring_sphi = [&]() -> C {
+        if constexpr (BOXED) return pbox[q * BX::ELEMS + rbase];
+        else return sr->phi;
+      };
+      sphi[p & WM][rslot] = cell_phase(rxg, ryg, zz, false, false, ring_at, ring_side, ring_sphi, qR, qB,
                                        SDP ? C(spl[D * NT + ring_q(p) * RN + tid]) : C(0));
     }
   };
@@ -1076,7 +1134,12 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
       if constexpr (PART) {
         if (parts) {
           int8_t fn, fo;
-          flags_of(side + qz * NT + tid, cell, fn, fo);
+          if constexpr (BOXED) {
+            fn = int8_t(fbox[qz * 2 * BX::FB + ofb]);
+            fo = int8_t(fbox[qz * 2 * BX::FB + BX::FB + ofb]);
+          } else {
+            flags_of(side + qz * NT + tid, cell, fn, fo);
+          }
           // a solid cell keeps the plain pull (see below)
           collide = fn == LBX_FLUID_FLUID;
           // make_fluid already wrote a new node's populations (stored form) into B
@@ -1166,9 +1229,12 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
         }
         done = recolour_sums<C, SD, SDP, R::RX>(K, rx, rRc, rBc, px, py, pz, Store<S>::shifted, gp, win, own);
         // stored on each path by itself: one set of values per path, no
-        // register copies to merge the two (with spheres, where more state is
-        // live, the persistent multi-box kernel would spill: one store there)
-        if constexpr (!PART)
+        // register copies to merge the two (FP16 128^3: 806 -> 718
+        // instructions per cell with the other changes of the box staging).
+        // With spheres one store after the merge measured faster (838
+        // against 856 instructions per cell, 111 against 114 us at 128^3 with
+        // 160 spheres), and the persistent multi-box kernel would spill.
+        if constexpr (SPLIT_STORE)
           if (done) store_all(gp);
       }
       if (!done) {
@@ -1194,9 +1260,9 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
           for (int l = 0; l < Q; ++l)
             gp[l].y = fm(-win[1 + ez(l)][own + ey(l) * R::RX + ex(l)], gp[l].x + K.ssd[0][wclass(l)], gp[l].y);
         }
-        if constexpr (!PART) store_all(gp);
+        if constexpr (SPLIT_STORE) store_all(gp);
       }
-      if constexpr (PART) store_all(gp);
+      if constexpr (!SPLIT_STORE) store_all(gp);
       if constexpr (SDP) split_out[size_t(unsigned(cell))] = sphi[z & WM][own];  // what the receivers decode with
     }
     // boxes: plane z is not read again; its slot takes plane z+3 next iteration
@@ -1383,7 +1449,9 @@ static int prepare_lean_multi() {
 
 // Box copies (16-bit storage): when nx is a multiple of 4 (a 16-byte granule
 // then never straddles the periodic x edge) unless switched off
-static bool use_boxes(const Ctx& c) { return c.lean_copies == 1 && c.nx % 4 == 0; }
+static bool use_boxes(const Ctx& c, bool part = false) {
+  return c.lean_copies == 1 && c.nx % (part ? 16 : 4) == 0;
+}
 
 template <typename S, int TX, int TY, int MINB, bool PART, bool SD = false, bool SDP = false, bool BOX = false>
 static int launch_lean_as(Ctx& c, int zlen_override, LeanPart<typename Store<S>::C> pt) {
@@ -1410,7 +1478,7 @@ static int launch_lean_as(Ctx& c, int zlen_override, LeanPart<typename Store<S>:
 template <typename S, int TX, int TY, int MINB, bool PART, bool SD = false, bool SDP = false>
 static int launch_lean(Ctx& c, int zlen_override, LeanPart<typename Store<S>::C> pt) {
   if constexpr (kStaged<S, PART>) {
-    if (use_boxes(c)) return launch_lean_as<S, TX, TY, MINB, PART, SD, SDP, true>(c, zlen_override, pt);
+    if (use_boxes(c, PART)) return launch_lean_as<S, TX, TY, MINB, PART, SD, SDP, true>(c, zlen_override, pt);
   }
   return launch_lean_as<S, TX, TY, MINB, PART, SD, SDP, false>(c, zlen_override, pt);
 }
@@ -1481,8 +1549,7 @@ int ensemble_launch(const std::vector<Ctx*>& boxes, int shape, const std::vector
   // The persistent kernel keeps each work item's box descriptor in
   // registers, which leaves no room for the box copies' per-thread state
   // without spills (measured: 8-16 bytes per thread), so it stages its 16-bit
-  // pulls one copy per pull.
-  const bool boxed = false;
+  // pulls one copy per pull (BOX = false).
   return by_storage(c0, [&](auto* tag) -> int {
     using S = std::remove_pointer_t<decltype(tag)>;
     using C = typename Store<S>::C;
@@ -1511,22 +1578,18 @@ int ensemble_launch(const std::vector<Ctx*>& boxes, int shape, const std::vector
       if (desc.size() * sizeof(BoxDesc<C>) > 512 * desc.size()) return LBX_ERR_STATE;
       // shared-memory opt-in of every variant, before any capture
       int rp = 0;
-      auto prep = [&](auto box_tag) {
-        constexpr bool BX = decltype(box_tag)::value;
-        if constexpr (std::is_same<S, double>::value) {
-          rp = prepare_lean_multi<S, 32, 8, 1, true>();
-        } else if constexpr (std::is_same<S, float>::value) {
-          rp = prepare_lean_multi<S, 32, 16, 1, true>();
-          if (!rp) rp = prepare_lean_multi<S, 32, 8, 2, true>();
-        } else if (c0.sd) {
-          rp = prepare_lean_multi<S, 32, 16, 1, true, true, BX>();
-          if (!rp) rp = prepare_lean_multi<S, 32, 8, 2, true, true, BX>();
-        } else {
-          rp = prepare_lean_multi<S, 32, 16, 1, true, false, BX>();
-          if (!rp) rp = prepare_lean_multi<S, 32, 8, 2, true, false, BX>();
-        }
-      };
-      prep(std::false_type{});
+      if constexpr (std::is_same<S, double>::value) {
+        rp = prepare_lean_multi<S, 32, 8, 1, true>();
+      } else if constexpr (std::is_same<S, float>::value) {
+        rp = prepare_lean_multi<S, 32, 16, 1, true>();
+        if (!rp) rp = prepare_lean_multi<S, 32, 8, 2, true>();
+      } else if (c0.sd) {
+        rp = prepare_lean_multi<S, 32, 16, 1, true, true>();
+        if (!rp) rp = prepare_lean_multi<S, 32, 8, 2, true, true>();
+      } else {
+        rp = prepare_lean_multi<S, 32, 16, 1, true>();
+        if (!rp) rp = prepare_lean_multi<S, 32, 8, 2, true>();
+      }
       if (rp) return rp;
       if (cudaMemcpy(d_desc, desc.data(), desc.size() * sizeof(BoxDesc<C>), cudaMemcpyHostToDevice) != cudaSuccess)
         return LBX_ERR_CUDA;
@@ -1548,20 +1611,17 @@ int ensemble_launch(const std::vector<Ctx*>& boxes, int shape, const std::vector
         k_cg_lean_multi<S, 32, 8, 2, true><<<std::min(nwork, 296), dim3(32, 8), LeanSmem<S, 32, 8, true>::BYTES,
                                                stream>>>(D, W, nwork, K);
     } else {
-      auto go = [&](auto sd_tag, auto box_tag) {
-        constexpr bool SDV = decltype(sd_tag)::value, BX = decltype(box_tag)::value;
+      auto go = [&](auto sd_tag) {
+        constexpr bool SDV = decltype(sd_tag)::value;
         if (shape == 1)
-          k_cg_lean_multi<S, 32, 16, 1, true, SDV, BX>
-              <<<std::min(nwork, 148), dim3(32, 16), LeanSmem<S, 32, 16, true, false, BX>::BYTES, stream>>>(D, W,
-                                                                                                         nwork, K);
+          k_cg_lean_multi<S, 32, 16, 1, true, SDV>
+              <<<std::min(nwork, 148), dim3(32, 16), LeanSmem<S, 32, 16, true>::BYTES, stream>>>(D, W, nwork, K);
         else
-          k_cg_lean_multi<S, 32, 8, 2, true, SDV, BX>
-              <<<std::min(nwork, 296), dim3(32, 8), LeanSmem<S, 32, 8, true, false, BX>::BYTES, stream>>>(D, W, nwork,
-                                                                                                        K);
+          k_cg_lean_multi<S, 32, 8, 2, true, SDV>
+              <<<std::min(nwork, 296), dim3(32, 8), LeanSmem<S, 32, 8, true>::BYTES, stream>>>(D, W, nwork, K);
       };
-      (void)boxed;
-      if (c0.sd) go(std::true_type{}, std::false_type{});
-      else go(std::false_type{}, std::false_type{});
+      if (c0.sd) go(std::true_type{});
+      else go(std::false_type{});
     }
     return launch_status();
   });

@@ -494,9 +494,11 @@ __device__ __forceinline__ void pulled_rho(const S* A, const Geom& g, const Shif
 // (rdim + sqrt 3) of a sphere's centre: the bounce-back of this step at the
 // fluid end of each surface link, the wetting and fill kernels in the first
 // (D3Q27) belt of a surface or uncovered cell, the drain of the next step at
-// the cells the spheres then cover.  The shell is that ball around the
-// current centre and, for a sphere that changed cell, around the previous
-// one (its uncovered cells).  The rare second-belt fallbacks pull their own.
+// the cells the spheres then cover: all of them fluid cells with a D3Q27
+// neighbour in the template.  The shell is that belt (and the template cells
+// the tile-list coverage may have left fluid) around the current centre and,
+// for a sphere that changed cell, around the previous one (its uncovered
+// cells).  The rare second-belt fallbacks pull their own.
 template <typename S>
 __global__ void __launch_bounds__(256) k_rho_shell(PDev P, const double* __restrict__ pos_cur,
                                                    const double* __restrict__ pos_old, const S* A, Geom g,
@@ -510,26 +512,14 @@ __global__ void __launch_bounds__(256) k_rho_shell(PDev P, const double* __restr
   const int cn[3] = {nint_idx(pc[0], g.nx), nint_idx(pc[1], g.ny), nint_idx(pc[2], g.nz)};
   const int co[3] = {nint_idx(po[0], g.nx), nint_idx(po[1], g.ny), nint_idx(po[2], g.nz)};
   const bool mv = moved(pc, po);
-  // old centre relative to the new one (minimum image)
-  const int nn[3] = {g.nx, g.ny, g.nz};
-  int sft[3];
-  for (int d = 0; d < 3; ++d) {
-    int v = co[d] - cn[d];
-    if (2 * v > nn[d]) v -= nn[d];
-    if (2 * v < -nn[d]) v += nn[d];
-    sft[d] = v;
-  }
   const int tot = mv ? 2 * P.n_shell : P.n_shell;
   for (int t = threadIdx.x; t < tot; t += blockDim.x) {
     const bool second = t >= P.n_shell;
     int dx, dy, dz, tv;
     unpack_off(P.offs_shell[second ? t - P.n_shell : t], dx, dy, dz, tv);
-    const int* c0 = cn;
-    if (second) {  // around the old centre, minus what the new ball covers
-      const int ex_ = dx + sft[0], ey_ = dy + sft[1], ez_ = dz + sft[2];
-      if (ex_ * ex_ + ey_ * ey_ + ez_ * ez_ <= P.shell_r2) continue;
-      c0 = co;
-    }
+    // around the old centre too (its uncovered cells' belt); a cell near
+    // both centres is summed twice, with the same result
+    const int* c0 = second ? co : cn;
     const int i1 = wrap1(c0[0] + dx, g.nx), j1 = wrap1(c0[1] + dy, g.ny), k1 = wrap1(c0[2] + dz, g.nz);
     const int y = cell0(g, i1, j1, k1);
     // outside the sphere's own template the cell is nearly always fluid: the
@@ -807,6 +797,41 @@ __device__ __forceinline__ void wall_velocity(const PDev& P, const double* pc, c
 // points one each, with the same results).
 constexpr int BB_N2P = 1, BB_COPY = 2, BB_WALL = 4, BB_ALL = 7;
 
+// Whether another sphere's template can reach into the bounce-back reach of
+// sphere a (offsets d^2 < sphereMax around its rounded centre c): such a
+// sphere has a template cell inside a's box, so it is listed in one of the
+// bins of a's box, and its rounded centre lies within 2 rmax of c (minimum
+// image).  With rmax <= BINW the box spans at most three bins per axis, those
+// of c - rmax, c and c + rmax; larger radii answer yes.  Called by every
+// thread of the CTA (a CTA-wide vote).
+__device__ bool crowded_reach(const PDev& P, const double* __restrict__ pos, const Geom& g, int a, const int c[3]) {
+  bool hit = P.rmax > BINW;
+  const int t = threadIdx.x;
+  if (!hit && t < 27) {
+    const int s[3] = {(t % 3 - 1) * P.rmax, ((t / 3) % 3 - 1) * P.rmax, (t / 9 - 1) * P.rmax};
+    const int x0 = wrap1(c[0] + s[0], g.nx) - 1, y0 = wrap1(c[1] + s[1], g.ny) - 1, z0 = wrap1(c[2] + s[2], g.nz) - 1;
+    const int bin = bin_of(P, x0, y0, z0);
+    const int cnt = min(P.bin_cnt[bin], BIN_CAP);
+    const int* L = P.bin_list + size_t(bin) * BIN_CAP;
+    const int n[3] = {g.nx, g.ny, g.nz};
+    const int lim = (2 * P.rmax + 1) * (2 * P.rmax + 1);
+    for (int u = 0; u < cnt && !hit; ++u) {
+      const int q = L[u];
+      if (q == a) continue;
+      const double* pq = pos + size_t(q) * PS;
+      const int cq[3] = {nint_idx(pq[0], g.nx), nint_idx(pq[1], g.ny), nint_idx(pq[2], g.nz)};
+      int d2 = 0;
+      for (int d = 0; d < 3; ++d) {
+        int v = cq[d] - c[d];
+        v -= n[d] * int(floorf(float(v) / float(n[d]) + 0.5f));  // minimum image
+        d2 += v * v;
+      }
+      hit = d2 < lim;
+    }
+  }
+  return __syncthreads_or(hit) != 0;
+}
+
 template <typename S>
 __global__ void __launch_bounds__(256) k_bb(PDev P, const double* __restrict__ pos, double* acc, S* B, Geom g,
                                             Shift<typename Store<S>::C> sh, LatticeT<typename Store<S>::C> L,
@@ -823,7 +848,13 @@ __global__ void __launch_bounds__(256) k_bb(PDev P, const double* __restrict__ p
   double ola[3];
   lab_omega(P, pc, ola);
   double s[6] = {0, 0, 0, 0, 0, 0};
-  for (int t = threadIdx.x; t < P.n_bb; t += blockDim.x) {
+  // Past the sphere's own surface cells (pass 0), the reach holds its dead
+  // cells and fluid cells, which no link crosses, unless another sphere's
+  // template reaches into it: pass 1 runs only then.
+  for (int pass = 0; pass < 2; ++pass) {
+  if (pass == 1 && !crowded_reach(P, pos, g, a, c)) break;
+  const int t0 = pass ? P.n_surf : 0, t1 = pass ? P.n_bb : P.n_surf;
+  for (int t = t0 + int(threadIdx.x); t < t1; t += blockDim.x) {
     int dx, dy, dz, tv, i1, j1, k1;
     unpack_off(P.offs_bb[t], dx, dy, dz, tv);
     if (!offset_cell(P, g, c, dx, dy, dz, i1, j1, k1)) continue;
@@ -952,6 +983,7 @@ __global__ void __launch_bounds__(256) k_bb(PDev P, const double* __restrict__ p
       p[0] = hR[it];
       p[1] = hB[it];
     }
+  }
   }
   double out[6] = {0, 0, 0, 0, 0, 0};
   block_sum<6>(s, out);
@@ -1449,20 +1481,30 @@ int particles_create(Ctx& c) {
         if (i * i + j * j + k * k < s->sphereMax && tv(i, j, k) != LBX_FLUID_SPHERELIST)
           offs.push_back(pack_off(i, j, k, tv(i, j, k)));
   s->n_bb = int(offs.size()) - s->n_solid;
-  // density shell: every offset within (rdim + sqrt 3) of the centre
+  // density shell: the template's fluid belt (every offset outside the
+  // template with a D3Q27 neighbour inside it; all lie within rdim + sqrt 3 of
+  // the centre), then the template cells with their values (solid template
+  // cells are fluid only when the tile-list coverage left them out, so they
+  // are tested before pulling)
   const double rs = s->rdim + std::sqrt(3.0);
   s->shell_r2 = int(std::floor(rs * rs));
   const int RS = int(std::ceil(rs));
   if (RS > 60) return LBX_ERR_ARG;  // offsets are packed in 8 bits
-  // (each with its template value: solid template cells are fluid only when
-  // the tile-list coverage left them out, so they are tested before pulling)
+  auto solid = [&](int i, int j, int k) {
+    return std::abs(i) <= R && std::abs(j) <= R && std::abs(k) <= R && tv(i, j, k) != LBX_FLUID_FLUID;
+  };
   for (int k = -RS; k <= RS; ++k)
     for (int j = -RS; j <= RS; ++j)
-      for (int i = -RS; i <= RS; ++i)
-        if (i * i + j * j + k * k <= s->shell_r2) {
-          const bool in_box = std::abs(i) <= R && std::abs(j) <= R && std::abs(k) <= R;
-          offs.push_back(pack_off(i, j, k, in_box ? tv(i, j, k) : LBX_FLUID_FLUID));
-        }
+      for (int i = -RS; i <= RS; ++i) {
+        if (solid(i, j, k)) continue;
+        bool belt = false;
+        for (int e = 1; e < Q27 && !belt; ++e) belt = solid(i + ex27(e), j + ey27(e), k + ez27(e));
+        if (belt) offs.push_back(pack_off(i, j, k, LBX_FLUID_FLUID));
+      }
+  for (int k = -R; k <= R; ++k)
+    for (int j = -R; j <= R; ++j)
+      for (int i = -R; i <= R; ++i)
+        if (solid(i, j, k)) offs.push_back(pack_off(i, j, k, tv(i, j, k)));
   s->n_shell = int(offs.size()) - s->n_solid - s->n_bb;
   if (!ok(cudaMalloc(&s->offs, offs.size() * 4))) return LBX_ERR_ALLOC;
   cudaMemcpyAsync(s->offs, offs.data(), offs.size() * 4, cudaMemcpyHostToDevice, c.stream);
