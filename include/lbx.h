@@ -310,6 +310,23 @@ int lbx_ensemble_time(void* ens, int32_t nsteps, double* ms);
  * that kernel's time per step. */
 int lbx_ensemble_tune(void* ens, int32_t trial, int32_t* chosen, double* best_ms);
 
+/* ---- z-slab decomposition --------------------------------------------- */
+/* Replaces the reference's MPI z-slab split (main.CUF:504-1000 halo swaps,
+ * setupMPI.CUF:26-30 rank layout): one context per slab holds its own planes
+ * [zlo, zhi) plus at least two halo planes on each side; lbx_step then
+ * computes and writes the own planes only.  zlo = zhi = 0 restores the
+ * whole periodic box.  Colour-gradient model on the lean kernel, no spheres
+ * (else LBX_ERR_STATE); zlo >= 2, zhi <= nz - 2 (else LBX_ERR_ARG). */
+int lbx_set_zrange(void* ctx, int32_t zlo, int32_t zhi);
+/* Bytes of a packed buffer of nplanes planes (lbx_pack_planes). */
+int lbx_plane_bytes(void* ctx, int32_t nplanes, int64_t* bytes);
+/* Planes [z0, z0 + nplanes) of the current populations (stored form; with
+ * sum / predicted-split pairs followed by their split field) to / from a
+ * packed DEVICE buffer: the halo exchange of a slab.  Enqueued on the
+ * context's stream: lbx_sync before the buffer is used elsewhere. */
+int lbx_pack_planes(void* ctx, int32_t z0, int32_t nplanes, void* dev_buf);
+int lbx_unpack_planes(void* ctx, int32_t z0, int32_t nplanes, const void* dev_buf);
+
 /* ---- measurement ------------------------------------------------------- */
 /* Colour-gradient schedule: 2 = lean single-pass kernel (default), 1 = the
  * first single-pass kernel, 0 = two passes (phase field, then collision).

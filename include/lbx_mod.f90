@@ -118,5 +118,29 @@ module lbx_mod
       import :: c_int, c_ptr
       type(c_ptr), value :: ctx
     end function
+    ! z-slab decomposition: an MPI host (one rank per slab, as setupMPI.CUF)
+    ! packs its boundary planes into a device buffer, passes it to the
+    ! neighbour rank (CUDA-aware MPI or NCCL) and unpacks the received halo
+    integer(c_int) function lbx_set_zrange(ctx, zlo, zhi) bind(C, name="lbx_set_zrange")
+      import :: c_int, c_int32_t, c_ptr
+      type(c_ptr), value :: ctx
+      integer(c_int32_t), value :: zlo, zhi
+    end function
+    integer(c_int) function lbx_plane_bytes(ctx, nplanes, bytes) bind(C, name="lbx_plane_bytes")
+      import :: c_int, c_int32_t, c_int64_t, c_ptr
+      type(c_ptr), value :: ctx
+      integer(c_int32_t), value :: nplanes
+      integer(c_int64_t), intent(out) :: bytes
+    end function
+    integer(c_int) function lbx_pack_planes(ctx, z0, nplanes, dev_buf) bind(C, name="lbx_pack_planes")
+      import :: c_int, c_int32_t, c_ptr
+      type(c_ptr), value :: ctx, dev_buf
+      integer(c_int32_t), value :: z0, nplanes
+    end function
+    integer(c_int) function lbx_unpack_planes(ctx, z0, nplanes, dev_buf) bind(C, name="lbx_unpack_planes")
+      import :: c_int, c_int32_t, c_ptr
+      type(c_ptr), value :: ctx, dev_buf
+      integer(c_int32_t), value :: z0, nplanes
+    end function
   end interface
 end module lbx_mod

@@ -97,6 +97,10 @@ SIGNATURES = {
     "lbx_set_schedule": (C.c_int, [_P, C.c_int32]),
     "lbx_set_lean_shape": (C.c_int, [_P, C.c_int32, C.c_int32]),
     "lbx_set_lean_copies": (C.c_int, [_P, C.c_int32]),
+    "lbx_set_zrange": (C.c_int, [_P, C.c_int32, C.c_int32]),
+    "lbx_plane_bytes": (C.c_int, [_P, C.c_int32, C.POINTER(C.c_int64)]),
+    "lbx_pack_planes": (C.c_int, [_P, C.c_int32, C.c_int32, _P]),
+    "lbx_unpack_planes": (C.c_int, [_P, C.c_int32, C.c_int32, _P]),
     "lbx_time_steps": (C.c_int, [_P, C.c_int32, _D, _D, _I64]),
 }
 

@@ -444,6 +444,7 @@ int lbx_set_schedule(void* ctx, int32_t fused) {
   if (fused < 0 || fused > 2) return LBX_ERR_ARG;
   if (c->p.model >= LBX_MODEL_CG_DIFFDENS && fused != 0) return LBX_ERR_ARG;
   if (c->sd && fused != 2) return LBX_ERR_ARG;  // sum / difference pairs: lean kernel only
+  if (c->zhi > 0 && fused != 2) return LBX_ERR_STATE;  // a z-slab steps on the lean kernel
   c->fused = fused;
   return 0;
 }
@@ -456,6 +457,77 @@ int lbx_set_lean_shape(void* ctx, int32_t shape, int32_t zlen) {
   c->lean_shape = shape;
   c->lean_zlen = zlen;
   return 0;
+}
+
+/* ---- z-slab decomposition ------------------------------------------------
+ * The reference splits the box into z-slabs, one MPI rank each, and swaps
+ * halo planes of populations between neighbours every step
+ * (main.CUF:504-1000, setupMPI.CUF:26-30).  Here a slab is a context of its
+ * own planes plus two halo planes on each side; the step computes the own
+ * planes only, and the host moves the halo planes between contexts or GPUs
+ * (lbcuda_b200/slabs.py) through these packed copies. */
+int lbx_set_zrange(void* ctx, int32_t zlo, int32_t zhi) {
+  Ctx* c = as_ctx(ctx);
+  if (!c) return LBX_ERR_ARG;
+  if (zlo == 0 && zhi == 0) {  // the whole box again
+    c->zlo = c->zhi = 0;
+    return 0;
+  }
+  // the step pulls from planes zlo - 2 .. zhi + 1 (the phase field of the
+  // planes next to the own ones): they must exist without a wrap
+  if (zlo < 2 || zhi > c->nz - 2 || zlo >= zhi) return LBX_ERR_ARG;
+  // the lean colour-gradient kernel only, without spheres
+  if (c->ncomp != 2 || c->q != 19 || c->p.model != LBX_MODEL_CG || c->fused != 2 || lbx::particles_active(*c) ||
+      c->p.max_particles > 0)
+    return LBX_ERR_STATE;
+  c->zlo = zlo;
+  c->zhi = zhi;
+  return 0;
+}
+
+static size_t pair_bytes(const Ctx& c) { return c.elem * size_t(c.ncomp); }
+
+/* Bytes of lbx_pack_planes for nplanes planes. */
+int lbx_plane_bytes(void* ctx, int32_t nplanes, int64_t* bytes) {
+  Ctx* c = as_ctx(ctx);
+  if (!c || !bytes || nplanes < 0) return LBX_ERR_ARG;
+  const size_t cells = size_t(nplanes) * size_t(c->nx) * size_t(c->ny);
+  *bytes = int64_t(cells * pair_bytes(*c) * size_t(c->q) + (c->sdp ? cells * sizeof(float) : 0));
+  return 0;
+}
+
+// planes [z0, z0 + np) of the current populations <-> a packed device buffer
+static int move_planes(Ctx* c, int z0, int np, char* buf, bool pack) {
+  if (!c || !buf || np <= 0 || z0 < 0 || z0 + np > c->nz) return LBX_ERR_ARG;
+  const size_t plane = size_t(c->nx) * size_t(c->ny), pb = pair_bytes(*c);
+  const size_t width = size_t(np) * plane * pb, pitch = size_t(c->n) * pb;
+  char* pops = static_cast<char*>(c->pops[c->cur]) + size_t(z0) * plane * pb;
+  cudaError_t e = pack ? cudaMemcpy2DAsync(buf, width, pops, pitch, width, size_t(c->q), cudaMemcpyDeviceToDevice,
+                                           c->stream)
+                       : cudaMemcpy2DAsync(pops, pitch, buf, width, width, size_t(c->q), cudaMemcpyDeviceToDevice,
+                                           c->stream);
+  if (e == cudaSuccess && c->sdp) {  // the phase field the pairs of these planes were encoded against
+    char* sp = reinterpret_cast<char*>(c->split[c->cur] + size_t(z0) * plane);
+    char* bs = buf + width * size_t(c->q);
+    const size_t sb = size_t(np) * plane * sizeof(float);
+    e = pack ? cudaMemcpyAsync(bs, sp, sb, cudaMemcpyDeviceToDevice, c->stream)
+             : cudaMemcpyAsync(sp, bs, sb, cudaMemcpyDeviceToDevice, c->stream);
+  }
+  return cuda_rc(e);
+}
+
+/* Copy planes [z0, z0 + nplanes) of the current populations (stored form,
+ * all directions and components; with sum / predicted-split pairs also the
+ * split field of those planes) into a packed device buffer of
+ * lbx_plane_bytes bytes: direction by direction, nplanes * nx * ny pairs each.
+ * Enqueued on the context's stream (lbx_sync before another stream reads it). */
+int lbx_pack_planes(void* ctx, int32_t z0, int32_t nplanes, void* dev_buf) {
+  return move_planes(as_ctx(ctx), z0, nplanes, static_cast<char*>(dev_buf), true);
+}
+
+/* The reverse: write a packed buffer into planes [z0, z0 + nplanes). */
+int lbx_unpack_planes(void* ctx, int32_t z0, int32_t nplanes, const void* dev_buf) {
+  return move_planes(as_ctx(ctx), z0, nplanes, static_cast<char*>(const_cast<void*>(dev_buf)), false);
 }
 
 /* Staging of the lean kernel's 16-bit pulls: 1 = box granules, 0 = one copy per pull. */

@@ -49,8 +49,12 @@ struct Ctx {
   int lean_shape = 0;       // lean kernel CTA: 0 = 32x8 (2 per SM), 1 = 32x16
   int lean_zlen = 0;        // z-segment length of the lean kernel (0 = automatic)
   int lean_copies = 1;      // 16-bit pulls: 1 = 16-byte box granules (when nx % 4 == 0), 0 = one copy per pull
+  // z-slab of a decomposed box: the step computes planes [zlo, zhi) only (the
+  // others are halo planes written by the exchange); zhi == 0: every plane
+  int zlo = 0, zhi = 0;
   void* lean_plan = nullptr;  // device table of the lean kernel's paired segments (int4 per CTA), or null
-  int lean_plan_n = 0, lean_plan_key = 0;
+  int lean_plan_n = 0;
+  int64_t lean_plan_key = 0;
   // timing of the dominant kernel (opt-in)
   int kt_on = 0;
   std::vector<cudaEvent_t> kt_ev;

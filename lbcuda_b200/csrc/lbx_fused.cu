@@ -1369,7 +1369,7 @@ static const int4* paired_plan(Ctx& c, int TX, int TY, int resident, int* n) {
   const int ncx = (c.nx + TX - 1) / TX, ncy = (c.ny + TY - 1) / TY, cols = ncx * ncy;
   const int b = std::min(cols, std::min(resident / 8, resident - 4 * cols));  // columns cut 1 + 4
   if (c.nz < 64 || 4 * cols >= resident || 5 * cols <= resident || b <= 0) return nullptr;
-  const int key = resident * 4096 + TX * 64 + TY;
+  const int64_t key = int64_t(resident) * 4096 + TX * 64 + TY;
   if (c.lean_plan && c.lean_plan_key == key) {
     *n = c.lean_plan_n;
     return static_cast<const int4*>(c.lean_plan);
@@ -1395,6 +1395,40 @@ static const int4* paired_plan(Ctx& c, int TX, int TY, int resident, int* n) {
   }
   cudaMemcpy(c.lean_plan, lng.data(), lng.size() * sizeof(int4), cudaMemcpyHostToDevice);
   c.lean_plan_n = int(lng.size());
+  c.lean_plan_key = key;
+  *n = c.lean_plan_n;
+  return static_cast<const int4*>(c.lean_plan);
+}
+
+// Plan of a z-slab (lbx_set_zrange): every column marched over the own planes
+// [zlo, zhi) only, in equal segments of at most 32 planes (as many as fill
+// the resident CTA slots when there are fewer).  Cached in the context like
+// the paired plan.
+static const int4* range_plan(Ctx& c, int TX, int TY, int resident, int* n) {
+  const int ncx = (c.nx + TX - 1) / TX, ncy = (c.ny + TY - 1) / TY, cols = ncx * ncy;
+  const int own = c.zhi - c.zlo;
+  long segs = (own + 31) / 32;
+  if (long(cols) * segs <= resident) segs = std::max(segs, long(resident) / cols);
+  segs = std::max(1L, std::min<long>(segs, own));
+  // negative: never a paired plan's key
+  const int64_t key = -(1 + int64_t(c.zlo) + 65536 * (int64_t(c.zhi) + 65536 * (int64_t(TY) + 64 * segs)));
+  if (c.lean_plan && c.lean_plan_key == key) {
+    *n = c.lean_plan_n;
+    return static_cast<const int4*>(c.lean_plan);
+  }
+  std::vector<int4> plan;
+  for (long k = 0; k < segs; ++k)
+    for (int col = 0; col < cols; ++col)
+      plan.push_back(make_int4((col % ncx) * TX, (col / ncx) * TY, c.zlo + int(k * own / segs),
+                               c.zlo + int((k + 1) * own / segs)));
+  if (c.lean_plan) cudaFree(c.lean_plan);
+  c.lean_plan = nullptr;
+  if (cudaMalloc(&c.lean_plan, plan.size() * sizeof(int4)) != cudaSuccess) {
+    c.lean_plan = nullptr;
+    return nullptr;
+  }
+  cudaMemcpy(c.lean_plan, plan.data(), plan.size() * sizeof(int4), cudaMemcpyHostToDevice);
+  c.lean_plan_n = int(plan.size());
   c.lean_plan_key = key;
   *n = c.lean_plan_n;
   return static_cast<const int4*>(c.lean_plan);
@@ -1466,7 +1500,13 @@ static int launch_lean_as(Ctx& c, int zlen_override, LeanPart<typename Store<S>:
   // their pairs from L2, which neighbouring columns out of step in z defeat
   // (FP32 128^3: 185 us with the plan, 148 us without; FP16 96 against 101)
   int nplan = 0;
-  const int4* plan = (zlen_override > 0 || !kStaged<S, PART>) ? nullptr : paired_plan(c, TX, TY, resident, &nplan);
+  const int4* plan = nullptr;
+  if (c.zhi > 0) {  // a z-slab: only its own planes
+    plan = range_plan(c, TX, TY, resident, &nplan);
+    if (!plan) return LBX_ERR_ALLOC;
+  } else if (zlen_override <= 0 && kStaged<S, PART>) {
+    plan = paired_plan(c, TX, TY, resident, &nplan);
+  }
   if (plan) grid = dim3(unsigned(nplan), 1, 1);
   k_cg_lean<S, TX, TY, MINB, PART, SD, SDP, BOX>
       <<<grid, block, LeanSmem<S, TX, TY, PART, SDP, BOX>::BYTES, c.stream>>>(

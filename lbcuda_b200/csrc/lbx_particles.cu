@@ -209,6 +209,39 @@ __device__ __forceinline__ void cross(const double a[3], const double b[3], doub
   o[2] = a[0] * b[1] - a[1] * b[0];
 }
 
+// both components of a direction and cell (adjacent, aligned to their pair)
+// in one load / store
+__device__ __forceinline__ void ld_two(const __half* p, __half& a, __half& b) {
+  const __half2 v = __ldg(reinterpret_cast<const __half2*>(p));
+  a = __low2half(v);
+  b = __high2half(v);
+}
+__device__ __forceinline__ void ld_two(const __nv_bfloat16* p, __nv_bfloat16& a, __nv_bfloat16& b) {
+  const __nv_bfloat162 v = __ldg(reinterpret_cast<const __nv_bfloat162*>(p));
+  a = __low2bfloat16(v);
+  b = __high2bfloat16(v);
+}
+__device__ __forceinline__ void ld_two(const float* p, float& a, float& b) {
+  const float2 v = __ldg(reinterpret_cast<const float2*>(p));
+  a = v.x;
+  b = v.y;
+}
+__device__ __forceinline__ void ld_two(const double* p, double& a, double& b) {
+  const double2 v = __ldg(reinterpret_cast<const double2*>(p));
+  a = v.x;
+  b = v.y;
+}
+__device__ __forceinline__ void st_two(__half* p, __half a, __half b) {
+  *reinterpret_cast<__half2*>(p) = __halves2half2(a, b);
+}
+__device__ __forceinline__ void st_two(__nv_bfloat16* p, __nv_bfloat16 a, __nv_bfloat16 b) {
+  *reinterpret_cast<__nv_bfloat162*>(p) = __halves2bfloat162(a, b);
+}
+__device__ __forceinline__ void st_two(float* p, float a, float b) { *reinterpret_cast<float2*>(p) = make_float2(a, b); }
+__device__ __forceinline__ void st_two(double* p, double a, double b) {
+  *reinterpret_cast<double2*>(p) = make_double2(a, b);
+}
+
 // fixed-order CTA reduction of NV doubles (blockDim.x == 256)
 template <int NV>
 __device__ void block_sum(double v[NV], double* out /* NV, added */) {
@@ -814,7 +847,10 @@ __device__ bool crowded_reach(const PDev& P, const double* __restrict__ pos, con
     const int cnt = min(P.bin_cnt[bin], BIN_CAP);
     const int* L = P.bin_list + size_t(bin) * BIN_CAP;
     const int n[3] = {g.nx, g.ny, g.nz};
-    const int lim = (2 * P.rmax + 1) * (2 * P.rmax + 1);
+    // a template cell of q (|o|^2 <= rdim^2) inside a's reach (|r|^2 <
+    // sphereMax): |c_q - c| = |r - o| < rdim + sqrt(sphereMax)
+    const double lim_r = P.rdim + sqrt(double(P.sphereMax));
+    const double lim = lim_r * lim_r;
     for (int u = 0; u < cnt && !hit; ++u) {
       const int q = L[u];
       if (q == a) continue;
@@ -826,7 +862,7 @@ __device__ bool crowded_reach(const PDev& P, const double* __restrict__ pos, con
         v -= n[d] * int(floorf(float(v) / float(n[d]) + 0.5f));  // minimum image
         d2 += v * v;
       }
-      hit = d2 < lim;
+      hit = double(d2) < lim;
     }
   }
   return __syncthreads_or(hit) != 0;
@@ -908,8 +944,7 @@ __global__ void __launch_bounds__(256) k_bb(PDev P, const double* __restrict__ p
         const int lf = h ? 2 * it + 1 : 2 * it + 2, lr = h ? 2 * it + 2 : 2 * it + 1;
         // the fluid end's population, or (wall phase alone) the copy already in place
         const S* p = (n2p || (mode & BB_COPY)) ? B + pidx(g, 0, lf, xf[it]) : B + pidx(g, 0, lr, cell);
-        hR[it] = __ldg(p);
-        hB[it] = __ldg(p + 1);
+        ld_two(p, hR[it], hB[it]);
         rR[it] = rhoR[xf[it]];
         rB[it] = rhoB[xf[it]];
         if (sh.sd) {  // sum / difference pairs: the wall term of each half is linear in its density
@@ -980,8 +1015,7 @@ __global__ void __launch_bounds__(256) k_bb(PDev P, const double* __restrict__ p
       if (!(act >> it & 1)) continue;
       const int lr = (hib >> it & 1) ? 2 * it + 2 : 2 * it + 1;
       S* p = B + pidx(g, 0, lr, cell);
-      p[0] = hR[it];
-      p[1] = hB[it];
+      st_two(p, hR[it], hB[it]);
     }
   }
   }
