@@ -36,7 +36,10 @@ SIGMA, BETA = 0.02, 0.7
 LB_PER_STEP = 500
 # DRAM bytes (read + write) of one k_cg_lean launch at 128^3, from the ncu
 # captures summarised in profiles/ (None where no capture of that storage)
-TRAFFIC = {"f16": 292.7e6, "f16sd": 292.0e6, "f16sdp": 310.8e6, "f32": 622.6e6}
+# DRAM read + write bytes of one launch of the fluid kernel at 128^3 (ncu
+# dram__bytes_read.sum + dram__bytes_write.sum, the captures summarised in
+# profiles/k_cg_lean_*_128cube.md); measured, so they change with the kernel
+TRAFFIC = {"f16": 370.1e6, "f16sd": 368.9e6, "f16sdp": 393.7e6, "f32": 622.6e6}
 BYTES_PER_CELL = {"f16": 160, "bf16": 160, "f16sd": 160, "bf16sd": 160, "f16sdp": 160, "bf16sdp": 160, "f32": 312,
                   "f64": 616}  # algorithmic bytes per cell-step
 MINIMAL_BYTES = {"f16": 152, "bf16": 152, "f16sd": 152, "f16sdp": 160, "f32": 304, "f64": 608}  # bytes the kernel must move
@@ -672,6 +675,9 @@ def main():
     ap.add_argument("--box", type=int, default=L, help="lattice edge of the --only storage runs")
     ap.add_argument("--zlen", type=int, default=0,
                     help="--only storage runs: equal z-segments of this length (0: automatic plan)")
+    ap.add_argument("--decomp", default="replicas", choices=["replicas", "slab"],
+                    help="headline with N GPUs: independent boxes (default) or z-slabs of one box, halo planes "
+                         "exchanged over NCCL every lattice step")
     ap.add_argument("--shape", type=int, default=0, help="--only storage runs: lean kernel CTA, 0 = 32x8, 1 = 32x16")
     ap.add_argument("--lean-copies", type=int, default=1,
                     help="--only storage runs: 16-bit pulls as box granules (1) or one copy per pull (0)")
@@ -720,9 +726,40 @@ def main():
         s.close()
         return total_ms, kernel_ms, launches, clocks, code
 
+    def run_slab(storage, timed_steps, warm):
+        """Rank r's 128^3 z-slab of a 128 x 128 x (128 N) periodic box: halo planes swapped with the
+        neighbouring ranks every lattice step (NCCL; one rank: with itself), CUDA events on the slab's
+        stream.  Returns the same tuple as run_storage (the kernel time is not split out)."""
+        from lbcuda_b200.slabs import DistExchange, LocalExchange, Slab
+        pg_ = make_params(L, L, L * ws, model="cg", storage=storage, sigma=SIGMA, beta=BETA)
+        gR, gB = seeded_noise_fields(L, L, L * ws, seed=SEED)
+        slab = Slab(pg_, rank, ws)
+        slab.set_fields(gR, gB)
+        ex = DistExchange(slab, "cuda") if pg is not None else LocalExchange([slab])
+        for _ in range(warm):
+            ex.step(LB_PER_STEP)
+        slab.sync()
+        barrier()
+        clk = Clocks(local)
+        clk.start()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(slab.stream)
+        ex.step(timed_steps * LB_PER_STEP)
+        e1.record(slab.stream)
+        e1.synchronize()
+        clocks_ = clk.stop()
+        barrier()
+        code = slab.sim.status()[0]
+        slab.close()
+        # one fluid kernel per lattice step (the halo copies are not kernels)
+        return e0.elapsed_time(e1), 0.0, timed_steps * LB_PER_STEP, clocks_, code
+
     # headline: FP16 storage as sum / difference pairs (R + B - w (rho0R + rho0B), R - B); beside it the
     # FP16 (R, B) pairs the sphere path stores, and FP32
-    tot16, k16, n16, clocks, code16 = run_storage("f16sd", args.steps, args.warmup)
+    if args.decomp == "slab":
+        tot16, k16, n16, clocks, code16 = run_slab("f16sd", args.steps, args.warmup)
+    else:
+        tot16, k16, n16, clocks, code16 = run_storage("f16sd", args.steps, args.warmup)
     tot32, k32, n32, _, code32 = run_storage("f32", args.steps, args.warmup)
     totrb, krb, nrb, _, coderb = run_storage("f16", args.steps, args.warmup)
     totsp, ksp, nsp, _, codesp = run_storage("f16sdp", args.steps, args.warmup)
@@ -810,8 +847,9 @@ def main():
             "config": workload_config(),
             "storage": "f16 sum / difference pairs (f_R + f_B - w*1, f_R - f_B), FP32 arithmetic",
             "lattice_steps_per_bench_step": LB_PER_STEP,
-            "parallelism": "replicas" if ws > 1 else "single",
-            "roofline": roofline("f16sd", k16, n16),
+            "parallelism": ("z-slabs, halo planes over NCCL" if args.decomp == "slab" else "replicas")
+            if ws > 1 else ("one z-slab exchanging with itself" if args.decomp == "slab" else "single"),
+            "roofline": roofline("f16sd", k16, n16) if k16 > 0 else None,
             "fp32_storage": {"value": mlups32, "unit": "MLUPS", "ms_per_step": tot32 / args.steps,
                              "roofline": roofline("f32", k32, n32)},
             "fp16_over_fp32": mlups16 / mlups32,

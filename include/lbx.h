@@ -326,6 +326,10 @@ int lbx_plane_bytes(void* ctx, int32_t nplanes, int64_t* bytes);
  * context's stream: lbx_sync before the buffer is used elsewhere. */
 int lbx_pack_planes(void* ctx, int32_t z0, int32_t nplanes, void* dev_buf);
 int lbx_unpack_planes(void* ctx, int32_t z0, int32_t nplanes, const void* dev_buf);
+/* The context's CUDA stream (a cudaStream_t): a host that moves the packed
+ * planes itself (NCCL, CUDA-aware MPI) orders its transfers after the pack
+ * and before the unpack on it, without waiting on the host. */
+int lbx_get_stream(void* ctx, void** stream);
 
 /* ---- measurement ------------------------------------------------------- */
 /* Colour-gradient schedule: 2 = lean single-pass kernel (default), 1 = the

@@ -142,5 +142,10 @@ module lbx_mod
       type(c_ptr), value :: ctx, dev_buf
       integer(c_int32_t), value :: z0, nplanes
     end function
+    integer(c_int) function lbx_get_stream(ctx, stream) bind(C, name="lbx_get_stream")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: ctx
+      type(c_ptr), intent(out) :: stream
+    end function
   end interface
 end module lbx_mod

@@ -101,6 +101,7 @@ SIGNATURES = {
     "lbx_plane_bytes": (C.c_int, [_P, C.c_int32, C.POINTER(C.c_int64)]),
     "lbx_pack_planes": (C.c_int, [_P, C.c_int32, C.c_int32, _P]),
     "lbx_unpack_planes": (C.c_int, [_P, C.c_int32, C.c_int32, _P]),
+    "lbx_get_stream": (C.c_int, [_P, _PP]),
     "lbx_time_steps": (C.c_int, [_P, C.c_int32, _D, _D, _I64]),
 }
 

@@ -1366,24 +1366,27 @@ static int lean_zlen(const Ctx& c, int tx, int ty, int resident) {
 // Returns the device table (x0, y0, z0, zend per CTA) kept in the context, or
 // nullptr when the equal segments are used.
 static const int4* paired_plan(Ctx& c, int TX, int TY, int resident, int* n) {
+  // the planes marched: the whole box, or a z-slab's own planes
+  const int zb = c.zhi > 0 ? c.zlo : 0, nzr = (c.zhi > 0 ? c.zhi : c.nz) - zb;
   const int ncx = (c.nx + TX - 1) / TX, ncy = (c.ny + TY - 1) / TY, cols = ncx * ncy;
   const int b = std::min(cols, std::min(resident / 8, resident - 4 * cols));  // columns cut 1 + 4
-  if (c.nz < 64 || 4 * cols >= resident || 5 * cols <= resident || b <= 0) return nullptr;
-  const int64_t key = int64_t(resident) * 4096 + TX * 64 + TY;
+  if (nzr < 64 || 4 * cols >= resident || 5 * cols <= resident || b <= 0) return nullptr;
+  const int64_t key = ((int64_t(resident) * 4096 + TX * 64 + TY) * 65536 + zb) * 65536 + nzr;
   if (c.lean_plan && c.lean_plan_key == key) {
     *n = c.lean_plan_n;
     return static_cast<const int4*>(c.lean_plan);
   }
   std::vector<int4> lng, sht;
-  const int L1 = c.nz / 4, rest = c.nz - L1;
+  const int L1 = nzr / 4, rest = nzr - L1;
   for (int col = 0; col < cols; ++col) {
     const int x0 = (col % ncx) * TX, y0 = (col / ncx) * TY;
     const bool cut = (long(col) * b) / cols != (long(col + 1) * b) / cols;  // b columns spread over all
     if (!cut) {
-      for (int k = 0; k < 4; ++k) lng.push_back(make_int4(x0, y0, k * c.nz / 4, (k + 1) * c.nz / 4));
+      for (int k = 0; k < 4; ++k) lng.push_back(make_int4(x0, y0, zb + k * nzr / 4, zb + (k + 1) * nzr / 4));
     } else {
-      lng.push_back(make_int4(x0, y0, 0, L1));
-      for (int k = 0; k < 4; ++k) sht.push_back(make_int4(x0, y0, L1 + k * rest / 4, L1 + (k + 1) * rest / 4));
+      lng.push_back(make_int4(x0, y0, zb, zb + L1));
+      for (int k = 0; k < 4; ++k)
+        sht.push_back(make_int4(x0, y0, zb + L1 + k * rest / 4, zb + L1 + (k + 1) * rest / 4));
     }
   }
   lng.insert(lng.end(), sht.begin(), sht.end());
@@ -1501,11 +1504,10 @@ static int launch_lean_as(Ctx& c, int zlen_override, LeanPart<typename Store<S>:
   // (FP32 128^3: 185 us with the plan, 148 us without; FP16 96 against 101)
   int nplan = 0;
   const int4* plan = nullptr;
-  if (c.zhi > 0) {  // a z-slab: only its own planes
+  if (zlen_override <= 0 && kStaged<S, PART>) plan = paired_plan(c, TX, TY, resident, &nplan);
+  if (!plan && c.zhi > 0) {  // a z-slab: only its own planes
     plan = range_plan(c, TX, TY, resident, &nplan);
     if (!plan) return LBX_ERR_ALLOC;
-  } else if (zlen_override <= 0 && kStaged<S, PART>) {
-    plan = paired_plan(c, TX, TY, resident, &nplan);
   }
   if (plan) grid = dim3(unsigned(nplan), 1, 1);
   k_cg_lean<S, TX, TY, MINB, PART, SD, SDP, BOX>

@@ -835,11 +835,12 @@ constexpr int BB_N2P = 1, BB_COPY = 2, BB_WALL = 4, BB_ALL = 7;
 // sphere has a template cell inside a's box, so it is listed in one of the
 // bins of a's box, and its rounded centre lies within 2 rmax of c (minimum
 // image).  With rmax <= BINW the box spans at most three bins per axis, those
-// of c - rmax, c and c + rmax; larger radii answer yes.  Called by every
-// thread of the CTA (a CTA-wide vote).
+// of c - rmax, c and c + rmax; larger radii answer yes.  A vote of the calling
+// warp (lanes 0..26 take one bin each; no CTA barrier), called by all its
+// lanes.
 __device__ bool crowded_reach(const PDev& P, const double* __restrict__ pos, const Geom& g, int a, const int c[3]) {
   bool hit = P.rmax > BINW;
-  const int t = threadIdx.x;
+  const int t = threadIdx.x & 31;
   if (!hit && t < 27) {
     const int s[3] = {(t % 3 - 1) * P.rmax, ((t / 3) % 3 - 1) * P.rmax, (t / 9 - 1) * P.rmax};
     const int x0 = wrap1(c[0] + s[0], g.nx) - 1, y0 = wrap1(c[1] + s[1], g.ny) - 1, z0 = wrap1(c[2] + s[2], g.nz) - 1;
@@ -865,7 +866,7 @@ __device__ bool crowded_reach(const PDev& P, const double* __restrict__ pos, con
       hit = double(d2) < lim;
     }
   }
-  return __syncthreads_or(hit) != 0;
+  return __any_sync(0xffffffffu, hit);
 }
 
 template <typename S>
@@ -886,7 +887,8 @@ __global__ void __launch_bounds__(256) k_bb(PDev P, const double* __restrict__ p
   double s[6] = {0, 0, 0, 0, 0, 0};
   // Past the sphere's own surface cells (pass 0), the reach holds its dead
   // cells and fluid cells, which no link crosses, unless another sphere's
-  // template reaches into it: pass 1 runs only then.
+  // template reaches into it: pass 1 runs only then (each warp decides when
+  // it gets there; every lane of a warp is still in the loop at that point).
   for (int pass = 0; pass < 2; ++pass) {
   if (pass == 1 && !crowded_reach(P, pos, g, a, c)) break;
   const int t0 = pass ? P.n_surf : 0, t1 = pass ? P.n_bb : P.n_surf;

@@ -80,6 +80,16 @@ class Slab:
     def sync(self):
         self.sim.sync()
 
+    @property
+    def stream(self):
+        """The context's CUDA stream, as a torch stream (packs, unpacks and steps are enqueued on it)."""
+        import torch
+        if getattr(self, "_stream", None) is None:
+            ptr = capi.C.c_void_p()
+            capi.check(self.sim._L.lbx_get_stream(self.sim._h, capi.C.byref(ptr)), "lbx_get_stream")
+            self._stream = torch.cuda.ExternalStream(ptr.value or 0)
+        return self._stream
+
     def step_own(self):
         self.sim.step(1)
 
@@ -97,33 +107,51 @@ class Slab:
 
 
 class LocalExchange:
-    """All slabs of a box in this process; packed planes move by device copies."""
+    """All slabs of a box in this process; packed planes move by device copies.
+
+    Nothing waits on the host: slab i's stream records an event after its
+    packs, and the two neighbours' streams wait on it before they unpack.  The
+    buffers alternate between two sets, so a pack never overwrites a buffer a
+    neighbour may not have unpacked yet (that unpack precedes, on the
+    neighbour's stream, the pack this slab waited for one exchange later)."""
 
     def __init__(self, slabs):
         import torch
         self.slabs = slabs
         dev = torch.device("cuda", torch.cuda.current_device())
-        self.low = [torch.empty(s.halo_bytes, dtype=torch.uint8, device=dev) for s in slabs]
-        self.high = [torch.empty(s.halo_bytes, dtype=torch.uint8, device=dev) for s in slabs]
+        mk = lambda s: torch.empty(s.halo_bytes, dtype=torch.uint8, device=dev)
+        self.low = [[mk(s) for s in slabs] for _ in range(2)]
+        self.high = [[mk(s) for s in slabs] for _ in range(2)]
+        self.parity = 0
 
     def exchange(self):
+        import torch
         n = len(self.slabs)
-        for s, lo, hi in zip(self.slabs, self.low, self.high):
-            s.pack("low", lo)
-            s.pack("high", hi)
-        for s in self.slabs:
-            s.sync()
+        lo, hi = self.low[self.parity], self.high[self.parity]
+        self.parity ^= 1
+        packed = []
         for i, s in enumerate(self.slabs):
-            self.slabs[(i - 1) % n].unpack("high", self.low[i])
-            self.slabs[(i + 1) % n].unpack("low", self.high[i])
-        for s in self.slabs:
-            s.sync()
+            s.pack("low", lo[i])
+            s.pack("high", hi[i])
+            ev = torch.cuda.Event()
+            ev.record(s.stream)
+            packed.append(ev)
+        for i, s in enumerate(self.slabs):
+            up, down = (i + 1) % n, (i - 1) % n
+            s.stream.wait_event(packed[up])
+            s.stream.wait_event(packed[down])
+            s.unpack("high", lo[up])  # the first own planes of the slab above
+            s.unpack("low", hi[down])  # the last own planes of the slab below
 
     def step(self, nsteps=1):
         for _ in range(nsteps):
             self.exchange()
             for s in self.slabs:
                 s.step_own()
+
+    def sync(self):
+        for s in self.slabs:
+            s.sync()
 
 
 class DistExchange:
@@ -147,9 +175,23 @@ class DistExchange:
     def exchange(self):
         import torch
         s = self.slab
-        s.pack("low", self.send_low)
-        s.pack("high", self.send_high)
-        s.sync()  # the context's stream has written the send buffers
+        if self.cuda:
+            # every copy and transfer on the context's stream: the collectives
+            # wait for the packs, the unpacks for the collectives
+            with torch.cuda.stream(s.stream):
+                self._swap()
+        else:
+            s.pack("low", self.send_low)
+            s.pack("high", self.send_high)
+            s.sync()
+            self._swap(packed=True)
+            s.sync()
+
+    def _swap(self, packed=False):
+        s = self.slab
+        if not packed:
+            s.pack("low", self.send_low)
+            s.pack("high", self.send_high)
         if self.world == 1:  # periodic with itself
             self.recv_high.copy_(self.send_low)
             self.recv_low.copy_(self.send_high)
@@ -162,11 +204,8 @@ class DistExchange:
                    d.P2POp(d.isend, self.send_high, up, tag=2), d.P2POp(d.irecv, self.recv_low, down, tag=2)]
             for w in d.batch_isend_irecv(ops):
                 w.wait()
-        if self.cuda:
-            torch.cuda.current_stream().synchronize()  # received before the context's stream reads them
         s.unpack("high", self.recv_high)
         s.unpack("low", self.recv_low)
-        s.sync()
 
     def step(self, nsteps=1):
         for _ in range(nsteps):

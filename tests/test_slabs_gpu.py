@@ -61,3 +61,38 @@ def test_zrange_arguments():
     q = LBSim(make_params(32, 24, 24, model="cg", storage="f16", max_particles=1, radius=3.0))
     assert L.lbx_set_zrange(q._h, 2, 22) == LBX_ERR_STATE
     q.close()
+
+
+def test_dist_exchange_single_rank_equals_whole_box():
+    """DistExchange (the per-rank transport) with a process group of one: the slab exchanges with itself on
+    its context's stream, and the periodic box comes out as stepped whole."""
+    import os
+    import socket
+
+    import torch.distributed as dist
+
+    from lbcuda_b200.slabs import DistExchange
+    with socket.socket() as so:
+        so.bind(("127.0.0.1", 0))
+        port = so.getsockname()[1]
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=0, world_size=1)
+    try:
+        nx, ny, nz, steps = 32, 16, 24, 9
+        p = make_params(nx, ny, nz, model="cg", storage="f16sd", sigma=0.02, beta=0.7)
+        rR, rB = seeded_noise_fields(nx, ny, nz, seed=8)
+        whole = LBSim(p)
+        whole.set_fields(rR, rB)
+        whole.step(steps)
+        ref = whole.get_pops()
+        whole.close()
+        s = Slab(p, 0, 1)
+        s.set_fields(rR, rB)
+        ex = DistExchange(s, "cuda")
+        ex.step(steps)
+        ex.exchange()
+        for a, b in zip(s.own_pops(), ref):
+            assert np.array_equal(a, b)
+        s.close()
+    finally:
+        dist.destroy_process_group()
