@@ -833,8 +833,8 @@ constexpr int BB_N2P = 1, BB_COPY = 2, BB_WALL = 4, BB_ALL = 7;
 // Whether another sphere's template can reach into the bounce-back reach of
 // sphere a (offsets d^2 < sphereMax around its rounded centre c): such a
 // sphere has a template cell inside a's box, so it is listed in one of the
-// bins of a's box, and its rounded centre lies within 2 rmax of c (minimum
-// image).  With rmax <= BINW the box spans at most three bins per axis, those
+// bins of a's box, and its rounded centre lies within the bound below
+// (minimum image).  With rmax <= BINW the box spans at most three bins per axis, those
 // of c - rmax, c and c + rmax; larger radii answer yes.  A vote of the calling
 // warp (lanes 0..26 take one bin each; no CTA barrier), called by all its
 // lanes.
@@ -887,10 +887,10 @@ __global__ void __launch_bounds__(256) k_bb(PDev P, const double* __restrict__ p
   double s[6] = {0, 0, 0, 0, 0, 0};
   // Past the sphere's own surface cells (pass 0), the reach holds its dead
   // cells and fluid cells, which no link crosses, unless another sphere's
-  // template reaches into it: pass 1 runs only then (each warp decides when
-  // it gets there; every lane of a warp is still in the loop at that point).
+  // template reaches into it: pass 1 runs only then (a vote of each warp).
+  const bool crowd = crowded_reach(P, pos, g, a, c);
   for (int pass = 0; pass < 2; ++pass) {
-  if (pass == 1 && !crowded_reach(P, pos, g, a, c)) break;
+  if (pass == 1 && !crowd) break;
   const int t0 = pass ? P.n_surf : 0, t1 = pass ? P.n_bb : P.n_surf;
   for (int t = t0 + int(threadIdx.x); t < t1; t += blockDim.x) {
     int dx, dy, dz, tv, i1, j1, k1;
