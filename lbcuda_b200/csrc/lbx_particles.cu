@@ -67,6 +67,10 @@ struct ParticleState {
   int* nbr = nullptr;         // np x NBCAP
   int* nbr_cnt = nullptr;
   float* corr = nullptr;      // np x NBCAP x 12
+  // second stream of the step's post stage: the pair forces and the
+  // clearing of the previous flags run beside the bounce-back
+  cudaStream_t aux = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
 };
 
 struct PDev {  // by-value kernel argument
@@ -1550,6 +1554,10 @@ int particles_create(Ctx& c) {
   if (!ok(cudaMalloc(&s->wclosure, size_t(LBX_CLOSURE_NWEIGHTS) * 4))) return LBX_ERR_ALLOC;
   if (!ok(cudaMalloc(&s->nbr, size_t(cap) * NBCAP * 4))) return LBX_ERR_ALLOC;
   if (!ok(cudaMalloc(&s->nbr_cnt, size_t(cap) * 4))) return LBX_ERR_ALLOC;
+  if (!ok(cudaStreamCreateWithFlags(&s->aux, cudaStreamNonBlocking)) ||
+      !ok(cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming)) ||
+      !ok(cudaEventCreateWithFlags(&s->ev_join, cudaEventDisableTiming)))
+    return LBX_ERR_CUDA;
   if (!ok(cudaMalloc(&s->corr, size_t(cap) * NBCAP * 12 * 4))) return LBX_ERR_ALLOC;
   cudaMemsetAsync(s->acc, 0, size_t(cap) * AS * 8, c.stream);
   cudaMemsetAsync(s->owner, 0xFF, size_t(c.n) * 4, c.stream);
@@ -1575,6 +1583,9 @@ void particles_destroy(Ctx& c) {
   if (s->nbr) cudaFree(s->nbr);
   if (s->nbr_cnt) cudaFree(s->nbr_cnt);
   if (s->corr) cudaFree(s->corr);
+  if (s->ev_fork) cudaEventDestroy(s->ev_fork);
+  if (s->ev_join) cudaEventDestroy(s->ev_join);
+  if (s->aux) cudaStreamDestroy(s->aux);
   delete s;
   c.part = nullptr;
 }
@@ -1789,7 +1800,7 @@ int part_bb(Ctx& c, int mode) {
 }
 
 // inter_force_particles: Hertz and analytic lubrication, then the closure
-int part_pairs(Ctx& c) {
+static int pairs_on(Ctx& c, cudaStream_t st) {
   Stage t(c);
   ParticleState& s = t.s;
   const int warp_blocks = (s.np * 32 + 255) / 256;
@@ -1799,27 +1810,34 @@ int part_pairs(Ctx& c) {
   const double cut = c.p.closure ? fmax(double(c.p.closure_gap_max) * s.rdim + 1.75,
                                         c.p.lubrication ? double(c.p.lubric_rmin) : 0.0)
                                  : 0.0;
-  k_pairs<<<warp_blocks, 256, 0, c.stream>>>(t.P, t.pc, s.acc, t.g, cut, c.p.closure ? s.nbr : nullptr, s.nbr_cnt,
-                                              c.d_err, t.st);
+  k_pairs<<<warp_blocks, 256, 0, st>>>(t.P, t.pc, s.acc, t.g, cut, c.p.closure ? s.nbr : nullptr, s.nbr_cnt,
+                                        c.d_err, t.st);
   if (c.p.closure) {
     const int use_net = s.closure_ready;
     size_t smem = sizeof(float) * (size_t(LBX_CLOSURE_NWEIGHTS) + 8 * 2 * H);
     int blocks = (s.np * NBCAP + 7) / 8;
     if (blocks > 148 * 4) blocks = 148 * 4;
-    k_closure_pairs<<<blocks, 256, smem, c.stream>>>(t.P, t.pc, t.g, s.wclosure, use_net, s.nbr, s.nbr_cnt, s.corr);
-    k_closure_accum<<<(s.np + 127) / 128, 128, 0, c.stream>>>(t.P, s.nbr, s.nbr_cnt, s.corr, s.acc);
+    k_closure_pairs<<<blocks, 256, smem, st>>>(t.P, t.pc, t.g, s.wclosure, use_net, s.nbr, s.nbr_cnt, s.corr);
+    k_closure_accum<<<(s.np + 127) / 128, 128, 0, st>>>(t.P, s.nbr, s.nbr_cnt, s.corr, s.acc);
   }
+  return launch_status();
+}
+
+int part_pairs(Ctx& c) { return pairs_on(c, c.stream); }
+
+// the previous step's flags (stamped at the previous positions) are not read
+// again: clear them, so that the next step stamps into a fluid slot
+static int unstamp_on(Ctx& c, cudaStream_t st) {
+  Stage t(c);
+  k_unstamp<<<t.s.np, 256, 0, st>>>(t.P, t.po, t.g, c.flags[t.fo], nullptr);
   return launch_status();
 }
 
 // time_step_force_particles, then the end of the step: every ping-pong
 // index (populations, flags, particle records) flips
-int part_integrate(Ctx& c) {
+static int integrate_flip(Ctx& c) {
   Stage t(c);
   ParticleState& s = t.s;
-  // the previous step's flags (stamped at the previous positions) are not
-  // read again: clear them, so that the next step stamps into a fluid slot
-  k_unstamp<<<s.np, 256, 0, c.stream>>>(t.P, t.po, t.g, c.flags[t.fo], nullptr);
   k_integrate<<<(s.np + 127) / 128, 128, 0, c.stream>>>(t.P, t.pc, s.pos[1 - s.pcur], s.frc[s.pcur],
                                                         s.frc[1 - s.pcur], s.acc, t.g, c.d_err, t.st);
   int rc = launch_status();
@@ -1832,10 +1850,26 @@ int part_integrate(Ctx& c) {
   return 0;
 }
 
+int part_integrate(Ctx& c) {
+  int rc = unstamp_on(c, c.stream);
+  return rc ? rc : integrate_flip(c);
+}
+
+// The bounce-back on the context's stream; beside it, on the second stream,
+// the pair forces (accumulators of their own, acc[6..14], against acc[0..5]
+// of the bounce-back) and the clearing of the previous step's flags (the
+// bounce-back reads this step's); both join before the integrator, which
+// overwrites the previous positions the clearing reads.
 int particles_post(Ctx& c) {
-  int rc = part_bb(c, BB_ALL);
-  if (!rc) rc = part_pairs(c);
-  if (!rc) rc = part_integrate(c);
+  ParticleState& s = *c.part;
+  if (cudaEventRecord(s.ev_fork, c.stream) != cudaSuccess || cudaStreamWaitEvent(s.aux, s.ev_fork, 0) != cudaSuccess)
+    return LBX_ERR_CUDA;
+  int rc = pairs_on(c, s.aux);
+  if (!rc) rc = unstamp_on(c, s.aux);
+  if (!rc && cudaEventRecord(s.ev_join, s.aux) != cudaSuccess) rc = LBX_ERR_CUDA;
+  if (!rc) rc = part_bb(c, BB_ALL);
+  if (!rc && cudaStreamWaitEvent(c.stream, s.ev_join, 0) != cudaSuccess) rc = LBX_ERR_CUDA;
+  if (!rc) rc = integrate_flip(c);
   return rc;
 }
 
