@@ -166,7 +166,7 @@ __global__ void __launch_bounds__(256) k_cg_phi(const S* __restrict__ A, Geom g,
   // the phase field the gradient takes (psi_shifted, kernels_fluid_CG.CUF:
   // 728-729: scaled by the fluid densities, 1 and 1 for a single density)
   phi[cell] = (rR / densR - rB / densB) / (rR / densR + rB / densB);
-  if (rhoR) { rhoR[cell] = rR; rhoB[cell] = rB; }
+  if (rhoR) { rhoR[2 * size_t(cell)] = rR; rhoB[2 * size_t(cell)] = rB; }
 }
 
 // time_step_CG + streaming, two-pass schedule: pull, densities, gradient from
@@ -198,9 +198,9 @@ __global__ void __launch_bounds__(256) k_cg_collide(const S* __restrict__ A, S* 
     // arrays
     C psR[3], psB[3], sx, sy, sz;
     grad27(K.L, [&](int dx, int dy, int dz) { return __ldg(phi + at(b, dx, dy, dz)); }, psix, psiy, psiz);
-    grad27(K.L, [&](int dx, int dy, int dz) { return __ldg(rhoRa + at(b, dx, dy, dz)); }, sx, sy, sz);
+    grad27(K.L, [&](int dx, int dy, int dz) { return __ldg(rhoRa + 2 * size_t(at(b, dx, dy, dz))); }, sx, sy, sz);
     psR[0] = sx; psR[1] = sy; psR[2] = sz;
-    grad27(K.L, [&](int dx, int dy, int dz) { return __ldg(rhoBa + at(b, dx, dy, dz)); }, sx, sy, sz);
+    grad27(K.L, [&](int dx, int dy, int dz) { return __ldg(rhoBa + 2 * size_t(at(b, dx, dy, dz))); }, sx, sy, sz);
     psB[0] = sx; psB[1] = sy; psB[2] = sz;
     cg_collide_cell_dd<QQ>(K, fR, fB, rR, rB, psix, psiy, psiz, psR, psB);
   } else {
@@ -469,8 +469,11 @@ int fluid_alloc(Ctx& c) {
     if (cudaMalloc(&c.pops[i], bytes) != cudaSuccess) return LBX_ERR_ALLOC;
   size_t cb = (c.storage == LBX_STORE_F64) ? 8 : 4;
   if (cudaMalloc(&c.phi, size_t(c.n) * cb) != cudaSuccess) return LBX_ERR_ALLOC;
-  for (int i = 0; i < 2; ++i)
-    if (cudaMalloc(&c.rho[i], size_t(c.n) * cb) != cudaSuccess) return LBX_ERR_ALLOC;
+  // densities interleaved, (rhoR, rhoB) of a cell side by side: one sector
+  // per scattered read of both (the sphere kernels read them at the fluid
+  // ends of links); rho[1] is rho[0] one element on, both indexed 2 * cell
+  if (cudaMalloc(&c.rho[0], 2 * size_t(c.n) * cb) != cudaSuccess) return LBX_ERR_ALLOC;
+  c.rho[1] = static_cast<char*>(c.rho[0]) + cb;
   for (int i = 0; i < 2; ++i) {
     if (cudaMalloc(&c.flags[i], size_t(c.n)) != cudaSuccess) return LBX_ERR_ALLOC;
     cudaMemsetAsync(c.flags[i], LBX_FLUID_FLUID, size_t(c.n), c.stream);
@@ -488,10 +491,11 @@ int fluid_alloc(Ctx& c) {
 void fluid_free(Ctx& c) {
   for (int i = 0; i < 2; ++i) {
     if (c.pops[i]) cudaFree(c.pops[i]);
-    if (c.rho[i]) cudaFree(c.rho[i]);
     if (c.flags[i]) cudaFree(c.flags[i]);
-    c.pops[i] = nullptr; c.rho[i] = nullptr; c.flags[i] = nullptr;
+    c.pops[i] = nullptr; c.flags[i] = nullptr;
   }
+  if (c.rho[0]) cudaFree(c.rho[0]);  // rho[1] points into it
+  c.rho[0] = c.rho[1] = nullptr;
   if (c.phi) cudaFree(c.phi);
   c.phi = nullptr;
   for (int i = 0; i < 2; ++i) {

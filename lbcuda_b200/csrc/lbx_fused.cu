@@ -1005,8 +1005,8 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
           if (fn == LBX_FLUID_SPHERELIST) return side_phi();
           if (fn == LBX_FLUID_FLUID) {  // new fluid cell
             if (is_own) {
-              rR = PT.rhoR[size_t(unsigned(cell))];
-              rB = PT.rhoB[size_t(unsigned(cell))];
+              rR = PT.rhoR[2 * size_t(unsigned(cell))];  // interleaved densities
+              rB = PT.rhoB[2 * size_t(unsigned(cell))];
             }
             return side_phi();
           }

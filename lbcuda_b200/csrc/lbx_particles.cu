@@ -149,11 +149,11 @@ __device__ __forceinline__ bool offset_cell(const PDev& P, const Geom& g, const 
          get_delta(k1, c[2], g.nz, P.rdim) == dz;
 }
 
-// Tile-list coverage of makeListAtomsGPU: whether the reference's 8x4x4 tile
-// (ti,tj,tk, 1-based) holds particle position x (the list of the current step).
-__device__ bool tile_covered(const double x[3], const int n[3], double rdim, int ti, int tj, int tk) {
+// Tile-list coverage of makeListAtomsGPU: the reference's 8x4x4 tiles
+// (1-based indices) that hold particle position x in the list of the current
+// step, as two ranges [lo0, hi0] and [lo1, hi1] per axis (R[4 d + 0..3]).
+__device__ void tile_ranges(const double x[3], const int n[3], double rdim, int R[12]) {
   const int td[3] = {TILEX, TILEY, TILEZ};
-  const int t[3] = {ti, tj, tk};
   for (int d = 0; d < 3; ++d) {
     int ci = int(ceil(x[d]));
     int b0 = int(x[d] - rdim), b1 = int(x[d] + rdim), b2, b3;  // real -> integer truncation
@@ -164,14 +164,25 @@ __device__ bool tile_covered(const double x[3], const int n[3], double rdim, int
     } else {
       b2 = td[d]; b3 = -td[d];
     }
-    bool hit = false;
-    int lo0 = (b0 - 1) / td[d] + 1, hi0 = (b1 - 1) / td[d] + 1;
-    int lo1 = (b2 - 1) / td[d] + 1, hi1 = (b3 - 1) / td[d] + 1;
-    if (t[d] >= lo0 && t[d] <= hi0) hit = true;
-    if (t[d] >= lo1 && t[d] <= hi1) hit = true;
-    if (!hit) return false;
+    R[4 * d + 0] = (b0 - 1) / td[d] + 1;
+    R[4 * d + 1] = (b1 - 1) / td[d] + 1;
+    R[4 * d + 2] = (b2 - 1) / td[d] + 1;
+    R[4 * d + 3] = (b3 - 1) / td[d] + 1;
   }
-  return true;
+}
+__device__ __forceinline__ bool in_tile_ranges(const int* R, int ti, int tj, int tk) {
+  const int t[3] = {ti, tj, tk};
+  bool ok = true;
+#pragma unroll
+  for (int d = 0; d < 3; ++d)
+    ok = ok && ((t[d] >= R[4 * d] && t[d] <= R[4 * d + 1]) || (t[d] >= R[4 * d + 2] && t[d] <= R[4 * d + 3]));
+  return ok;
+}
+// whether the tile (ti, tj, tk) holds particle position x
+__device__ bool tile_covered(const double x[3], const int n[3], double rdim, int ti, int tj, int tk) {
+  int R[12];
+  tile_ranges(x, n, rdim, R);
+  return in_tile_ranges(R, ti, tj, tk);
 }
 
 // q (0,v) q*  (qtrimult, kernels_fluid_PART.CUF:1830-1871)
@@ -423,7 +434,7 @@ __global__ void __launch_bounds__(256) k_drain(PDev P, const double* __restrict_
     pull_dead(A, Bold, g, b, 0, sh, fold, qR);
     pull_dead(A, Bold, g, b, 1, sh, fold, qB);
     if (sh.sd) sd_to_rb(qR, qB);  // sum / difference pairs: the components' momenta below
-    C rR = rhoR[cell], rB = rhoB[cell];
+    C rR = rhoR[2 * size_t(cell)], rB = rhoB[2 * size_t(cell)];
     C invrho = C(1) / (rR + rB);
     C u = invrho * mx(qR) + invrho * mx(qB);
     C v = invrho * my(qR) + invrho * my(qB);
@@ -475,8 +486,8 @@ __global__ void __launch_bounds__(256) k_rho_p(const S* __restrict__ A, const S*
     if (rR < C(0)) rR = C(0);
     if (rB < C(0)) rB = C(0);
   }
-  rhoR[cell] = rR;
-  rhoB[cell] = rB;
+  rhoR[2 * size_t(cell)] = rR;
+  rhoB[2 * size_t(cell)] = rB;
   phi[cell] = (rR - rB) / (rR + rB);
 }
 
@@ -566,8 +577,8 @@ __global__ void __launch_bounds__(256) k_rho_shell(PDev P, const double* __restr
     C rR, rB;
     pulled_rho(A, g, sh, i1, j1, k1, rR, rB);
     if (fn != LBX_FLUID_FLUID || fo != LBX_FLUID_FLUID) continue;
-    rhoR[y] = rR;
-    rhoB[y] = rB;
+    rhoR[2 * size_t(y)] = rR;
+    rhoB[2 * size_t(y)] = rB;
   }
 }
 
@@ -604,7 +615,7 @@ __global__ void __launch_bounds__(256) k_fill(PDev P, const double* __restrict__
       int yi = wrap1(i1 + ex27(l), g.nx), yj = wrap1(j1 + ey27(l), g.ny), yk = wrap1(k1 + ez27(l), g.nz);
       int y = cell0(g, yi, yj, yk);
       if (fnew[y] == LBX_FLUID_FLUID && fold[y] == LBX_FLUID_FLUID) {
-        Rs = Rs + rhoR[y]; Bs = Bs + rhoB[y]; ++D;
+        Rs = Rs + rhoR[2 * size_t(y)]; Bs = Bs + rhoB[2 * size_t(y)]; ++D;
       }
     }
     if (D) { Rs = Rs / C(D); Bs = Bs / C(D); }
@@ -626,8 +637,8 @@ __global__ void __launch_bounds__(256) k_fill(PDev P, const double* __restrict__
       // else fix_onebelt_density_twofluids (empty in the reference): zero density
     }
     C u = C(pc[3]), v = C(pc[4]), w = C(pc[5]);
-    rhoR[cell] = Rs;
-    rhoB[cell] = Bs;
+    rhoR[2 * size_t(cell)] = Rs;
+    rhoB[2 * size_t(cell)] = Bs;
     phi[cell] = (Rs - Bs) / (Rs + Bs);
     C usq = L.half_inv_cssq * (u * u + v * v + w * w);
     for (int comp = 0; comp < 2; ++comp) {
@@ -694,7 +705,7 @@ __global__ void __launch_bounds__(256) k_virtual(PDev P, const double* __restric
         int y = cell0(g, yi, yj, yk);
         if (fnew[y] == LBX_FLUID_FLUID) {
           C w = L.p27[wclass27(l)];
-          Rs = Rs + w * rhoR[y]; Bs = Bs + w * rhoB[y]; Ds = Ds + w;
+          Rs = Rs + w * rhoR[2 * size_t(y)]; Bs = Bs + w * rhoB[2 * size_t(y)]; Ds = Ds + w;
         }
       }
       if (Ds != C(0)) { R = Rs / Ds; Bv = Bs / Ds; }
@@ -718,8 +729,8 @@ __global__ void __launch_bounds__(256) k_virtual(PDev P, const double* __restric
         Bv = D ? Bs / C(D) : C(0);
       }
     }
-    rhoR[cell] = R;
-    rhoB[cell] = Bv;
+    rhoR[2 * size_t(cell)] = R;
+    rhoB[2 * size_t(cell)] = Bv;
     phi[cell] = (R - Bv) / (R + Bv);
   }
 }
@@ -761,14 +772,14 @@ __global__ void __launch_bounds__(256) k_collide_p(const S* __restrict__ A, S* B
           K,
           [&](int dx, int dy, int dz, C& rs, C& bs) {
             const int y = at(b, dx, dy, dz);
-            rs = rhoR[y];
-            bs = rhoB[y];
+            rs = rhoR[2 * size_t(y)];
+            bs = rhoB[2 * size_t(y)];
           },
           psix, psiy, psiz, psR, psB);
-      cg_collide_cell_dd(K, fR, fB, rhoR[cell], rhoB[cell], psix, psiy, psiz, psR, psB);
+      cg_collide_cell_dd(K, fR, fB, rhoR[2 * size_t(cell)], rhoB[2 * size_t(cell)], psix, psiy, psiz, psR, psB);
     } else {
       grad27(K.L, [&](int dx, int dy, int dz) { return phi[at(b, dx, dy, dz)]; }, psix, psiy, psiz);
-      cg_collide_cell(K, fR, fB, rhoR[cell], rhoB[cell], psix, psiy, psiz);
+      cg_collide_cell(K, fR, fB, rhoR[2 * size_t(cell)], rhoB[2 * size_t(cell)], psix, psiy, psiz);
     }
   }
   store_all(B, g, cell, 0, sh, fR);
@@ -806,6 +817,23 @@ __device__ __forceinline__ void link_geo_ol(const PDev& P, const Geom& g, const 
   G.ol[1] = ol[1];
   G.ol[2] = ol[2];
   if (P.lrotate) lever(g, pc, i1, j1, k1, true, P.rdim, G.rv);
+}
+
+// the same for a cell at offset d of the sphere's own offset lists: the
+// minimum image of (cell - centre) is d + (nint(centre) - centre), so the
+// lever needs no image division
+__device__ __forceinline__ void own_link_geo(const PDev& P, const double* pc, const int c[3], const double ol[3],
+                                             int dx, int dy, int dz, LinkGeo& G) {
+  G.rv[0] = G.rv[1] = G.rv[2] = 0;
+  G.ol[0] = ol[0];
+  G.ol[1] = ol[1];
+  G.ol[2] = ol[2];
+  if (P.lrotate) {
+    double r[3] = {double(dx) + (double(c[0]) - pc[0]), double(dy) + (double(c[1]) - pc[1]),
+                   double(dz) + (double(c[2]) - pc[2])};
+    const double m = sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+    for (int d = 0; d < 3; ++d) G.rv[d] = P.rdim / m * r[d];
+  }
 }
 
 __device__ __forceinline__ void wall_velocity(const PDev& P, const double* pc, const LinkGeo& G, int lr,
@@ -874,7 +902,7 @@ __device__ bool crowded_reach(const PDev& P, const double* __restrict__ pos, con
 }
 
 template <typename S>
-__global__ void __launch_bounds__(256) k_bb(PDev P, const double* __restrict__ pos, double* acc, S* B, Geom g,
+__global__ void __launch_bounds__(256, sizeof(S) == 8 ? 1 : 2) k_bb(PDev P, const double* __restrict__ pos, double* acc, S* B, Geom g,
                                             Shift<typename Store<S>::C> sh, LatticeT<typename Store<S>::C> L,
                                             const int8_t* __restrict__ fnew,
                                             const typename Store<S>::C* __restrict__ rhoR,
@@ -888,6 +916,10 @@ __global__ void __launch_bounds__(256) k_bb(PDev P, const double* __restrict__ p
   const C buz = C(2) / L.cssq;  // pref_bouzidi, dimensions_m.CUF:95
   double ola[3];
   lab_omega(P, pc, ola);
+  // the sphere's tile ranges (its tile-list coverage), once per CTA
+  __shared__ int tiles[12];
+  if (threadIdx.x == 0) tile_ranges(pc, nn3, P.rdim, tiles);
+  __syncthreads();
   double s[6] = {0, 0, 0, 0, 0, 0};
   // Past the sphere's own surface cells (pass 0), the reach holds its dead
   // cells and fluid cells, which no link crosses, unless another sphere's
@@ -921,7 +953,7 @@ __global__ void __launch_bounds__(256) k_bb(PDev P, const double* __restrict__ p
     const int ti = x0 / TILEX + 1, tj = y0 / TILEY + 1, tk = z0 / TILEZ + 1;
     // node -> particle momentum exchange for this sphere (atmDist < sphereMax)
     const bool n2p = (mode & BB_N2P) && dx * dx + dy * dy + dz * dz < P.sphereMax &&
-                     (!P.exact_tiles || tile_covered(pc, nn3, P.rdim, ti, tj, tk));
+                     (!P.exact_tiles || in_tile_ranges(tiles, ti, tj, tk));
     const bool own = (mode & (BB_COPY | BB_WALL)) && ow == a;
     if (!n2p && !own) continue;
     if (!likely) fl = nbr_fluid();
@@ -951,8 +983,7 @@ __global__ void __launch_bounds__(256) k_bb(PDev P, const double* __restrict__ p
         // the fluid end's population, or (wall phase alone) the copy already in place
         const S* p = (n2p || (mode & BB_COPY)) ? B + pidx(g, 0, lf, xf[it]) : B + pidx(g, 0, lr, cell);
         ld_two(p, hR[it], hB[it]);
-        rR[it] = rhoR[xf[it]];
-        rB[it] = rhoB[xf[it]];
+        ld_two(rhoR + 2 * size_t(xf[it]), rR[it], rB[it]);  // interleaved densities
         if (sh.sd) {  // sum / difference pairs: the wall term of each half is linear in its density
           const C t = rR[it];
           rR[it] = t + rB[it];
@@ -962,7 +993,7 @@ __global__ void __launch_bounds__(256) k_bb(PDev P, const double* __restrict__ p
     }
     if (n2p) {
       LinkGeo G;
-      link_geo_ol(P, g, pc, ola, i1, j1, k1, G);
+      own_link_geo(P, pc, c, ola, dx, dy, dz, G);
 #pragma unroll
       for (int it = 0; it < 9; ++it) {
         if (!(act >> it & 1)) continue;
@@ -999,9 +1030,10 @@ __global__ void __launch_bounds__(256) k_bb(PDev P, const double* __restrict__ p
           ej = get_delta(j1, nint_idx(pq[1], g.ny), g.ny, P.rdim),
           ek = get_delta(k1, nint_idx(pq[2], g.nz), g.nz, P.rdim);
       if (ei * ei + ej * ej + ek * ek >= P.sphereMax) continue;
-      if (P.exact_tiles && !tile_covered(pq, nn3, P.rdim, ti, tj, tk)) continue;
+      if (P.exact_tiles && !(q == a ? in_tile_ranges(tiles, ti, tj, tk) : tile_covered(pq, nn3, P.rdim, ti, tj, tk)))
+        continue;
       LinkGeo G;
-      if (q == a) link_geo_ol(P, g, pq, ola, i1, j1, k1, G);
+      if (q == a) own_link_geo(P, pc, c, ola, dx, dy, dz, G);  // (ei, ej, ek) is (dx, dy, dz) here
       else link_geo(P, g, pq, i1, j1, k1, G);
 #pragma unroll
       for (int it = 0; it < 9; ++it) {
