@@ -70,7 +70,7 @@ struct ParticleState {
   // second stream of the step's post stage: the pair forces and the
   // clearing of the previous flags run beside the bounce-back
   cudaStream_t aux = nullptr;
-  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_flags = nullptr;
 };
 
 struct PDev {  // by-value kernel argument
@@ -1588,7 +1588,8 @@ int particles_create(Ctx& c) {
   if (!ok(cudaMalloc(&s->nbr_cnt, size_t(cap) * 4))) return LBX_ERR_ALLOC;
   if (!ok(cudaStreamCreateWithFlags(&s->aux, cudaStreamNonBlocking)) ||
       !ok(cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming)) ||
-      !ok(cudaEventCreateWithFlags(&s->ev_join, cudaEventDisableTiming)))
+      !ok(cudaEventCreateWithFlags(&s->ev_join, cudaEventDisableTiming)) ||
+      !ok(cudaEventCreateWithFlags(&s->ev_flags, cudaEventDisableTiming)))
     return LBX_ERR_CUDA;
   if (!ok(cudaMalloc(&s->corr, size_t(cap) * NBCAP * 12 * 4))) return LBX_ERR_ALLOC;
   cudaMemsetAsync(s->acc, 0, size_t(cap) * AS * 8, c.stream);
@@ -1617,19 +1618,20 @@ void particles_destroy(Ctx& c) {
   if (s->corr) cudaFree(s->corr);
   if (s->ev_fork) cudaEventDestroy(s->ev_fork);
   if (s->ev_join) cudaEventDestroy(s->ev_join);
+  if (s->ev_flags) cudaEventDestroy(s->ev_flags);
   if (s->aux) cudaStreamDestroy(s->aux);
   delete s;
   c.part = nullptr;
 }
 
-static int rebuild_bins(Ctx& c, const double* pos) {
+static int rebuild_bins(Ctx& c, const double* pos, cudaStream_t st) {
   ParticleState& s = *c.part;
   PDev P = pdev(c);
   Geom g = geom(c);
   size_t nbins = size_t(s.nbx) * s.nby * s.nbz;
-  cudaMemsetAsync(s.bin_cnt, 0, nbins * 4, c.stream);
-  k_bins<<<(s.np * 32 + 255) / 256, 256, 0, c.stream>>>(P, pos, g, c.d_err, c.step + 1);
-  k_bins_sort<<<int((nbins + 255) / 256), 256, 0, c.stream>>>(P, int(nbins));
+  cudaMemsetAsync(s.bin_cnt, 0, nbins * 4, st);
+  k_bins<<<(s.np * 32 + 255) / 256, 256, 0, st>>>(P, pos, g, c.d_err, c.step + 1);
+  k_bins_sort<<<int((nbins + 255) / 256), 256, 0, st>>>(P, int(nbins));
   return launch_status();
 }
 
@@ -1682,7 +1684,7 @@ int particles_set(Ctx& c, int n, const double* h_x, const double* h_v, const dou
   // step-0 flags into the slot the first step will recompute; the slot the
   // first step treats as "previous" stays all fluid, as in the reference
   int slot = 1 - c.fcur;
-  int rc = rebuild_bins(c, s->pos[0]);
+  int rc = rebuild_bins(c, s->pos[0], c.stream);
   if (rc) return rc;
   // both flag slots all fluid (the step-0 flags go into `slot`)
   cudaMemsetAsync(c.flags[1 - slot], LBX_FLUID_FLUID, size_t(c.n), c.stream);
@@ -1715,27 +1717,31 @@ struct Stage {  // the buffers and constants every stage launch needs
 };
 }  // namespace
 
-int part_lists(Ctx& c) {
+static int lists_on(Ctx& c, cudaStream_t st) {
   Stage t(c);
-  return rebuild_bins(c, t.pc);
+  return rebuild_bins(c, t.pc, st);
 }
+
+int part_lists(Ctx& c) { return lists_on(c, c.stream); }
 
 int part_flags(Ctx& c) {
   Stage t(c);
   return compute_flags(c, t.pc, c.flags[t.fn], t.po);
 }
 
-int part_drain(Ctx& c) {
+static int drain_on(Ctx& c, cudaStream_t st) {
   Stage t(c);
   return by_storage(c, [&](auto* tag) {
     using S = std::remove_pointer_t<decltype(tag)>;
     using C = typename Store<S>::C;
-    k_drain<S><<<t.s.np, 256, 0, c.stream>>>(t.P, t.pc, t.po, t.s.acc, (const S*)c.pops[c.cur],
+    k_drain<S><<<t.s.np, 256, 0, st>>>(t.P, t.pc, t.po, t.s.acc, (const S*)c.pops[c.cur],
                                               (const S*)c.pops[1 - c.cur], t.g, make_shift<C>(c), c.flags[t.fo],
                                               c.flags[t.fn], (const C*)c.rho[0], (const C*)c.rho[1]);
     return launch_status();
   });
 }
+
+int part_drain(Ctx& c) { return drain_on(c, c.stream); }
 
 // init_rho*_CG with flags: every cell (two-pass schedule) or only the fluid
 // cells the particle kernels read (single-pass schedule, whose fluid kernel
@@ -1783,11 +1789,36 @@ int part_virtual(Ctx& c) {
   });
 }
 
+// With the single-pass schedule the stages that do not feed the next one run
+// on the second stream: the particle lists (read by the bounce-back only)
+// beside the flags, and the drain (it reads the densities of the cells the
+// spheres now cover, which the density shell does not write) beside the
+// density shell.  The fill adds to the same accumulators as the drain, after
+// it, and the fluid kernel's flags wait for nothing else: the join is before
+// the fill.  The two-pass schedule's density pass writes every cell, so it
+// keeps the reference's order on one stream.
 int particles_pre(Ctx& c) {
-  int rc = part_lists(c);
+  ParticleState& s = *c.part;
+  if (c.fused != 2) {
+    int rc = part_lists(c);
+    if (!rc) rc = part_flags(c);
+    if (!rc) rc = part_drain(c);
+    if (!rc) rc = part_rho(c);
+    if (!rc) rc = part_fill(c);
+    if (!rc) rc = part_virtual(c);
+    return rc;
+  }
+  if (cudaEventRecord(s.ev_fork, c.stream) != cudaSuccess || cudaStreamWaitEvent(s.aux, s.ev_fork, 0) != cudaSuccess)
+    return LBX_ERR_CUDA;
+  int rc = lists_on(c, s.aux);
   if (!rc) rc = part_flags(c);
-  if (!rc) rc = part_drain(c);
+  if (!rc && (cudaEventRecord(s.ev_flags, c.stream) != cudaSuccess ||
+              cudaStreamWaitEvent(s.aux, s.ev_flags, 0) != cudaSuccess))
+    rc = LBX_ERR_CUDA;
+  if (!rc) rc = drain_on(c, s.aux);
+  if (!rc && cudaEventRecord(s.ev_join, s.aux) != cudaSuccess) rc = LBX_ERR_CUDA;
   if (!rc) rc = part_rho(c);
+  if (!rc && cudaStreamWaitEvent(c.stream, s.ev_join, 0) != cudaSuccess) rc = LBX_ERR_CUDA;
   if (!rc) rc = part_fill(c);
   if (!rc) rc = part_virtual(c);
   return rc;
