@@ -149,6 +149,25 @@ __device__ __forceinline__ bool offset_cell(const PDev& P, const Geom& g, const 
          get_delta(k1, c[2], g.nz, P.rdim) == dz;
 }
 
+// whether the (2 rmax + 1)^3 box around centre c lies inside the lattice:
+// then no offset of the template lists (|d| <= rmax, and rdim <= rmax)
+// wraps, getDelta is the plain difference, and offset_cell is the sum c + d
+// for every offset
+__device__ __forceinline__ bool box_inside(const PDev& P, const Geom& g, const int c[3]) {
+  return c[0] - P.rmax >= 1 && c[0] + P.rmax <= g.nx && c[1] - P.rmax >= 1 && c[1] + P.rmax <= g.ny &&
+         c[2] - P.rmax >= 1 && c[2] + P.rmax <= g.nz;
+}
+__device__ __forceinline__ bool offset_cell_in(const PDev& P, const Geom& g, bool inside, const int c[3], int dx,
+                                               int dy, int dz, int& i1, int& j1, int& k1) {
+  if (inside) {
+    i1 = c[0] + dx;
+    j1 = c[1] + dy;
+    k1 = c[2] + dz;
+    return true;
+  }
+  return offset_cell(P, g, c, dx, dy, dz, i1, j1, k1);
+}
+
 // Tile-list coverage of makeListAtomsGPU: the reference's 8x4x4 tiles
 // (1-based indices) that hold particle position x in the list of the current
 // step, as two ranges [lo0, hi0] and [lo1, hi1] per axis (R[4 d + 0..3]).
@@ -341,11 +360,17 @@ __global__ void __launch_bounds__(256) k_stamp(PDev P, const double* __restrict_
   const double* p = pos + size_t(a) * PS;
   const int c[3] = {nint_idx(p[0], g.nx), nint_idx(p[1], g.ny), nint_idx(p[2], g.nz)};
   const int nn[3] = {g.nx, g.ny, g.nz};
+  const bool inside = box_inside(P, g, c);
+  __shared__ int tiles[12];  // the sphere's tile ranges, once per CTA
+  if (P.exact_tiles) {
+    if (threadIdx.x == 0) tile_ranges(p, nn, P.rdim, tiles);
+    __syncthreads();
+  }
   for (int t = threadIdx.x; t < P.n_solid; t += blockDim.x) {
     int dx, dy, dz, v, i1, j1, k1;
     unpack_off(P.offs[t], dx, dy, dz, v);
-    if (!offset_cell(P, g, c, dx, dy, dz, i1, j1, k1)) continue;
-    if (P.exact_tiles && !tile_covered(p, nn, P.rdim, (i1 - 1) / TILEX + 1, (j1 - 1) / TILEY + 1, (k1 - 1) / TILEZ + 1))
+    if (!offset_cell_in(P, g, inside, c, dx, dy, dz, i1, j1, k1)) continue;
+    if (P.exact_tiles && !in_tile_ranges(tiles, (i1 - 1) / TILEX + 1, (j1 - 1) / TILEY + 1, (k1 - 1) / TILEZ + 1))
       continue;
     atomicMin(reinterpret_cast<unsigned*>(P.owner) + cell0(g, i1, j1, k1), unsigned(a));
   }
@@ -356,10 +381,11 @@ __global__ void __launch_bounds__(256) k_stamp_flags(PDev P, const double* __res
   const int a = blockIdx.x;
   const double* p = pos + size_t(a) * PS;
   const int c[3] = {nint_idx(p[0], g.nx), nint_idx(p[1], g.ny), nint_idx(p[2], g.nz)};
+  const bool inside = box_inside(P, g, c);
   for (int t = threadIdx.x; t < P.n_solid; t += blockDim.x) {
     int dx, dy, dz, v, i1, j1, k1;
     unpack_off(P.offs[t], dx, dy, dz, v);
-    if (!offset_cell(P, g, c, dx, dy, dz, i1, j1, k1)) continue;
+    if (!offset_cell_in(P, g, inside, c, dx, dy, dz, i1, j1, k1)) continue;
     const int cell = cell0(g, i1, j1, k1);
     if (P.owner[cell] == a) flags_new[cell] = int8_t(v);
   }
@@ -374,10 +400,11 @@ __global__ void __launch_bounds__(256) k_unstamp(PDev P, const double* __restric
   const int a = blockIdx.x;
   const double* p = pos + size_t(a) * PS;
   const int c[3] = {nint_idx(p[0], g.nx), nint_idx(p[1], g.ny), nint_idx(p[2], g.nz)};
+  const bool inside = box_inside(P, g, c);
   for (int t = threadIdx.x; t < P.n_solid; t += blockDim.x) {
     int dx, dy, dz, v, i1, j1, k1;
     unpack_off(P.offs[t], dx, dy, dz, v);
-    if (!offset_cell(P, g, c, dx, dy, dz, i1, j1, k1)) continue;
+    if (!offset_cell_in(P, g, inside, c, dx, dy, dz, i1, j1, k1)) continue;
     const int cell = cell0(g, i1, j1, k1);
     if (flags) flags[cell] = LBX_FLUID_FLUID;
     if (owner) owner[cell] = -1;
