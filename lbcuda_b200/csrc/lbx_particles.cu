@@ -67,6 +67,7 @@ struct ParticleState {
   int* nbr = nullptr;         // np x NBCAP
   int* nbr_cnt = nullptr;
   float* corr = nullptr;      // np x NBCAP x 12
+  int8_t* crowd = nullptr;    // per sphere: another sphere's template can reach into its bounce-back reach
   // second stream of the step's post stage: the pair forces and the
   // clearing of the previous flags run beside the bounce-back
   cudaStream_t aux = nullptr;
@@ -93,6 +94,7 @@ struct PDev {  // by-value kernel argument
   int closure;
   float cl_gmin, cl_gmax, cl_vmax;
   int exact_tiles;
+  int8_t* crowd;  // k_crowd's vote per sphere, read by k_bb
 };
 
 // ---------------------------------------------------------------------------
@@ -928,6 +930,17 @@ __device__ bool crowded_reach(const PDev& P, const double* __restrict__ pos, con
   return __any_sync(0xffffffffu, hit);
 }
 
+// the vote once per sphere, after the lists are built (one warp per sphere),
+// so that the bounce-back starts from one byte instead of the bins
+__global__ void __launch_bounds__(256) k_crowd(PDev P, const double* __restrict__ pos, Geom g) {
+  const int a = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (a >= P.np) return;  // whole warps: np * 32 threads, rounded up to full CTAs
+  const double* p = pos + size_t(a) * PS;
+  const int c[3] = {nint_idx(p[0], g.nx), nint_idx(p[1], g.ny), nint_idx(p[2], g.nz)};
+  const bool hit = crowded_reach(P, pos, g, a, c);
+  if ((threadIdx.x & 31) == 0) P.crowd[a] = int8_t(hit);
+}
+
 template <typename S>
 __global__ void __launch_bounds__(256, sizeof(S) == 8 ? 1 : 2) k_bb(PDev P, const double* __restrict__ pos, double* acc, S* B, Geom g,
                                             Shift<typename Store<S>::C> sh, LatticeT<typename Store<S>::C> L,
@@ -950,8 +963,8 @@ __global__ void __launch_bounds__(256, sizeof(S) == 8 ? 1 : 2) k_bb(PDev P, cons
   double s[6] = {0, 0, 0, 0, 0, 0};
   // Past the sphere's own surface cells (pass 0), the reach holds its dead
   // cells and fluid cells, which no link crosses, unless another sphere's
-  // template reaches into it: pass 1 runs only then (a vote of each warp).
-  const bool crowd = crowded_reach(P, pos, g, a, c);
+  // template reaches into it: pass 1 runs only then (k_crowd's vote).
+  const bool crowd = P.crowd[a] != 0;
   for (int pass = 0; pass < 2; ++pass) {
   if (pass == 1 && !crowd) break;
   const int t0 = pass ? P.n_surf : 0, t1 = pass ? P.n_bb : P.n_surf;
@@ -1047,11 +1060,16 @@ __global__ void __launch_bounds__(256, sizeof(S) == 8 ? 1 : 2) k_bb(PDev P, cons
     if (!own) continue;
     // p2n phase 1: B(lr, cell) = B(lf, fluid end); lr and lf share their shift
     // p2n phase 2: moving-wall corrections of the spheres in reach
-    const int bin = bin_of(P, x0, y0, z0);
-    const int nlist = (mode & BB_WALL) ? min(P.bin_cnt[bin], BIN_CAP) : 0;
+    // A sphere no other template reaches (crowd false) is the only one of
+    // its bins within sphereMax of its surface cells: its rounded centre is at
+    // least rdim + sqrt(sphereMax) from every other listed centre (minimum
+    // image; getDelta's offsets are no shorter), and a surface cell is within
+    // rdim of its own.  The walk is then the sphere itself.
+    const int bin = crowd ? bin_of(P, x0, y0, z0) : 0;
+    const int nlist = !(mode & BB_WALL) ? 0 : crowd ? min(P.bin_cnt[bin], BIN_CAP) : 1;
     const int* Lst = P.bin_list + size_t(bin) * BIN_CAP;
     for (int u = 0; u < nlist; ++u) {
-      const int q = Lst[u];
+      const int q = crowd ? Lst[u] : a;
       const double* pq = pos + size_t(q) * PS;
       int ei = get_delta(i1, nint_idx(pq[0], g.nx), g.nx, P.rdim),
           ej = get_delta(j1, nint_idx(pq[1], g.ny), g.ny, P.rdim),
@@ -1501,6 +1519,7 @@ static PDev pdev(const Ctx& c) {
   d.cl_gmax = c.p.closure_gap_max;
   d.cl_vmax = c.p.closure_vmax;
   d.exact_tiles = c.p.exact_tiles;
+  d.crowd = s.crowd;
   return d;
 }
 
@@ -1613,6 +1632,7 @@ int particles_create(Ctx& c) {
   if (!ok(cudaMalloc(&s->wclosure, size_t(LBX_CLOSURE_NWEIGHTS) * 4))) return LBX_ERR_ALLOC;
   if (!ok(cudaMalloc(&s->nbr, size_t(cap) * NBCAP * 4))) return LBX_ERR_ALLOC;
   if (!ok(cudaMalloc(&s->nbr_cnt, size_t(cap) * 4))) return LBX_ERR_ALLOC;
+  if (!ok(cudaMalloc(&s->crowd, size_t(cap)))) return LBX_ERR_ALLOC;
   if (!ok(cudaStreamCreateWithFlags(&s->aux, cudaStreamNonBlocking)) ||
       !ok(cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming)) ||
       !ok(cudaEventCreateWithFlags(&s->ev_join, cudaEventDisableTiming)) ||
@@ -1642,6 +1662,7 @@ void particles_destroy(Ctx& c) {
   if (s->wclosure) cudaFree(s->wclosure);
   if (s->nbr) cudaFree(s->nbr);
   if (s->nbr_cnt) cudaFree(s->nbr_cnt);
+  if (s->crowd) cudaFree(s->crowd);
   if (s->corr) cudaFree(s->corr);
   if (s->ev_fork) cudaEventDestroy(s->ev_fork);
   if (s->ev_join) cudaEventDestroy(s->ev_join);
@@ -1659,6 +1680,7 @@ static int rebuild_bins(Ctx& c, const double* pos, cudaStream_t st) {
   cudaMemsetAsync(s.bin_cnt, 0, nbins * 4, st);
   k_bins<<<(s.np * 32 + 255) / 256, 256, 0, st>>>(P, pos, g, c.d_err, c.step + 1);
   k_bins_sort<<<int((nbins + 255) / 256), 256, 0, st>>>(P, int(nbins));
+  k_crowd<<<(s.np * 32 + 255) / 256, 256, 0, st>>>(P, pos, g);
   return launch_status();
 }
 
