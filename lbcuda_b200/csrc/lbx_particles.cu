@@ -583,7 +583,11 @@ __global__ void __launch_bounds__(256) k_rho_shell(PDev P, const double* __restr
                                                    const int8_t* __restrict__ fnew, typename Store<S>::C* rhoR,
                                                    typename Store<S>::C* rhoB) {
   using C = typename Store<S>::C;
-  const int a = blockIdx.x;
+  // spheres in reverse order: the bounce-back before this kernel (the end of
+  // the previous step) rewrote the belts' links sphere by sphere in
+  // ascending order, so the last ones are still in L2 (the values do not
+  // depend on the order: a cell in two belts gets the same sums)
+  const int a = P.np - 1 - int(blockIdx.x);
   const double* pc = pos_cur + size_t(a) * PS;
   const double* po = pos_old + size_t(a) * PS;
   const int cn[3] = {nint_idx(pc[0], g.nx), nint_idx(pc[1], g.ny), nint_idx(pc[2], g.nz)};
