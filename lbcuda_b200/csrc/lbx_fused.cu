@@ -1127,7 +1127,7 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
     // otherwise planes z-1 and z before the wait (written before the previous
     // plane's barrier, rewritten only after this one) and z+1 after it.
     const int cell = x + g.nx * (y + g.ny * z);
-    bool collide = true, fresh = false;
+    bool collide = true;
     C px = 0, py = 0, pz = 0;
     Relaxed<C> rx;
     if (active) {
@@ -1140,22 +1140,21 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
           } else {
             flags_of(side + qz * NT + tid, cell, fn, fo);
           }
-          // a solid cell keeps the plain pull (see below)
+          // a solid cell keeps the plain pull (see below); a cell that
+          // turns fluid pulls the populations make_fluid wrote into the
+          // slots it pulls from
           collide = fn == LBX_FLUID_FLUID;
-          // make_fluid already wrote a new node's populations (stored form) into B
-          fresh = collide && fo != LBX_FLUID_FLUID;
         }
       }
     }
     // Stored pairs of this cell: the pull (in the stage since two
-    // iterations, or issued here), or a new node's populations in B.
+    // iterations, or issued here).
     const SR* const zb = BOXED ? box_slot(qz) + obase : nullptr;
     auto pulled = [&](int l) -> SR {
       if constexpr (BOXED) return zb[l * BX::ELEMS - ex(l)];
       else if constexpr (STAGED) return own_slot(qz)[l * NT];
       else return SPair<S>::ldr(Ap.at(l, pull_one(g, x, y, z, l)));
     };
-    auto refilled = [&](int l) -> SR { return SPair<S>::ldr(Bp.at(l, cell)); };
     if (active && collide) {
       // the colour gradient from planes z-1 and z (synchronous pulls only),
       // then the BGK half
@@ -1177,12 +1176,6 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
       C Ssum[Q];
 #pragma unroll
       for (int l = 0; l < Q; ++l) Ssum[l] = SD ? SPair<S>::first(pulled(l)) : SPair<S>::sum(pulled(l));
-      if constexpr (PART) {
-        if (fresh) {
-#pragma unroll
-          for (int l = 0; l < Q; ++l) Ssum[l] = SD ? SPair<S>::first(refilled(l)) : SPair<S>::sum(refilled(l));
-        }
-      }
       rx = relax_sums(K, Ssum, rRc, rBc, Store<S>::shifted);
     }
     if (!mbar_wait(bar, sy.bar)) raise_error(err, LBX_DEV_WAIT_TIMEOUT, step, -1);
@@ -1244,12 +1237,6 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
           const C ph = spl[qz * NT + tid];
 #pragma unroll
           for (int l = 0; l < Q; ++l) gp[l].y = fm(ph, gp[l].x + K.ssd[0][wclass(l)], gp[l].y);
-        }
-        if constexpr (PART) {
-          if (fresh) {
-#pragma unroll
-            for (int l = 0; l < Q; ++l) gp[l] = SPair<S>::cvt(refilled(l));
-          }
         }
         if (collide) {
           if constexpr (SD) bgk_components<C, STAGED, true>(K, rx, rRc + rBc, rRc - rBc, Store<S>::shifted, gp);

@@ -618,14 +618,18 @@ __global__ void __launch_bounds__(256) k_rho_shell(PDev P, const double* __restr
 // make_fluid: cells solid in the previous step and fluid now get the mean
 // density of their fluid neighbours (D3Q27 belt, then the 98-cell second
 // belt) and the equilibrium at the sphere's velocity; the sphere pays the
-// momentum.
+// momentum.  The populations go where the fluid step reads them: with the
+// two-pass schedule into B at the cell (its collision reads a new cell
+// there), with the single-pass kernel (pulls != nullptr, the populations A
+// of this step) into the slots the cell pulls from, A(l, x - e_l): only cell
+// x pulls each of them, so the fluid kernel needs no case for new cells.
 template <typename S>
 __global__ void __launch_bounds__(256) k_fill(PDev P, const double* __restrict__ pos_cur,
-                                              const double* __restrict__ pos_old, double* acc, const S* A, S* B, Geom g,
-                                              Shift<typename Store<S>::C> sh, LatticeT<typename Store<S>::C> L,
-                                              const int8_t* __restrict__ fold, const int8_t* __restrict__ fnew,
-                                              typename Store<S>::C* rhoR, typename Store<S>::C* rhoB,
-                                              typename Store<S>::C* phi) {
+                                              const double* __restrict__ pos_old, double* acc, const S* A, S* B,
+                                              S* pulls, Geom g, Shift<typename Store<S>::C> sh,
+                                              LatticeT<typename Store<S>::C> L, const int8_t* __restrict__ fold,
+                                              const int8_t* __restrict__ fnew, typename Store<S>::C* rhoR,
+                                              typename Store<S>::C* rhoB, typename Store<S>::C* phi) {
   using C = typename Store<S>::C;
   const int a = blockIdx.x;
   const double* pc = pos_cur + size_t(a) * PS;
@@ -674,12 +678,16 @@ __global__ void __launch_bounds__(256) k_fill(PDev P, const double* __restrict__
     rhoB[2 * size_t(cell)] = Bs;
     phi[cell] = (Rs - Bs) / (Rs + Bs);
     C usq = L.half_inv_cssq * (u * u + v * v + w * w);
+    Nbr b;
+    make_nbr(g, i1 - 1, j1 - 1, k1 - 1, b);
     for (int comp = 0; comp < 2; ++comp) {
       // sum / difference pairs store the equilibria of rho and rhoR - rhoB
       C r = sh.sd ? (comp ? Rs - Bs : Rs + Bs) : (comp ? Bs : Rs);
 #pragma unroll
-      for (int l = 0; l < Q; ++l)
-        Store<S>::st(B + pidx(g, comp, l, cell), equil_u(L, r, edot(l, u, v, w), usq, l), sh.at(comp, l));
+      for (int l = 0; l < Q; ++l) {
+        S* dst = pulls ? pulls + pidx(g, comp, l, at(b, -ex(l), -ey(l), -ez(l))) : B + pidx(g, comp, l, cell);
+        Store<S>::st(dst, equil_u(L, r, edot(l, u, v, w), usq, l), sh.at(comp, l));
+      }
     }
     double ft[3] = {double(-(Rs + Bs) * u), double(-(Rs + Bs) * v), double(-(Rs + Bs) * w)};
     s[0] += ft[0]; s[1] += ft[1]; s[2] += ft[2];
@@ -1823,8 +1831,9 @@ int part_fill(Ctx& c) {
     using S = std::remove_pointer_t<decltype(tag)>;
     using C = typename Store<S>::C;
     k_fill<S><<<t.s.np, 256, 0, c.stream>>>(t.P, t.pc, t.po, t.s.acc, (const S*)c.pops[c.cur], (S*)c.pops[1 - c.cur],
-                                             t.g, make_shift<C>(c), make_lattice<C>(), c.flags[t.fo], c.flags[t.fn],
-                                             (C*)c.rho[0], (C*)c.rho[1], (C*)c.phi);
+                                             c.fused == 2 ? (S*)c.pops[c.cur] : nullptr, t.g, make_shift<C>(c),
+                                             make_lattice<C>(), c.flags[t.fo], c.flags[t.fn], (C*)c.rho[0],
+                                             (C*)c.rho[1], (C*)c.phi);
     return launch_status();
   });
 }
