@@ -1226,7 +1226,9 @@ __device__ __forceinline__ void lean_column(const S* __restrict__ A, S* __restri
         // instructions per cell with the other changes of the box staging).
         // With spheres one store after the merge measured faster (838
         // against 856 instructions per cell, 111 against 114 us at 128^3 with
-        // 160 spheres), and the persistent multi-box kernel would spill.
+        // 160 spheres; without the new-cell case 827 against 817 and 110 us
+        // both, but 691 against 701 us at 256^3 with 1280 spheres), and the
+        // persistent multi-box kernel would spill.
         if constexpr (SPLIT_STORE)
           if (done) store_all(gp);
       }
