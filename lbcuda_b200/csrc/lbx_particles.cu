@@ -71,7 +71,10 @@ struct ParticleState {
   // second stream of the step's post stage: the pair forces and the
   // clearing of the previous flags run beside the bounce-back
   cudaStream_t aux = nullptr;
-  cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_flags = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_flags = nullptr, ev_owner = nullptr;
+  // the owners of the last stamping are already cleared (the end of the
+  // step did it beside the integrator): the next flag stage skips that
+  int owner_clear = 0;
 };
 
 struct PDev {  // by-value kernel argument
@@ -1648,7 +1651,8 @@ int particles_create(Ctx& c) {
   if (!ok(cudaStreamCreateWithFlags(&s->aux, cudaStreamNonBlocking)) ||
       !ok(cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming)) ||
       !ok(cudaEventCreateWithFlags(&s->ev_join, cudaEventDisableTiming)) ||
-      !ok(cudaEventCreateWithFlags(&s->ev_flags, cudaEventDisableTiming)))
+      !ok(cudaEventCreateWithFlags(&s->ev_flags, cudaEventDisableTiming)) ||
+      !ok(cudaEventCreateWithFlags(&s->ev_owner, cudaEventDisableTiming)))
     return LBX_ERR_CUDA;
   if (!ok(cudaMalloc(&s->corr, size_t(cap) * NBCAP * 12 * 4))) return LBX_ERR_ALLOC;
   cudaMemsetAsync(s->acc, 0, size_t(cap) * AS * 8, c.stream);
@@ -1679,6 +1683,7 @@ void particles_destroy(Ctx& c) {
   if (s->ev_fork) cudaEventDestroy(s->ev_fork);
   if (s->ev_join) cudaEventDestroy(s->ev_join);
   if (s->ev_flags) cudaEventDestroy(s->ev_flags);
+  if (s->ev_owner) cudaEventDestroy(s->ev_owner);
   if (s->aux) cudaStreamDestroy(s->aux);
   delete s;
   c.part = nullptr;
@@ -1705,11 +1710,12 @@ static int compute_flags(Ctx& c, const double* pos, int8_t* flags, const double*
   PDev P = pdev(c);
   Geom g = geom(c);
   if (prev) {
-    k_unstamp<<<s.np, 256, 0, c.stream>>>(P, prev, g, nullptr, s.owner);
+    if (!s.owner_clear) k_unstamp<<<s.np, 256, 0, c.stream>>>(P, prev, g, nullptr, s.owner);
   } else {
     cudaMemsetAsync(flags, LBX_FLUID_FLUID, size_t(c.n), c.stream);
     cudaMemsetAsync(s.owner, 0xFF, size_t(c.n) * 4, c.stream);
   }
+  s.owner_clear = 0;
   k_stamp<<<s.np, 256, 0, c.stream>>>(P, pos, g);
   k_stamp_flags<<<s.np, 256, 0, c.stream>>>(P, pos, g, flags);
   return launch_status();
@@ -1984,7 +1990,11 @@ int part_integrate(Ctx& c) {
 // the pair forces (accumulators of their own, acc[6..14], against acc[0..5]
 // of the bounce-back) and the clearing of the previous step's flags (the
 // bounce-back reads this step's); both join before the integrator, which
-// overwrites the previous positions the clearing reads.
+// overwrites the previous positions the clearing reads.  After the
+// bounce-back, the last reader of the owners, the second stream clears them
+// at this step's positions beside the integrator (which writes the next
+// positions, not these), joined at the end of the step; the next flag stage
+// then stamps without clearing first.
 int particles_post(Ctx& c) {
   ParticleState& s = *c.part;
   if (cudaEventRecord(s.ev_fork, c.stream) != cudaSuccess || cudaStreamWaitEvent(s.aux, s.ev_fork, 0) != cudaSuccess)
@@ -1993,8 +2003,19 @@ int particles_post(Ctx& c) {
   if (!rc) rc = unstamp_on(c, s.aux);
   if (!rc && cudaEventRecord(s.ev_join, s.aux) != cudaSuccess) rc = LBX_ERR_CUDA;
   if (!rc) rc = part_bb(c, BB_ALL);
+  if (!rc && (cudaEventRecord(s.ev_flags, c.stream) != cudaSuccess ||
+              cudaStreamWaitEvent(s.aux, s.ev_flags, 0) != cudaSuccess))
+    rc = LBX_ERR_CUDA;
+  if (!rc) {
+    Stage t(c);
+    k_unstamp<<<s.np, 256, 0, s.aux>>>(t.P, t.pc, t.g, nullptr, s.owner);
+    rc = launch_status();
+  }
+  if (!rc && cudaEventRecord(s.ev_owner, s.aux) != cudaSuccess) rc = LBX_ERR_CUDA;
   if (!rc && cudaStreamWaitEvent(c.stream, s.ev_join, 0) != cudaSuccess) rc = LBX_ERR_CUDA;
   if (!rc) rc = integrate_flip(c);
+  if (!rc && cudaStreamWaitEvent(c.stream, s.ev_owner, 0) != cudaSuccess) rc = LBX_ERR_CUDA;
+  if (!rc) s.owner_clear = 1;
   return rc;
 }
 
