@@ -29,8 +29,8 @@ struct WorkItem;
 template <typename C> LeanConst<C> make_lean(const Ctx& c);
 
 int particles_active(const Ctx& c);
-int particles_pre(Ctx& c);
-int particles_post(Ctx& c);
+int particles_pre(Ctx& c, bool forks);
+int particles_post(Ctx& c, bool forks);
 
 // implemented in lbx_fused.cu
 int ensemble_launch(const std::vector<Ctx*>& boxes, int shape, const std::vector<int>& zlen, void* d_desc,
@@ -102,14 +102,15 @@ int step_once(Ensemble& e, cudaEvent_t ta = nullptr, cudaEvent_t tb = nullptr) {
   const int parity = e.boxes[0]->cur;
   for (auto* c : e.boxes)
     if (c->cur != parity) return LBX_ERR_STATE;  // boxes must be stepped together
-  int rc = boxes_side_by_side(e, [](lbx::Ctx& c) { return lbx::particles_pre(c); });
+  // each box's sphere stages on its own stream only (no second stream per box)
+  int rc = boxes_side_by_side(e, [](lbx::Ctx& c) { return lbx::particles_pre(c, false); });
   if (rc) return rc;
   if (ta) cudaEventRecord(ta, e.stream);
   rc = lbx::ensemble_launch(e.boxes, e.shape, e.zlen, e.d_desc[parity], e.d_work[parity], e.nwork, e.stream, 0,
                             parity);
   if (tb) cudaEventRecord(tb, e.stream);
   if (rc) return rc;
-  rc = boxes_side_by_side(e, [](lbx::Ctx& c) { return lbx::particles_post(c); });
+  rc = boxes_side_by_side(e, [](lbx::Ctx& c) { return lbx::particles_post(c, false); });
   if (rc) return rc;
   for (auto* c : e.boxes)
     if (!lbx::particles_active(*c)) {
