@@ -1870,6 +1870,10 @@ int part_virtual(Ctx& c) {
 // against 1.38 ms per step with 48 boxes).
 int particles_pre(Ctx& c, bool forks) {
   ParticleState& s = *c.part;
+  // without forks the step's end clears no owners, and a graph captured
+  // from these stages replays them unchanged: clear them here every time
+  // (again, if a step with forks already did; clearing is idempotent)
+  if (!forks) s.owner_clear = 0;
   if (c.fused != 2 || !forks) {
     int rc = part_lists(c);
     if (!rc) rc = part_flags(c);
