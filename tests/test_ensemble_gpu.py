@@ -62,3 +62,39 @@ def test_ensemble_tuner_keeps_results_consistent():
         m, _ = b.get_sums()
         assert np.isfinite(m).all()
     ens.close()
+
+
+def test_ensemble_after_a_box_stepped_alone():
+    """A box stepped by itself (the single-box step clears its spheres' owners at the end of the step and
+    records that on the host) and then with the ensemble (whose captured graph replays its sphere stages
+    without that record) still equals the same box advanced alone throughout; the spheres move across cells,
+    so stale owners would change the flags."""
+    spec = random_boxes(4, seed=11, edges=(32, 48), max_spheres=5)
+    params = [_params(L, len(x), "f16sd") for L, x in spec]
+    ens = Ensemble(params)
+    alone = []
+    for i, ((L, x), p) in enumerate(zip(spec, params)):
+        rR, rB = seeded_noise_fields(L, L, L, seed=30 + i)
+        v = np.full_like(x, 0.1)
+        for sim in (ens.boxes[i], None):
+            if sim is None:
+                sim = LBSim(p)
+                alone.append(sim)
+            sim.set_fields(rR, rB)
+            if len(x):
+                sim.set_particles(x, v)
+    for b in ens.boxes:
+        b.step(3)
+    ens.step(9)
+    for s in alone:
+        s.step(12)
+    for i, s in enumerate(alone):
+        assert ens.boxes[i].status()[0] == 0 and s.status()[0] == 0
+        assert np.array_equal(ens.boxes[i].get_flags(), s.get_flags()), i
+        for fa, fb in zip(ens.boxes[i].get_fields(), s.get_fields()):
+            assert np.array_equal(fa, fb), i
+        if len(spec[i][1]):
+            assert np.array_equal(ens.boxes[i].get_particles()["x"], s.get_particles()["x"]), i
+    ens.close()
+    for s in alone:
+        s.close()
