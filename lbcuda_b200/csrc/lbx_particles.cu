@@ -1379,8 +1379,11 @@ __global__ void k_closure_accum(PDev P, const int* __restrict__ nbr, const int* 
 // f_bb(t-1/2))/2, leap-frog translation with the centred periodic image,
 // the implicit mid-step quaternion update, then the accumulators restart
 // from the external force and torque.
-__global__ void k_integrate(PDev P, const double* __restrict__ pos_cur, double* pos_next, double* frc_cur,
-                            double* frc_next, double* acc, Geom g, unsigned long long* err, int64_t step) {
+// the five records are distinct allocations (the two position and force
+// slots and the accumulators): no store aliases a later load
+__global__ void k_integrate(PDev P, const double* __restrict__ pos_cur, double* __restrict__ pos_next,
+                            double* __restrict__ frc_cur, double* __restrict__ frc_next, double* __restrict__ acc,
+                            Geom g, unsigned long long* err, int64_t step) {
   int a = blockIdx.x * blockDim.x + threadIdx.x;
   if (a >= P.np) return;
   const double* pc = pos_cur + size_t(a) * PS;
