@@ -713,7 +713,7 @@ __global__ void __launch_bounds__(256) k_fill(PDev P, const double* __restrict__
 // virtual densities of the surface cells a sphere owns: Janus
 // (compute_virtual_rho) or neutral wetting (compute_densities_wall)
 template <typename S, typename C = typename Store<S>::C>
-__global__ void __launch_bounds__(256) k_virtual(PDev P, const double* __restrict__ pos, Geom g, int neutral,
+__global__ void __launch_bounds__(256, 3) k_virtual(PDev P, const double* __restrict__ pos, Geom g, int neutral,
                                                  const S* A, Shift<C> sh,
                                                  const int8_t* __restrict__ fold, const int8_t* __restrict__ fnew,
                                                  C* rhoR, C* rhoB, C* phi, LatticeT<C> L) {
@@ -743,13 +743,34 @@ __global__ void __launch_bounds__(256) k_virtual(PDev P, const double* __restric
       if (cs < 0.0) { R = 0; Bv = 1; }
       else { R = 1; Bv = 0; }
     } else {
+      // compute_onebelt_density_2fl_weights, nine neighbours at a time (the
+      // periodic rows and planes of the cell from make_nbr): their flags, the
+      // fluid ones' densities, then the sums in ascending direction order
+      Nbr b;
+      make_nbr(g, i1 - 1, j1 - 1, k1 - 1, b);
       C Rs = 0, Bs = 0, Ds = 0;
-      for (int l = 1; l < Q27; ++l) {  // compute_onebelt_density_2fl_weights
-        int yi = wrap1(i1 + ex27(l), g.nx), yj = wrap1(j1 + ey27(l), g.ny), yk = wrap1(k1 + ez27(l), g.nz);
-        int y = cell0(g, yi, yj, yk);
-        if (fnew[y] == LBX_FLUID_FLUID) {
-          C w = L.p27[wclass27(l)];
-          Rs = Rs + w * rhoR[2 * size_t(y)]; Bs = Bs + w * rhoB[2 * size_t(y)]; Ds = Ds + w;
+#pragma unroll
+      for (int l0 = 1; l0 < Q27; l0 += 9) {
+        bool fl[9];
+        C vr[9], vb[9];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) {
+          const int l = l0 + k;
+          fl[k] = l < Q27 && fnew[at(b, ex27(l), ey27(l), ez27(l))] == LBX_FLUID_FLUID;
+        }
+#pragma unroll
+        for (int k = 0; k < 9; ++k) {
+          const int l = l0 + k;
+          vr[k] = vb[k] = C(0);
+          if (l < Q27 && fl[k]) ld_two(rhoR + 2 * size_t(at(b, ex27(l), ey27(l), ez27(l))), vr[k], vb[k]);
+        }
+#pragma unroll
+        for (int k = 0; k < 9; ++k) {
+          const int l = l0 + k;
+          if (l < Q27 && fl[k]) {
+            C w = L.p27[wclass27(l)];
+            Rs = Rs + w * vr[k]; Bs = Bs + w * vb[k]; Ds = Ds + w;
+          }
         }
       }
       if (Ds != C(0)) { R = Rs / Ds; Bv = Bs / Ds; }
